@@ -1,0 +1,127 @@
+"""ctypes mirror of ``include/gridsim_b200.h`` and the loader of the in-tree engine library.
+
+The structures below must match the header field for field; ``tests/test_abi.py`` checks the exported
+symbol list against the header. Loading fails loudly when the shared library is missing: there is no
+fallback path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgridsim_b200.so")
+
+c_i32, c_f64, c_u8, c_vp = ctypes.c_int32, ctypes.c_double, ctypes.c_uint8, ctypes.c_void_p
+
+GS_OK, GS_ERR_INVALID_ARG, GS_ERR_CUDA, GS_ERR_OOM, GS_ERR_NO_DEVICE = 0, 1, 2, 3, 4
+GS_ERR_TIMEOUT, GS_ERR_STATE, GS_ERR_UNSUPPORTED, GS_ERR_INTERNAL, GS_ERR_CAPACITY = 5, 6, 7, 8, 9
+
+PF_CONVERGED, PF_MAX_ITERATIONS, PF_NON_FINITE, PF_DIVERGED, PF_SINGULAR_PIVOT, PF_TIMEOUT, PF_NOT_RUN = range(7)
+PF_STATUS_NAMES = ["Converged", "MaxIterations", "NonFinite", "Diverged", "SingularPivot", "Timeout", "NotRun"]
+
+PREC_FP64, PREC_MIXED = 0, 1
+VIOL_BRANCH_OVERLOAD, VIOL_BOUNDARY_OVERLOAD, VIOL_UNDERVOLTAGE, VIOL_OVERVOLTAGE = 0, 1, 2, 3
+
+
+class CtxOpts(ctypes.Structure):
+    _fields_ = [("probe_timeout_ms", c_i32), ("reserved", c_i32 * 7)]
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [
+        ("n_bus", c_i32), ("n_gen", c_i32), ("n_branch", c_i32), ("reserved0", c_i32), ("base_mva", c_f64),
+        ("bus_id", c_vp), ("bus_type", c_vp), ("pd", c_vp), ("qd", c_vp), ("gs", c_vp), ("bs", c_vp),
+        ("vm", c_vp), ("va_deg", c_vp), ("vmin_pu", c_vp), ("vmax_pu", c_vp),
+        ("gen_bus", c_vp), ("pg", c_vp), ("qg", c_vp), ("vg", c_vp), ("qmin", c_vp), ("qmax", c_vp),
+        ("gen_in_service", c_vp),
+        ("br_from", c_vp), ("br_to", c_vp), ("r", c_vp), ("x", c_vp), ("b", c_vp), ("tap", c_vp),
+        ("shift_deg", c_vp), ("rate_a", c_vp), ("br_in_service", c_vp),
+    ]
+
+
+class PfOpts(ctypes.Structure):
+    _fields_ = [
+        ("tolerance", c_f64), ("diverge_limit_pu", c_f64), ("max_iterations", c_i32), ("flat_start", c_i32),
+        ("enforce_q_limits", c_i32), ("retry_from_dc_start", c_i32), ("per_bus_voltage_limits", c_i32),
+        ("precision", c_i32), ("warm_start_from_base", c_i32), ("batch_width", c_i32), ("reserved", c_i32 * 8),
+    ]
+
+
+class PfResult(ctypes.Structure):
+    _fields_ = [
+        ("status", c_i32), ("iterations", c_i32), ("max_mismatch", c_f64),
+        ("vm", c_vp), ("va_deg", c_vp), ("p_inj_mw", c_vp), ("q_inj_mvar", c_vp), ("loading_pct", c_vp),
+        ("sf_mva", c_vp), ("st_mva", c_vp),
+    ]
+
+
+class N1Result(ctypes.Structure):
+    _fields_ = [
+        ("status", c_vp), ("iterations", c_vp), ("max_mismatch", c_vp), ("min_vm", c_vp), ("max_vm", c_vp),
+        ("max_loading_pct", c_vp), ("viol_ptr", c_vp), ("viol_capacity", c_i32), ("viol_count", c_i32),
+        ("viol_kind", c_vp), ("viol_element", c_vp), ("viol_value", c_vp), ("vm", c_vp), ("va_deg", c_vp),
+        ("base_status", c_i32), ("base_iterations", c_i32), ("device_ms", c_f64), ("n_singular_pivot", c_i32),
+        ("n_batches", c_i32),
+    ]
+
+
+class GridInfo(ctypes.Structure):
+    _fields_ = [
+        ("n_bus", c_i32), ("n_branch", c_i32), ("n_pv", c_i32), ("n_pq", c_i32), ("m", c_i32), ("nnz_y", c_i32),
+        ("nnz_j", c_i32), ("nnz_lu", ctypes.c_int64), ("lu_flops", ctypes.c_int64), ("n_levels", c_i32),
+        ("reserved", c_i32 * 7),
+    ]
+
+
+# Every entry point the header declares, with its ctypes signature.
+EXPORTS = {
+    "gs_abi_version": (c_i32, []),
+    "gs_status_str": (ctypes.c_char_p, [c_i32]),
+    "gs_pf_opts_default": (None, [ctypes.POINTER(PfOpts)]),
+    "gs_ctx_create": (c_i32, [c_i32, ctypes.POINTER(CtxOpts), ctypes.POINTER(c_vp)]),
+    "gs_ctx_destroy": (c_i32, [c_vp]),
+    "gs_last_error": (c_i32, [c_vp, ctypes.c_char_p, ctypes.c_size_t]),
+    "gs_grid_create": (c_i32, [c_vp, ctypes.POINTER(GridDesc), ctypes.POINTER(c_vp)]),
+    "gs_grid_destroy": (c_i32, [c_vp]),
+    "gs_grid_info_get": (c_i32, [c_vp, ctypes.POINTER(GridInfo)]),
+    "gs_pf_solve": (c_i32, [c_vp, ctypes.POINTER(PfOpts), ctypes.POINTER(PfResult)]),
+    "gs_pf_solve_batch": (c_i32, [c_vp, c_i32, c_vp, c_vp, ctypes.POINTER(PfOpts), c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "gs_n1_screen": (c_i32, [c_vp, c_i32, c_vp, ctypes.POINTER(PfOpts), ctypes.POINTER(N1Result)]),
+}
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the engine library (once). Raises if it has not been built: there is no CPU fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"gridsim_b200 engine library not built: {path} is missing "
+                           "(run __graft_entry__.build() or python -m gridsim_b200.build)")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in EXPORTS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def default_opts() -> PfOpts:
+    """PowerFlowOptions() defaults (``PowerFlow/PowerFlowOptions.cs``), written here so that option
+    handling works without loading the engine."""
+    o = PfOpts()
+    o.tolerance = 1e-8
+    o.diverge_limit_pu = 10.0
+    o.max_iterations = 30
+    o.flat_start = 0
+    o.enforce_q_limits = 0
+    o.retry_from_dc_start = 0
+    o.per_bus_voltage_limits = 0
+    o.precision = PREC_FP64
+    o.warm_start_from_base = 0
+    o.batch_width = 0
+    return o

@@ -1,0 +1,312 @@
+"""Grid model and the two case formats the load-flow path reads.
+
+``GridModel`` holds the fields of GridSim's ``GridModel`` that the load flow uses (Bus
+``src/GridSim.Core/Model/Model.cs:20-35``, Generator ``:91-114``, Branch ``:253-275``) as flat numpy
+arrays, in model order. Bus references inside the arrays are 0-based positions; ``bus_id`` keeps the
+external ids (the key of voltage violations).
+
+Loaders:
+
+* :func:`load_matpower` — MATPOWER ``.m`` files, following ``IO/Matpower/MatpowerParser.cs:128-401``:
+  isolated (type 4) buses and out-of-service branches are dropped with everything incident to them,
+  out-of-service generators are kept but not solved, a PV bus with no in-service generator is solved
+  as PQ, VMAX/VMIN become the bus's own limits, TAP 0 means a line (ratio 1).
+* :func:`load_case_dir` / :func:`save_case_dir` — GridSim's v1 JSON case directory
+  (``IO/Json/JsonGridLoader.cs:55-255``): ``system.json``, ``buses.json``, ``generation.json``,
+  ``demand.json``, ``transmission.json``. Only the keys this path needs are read; ``"dispatch": false``
+  keeps the written generator outputs (``:254``), which is what every case written here uses.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import math
+import os
+import re
+from dataclasses import dataclass, field
+
+import numpy as np
+
+PQ, PV, SLACK = 1, 2, 3
+
+
+@dataclass
+class GridModel:
+    name: str
+    base_mva: float
+    # buses
+    bus_id: np.ndarray
+    bus_type: np.ndarray
+    pd: np.ndarray
+    qd: np.ndarray
+    gs: np.ndarray
+    bs: np.ndarray
+    vm: np.ndarray
+    va_deg: np.ndarray
+    vmin: np.ndarray  # NaN = no own limit
+    vmax: np.ndarray
+    base_kv: np.ndarray
+    # generators
+    gen_bus: np.ndarray  # bus positions
+    pg: np.ndarray
+    qg: np.ndarray
+    vg: np.ndarray
+    qmin: np.ndarray
+    qmax: np.ndarray
+    gen_in_service: np.ndarray
+    # branches
+    br_from: np.ndarray  # bus positions
+    br_to: np.ndarray
+    r: np.ndarray
+    x: np.ndarray
+    b: np.ndarray
+    tap: np.ndarray
+    shift_deg: np.ndarray
+    rate_a: np.ndarray
+    br_in_service: np.ndarray
+    is_transformer: np.ndarray
+    _keep: list = field(default_factory=list, repr=False)
+
+    @property
+    def n_bus(self) -> int:
+        return int(self.bus_id.shape[0])
+
+    @property
+    def n_branch(self) -> int:
+        return int(self.br_from.shape[0])
+
+    @property
+    def n_gen(self) -> int:
+        return int(self.gen_bus.shape[0])
+
+    def copy(self) -> "GridModel":
+        kw = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in self.__dict__.items() if k != "_keep"}
+        return GridModel(**kw)
+
+    def with_voltages(self, vm: np.ndarray, va_deg: np.ndarray) -> "GridModel":
+        """Warm start: every bus starts at the given state (GridScenario.WithSolvedVoltages,
+        ``src/GridSim.Core/Simulation/GridScenario.cs:35-52``)."""
+        m = self.copy()
+        m.vm = np.ascontiguousarray(vm, dtype=np.float64).copy()
+        m.va_deg = np.ascontiguousarray(va_deg, dtype=np.float64).copy()
+        return m
+
+    def in_service_branches(self) -> np.ndarray:
+        """ContingencyAnalysis.InServiceBranchIndices (``ContingencyAnalysis.cs:283-289``)."""
+        return np.nonzero(self.br_in_service)[0].astype(np.int32)
+
+    def desc(self):
+        """A ``gs_grid_desc`` pointing at this model's arrays (kept alive by the model)."""
+        from ._abi import GridDesc
+
+        def arr(a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            self._keep.append(a)
+            return a.ctypes.data_as(ctypes.c_void_p)
+
+        d = GridDesc()
+        d.n_bus, d.n_gen, d.n_branch = self.n_bus, self.n_gen, self.n_branch
+        d.base_mva = float(self.base_mva)
+        d.bus_id = arr(self.bus_id, np.int32)
+        d.bus_type = arr(self.bus_type, np.int32)
+        d.pd, d.qd = arr(self.pd, np.float64), arr(self.qd, np.float64)
+        d.gs, d.bs = arr(self.gs, np.float64), arr(self.bs, np.float64)
+        d.vm, d.va_deg = arr(self.vm, np.float64), arr(self.va_deg, np.float64)
+        d.vmin_pu, d.vmax_pu = arr(self.vmin, np.float64), arr(self.vmax, np.float64)
+        d.gen_bus = arr(self.gen_bus, np.int32)
+        d.pg, d.qg, d.vg = arr(self.pg, np.float64), arr(self.qg, np.float64), arr(self.vg, np.float64)
+        d.qmin, d.qmax = arr(self.qmin, np.float64), arr(self.qmax, np.float64)
+        d.gen_in_service = arr(self.gen_in_service, np.uint8)
+        d.br_from, d.br_to = arr(self.br_from, np.int32), arr(self.br_to, np.int32)
+        d.r, d.x, d.b = arr(self.r, np.float64), arr(self.x, np.float64), arr(self.b, np.float64)
+        d.tap, d.shift_deg = arr(self.tap, np.float64), arr(self.shift_deg, np.float64)
+        d.rate_a = arr(self.rate_a, np.float64)
+        d.br_in_service = arr(self.br_in_service, np.uint8)
+        return d
+
+    # ---- JSON round trip of the whole model (golden fixtures) -------------------------------------
+    def to_dict(self) -> dict:
+        out = {"name": self.name, "base_mva": self.base_mva}
+        for k, v in self.__dict__.items():
+            if isinstance(v, np.ndarray):
+                out[k] = [None if (isinstance(t, float) and math.isnan(t)) else t for t in v.tolist()]
+        return out
+
+    @staticmethod
+    def from_dict(d: dict) -> "GridModel":
+        f64 = lambda k: np.array([np.nan if t is None else t for t in d[k]], dtype=np.float64)  # noqa: E731
+        i32 = lambda k: np.array(d[k], dtype=np.int32)  # noqa: E731
+        u8 = lambda k: np.array(d[k], dtype=np.uint8)  # noqa: E731
+        return GridModel(
+            name=d["name"], base_mva=float(d["base_mva"]),
+            bus_id=i32("bus_id"), bus_type=i32("bus_type"), pd=f64("pd"), qd=f64("qd"), gs=f64("gs"),
+            bs=f64("bs"), vm=f64("vm"), va_deg=f64("va_deg"), vmin=f64("vmin"), vmax=f64("vmax"),
+            base_kv=f64("base_kv"), gen_bus=i32("gen_bus"), pg=f64("pg"), qg=f64("qg"), vg=f64("vg"),
+            qmin=f64("qmin"), qmax=f64("qmax"), gen_in_service=u8("gen_in_service"), br_from=i32("br_from"),
+            br_to=i32("br_to"), r=f64("r"), x=f64("x"), b=f64("b"), tap=f64("tap"), shift_deg=f64("shift_deg"),
+            rate_a=f64("rate_a"), br_in_service=u8("br_in_service"), is_transformer=u8("is_transformer"))
+
+
+# =============================================================================================
+# MATPOWER .m (MatpowerParser.cs)
+
+def _matrix(text: str, name: str):
+    m = re.search(r"mpc\." + name + r"\s*=\s*\[(.*?)\];", text, re.S)
+    if not m:
+        return None
+    rows = []
+    for line in m.group(1).replace("...", " ").split(";"):
+        vals = line.split()
+        if vals:
+            rows.append([float(v) for v in vals])
+    return rows
+
+
+def parse_matpower(text: str, name: str = "matpower") -> GridModel:
+    text = re.sub(r"%[^\n]*", "", text)  # comments
+    mb = re.search(r"mpc\.baseMVA\s*=\s*([0-9.eE+-]+)", text)
+    base = float(mb.group(1)) if mb else 100.0
+    bus_rows = _matrix(text, "bus")
+    gen_rows = _matrix(text, "gen") or []
+    br_rows = _matrix(text, "branch") or []
+    buses = [r for r in bus_rows if int(r[1]) != 4]
+    live = {int(r[0]) for r in buses}
+    pos = {int(r[0]): i for i, r in enumerate(buses)}
+    gens = [g for g in gen_rows if int(g[0]) in live]
+    gen_on = {int(g[0]) for g in gens if int(g[7]) > 0}
+    btype = []
+    for r in buses:
+        t = {3: SLACK, 2: PV}.get(int(r[1]), PQ)
+        if t == PV and int(r[0]) not in gen_on:  # :341-349
+            t = PQ
+        btype.append(t)
+
+    def limits(r):
+        if len(r) >= 13:
+            hi, lo = r[11], r[12]
+            if math.isfinite(lo) and math.isfinite(hi) and lo > 0 and hi > 0 and lo <= hi:
+                return lo, hi
+        return math.nan, math.nan
+
+    lim = [limits(r) for r in buses]
+    brs = [r for r in br_rows if int(r[10]) != 0 and int(r[0]) in live and int(r[1]) in live]
+    g = lambda rows, i, d=0.0: np.array([r[i] if i < len(r) else d for r in rows], dtype=np.float64)  # noqa: E731
+    tap_raw = g(brs, 8)
+    return GridModel(
+        name=name, base_mva=base,
+        bus_id=np.array([int(r[0]) for r in buses], np.int32), bus_type=np.array(btype, np.int32),
+        pd=g(buses, 2), qd=g(buses, 3), gs=g(buses, 4), bs=g(buses, 5), vm=g(buses, 7, 1.0), va_deg=g(buses, 8),
+        vmin=np.array([v[0] for v in lim]), vmax=np.array([v[1] for v in lim]), base_kv=g(buses, 9),
+        gen_bus=np.array([pos[int(r[0])] for r in gens], np.int32), pg=g(gens, 1), qg=g(gens, 2),
+        vg=g(gens, 5, 1.0), qmin=g(gens, 4, -np.inf), qmax=g(gens, 3, np.inf),
+        gen_in_service=np.array([1 if int(r[7]) > 0 else 0 for r in gens], np.uint8),
+        br_from=np.array([pos[int(r[0])] for r in brs], np.int32),
+        br_to=np.array([pos[int(r[1])] for r in brs], np.int32),
+        r=g(brs, 2), x=g(brs, 3), b=g(brs, 4), tap=np.where(tap_raw != 0.0, tap_raw, 1.0), shift_deg=g(brs, 9),
+        rate_a=g(brs, 5), br_in_service=np.ones(len(brs), np.uint8),
+        is_transformer=(tap_raw != 0.0).astype(np.uint8))
+
+
+def load_matpower(path: str) -> GridModel:
+    with open(path) as fh:
+        return parse_matpower(fh.read(), os.path.splitext(os.path.basename(path))[0])
+
+
+# =============================================================================================
+# GridSim v1 JSON case directory (JsonGridLoader.cs:55-255), the subset this path uses.
+
+def save_case_dir(m: GridModel, path: str) -> None:
+    os.makedirs(path, exist_ok=True)
+    tname = {PQ: "pq", PV: "pv", SLACK: "slack"}
+
+    def dump(fn, obj):
+        with open(os.path.join(path, fn), "w") as fh:
+            json.dump(obj, fh, indent=1)
+
+    dump("system.json", {"name": m.name, "baseMva": m.base_mva, "frequencyHz": 50.0, "dispatch": False})
+    buses = []
+    for i in range(m.n_bus):
+        d = {"id": int(m.bus_id[i]), "type": tname[int(m.bus_type[i])], "baseKv": float(m.base_kv[i]),
+             "vm": float(m.vm[i]), "vaDeg": float(m.va_deg[i]), "gs": float(m.gs[i]), "bs": float(m.bs[i])}
+        if not math.isnan(m.vmin[i]):
+            d["vminPu"] = float(m.vmin[i])
+        if not math.isnan(m.vmax[i]):
+            d["vmaxPu"] = float(m.vmax[i])
+        buses.append(d)
+    dump("buses.json", buses)
+    gens = []
+    for k in range(m.n_gen):
+        bi = int(m.gen_bus[k])
+        gens.append({"name": f"G{k}", "bus": int(m.bus_id[bi]),
+                     "role": "slack" if m.bus_type[bi] == SLACK else "pv",
+                     "capacityMva": float(max(abs(m.qmax[k]), abs(m.qmin[k]), abs(m.pg[k]), 1.0)),
+                     "outputMw": float(m.pg[k]), "qOutputMvar": float(m.qg[k]),
+                     "voltageSetpoint": float(m.vg[k]), "qMinMvar": float(m.qmin[k]), "qMaxMvar": float(m.qmax[k]),
+                     "inService": bool(m.gen_in_service[k])})
+    dump("generation.json", gens)
+    dump("demand.json", [{"name": f"D{i}", "bus": int(m.bus_id[i]), "pMw": float(m.pd[i]), "qMvar": float(m.qd[i])}
+                         for i in range(m.n_bus) if m.pd[i] != 0 or m.qd[i] != 0])
+    lines = []
+    for k in range(m.n_branch):
+        lines.append({"name": f"L{k}", "from": int(m.bus_id[m.br_from[k]]), "to": int(m.bus_id[m.br_to[k]]),
+                      "rPu": float(m.r[k]), "xPu": float(m.x[k]), "bPu": float(m.b[k]),
+                      "ratingMva": float(m.rate_a[k]), "tapRatio": float(m.tap[k]),
+                      "phaseShiftDeg": float(m.shift_deg[k]), "isTransformer": bool(m.is_transformer[k])})
+    dump("transmission.json", lines)
+
+
+def load_case_dir(path: str) -> GridModel:
+    def read(fn, default):
+        p = os.path.join(path, fn)
+        if not os.path.exists(p):
+            return default
+        with open(p) as fh:
+            return json.load(fh)
+
+    sysd = read("system.json", {})
+    buses = read("buses.json", [])
+    gens = read("generation.json", [])
+    dem = read("demand.json", [])
+    lines = read("transmission.json", [])
+    if not buses:
+        raise ValueError("buses.json is empty or missing")
+    if sysd.get("dispatch", True):
+        raise ValueError("only cases with \"dispatch\": false are read (the written outputs are the dispatch)")
+    pos = {int(b["id"]): i for i, b in enumerate(buses)}
+    n = len(buses)
+    btype = np.array([{"pq": PQ, "pv": PV, "slack": SLACK}[b.get("type", "pq").lower()] for b in buses], np.int32)
+    for g in gens:  # JsonGridLoader.cs:121-127: generator roles raise bus types
+        if not g.get("inService", True):
+            continue
+        i = pos[int(g["bus"])]
+        role = g.get("role", "pv").lower()
+        if role == "slack":
+            btype[i] = SLACK
+        elif role != "pq" and btype[i] != SLACK:
+            btype[i] = PV
+    pd = np.zeros(n)
+    qd = np.zeros(n)
+    for d in dem:
+        i = pos[int(d["bus"])]
+        pd[i] += d["pMw"]
+        qd[i] += d["qMvar"] if d.get("qMvar") is not None else d["pMw"] * math.tan(math.acos(d.get("powerFactor", 0.95)))
+    f = lambda rows, k, dflt=0.0: np.array([float(r.get(k, dflt)) if r.get(k) is not None else dflt  # noqa: E731
+                                           for r in rows], np.float64)
+    circ = np.array([int(l.get("circuits", 1)) for l in lines], np.float64)
+    cap = f(gens, "capacityMva")
+    return GridModel(
+        name=sysd.get("name", os.path.basename(os.path.normpath(path))), base_mva=float(sysd.get("baseMva", 100.0)),
+        bus_id=np.array([int(b["id"]) for b in buses], np.int32), bus_type=btype, pd=pd, qd=qd,
+        gs=f(buses, "gs"), bs=f(buses, "bs"), vm=f(buses, "vm", 1.0), va_deg=f(buses, "vaDeg"),
+        vmin=f(buses, "vminPu", math.nan), vmax=f(buses, "vmaxPu", math.nan), base_kv=f(buses, "baseKv"),
+        gen_bus=np.array([pos[int(g["bus"])] for g in gens], np.int32), pg=f(gens, "outputMw"),
+        qg=f(gens, "qOutputMvar"), vg=f(gens, "voltageSetpoint", 1.0),
+        qmin=np.array([g["qMinMvar"] if g.get("qMinMvar") is not None else -c for g, c in zip(gens, cap)], np.float64),
+        qmax=np.array([g["qMaxMvar"] if g.get("qMaxMvar") is not None else c for g, c in zip(gens, cap)], np.float64),
+        gen_in_service=np.array([1 if g.get("inService", True) else 0 for g in gens], np.uint8),
+        br_from=np.array([pos[int(l["from"])] for l in lines], np.int32),
+        br_to=np.array([pos[int(l["to"])] for l in lines], np.int32),
+        r=f(lines, "rPu") / circ, x=f(lines, "xPu") / circ, b=f(lines, "bPu") * circ, tap=f(lines, "tapRatio", 1.0),
+        shift_deg=f(lines, "phaseShiftDeg"), rate_a=f(lines, "ratingMva") * circ,
+        br_in_service=np.ones(len(lines), np.uint8),
+        is_transformer=np.array([1 if l.get("isTransformer", False) else 0 for l in lines], np.uint8))

@@ -1,0 +1,230 @@
+/*
+ * gridsim_b200.h — C ABI of the B200-native AC load-flow / N-1 contingency engine.
+ *
+ * This is the drop-in boundary for GridSim.Core's sparse Newton-Raphson load flow and its
+ * N-1 branch-outage screen. Every entry point is `extern "C"`, takes plain pointers and sizes,
+ * returns an int status (0 = GS_OK) and never throws across the boundary. Conventions follow
+ * the reference's P/Invoke layer (src/GridSim.Gpu/RocmInterop.cs:115-134 int statuses,
+ * :196-237 opaque IntPtr handles and caller-owned arrays).
+ *
+ * Ownership: the caller allocates every input and output array; the library never keeps a
+ * caller pointer past the call that received it. Threading: a gs_ctx may be shared by threads
+ * for create/destroy of grids; each gs_grid admits one caller at a time (the reference's
+ * solvers are "one instance per thread", src/GridSim.Core/PowerFlow/CpuSparseLuSolver.cs:17-20).
+ *
+ * Reference interfaces replaced (paths relative to the GridSim source tree):
+ *   IPowerFlowSolver.Solve              src/GridSim.Core/Abstractions/IPowerFlowSolver.cs:10-13
+ *   ContingencyAnalysis.ScreenBranches* src/GridSim.Core/Analysis/ContingencyAnalysis.cs:306-344,
+ *                                       src/GridSim.Core/Analysis/ContingencyAnalysis.Batched.cs:55-136
+ *   ContingencyAnalysis.ScreenBaseCase  src/GridSim.Core/Analysis/ContingencyAnalysis.cs:958-962
+ *   ISparseLinearSolver.Solve           src/GridSim.Core/Abstractions/ISparseLinearSolver.cs:12-17
+ *   IBatchedSparseLinearSolver.SolveBatch src/GridSim.Core/Abstractions/IBatchedSparseLinearSolver.cs:19-37
+ */
+#ifndef GRIDSIM_B200_H
+#define GRIDSIM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GS_ABI_VERSION 1
+
+/* ---- call-level status codes ------------------------------------------------------------ */
+enum gs_status {
+    GS_OK = 0,
+    GS_ERR_INVALID_ARG = 1, /* malformed call: null pointer, bad size, bad index (ArgumentException) */
+    GS_ERR_CUDA = 2,        /* a CUDA runtime call failed; gs_last_error has the text           */
+    GS_ERR_OOM = 3,         /* device allocation failed (RocmSparseLinearSolver.cs:297-331 kept OOM apart) */
+    GS_ERR_NO_DEVICE = 4,   /* no usable CUDA device / driver probe failed or timed out          */
+    GS_ERR_TIMEOUT = 5,     /* a bounded wait ran out                                            */
+    GS_ERR_STATE = 6,       /* wrong call order (e.g. solve before analyze)                      */
+    GS_ERR_UNSUPPORTED = 7, /* an option this build does not implement (named in gs_last_error)  */
+    GS_ERR_INTERNAL = 8,
+    GS_ERR_CAPACITY = 9     /* a caller-supplied output array is too small; the needed size is returned */
+};
+
+/* ---- per-system solve status: PowerFlowStatus (src/GridSim.Core/PowerFlow/PowerFlowResult.cs:5-22)
+ *      in the same order, plus two device-side outcomes --------------------------------------- */
+enum gs_pf_status {
+    GS_PF_CONVERGED = 0,
+    GS_PF_MAX_ITERATIONS = 1,
+    GS_PF_NON_FINITE = 2,
+    GS_PF_DIVERGED = 3,
+    GS_PF_SINGULAR_PIVOT = 4, /* a static pivot collapsed below its floor: the step could not be taken
+                                 (the reference reports this state as MaxIterations, NewtonShell.cs:74-120) */
+    GS_PF_TIMEOUT = 5,
+    GS_PF_NOT_RUN = 6
+};
+
+/* Arithmetic of the linear step (Jacobian values, LU, triangular solves). Mismatch, update and
+ * convergence test are always FP64. */
+enum gs_precision { GS_PREC_FP64 = 0, GS_PREC_MIXED = 1 /* FP32 LU + solves, FP64 residual */ };
+
+/* ContingencyViolationKind (src/GridSim.Core/Analysis/ContingencyAnalysis.cs:144-154), same order. */
+enum gs_violation_kind {
+    GS_VIOL_BRANCH_OVERLOAD = 0,
+    GS_VIOL_BOUNDARY_OVERLOAD = 1,
+    GS_VIOL_UNDERVOLTAGE = 2,
+    GS_VIOL_OVERVOLTAGE = 3
+};
+
+typedef struct gs_ctx gs_ctx;
+typedef struct gs_grid gs_grid;
+
+/* ---- context ----------------------------------------------------------------------------- */
+typedef struct gs_ctx_opts {
+    int32_t probe_timeout_ms; /* bound on the device probe + FP64 self-test (GpuContext.cs:311-363); 0 = 10000 */
+    int32_t reserved[7];
+} gs_ctx_opts;
+
+/* ---- grid description: the fields of GridModel the load flow reads (Model/Model.cs:20-35 Bus,
+ *      :91-114 Generator, :253-275 Branch). Bus references are 0-based POSITIONS in the bus arrays,
+ *      not bus ids (the reference resolves ids to positions first, SparseNewtonRaphsonPowerFlow.cs:76-78). */
+typedef struct gs_grid_desc {
+    int32_t n_bus;
+    int32_t n_gen;
+    int32_t n_branch;
+    int32_t reserved0;
+    double base_mva;
+    /* buses [n_bus] */
+    const int32_t *bus_id;   /* external id, the key of voltage violations */
+    const int32_t *bus_type; /* 1 = PQ, 2 = PV, 3 = slack */
+    const double *pd, *qd;   /* MW, MVAr */
+    const double *gs, *bs;   /* MW / MVAr at 1 pu */
+    const double *vm;        /* start / fixed magnitude, pu */
+    const double *va_deg;    /* start / fixed angle, degrees */
+    const double *vmin_pu;   /* own voltage limits; NaN = none; the array itself may be NULL */
+    const double *vmax_pu;
+    /* generators [n_gen] */
+    const int32_t *gen_bus; /* bus position */
+    const double *pg, *qg, *vg, *qmin, *qmax;
+    const uint8_t *gen_in_service; /* NULL = all in service */
+    /* branches [n_branch], in GridModel.Branches order */
+    const int32_t *br_from, *br_to; /* bus positions */
+    const double *r, *x, *b;        /* series R, X and total charging B, pu */
+    const double *tap;              /* off-nominal ratio, 0 = 1 (AdmittanceStamp.cs:63-66) */
+    const double *shift_deg;
+    const double *rate_a;           /* MVA, 0 = unrated */
+    const uint8_t *br_in_service;   /* NULL = all in service */
+} gs_grid_desc;
+
+/* ---- options: PowerFlowOptions (src/GridSim.Core/PowerFlow/PowerFlowOptions.cs:15-158) ---- */
+typedef struct gs_pf_opts {
+    double tolerance;               /* pu, default 1e-8 */
+    double diverge_limit_pu;        /* default 10; +inf turns the stop off */
+    int32_t max_iterations;         /* default 30 (StudyOptions 100) */
+    int32_t flat_start;             /* default 0 */
+    int32_t enforce_q_limits;       /* must be 0 in this build (GS_ERR_UNSUPPORTED otherwise) */
+    int32_t retry_from_dc_start;    /* must be 0 in this build */
+    int32_t per_bus_voltage_limits; /* judge buses against their own vmin/vmax (VoltageLimits.cs:55-67) */
+    int32_t precision;              /* enum gs_precision */
+    int32_t warm_start_from_base;   /* screens: solve the intact grid first and start every outage from
+                                       its solution (GridScenario.WithSolvedVoltages, Simulation/GridScenario.cs:35-52) */
+    int32_t batch_width;            /* systems per device batch; 0 = choose from free HBM */
+    int32_t reserved[8];
+} gs_pf_opts;
+
+/* Fill `o` with the reference defaults (PowerFlowOptions()) plus precision = FP64. */
+void gs_pf_opts_default(gs_pf_opts *o);
+
+/* ---- single-solve result: PowerFlowResult (PowerFlow/PowerFlowResult.cs) -------------------- */
+typedef struct gs_pf_result {
+    int32_t status;       /* enum gs_pf_status */
+    int32_t iterations;
+    double max_mismatch;  /* pu */
+    /* caller-owned arrays, each may be NULL */
+    double *vm;           /* [n_bus] pu */
+    double *va_deg;       /* [n_bus] degrees */
+    double *p_inj_mw;     /* [n_bus] */
+    double *q_inj_mvar;   /* [n_bus] */
+    double *loading_pct;  /* [n_branch], 0 for an out-of-service or unrated branch */
+    double *sf_mva;       /* [2*n_branch] from-end complex power (re, im) MW / MVAr */
+    double *st_mva;       /* [2*n_branch] to-end complex power */
+} gs_pf_result;
+
+/* ---- N-1 screen result (ContingencyResult, Analysis/ContingencyAnalysis.cs:9-96, with Details
+ *      as a CSR list of (kind, element, value) per outage) ----------------------------------- */
+typedef struct gs_n1_result {
+    /* per outage [n_out] */
+    int32_t *status;
+    int32_t *iterations;
+    double *max_mismatch;
+    double *min_vm, *max_vm;   /* 0 when not converged (ContingencyAnalysis.cs:1661-1662) */
+    double *max_loading_pct;
+    /* violation details, CSR: entries viol_ptr[k] .. viol_ptr[k+1]-1 belong to outage k */
+    int32_t *viol_ptr;         /* [n_out+1] */
+    int32_t viol_capacity;     /* length of the three arrays below */
+    int32_t viol_count;        /* out: entries written (or needed, with GS_ERR_CAPACITY) */
+    int32_t *viol_kind;        /* enum gs_violation_kind */
+    int32_t *viol_element;     /* original branch index, or bus id */
+    double *viol_value;        /* loading % or Vm pu */
+    /* optional full states [n_out * n_bus], may be NULL */
+    double *vm;
+    double *va_deg;
+    /* base case (ScreenBaseCase) when warm_start_from_base is set, else status GS_PF_NOT_RUN */
+    int32_t base_status;
+    int32_t base_iterations;
+    /* device timing of the screen, milliseconds (CUDA events) */
+    double device_ms;
+    int32_t n_singular_pivot;  /* systems whose static pivot failed */
+    int32_t n_batches;
+} gs_n1_result;
+
+/* ---- context -------------------------------------------------------------------------------- */
+
+/* Open `device`, run a bounded FP64 self-test (GpuContext.cs:227-254, probe bound :325-345). */
+int gs_ctx_create(int device, const gs_ctx_opts *opts, gs_ctx **out);
+int gs_ctx_destroy(gs_ctx *ctx);
+/* Last error text of calls on this context (NUL-terminated, truncated to len). */
+int gs_last_error(gs_ctx *ctx, char *buf, size_t len);
+const char *gs_status_str(int status);
+int gs_abi_version(void);
+
+/* ---- grid ----------------------------------------------------------------------------------- */
+
+/* Copy the grid in, build the base Y-bus (SparseNewtonRaphsonPowerFlow.BuildY :382-402 with
+ * AdmittanceStamp.Branch, AdmittanceStamp.cs:35-76) and the shared symbolic analysis: equation
+ * numbering (NewtonShell.EquationPositions, NewtonShell.cs:327-336), Jacobian superset pattern
+ * (SparseNewtonRaphsonPowerFlow.BuildJacobianStructure :296-332), minimum-degree order
+ * (Numerics/MinimumDegreeOrdering.cs:23-121), static-pivot LU pattern, level schedule; upload. */
+int gs_grid_create(gs_ctx *ctx, const gs_grid_desc *desc, gs_grid **out);
+int gs_grid_destroy(gs_grid *grid);
+
+typedef struct gs_grid_info {
+    int32_t n_bus, n_branch, n_pv, n_pq;
+    int32_t m;          /* unknowns (n-1) + n_pq */
+    int32_t nnz_y;
+    int32_t nnz_j;      /* Jacobian superset pattern */
+    int64_t nnz_lu;     /* L + U incl. diagonal, static-pivot pattern */
+    int64_t lu_flops;   /* multiply-adds of one numeric factorisation */
+    int32_t n_levels;   /* elimination-tree levels of the numeric schedule */
+    int32_t reserved[7];
+} gs_grid_info;
+int gs_grid_info_get(gs_grid *grid, gs_grid_info *info);
+
+/* ---- solves --------------------------------------------------------------------------------- */
+
+/* IPowerFlowSolver.Solve on the intact grid (SparseNewtonRaphsonPowerFlow.Solve :48-54). */
+int gs_pf_solve(gs_grid *grid, const gs_pf_opts *opts, gs_pf_result *res);
+
+/* `count` independent load flows of the same grid in one device batch. Case k scales every bus's
+ * Pd and Qd by load_scale[k*n_bus + i] (NULL = 1) and removes branch outage[k] (NULL or -1 = none).
+ * Results go to vm/va_deg [count*n_bus] (may be NULL) and status/iterations/max_mismatch [count]. */
+int gs_pf_solve_batch(gs_grid *grid, int32_t count, const double *load_scale, const int32_t *outage,
+                      const gs_pf_opts *opts, int32_t *status, int32_t *iterations, double *max_mismatch,
+                      double *vm, double *va_deg);
+
+/* ContingencyAnalysis.ScreenBranches / ScreenBranchesParallel / ScreenBranchesBatched: one full
+ * Newton solve per outaged branch (indices into the branch arrays; each must be in service), then
+ * the ScreenStateCore classification (ContingencyAnalysis.cs:1105-1238) on the device. Results are
+ * in the order of `branch_idx`. */
+int gs_n1_screen(gs_grid *grid, int32_t n_out, const int32_t *branch_idx, const gs_pf_opts *opts,
+                 gs_n1_result *res);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GRIDSIM_B200_H */

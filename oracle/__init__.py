@@ -1,0 +1,147 @@
+"""CPU ORACLE for the gridsim_b200 load-flow path — TEST INFRASTRUCTURE ONLY.
+
+Python binding of ``oracle/gs_oracle.cpp``, the C++17 restatement of GridSim.Core's FP64 sparse
+Gilbert-Peierls Newton-Raphson load flow and N-1 screen. Only the tests, the smoke check and the
+benchmark's CPU-baseline leg may import this package, and only as the checker; the engine never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from gridsim_b200 import _abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SRC = os.path.join(_HERE, "gs_oracle.cpp")
+_LIB = os.path.join(_HERE, "_build", "libgs_oracle.so")
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with g++ (the recipe is this function: one source file, no dependencies)."""
+    os.makedirs(os.path.dirname(_LIB), exist_ok=True)
+    if force or not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(_SRC):
+        subprocess.check_call(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-pthread", "-o", _LIB, _SRC])
+    return _LIB
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        build()
+        lib = ctypes.CDLL(_LIB)
+        vp, i32 = ctypes.c_void_p, ctypes.c_int32
+        lib.gso_pf_solve.argtypes = [ctypes.POINTER(_abi.GridDesc), ctypes.POINTER(_abi.PfOpts),
+                                     ctypes.POINTER(_abi.PfResult)]
+        lib.gso_n1_screen.argtypes = [ctypes.POINTER(_abi.GridDesc), i32, vp, ctypes.POINTER(_abi.PfOpts), i32,
+                                      ctypes.POINTER(_abi.N1Result)]
+        lib.gso_jacobian.argtypes = [ctypes.POINTER(_abi.GridDesc), vp, vp, vp, vp, vp, i32, vp, i32]
+        lib.gso_md_order.argtypes = [i32, vp, vp, vp]
+        lib.gso_sparse_solve.argtypes = [i32, vp, vp, vp, vp, vp]
+        _lib = lib
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def solve(model, opts=None) -> dict:
+    """IPowerFlowSolver.Solve with the reference's CPU sparse Newton engine."""
+    lib = _load()
+    o = opts or _abi.default_opts()
+    n, nb = model.n_bus, model.n_branch
+    out = {k: np.zeros(n) for k in ("vm", "va_deg", "p_inj_mw", "q_inj_mvar")}
+    out["loading_pct"] = np.zeros(nb)
+    out["sf_mva"] = np.zeros(2 * nb)
+    out["st_mva"] = np.zeros(2 * nb)
+    r = _abi.PfResult()
+    for k, v in out.items():
+        setattr(r, k, _p(v))
+    d = model.desc()
+    rc = lib.gso_pf_solve(ctypes.byref(d), ctypes.byref(o), ctypes.byref(r))
+    if rc != 0:
+        raise RuntimeError(f"oracle solve failed: {rc}")
+    out.update(status=r.status, iterations=r.iterations, max_mismatch=r.max_mismatch)
+    return out
+
+
+def screen(model, branch_idx, opts=None, threads: int = 0, keep_states: bool = False) -> dict:
+    """ScreenBranchesParallel on `threads` host threads (0 = all)."""
+    lib = _load()
+    o = opts or _abi.default_opts()
+    idx = np.ascontiguousarray(branch_idx, dtype=np.int32)
+    k = idx.shape[0]
+    n = model.n_bus
+    cap = max(64, k * 8)
+    while True:
+        out = dict(status=np.zeros(k, np.int32), iterations=np.zeros(k, np.int32), max_mismatch=np.zeros(k),
+                   min_vm=np.zeros(k), max_vm=np.zeros(k), max_loading_pct=np.zeros(k),
+                   viol_ptr=np.zeros(k + 1, np.int32), viol_kind=np.zeros(cap, np.int32),
+                   viol_element=np.zeros(cap, np.int32), viol_value=np.zeros(cap))
+        if keep_states:
+            out["vm"] = np.zeros(k * n)
+            out["va_deg"] = np.zeros(k * n)
+        r = _abi.N1Result()
+        for key, v in out.items():
+            setattr(r, key, _p(v))
+        r.viol_capacity = cap
+        d = model.desc()
+        rc = lib.gso_n1_screen(ctypes.byref(d), k, _p(idx), ctypes.byref(o), threads, ctypes.byref(r))
+        if rc == _abi.GS_ERR_CAPACITY:
+            cap = r.viol_count + 16
+            continue
+        if rc != 0:
+            raise RuntimeError(f"oracle screen failed: {rc}")
+        break
+    nv = r.viol_count
+    for key in ("viol_kind", "viol_element", "viol_value"):
+        out[key] = out[key][:nv]
+    if keep_states:
+        out["vm"] = out["vm"].reshape(k, n)
+        out["va_deg"] = out["va_deg"].reshape(k, n)
+    out["base_status"] = r.base_status
+    out["base_iterations"] = r.base_iterations
+    return out
+
+
+def jacobian(model):
+    """The reference's Jacobian (CSR) and mismatch at the model's start point."""
+    lib = _load()
+    d = model.desc()
+    m = ctypes.c_int32()
+    nnz = ctypes.c_int32()
+    lib.gso_jacobian(ctypes.byref(d), ctypes.byref(m), ctypes.byref(nnz), None, None, None, 0, None, 0)
+    rp = np.zeros(m.value + 1, np.int32)
+    ci = np.zeros(nnz.value, np.int32)
+    val = np.zeros(nnz.value)
+    mis = np.zeros(m.value)
+    rc = lib.gso_jacobian(ctypes.byref(d), ctypes.byref(m), ctypes.byref(nnz), _p(rp), _p(ci), _p(val), nnz.value,
+                          _p(mis), m.value)
+    if rc != 0:
+        raise RuntimeError(f"oracle jacobian failed: {rc}")
+    return rp, ci, val, mis
+
+
+def md_order(row_ptr, col_idx):
+    lib = _load()
+    rp = np.ascontiguousarray(row_ptr, np.int32)
+    ci = np.ascontiguousarray(col_idx, np.int32)
+    n = rp.shape[0] - 1
+    q = np.zeros(n, np.int32)
+    lib.gso_md_order(n, _p(rp), _p(ci), _p(q))
+    return q
+
+
+def sparse_solve(row_ptr, col_idx, val, b):
+    lib = _load()
+    rp = np.ascontiguousarray(row_ptr, np.int32)
+    ci = np.ascontiguousarray(col_idx, np.int32)
+    v = np.ascontiguousarray(val, np.float64)
+    bb = np.ascontiguousarray(b, np.float64)
+    x = np.zeros(rp.shape[0] - 1)
+    rc = lib.gso_sparse_solve(rp.shape[0] - 1, _p(rp), _p(ci), _p(v), _p(bb), _p(x))
+    return None if rc else x

@@ -1,0 +1,1073 @@
+// gs_oracle.cpp — CPU ORACLE for the gridsim_b200 load-flow path. TEST INFRASTRUCTURE ONLY.
+//
+// A plain C++17 restatement of GridSim.Core's FP64 sparse polar Newton-Raphson load flow and its N-1
+// branch-outage screen, operation for operation where cheap. It exists to check the CUDA engine (tests,
+// the smoke check and the CPU-baseline leg of the benchmark); the product never links or calls it.
+// Every function cites the reference file:line it follows (paths relative to the GridSim source tree).
+//
+// Deliberate deviations (documented in the design notes):
+//   * sin/cos come from libm, not the reference's fdlibm port (Numerics/DetMath.cs:66-71); the parity
+//     target (1e-8) does not need cross-OS bit identity.
+//   * ContingencyAnalysis.ProvablyUnsolvablePart (:1700-1830) is not restated: it only short-cuts states
+//     the Newton solve reports non-converged anyway, with the same result.
+//   * the DC-angle retry (NewtonShell.cs:227-268) is not restated; options with it set are refused.
+#include "../include/gridsim_b200.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+
+using cplx = std::complex<double>;
+constexpr double kPi = 3.14159265358979323846;
+
+// ---------------------------------------------------------------------------------------------
+// Model: the GridModel fields the load flow reads (Model/Model.cs:20-35, 91-114, 253-275).
+struct Gen { int bus; double pg, qg, vg, qmin, qmax; };
+struct Br {
+    int f, t;
+    double r, x, b, tap, shift, rateA;
+    bool inService;
+};
+struct Model {
+    int n = 0;
+    double base = 100.0;
+    std::vector<int> id, type;  // 1 PQ, 2 PV, 3 slack
+    std::vector<double> pd, qd, gs, bs, vm, vaDeg, vmin, vmax;
+    std::vector<Gen> gens;      // in-service units only (GridModel.Generators)
+    std::vector<Br> br;         // GridModel.Branches order
+};
+
+Model FromDesc(const gs_grid_desc* d) {
+    Model m;
+    m.n = d->n_bus;
+    m.base = d->base_mva;
+    m.id.assign(d->bus_id, d->bus_id + m.n);
+    m.type.assign(d->bus_type, d->bus_type + m.n);
+    m.pd.assign(d->pd, d->pd + m.n);
+    m.qd.assign(d->qd, d->qd + m.n);
+    m.gs.assign(d->gs, d->gs + m.n);
+    m.bs.assign(d->bs, d->bs + m.n);
+    m.vm.assign(d->vm, d->vm + m.n);
+    m.vaDeg.assign(d->va_deg, d->va_deg + m.n);
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    m.vmin.assign(m.n, nan);
+    m.vmax.assign(m.n, nan);
+    if (d->vmin_pu) m.vmin.assign(d->vmin_pu, d->vmin_pu + m.n);
+    if (d->vmax_pu) m.vmax.assign(d->vmax_pu, d->vmax_pu + m.n);
+    for (int g = 0; g < d->n_gen; g++) {
+        if (d->gen_in_service && !d->gen_in_service[g]) continue;
+        m.gens.push_back({d->gen_bus[g], d->pg[g], d->qg[g], d->vg[g], d->qmin[g], d->qmax[g]});
+    }
+    for (int k = 0; k < d->n_branch; k++) {
+        m.br.push_back({d->br_from[k], d->br_to[k], d->r[k], d->x[k], d->b[k], d->tap[k], d->shift_deg[k],
+                        d->rate_a[k], d->br_in_service ? d->br_in_service[k] != 0 : true});
+    }
+    return m;
+}
+
+// ---------------------------------------------------------------------------------------------
+// AdmittanceStamp.Branch / FromAdmittance (PowerFlow/AdmittanceStamp.cs:35-76), h = 1.
+struct Stamp { cplx yff, ytt, yft, ytf; };
+Stamp BranchStamp(double r, double x, double b, double tapRatio, double shiftDeg) {
+    cplx ys = cplx(1.0, 0.0) / cplx(r, x);
+    cplx bc(0.0, b / 2.0);
+    double a = tapRatio == 0 ? 1.0 : tapRatio;
+    double shift = shiftDeg * kPi / 180.0;
+    cplx tap(a * std::cos(shift), a * std::sin(shift));
+    Stamp s;
+    s.yff = (ys + bc) / (a * a);
+    s.ytt = ys + bc;
+    s.yft = -ys / std::conj(tap);
+    s.ytf = -ys / tap;
+    return s;
+}
+
+// ---------------------------------------------------------------------------------------------
+// ComplexCsr and its builder (Numerics/Sparse.cs:134-224): insertion order kept per cell (stable by
+// column), duplicates summed in that order from +0.0, a zero diagonal injected where none is stamped.
+struct ComplexCsr {
+    int n = 0;
+    std::vector<int> rowPtr, colIdx, diag;
+    std::vector<double> G, B;
+};
+struct ComplexBuilder {
+    int n;
+    std::vector<int> r, c;
+    std::vector<double> g, b;
+    explicit ComplexBuilder(int n_) : n(n_) {}
+    void Add(int row, int col, double gv, double bv) {
+        if (gv == 0.0 && bv == 0.0) return;  // Sparse.cs:151
+        r.push_back(row); c.push_back(col); g.push_back(gv); b.push_back(bv);
+    }
+    ComplexCsr Build() const {
+        int nnz = (int)g.size();
+        std::vector<int> rowStart(n + 1, 0);
+        for (int t = 0; t < nnz; t++) rowStart[r[t] + 1]++;
+        for (int i = 0; i < n; i++) rowStart[i + 1] += rowStart[i];
+        std::vector<int> col(nnz), fill(rowStart);
+        std::vector<double> gv(nnz), bv(nnz);
+        for (int t = 0; t < nnz; t++) { int p = fill[r[t]]++; col[p] = c[t]; gv[p] = g[t]; bv[p] = b[t]; }
+        ComplexCsr y;
+        y.n = n;
+        y.rowPtr.assign(n + 1, 0);
+        y.diag.assign(n, -1);
+        std::vector<int> order;
+        for (int i = 0; i < n; i++) {
+            int s = rowStart[i], e = rowStart[i + 1];
+            order.resize(e - s);
+            for (int k = 0; k < e - s; k++) order[k] = s + k;
+            std::stable_sort(order.begin(), order.end(), [&](int a, int bb) { return col[a] < col[bb]; });
+            y.rowPtr[i] = (int)y.colIdx.size();
+            int prev = std::numeric_limits<int>::min();
+            bool diagWritten = false;
+            for (int o : order) {
+                int cc = col[o];
+                if (cc == prev) { y.G.back() += gv[o]; y.B.back() += bv[o]; continue; }
+                if (!diagWritten && prev < i && cc > i) {
+                    y.diag[i] = (int)y.colIdx.size();
+                    y.colIdx.push_back(i); y.G.push_back(0); y.B.push_back(0);
+                    diagWritten = true;
+                }
+                y.colIdx.push_back(cc); y.G.push_back(0.0 + gv[o]); y.B.push_back(0.0 + bv[o]);
+                prev = cc;
+                if (cc == i) { y.diag[i] = (int)y.colIdx.size() - 1; diagWritten = true; }
+            }
+            if (!diagWritten) {
+                y.diag[i] = (int)y.colIdx.size();
+                y.colIdx.push_back(i); y.G.push_back(0); y.B.push_back(0);
+            }
+        }
+        y.rowPtr[n] = (int)y.colIdx.size();
+        return y;
+    }
+};
+
+// SparseNewtonRaphsonPowerFlow.BuildY (:382-402). `skip` removes one branch (ScreenOutageCore's
+// WithoutMany, ContingencyAnalysis.cs:1839-1845, keeps the remaining branches in model order).
+ComplexCsr BuildY(const Model& m, int skip) {
+    ComplexBuilder b(m.n);
+    for (int k = 0; k < (int)m.br.size(); k++) {
+        const Br& br = m.br[k];
+        if (k == skip || !br.inService) continue;
+        Stamp s = BranchStamp(br.r, br.x, br.b, br.tap, br.shift);
+        b.Add(br.f, br.f, s.yff.real(), s.yff.imag());
+        b.Add(br.t, br.t, s.ytt.real(), s.ytt.imag());
+        b.Add(br.f, br.t, s.yft.real(), s.yft.imag());
+        b.Add(br.t, br.f, s.ytf.real(), s.ytf.imag());
+    }
+    for (int i = 0; i < m.n; i++) {
+        if (m.gs[i] == 0 && m.bs[i] == 0) continue;
+        b.Add(i, i, m.gs[i] / m.base, m.bs[i] / m.base);
+    }
+    return b.Build();
+}
+
+// ---------------------------------------------------------------------------------------------
+// Real CSR with the CsrMatrix.Builder semantics (Numerics/Sparse.cs:33-127).
+struct Csr {
+    int n = 0;
+    std::vector<int> rowPtr, colIdx;
+    std::vector<double> val;
+};
+Csr BuildCsrPattern(int n, const std::vector<std::pair<int, int>>& cells) {
+    // Every cell carries the placeholder 1.0, so duplicates only merge; the diagonal is injected where
+    // absent (ensureDiagonal, the Build() default).
+    std::vector<std::vector<int>> rows(n);
+    for (auto& rc : cells) rows[rc.first].push_back(rc.second);
+    Csr a;
+    a.n = n;
+    a.rowPtr.assign(n + 1, 0);
+    for (int i = 0; i < n; i++) {
+        auto& r = rows[i];
+        r.push_back(i);
+        std::sort(r.begin(), r.end());
+        r.erase(std::unique(r.begin(), r.end()), r.end());
+        a.rowPtr[i] = (int)a.colIdx.size();
+        for (int c : r) a.colIdx.push_back(c);
+    }
+    a.rowPtr[n] = (int)a.colIdx.size();
+    a.val.assign(a.colIdx.size(), 1.0);
+    return a;
+}
+int Locate(const Csr& a, int row, int col) {  // SparseNewtonRaphsonPowerFlow.Locate (:335-336)
+    auto b = a.colIdx.begin() + a.rowPtr[row], e = a.colIdx.begin() + a.rowPtr[row + 1];
+    auto it = std::lower_bound(b, e, col);
+    return (it != e && *it == col) ? (int)(it - a.colIdx.begin()) : -1;
+}
+
+// ---------------------------------------------------------------------------------------------
+// MinimumDegreeOrdering.Order (Numerics/MinimumDegreeOrdering.cs:23-121): exact minimum degree on the
+// pattern of A + A^T, explicit elimination graph, LIFO bucket queue, initial insertion in descending index.
+std::vector<int> MinimumDegree(int n, const std::vector<int>& rowPtr, const std::vector<int>& colIdx) {
+    std::vector<int> order(n);
+    if (n == 0) return order;
+    std::vector<int> cnt(n, 0);
+    for (int i = 0; i < n; i++)
+        for (int k = rowPtr[i]; k < rowPtr[i + 1]; k++) {
+            int j = colIdx[k];
+            if (j != i) { cnt[i]++; cnt[j]++; }
+        }
+    std::vector<std::vector<int>> adj(n);
+    for (int i = 0; i < n; i++) adj[i].resize(cnt[i]);
+    std::vector<int> len(n, 0);
+    for (int i = 0; i < n; i++)
+        for (int k = rowPtr[i]; k < rowPtr[i + 1]; k++) {
+            int j = colIdx[k];
+            if (j == i) continue;
+            adj[i][len[i]++] = j;
+            adj[j][len[j]++] = i;
+        }
+    std::vector<int> stamp(n, 0);
+    int st = 0;
+    for (int i = 0; i < n; i++) {
+        st++;
+        int w = 0;
+        for (int p = 0; p < len[i]; p++) {
+            int j = adj[i][p];
+            if (stamp[j] != st) { stamp[j] = st; adj[i][w++] = j; }
+        }
+        len[i] = w;
+    }
+    std::vector<int> head(n + 1, -1), next(n), prev(n), deg(n);
+    auto insert = [&](int v, int d) {
+        deg[v] = d; prev[v] = -1; next[v] = head[d];
+        if (head[d] >= 0) prev[head[d]] = v;
+        head[d] = v;
+    };
+    auto remove = [&](int v) {
+        int d = deg[v];
+        if (prev[v] >= 0) next[prev[v]] = next[v]; else head[d] = next[v];
+        if (next[v] >= 0) prev[next[v]] = prev[v];
+    };
+    for (int i = n - 1; i >= 0; i--) insert(i, len[i]);
+    std::vector<char> dead(n, 0);
+    std::vector<int> nb(n);
+    int minDeg = 0;
+    for (int s = 0; s < n; s++) {
+        while (head[minDeg] < 0) minDeg++;
+        int v = head[minDeg];
+        remove(v);
+        dead[v] = 1;
+        order[s] = v;
+        int nbCount = 0;
+        for (int p = 0; p < len[v]; p++) {
+            int u = adj[v][p];
+            if (!dead[u]) nb[nbCount++] = u;
+        }
+        st++;
+        for (int t = 0; t < nbCount; t++) stamp[nb[t]] = st;
+        int nbStamp = st;
+        for (int t = 0; t < nbCount; t++) {
+            int u = nb[t];
+            remove(u);
+            auto& au = adj[u];
+            int w = 0;
+            for (int p = 0; p < len[u]; p++) {
+                int x = au[p];
+                if (x != v && !dead[x] && stamp[x] != nbStamp) au[w++] = x;
+            }
+            int need = w + nbCount - 1;
+            if ((int)au.size() < need) au.resize(std::max(need, (int)au.size() * 2));
+            for (int q = 0; q < nbCount; q++)
+                if (nb[q] != u) au[w++] = nb[q];
+            len[u] = w;
+            insert(u, w);
+        }
+        adj[v].clear();
+        len[v] = 0;
+        if (minDeg > 0) minDeg--;
+    }
+    return order;
+}
+
+// ---------------------------------------------------------------------------------------------
+// SparseLuFactorization.Factor (Numerics/SparseLuFactorization.cs:69-195) with SpSolve / Reach / Dfs
+// (:753-821): left-looking Gilbert-Peierls LU = P A Q, partial pivoting with the per-row floor
+// 1e-12 * max|A(row,:)| (NumericTolerances.cs:36, RowPivotFloorsCsc :99-116). Solve (:338-371).
+struct SparseLu {
+    int n = 0;
+    std::vector<int> lp, li, up, ui, pinv, q;
+    std::vector<double> lx, ux;
+    std::vector<double> Solve(const std::vector<double>& b) const {
+        std::vector<double> x(n), out(n);
+        for (int k = 0; k < n; k++) x[pinv[k]] = b[k];
+        for (int j = 0; j < n; j++) {
+            double xj = x[j];
+            for (int p = lp[j] + 1; p < lp[j + 1]; p++) x[li[p]] -= lx[p] * xj;
+        }
+        for (int j = n - 1; j >= 0; j--) {
+            double xj = x[j] / ux[up[j + 1] - 1];
+            x[j] = xj;
+            for (int p = up[j]; p < up[j + 1] - 1; p++) x[ui[p]] -= ux[p] * xj;
+        }
+        for (int k = 0; k < n; k++) out[q[k]] = x[k];
+        return out;
+    }
+};
+
+// Returns false when singular (the reference returns null).
+bool GpFactor(int n, const std::vector<int>& ap, const std::vector<int>& ai, const std::vector<double>& ax,
+              const std::vector<int>& q, SparseLu& F) {
+    int nnzA = ap[n];
+    double aNorm = 0.0;
+    for (int p = 0; p < nnzA; p++) {
+        if (std::isnan(ax[p])) return false;  // the reference throws; SolveStep refused non-finite J already
+        aNorm = std::max(aNorm, std::fabs(ax[p]));
+    }
+    if (std::isinf(aNorm)) return false;
+    std::vector<double> rowFloor(n, 0.0);
+    for (int p = 0; p < nnzA; p++) rowFloor[ai[p]] = std::max(rowFloor[ai[p]], std::fabs(ax[p]));
+    for (int r = 0; r < n; r++) rowFloor[r] *= 1e-12;
+
+    F.n = n;
+    F.q = q;
+    F.lp.assign(n + 1, 0);
+    F.up.assign(n + 1, 0);
+    F.li.clear(); F.lx.clear(); F.ui.clear(); F.ux.clear();
+    F.pinv.assign(n, -1);
+    std::vector<double> x(n, 0.0);
+    std::vector<int> xi(n), pstack(n);
+    std::vector<char> marked(n, 0);
+
+    auto dfs = [&](int j, int top) {
+        int head = 0;
+        xi[0] = j;
+        while (head >= 0) {
+            j = xi[head];
+            int jcol = F.pinv[j];
+            if (!marked[j]) {
+                marked[j] = 1;
+                pstack[head] = jcol < 0 ? 0 : F.lp[jcol] + 1;
+            }
+            bool done = true;
+            int pend = jcol < 0 ? 0 : F.lp[jcol + 1];
+            for (int p = pstack[head]; p < pend; p++) {
+                int i = F.li[p];
+                if (marked[i]) continue;
+                pstack[head] = p + 1;
+                xi[++head] = i;
+                done = false;
+                break;
+            }
+            if (done) { head--; xi[--top] = j; }
+        }
+        return top;
+    };
+
+    for (int k = 0; k < n; k++) {
+        F.lp[k] = (int)F.li.size();
+        F.up[k] = (int)F.ui.size();
+        int col = q[k];
+        // Reach (:783-792)
+        int top = n;
+        for (int p = ap[col]; p < ap[col + 1]; p++) {
+            int j = ai[p];
+            if (!marked[j]) top = dfs(j, top);
+        }
+        for (int p = top; p < n; p++) marked[xi[p]] = 0;
+        // SpSolve (:753-780)
+        for (int p = top; p < n; p++) x[xi[p]] = 0.0;
+        for (int p = ap[col]; p < ap[col + 1]; p++) x[ai[p]] = ax[p];
+        for (int px = top; px < n; px++) {
+            int j = xi[px];
+            int jcol = F.pinv[j];
+            if (jcol < 0) continue;
+            double xj = x[j];
+            for (int p = F.lp[jcol] + 1; p < F.lp[jcol + 1]; p++) x[F.li[p]] -= F.lx[p] * xj;
+        }
+        // partial pivot (:129-162)
+        int ipiv = -1;
+        double best = -1.0;
+        for (int px = top; px < n; px++) {
+            int i = xi[px];
+            if (F.pinv[i] < 0) {
+                double t = std::fabs(x[i]);
+                if (t > best) { best = t; ipiv = i; }
+            } else {
+                F.ui.push_back(F.pinv[i]);
+                F.ux.push_back(x[i]);
+            }
+        }
+        if (ipiv < 0 || best <= rowFloor[ipiv]) return false;
+        double pivot = x[ipiv];
+        F.ui.push_back(k); F.ux.push_back(pivot);
+        F.pinv[ipiv] = k;
+        F.li.push_back(ipiv); F.lx.push_back(1.0);
+        for (int px = top; px < n; px++) {
+            int i = xi[px];
+            if (F.pinv[i] < 0) { F.li.push_back(i); F.lx.push_back(x[i] / pivot); }
+            x[i] = 0.0;
+        }
+    }
+    F.lp[n] = (int)F.li.size();
+    F.up[n] = (int)F.ui.size();
+    for (auto& r : F.li) r = F.pinv[r];
+    return true;
+}
+
+// CpuSparseLuSolver (PowerFlow/CpuSparseLuSolver.cs:30-48): MD ordering cached by CSR pattern, then
+// SparseLu.ToCsc that DROPS exact zeros (Numerics/SparseLu.cs:63-91), then the factorisation.
+struct CpuSparseLuSolver {
+    std::vector<int> q, rowPtr, colIdx;
+    bool Solve(const Csr& a, const std::vector<double>& b, std::vector<double>& x) {
+        int n = a.n;
+        if (q.empty() || rowPtr != a.rowPtr || colIdx != a.colIdx) {
+            q = MinimumDegree(n, a.rowPtr, a.colIdx);
+            rowPtr = a.rowPtr;
+            colIdx = a.colIdx;
+        }
+        std::vector<int> ap(n + 1, 0);
+        for (size_t k = 0; k < a.colIdx.size(); k++)
+            if (a.val[k] != 0.0) ap[a.colIdx[k] + 1]++;
+        for (int c = 0; c < n; c++) ap[c + 1] += ap[c];
+        std::vector<int> ai(ap[n]), fill(ap.begin(), ap.end() - 1);
+        std::vector<double> ax(ap[n]);
+        for (int i = 0; i < n; i++)
+            for (int k = a.rowPtr[i]; k < a.rowPtr[i + 1]; k++) {
+                double v = a.val[k];
+                if (v == 0.0) continue;
+                int dst = fill[a.colIdx[k]]++;
+                ai[dst] = i;
+                ax[dst] = v;
+            }
+        SparseLu F;
+        if (!GpFactor(n, ap, ai, ax, q, F)) return false;
+        for (double v : b)
+            if (!std::isfinite(v)) return false;
+        x = F.Solve(b);
+        return true;
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// The SolveStep fallback when the sparse LU reports singular (NewtonShell.cs:100-105): ILU(0) with the
+// row-relative pivot guard (Numerics/Sparse.cs:232-300, NumericTolerances.Ilu0PivotGuard :226-234) and
+// ILU-preconditioned BiCGSTAB with the true-residual acceptance (Sparse.cs:305-405), tolerance
+// min(1e-10, tol*1e-3) and cap 4m + 200 (NumericTolerances.cs:256-260).
+void CsrMultiply(const Csr& a, const std::vector<double>& x, std::vector<double>& y) {
+    for (int i = 0; i < a.n; i++) {
+        double s = 0;
+        for (int k = a.rowPtr[i]; k < a.rowPtr[i + 1]; k++) s += a.val[k] * x[a.colIdx[k]];
+        y[i] = s;
+    }
+}
+struct Ilu0 {
+    const Csr* a = nullptr;
+    std::vector<double> lu;
+    std::vector<int> diag;
+    void Factor(const Csr& A) {
+        a = &A;
+        int n = A.n;
+        diag.assign(n, -1);
+        for (int i = 0; i < n; i++)
+            for (int k = A.rowPtr[i]; k < A.rowPtr[i + 1]; k++)
+                if (A.colIdx[k] == i) diag[i] = k;
+        lu = A.val;
+        std::vector<int> iw(n, -1);
+        for (int i = 0; i < n; i++) {
+            for (int k = A.rowPtr[i]; k < A.rowPtr[i + 1]; k++) iw[A.colIdx[k]] = k;
+            for (int k = A.rowPtr[i]; k < diag[i]; k++) {
+                int j = A.colIdx[k];
+                double piv = lu[diag[j]];
+                double lij = (piv != 0.0) ? lu[k] / piv : 0.0;
+                lu[k] = lij;
+                if (lij == 0.0) continue;
+                for (int kk = diag[j] + 1; kk < A.rowPtr[j + 1]; kk++) {
+                    int pos = iw[A.colIdx[kk]];
+                    if (pos != -1) lu[pos] -= lij * lu[kk];
+                }
+            }
+            double rowScale = 0.0;
+            for (int k = A.rowPtr[i]; k < A.rowPtr[i + 1]; k++) rowScale = std::max(rowScale, std::fabs(A.val[k]));
+            double guard = 1e-12 * (rowScale > 0.0 ? rowScale : 1.0);
+            double d = lu[diag[i]];
+            if (std::fabs(d) < guard) lu[diag[i]] = d < 0 ? -guard : guard;
+            for (int k = A.rowPtr[i]; k < A.rowPtr[i + 1]; k++) iw[A.colIdx[k]] = -1;
+        }
+    }
+    void Apply(const std::vector<double>& r, std::vector<double>& z) const {
+        int n = a->n;
+        for (int i = 0; i < n; i++) {
+            double s = r[i];
+            for (int k = a->rowPtr[i]; k < diag[i]; k++) s -= lu[k] * z[a->colIdx[k]];
+            z[i] = s;
+        }
+        for (int i = n - 1; i >= 0; i--) {
+            double s = z[i];
+            for (int k = diag[i] + 1; k < a->rowPtr[i + 1]; k++) s -= lu[k] * z[a->colIdx[k]];
+            z[i] = s / lu[diag[i]];
+        }
+    }
+};
+double Dot(const std::vector<double>& a, const std::vector<double>& b) {
+    double s = 0;
+    for (size_t i = 0; i < a.size(); i++) s += a[i] * b[i];
+    return s;
+}
+bool BiCgStab(const Csr& a, const std::vector<double>& b, std::vector<double>& x, const Ilu0& pc, double tol,
+              int maxIter) {
+    int n = a.n;
+    x.assign(n, 0.0);
+    std::vector<double> r = b, rhat = b, p(n, 0), v(n, 0), s(n), t(n), ph(n), sh(n);
+    double bnorm = std::sqrt(Dot(b, b));
+    if (bnorm == 0) {
+        for (double bi : b) if (bi != 0.0) return false;
+        return true;
+    }
+    auto trueResidual = [&]() {
+        CsrMultiply(a, x, t);
+        double sum = 0;
+        for (int i = 0; i < n; i++) { double d = b[i] - t[i]; sum += d * d; }
+        return std::sqrt(sum) / bnorm < tol;
+    };
+    double rho = 1, alpha = 1, omega = 1;
+    const double underflowGuard = 1e-300;
+    for (int it = 0; it < maxIter; it++) {
+        double rhoNew = Dot(rhat, r);
+        if (std::fabs(rhoNew) < underflowGuard || std::isnan(rhoNew)) return false;
+        double beta = (rhoNew / rho) * (alpha / omega);
+        for (int i = 0; i < n; i++) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+        pc.Apply(p, ph);
+        CsrMultiply(a, ph, v);
+        double rhatV = Dot(rhat, v);
+        if (rhatV == 0.0 || std::isnan(rhatV)) return false;
+        alpha = rhoNew / rhatV;
+        for (int i = 0; i < n; i++) s[i] = r[i] - alpha * v[i];
+        if (std::sqrt(Dot(s, s)) / bnorm < tol) {
+            for (int i = 0; i < n; i++) x[i] += alpha * ph[i];
+            return trueResidual();
+        }
+        pc.Apply(s, sh);
+        CsrMultiply(a, sh, t);
+        double tt = Dot(t, t);
+        omega = tt > 0 ? Dot(t, s) / tt : 0.0;
+        for (int i = 0; i < n; i++) { x[i] += alpha * ph[i] + omega * sh[i]; r[i] = s[i] - omega * t[i]; }
+        rho = rhoNew;
+        if (std::sqrt(Dot(r, r)) / bnorm < tol) return trueResidual();
+        if (omega == 0) return false;
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------------------------
+// NewtonShell.BuildBusSpec (PowerFlow/NewtonShell.cs:433-486).
+struct BusSpec {
+    std::vector<int> type0;  // 1 PQ, 2 PV, 3 slack
+    std::vector<double> vm, va, pspec, qspec, qd, qmin, qmax, vg;
+};
+BusSpec BuildBusSpec(const Model& m, bool flatStart) {
+    int n = m.n;
+    BusSpec s;
+    std::vector<double> pg(n, 0), qg(n, 0), vg(n, 0);
+    std::vector<char> hasGen(n, 0);
+    s.qmin.assign(n, 0); s.qmax.assign(n, 0);
+    for (const Gen& g : m.gens) {
+        pg[g.bus] += g.pg;
+        qg[g.bus] += g.qg;
+        s.qmin[g.bus] += g.qmin;
+        s.qmax[g.bus] += g.qmax;
+        vg[g.bus] = g.vg;  // the last generator at the bus wins (:448)
+        hasGen[g.bus] = 1;
+    }
+    s.type0.resize(n); s.vm.resize(n); s.va.resize(n); s.pspec.resize(n); s.qspec.resize(n);
+    s.qd = m.qd;
+    s.vg = vg;
+    for (int i = 0; i < n; i++) {
+        s.type0[i] = (m.type[i] == 2 && !hasGen[i]) ? 1 : m.type[i];
+        bool vc = s.type0[i] == 3 || s.type0[i] == 2;
+        s.vm[i] = (vc && hasGen[i]) ? vg[i] : (s.type0[i] == 3 ? m.vm[i] : (flatStart ? 1.0 : m.vm[i]));
+        s.va[i] = m.type[i] == 3 ? m.vaDeg[i] * kPi / 180.0 : (flatStart ? 0.0 : m.vaDeg[i] * kPi / 180.0);
+        s.pspec[i] = (pg[i] - m.pd[i]) / m.base;
+        s.qspec[i] = (qg[i] - m.qd[i]) / m.base;
+    }
+    return s;
+}
+
+// NewtonShell.EquationPositions (:327-336).
+int EquationPositions(const std::vector<int>& type, std::vector<int>& pPos, std::vector<int>& qPos) {
+    int n = (int)type.size();
+    pPos.assign(n, -1);
+    qPos.assign(n, -1);
+    int m = 0;
+    for (int i = 0; i < n; i++) if (type[i] != 3) pPos[i] = m++;
+    for (int i = 0; i < n; i++) if (type[i] == 1) qPos[i] = m++;
+    return m;
+}
+
+// SparseNewtonRaphsonPowerFlow.ComputeInjections (:269-289).
+void ComputeInjections(const ComplexCsr& y, const std::vector<double>& Vm, const std::vector<double>& Va,
+                       std::vector<double>& P, std::vector<double>& Q) {
+    for (int i = 0; i < y.n; i++) {
+        double pi = 0, qi = 0, vai = Va[i];
+        for (int k = y.rowPtr[i]; k < y.rowPtr[i + 1]; k++) {
+            int j = y.colIdx[k];
+            double th = vai - Va[j];
+            double sn = std::sin(th), cs = std::cos(th);
+            double vmj = Vm[j];
+            pi += vmj * (y.G[k] * cs + y.B[k] * sn);
+            qi += vmj * (y.G[k] * sn - y.B[k] * cs);
+        }
+        P[i] = Vm[i] * pi;
+        Q[i] = Vm[i] * qi;
+    }
+}
+
+// BuildJacobianStructure (:296-332).
+Csr BuildJacobianStructure(const ComplexCsr& y, const std::vector<int>& pPos, const std::vector<int>& qPos, int m,
+                           std::vector<int>& slots) {
+    std::vector<std::pair<int, int>> cells;
+    for (int i = 0; i < y.n; i++) {
+        int pi = pPos[i], qi = qPos[i];
+        if (pi < 0 && qi < 0) continue;
+        for (int k = y.rowPtr[i]; k < y.rowPtr[i + 1]; k++) {
+            int j = y.colIdx[k], pj = pPos[j], qj = qPos[j];
+            if (pi >= 0 && pj >= 0) cells.push_back({pi, pj});
+            if (pi >= 0 && qj >= 0) cells.push_back({pi, qj});
+            if (qi >= 0 && pj >= 0) cells.push_back({qi, pj});
+            if (qi >= 0 && qj >= 0) cells.push_back({qi, qj});
+        }
+    }
+    Csr jac = BuildCsrPattern(m, cells);
+    slots.assign(4 * y.rowPtr[y.n], -1);
+    for (int i = 0; i < y.n; i++) {
+        int pi = pPos[i], qi = qPos[i];
+        for (int k = y.rowPtr[i]; k < y.rowPtr[i + 1]; k++) {
+            int j = y.colIdx[k], pj = pPos[j], qj = qPos[j];
+            slots[4 * k + 0] = (pi >= 0 && pj >= 0) ? Locate(jac, pi, pj) : -1;
+            slots[4 * k + 1] = (pi >= 0 && qj >= 0) ? Locate(jac, pi, qj) : -1;
+            slots[4 * k + 2] = (qi >= 0 && pj >= 0) ? Locate(jac, qi, pj) : -1;
+            slots[4 * k + 3] = (qi >= 0 && qj >= 0) ? Locate(jac, qi, qj) : -1;
+        }
+    }
+    return jac;
+}
+
+// RefillJacobian (:342-380).
+void RefillJacobian(Csr& jac, const std::vector<int>& slots, const ComplexCsr& y, const std::vector<double>& Vm,
+                    const std::vector<double>& Va, const std::vector<double>& P, const std::vector<double>& Q) {
+    std::fill(jac.val.begin(), jac.val.end(), 0.0);
+    for (int i = 0; i < y.n; i++) {
+        for (int k = y.rowPtr[i]; k < y.rowPtr[i + 1]; k++) {
+            int j = y.colIdx[k];
+            double Gij = y.G[k], Bij = y.B[k];
+            double H, N, M, L;
+            if (i == j) {
+                H = -Q[i] - Bij * Vm[i] * Vm[i];
+                N = P[i] / Vm[i] + Gij * Vm[i];
+                M = P[i] - Gij * Vm[i] * Vm[i];
+                L = Q[i] / Vm[i] - Bij * Vm[i];
+            } else {
+                double th = Va[i] - Va[j];
+                double sn = std::sin(th), cs = std::cos(th);
+                H = Vm[i] * Vm[j] * (Gij * sn - Bij * cs);
+                N = Vm[i] * (Gij * cs + Bij * sn);
+                M = -Vm[i] * Vm[j] * (Gij * cs + Bij * sn);
+                L = Vm[i] * (Gij * sn - Bij * cs);
+            }
+            int s;
+            if ((s = slots[4 * k + 0]) >= 0) jac.val[s] = H;
+            if ((s = slots[4 * k + 1]) >= 0) jac.val[s] = N;
+            if ((s = slots[4 * k + 2]) >= 0) jac.val[s] = M;
+            if ((s = slots[4 * k + 3]) >= 0) jac.val[s] = L;
+        }
+    }
+}
+
+constexpr double kMaxUndampedStep = 0.4;  // NewtonShell.cs:38
+constexpr double kVmFloorPu = 0.01;       // NewtonShell.cs:48
+constexpr double kQLimitTolMva = 1e-3;    // NewtonShell.cs:26
+constexpr double kRevertVoltTolPu = 1e-4; // NewtonShell.cs:31
+
+struct RunEnd { bool converged = false, diverged = false; int iters = 0; double maxMis = INFINITY; };
+
+// RunNewton (:168-265) with NewtonShell.SolveStep (:74-120) and ApplyStep (:128-136).
+RunEnd RunNewton(CpuSparseLuSolver& solver, const ComplexCsr& y, const std::vector<int>& type, std::vector<double>& Vm,
+                 std::vector<double>& Va, const std::vector<double>& Pspec, const std::vector<double>& Qspec,
+                 std::vector<double>& P, std::vector<double>& Q, const gs_pf_opts& opt) {
+    int n = y.n;
+    std::vector<int> pPos, qPos;
+    int m = EquationPositions(type, pPos, qPos);
+    std::vector<double> f(m), dx(m);
+    std::vector<int> slots;
+    Csr jac = BuildJacobianStructure(y, pPos, qPos, m, slots);
+    RunEnd r;
+    double startMis = NAN;
+    int iter = 0;
+    for (;; iter++) {
+        ComputeInjections(y, Vm, Va, P, Q);
+        for (int i = 0; i < n; i++) {
+            if (pPos[i] >= 0) f[pPos[i]] = Pspec[i] - P[i];
+            if (qPos[i] >= 0) f[qPos[i]] = Qspec[i] - Q[i];
+        }
+        double maxMis = 0;
+        for (int k = 0; k < m; k++) maxMis = std::max(maxMis, std::fabs(f[k]));
+        // Math.Max propagates NaN; std::max does not: restate the .NET rule explicitly.
+        for (int k = 0; k < m; k++) if (std::isnan(f[k])) maxMis = NAN;
+        r.maxMis = maxMis;
+        if (iter == 0) startMis = maxMis;
+        if (maxMis < opt.tolerance) { r.converged = true; break; }
+        // NewtonShell.DivergedBeyondLimit (:177-178): Math.Max propagates a NaN, which then compares false.
+        double lim = std::isnan(startMis) ? NAN : std::max(opt.diverge_limit_pu, startMis);
+        if (maxMis > lim) { r.diverged = true; break; }
+        if (iter >= opt.max_iterations) break;
+        RefillJacobian(jac, slots, y, Vm, Va, P, Q);
+        bool ok = true;
+        for (double v : jac.val) if (!std::isfinite(v)) { ok = false; break; }
+        if (ok) for (double v : f) if (!std::isfinite(v)) { ok = false; break; }
+        std::vector<double> sol;
+        if (!ok) break;
+        if (!solver.Solve(jac, f, sol)) {
+            Ilu0 pc;
+            pc.Factor(jac);
+            if (!BiCgStab(jac, f, sol, pc, std::min(1e-10, opt.tolerance * 1e-3), 4 * m + 200)) break;
+        }
+        double maxAbs = 0;
+        for (int k = 0; k < m; k++) {
+            if (!std::isfinite(sol[k])) { ok = false; break; }
+            maxAbs = std::max(maxAbs, std::fabs(sol[k]));
+        }
+        if (!ok) break;
+        dx = sol;
+        double damp = maxAbs > kMaxUndampedStep ? kMaxUndampedStep / maxAbs : 1.0;
+        for (int i = 0; i < n; i++) {
+            if (pPos[i] >= 0) Va[i] += damp * dx[pPos[i]];
+            if (qPos[i] >= 0) { Vm[i] += damp * dx[qPos[i]]; if (Vm[i] < kVmFloorPu) Vm[i] = kVmFloorPu; }
+        }
+    }
+    r.iters = iter;
+    return r;
+}
+
+enum QPin { kPinNone = 0, kPinMax = 1, kPinMin = -1, kPinFixed = 2 };
+
+// NewtonShell.TryRevertPin (:563-576).
+bool TryRevertPin(int i, std::vector<int>& eff, std::vector<double>& vm, const std::vector<double>& vg,
+                  std::vector<int>& pinned, std::vector<int>& revertCount) {
+    if (pinned[i] == kPinNone || pinned[i] == kPinFixed || revertCount[i] >= 1) return false;
+    bool rMax = pinned[i] == kPinMax && vm[i] > vg[i] + kRevertVoltTolPu;
+    bool rMin = pinned[i] == kPinMin && vm[i] < vg[i] - kRevertVoltTolPu;
+    if (!(rMax || rMin)) return false;
+    eff[i] = 2;
+    vm[i] = vg[i];
+    pinned[i] = kPinNone;
+    revertCount[i]++;
+    return true;
+}
+
+// NewtonShell.ApplyQLimits (:519-558), constant-power loads, revert off by default.
+bool ApplyQLimits(const BusSpec& s, std::vector<int>& eff, const std::vector<double>& Q, std::vector<double>& qspec,
+                  double base, std::vector<double>& vm, std::vector<int>& pinned, std::vector<int>& revertCount,
+                  bool revert) {
+    bool changed = false;
+    for (size_t i = 0; i < eff.size(); i++) {
+        if (s.type0[i] != 2) continue;
+        if (eff[i] == 2) {
+            double qGen = Q[i] * base + s.qd[i];
+            if (qGen > s.qmax[i] + kQLimitTolMva) {
+                eff[i] = 1;
+                qspec[i] = (s.qmax[i] - s.qd[i]) / base;
+                pinned[i] = s.qmin[i] == s.qmax[i] ? kPinFixed : kPinMax;
+                changed = true;
+            } else if (qGen < s.qmin[i] - kQLimitTolMva) {
+                eff[i] = 1;
+                qspec[i] = (s.qmin[i] - s.qd[i]) / base;
+                pinned[i] = s.qmin[i] == s.qmax[i] ? kPinFixed : kPinMin;
+                changed = true;
+            }
+        } else if (revert) {
+            if (TryRevertPin((int)i, eff, vm, s.vg, pinned, revertCount)) changed = true;
+        }
+    }
+    return changed;
+}
+
+// RevertBrokenPins (:593-603).
+bool RevertBrokenPins(const BusSpec& s, std::vector<int>& eff, std::vector<double>& vm, std::vector<int>& pinned,
+                      std::vector<int>& revertCount) {
+    bool changed = false;
+    for (size_t i = 0; i < eff.size(); i++) {
+        if (s.type0[i] != 2 || eff[i] != 1) continue;
+        if (TryRevertPin((int)i, eff, vm, s.vg, pinned, revertCount)) changed = true;
+    }
+    return changed;
+}
+
+struct SolveOut {
+    int status = GS_PF_NOT_RUN;
+    int iterations = 0;
+    double maxMis = NAN;
+    std::vector<double> vm, va, p, q;  // va in radians; p, q in pu
+};
+
+// SparseNewtonRaphsonPowerFlow.SolveAcAttempt (:69-166) + NewtonShell.AssembleResult status (:649-693).
+// `vmStart/vaStart` (radians) replace the model's stored start when given (warm start, GridScenario.cs:35-52).
+SolveOut SolveModel(const Model& m, int skip, const gs_pf_opts& opt, const double* vmStart, const double* vaStartRad) {
+    int n = m.n;
+    ComplexCsr y = BuildY(m, skip);
+    Model mm;  // only the start values can differ
+    const Model* src = &m;
+    if (vmStart) {
+        mm = m;
+        for (int i = 0; i < n; i++) { mm.vm[i] = vmStart[i]; mm.vaDeg[i] = vaStartRad[i] * 180.0 / kPi; }
+        src = &mm;
+    }
+    BusSpec s = BuildBusSpec(*src, opt.flat_start != 0);
+    if (vmStart) {  // keep the radian start exactly (the degree round trip is not needed)
+        for (int i = 0; i < n; i++)
+            if (src->type[i] != 3 && !opt.flat_start) s.va[i] = vaStartRad[i];
+    }
+    std::vector<int> eff = s.type0, pinned(n, kPinNone), revertCount(n, 0);
+    std::vector<double> Vm = s.vm, Va = s.va, P(n), Q(n), qspec = s.qspec;
+    CpuSparseLuSolver solver;
+    bool converged = false;
+    int total = 0;
+    RunEnd re;
+    int qPasses = opt.enforce_q_limits ? 100 : 1;  // PowerFlowOptions.MaxQLimitPasses default (:101)
+    bool switchPending = false;
+    for (int qp = 0; qp < qPasses; qp++) {
+        switchPending = false;
+        re = RunNewton(solver, y, eff, Vm, Va, s.pspec, qspec, P, Q, opt);
+        converged = re.converged;
+        total += re.iters;
+        if (!opt.enforce_q_limits) break;
+        if (!converged) break;
+        bool changed = ApplyQLimits(s, eff, Q, qspec, m.base, Vm, pinned, revertCount, false);
+        if (!changed) changed = RevertBrokenPins(s, eff, Vm, pinned, revertCount);
+        switchPending = changed;
+        if (!changed) break;
+    }
+    if (switchPending) {
+        re = RunNewton(solver, y, eff, Vm, Va, s.pspec, qspec, P, Q, opt);
+        total += re.iters;
+        converged = false;
+    }
+    ComputeInjections(y, Vm, Va, P, Q);
+    SolveOut o;
+    bool finite = std::isfinite(re.maxMis);
+    for (int i = 0; i < n; i++)
+        finite = finite && std::isfinite(Vm[i]) && std::isfinite(Va[i]) && std::isfinite(P[i] * m.base) &&
+                 std::isfinite(Q[i] * m.base);
+    o.status = !finite ? GS_PF_NON_FINITE
+             : converged ? GS_PF_CONVERGED
+             : (!converged && re.diverged) ? GS_PF_DIVERGED
+             : GS_PF_MAX_ITERATIONS;
+    o.iterations = total;
+    o.maxMis = re.maxMis;
+    o.vm = Vm; o.va = Va; o.p = P; o.q = Q;
+    return o;
+}
+
+// NewtonShell.ComputeLineFlows (:699-734): per-branch complex flows (MVA) and loading %.
+void LineFlows(const Model& m, int skip, const std::vector<double>& vm, const std::vector<double>& va,
+               double* loading, double* sf, double* st) {
+    for (int k = 0; k < (int)m.br.size(); k++) {
+        const Br& br = m.br[k];
+        if (k == skip || !br.inService) {
+            if (loading) loading[k] = 0;
+            if (sf) { sf[2 * k] = 0; sf[2 * k + 1] = 0; }
+            if (st) { st[2 * k] = 0; st[2 * k + 1] = 0; }
+            continue;
+        }
+        cplx vf = std::polar(vm[br.f], va[br.f]);
+        cplx vt = std::polar(vm[br.t], va[br.t]);
+        Stamp s = BranchStamp(br.r, br.x, br.b, br.tap, br.shift);
+        cplx iF = s.yff * vf + s.yft * vt;
+        cplx iT = s.ytf * vf + s.ytt * vt;
+        cplx sF = vf * std::conj(iF) * m.base;
+        cplx sT = vt * std::conj(iT) * m.base;
+        double mva = std::max(std::abs(sF), std::abs(sT));
+        if (loading) loading[k] = br.rateA > 0 ? mva / br.rateA * 100.0 : 0.0;
+        if (sf) { sf[2 * k] = sF.real(); sf[2 * k + 1] = sF.imag(); }
+        if (st) { st[2 * k] = sT.real(); st[2 * k + 1] = sT.imag(); }
+    }
+}
+
+struct Violation { int kind, element; double value; };
+
+// ContingencyAnalysis.ScreenStateCore (:1105-1238), converged branch: thermal (:1156-1180, keyed by the
+// ORIGINAL branch index, threshold 100 %), voltage per-bus (:1196-1223) or the 0.94/1.06 band (:1226-1235,
+// VoltageLimits.cs:28-31). Boundaries do not exist in these grids.
+void Classify(const Model& m, int skip, const std::vector<double>& vm, const std::vector<double>& va, bool perBus,
+              double& maxLoad, double& minVm, double& maxVm, std::vector<Violation>& out) {
+    std::vector<double> loading(m.br.size());
+    LineFlows(m, skip, vm, va, loading.data(), nullptr, nullptr);
+    maxLoad = 0;
+    for (int k = 0; k < (int)m.br.size(); k++) {
+        if (k == skip) continue;  // the reduced model has no such branch
+        double l = loading[k];
+        if (l > maxLoad) maxLoad = l;
+        if (l > 100.0) out.push_back({GS_VIOL_BRANCH_OVERLOAD, k, l});
+    }
+    minVm = INFINITY; maxVm = -INFINITY;
+    for (int i = 0; i < m.n; i++) { minVm = std::min(minVm, vm[i]); maxVm = std::max(maxVm, vm[i]); }
+    bool hasPerBus = false;
+    for (int i = 0; i < m.n; i++) if (!std::isnan(m.vmin[i]) || !std::isnan(m.vmax[i])) hasPerBus = true;
+    for (int i = 0; i < m.n; i++) {
+        double lo = 0.94, hi = 1.06;
+        if (perBus && hasPerBus) {
+            if (!std::isnan(m.vmin[i])) lo = m.vmin[i];
+            if (!std::isnan(m.vmax[i])) hi = m.vmax[i];
+        }
+        if (vm[i] < lo) out.push_back({GS_VIOL_UNDERVOLTAGE, m.id[i], vm[i]});
+        else if (vm[i] > hi) out.push_back({GS_VIOL_OVERVOLTAGE, m.id[i], vm[i]});
+    }
+}
+
+bool OptionsSupported(const gs_pf_opts* o) { return o && !o->retry_from_dc_start; }
+
+}  // namespace
+
+// =============================================================================================
+// C API of the oracle (test infrastructure). All outputs are caller-owned.
+extern "C" {
+
+int gso_pf_solve(const gs_grid_desc* d, const gs_pf_opts* opt, gs_pf_result* res) {
+    if (!d || !res || !OptionsSupported(opt)) return GS_ERR_INVALID_ARG;
+    Model m = FromDesc(d);
+    SolveOut o = SolveModel(m, -1, *opt, nullptr, nullptr);
+    res->status = o.status;
+    res->iterations = o.iterations;
+    res->max_mismatch = o.maxMis;
+    for (int i = 0; i < m.n; i++) {
+        if (res->vm) res->vm[i] = o.vm[i];
+        if (res->va_deg) res->va_deg[i] = o.va[i] * 180.0 / kPi;
+        if (res->p_inj_mw) res->p_inj_mw[i] = o.p[i] * m.base;
+        if (res->q_inj_mvar) res->q_inj_mvar[i] = o.q[i] * m.base;
+    }
+    LineFlows(m, -1, o.vm, o.va, res->loading_pct, res->sf_mva, res->st_mva);
+    return GS_OK;
+}
+
+// Jacobian of the intact grid at its start point, in the reference's own CSR (for kernel checks).
+// Returns m; fills rowPtr [m+1], colIdx/val [nnz] when the capacities allow (nnz returned in *nnz).
+int gso_jacobian(const gs_grid_desc* d, int32_t* m_out, int32_t* nnz_out, int32_t* rowPtr, int32_t* colIdx,
+                 double* val, int32_t cap, double* mismatch, int32_t mis_cap) {
+    if (!d) return GS_ERR_INVALID_ARG;
+    Model mdl = FromDesc(d);
+    ComplexCsr y = BuildY(mdl, -1);
+    BusSpec s = BuildBusSpec(mdl, false);
+    std::vector<int> pPos, qPos, slots;
+    int m = EquationPositions(s.type0, pPos, qPos);
+    Csr jac = BuildJacobianStructure(y, pPos, qPos, m, slots);
+    std::vector<double> P(mdl.n), Q(mdl.n);
+    ComputeInjections(y, s.vm, s.va, P, Q);
+    RefillJacobian(jac, slots, y, s.vm, s.va, P, Q);
+    *m_out = m;
+    *nnz_out = (int32_t)jac.colIdx.size();
+    if (mismatch && mis_cap >= m) {
+        for (int i = 0; i < mdl.n; i++) {
+            if (pPos[i] >= 0) mismatch[pPos[i]] = s.pspec[i] - P[i];
+            if (qPos[i] >= 0) mismatch[qPos[i]] = s.qspec[i] - Q[i];
+        }
+    }
+    if (cap < (int)jac.colIdx.size()) return GS_ERR_CAPACITY;
+    for (int i = 0; i <= m; i++) rowPtr[i] = jac.rowPtr[i];
+    for (size_t k = 0; k < jac.colIdx.size(); k++) { colIdx[k] = jac.colIdx[k]; val[k] = jac.val[k]; }
+    return GS_OK;
+}
+
+// Minimum-degree order of a CSR pattern (for ordering tests).
+int gso_md_order(int32_t n, const int32_t* rowPtr, const int32_t* colIdx, int32_t* order) {
+    std::vector<int> rp(rowPtr, rowPtr + n + 1), ci(colIdx, colIdx + rowPtr[n]);
+    std::vector<int> q = MinimumDegree(n, rp, ci);
+    for (int i = 0; i < n; i++) order[i] = q[i];
+    return GS_OK;
+}
+
+// Sparse direct solve A x = b (ISparseLinearSolver via CpuSparseLuSolver). Returns 1 when singular.
+int gso_sparse_solve(int32_t n, const int32_t* rowPtr, const int32_t* colIdx, const double* val, const double* b,
+                     double* x) {
+    Csr a;
+    a.n = n;
+    a.rowPtr.assign(rowPtr, rowPtr + n + 1);
+    a.colIdx.assign(colIdx, colIdx + rowPtr[n]);
+    a.val.assign(val, val + rowPtr[n]);
+    CpuSparseLuSolver s;
+    std::vector<double> bv(b, b + n), xv;
+    if (!s.Solve(a, bv, xv)) return 1;
+    for (int i = 0; i < n; i++) x[i] = xv[i];
+    return GS_OK;
+}
+
+// ScreenBranchesParallel (ContingencyAnalysis.cs:323-344): one outage per task on `threads` host threads
+// (0 = all). Output layout is gs_n1_result's. With warm_start_from_base the intact grid is solved first
+// and its state starts every outage (GridScenario.WithSolvedVoltages).
+int gso_n1_screen(const gs_grid_desc* d, int32_t nOut, const int32_t* idx, const gs_pf_opts* opt, int32_t threads,
+                  gs_n1_result* res) {
+    if (!d || !res || !OptionsSupported(opt) || nOut < 0) return GS_ERR_INVALID_ARG;
+    Model m = FromDesc(d);
+    for (int k = 0; k < nOut; k++)
+        if (idx[k] < 0 || idx[k] >= (int)m.br.size() || !m.br[idx[k]].inService) return GS_ERR_INVALID_ARG;
+    std::vector<double> vm0, va0;
+    res->base_status = GS_PF_NOT_RUN;
+    res->base_iterations = 0;
+    if (opt->warm_start_from_base) {
+        SolveOut b = SolveModel(m, -1, *opt, nullptr, nullptr);
+        res->base_status = b.status;
+        res->base_iterations = b.iterations;
+        vm0 = b.vm;
+        va0 = b.va;
+    }
+    std::vector<SolveOut> outs(nOut);
+    std::vector<std::vector<Violation>> viol(nOut);
+    std::vector<double> maxLoad(nOut, 0), minVm(nOut, 0), maxVm(nOut, 0);
+    std::atomic<int> cursor{0};
+    auto work = [&]() {
+        for (;;) {
+            int k = cursor.fetch_add(1);
+            if (k >= nOut) return;
+            outs[k] = SolveModel(m, idx[k], *opt, vm0.empty() ? nullptr : vm0.data(),
+                                 va0.empty() ? nullptr : va0.data());
+            if (outs[k].status == GS_PF_CONVERGED)
+                Classify(m, idx[k], outs[k].vm, outs[k].va, opt->per_bus_voltage_limits != 0, maxLoad[k], minVm[k],
+                         maxVm[k], viol[k]);
+        }
+    };
+    int nt = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    nt = std::max(1, std::min(nt, std::max(1, nOut)));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; t++) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+
+    int total = 0;
+    for (int k = 0; k < nOut; k++) total += (int)viol[k].size();
+    res->viol_count = total;
+    bool fits = total <= res->viol_capacity;
+    int w = 0;
+    for (int k = 0; k < nOut; k++) {
+        if (res->status) res->status[k] = outs[k].status;
+        if (res->iterations) res->iterations[k] = outs[k].iterations;
+        if (res->max_mismatch) res->max_mismatch[k] = outs[k].maxMis;
+        if (res->min_vm) res->min_vm[k] = minVm[k];
+        if (res->max_vm) res->max_vm[k] = maxVm[k];
+        if (res->max_loading_pct) res->max_loading_pct[k] = maxLoad[k];
+        if (res->viol_ptr) res->viol_ptr[k] = w;
+        for (const Violation& v : viol[k]) {
+            if (fits && res->viol_kind) {
+                res->viol_kind[w] = v.kind;
+                res->viol_element[w] = v.element;
+                res->viol_value[w] = v.value;
+            }
+            w++;
+        }
+        if (res->vm)
+            for (int i = 0; i < m.n; i++) res->vm[(size_t)k * m.n + i] = outs[k].vm[i];
+        if (res->va_deg)
+            for (int i = 0; i < m.n; i++) res->va_deg[(size_t)k * m.n + i] = outs[k].va[i] * 180.0 / kPi;
+    }
+    if (res->viol_ptr) res->viol_ptr[nOut] = w;
+    return fits ? GS_OK : GS_ERR_CAPACITY;
+}
+
+}  // extern "C"

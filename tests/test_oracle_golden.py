@@ -1,0 +1,68 @@
+"""The oracle pinned against the reference's own known answers (CPU only).
+
+Sources: PowerFlowTests.cs:11-15,38-60 (case9), IeeeCasesTests.cs:16-24,91-95 (case14/57/118/300),
+ContingencyCorrectnessTests.cs:143-154 (case118 N-1 counts), :209-237 (case14 base case and raw counts).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from gridsim_b200 import _abi
+from tests.conftest import golden_model
+
+
+@pytest.mark.parametrize("name", ["case9", "case14", "case57", "case118", "case300"])
+def test_published_voltages(name):
+    m, pub = golden_model(name)
+    o = _abi.default_opts()
+    o.enforce_q_limits = 1  # the reference tests solve with the default options (Q limits on)
+    r = oracle.solve(m, o)
+    assert r["status"] == _abi.PF_CONVERGED
+    assert r["max_mismatch"] < 1e-8
+    slack = int(np.nonzero(m.bus_type == 3)[0][0])
+    va = r["va_deg"] - r["va_deg"][slack] + pub["va_deg"][slack]  # re-referenced as IeeeCasesTests does
+    assert np.max(np.abs(r["vm"] - pub["vm"])) <= pub["vm_tol"]
+    assert np.max(np.abs(va - pub["va_deg"])) <= pub["va_tol_deg"]
+
+
+def test_case9_slack_and_losses():
+    m, _ = golden_model("case9")
+    r = oracle.solve(m)
+    assert abs(r["p_inj_mw"][0] - 71.64) < 0.05   # PowerFlowTests.cs:52-55
+    assert abs(r["p_inj_mw"].sum() - 4.641) < 0.005
+    assert r["iterations"] <= 6
+
+
+def test_case9_iteration_cap_reports_max_iterations():
+    m, _ = golden_model("case9")
+    o = _abi.default_opts()
+    o.max_iterations = 1
+    o.flat_start = 1
+    r = oracle.solve(m, o)
+    assert r["status"] == _abi.PF_MAX_ITERATIONS  # PowerFlowTests.cs:27-36
+
+
+def _counts(r):
+    conv = r["status"] == _abi.PF_CONVERGED
+    nv = np.diff(r["viol_ptr"])
+    return int(np.sum(conv & (nv == 0))), int(np.sum(conv & (nv > 0))), int(np.sum(~conv))
+
+
+def test_case118_n1_counts_under_study_options(study_opts):
+    m, _ = golden_model("case118")
+    r = oracle.screen(m, m.in_service_branches(), study_opts)
+    assert _counts(r) == (164, 13, 9)
+
+
+def test_case14_base_and_raw_counts(study_opts):
+    m, _ = golden_model("case14")
+    b = oracle.screen(m, np.zeros(0, np.int32), study_opts)
+    # the base case through the same classification: solve the intact grid as a screen of no outage
+    base = oracle.solve(m, study_opts)
+    assert base["status"] == _abi.PF_CONVERGED
+    over = [int(m.bus_id[i]) for i in range(m.n_bus) if base["vm"][i] > 1.06]
+    assert over == [6, 7, 8]
+    assert abs(base["vm"][list(m.bus_id).index(8)] - 1.09) < 1e-12
+    raw = oracle.screen(m, m.in_service_branches(), study_opts)
+    assert _counts(raw) == (0, 19, 1)
+    assert b["viol_ptr"].shape == (1,)
