@@ -65,6 +65,7 @@ class GridModel:
     rate_a: np.ndarray
     br_in_service: np.ndarray
     is_transformer: np.ndarray
+    meta: dict = field(default_factory=dict)
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -80,7 +81,8 @@ class GridModel:
         return int(self.gen_bus.shape[0])
 
     def copy(self) -> "GridModel":
-        kw = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in self.__dict__.items() if k != "_keep"}
+        kw = {k: (v.copy() if isinstance(v, (np.ndarray, dict)) else v) for k, v in self.__dict__.items()
+              if k != "_keep"}
         return GridModel(**kw)
 
     def with_voltages(self, vm: np.ndarray, va_deg: np.ndarray) -> "GridModel":
