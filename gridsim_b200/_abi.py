@@ -44,7 +44,8 @@ class PfOpts(ctypes.Structure):
     _fields_ = [
         ("tolerance", c_f64), ("diverge_limit_pu", c_f64), ("max_iterations", c_i32), ("flat_start", c_i32),
         ("enforce_q_limits", c_i32), ("retry_from_dc_start", c_i32), ("per_bus_voltage_limits", c_i32),
-        ("precision", c_i32), ("warm_start_from_base", c_i32), ("batch_width", c_i32), ("reserved", c_i32 * 8),
+        ("precision", c_i32), ("warm_start_from_base", c_i32), ("batch_width", c_i32), ("phase_timing", c_i32),
+        ("reserved", c_i32 * 7),
     ]
 
 
@@ -62,7 +63,8 @@ class N1Result(ctypes.Structure):
         ("max_loading_pct", c_vp), ("viol_ptr", c_vp), ("viol_capacity", c_i32), ("viol_count", c_i32),
         ("viol_kind", c_vp), ("viol_element", c_vp), ("viol_value", c_vp), ("vm", c_vp), ("va_deg", c_vp),
         ("base_status", c_i32), ("base_iterations", c_i32), ("device_ms", c_f64), ("n_singular_pivot", c_i32),
-        ("n_batches", c_i32),
+        ("n_batches", c_i32), ("kernel_launches", ctypes.c_int64), ("newton_iterations", c_i32), ("reserved1", c_i32),
+        ("factor_ms", c_f64), ("solve_ms", c_f64), ("mismatch_ms", c_f64), ("other_ms", c_f64), ("factor_bytes", c_f64),
     ]
 
 
@@ -88,6 +90,7 @@ EXPORTS = {
     "gs_pf_solve": (c_i32, [c_vp, ctypes.POINTER(PfOpts), ctypes.POINTER(PfResult)]),
     "gs_pf_solve_batch": (c_i32, [c_vp, c_i32, c_vp, c_vp, ctypes.POINTER(PfOpts), c_vp, c_vp, c_vp, c_vp, c_vp]),
     "gs_n1_screen": (c_i32, [c_vp, c_i32, c_vp, ctypes.POINTER(PfOpts), ctypes.POINTER(N1Result)]),
+    "gs_analyze_host": (c_i32, [ctypes.POINTER(GridDesc), ctypes.POINTER(GridInfo)]),
 }
 
 _lib = None

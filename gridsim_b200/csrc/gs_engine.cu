@@ -1,0 +1,1505 @@
+// gs_engine.cu — the batched Newton-Raphson load-flow engine and its C ABI (sm_100a).
+//
+// One Newton iteration of a batch of B systems (contingencies, load scalings, requests) of one grid:
+//   1. k_mismatch_jac  — per (bus, system): injections P_i, Q_i over row i of Y (FP64, the outaged
+//                        branch's four cells replaced by their reduced values), mismatch into the
+//                        right-hand side, max-norm per system, Jacobian blocks H/N/M/L written straight
+//                        into the LU slots of the shared static-pivot pattern
+//                        (ComputeInjections :269-289, mismatch :216-235, RefillJacobian :342-380 of
+//                        src/GridSim.Core/PowerFlow/SparseNewtonRaphsonPowerFlow.cs);
+//   2. k_status        — per system: converged / diverged / cap / non-finite tests in the reference's
+//                        order (RunNewton :235-238, NewtonShell.DivergedBeyondLimit :177-178);
+//   3. factorisation   — per elimination-tree level, two phases (pivots, upper and forward entries; then
+//                        lower entries): every entry its own sparse dot product over the row subtree of its
+//                        node (k_level launches for the wide levels, one k_persistent launch for the
+//                        narrow top of the tree);
+//   4. backward substitution, levels top down (k_persistent, then k_level launches);
+//   5. k_dxmax, k_update — max |dx| per system, damped update with the Vm floor
+//                        (NewtonShell.ApplyStep :128-136, MaxUndampedStep 0.4, VmFloorPu 0.01).
+// Steps 3-5 are captured once per batch into a CUDA graph and replayed every iteration; the host reads
+// one counter (systems still active) per iteration.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "gs_host.h"
+#include "gs_kernels.cuh"
+
+namespace gs {
+
+constexpr double kMaxUndampedStep = 0.4;
+constexpr double kRefineBelowPu = 1e-3;
+constexpr double kVmFloorPu = 0.01;
+
+__device__ __forceinline__ void atomicMaxNonNeg(unsigned long long* a, double v) {
+    atomicMax(a, (unsigned long long)__double_as_longlong(v));
+}
+
+// ---------------------------------------------------------------------------------------------
+// 1. mismatch + Jacobian fill. Block (32, 8): lane = system, y = bus within the block.
+template <typename T>
+__global__ void __launch_bounds__(256) k_mismatch_jac(DevGrid g, DevBatch b, int fillJac, double* pOut, double* qOut) {
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int s = blockIdx.y * 32 + lane;
+    const int i = blockIdx.x * 8 + w;
+    const size_t B = (size_t)b.B;
+    double localMax = 0.0;
+    int bad = 0;  // 1: mismatch not finite, 2: Jacobian not finite
+    const bool live = i < g.n && s < b.count && b.active[s];
+    if (live) {
+        const int o = b.outage[s];
+        int c0 = -1, c1 = -1, c2 = -1, c3 = -1;
+        if (o >= 0) { c0 = g.brCell[4 * o]; c1 = g.brCell[4 * o + 1]; c2 = g.brCell[4 * o + 2]; c3 = g.brCell[4 * o + 3]; }
+        const double vmi = b.vm[i * B + s], vai = b.va[i * B + s];
+        double pi = 0.0, qi = 0.0;
+        const int p0 = g.yRowPtr[i], p1 = g.yRowPtr[i + 1];
+        for (int p = p0; p < p1; p++) {
+            const int j = g.yCol[p];
+            double G = g.yG[p], Bv = g.yB[p];
+            if (p == c0) { G = g.brRed[8 * o + 0]; Bv = g.brRed[8 * o + 1]; }
+            else if (p == c1) { G = g.brRed[8 * o + 2]; Bv = g.brRed[8 * o + 3]; }
+            else if (p == c2) { G = g.brRed[8 * o + 4]; Bv = g.brRed[8 * o + 5]; }
+            else if (p == c3) { G = g.brRed[8 * o + 6]; Bv = g.brRed[8 * o + 7]; }
+            double sn, cs;
+            sincos(vai - b.va[j * B + s], &sn, &cs);
+            const double vmj = b.vm[j * B + s];
+            pi += vmj * (G * cs + Bv * sn);
+            qi += vmj * (G * sn - Bv * cs);
+        }
+        const double P = vmi * pi, Q = vmi * qi;
+        if (pOut) { pOut[i * B + s] = P; qOut[i * B + s] = Q; }
+        double sc = b.loadScale ? b.loadScale[i * B + s] : 1.0;
+        const double pspec = b.loadScale ? g.pgen[i] - sc * g.pload[i] : g.pgen[i] - g.pload[i];
+        const double qspec = b.loadScale ? g.qgen[i] - sc * g.qload[i] : g.qgen[i] - g.qload[i];
+        T* y = (T*)b.y;
+        const int kp = g.busP[i], kq = g.busQ[i];
+        if (kp >= 0) {
+            const double f = pspec - P;
+            y[kp * B + s] = (T)f;
+            if (b.rhs64) b.rhs64[kp * B + s] = f;
+            localMax = fmax(localMax, fabs(f));
+            bad |= isfinite(f) ? 0 : 1;
+        }
+        if (kq >= 0) {
+            const double f = qspec - Q;
+            y[kq * B + s] = (T)f;
+            if (b.rhs64) b.rhs64[kq * B + s] = f;
+            localMax = fmax(localMax, fabs(f));
+            bad |= isfinite(f) ? 0 : 1;
+        }
+        if (fillJac && (kp >= 0 || kq >= 0)) {
+            T* lu = (T*)b.lu;
+            for (int p = p0; p < p1; p++) {
+                const int j = g.yCol[p];
+                double G = g.yG[p], Bv = g.yB[p];
+                if (p == c0) { G = g.brRed[8 * o + 0]; Bv = g.brRed[8 * o + 1]; }
+                else if (p == c1) { G = g.brRed[8 * o + 2]; Bv = g.brRed[8 * o + 3]; }
+                else if (p == c2) { G = g.brRed[8 * o + 4]; Bv = g.brRed[8 * o + 5]; }
+                else if (p == c3) { G = g.brRed[8 * o + 6]; Bv = g.brRed[8 * o + 7]; }
+                double H, N, M, L;
+                if (i == j) {
+                    H = -Q - Bv * vmi * vmi;
+                    N = P / vmi + G * vmi;
+                    M = P - G * vmi * vmi;
+                    L = Q / vmi - Bv * vmi;
+                } else {
+                    double sn, cs;
+                    sincos(vai - b.va[j * B + s], &sn, &cs);
+                    const double vmj = b.vm[j * B + s];
+                    H = vmi * vmj * (G * sn - Bv * cs);
+                    N = vmi * (G * cs + Bv * sn);
+                    M = -vmi * vmj * (G * cs + Bv * sn);
+                    L = vmi * (G * sn - Bv * cs);
+                }
+                const int4 sl = *reinterpret_cast<const int4*>(g.ySlot + 4 * p);
+                if (sl.x >= 0) lu[sl.x * B + s] = (T)H;
+                if (sl.y >= 0) lu[sl.y * B + s] = (T)N;
+                if (sl.z >= 0) lu[sl.z * B + s] = (T)M;
+                if (sl.w >= 0) lu[sl.w * B + s] = (T)L;
+                bad |= (isfinite(H) && isfinite(N) && isfinite(M) && isfinite(L)) ? 0 : 2;
+            }
+        }
+    }
+    __shared__ double red[8][32];
+    __shared__ int redBad[8][32];
+    red[w][lane] = localMax;
+    redBad[w][lane] = bad;
+    __syncthreads();
+    if (w == 0 && s < b.count) {
+        double mx = red[0][lane];
+        int anyBad = redBad[0][lane];
+        for (int q = 1; q < 8; q++) { mx = fmax(mx, red[q][lane]); anyBad |= redBad[q][lane]; }
+        if (mx > 0.0) atomicMaxNonNeg(&b.maxMis[s], mx);
+        if (anyBad & 1) atomicOr(&b.flags[s], kFlagNonFinite);
+        if (anyBad & 2) atomicOr(&b.flags[s], kFlagJacBad);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// 2. per-system Newton control (RunNewton :218-238). With `polish` > 0 (mixed precision), a system that
+//    has met the tolerance keeps its Converged status and takes at most `polish` more steps while its
+//    mismatch is above tol * 1e-3: the FP32 step converges linearly, so the first state under the
+//    tolerance can sit ~||J^-1|| * tol from the root; the extra steps bring it to the root the FP64
+//    iteration reaches. The status (and so every convergence flag) is decided at the first crossing.
+__global__ void k_status(DevBatch b, int iter, double tol, double divLimit, int maxIter, int polish) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= b.count || !b.active[s]) return;
+    const double mis = __longlong_as_double((long long)b.maxMis[s]);
+    b.maxMis[s] = 0ull;
+    b.maxDx[s] = 0ull;
+    const int fl = b.flags[s];
+    if (b.convAt[s] >= 0) {  // polishing a converged state
+        const bool ok = !(fl & (kFlagNonFinite | kFlagStepBad | kFlagJacBad)) && mis < tol;
+        if (ok) b.finalMis[s] = mis;
+        if (!ok || mis < tol * 1e-3 || iter - b.convAt[s] >= polish) { b.active[s] = 0; return; }
+        atomicAdd(b.activeCount, 1);
+        return;
+    }
+    if (fl & kFlagNonFinite) {  // a NaN mismatch never converges; the non-finite step then stops the run
+        b.finalMis[s] = NAN;
+        b.status[s] = GS_PF_NON_FINITE;
+        b.active[s] = 0;
+        return;
+    }
+    if (fl & kFlagStepBad) {  // the previous step was refused: the run stops, state unchanged
+        b.status[s] = GS_PF_MAX_ITERATIONS;
+        b.active[s] = 0;
+        return;
+    }
+    b.finalMis[s] = mis;
+    if (iter == 0) b.startMis[s] = mis;
+    if (mis < tol) {
+        b.status[s] = GS_PF_CONVERGED;
+        b.convIters[s] = b.iters[s];
+        if (polish > 0 && mis >= tol * 1e-3 && !(fl & kFlagJacBad)) {
+            b.convAt[s] = iter;
+            atomicAdd(b.activeCount, 1);
+        } else {
+            b.active[s] = 0;
+        }
+        return;
+    }
+    if (mis > fmax(divLimit, b.startMis[s])) { b.status[s] = GS_PF_DIVERGED; b.active[s] = 0; return; }
+    if (iter >= maxIter) { b.status[s] = GS_PF_MAX_ITERATIONS; b.active[s] = 0; return; }
+    if (fl & kFlagJacBad) { b.status[s] = GS_PF_MAX_ITERATIONS; b.active[s] = 0; return; }  // SolveStep refuses it
+    // Mixed precision refines the FP32 step with the FP64 residual once the mismatch is small: far from the
+    // root the Newton step is self-correcting and an FP32 step error of ~kappa * 2^-24 changes nothing.
+    if (b.refine) b.refine[s] = mis < kRefineBelowPu ? 1 : 0;
+    atomicAdd(b.activeCount, 1);
+}
+
+// ---------------------------------------------------------------------------------------------
+// 3. fused factorisation + forward substitution of one elimination-tree level.
+//
+// Warp layout of the LU kernels: S systems x P = 32 / S pair lanes (S = 8 for FP32, 4 for FP64, so that the
+// lanes of one pair lane read exactly one 32-byte sector). An entry's index pairs are dealt round-robin to the
+// P pair lanes; each lane accumulates its products, then a fixed butterfly over the pair lanes sums them (a
+// fixed order: the result is deterministic). A warp therefore finishes a 32-pair batch in one round of loads
+// instead of 32 / 8 rounds, and there are P times more warps per level than with one system per lane.
+template <typename T>
+struct Lay {
+    static constexpr int S = sizeof(T) == 4 ? 8 : 4;  // systems per warp
+    static constexpr int P = 32 / S;                  // pair lanes
+};
+
+// sum over pairs q in [q0, q1) of lu[a] * rhs[c] for this lane's system, complete in every pair lane.
+template <typename T>
+__device__ __forceinline__ T dotSP(const T* __restrict__ lu, const T* __restrict__ rhs, const int2* __restrict__ pr,
+                                   int64_t q0, int64_t q1, size_t B, int s) {
+    constexpr int S = Lay<T>::S, P = Lay<T>::P;
+    const int lane = threadIdx.x & 31;
+    const int pl = lane / S;
+    T acc = T(0);
+    for (int64_t base = q0; base < q1; base += 32) {
+        const int cnt = (int)min((int64_t)32, q1 - base);
+        const int2 mine = lane < cnt ? __ldg(pr + base + lane) : make_int2(0, 0);
+        T l[S], r[S];
+#pragma unroll
+        for (int u = 0; u < S; u++) {
+            const int src = pl + P * u;
+            const int a = __shfl_sync(0xffffffffu, mine.x, src);
+            const int c = __shfl_sync(0xffffffffu, mine.y, src);
+            const bool ok = src < cnt;
+            l[u] = ok ? lu[a * B + s] : T(0);
+            r[u] = ok ? rhs[c * B + s] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < S; u++) acc += l[u] * r[u];
+    }
+#pragma unroll
+    for (int off = S; off < 32; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    return acc;
+}
+
+template <typename T>
+__device__ __forceinline__ T pivotFloor();
+template <>
+__device__ __forceinline__ double pivotFloor<double>() { return 1e-12; }
+template <>
+__device__ __forceinline__ float pivotFloor<float>() { return 1e-6f; }
+
+// one lane group's sum over pairs q in [q0, q1) of lu[a] * rhs[c] for its system (serial in q)
+template <typename T>
+__device__ __forceinline__ T dotSerial(const T* __restrict__ lu, const T* __restrict__ rhs, const int2* __restrict__ pr,
+                                       int64_t q0, int64_t q1, size_t B, int s) {
+    T acc = T(0);
+    int64_t q = q0;
+    for (; q + 4 <= q1; q += 4) {
+        const int2 a0 = __ldg(pr + q), a1 = __ldg(pr + q + 1), a2 = __ldg(pr + q + 2), a3 = __ldg(pr + q + 3);
+        const T l0 = lu[a0.x * B + s], r0 = rhs[a0.y * B + s];
+        const T l1 = lu[a1.x * B + s], r1 = rhs[a1.y * B + s];
+        const T l2 = lu[a2.x * B + s], r2 = rhs[a2.y * B + s];
+        const T l3 = lu[a3.x * B + s], r3 = rhs[a3.y * B + s];
+        acc += l0 * r0;
+        acc += l1 * r1;
+        acc += l2 * r2;
+        acc += l3 * r3;
+    }
+    for (; q < q1; q++) {
+        const int2 a = __ldg(pr + q);
+        acc += lu[a.x * B + s] * rhs[a.y * B + s];
+    }
+    return acc;
+}
+
+// One entry of the fused factorisation: A - sum(left * right), divided by the node's pivot for lower entries;
+// the diagonal's result is the pivot (kept in its own array: the diagonal slot keeps A(k, k)). `wide`: the
+// whole warp computes this entry (pair lanes + butterfly), else this lane group alone.
+template <typename T>
+__device__ __forceinline__ void factorEntry(const DevGrid& g, const DevBatch& b, int e, int s, bool act, bool wide) {
+    const size_t B = (size_t)b.B;
+    T* lu = (T*)b.lu;
+    T* y = (T*)b.y;
+    const int kind = g.entKind[e];
+    const int slot = g.entSlot[e];
+    const int node = g.entNode[e];
+    const int64_t q0 = g.entPairPtr[e], q1 = g.entPairPtr[e + 1];
+    const T* rhs = kind == kFwd ? y : lu;
+    const T dot = wide ? dotSP<T>(lu, rhs, g.pairs, q0, q1, B, s) : dotSerial<T>(lu, rhs, g.pairs, q0, q1, B, s);
+    const bool writer = !wide || (threadIdx.x & 31) < Lay<T>::S;
+    if (kind == kFwd) {
+        const T v = y[slot * B + s] - dot;
+        if (writer) y[slot * B + s] = v;
+        return;
+    }
+    const T a = g.entHasA[e] ? lu[slot * B + s] : T(0);
+    T v = a - dot;
+    if (kind == kDiag) {
+        const T fl = pivotFloor<T>() * (fabs(a) > T(1) ? fabs(a) : T(1));
+        if (!(fabs(v) > fl)) {  // static pivot collapsed (or NaN): perturb, flag, keep going
+            if (act && writer) atomicOr(&b.flags[s], kFlagPivotPerturbed);
+            v = (v < T(0)) ? -fl : fl;
+        }
+        if (writer) ((T*)b.piv)[node * B + s] = v;
+        return;
+    }
+    if (kind == kLower) v = v / ((const T*)b.piv)[node * B + s];
+    if (writer) lu[slot * B + s] = v;
+}
+
+// backward substitution of node levelNodes[q]: x(k) = (y(k) - sum U(k, r) x(r)) / U(k, k), in place
+template <typename T>
+__device__ __forceinline__ void backwardNode(const DevGrid& g, const DevBatch& b, T* y, int q, int s, bool wide) {
+    constexpr int S = Lay<T>::S, P = Lay<T>::P;
+    const size_t B = (size_t)b.B;
+    const T* lu = (const T*)b.lu;
+    const int k = g.levelNodes[q];
+    const int64_t base = g.luBase[k];
+    const int c = g.luCnt[k];
+    const int* rows = g.pRows + g.pRowPtr[k];
+    T acc = T(0);
+    if (wide) {
+        const int lane = threadIdx.x & 31;
+        const int pl = lane / S;
+        for (int t0 = 0; t0 < c; t0 += 32) {
+            const int cnt = min(32, c - t0);
+            const int mine = lane < cnt ? __ldg(rows + t0 + lane) : 0;
+            const int uMax = (cnt + P - 1) / P;
+            for (int v = 0; v < uMax; v++) {
+                const int src = pl + P * v;
+                const int r = __shfl_sync(0xffffffffu, mine, src);
+                if (src < cnt) acc += lu[(base + 1 + t0 + src) * B + s] * y[r * B + s];
+            }
+        }
+#pragma unroll
+        for (int off = S; off < 32; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    } else {
+        int t = 0;
+        for (; t + 4 <= c; t += 4) {
+            const int r0 = __ldg(rows + t), r1 = __ldg(rows + t + 1), r2 = __ldg(rows + t + 2), r3 = __ldg(rows + t + 3);
+            const T u0 = lu[(base + 1 + t) * B + s], x0 = y[r0 * B + s];
+            const T u1 = lu[(base + 2 + t) * B + s], x1 = y[r1 * B + s];
+            const T u2 = lu[(base + 3 + t) * B + s], x2 = y[r2 * B + s];
+            const T u3 = lu[(base + 4 + t) * B + s], x3 = y[r3 * B + s];
+            acc += u0 * x0;
+            acc += u1 * x1;
+            acc += u2 * x2;
+            acc += u3 * x3;
+        }
+        for (; t < c; t++) acc += lu[(base + 1 + t) * B + s] * y[__ldg(rows + t) * B + s];
+    }
+    const T xk = (y[k * B + s] - acc) / ((const T*)b.piv)[k * B + s];
+    if (!wide || (threadIdx.x & 31) < S) y[k * B + s] = xk;
+}
+
+// forward substitution of a second right-hand side v: v(k) -= sum L(k, j) v(j), with node k's forward entry
+template <typename T>
+__device__ __forceinline__ void forwardEntry(const DevGrid& g, const DevBatch& b, T* v, int e, int s, bool wide) {
+    const size_t B = (size_t)b.B;
+    const int k = g.entNode[e];
+    const int64_t q0 = g.entPairPtr[e], q1 = g.entPairPtr[e + 1];
+    const T* lu = (const T*)b.lu;
+    const T dot = wide ? dotSP<T>(lu, v, g.pairs, q0, q1, B, s) : dotSerial<T>(lu, v, g.pairs, q0, q1, B, s);
+    const T r = v[k * B + s] - dot;
+    if (!wide || (threadIdx.x & 31) < Lay<T>::S) v[k * B + s] = r;
+}
+
+// the system of this lane in a warp of group `grp`
+template <typename T>
+__device__ __forceinline__ int laneSystem(int grp) { return grp * Lay<T>::S + ((threadIdx.x & 31) % Lay<T>::S); }
+
+// Run one work item: a wide piece by the whole warp, or up to `count` short pieces over the lane groups.
+template <typename T, typename F>
+__device__ __forceinline__ void runItem(const int* __restrict__ work, const int* __restrict__ items, int it, F&& f) {
+    const int start = __ldg(items + 2 * it), count = __ldg(items + 2 * it + 1);
+    if (count < 0) {
+        f(__ldg(work + start), true);
+    } else {
+        for (int p = (threadIdx.x & 31) / Lay<T>::S; p < count; p += Lay<T>::P) f(__ldg(work + start + p), false);
+    }
+}
+
+enum WhichWork { kWorkFactor = 0, kWorkBackward = 1, kWorkForward = 2 };
+
+template <typename T, int W>
+__device__ __forceinline__ void doItem(const DevGrid& g, const DevBatch& b, T* vec, int it, int s, bool act) {
+    if (W == kWorkFactor)
+        runItem<T>(g.fWork, g.fItems, it, [&](int e, bool wide) { factorEntry<T>(g, b, e, s, act, wide); });
+    else if (W == kWorkBackward)
+        runItem<T>(g.bWork, g.bItems, it, [&](int q, bool wide) { backwardNode<T>(g, b, vec, q, s, wide); });
+    else
+        runItem<T>(g.vWork, g.vItems, it, [&](int e, bool wide) { forwardEntry<T>(g, b, vec, e, s, wide); });
+}
+
+// One level (or phase) of a schedule, items [i0, i1): block (32, 4), a warp per item, S systems per warp.
+template <typename T, int W>
+__global__ void __launch_bounds__(128) k_level(DevGrid g, DevBatch b, T* vec, int i0, int i1) {
+    const int it = i0 + blockIdx.x * 4 + threadIdx.y;
+    const int s = laneSystem<T>(blockIdx.y);
+    if (it >= i1) return;
+    bool act = s < b.count && b.active[s];
+    if (W != kWorkFactor && vec != (T*)b.y) act = act && b.refine[s];
+    if (!__any_sync(0xffffffffu, act)) return;
+    doItem<T, W>(g, b, vec, it, s, act);
+}
+
+// The narrow top of the elimination tree: one CTA per system group walks its levels itself, its warps
+// sharing each level's items, with a block barrier between levels and phases (a CTA's systems are read and
+// written by that CTA only, so no grid-wide synchronisation is needed; CTAs beyond one wave run later).
+// `ptr` is the schedule's item pointer per level (per phase for the factorisation); `up` walks levels upward.
+constexpr int kPersistWarps = 16;
+
+template <typename T, int W>
+__global__ void __launch_bounds__(32 * kPersistWarps) k_persistent(DevGrid g, DevBatch b, T* vec, int l0, int l1) {
+    const int s = laneSystem<T>(blockIdx.x);
+    bool act = s < b.count && b.active[s];
+    if (W != kWorkFactor && vec != (T*)b.y) act = act && b.refine[s];
+    if (!__syncthreads_or(act)) return;
+    const int* ptr = W == kWorkFactor ? g.fLevelPtr : (W == kWorkBackward ? g.bLevelPtr : g.vLevelPtr);
+    const int phases = W == kWorkFactor ? 2 : 1;
+    for (int step = 0; step < l1 - l0; step++) {
+        const int l = W == kWorkBackward ? l1 - 1 - step : l0 + step;
+        for (int ph = 0; ph < phases; ph++) {
+            const int i0 = ptr[phases * l + ph], i1 = ptr[phases * l + ph + 1];
+            for (int it = i0 + threadIdx.y; it < i1; it += kPersistWarps) doItem<T, W>(g, b, vec, it, s, act);
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Mixed precision: FP64 residual of the FP32 step, r = f - J dx, with J applied matrix-free from Y in FP64
+// (the same H/N/M/L expressions as the fill). The correction solve of r with the same FP32 factors makes the
+// step accurate to ~(kappa * 2^-24)^2, so the Newton path follows the FP64 path and stops where it stops.
+template <typename T>
+__global__ void __launch_bounds__(256) k_residual(DevGrid g, DevBatch b) {
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int s = blockIdx.y * 32 + lane;
+    const int i = blockIdx.x * 8 + w;
+    if (i >= g.n || s >= b.count || !b.active[s]) return;
+    const size_t B = (size_t)b.B;
+    const int kp = g.busP[i], kq = g.busQ[i];
+    if (kp < 0 && kq < 0) return;
+    const T* dx = (const T*)b.y;
+    T* z = (T*)b.z;
+    if (!b.refine[s]) {
+        if (kp >= 0) z[kp * B + s] = T(0);
+        if (kq >= 0) z[kq * B + s] = T(0);
+        return;
+    }
+    const int o = b.outage[s];
+    int c0 = -1, c1 = -1, c2 = -1, c3 = -1;
+    if (o >= 0) { c0 = g.brCell[4 * o]; c1 = g.brCell[4 * o + 1]; c2 = g.brCell[4 * o + 2]; c3 = g.brCell[4 * o + 3]; }
+    const double vmi = b.vm[i * B + s], vai = b.va[i * B + s];
+    const int p0 = g.yRowPtr[i], p1 = g.yRowPtr[i + 1];
+    double pi = 0.0, qi = 0.0;
+    for (int p = p0; p < p1; p++) {
+        const int j = g.yCol[p];
+        double G = g.yG[p], Bv = g.yB[p];
+        if (p == c0) { G = g.brRed[8 * o + 0]; Bv = g.brRed[8 * o + 1]; }
+        else if (p == c1) { G = g.brRed[8 * o + 2]; Bv = g.brRed[8 * o + 3]; }
+        else if (p == c2) { G = g.brRed[8 * o + 4]; Bv = g.brRed[8 * o + 5]; }
+        else if (p == c3) { G = g.brRed[8 * o + 6]; Bv = g.brRed[8 * o + 7]; }
+        double sn, cs;
+        sincos(vai - b.va[j * B + s], &sn, &cs);
+        const double vmj = b.vm[j * B + s];
+        pi += vmj * (G * cs + Bv * sn);
+        qi += vmj * (G * sn - Bv * cs);
+    }
+    const double P = vmi * pi, Q = vmi * qi;
+    double jp = 0.0, jq = 0.0;
+    for (int p = p0; p < p1; p++) {
+        const int j = g.yCol[p];
+        double G = g.yG[p], Bv = g.yB[p];
+        if (p == c0) { G = g.brRed[8 * o + 0]; Bv = g.brRed[8 * o + 1]; }
+        else if (p == c1) { G = g.brRed[8 * o + 2]; Bv = g.brRed[8 * o + 3]; }
+        else if (p == c2) { G = g.brRed[8 * o + 4]; Bv = g.brRed[8 * o + 5]; }
+        else if (p == c3) { G = g.brRed[8 * o + 6]; Bv = g.brRed[8 * o + 7]; }
+        double H, N, M, L;
+        if (i == j) {
+            H = -Q - Bv * vmi * vmi;
+            N = P / vmi + G * vmi;
+            M = P - G * vmi * vmi;
+            L = Q / vmi - Bv * vmi;
+        } else {
+            double sn, cs;
+            sincos(vai - b.va[j * B + s], &sn, &cs);
+            const double vmj = b.vm[j * B + s];
+            H = vmi * vmj * (G * sn - Bv * cs);
+            N = vmi * (G * cs + Bv * sn);
+            M = -vmi * vmj * (G * cs + Bv * sn);
+            L = vmi * (G * sn - Bv * cs);
+        }
+        const int jP = g.busP[j], jQ = g.busQ[j];
+        const double dth = jP >= 0 ? (double)dx[jP * B + s] : 0.0;
+        const double dv = jQ >= 0 ? (double)dx[jQ * B + s] : 0.0;
+        jp += H * dth + N * dv;
+        jq += M * dth + L * dv;
+    }
+    if (kp >= 0) z[kp * B + s] = (T)(b.rhs64[kp * B + s] - jp);
+    if (kq >= 0) z[kq * B + s] = (T)(b.rhs64[kq * B + s] - jq);
+}
+
+// ---------------------------------------------------------------------------------------------
+// 5. max |dx| per system, then the damped update.
+template <typename T>
+__global__ void __launch_bounds__(256) k_dxmax(DevGrid g, DevBatch b, int rowsPerBlock, int refine) {
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int s = blockIdx.y * 32 + lane;
+    const size_t B = (size_t)b.B;
+    const T* y = (const T*)b.y;
+    const T* z = (const T*)b.z;
+    const int r0 = blockIdx.x * rowsPerBlock, r1 = min(g.m, r0 + rowsPerBlock);
+    double mx = 0.0;
+    bool bad = false;
+    if (s < b.count && b.active[s]) {
+        for (int k = r0 + w; k < r1; k += 8) {
+            const double v = (double)y[k * B + s] + (refine && b.refine[s] ? (double)z[k * B + s] : 0.0);
+            bad |= !isfinite(v);
+            mx = fmax(mx, fabs(v));
+        }
+    }
+    __shared__ double red[8][32];
+    __shared__ int redBad[8][32];
+    red[w][lane] = mx;
+    redBad[w][lane] = bad;
+    __syncthreads();
+    if (w == 0 && s < b.count) {
+        double m = red[0][lane];
+        int anyBad = redBad[0][lane];
+        for (int q = 1; q < 8; q++) { m = fmax(m, red[q][lane]); anyBad |= redBad[q][lane]; }
+        if (m > 0.0) atomicMaxNonNeg(&b.maxDx[s], m);
+        if (anyBad) atomicOr(&b.flags[s], kFlagStepBad);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_update(DevGrid g, DevBatch b, int refine) {
+    const int lane = threadIdx.x;
+    const int s = blockIdx.y * 32 + lane;
+    const int i = blockIdx.x * 8 + threadIdx.y;
+    if (i >= g.n || s >= b.count || !b.active[s]) return;
+    if (b.flags[s] & kFlagStepBad) return;
+    const size_t B = (size_t)b.B;
+    const T* y = (const T*)b.y;
+    const T* z = (const T*)b.z;
+    refine = refine && b.refine[s];
+    const double mx = __longlong_as_double((long long)b.maxDx[s]);
+    const double damp = mx > kMaxUndampedStep ? kMaxUndampedStep / mx : 1.0;
+    const int kp = g.busP[i], kq = g.busQ[i];
+    if (kp >= 0) b.va[i * B + s] += damp * ((double)y[kp * B + s] + (refine ? (double)z[kp * B + s] : 0.0));
+    if (kq >= 0) {
+        double v = b.vm[i * B + s] + damp * ((double)y[kq * B + s] + (refine ? (double)z[kq * B + s] : 0.0));
+        if (v < kVmFloorPu) v = kVmFloorPu;
+        b.vm[i * B + s] = v;
+    }
+    if (i == 0) b.iters[s] += 1;
+}
+
+// ---------------------------------------------------------------------------------------------
+// start state: every system from the shared start (vm0/va0) or from a base state of one system.
+__global__ void k_init(DevGrid g, DevBatch b, const double* vmStart, const double* vaStart) {
+    const int lane = threadIdx.x;
+    const int s = blockIdx.y * 32 + lane;
+    const int i = blockIdx.x * 8 + threadIdx.y;
+    if (i >= g.n || s >= b.B) return;
+    const size_t B = (size_t)b.B;
+    double vm = vmStart ? vmStart[i] : g.vm0[i];
+    double va = vaStart ? vaStart[i] : g.va0[i];
+    // PV and slack magnitudes are set points whatever the start (NewtonShell.BuildBusSpec :467-469)
+    if (g.busType[i] != 1) vm = g.vm0[i];
+    if (g.busType[i] == 3) va = g.va0[i];
+    b.vm[i * B + s] = vm;
+    b.va[i * B + s] = va;
+    if (i == 0) {
+        b.maxMis[s] = 0ull;
+        b.maxDx[s] = 0ull;
+        b.startMis[s] = 0.0;
+        b.finalMis[s] = NAN;
+        b.status[s] = s < b.count ? GS_PF_MAX_ITERATIONS : GS_PF_NOT_RUN;
+        b.iters[s] = 0;
+        b.convIters[s] = 0;
+        b.convAt[s] = -1;
+        if (b.refine) b.refine[s] = 0;
+        b.active[s] = s < b.count ? 1 : 0;
+        b.flags[s] = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Post-processing of converged systems (ContingencyAnalysis.ScreenStateCore :1150-1235): branch
+// loading (NewtonShell.ComputeLineFlows :699-734), the thermal test (> 100 %), the voltage test against
+// each bus's limits (per-bus or the 0.94 / 1.06 band, VoltageLimits.cs:28-67). Items are the branches in
+// order, then the buses in order, which is the order of ContingencyResult.Details.
+struct Classify {
+    const double* lo;  // [n] effective lower limit
+    const double* hi;
+    uint8_t* code;     // [items][B]: 0 none, 1 overload, 2 under, 3 over
+    double* value;     // [items][B]
+    unsigned long long* maxLoad;  // [B]
+    unsigned long long* minVmNeg; // [B] max of (-Vm) stored as bits of (100 - Vm) (positive)
+    unsigned long long* maxVm;    // [B]
+    int* chunkCount;   // [nChunks][B]
+    int chunk;
+};
+
+__global__ void k_classify(DevGrid g, DevBatch b, Classify c) {
+    const int lane = threadIdx.x;
+    const int s = blockIdx.y * 32 + lane;
+    const int item = blockIdx.x * 8 + threadIdx.y;
+    const int nItems = g.nbr + g.n;
+    if (item >= nItems || s >= b.count) return;
+    const size_t B = (size_t)b.B;
+    uint8_t code = 0;
+    double val = 0.0;
+    if (b.status[s] == GS_PF_CONVERGED) {
+        if (item < g.nbr) {
+            const int k = item;
+            if (g.brOn[k] && k != b.outage[s]) {
+                const int f = g.brF[k], t = g.brT[k];
+                double sf, cf, st, ct;
+                sincos(b.va[f * B + s], &sf, &cf);
+                sincos(b.va[t * B + s], &st, &ct);
+                const double vfr = b.vm[f * B + s] * cf, vfi = b.vm[f * B + s] * sf;
+                const double vtr = b.vm[t * B + s] * ct, vti = b.vm[t * B + s] * st;
+                const double* y = g.brStamp + 8 * k;
+                // iF = yff vf + yft vt ; iT = ytf vf + ytt vt
+                const double ifr = y[0] * vfr - y[1] * vfi + y[4] * vtr - y[5] * vti;
+                const double ifi = y[0] * vfi + y[1] * vfr + y[4] * vti + y[5] * vtr;
+                const double itr = y[6] * vfr - y[7] * vfi + y[2] * vtr - y[3] * vti;
+                const double iti = y[6] * vfi + y[7] * vfr + y[2] * vti + y[3] * vtr;
+                // S = V conj(I) * base
+                const double sFr = vfr * ifr + vfi * ifi, sFi = vfi * ifr - vfr * ifi;
+                const double sTr = vtr * itr + vti * iti, sTi = vti * itr - vtr * iti;
+                // base_mva folded into rateA (the host passes rateA / base)
+                const double mva = fmax(hypot(sFr, sFi), hypot(sTr, sTi));
+                const double r = g.rateA[k];
+                val = r > 0 ? mva / r * 100.0 : 0.0;
+                if (val > 0.0) atomicMaxNonNeg(&c.maxLoad[s], val);
+                if (val > 100.0) code = 1;
+            }
+        } else {
+            const int i = item - g.nbr;
+            val = b.vm[i * B + s];
+            if (val < c.lo[i]) code = 2;
+            else if (val > c.hi[i]) code = 3;
+            atomicMaxNonNeg(&c.maxVm[s], val);
+            atomicMaxNonNeg(&c.minVmNeg[s], 100.0 - val);
+        }
+    }
+    c.code[(size_t)item * B + s] = code;
+    c.value[(size_t)item * B + s] = val;
+    if (code) atomicAdd(&c.chunkCount[(size_t)(item / c.chunk) * B + s], 1);
+}
+
+// Ordered compaction: one warp per (chunk, 32 systems); each lane walks the chunk in item order.
+__global__ void k_compact(DevGrid g, DevBatch b, Classify c, const int* chunkOffset, int* outKind, int* outElem,
+                          double* outVal, const int* busId) {
+    const int lane = threadIdx.x;
+    const int s = blockIdx.y * 32 + lane;
+    const int ch = blockIdx.x * 4 + threadIdx.y;
+    const int nItems = g.nbr + g.n;
+    const int nChunks = (nItems + c.chunk - 1) / c.chunk;
+    if (ch >= nChunks || s >= b.count) return;
+    const size_t B = (size_t)b.B;
+    int w = chunkOffset[(size_t)ch * B + s];
+    const int e = min(nItems, (ch + 1) * c.chunk);
+    for (int item = ch * c.chunk; item < e; item++) {
+        const uint8_t code = c.code[(size_t)item * B + s];
+        if (!code) continue;
+        outKind[w] = code == 1 ? GS_VIOL_BRANCH_OVERLOAD : (code == 2 ? GS_VIOL_UNDERVOLTAGE : GS_VIOL_OVERVOLTAGE);
+        outElem[w] = code == 1 ? item : busId[item - g.nbr];
+        outVal[w] = c.value[(size_t)item * B + s];
+        w++;
+    }
+}
+
+// Line flows of system 0 (single solve result).
+__global__ void k_lineflows(DevGrid g, DevBatch b, double base, double* loading, double* sfo, double* sto) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= g.nbr) return;
+    const size_t B = (size_t)b.B;
+    if (!g.brOn[k]) {
+        loading[k] = 0; sfo[2 * k] = sfo[2 * k + 1] = sto[2 * k] = sto[2 * k + 1] = 0;
+        return;
+    }
+    const int f = g.brF[k], t = g.brT[k];
+    double sf, cf, st, ct;
+    sincos(b.va[f * B], &sf, &cf);
+    sincos(b.va[t * B], &st, &ct);
+    const double vfr = b.vm[f * B] * cf, vfi = b.vm[f * B] * sf;
+    const double vtr = b.vm[t * B] * ct, vti = b.vm[t * B] * st;
+    const double* y = g.brStamp + 8 * k;
+    const double ifr = y[0] * vfr - y[1] * vfi + y[4] * vtr - y[5] * vti;
+    const double ifi = y[0] * vfi + y[1] * vfr + y[4] * vti + y[5] * vtr;
+    const double itr = y[6] * vfr - y[7] * vfi + y[2] * vtr - y[3] * vti;
+    const double iti = y[6] * vfi + y[7] * vfr + y[2] * vti + y[3] * vtr;
+    const double sFr = (vfr * ifr + vfi * ifi) * base, sFi = (vfi * ifr - vfr * ifi) * base;
+    const double sTr = (vtr * itr + vti * iti) * base, sTi = (vti * itr - vtr * iti) * base;
+    sfo[2 * k] = sFr; sfo[2 * k + 1] = sFi;
+    sto[2 * k] = sTr; sto[2 * k + 1] = sTi;
+    const double mva = fmax(hypot(sFr, sFi), hypot(sTr, sTi));
+    const double r = g.rateA[k] * base;
+    loading[k] = r > 0 ? mva / r * 100.0 : 0.0;
+}
+
+// FP64 self-test (GpuContext.cs:227-254): (1 + 2^-40) - 1 must be 2^-40 exactly.
+__global__ void k_selftest(double* out) {
+    volatile double one = 1.0;
+    double e = ldexp(1.0, -40);
+    out[0] = (one + e) - one;
+}
+
+}  // namespace gs
+
+// =============================================================================================
+// Host side.
+namespace gs {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { if (p) cudaFree(p); }
+    cudaError_t alloc(size_t n) {
+        if (p && bytes >= n) return cudaSuccess;
+        if (p) { cudaFree(p); p = nullptr; bytes = 0; }
+        if (n == 0) n = 16;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e == cudaSuccess) bytes = n; else p = nullptr;
+        return e;
+    }
+    template <typename X> X* as() const { return reinterpret_cast<X*>(p); }
+};
+
+struct Workspace {
+    int B = 0;
+    int precision = -1;
+    DevBuf vm, va, lu, piv, y, z, rhs64, refine, maxMis, maxDx, startMis, finalMis, status, iters, convIters, convAt, active, flags, outage,
+        loadScale, activeCount;
+    DevBuf code, value, maxLoad, minVmNeg, maxVmB, chunkCount, chunkOffset, outKind, outElem, outVal, pq;
+    DevBuf startVm, startVa;
+};
+
+}  // namespace gs
+
+struct gs_ctx {
+    int device = 0;
+    std::string lastError;
+    std::mutex mu;
+    cudaStream_t stream = nullptr;
+    int* pinnedCount = nullptr;
+};
+
+struct gs_grid {
+    gs_ctx* ctx = nullptr;
+    gs::HostGrid host;
+    gs::Symbolic sym;
+    std::vector<std::unique_ptr<gs::DevBuf>> bufs;
+    gs::DevGrid view{};
+    std::vector<double> pgen, qgen, pload, qload;
+    gs::Workspace ws;
+    int split = 0;  // first level run by the persistent kernels
+};
+
+namespace gs {
+namespace {
+
+int SetErr(gs_ctx* c, int code, const std::string& msg) {
+    if (c) { std::lock_guard<std::mutex> l(c->mu); c->lastError = msg; }
+    return code;
+}
+
+#define GS_CUDA(call)                                                                                   \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess) {                                                                        \
+            int code_ = (e_ == cudaErrorMemoryAllocation) ? GS_ERR_OOM : GS_ERR_CUDA;                   \
+            return SetErr(ctx, code_, std::string(#call) + ": " + cudaGetErrorString(e_));              \
+        }                                                                                               \
+    } while (0)
+
+template <typename X>
+int Upload(gs_grid* G, const std::vector<X>& v, const X** out) {
+    gs_ctx* ctx = G->ctx;
+    auto buf = std::make_unique<DevBuf>();
+    GS_CUDA(buf->alloc(std::max<size_t>(sizeof(X), v.size() * sizeof(X))));
+    if (!v.empty()) GS_CUDA(cudaMemcpy(buf->p, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice));
+    *out = buf->as<X>();
+    G->bufs.push_back(std::move(buf));
+    return GS_OK;
+}
+
+int UploadGrid(gs_grid* G) {
+    const HostGrid& h = G->host;
+    const Symbolic& s = G->sym;
+    DevGrid& v = G->view;
+    v.n = s.n; v.m = s.m; v.nnzY = s.nnzY; v.nbr = s.nbr; v.nnzLU = s.nnzLU;
+    const int n = h.n;
+    G->pgen.assign(n, 0.0); G->qgen.assign(n, 0.0);
+    for (int k = 0; k < h.ngen; k++) {
+        if (!h.genOn[k]) continue;
+        G->pgen[h.genBus[k]] += h.pg[k];
+        G->qgen[h.genBus[k]] += h.qg[k];
+    }
+    G->pload.resize(n); G->qload.resize(n);
+    for (int i = 0; i < n; i++) {
+        G->pgen[i] /= h.base; G->qgen[i] /= h.base;
+        G->pload[i] = h.pd[i] / h.base; G->qload[i] = h.qd[i] / h.base;
+    }
+    std::vector<double> rate(h.nbr);
+    for (int k = 0; k < h.nbr; k++) rate[k] = h.rateA[k] / h.base;
+    std::vector<int2> pairs(s.pairs.size() / 2);
+    for (size_t q = 0; q < pairs.size(); q++) pairs[q] = make_int2(s.pairs[2 * q], s.pairs[2 * q + 1]);
+    int rc;
+#define UP(vec, field) if ((rc = Upload(G, vec, &v.field)) != GS_OK) return rc
+    UP(s.yRowPtr, yRowPtr); UP(s.yCol, yCol); UP(s.yG, yG); UP(s.yB, yB);
+    UP(s.brCell, brCell); UP(s.brRed, brRed); UP(s.brStamp, brStamp);
+    UP(h.brF, brF); UP(h.brT, brT); UP(rate, rateA); UP(h.brOn, brOn);
+    UP(G->pgen, pgen); UP(G->qgen, qgen); UP(G->pload, pload); UP(G->qload, qload);
+    UP(s.vm0, vm0); UP(s.va0, va0); UP(s.type0, busType); UP(s.busP, busP); UP(s.busQ, busQ); UP(s.ySlot, ySlot);
+    UP(s.entSlot, entSlot); UP(s.entKind, entKind); UP(s.entHasA, entHasA);
+    UP(s.entPairPtr, entPairPtr); UP(pairs, pairs); UP(s.diagPairNode, diagEnt); UP(s.levelNodes, levelNodes);
+    UP(s.luBase, luBase); UP(s.luCnt, luCnt); UP(s.pRowPtr, pRowPtr); UP(s.pRows, pRows);
+    UP(s.levelNodePtr, levelNodePtr); UP(s.entNode, entNode);
+    UP(s.factor.work, fWork); UP(s.factor.items, fItems); UP(s.factor.levelItemPtr, fLevelPtr);
+    UP(s.backward.work, bWork); UP(s.backward.items, bItems); UP(s.backward.levelItemPtr, bLevelPtr);
+    UP(s.forward.work, vWork); UP(s.forward.items, vItems); UP(s.forward.levelItemPtr, vLevelPtr);
+#undef UP
+    // the persistent kernels take every level from the first one whose items (and those of all levels above
+    // it) fit twice in a CTA's warps in each phase
+    G->split = s.nLevels;
+    for (int l = s.nLevels - 1; l >= 0; l--) {
+        const auto& fp = s.factor.levelItemPtr;
+        const int a = fp[2 * l + 1] - fp[2 * l], bb = fp[2 * l + 2] - fp[2 * l + 1];
+        const int c = s.backward.levelItemPtr[l + 1] - s.backward.levelItemPtr[l];
+        if (std::max(std::max(a, bb), c) > 2 * kPersistWarps) break;
+        G->split = l;
+    }
+    return GS_OK;
+}
+
+size_t PerSystemBytes(const Symbolic& s, int precision) {
+    size_t t = precision == GS_PREC_MIXED ? 4 : 8;
+    size_t refine = precision == GS_PREC_MIXED ? (size_t)s.m * (t + 8) : 0;
+    return (size_t)s.nnzLU * t + 2 * (size_t)s.m * t + refine + (size_t)s.n * 16 + (size_t)(s.nbr + s.n) * 9 + 256;
+}
+
+int EnsureWorkspace(gs_grid* G, int B, int precision, bool classify, bool loadScale) {
+    gs_ctx* ctx = G->ctx;
+    Workspace& w = G->ws;
+    const Symbolic& s = G->sym;
+    size_t t = precision == GS_PREC_MIXED ? 4 : 8;
+    size_t Bz = (size_t)B;
+    GS_CUDA(w.vm.alloc(s.n * Bz * 8));
+    GS_CUDA(w.va.alloc(s.n * Bz * 8));
+    GS_CUDA(w.lu.alloc((size_t)s.nnzLU * Bz * t));
+    GS_CUDA(w.y.alloc((size_t)s.m * Bz * t));
+    GS_CUDA(w.piv.alloc((size_t)s.m * Bz * t));
+    if (precision == GS_PREC_MIXED) {
+        GS_CUDA(w.z.alloc((size_t)s.m * Bz * t));
+        GS_CUDA(w.rhs64.alloc((size_t)s.m * Bz * 8));
+        GS_CUDA(w.refine.alloc(Bz * 4));
+    }
+    GS_CUDA(w.maxMis.alloc(Bz * 8)); GS_CUDA(w.maxDx.alloc(Bz * 8));
+    GS_CUDA(w.startMis.alloc(Bz * 8)); GS_CUDA(w.finalMis.alloc(Bz * 8));
+    GS_CUDA(w.status.alloc(Bz * 4)); GS_CUDA(w.iters.alloc(Bz * 4)); GS_CUDA(w.active.alloc(Bz * 4));
+    GS_CUDA(w.convIters.alloc(Bz * 4)); GS_CUDA(w.convAt.alloc(Bz * 4));
+    GS_CUDA(w.flags.alloc(Bz * 4)); GS_CUDA(w.outage.alloc(Bz * 4)); GS_CUDA(w.activeCount.alloc(16));
+    GS_CUDA(w.startVm.alloc(s.n * 8)); GS_CUDA(w.startVa.alloc(s.n * 8));
+    if (loadScale) GS_CUDA(w.loadScale.alloc(s.n * Bz * 8));
+    if (classify) {
+        const int nItems = s.nbr + s.n;
+        GS_CUDA(w.code.alloc((size_t)nItems * Bz));
+        GS_CUDA(w.value.alloc((size_t)nItems * Bz * 8));
+        GS_CUDA(w.maxLoad.alloc(Bz * 8)); GS_CUDA(w.minVmNeg.alloc(Bz * 8)); GS_CUDA(w.maxVmB.alloc(Bz * 8));
+    }
+    w.B = B;
+    w.precision = precision;
+    return GS_OK;
+}
+
+DevBatch MakeBatch(gs_grid* G, int count, bool useScale) {
+    Workspace& w = G->ws;
+    DevBatch b{};
+    b.B = w.B; b.count = count;
+    b.vm = w.vm.as<double>(); b.va = w.va.as<double>(); b.lu = w.lu.p; b.y = w.y.p; b.piv = w.piv.p;
+    const bool mixed = w.precision == GS_PREC_MIXED;
+    b.z = mixed ? w.z.p : nullptr;
+    b.rhs64 = mixed ? w.rhs64.as<double>() : nullptr;
+    b.refine = mixed ? w.refine.as<int>() : nullptr;
+    b.maxMis = w.maxMis.as<unsigned long long>(); b.maxDx = w.maxDx.as<unsigned long long>();
+    b.startMis = w.startMis.as<double>(); b.finalMis = w.finalMis.as<double>();
+    b.status = w.status.as<int>(); b.iters = w.iters.as<int>(); b.active = w.active.as<int>();
+    b.convIters = w.convIters.as<int>(); b.convAt = w.convAt.as<int>();
+    b.flags = w.flags.as<int>(); b.outage = w.outage.as<int>();
+    b.loadScale = useScale ? w.loadScale.as<double>() : nullptr;
+    b.activeCount = w.activeCount.as<int>();
+    return b;
+}
+
+// Run the Newton iteration of `count` systems already placed in the workspace (outage, loadScale).
+// `startFromWs`: start every system from ws.startVm / startVa (a solved base), else from the grid start.
+struct NewtonStats {
+    int64_t launches = 0;
+    int iterations = 0;
+    double factorMs = 0, solveMs = 0, mismatchMs = 0, otherMs = 0;
+    double factorBytes = 0;
+};
+
+template <typename T>
+int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_opts& o, float* ms,
+           NewtonStats* stats = nullptr) {
+    gs_ctx* ctx = G->ctx;
+    const Symbolic& s = G->sym;
+    Workspace& w = G->ws;
+    cudaStream_t st = ctx->stream;
+    DevBatch b = MakeBatch(G, count, useScale);
+    const DevGrid& g = G->view;
+    const int groups = w.B / 32;
+    cudaEvent_t e0, e1;
+    GS_CUDA(cudaEventCreate(&e0));
+    GS_CUDA(cudaEventCreate(&e1));
+    GS_CUDA(cudaEventRecord(e0, st));
+    dim3 blk8(32, 8), blk4(32, 4);
+    k_init<<<dim3((s.n + 7) / 8, groups), blk8, 0, st>>>(g, b, startFromWs ? w.startVm.as<double>() : nullptr,
+                                                          startFromWs ? w.startVa.as<double>() : nullptr);
+    GS_CUDA(cudaGetLastError());
+    // the step (factor levels, backward levels, refinement, max |dx|, update) as one graph
+    const int refine = sizeof(T) < sizeof(double) ? 1 : 0;
+    const bool timed = o.phase_timing != 0;
+    cudaEvent_t ev[5];
+    if (timed) for (auto& e : ev) GS_CUDA(cudaEventCreate(&e));
+    int64_t stepLaunches = 0;
+    // levels [0, split) run one launch per level (wide: thousands of tasks); levels [split, nLevels) run in
+    // one persistent launch per phase (narrow: a few tasks per level, latency-bound)
+    const int split = G->split;
+    const int persistThreads = 32;
+    const int luGroups = w.B / Lay<T>::S;  // warps of the LU kernels cover S systems each
+    auto launchLevel = [&](auto kernel, T* vec, int i0, int i1) {
+        if (i1 > i0) { kernel<<<dim3((i1 - i0 + 3) / 4, luGroups), blk4, 0, st>>>(g, b, vec, i0, i1); stepLaunches++; }
+    };
+    const auto& fp = s.factor.levelItemPtr;
+    const auto& bp = s.backward.levelItemPtr;
+    const auto& vp = s.forward.levelItemPtr;
+    auto factorPhase = [&]() {
+        for (int l = 0; l < split; l++) {
+            launchLevel(k_level<T, kWorkFactor>, (T*)b.y, fp[2 * l], fp[2 * l + 1]);
+            launchLevel(k_level<T, kWorkFactor>, (T*)b.y, fp[2 * l + 1], fp[2 * l + 2]);
+        }
+        if (split < s.nLevels) {
+            k_persistent<T, kWorkFactor><<<luGroups, dim3(persistThreads, kPersistWarps), 0, st>>>(g, b, (T*)b.y, split, s.nLevels);
+            stepLaunches++;
+        }
+    };
+    auto backward = [&](T* vec) {
+        if (split < s.nLevels) {
+            k_persistent<T, kWorkBackward><<<luGroups, dim3(persistThreads, kPersistWarps), 0, st>>>(g, b, vec, split, s.nLevels);
+            stepLaunches++;
+        }
+        for (int l = split - 1; l >= 0; l--) launchLevel(k_level<T, kWorkBackward>, vec, bp[l], bp[l + 1]);
+    };
+    auto solvePhase = [&]() {
+        backward((T*)b.y);
+        if (refine) {
+            k_residual<T><<<dim3((s.n + 7) / 8, groups), blk8, 0, st>>>(g, b);
+            stepLaunches++;
+            for (int l = 0; l < split; l++) launchLevel(k_level<T, kWorkForward>, (T*)b.z, vp[l], vp[l + 1]);
+            if (split < s.nLevels) {
+                k_persistent<T, kWorkForward><<<luGroups, dim3(persistThreads, kPersistWarps), 0, st>>>(g, b, (T*)b.z, split, s.nLevels);
+                stepLaunches++;
+            }
+            backward((T*)b.z);
+        }
+    };
+    const int rowsPerBlock = 512;
+    auto updatePhase = [&]() {
+        k_dxmax<T><<<dim3((s.m + rowsPerBlock - 1) / rowsPerBlock, groups), blk8, 0, st>>>(g, b, rowsPerBlock, refine);
+        k_update<T><<<dim3((s.n + 7) / 8, groups), blk8, 0, st>>>(g, b, refine);
+        stepLaunches += 2;
+    };
+    cudaGraph_t graph;
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t ce;
+    if (!timed) {
+        GS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        factorPhase();
+        solvePhase();
+        updatePhase();
+        ce = cudaStreamEndCapture(st, &graph);
+        if (ce != cudaSuccess) return SetErr(ctx, GS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) return SetErr(ctx, GS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+    } else {
+        stepLaunches = 0;
+    }
+    const int64_t launchesPerStep = stepLaunches;
+    const char* traceEnv = std::getenv("GS_TRACE_ITERATIONS");  // per-iteration phase times (with phase_timing)
+    const bool traceIters = traceEnv && traceEnv[0] == '1';
+    int64_t launches = 1;
+    int iterations = 0;
+    double fMs = 0, sMs = 0, mMs = 0, oMs = 0;
+    int rc = GS_OK;
+    for (int iter = 0; iter <= o.max_iterations + 4; iter++) {
+        if (timed) cudaEventRecord(ev[0], st);
+        k_mismatch_jac<T><<<dim3((s.n + 7) / 8, groups), blk8, 0, st>>>(g, b, 1, nullptr, nullptr);
+        if (timed) cudaEventRecord(ev[1], st);
+        cudaMemsetAsync(b.activeCount, 0, sizeof(int), st);
+        k_status<<<(count + 255) / 256, 256, 0, st>>>(b, iter, o.tolerance, o.diverge_limit_pu, o.max_iterations, 0);
+        launches += 2;
+        cudaMemcpyAsync(ctx->pinnedCount, b.activeCount, sizeof(int), cudaMemcpyDeviceToHost, st);
+        ce = cudaStreamSynchronize(st);
+        if (ce != cudaSuccess) { rc = SetErr(ctx, GS_ERR_CUDA, std::string("newton: ") + cudaGetErrorString(ce)); break; }
+        if (timed) { float t; cudaEventElapsedTime(&t, ev[0], ev[1]); mMs += t; }
+        if (*ctx->pinnedCount == 0) break;
+        iterations++;
+        if (!timed) {
+            ce = cudaGraphLaunch(exec, st);
+            launches += launchesPerStep;
+            if (ce != cudaSuccess) { rc = SetErr(ctx, GS_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(ce)); break; }
+        } else {
+            stepLaunches = 0;
+            cudaEventRecord(ev[1], st);
+            factorPhase();
+            cudaEventRecord(ev[2], st);
+            solvePhase();
+            cudaEventRecord(ev[3], st);
+            updatePhase();
+            cudaEventRecord(ev[4], st);
+            launches += stepLaunches;
+            ce = cudaEventSynchronize(ev[4]);
+            if (ce != cudaSuccess) { rc = SetErr(ctx, GS_ERR_CUDA, std::string("newton: ") + cudaGetErrorString(ce)); break; }
+            float t1, t2, t3;
+            cudaEventElapsedTime(&t1, ev[1], ev[2]);
+            cudaEventElapsedTime(&t2, ev[2], ev[3]);
+            cudaEventElapsedTime(&t3, ev[3], ev[4]);
+            fMs += t1; sMs += t2; oMs += t3;
+            if (traceIters)
+                std::fprintf(stderr, "gs: iteration %d active %d factor %.3f ms solve %.3f ms update %.3f ms\n", iter,
+                             *ctx->pinnedCount, t1, t2, t3);
+        }
+    }
+    if (timed) for (auto& e : ev) cudaEventDestroy(e);
+    if (stats) {
+        stats->launches += launches;
+        stats->iterations = std::max(stats->iterations, iterations);
+        stats->factorMs += fMs; stats->solveMs += sMs; stats->mismatchMs += mMs; stats->otherMs += oMs;
+        // algorithmic bytes of one factorisation per system: read J (nnzJ) + write L and U (nnzLU)
+        stats->factorBytes += (double)iterations * (double)count * (double)sizeof(T) * ((double)s.nnzJ + (double)s.nnzLU);
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    if (ms) cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+
+int NewtonDispatch(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_opts& o, float* ms,
+                   NewtonStats* stats = nullptr) {
+    if (o.precision == GS_PREC_MIXED) return Newton<float>(G, count, useScale, startFromWs, o, ms, stats);
+    return Newton<double>(G, count, useScale, startFromWs, o, ms, stats);
+}
+
+int CheckOpts(gs_ctx* ctx, const gs_pf_opts* o) {
+    if (!o) return SetErr(ctx, GS_ERR_INVALID_ARG, "null options");
+    if (o->enforce_q_limits)
+        return SetErr(ctx, GS_ERR_UNSUPPORTED, "enforce_q_limits: the PV->PQ switching loop is not built yet");
+    if (o->retry_from_dc_start)
+        return SetErr(ctx, GS_ERR_UNSUPPORTED, "retry_from_dc_start: the DC-angle retry is not built yet");
+    if (!(o->tolerance > 0) || o->tolerance > 1e-2) return SetErr(ctx, GS_ERR_INVALID_ARG, "tolerance must be in (0, 1e-2]");
+    if (o->max_iterations < 0) return SetErr(ctx, GS_ERR_INVALID_ARG, "max_iterations must be 0 or more");
+    if (!(o->diverge_limit_pu > 0)) return SetErr(ctx, GS_ERR_INVALID_ARG, "diverge_limit_pu must be above 0");
+    if (o->precision != GS_PREC_FP64 && o->precision != GS_PREC_MIXED)
+        return SetErr(ctx, GS_ERR_INVALID_ARG, "unknown precision");
+    return GS_OK;
+}
+
+int ChooseB(gs_grid* G, int want, const gs_pf_opts& o) {
+    size_t freeB = 0, total = 0;
+    cudaMemGetInfo(&freeB, &total);
+    size_t per = PerSystemBytes(G->sym, o.precision);
+    size_t cap = (size_t)(0.6 * (double)(freeB + (G->ws.lu.bytes + G->ws.vm.bytes + G->ws.va.bytes + G->ws.code.bytes +
+                                                 G->ws.value.bytes + G->ws.y.bytes))) / per;
+    int B = (int)std::min<size_t>(cap, (size_t)1 << 20);
+    if (o.batch_width > 0) B = std::min(B, o.batch_width);
+    B = std::min(B, ((want + 31) / 32) * 32);
+    B = (B / 32) * 32;
+    return std::max(B, 32);
+}
+
+// Solve the intact grid once in system 0 of the workspace (B = 32) and keep its state in startVm/Va.
+int SolveBase(gs_grid* G, const gs_pf_opts& o, int* status, int* iters, double* mis, float* ms) {
+    gs_ctx* ctx = G->ctx;
+    int rc = EnsureWorkspace(G, 32, o.precision, false, false);
+    if (rc) return rc;
+    std::vector<int> outage(G->ws.B, -1);
+    GS_CUDA(cudaMemcpy(G->ws.outage.p, outage.data(), outage.size() * 4, cudaMemcpyHostToDevice));
+    rc = NewtonDispatch(G, 1, false, false, o, ms);
+    if (rc) return rc;
+    const size_t B = G->ws.B;
+    const int n = G->sym.n;
+    // gather system 0 (strided) into the start arrays
+    GS_CUDA(cudaMemcpy2D(G->ws.startVm.p, 8, G->ws.vm.p, B * 8, 8, n, cudaMemcpyDeviceToDevice));
+    GS_CUDA(cudaMemcpy2D(G->ws.startVa.p, 8, G->ws.va.p, B * 8, 8, n, cudaMemcpyDeviceToDevice));
+    GS_CUDA(cudaMemcpy(status, G->ws.status.p, 4, cudaMemcpyDeviceToHost));
+    GS_CUDA(cudaMemcpy(iters, *status == GS_PF_CONVERGED ? G->ws.convIters.p : G->ws.iters.p, 4, cudaMemcpyDeviceToHost));
+    GS_CUDA(cudaMemcpy(mis, G->ws.finalMis.p, 8, cudaMemcpyDeviceToHost));
+    return GS_OK;
+}
+
+}  // namespace
+}  // namespace gs
+
+using namespace gs;
+
+extern "C" {
+
+int gs_ctx_create(int device, const gs_ctx_opts* opts, gs_ctx** out) {
+    if (!out) return GS_ERR_INVALID_ARG;
+    *out = nullptr;
+    int timeoutMs = (opts && opts->probe_timeout_ms > 0) ? opts->probe_timeout_ms : 10000;
+    // The probe runs on a worker thread and is bounded (GpuContext.ProbeWithTimeout, GpuContext.cs:325-345).
+    struct Probe { int rc = GS_ERR_TIMEOUT; std::string msg = "device probe timed out"; cudaStream_t stream = nullptr; };
+    auto probe = std::make_shared<Probe>();
+    auto done = std::make_shared<std::atomic<bool>>(false);
+    std::thread th([probe, done, device]() {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+            probe->rc = GS_ERR_NO_DEVICE; probe->msg = "no CUDA device " + std::to_string(device);
+        } else if (cudaSetDevice(device) != cudaSuccess) {
+            probe->rc = GS_ERR_NO_DEVICE; probe->msg = "cudaSetDevice failed";
+        } else {
+            double* d = nullptr;
+            double h = 0;
+            cudaStream_t s = nullptr;
+            if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess && cudaMalloc(&d, 8) == cudaSuccess) {
+                gs::k_selftest<<<1, 1, 0, s>>>(d);
+                if (cudaMemcpyAsync(&h, d, 8, cudaMemcpyDeviceToHost, s) == cudaSuccess && cudaStreamSynchronize(s) == cudaSuccess &&
+                    h == std::ldexp(1.0, -40)) {
+                    probe->rc = GS_OK; probe->msg = ""; probe->stream = s;
+                } else {
+                    probe->rc = GS_ERR_NO_DEVICE; probe->msg = "FP64 self-test failed";
+                }
+                cudaFree(d);
+            } else {
+                probe->rc = GS_ERR_NO_DEVICE; probe->msg = "device allocation failed in the probe";
+            }
+        }
+        done->store(true);
+    });
+    auto t0 = std::chrono::steady_clock::now();
+    while (!done->load() && std::chrono::steady_clock::now() - t0 < std::chrono::milliseconds(timeoutMs))
+        std::this_thread::sleep_for(std::chrono::milliseconds(2));
+    if (!done->load()) { th.detach(); return GS_ERR_TIMEOUT; }
+    th.join();
+    if (probe->rc != GS_OK) return probe->rc;
+    gs_ctx* c = new gs_ctx();
+    c->device = device;
+    c->stream = probe->stream;
+    if (cudaMallocHost(&c->pinnedCount, sizeof(int)) != cudaSuccess) { delete c; return GS_ERR_CUDA; }
+    *out = c;
+    return GS_OK;
+}
+
+int gs_ctx_destroy(gs_ctx* c) {
+    if (!c) return GS_ERR_INVALID_ARG;
+    cudaSetDevice(c->device);
+    if (c->pinnedCount) cudaFreeHost(c->pinnedCount);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return GS_OK;
+}
+
+int gs_last_error(gs_ctx* c, char* buf, size_t len) {
+    if (!c || !buf || len == 0) return GS_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> l(c->mu);
+    size_t k = std::min(len - 1, c->lastError.size());
+    std::memcpy(buf, c->lastError.data(), k);
+    buf[k] = 0;
+    return GS_OK;
+}
+
+int gs_grid_create(gs_ctx* ctx, const gs_grid_desc* desc, gs_grid** out) {
+    if (!ctx || !desc || !out) return GS_ERR_INVALID_ARG;
+    *out = nullptr;
+    auto G = std::make_unique<gs_grid>();
+    G->ctx = ctx;
+    std::string err = CopyGrid(desc, G->host);
+    if (!err.empty()) return SetErr(ctx, GS_ERR_INVALID_ARG, err);
+    err = Analyze(G->host, G->sym);
+    if (!err.empty()) return SetErr(ctx, GS_ERR_INVALID_ARG, err);
+    GS_CUDA(cudaSetDevice(ctx->device));
+    int rc = UploadGrid(G.get());
+    if (rc) return rc;
+    *out = G.release();
+    return GS_OK;
+}
+
+int gs_grid_destroy(gs_grid* g) {
+    if (!g) return GS_ERR_INVALID_ARG;
+    cudaSetDevice(g->ctx->device);
+    delete g;
+    return GS_OK;
+}
+
+int gs_grid_info_get(gs_grid* g, gs_grid_info* info) {
+    if (!g || !info) return GS_ERR_INVALID_ARG;
+    FillInfo(g->host, g->sym, info);
+    return GS_OK;
+}
+
+int gs_pf_solve(gs_grid* G, const gs_pf_opts* opts, gs_pf_result* res) {
+    if (!G || !res) return GS_ERR_INVALID_ARG;
+    gs_ctx* ctx = G->ctx;
+    int rc = CheckOpts(ctx, opts);
+    if (rc) return rc;
+    gs_pf_opts o = *opts;
+    if (o.flat_start) return SetErr(ctx, GS_ERR_UNSUPPORTED, "flat_start: pass a flat start in the descriptor");
+    GS_CUDA(cudaSetDevice(ctx->device));
+    int st = 0, it = 0;
+    double mis = 0;
+    float ms = 0;
+    rc = SolveBase(G, o, &st, &it, &mis, &ms);
+    if (rc) return rc;
+    res->status = st;
+    res->iterations = it;
+    res->max_mismatch = mis;
+    const int n = G->sym.n, nb = G->sym.nbr;
+    const size_t B = G->ws.B;
+    std::vector<double> vm(n), va(n);
+    GS_CUDA(cudaMemcpy(vm.data(), G->ws.startVm.p, n * 8, cudaMemcpyDeviceToHost));
+    GS_CUDA(cudaMemcpy(va.data(), G->ws.startVa.p, n * 8, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; i++) {
+        if (res->vm) res->vm[i] = vm[i];
+        if (res->va_deg) res->va_deg[i] = va[i] * 180.0 / 3.14159265358979323846;
+    }
+    if (res->p_inj_mw || res->q_inj_mvar) {
+        GS_CUDA(G->ws.pq.alloc(2 * (size_t)n * B * 8));
+        DevBatch b = MakeBatch(G, 1, false);
+        GS_CUDA(cudaMemset(b.active, 0, B * 4));
+        int one = 1;
+        GS_CUDA(cudaMemcpy(b.active, &one, 4, cudaMemcpyHostToDevice));
+        double* P = G->ws.pq.as<double>();
+        double* Q = P + (size_t)n * B;
+        if (o.precision == GS_PREC_MIXED)
+            k_mismatch_jac<float><<<dim3((n + 7) / 8, B / 32), dim3(32, 8), 0, ctx->stream>>>(G->view, b, 0, P, Q);
+        else
+            k_mismatch_jac<double><<<dim3((n + 7) / 8, B / 32), dim3(32, 8), 0, ctx->stream>>>(G->view, b, 0, P, Q);
+        GS_CUDA(cudaStreamSynchronize(ctx->stream));
+        std::vector<double> p(n), q(n);
+        GS_CUDA(cudaMemcpy2D(p.data(), 8, P, B * 8, 8, n, cudaMemcpyDeviceToHost));
+        GS_CUDA(cudaMemcpy2D(q.data(), 8, Q, B * 8, 8, n, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < n; i++) {
+            if (res->p_inj_mw) res->p_inj_mw[i] = p[i] * G->host.base;
+            if (res->q_inj_mvar) res->q_inj_mvar[i] = q[i] * G->host.base;
+        }
+    }
+    if (nb > 0 && (res->loading_pct || res->sf_mva || res->st_mva)) {
+        DevBuf tmp;
+        GS_CUDA(tmp.alloc((size_t)nb * 5 * 8));
+        double* ld = tmp.as<double>();
+        double* sf = ld + nb;
+        double* sto = sf + 2 * (size_t)nb;
+        DevBatch b = MakeBatch(G, 1, false);
+        k_lineflows<<<(nb + 127) / 128, 128, 0, ctx->stream>>>(G->view, b, G->host.base, ld, sf, sto);
+        GS_CUDA(cudaStreamSynchronize(ctx->stream));
+        std::vector<double> h((size_t)nb * 5);
+        GS_CUDA(cudaMemcpy(h.data(), ld, h.size() * 8, cudaMemcpyDeviceToHost));
+        for (int k = 0; k < nb; k++) {
+            if (res->loading_pct) res->loading_pct[k] = h[k];
+            if (res->sf_mva) { res->sf_mva[2 * k] = h[nb + 2 * k]; res->sf_mva[2 * k + 1] = h[nb + 2 * k + 1]; }
+            if (res->st_mva) { res->st_mva[2 * k] = h[3 * nb + 2 * k]; res->st_mva[2 * k + 1] = h[3 * nb + 2 * k + 1]; }
+        }
+    }
+    return GS_OK;
+}
+
+int gs_pf_solve_batch(gs_grid* G, int32_t count, const double* loadScale, const int32_t* outage, const gs_pf_opts* opts,
+                      int32_t* status, int32_t* iterations, double* maxMismatch, double* vmOut, double* vaOut) {
+    if (!G || count < 0) return GS_ERR_INVALID_ARG;
+    gs_ctx* ctx = G->ctx;
+    int rc = CheckOpts(ctx, opts);
+    if (rc) return rc;
+    gs_pf_opts o = *opts;
+    if (o.flat_start) return SetErr(ctx, GS_ERR_UNSUPPORTED, "flat_start: pass a flat start in the descriptor");
+    const Symbolic& s = G->sym;
+    if (outage)
+        for (int k = 0; k < count; k++)
+            if (outage[k] >= s.nbr || (outage[k] >= 0 && !G->host.brOn[outage[k]]))
+                return SetErr(ctx, GS_ERR_INVALID_ARG, "outage index out of range or out of service");
+    GS_CUDA(cudaSetDevice(ctx->device));
+    const int n = s.n;
+    int done = 0;
+    while (done < count) {
+        int B = ChooseB(G, count - done, o);
+        rc = EnsureWorkspace(G, B, o.precision, false, loadScale != nullptr);
+        if (rc) return rc;
+        int cnt = std::min(B, count - done);
+        std::vector<int> out(B, -1);
+        for (int k = 0; k < cnt; k++) out[k] = outage ? outage[done + k] : -1;
+        GS_CUDA(cudaMemcpy(G->ws.outage.p, out.data(), B * 4, cudaMemcpyHostToDevice));
+        if (loadScale) {
+            std::vector<double> sc((size_t)n * B, 1.0);
+            for (int k = 0; k < cnt; k++)
+                for (int i = 0; i < n; i++) sc[(size_t)i * B + k] = loadScale[(size_t)(done + k) * n + i];
+            GS_CUDA(cudaMemcpy(G->ws.loadScale.p, sc.data(), sc.size() * 8, cudaMemcpyHostToDevice));
+        }
+        float ms = 0;
+        rc = NewtonDispatch(G, cnt, loadScale != nullptr, false, o, &ms);
+        if (rc) return rc;
+        std::vector<int> st(cnt), it(cnt);
+        std::vector<double> mis(cnt);
+        GS_CUDA(cudaMemcpy(st.data(), G->ws.status.p, cnt * 4, cudaMemcpyDeviceToHost));
+        GS_CUDA(cudaMemcpy(it.data(), G->ws.iters.p, cnt * 4, cudaMemcpyDeviceToHost));
+        GS_CUDA(cudaMemcpy(mis.data(), G->ws.finalMis.p, cnt * 8, cudaMemcpyDeviceToHost));
+        for (int k = 0; k < cnt; k++) {
+            if (status) status[done + k] = st[k];
+            if (iterations) iterations[done + k] = it[k];
+            if (maxMismatch) maxMismatch[done + k] = mis[k];
+        }
+        if (vmOut || vaOut) {
+            std::vector<double> v((size_t)n * B);
+            for (int pass = 0; pass < 2; pass++) {
+                double* dst = pass == 0 ? vmOut : vaOut;
+                if (!dst) continue;
+                GS_CUDA(cudaMemcpy(v.data(), pass == 0 ? G->ws.vm.p : G->ws.va.p, v.size() * 8, cudaMemcpyDeviceToHost));
+                const double f = pass == 0 ? 1.0 : 180.0 / 3.14159265358979323846;
+                for (int k = 0; k < cnt; k++)
+                    for (int i = 0; i < n; i++) dst[(size_t)(done + k) * n + i] = v[(size_t)i * B + k] * f;
+            }
+        }
+        done += cnt;
+    }
+    return GS_OK;
+}
+
+int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts* opts, gs_n1_result* res) {
+    if (!G || !res || nOut < 0 || (nOut > 0 && !idx)) return GS_ERR_INVALID_ARG;
+    gs_ctx* ctx = G->ctx;
+    int rc = CheckOpts(ctx, opts);
+    if (rc) return rc;
+    gs_pf_opts o = *opts;
+    if (o.flat_start) return SetErr(ctx, GS_ERR_UNSUPPORTED, "flat_start: pass a flat start in the descriptor");
+    const Symbolic& s = G->sym;
+    const HostGrid& h = G->host;
+    for (int k = 0; k < nOut; k++)  // AN-02: an out-of-service branch is refused (ContingencyAnalysis.cs:290-300)
+        if (idx[k] < -1 || idx[k] >= s.nbr || (idx[k] >= 0 && !h.brOn[idx[k]]))
+            return SetErr(ctx, GS_ERR_INVALID_ARG, "branch " + std::to_string(idx[k]) + " is not an in-service branch");
+    GS_CUDA(cudaSetDevice(ctx->device));
+    const int n = s.n, nItems = s.nbr + s.n;
+    res->base_status = GS_PF_NOT_RUN;
+    res->base_iterations = 0;
+    res->n_singular_pivot = 0;
+    res->n_batches = 0;
+    double totalMs = 0;
+    bool warm = false;
+    if (o.warm_start_from_base) {
+        int st = 0, it = 0;
+        double mis = 0;
+        float ms = 0;
+        rc = SolveBase(G, o, &st, &it, &mis, &ms);
+        if (rc) return rc;
+        totalMs += ms;
+        res->base_status = st;
+        res->base_iterations = it;
+        warm = st == GS_PF_CONVERGED;
+    }
+    // effective voltage limits (VoltageLimits.OperationalLowFor / HighFor, :55-67)
+    bool perBus = false;
+    if (o.per_bus_voltage_limits)
+        for (int i = 0; i < n; i++) if (!std::isnan(h.vmin[i]) || !std::isnan(h.vmax[i])) perBus = true;
+    std::vector<double> lo(n, 0.94), hi(n, 1.06);
+    if (perBus)
+        for (int i = 0; i < n; i++) {
+            if (!std::isnan(h.vmin[i])) lo[i] = h.vmin[i];
+            if (!std::isnan(h.vmax[i])) hi[i] = h.vmax[i];
+        }
+    DevBuf dlo, dhi, dbusId;
+    GS_CUDA(dlo.alloc(n * 8)); GS_CUDA(dhi.alloc(n * 8)); GS_CUDA(dbusId.alloc(n * 4));
+    GS_CUDA(cudaMemcpy(dlo.p, lo.data(), n * 8, cudaMemcpyHostToDevice));
+    GS_CUDA(cudaMemcpy(dhi.p, hi.data(), n * 8, cudaMemcpyHostToDevice));
+    GS_CUDA(cudaMemcpy(dbusId.p, h.busId.data(), n * 4, cudaMemcpyHostToDevice));
+    const int chunk = 256;
+    const int nChunks = (nItems + chunk - 1) / chunk;
+    NewtonStats stats;
+    int written = 0;
+    bool capacityOk = true;
+    int done = 0;
+    while (done < nOut) {
+        int B = ChooseB(G, nOut - done, o);
+        rc = EnsureWorkspace(G, B, o.precision, true, false);
+        if (rc) return rc;
+        Workspace& w = G->ws;
+        const size_t Bz = (size_t)B;
+        const int cnt = std::min(B, nOut - done);
+        std::vector<int> out(B, -1);
+        for (int k = 0; k < cnt; k++) out[k] = idx[done + k];
+        GS_CUDA(cudaMemcpy(w.outage.p, out.data(), B * 4, cudaMemcpyHostToDevice));
+        float ms = 0;
+        rc = NewtonDispatch(G, cnt, false, warm, o, &ms, &stats);
+        if (rc) return rc;
+        totalMs += ms;
+        res->n_batches++;
+        stats.launches += 2;  // classification and compaction
+        // classification of converged systems
+        GS_CUDA(w.chunkCount.alloc((size_t)nChunks * Bz * 4));
+        GS_CUDA(w.chunkOffset.alloc((size_t)nChunks * Bz * 4));
+        GS_CUDA(cudaMemsetAsync(w.chunkCount.p, 0, (size_t)nChunks * Bz * 4, ctx->stream));
+        GS_CUDA(cudaMemsetAsync(w.maxLoad.p, 0, Bz * 8, ctx->stream));
+        GS_CUDA(cudaMemsetAsync(w.minVmNeg.p, 0, Bz * 8, ctx->stream));
+        GS_CUDA(cudaMemsetAsync(w.maxVmB.p, 0, Bz * 8, ctx->stream));
+        Classify c{dlo.as<double>(), dhi.as<double>(), w.code.as<uint8_t>(), w.value.as<double>(),
+                   w.maxLoad.as<unsigned long long>(), w.minVmNeg.as<unsigned long long>(),
+                   w.maxVmB.as<unsigned long long>(), w.chunkCount.as<int>(), chunk};
+        DevBatch b = MakeBatch(G, cnt, false);
+        k_classify<<<dim3((nItems + 7) / 8, B / 32), dim3(32, 8), 0, ctx->stream>>>(G->view, b, c);
+        GS_CUDA(cudaGetLastError());
+        std::vector<int> cc((size_t)nChunks * Bz), off((size_t)nChunks * Bz);
+        GS_CUDA(cudaMemcpyAsync(cc.data(), w.chunkCount.p, cc.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        std::vector<int> st(cnt), it(cnt), fl(cnt);
+        std::vector<double> mis(cnt);
+        std::vector<unsigned long long> mxl(cnt), mnv(cnt), mxv(cnt);
+        GS_CUDA(cudaMemcpyAsync(st.data(), w.status.p, cnt * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        GS_CUDA(cudaMemcpyAsync(it.data(), w.iters.p, cnt * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        std::vector<int> itc(cnt);
+        GS_CUDA(cudaMemcpyAsync(itc.data(), w.convIters.p, cnt * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        GS_CUDA(cudaMemcpyAsync(fl.data(), w.flags.p, cnt * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        GS_CUDA(cudaMemcpyAsync(mis.data(), w.finalMis.p, cnt * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        GS_CUDA(cudaMemcpyAsync(mxl.data(), w.maxLoad.p, cnt * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        GS_CUDA(cudaMemcpyAsync(mnv.data(), w.minVmNeg.p, cnt * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        GS_CUDA(cudaMemcpyAsync(mxv.data(), w.maxVmB.p, cnt * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        GS_CUDA(cudaStreamSynchronize(ctx->stream));
+        int batchTotal = 0;
+        std::vector<int> sysStart(cnt);
+        for (int k = 0; k < cnt; k++) {
+            sysStart[k] = batchTotal;
+            int acc = batchTotal;
+            for (int ch = 0; ch < nChunks; ch++) {
+                off[(size_t)ch * Bz + k] = acc;
+                acc += cc[(size_t)ch * Bz + k];
+            }
+            batchTotal = acc;
+        }
+        for (int k = 0; k < cnt; k++) {
+            const int g = done + k;
+            auto asD = [](unsigned long long u) { double d; std::memcpy(&d, &u, 8); return d; };
+            const bool conv = st[k] == GS_PF_CONVERGED;
+            if (res->status) res->status[g] = st[k];
+            if (res->iterations) res->iterations[g] = conv ? itc[k] : it[k];
+            if (res->max_mismatch) res->max_mismatch[g] = mis[k];
+            if (res->max_loading_pct) res->max_loading_pct[g] = conv ? asD(mxl[k]) : 0.0;
+            if (res->min_vm) res->min_vm[g] = conv ? 100.0 - asD(mnv[k]) : 0.0;
+            if (res->max_vm) res->max_vm[g] = conv ? asD(mxv[k]) : 0.0;
+            if (res->viol_ptr) res->viol_ptr[g] = written + sysStart[k];
+            if (fl[k] & kFlagPivotPerturbed) res->n_singular_pivot++;
+        }
+        if (written + batchTotal > res->viol_capacity || !res->viol_kind || !res->viol_element || !res->viol_value) {
+            capacityOk = false;
+        } else if (batchTotal > 0) {
+            GS_CUDA(cudaMemcpy(w.chunkOffset.p, off.data(), off.size() * 4, cudaMemcpyHostToDevice));
+            GS_CUDA(w.outKind.alloc((size_t)batchTotal * 4));
+            GS_CUDA(w.outElem.alloc((size_t)batchTotal * 4));
+            GS_CUDA(w.outVal.alloc((size_t)batchTotal * 8));
+            k_compact<<<dim3((nChunks + 3) / 4, B / 32), dim3(32, 4), 0, ctx->stream>>>(
+                G->view, b, c, w.chunkOffset.as<int>(), w.outKind.as<int>(), w.outElem.as<int>(), w.outVal.as<double>(),
+                dbusId.as<int>());
+            GS_CUDA(cudaGetLastError());
+            GS_CUDA(cudaMemcpyAsync(res->viol_kind + written, w.outKind.p, (size_t)batchTotal * 4, cudaMemcpyDeviceToHost, ctx->stream));
+            GS_CUDA(cudaMemcpyAsync(res->viol_element + written, w.outElem.p, (size_t)batchTotal * 4, cudaMemcpyDeviceToHost, ctx->stream));
+            GS_CUDA(cudaMemcpyAsync(res->viol_value + written, w.outVal.p, (size_t)batchTotal * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            GS_CUDA(cudaStreamSynchronize(ctx->stream));
+        }
+        written += batchTotal;
+        if (res->vm || res->va_deg) {
+            std::vector<double> v((size_t)n * Bz);
+            for (int pass = 0; pass < 2; pass++) {
+                double* dst = pass == 0 ? res->vm : res->va_deg;
+                if (!dst) continue;
+                GS_CUDA(cudaMemcpy(v.data(), pass == 0 ? w.vm.p : w.va.p, v.size() * 8, cudaMemcpyDeviceToHost));
+                const double f = pass == 0 ? 1.0 : 180.0 / 3.14159265358979323846;
+                for (int k = 0; k < cnt; k++)
+                    for (int i = 0; i < n; i++) dst[(size_t)(done + k) * n + i] = v[(size_t)i * Bz + k] * f;
+            }
+        }
+        done += cnt;
+    }
+    if (res->viol_ptr) res->viol_ptr[nOut] = written;
+    res->viol_count = written;
+    res->device_ms = totalMs;
+    res->kernel_launches = stats.launches;
+    res->newton_iterations = stats.iterations;
+    res->factor_ms = stats.factorMs;
+    res->solve_ms = stats.solveMs;
+    res->mismatch_ms = stats.mismatchMs;
+    res->other_ms = stats.otherMs;
+    res->factor_bytes = stats.factorBytes;
+    return capacityOk ? GS_OK : GS_ERR_CAPACITY;
+}
+
+}  // extern "C"

@@ -1,0 +1,121 @@
+// gs_host.cpp — host-only parts of the C ABI: descriptor validation and copy, the symbolic analysis
+// without a device, status strings, option defaults.
+#include <cmath>
+#include <cstring>
+
+#include "gs_host.h"
+
+namespace gs {
+
+std::string CopyGrid(const gs_grid_desc* d, HostGrid& g) {
+    if (!d) return "null grid descriptor";
+    if (d->n_bus <= 0 || d->n_gen < 0 || d->n_branch < 0) return "bus/generator/branch counts must be positive";
+    if (!(d->base_mva > 0) || !std::isfinite(d->base_mva)) return "base_mva must be a finite number above 0";
+    const void* need[] = {d->bus_id, d->bus_type, d->pd, d->qd, d->gs, d->bs, d->vm, d->va_deg};
+    for (const void* p : need) if (!p) return "a required bus array is null";
+    if (d->n_gen > 0 && (!d->gen_bus || !d->pg || !d->qg || !d->vg || !d->qmin || !d->qmax))
+        return "a required generator array is null";
+    if (d->n_branch > 0 && (!d->br_from || !d->br_to || !d->r || !d->x || !d->b || !d->tap || !d->shift_deg || !d->rate_a))
+        return "a required branch array is null";
+    int n = d->n_bus;
+    g = HostGrid();
+    g.n = n; g.ngen = d->n_gen; g.nbr = d->n_branch; g.base = d->base_mva;
+    g.busId.assign(d->bus_id, d->bus_id + n);
+    g.busType.assign(d->bus_type, d->bus_type + n);
+    g.pd.assign(d->pd, d->pd + n); g.qd.assign(d->qd, d->qd + n);
+    g.gsh.assign(d->gs, d->gs + n); g.bsh.assign(d->bs, d->bs + n);
+    g.vm.assign(d->vm, d->vm + n); g.vaDeg.assign(d->va_deg, d->va_deg + n);
+    g.vmin.assign(n, NAN); g.vmax.assign(n, NAN);
+    if (d->vmin_pu) g.vmin.assign(d->vmin_pu, d->vmin_pu + n);
+    if (d->vmax_pu) g.vmax.assign(d->vmax_pu, d->vmax_pu + n);
+    int slack = 0;
+    for (int i = 0; i < n; i++) {
+        if (g.busType[i] < 1 || g.busType[i] > 3) return "bus_type must be 1 (PQ), 2 (PV) or 3 (slack)";
+        if (g.busType[i] == 3) slack++;
+        if (!std::isfinite(g.vm[i]) || !std::isfinite(g.vaDeg[i])) return "bus start voltages must be finite";
+    }
+    if (slack == 0) return "the grid has no slack bus";
+    int ng = d->n_gen;
+    if (ng > 0) {
+        g.genBus.assign(d->gen_bus, d->gen_bus + ng);
+        g.pg.assign(d->pg, d->pg + ng); g.qg.assign(d->qg, d->qg + ng); g.vg.assign(d->vg, d->vg + ng);
+        g.qmin.assign(d->qmin, d->qmin + ng); g.qmax.assign(d->qmax, d->qmax + ng);
+    }
+    g.genOn.assign(ng, 1);
+    if (d->gen_in_service && ng > 0) g.genOn.assign(d->gen_in_service, d->gen_in_service + ng);
+    for (int k = 0; k < ng; k++) if (g.genBus[k] < 0 || g.genBus[k] >= n) return "gen_bus out of range";
+    int nb = d->n_branch;
+    if (nb > 0) {
+        g.brF.assign(d->br_from, d->br_from + nb); g.brT.assign(d->br_to, d->br_to + nb);
+        g.r.assign(d->r, d->r + nb); g.x.assign(d->x, d->x + nb); g.b.assign(d->b, d->b + nb);
+        g.tap.assign(d->tap, d->tap + nb); g.shift.assign(d->shift_deg, d->shift_deg + nb);
+        g.rateA.assign(d->rate_a, d->rate_a + nb);
+    }
+    g.brOn.assign(nb, 1);
+    if (d->br_in_service && nb > 0) g.brOn.assign(d->br_in_service, d->br_in_service + nb);
+    for (int k = 0; k < nb; k++) {
+        if (g.brF[k] < 0 || g.brF[k] >= n || g.brT[k] < 0 || g.brT[k] >= n) return "branch end out of range";
+        if (g.brF[k] == g.brT[k]) return "a branch joins a bus to itself";
+        if (g.tap[k] < 0 || std::isnan(g.tap[k])) return "a tap ratio must be 0 (a line) or above";  // AdmittanceStamp.cs:63-66
+        if (std::isnan(g.rateA[k])) return "a rating must be 0 (unrated) or a number above 0";
+        if (g.r[k] == 0 && g.x[k] == 0) return "a branch has zero impedance";
+    }
+    return "";
+}
+
+void FillInfo(const HostGrid& g, const Symbolic& s, gs_grid_info* info) {
+    std::memset(info, 0, sizeof(*info));
+    info->n_bus = g.n;
+    info->n_branch = g.nbr;
+    info->n_pv = s.npv;
+    info->n_pq = s.npq;
+    info->m = s.m;
+    info->nnz_y = s.nnzY;
+    info->nnz_j = s.nnzJ;
+    info->nnz_lu = s.nnzLU;
+    info->lu_flops = s.flops;
+    info->n_levels = s.nLevels;
+}
+
+}  // namespace gs
+
+extern "C" {
+
+int gs_abi_version(void) { return GS_ABI_VERSION; }
+
+const char* gs_status_str(int st) {
+    switch (st) {
+        case GS_OK: return "ok";
+        case GS_ERR_INVALID_ARG: return "invalid argument";
+        case GS_ERR_CUDA: return "CUDA error";
+        case GS_ERR_OOM: return "out of device memory";
+        case GS_ERR_NO_DEVICE: return "no usable CUDA device";
+        case GS_ERR_TIMEOUT: return "timed out";
+        case GS_ERR_STATE: return "wrong call order";
+        case GS_ERR_UNSUPPORTED: return "unsupported option";
+        case GS_ERR_INTERNAL: return "internal error";
+        case GS_ERR_CAPACITY: return "output capacity too small";
+        default: return "unknown status";
+    }
+}
+
+void gs_pf_opts_default(gs_pf_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->tolerance = 1e-8;        // PowerFlowOptions.cs:20-32
+    o->diverge_limit_pu = 10.0; // :92
+    o->max_iterations = 30;     // :53-65
+    o->precision = GS_PREC_FP64;
+}
+
+int gs_analyze_host(const gs_grid_desc* desc, gs_grid_info* info) {
+    if (!info) return GS_ERR_INVALID_ARG;
+    gs::HostGrid g;
+    if (!gs::CopyGrid(desc, g).empty()) return GS_ERR_INVALID_ARG;
+    gs::Symbolic s;
+    if (!gs::Analyze(g, s).empty()) return GS_ERR_INVALID_ARG;
+    gs::FillInfo(g, s, info);
+    return GS_OK;
+}
+
+}  // extern "C"

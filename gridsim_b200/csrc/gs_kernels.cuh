@@ -1,0 +1,97 @@
+// gs_kernels.cuh — device kernels of the gridsim_b200 batched Newton-Raphson engine (sm_100a).
+//
+// Layout: every per-system quantity is batch-interleaved, value[index * B + s], B a multiple of 32.
+// A warp always works on 32 consecutive systems of one item (bus, LU entry, branch), so its loads and
+// stores are single 128-byte (FP32) or 256-byte (FP64) transactions, and index data read by the warp is
+// a broadcast. Systems are independent; no kernel synchronises across blocks.
+#pragma once
+#include <cstdint>
+
+#include "gs_internal.h"
+
+namespace gs {
+
+// per-system flags
+enum : int32_t {
+    kFlagNonFinite = 1,       // the mismatch or the Jacobian held a NaN / Inf
+    kFlagStepBad = 2,         // the step was not finite (NewtonShell.SolveStep refuses it)
+    kFlagPivotPerturbed = 4,  // a static pivot fell below its floor and was perturbed
+    kFlagJacBad = 8,          // the Jacobian held a NaN / Inf (the step is refused)
+};
+
+struct DevGrid {
+    int n, m, nnzY, nbr;
+    int64_t nnzLU;
+    const int* yRowPtr;
+    const int* yCol;
+    const double* yG;
+    const double* yB;
+    const int* brCell;
+    const double* brRed;
+    const double* brStamp;
+    const int* brF;
+    const int* brT;
+    const double* rateA;
+    const uint8_t* brOn;
+    const double* pgen;   // generation per bus (pu)
+    const double* qgen;
+    const double* pload;  // load per bus (pu)
+    const double* qload;
+    const double* vm0;
+    const double* va0;
+    const int* busType;   // effective type (1 PQ, 2 PV, 3 slack)
+    const int* busP;
+    const int* busQ;
+    const int* ySlot;
+    const int32_t* entSlot;
+    const int32_t* entKind;
+    const int32_t* entHasA;
+    const int64_t* entPairPtr;
+    const int2* pairs;
+    const int32_t* diagEnt;
+    const int* levelNodes;
+    const int* levelNodePtr;
+    const int32_t* entNode;
+    // work schedules (see Symbolic::Schedule): factorisation, backward and forward substitution
+    const int* fWork;
+    const int* fItems;
+    const int* fLevelPtr;
+    const int* bWork;
+    const int* bItems;
+    const int* bLevelPtr;
+    const int* vWork;
+    const int* vItems;
+    const int* vLevelPtr;
+    const int64_t* luBase;
+    const int* luCnt;
+    const int* pRowPtr;
+    const int* pRows;
+};
+
+struct DevBatch {
+    int B;                  // interleave stride (multiple of 32)
+    int count;              // live systems
+    double* vm;             // [n][B]
+    double* va;             // [n][B]
+    void* lu;               // [nnzLU][B] of the LU type (diagonal slots keep A(k, k))
+    void* piv;              // [m][B] pivots U(k, k)
+    void* y;                // [m][B] right-hand side / step
+    void* z;                // [m][B] correction (mixed precision), or null
+    double* rhs64;          // [m][B] FP64 mismatch (mixed precision), or null
+    int* refine;            // [B] refine this step (mixed precision), or null
+    unsigned long long* maxMis;  // [B] bit pattern of a non-negative double
+    unsigned long long* maxDx;
+    double* startMis;       // [B]
+    double* finalMis;       // [B]
+    int* status;            // [B]
+    int* iters;             // [B] steps taken
+    int* convIters;         // [B] steps taken when the tolerance was first met
+    int* convAt;            // [B] iteration of the first crossing, -1 before
+    int* active;            // [B]
+    int* flags;             // [B]
+    const int* outage;      // [B] branch index or -1
+    const double* loadScale;  // [n][B] or null
+    int* activeCount;       // [1]
+};
+
+}  // namespace gs

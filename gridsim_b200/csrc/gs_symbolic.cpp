@@ -1,0 +1,412 @@
+// gs_symbolic.cpp — host symbolic analysis of the gridsim_b200 engine.
+//
+// One analysis per grid, shared by every system of every batch (contingencies of that grid, load
+// scalings, serving requests). It covers:
+//   * the Y-bus of the intact grid, stamped as SparseNewtonRaphsonPowerFlow.BuildY does
+//     (src/GridSim.Core/PowerFlow/SparseNewtonRaphsonPowerFlow.cs:382-402, AdmittanceStamp.cs:35-76,
+//     cell order and summation order of ComplexCsr.Builder, Numerics/Sparse.cs:134-224), and for every
+//     branch the values its four cells take when that branch is out (a single-branch outage is a
+//     rank-2 change of Y; the replacement values are summed in the order a rebuilt Y would sum them);
+//   * the bus specification and equation numbering (NewtonShell.BuildBusSpec :433-486,
+//     EquationPositions :327-336) and the Jacobian superset pattern (BuildJacobianStructure :296-332);
+//   * a minimum-degree order of that pattern (the same exact-degree method as
+//     Numerics/MinimumDegreeOrdering.cs:23-121) and the static-pivot LU pattern it implies: pivots on
+//     the permuted diagonal, so L and U^T share the pattern of the symmetric symbolic factor;
+//   * the elimination-tree levels and, per level, the warp tasks of the fused "Crout" factorisation
+//     with forward substitution: every L/U entry is its own sparse dot product over the row subtree of
+//     its node, with the index pairs precomputed here.
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <numeric>
+
+#include "gs_internal.h"
+
+namespace gs {
+namespace {
+
+using cplx = std::complex<double>;
+constexpr double kPi = 3.14159265358979323846;
+
+struct Stamp { cplx yff, ytt, yft, ytf; };
+
+Stamp BranchStamp(double r, double x, double b, double tapRatio, double shiftDeg) {
+    cplx ys = cplx(1.0, 0.0) / cplx(r, x);
+    cplx bc(0.0, b / 2.0);
+    double a = tapRatio == 0 ? 1.0 : tapRatio;
+    double sh = shiftDeg * kPi / 180.0;
+    cplx t(a * std::cos(sh), a * std::sin(sh));
+    return {(ys + bc) / (a * a), ys + bc, -ys / std::conj(t), -ys / t};
+}
+
+}  // namespace
+
+std::vector<int> MinimumDegreeOrder(int n, const std::vector<int>& rowPtr, const std::vector<int>& col) {
+    // Explicit elimination graph with exact degrees; bucket lists by degree, most recent insertion first;
+    // initial insertion in descending index so that the lowest index wins the first ties.
+    std::vector<int> order(n);
+    std::vector<std::vector<int>> adj(n);
+    for (int i = 0; i < n; i++)
+        for (int p = rowPtr[i]; p < rowPtr[i + 1]; p++) {
+            int j = col[p];
+            if (j != i) { adj[i].push_back(j); adj[j].push_back(i); }
+        }
+    for (auto& a : adj) { std::sort(a.begin(), a.end()); a.erase(std::unique(a.begin(), a.end()), a.end()); }
+    std::vector<int> head(n + 1, -1), nxt(n, -1), prv(n, -1), deg(n, 0);
+    auto push = [&](int v, int d) {
+        deg[v] = d; prv[v] = -1; nxt[v] = head[d];
+        if (head[d] >= 0) prv[head[d]] = v;
+        head[d] = v;
+    };
+    auto pop = [&](int v) {
+        if (prv[v] >= 0) nxt[prv[v]] = nxt[v]; else head[deg[v]] = nxt[v];
+        if (nxt[v] >= 0) prv[nxt[v]] = prv[v];
+    };
+    for (int i = n - 1; i >= 0; i--) push(i, (int)adj[i].size());
+    std::vector<char> gone(n, 0);
+    std::vector<int> mark(n, -1), nbr;
+    int dmin = 0;
+    for (int s = 0; s < n; s++) {
+        while (head[dmin] < 0) dmin++;
+        int v = head[dmin];
+        pop(v);
+        gone[v] = 1;
+        order[s] = v;
+        nbr.clear();
+        for (int u : adj[v]) if (!gone[u]) nbr.push_back(u);
+        for (int u : nbr) mark[u] = s;
+        for (int u : nbr) {
+            pop(u);
+            std::vector<int>& au = adj[u];
+            size_t w = 0;
+            for (size_t p = 0; p < au.size(); p++) {
+                int x = au[p];
+                if (x != v && !gone[x] && mark[x] != s) au[w++] = x;
+            }
+            au.resize(w);
+            for (int y : nbr) if (y != u) au.push_back(y);
+            push(u, (int)au.size());
+        }
+        std::vector<int>().swap(adj[v]);
+        if (dmin > 0) dmin--;
+    }
+    return order;
+}
+
+std::string Analyze(const HostGrid& g, Symbolic& s) {
+    const int n = g.n;
+    s = Symbolic();
+    s.n = n;
+    s.nbr = g.nbr;
+
+    // ---------------- Y-bus (stamping order: in-service branches in order, then bus shunts) ----------------
+    struct Contribution { int row, col, owner; double gv, bv; };  // owner: branch index or -1 (shunt)
+    std::vector<Contribution> contrib;
+    contrib.reserve(4 * g.nbr + n);
+    s.brStamp.assign(8 * (size_t)g.nbr, 0.0);
+    for (int k = 0; k < g.nbr; k++) {
+        Stamp st = BranchStamp(g.r[k], g.x[k], g.b[k], g.tap[k], g.shift[k]);
+        double* o = &s.brStamp[8 * (size_t)k];
+        o[0] = st.yff.real(); o[1] = st.yff.imag(); o[2] = st.ytt.real(); o[3] = st.ytt.imag();
+        o[4] = st.yft.real(); o[5] = st.yft.imag(); o[6] = st.ytf.real(); o[7] = st.ytf.imag();
+        if (!g.brOn[k]) continue;
+        int f = g.brF[k], t = g.brT[k];
+        const cplx v[4] = {st.yff, st.ytt, st.yft, st.ytf};
+        const int rr[4] = {f, t, f, t}, cc[4] = {f, t, t, f};
+        for (int q = 0; q < 4; q++)
+            if (!(v[q].real() == 0.0 && v[q].imag() == 0.0)) contrib.push_back({rr[q], cc[q], k, v[q].real(), v[q].imag()});
+    }
+    for (int i = 0; i < n; i++)
+        if (!(g.gsh[i] == 0 && g.bsh[i] == 0)) contrib.push_back({i, i, -1, g.gsh[i] / g.base, g.bsh[i] / g.base});
+    // cells: per row, columns ascending with the diagonal always present; contributions kept in order
+    std::vector<std::vector<int>> rowCols(n);
+    for (auto& c : contrib) rowCols[c.row].push_back(c.col);
+    s.yRowPtr.assign(n + 1, 0);
+    for (int i = 0; i < n; i++) {
+        auto& rc = rowCols[i];
+        rc.push_back(i);
+        std::sort(rc.begin(), rc.end());
+        rc.erase(std::unique(rc.begin(), rc.end()), rc.end());
+        s.yRowPtr[i + 1] = s.yRowPtr[i] + (int)rc.size();
+    }
+    s.nnzY = s.yRowPtr[n];
+    s.yCol.resize(s.nnzY);
+    for (int i = 0; i < n; i++) std::copy(rowCols[i].begin(), rowCols[i].end(), s.yCol.begin() + s.yRowPtr[i]);
+    auto cellOf = [&](int i, int j) {
+        auto b = s.yCol.begin() + s.yRowPtr[i], e = s.yCol.begin() + s.yRowPtr[i + 1];
+        return (int)(std::lower_bound(b, e, j) - s.yCol.begin());
+    };
+    std::vector<std::vector<int>> cellContrib(s.nnzY);
+    for (int c = 0; c < (int)contrib.size(); c++) cellContrib[cellOf(contrib[c].row, contrib[c].col)].push_back(c);
+    s.yG.assign(s.nnzY, 0.0);
+    s.yB.assign(s.nnzY, 0.0);
+    for (int p = 0; p < s.nnzY; p++) {
+        double gv = 0.0, bv = 0.0;
+        for (int c : cellContrib[p]) { gv += contrib[c].gv; bv += contrib[c].bv; }
+        s.yG[p] = gv;
+        s.yB[p] = bv;
+    }
+    s.brCell.assign(4 * (size_t)g.nbr, -1);
+    s.brRed.assign(8 * (size_t)g.nbr, 0.0);
+    for (int k = 0; k < g.nbr; k++) {
+        if (!g.brOn[k]) continue;
+        int f = g.brF[k], t = g.brT[k];
+        const int rr[4] = {f, t, f, t}, cc[4] = {f, t, t, f};
+        for (int q = 0; q < 4; q++) {
+            int p = cellOf(rr[q], cc[q]);
+            s.brCell[4 * (size_t)k + q] = p;
+            double gv = 0.0, bv = 0.0;
+            for (int c : cellContrib[p]) if (contrib[c].owner != k) { gv += contrib[c].gv; bv += contrib[c].bv; }
+            s.brRed[8 * (size_t)k + 2 * q] = gv;
+            s.brRed[8 * (size_t)k + 2 * q + 1] = bv;
+        }
+    }
+
+    // ---------------- bus specification and equation numbering ----------------
+    std::vector<double> pgB(n, 0), qgB(n, 0), vgB(n, 0);
+    std::vector<char> hasGen(n, 0);
+    for (int k = 0; k < g.ngen; k++) {
+        if (!g.genOn[k]) continue;
+        int i = g.genBus[k];
+        pgB[i] += g.pg[k];
+        qgB[i] += g.qg[k];
+        vgB[i] = g.vg[k];  // the last unit at the bus sets the voltage
+        hasGen[i] = 1;
+    }
+    s.type0.resize(n); s.vm0.resize(n); s.va0.resize(n); s.pspec.resize(n); s.qspec.resize(n);
+    for (int i = 0; i < n; i++) {
+        int t = g.busType[i];
+        s.type0[i] = (t == 2 && !hasGen[i]) ? 1 : t;  // a PV bus with no unit is solved as PQ
+        bool vc = s.type0[i] == 3 || s.type0[i] == 2;
+        s.vm0[i] = (vc && hasGen[i]) ? vgB[i] : g.vm[i];
+        s.va0[i] = g.vaDeg[i] * kPi / 180.0;
+        s.pspec[i] = (pgB[i] - g.pd[i]) / g.base;
+        s.qspec[i] = (qgB[i] - g.qd[i]) / g.base;
+    }
+    s.pPos.assign(n, -1);
+    s.qPos.assign(n, -1);
+    int m = 0;
+    for (int i = 0; i < n; i++) if (s.type0[i] != 3) s.pPos[i] = m++;
+    for (int i = 0; i < n; i++) if (s.type0[i] == 1) { s.qPos[i] = m++; s.npq++; }
+    for (int i = 0; i < n; i++) if (s.type0[i] == 2) s.npv++;
+    s.m = m;
+    if (m == 0) return "the grid has no unknowns";
+
+    // ---------------- Jacobian superset pattern ----------------
+    std::vector<std::vector<int>> jr(m);
+    for (int i = 0; i < n; i++) {
+        int pi = s.pPos[i], qi = s.qPos[i];
+        if (pi < 0 && qi < 0) continue;
+        for (int p = s.yRowPtr[i]; p < s.yRowPtr[i + 1]; p++) {
+            int j = s.yCol[p], pj = s.pPos[j], qj = s.qPos[j];
+            if (pi >= 0 && pj >= 0) jr[pi].push_back(pj);
+            if (pi >= 0 && qj >= 0) jr[pi].push_back(qj);
+            if (qi >= 0 && pj >= 0) jr[qi].push_back(pj);
+            if (qi >= 0 && qj >= 0) jr[qi].push_back(qj);
+        }
+    }
+    s.jRowPtr.assign(m + 1, 0);
+    for (int a = 0; a < m; a++) {
+        jr[a].push_back(a);
+        std::sort(jr[a].begin(), jr[a].end());
+        jr[a].erase(std::unique(jr[a].begin(), jr[a].end()), jr[a].end());
+        s.jRowPtr[a + 1] = s.jRowPtr[a] + (int)jr[a].size();
+    }
+    s.nnzJ = s.jRowPtr[m];
+    s.jCol.resize(s.nnzJ);
+    for (int a = 0; a < m; a++) std::copy(jr[a].begin(), jr[a].end(), s.jCol.begin() + s.jRowPtr[a]);
+
+    // ---------------- ordering and static-pivot LU pattern ----------------
+    s.perm = MinimumDegreeOrder(m, s.jRowPtr, s.jCol);
+    s.pinv.assign(m, -1);
+    for (int k = 0; k < m; k++) s.pinv[s.perm[k]] = k;
+    s.parent.assign(m, -1);
+    std::vector<std::vector<int>> children(m);
+    std::vector<std::vector<int>> P(m);
+    std::vector<int> mark(m, -1);
+    for (int k = 0; k < m; k++) {
+        std::vector<int>& pk = P[k];
+        mark[k] = k;
+        int a = s.perm[k];
+        for (int p = s.jRowPtr[a]; p < s.jRowPtr[a + 1]; p++) {
+            int l = s.pinv[s.jCol[p]];
+            if (l > k && mark[l] != k) { mark[l] = k; pk.push_back(l); }
+        }
+        for (int c : children[k])
+            for (int l : P[c])
+                if (l > k && mark[l] != k) { mark[l] = k; pk.push_back(l); }
+        std::sort(pk.begin(), pk.end());
+        if (!pk.empty()) { s.parent[k] = pk[0]; children[pk[0]].push_back(k); }
+    }
+    s.luBase.resize(m + 1);
+    s.luCnt.resize(m);
+    s.pRowPtr.assign(m + 1, 0);
+    int64_t off = 0;
+    for (int k = 0; k < m; k++) {
+        s.luBase[k] = off;
+        s.luCnt[k] = (int)P[k].size();
+        off += 1 + 2 * (int64_t)P[k].size();
+        s.pRowPtr[k + 1] = s.pRowPtr[k] + (int)P[k].size();
+    }
+    s.luBase[m] = off;
+    s.nnzLU = off;
+    if (off >= (int64_t)INT32_MAX) return "the LU factor is too large for 32-bit slot indices";
+    s.pRows.resize(s.pRowPtr[m]);
+    for (int k = 0; k < m; k++) std::copy(P[k].begin(), P[k].end(), s.pRows.begin() + s.pRowPtr[k]);
+    auto posIn = [&](int k, int l) {  // index of l in P_k (l > k)
+        const int* b = &s.pRows[s.pRowPtr[k]];
+        const int* e = b + s.luCnt[k];
+        const int* it = std::lower_bound(b, e, l);
+        return (it != e && *it == l) ? (int)(it - b) : -1;
+    };
+    auto slotOf = [&](int k, int l) -> int64_t {  // LU slot of permuted cell (k, l)
+        if (k == l) return s.luBase[k];
+        if (k < l) { int t = posIn(k, l); return t < 0 ? -1 : s.luBase[k] + 1 + t; }
+        int t = posIn(l, k);
+        return t < 0 ? -1 : s.luBase[l] + 1 + s.luCnt[l] + t;
+    };
+    // Y cell -> the four Jacobian blocks' LU slots
+    s.ySlot.assign(4 * (size_t)s.nnzY, -1);
+    for (int i = 0; i < n; i++) {
+        int pi = s.pPos[i], qi = s.qPos[i];
+        for (int p = s.yRowPtr[i]; p < s.yRowPtr[i + 1]; p++) {
+            int j = s.yCol[p], pj = s.pPos[j], qj = s.qPos[j];
+            int* o = &s.ySlot[4 * (size_t)p];
+            if (pi >= 0 && pj >= 0) o[0] = (int)slotOf(s.pinv[pi], s.pinv[pj]);
+            if (pi >= 0 && qj >= 0) o[1] = (int)slotOf(s.pinv[pi], s.pinv[qj]);
+            if (qi >= 0 && pj >= 0) o[2] = (int)slotOf(s.pinv[qi], s.pinv[pj]);
+            if (qi >= 0 && qj >= 0) o[3] = (int)slotOf(s.pinv[qi], s.pinv[qj]);
+        }
+    }
+    s.busP.assign(n, -1);
+    s.busQ.assign(n, -1);
+    for (int i = 0; i < n; i++) {
+        if (s.pPos[i] >= 0) s.busP[i] = s.pinv[s.pPos[i]];
+        if (s.qPos[i] >= 0) s.busQ[i] = s.pinv[s.qPos[i]];
+    }
+    // which LU slots hold a Jacobian value (the rest are fill, which start from zero)
+    std::vector<char> hasA(s.nnzLU, 0);
+    for (int v : s.ySlot) if (v >= 0) hasA[v] = 1;
+
+    // ---------------- levels ----------------
+    s.level.assign(m, 0);
+    for (int k = 0; k < m; k++)
+        if (s.parent[k] >= 0) s.level[s.parent[k]] = std::max(s.level[s.parent[k]], s.level[k] + 1);
+    s.nLevels = 0;
+    for (int k = 0; k < m; k++) s.nLevels = std::max(s.nLevels, s.level[k] + 1);
+    s.levelNodePtr.assign(s.nLevels + 1, 0);
+    for (int k = 0; k < m; k++) s.levelNodePtr[s.level[k] + 1]++;
+    for (int l = 0; l < s.nLevels; l++) s.levelNodePtr[l + 1] += s.levelNodePtr[l];
+    s.levelNodes.resize(m);
+    {
+        std::vector<int> fill(s.levelNodePtr.begin(), s.levelNodePtr.end() - 1);
+        for (int k = 0; k < m; k++) s.levelNodes[fill[s.level[k]]++] = k;
+    }
+
+    // ---------------- Crout entries and their index pairs ----------------
+    // Row subtree J_k = { j < k : k in P_j }, ascending.
+    std::vector<std::vector<int>> rowSub(m);
+    for (int j = 0; j < m; j++)
+        for (int t = s.pRowPtr[j]; t < s.pRowPtr[j + 1]; t++) rowSub[s.pRows[t]].push_back(j);
+    // Per node k the entries are: diag, U(k, P_k[t]) for each t, forward y(k), L(P_k[t], k) for each t.
+    s.entPairPtr.assign(1, 0);
+    s.diagPairNode.assign(m, -1);
+    std::vector<int> posK(m, -1);
+    std::vector<int64_t> cnt;
+    std::vector<std::vector<int32_t>> lists;
+    s.flops = 0;
+    for (int k = 0; k < m; k++) {
+        const int c = s.luCnt[k];
+        const int nE = 2 * c + 2;
+        for (int t = 0; t < c; t++) posK[s.pRows[s.pRowPtr[k] + t]] = t;
+        lists.assign(nE, {});
+        // entry indices: 0 diag, 1..c upper, c+1 fwd, c+2..2c+1 lower
+        for (int j : rowSub[k]) {
+            int tk = posIn(j, k);
+            int cj = s.luCnt[j];
+            int64_t Lkj = s.luBase[j] + 1 + cj + tk, Ujk = s.luBase[j] + 1 + tk;
+            lists[0].push_back((int32_t)Lkj); lists[0].push_back((int32_t)Ujk);
+            lists[c + 1].push_back((int32_t)Lkj); lists[c + 1].push_back(j);
+            for (int t = tk + 1; t < cj; t++) {
+                int r = s.pRows[s.pRowPtr[j] + t];
+                int tr = posK[r];  // r in P_k by the fill property
+                int64_t Ujr = s.luBase[j] + 1 + t, Lrj = s.luBase[j] + 1 + cj + t;
+                lists[1 + tr].push_back((int32_t)Lkj); lists[1 + tr].push_back((int32_t)Ujr);
+                lists[c + 2 + tr].push_back((int32_t)Lrj); lists[c + 2 + tr].push_back((int32_t)Ujk);
+            }
+        }
+        int e0 = (int)s.entSlot.size();
+        s.diagPairNode[k] = e0;
+        for (int e = 0; e < nE; e++) {
+            int32_t slot, kind;
+            if (e == 0) { slot = (int32_t)s.luBase[k]; kind = kDiag; }
+            else if (e <= c) { slot = (int32_t)(s.luBase[k] + e); kind = kUpper; }
+            else if (e == c + 1) { slot = k; kind = kFwd; }
+            else { slot = (int32_t)(s.luBase[k] + 1 + c + (e - c - 2)); kind = kLower; }
+            s.entSlot.push_back(slot);
+            s.entKind.push_back(kind);
+            s.entHasA.push_back(kind == kFwd ? 1 : (int32_t)hasA[slot]);
+            s.pairs.insert(s.pairs.end(), lists[e].begin(), lists[e].end());
+            s.entPairPtr.push_back((int64_t)s.pairs.size() / 2);
+            s.flops += (int64_t)lists[e].size() / 2;
+        }
+        for (int t = 0; t < c; t++) posK[s.pRows[s.pRowPtr[k] + t]] = -1;
+    }
+
+    // ---------------- work schedules per level ----------------
+    s.entNode.assign(s.entSlot.size(), 0);
+    for (int k = 0; k < m; k++)
+        for (int e = s.diagPairNode[k]; e < s.diagPairNode[k] + 2 * s.luCnt[k] + 2; e++) s.entNode[e] = k;
+    // Short pieces (at most kShort pairs) are packed kPack to an item (the most lane groups a warp has:
+    // 4 for FP32, 8 for FP64 -- the kernels take the first `count`); longer ones get a warp each.
+    const int kShort = 32, kPack = 8;
+    auto pack = [&](Symbolic::Schedule& sc, const std::vector<int32_t>& list, const std::vector<int64_t>& len) {
+        std::vector<int32_t> shortOnes;
+        for (size_t q = 0; q < list.size(); q++) {
+            if (len[q] > kShort) {
+                sc.work.push_back(list[q]);
+                sc.items.push_back((int32_t)sc.work.size() - 1);
+                sc.items.push_back(-1);
+            } else {
+                shortOnes.push_back(list[q]);
+            }
+        }
+        for (size_t q = 0; q < shortOnes.size(); q += kPack) {
+            int cnt = (int)std::min<size_t>(kPack, shortOnes.size() - q);
+            sc.items.push_back((int32_t)sc.work.size());
+            sc.items.push_back(cnt);
+            for (int t = 0; t < cnt; t++) sc.work.push_back(shortOnes[q + t]);
+        }
+        sc.levelItemPtr.push_back((int32_t)sc.items.size() / 2);
+    };
+    s.factor.levelItemPtr.assign(1, 0);
+    s.backward.levelItemPtr.assign(1, 0);
+    s.forward.levelItemPtr.assign(1, 0);
+    for (int l = 0; l < s.nLevels; l++) {
+        std::vector<int32_t> phaseA, phaseB, bwd, fwd;
+        std::vector<int64_t> lenA, lenB, lenBwd, lenFwd;
+        for (int q = s.levelNodePtr[l]; q < s.levelNodePtr[l + 1]; q++) {
+            const int k = s.levelNodes[q];
+            const int e0 = s.diagPairNode[k], c = s.luCnt[k];
+            for (int e = e0; e < e0 + 2 * c + 2; e++) {
+                const int64_t np = s.entPairPtr[e + 1] - s.entPairPtr[e];
+                const int kind = s.entKind[e];
+                // an upper or forward entry with no pairs keeps its value where it already is
+                if ((kind == kUpper || kind == kFwd) && np == 0 && s.entHasA[e]) continue;
+                if (kind == kLower) { phaseB.push_back(e); lenB.push_back(np); }
+                else { phaseA.push_back(e); lenA.push_back(np); }
+                if (kind == kFwd) { fwd.push_back(e); lenFwd.push_back(np); }
+            }
+            bwd.push_back(q);
+            lenBwd.push_back(c);
+        }
+        pack(s.factor, phaseA, lenA);
+        pack(s.factor, phaseB, lenB);
+        pack(s.backward, bwd, lenBwd);
+        pack(s.forward, fwd, lenFwd);
+    }
+    return "";
+}
+
+}  // namespace gs

@@ -1,0 +1,413 @@
+"""Python mirror of GridSim.Core's load-flow seams over the gridsim_b200 C ABI.
+
+* :class:`SparseNewtonRaphsonPowerFlow` — ``IPowerFlowSolver.Solve(GridModel, PowerFlowOptions)``
+  (``src/GridSim.Core/Abstractions/IPowerFlowSolver.cs:10-13``) on the B200 engine.
+* :class:`ContingencyAnalysis` — ``ScreenBranches`` / ``ScreenBranchesParallel`` / ``ScreenBaseCase`` /
+  ``NetAgainstBase`` (``src/GridSim.Core/Analysis/ContingencyAnalysis.cs:306-344, 958-1043``), with the
+  screen's Newton solves and ScreenStateCore classification running on the device.
+
+Every call goes through ``libgridsim_b200.so``; if the library is missing the import of this module
+succeeds but the first solve raises (there is no CPU path).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _abi
+from .model import GridModel
+
+# ---------------------------------------------------------------------------------------------
+
+
+@dataclass
+class PowerFlowOptions:
+    """PowerFlowOptions (``PowerFlow/PowerFlowOptions.cs``). Q-limit enforcement and the DC-angle retry are
+    reference features this engine does not run yet: they default to off here and are refused when set."""
+    tolerance: float = 1e-8
+    max_iterations: int = 30
+    diverge_limit_pu: float = 10.0
+    flat_start: bool = False
+    enforce_q_limits: bool = False
+    retry_from_dc_start: bool = False
+    per_bus_voltage_limits: bool = False
+    precision: str = "fp64"          # "fp64" or "mixed" (FP32 LU and solves, FP64 mismatch and update)
+    warm_start_from_base: bool = False
+    batch_width: int = 0
+    phase_timing: bool = False
+
+    def to_c(self) -> _abi.PfOpts:
+        o = _abi.default_opts()
+        o.tolerance = float(self.tolerance)
+        o.max_iterations = int(self.max_iterations)
+        o.diverge_limit_pu = float(self.diverge_limit_pu)
+        o.flat_start = int(self.flat_start)
+        o.enforce_q_limits = int(self.enforce_q_limits)
+        o.retry_from_dc_start = int(self.retry_from_dc_start)
+        o.per_bus_voltage_limits = int(self.per_bus_voltage_limits)
+        o.precision = {"fp64": _abi.PREC_FP64, "mixed": _abi.PREC_MIXED}[self.precision]
+        o.warm_start_from_base = int(self.warm_start_from_base)
+        o.batch_width = int(self.batch_width)
+        o.phase_timing = int(self.phase_timing)
+        return o
+
+
+# ContingencyAnalysis.StudyOptions (ContingencyAnalysis.cs:263-268) is 100 iterations with Q limits on; the
+# Q-limit loop is not built yet, so the study set here keeps only the iteration cap.
+STUDY_MAX_ITERATIONS = 100
+
+
+@dataclass
+class LineFlow:
+    loading_percent: float
+    sf_mva: complex
+    st_mva: complex
+
+
+@dataclass
+class PowerFlowResult:
+    """PowerFlowResult (``PowerFlow/PowerFlowResult.cs``)."""
+    status: int
+    iterations: int
+    max_mismatch: float
+    bus_ids: np.ndarray
+    vm: np.ndarray
+    va_deg: np.ndarray
+    p_inj_mw: np.ndarray
+    q_inj_mvar: np.ndarray
+    loading_percent: np.ndarray
+    sf_mva: np.ndarray
+    st_mva: np.ndarray
+
+    @property
+    def converged(self) -> bool:
+        return self.status == _abi.PF_CONVERGED
+
+    @property
+    def status_name(self) -> str:
+        return _abi.PF_STATUS_NAMES[self.status]
+
+    @property
+    def total_loss_mw(self) -> float:
+        return float(np.sum(self.p_inj_mw))
+
+
+class EngineError(RuntimeError):
+    pass
+
+
+# ---------------------------------------------------------------------------------------------
+class CudaContext:
+    """An open device (gs_ctx): bounded probe and FP64 self-test on creation."""
+
+    _default: Optional["CudaContext"] = None
+
+    def __init__(self, device: int = 0, probe_timeout_ms: int = 10000):
+        self.lib = _abi.load_library()
+        self.handle = ctypes.c_void_p()
+        o = _abi.CtxOpts()
+        o.probe_timeout_ms = probe_timeout_ms
+        rc = self.lib.gs_ctx_create(device, ctypes.byref(o), ctypes.byref(self.handle))
+        if rc != _abi.GS_OK:
+            raise EngineError(f"gs_ctx_create({device}) failed: {self.lib.gs_status_str(rc).decode()}")
+
+    @classmethod
+    def default(cls) -> "CudaContext":
+        if cls._default is None:
+            cls._default = CudaContext(0)
+        return cls._default
+
+    def last_error(self) -> str:
+        buf = ctypes.create_string_buffer(1024)
+        self.lib.gs_last_error(self.handle, buf, 1024)
+        return buf.value.decode()
+
+    def check(self, rc: int, what: str) -> None:
+        if rc != _abi.GS_OK:
+            raise EngineError(f"{what}: {self.lib.gs_status_str(rc).decode()}: {self.last_error()}")
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.gs_ctx_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+
+class CudaGrid:
+    """A grid uploaded with its shared symbolic analysis (gs_grid)."""
+
+    def __init__(self, model: GridModel, ctx: Optional[CudaContext] = None):
+        self.ctx = ctx or CudaContext.default()
+        self.model = model
+        self.handle = ctypes.c_void_p()
+        d = model.desc()
+        self.ctx.check(self.ctx.lib.gs_grid_create(self.ctx.handle, ctypes.byref(d), ctypes.byref(self.handle)),
+                       "gs_grid_create")
+
+    def info(self) -> _abi.GridInfo:
+        i = _abi.GridInfo()
+        self.ctx.check(self.ctx.lib.gs_grid_info_get(self.handle, ctypes.byref(i)), "gs_grid_info_get")
+        return i
+
+    def close(self) -> None:
+        if self.handle:
+            self.ctx.lib.gs_grid_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _p(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+# ---------------------------------------------------------------------------------------------
+class SparseNewtonRaphsonPowerFlow:
+    """IPowerFlowSolver on the B200 engine. One instance per thread (as the reference's engines)."""
+
+    def __init__(self, precision: str = "fp64", ctx: Optional[CudaContext] = None):
+        self.precision = precision
+        self.ctx = ctx
+        self._grid: Optional[CudaGrid] = None
+        self._model_key = None
+
+    def grid_for(self, model: GridModel) -> CudaGrid:
+        key = id(model)
+        if self._grid is None or self._model_key != key or self._grid.model is not model:
+            self._grid = CudaGrid(model, self.ctx)
+            self._model_key = key
+        return self._grid
+
+    def solve(self, model: GridModel, options: Optional[PowerFlowOptions] = None) -> PowerFlowResult:
+        opt = options or PowerFlowOptions(precision=self.precision)
+        g = self.grid_for(model)
+        n, nb = model.n_bus, model.n_branch
+        out = {k: np.zeros(n) for k in ("vm", "va_deg", "p_inj_mw", "q_inj_mvar")}
+        out["loading_percent"] = np.zeros(nb)
+        out["sf"] = np.zeros(2 * max(nb, 1))
+        out["st"] = np.zeros(2 * max(nb, 1))
+        r = _abi.PfResult()
+        r.vm, r.va_deg, r.p_inj_mw, r.q_inj_mvar = (_p(out[k]) for k in ("vm", "va_deg", "p_inj_mw", "q_inj_mvar"))
+        r.loading_pct, r.sf_mva, r.st_mva = _p(out["loading_percent"]), _p(out["sf"]), _p(out["st"])
+        c = opt.to_c()
+        g.ctx.check(g.ctx.lib.gs_pf_solve(g.handle, ctypes.byref(c), ctypes.byref(r)), "gs_pf_solve")
+        sf = out["sf"][: 2 * nb].reshape(-1, 2)
+        st = out["st"][: 2 * nb].reshape(-1, 2)
+        return PowerFlowResult(status=r.status, iterations=r.iterations, max_mismatch=r.max_mismatch,
+                               bus_ids=model.bus_id.copy(), vm=out["vm"], va_deg=out["va_deg"],
+                               p_inj_mw=out["p_inj_mw"], q_inj_mvar=out["q_inj_mvar"],
+                               loading_percent=out["loading_percent"], sf_mva=sf[:, 0] + 1j * sf[:, 1],
+                               st_mva=st[:, 0] + 1j * st[:, 1])
+
+    def solve_batch(self, model: GridModel, load_scale: Optional[np.ndarray] = None,
+                    outage: Optional[np.ndarray] = None, options: Optional[PowerFlowOptions] = None,
+                    keep_states: bool = False) -> dict:
+        """Many load flows of one grid in device batches (``gs_pf_solve_batch``)."""
+        opt = options or PowerFlowOptions(precision=self.precision)
+        g = self.grid_for(model)
+        n = model.n_bus
+        count = (load_scale.shape[0] if load_scale is not None else outage.shape[0])
+        ls = None if load_scale is None else np.ascontiguousarray(load_scale, np.float64)
+        og = None if outage is None else np.ascontiguousarray(outage, np.int32)
+        st = np.zeros(count, np.int32)
+        it = np.zeros(count, np.int32)
+        mis = np.zeros(count)
+        vm = np.zeros(count * n) if keep_states else None
+        va = np.zeros(count * n) if keep_states else None
+        c = opt.to_c()
+        g.ctx.check(g.ctx.lib.gs_pf_solve_batch(g.handle, count, _p(ls), _p(og), ctypes.byref(c), _p(st), _p(it),
+                                                _p(mis), _p(vm), _p(va)), "gs_pf_solve_batch")
+        out = {"status": st, "iterations": it, "max_mismatch": mis}
+        if keep_states:
+            out["vm"] = vm.reshape(count, n)
+            out["va_deg"] = va.reshape(count, n)
+        return out
+
+
+# ---------------------------------------------------------------------------------------------
+@dataclass
+class ContingencyViolation:
+    """ContingencyViolation (ContingencyAnalysis.cs:156-163)."""
+    kind: int      # _abi.VIOL_*
+    element: int   # original branch index, or bus id
+    value: float   # loading % or Vm pu
+    name: str = ""
+
+
+@dataclass
+class ContingencyResult:
+    """ContingencyResult (ContingencyAnalysis.cs:9-96)."""
+    outage: str
+    converged: bool
+    max_branch_loading_percent: float
+    worst_boundary_loading_percent: float
+    min_vm: float
+    max_vm: float
+    violations: list
+    details: list = field(default_factory=list)
+    status: int = _abi.PF_CONVERGED
+    iterations: int = 0
+    max_mismatch: float = 0.0
+    netted_against_base: bool = False
+    pre_existing_violations: list = field(default_factory=list)
+    worsened_pre_existing_violations: list = field(default_factory=list)
+
+    @property
+    def secure(self) -> bool:
+        return self.converged and len(self.violations) == 0
+
+
+def _branch_label(model: GridModel, k: int) -> str:
+    """ContingencyAnalysis.Label (:1832-1833): the name (none here: "from-to" bus ids) plus " (tx)"."""
+    lab = f"{int(model.bus_id[model.br_from[k]])}-{int(model.bus_id[model.br_to[k]])}"
+    return lab + (" (tx)" if model.is_transformer[k] else "")
+
+
+def _violation_texts(model: GridModel, details: Sequence[ContingencyViolation]) -> list:
+    """ContingencyAnalysis.ViolationTexts (:1050-1067)."""
+    texts = [f"branch {d.name} {d.value:.0f}%" for d in details if d.kind == _abi.VIOL_BRANCH_OVERLOAD]
+    under = [d.value for d in details if d.kind == _abi.VIOL_UNDERVOLTAGE]
+    over = [d.value for d in details if d.kind == _abi.VIOL_OVERVOLTAGE]
+    if under:
+        texts.append(f"undervoltage {min(under):.3f} p.u.")
+    if over:
+        texts.append(f"overvoltage {max(over):.3f} p.u.")
+    return texts
+
+
+def _branch_name(model: GridModel, k: int) -> str:
+    return f"{int(model.bus_id[model.br_from[k]])}-{int(model.bus_id[model.br_to[k]])}"
+
+
+class ContingencyAnalysis:
+    """The N-1 branch screen of ``Analysis/ContingencyAnalysis.cs`` on the B200 engine."""
+
+    WORSENED_LOADING_MARGIN_PERCENT = 1.0   # :986
+    WORSENED_VOLTAGE_MARGIN_PU = 0.005      # :990
+    BASE_CASE_LABEL = "base case"           # :279
+
+    @staticmethod
+    def screen_raw(model: GridModel, branch_indices: Sequence[int], solver: SparseNewtonRaphsonPowerFlow,
+                   options: PowerFlowOptions, keep_states: bool = False) -> dict:
+        """One ``gs_n1_screen`` call; returns the raw arrays (status, iterations, violation CSR, ...)."""
+        g = solver.grid_for(model)
+        idx = np.ascontiguousarray(branch_indices, dtype=np.int32)
+        k = idx.shape[0]
+        n = model.n_bus
+        # violation capacity: remembered per grid (a too small buffer makes the engine report the size
+        # needed, and the screen is run again)
+        cap = max(256, 16 * k, int(getattr(g, "viol_per_outage", 0) * k * 1.25) + 64)
+        while True:
+            out = dict(status=np.zeros(k, np.int32), iterations=np.zeros(k, np.int32), max_mismatch=np.zeros(k),
+                       min_vm=np.zeros(k), max_vm=np.zeros(k), max_loading_pct=np.zeros(k),
+                       viol_ptr=np.zeros(k + 1, np.int32), viol_kind=np.zeros(cap, np.int32),
+                       viol_element=np.zeros(cap, np.int32), viol_value=np.zeros(cap))
+            if keep_states:
+                out["vm"] = np.zeros(k * n)
+                out["va_deg"] = np.zeros(k * n)
+            r = _abi.N1Result()
+            for key, v in out.items():
+                setattr(r, key, _p(v))
+            r.viol_capacity = cap
+            c = options.to_c()
+            rc = g.ctx.lib.gs_n1_screen(g.handle, k, _p(idx), ctypes.byref(c), ctypes.byref(r))
+            if rc == _abi.GS_ERR_CAPACITY:
+                cap = r.viol_count + 64
+                g.viol_per_outage = max(getattr(g, "viol_per_outage", 0), r.viol_count / max(k, 1))
+                continue
+            g.ctx.check(rc, "gs_n1_screen")
+            break
+        nv = r.viol_count
+        for key in ("viol_kind", "viol_element", "viol_value"):
+            out[key] = out[key][:nv]
+        if keep_states:
+            out["vm"] = out["vm"].reshape(k, n)
+            out["va_deg"] = out["va_deg"].reshape(k, n)
+        out.update(base_status=r.base_status, base_iterations=r.base_iterations, device_ms=r.device_ms,
+                   n_singular_pivot=r.n_singular_pivot, n_batches=r.n_batches, kernel_launches=r.kernel_launches,
+                   newton_iterations=r.newton_iterations, factor_ms=r.factor_ms, solve_ms=r.solve_ms,
+                   mismatch_ms=r.mismatch_ms, other_ms=r.other_ms, factor_bytes=r.factor_bytes)
+        return out
+
+    @classmethod
+    def _results(cls, model: GridModel, idx: Sequence[int], raw: dict) -> list:
+        res = []
+        for j, k in enumerate(idx):
+            st = int(raw["status"][j])
+            label = _branch_label(model, int(k)) if k >= 0 else cls.BASE_CASE_LABEL
+            if st != _abi.PF_CONVERGED:  # NonConverged (:1661-1662); islanding is not screened here
+                res.append(ContingencyResult(label, False, 0.0, 0.0, 0.0, 0.0, ["no solution"], [], st,
+                                             int(raw["iterations"][j]), float(raw["max_mismatch"][j])))
+                continue
+            a, b = raw["viol_ptr"][j], raw["viol_ptr"][j + 1]
+            det = []
+            for q in range(a, b):
+                kind = int(raw["viol_kind"][q])
+                el = int(raw["viol_element"][q])
+                det.append(ContingencyViolation(kind, el, float(raw["viol_value"][q]),
+                                                _branch_name(model, el) if kind == _abi.VIOL_BRANCH_OVERLOAD else ""))
+            res.append(ContingencyResult(label, True, float(raw["max_loading_pct"][j]), 0.0, float(raw["min_vm"][j]),
+                                         float(raw["max_vm"][j]), _violation_texts(model, det), det, st,
+                                         int(raw["iterations"][j]), float(raw["max_mismatch"][j])))
+        return res
+
+    @classmethod
+    def screen_branches(cls, model: GridModel, solver: Optional[SparseNewtonRaphsonPowerFlow] = None,
+                        options: Optional[PowerFlowOptions] = None,
+                        branch_indices: Optional[Sequence[int]] = None) -> list:
+        """ScreenBranches / ScreenBranchesParallel / ScreenBranchesBatched: results in branch order."""
+        solver = solver or SparseNewtonRaphsonPowerFlow()
+        options = options or PowerFlowOptions(precision=solver.precision)
+        idx = model.in_service_branches() if branch_indices is None else np.asarray(branch_indices, np.int32)
+        raw = cls.screen_raw(model, idx, solver, options)
+        return cls._results(model, idx, raw)
+
+    screen_branches_parallel = screen_branches
+    screen_branches_batched = screen_branches
+
+    @classmethod
+    def screen_base_case(cls, model: GridModel, solver: Optional[SparseNewtonRaphsonPowerFlow] = None,
+                         options: Optional[PowerFlowOptions] = None) -> ContingencyResult:
+        """ScreenBaseCase (:958-962): the intact grid through the same classification."""
+        solver = solver or SparseNewtonRaphsonPowerFlow()
+        options = options or PowerFlowOptions(precision=solver.precision)
+        raw = cls.screen_raw(model, np.array([-1], np.int32), solver, options)
+        return cls._results(model, [-1], raw)[0]
+
+    @classmethod
+    def net_against_base(cls, model: GridModel, outage: ContingencyResult, base: ContingencyResult,
+                         count_worsened: bool = False) -> ContingencyResult:
+        """NetAgainstBase (:1000-1034)."""
+        if not base.converged:
+            raise ValueError("Contingency netting: the base case did not converge, so there is no base state to net "
+                             "the outage violations against.")
+        import dataclasses
+        if not outage.converged:
+            return dataclasses.replace(outage, netted_against_base=True)
+        before = {(v.kind, v.element): v.value for v in base.details}
+        fresh, pre, worse = [], [], []
+        for v in outage.details:
+            if (v.kind, v.element) not in before:
+                fresh.append(v)
+                continue
+            b = before[(v.kind, v.element)]
+            if v.kind == _abi.VIOL_UNDERVOLTAGE:
+                w = v.value < b - cls.WORSENED_VOLTAGE_MARGIN_PU
+            elif v.kind == _abi.VIOL_OVERVOLTAGE:
+                w = v.value > b + cls.WORSENED_VOLTAGE_MARGIN_PU
+            else:
+                w = v.value > b + cls.WORSENED_LOADING_MARGIN_PERCENT
+            if w:
+                worse.append(v)
+            (fresh if (w and count_worsened) else pre).append(v)
+        return dataclasses.replace(outage, violations=_violation_texts(model, fresh),
+                                   pre_existing_violations=_violation_texts(model, pre),
+                                   worsened_pre_existing_violations=_violation_texts(model, worse),
+                                   netted_against_base=True)

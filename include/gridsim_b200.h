@@ -124,7 +124,8 @@ typedef struct gs_pf_opts {
     int32_t warm_start_from_base;   /* screens: solve the intact grid first and start every outage from
                                        its solution (GridScenario.WithSolvedVoltages, Simulation/GridScenario.cs:35-52) */
     int32_t batch_width;            /* systems per device batch; 0 = choose from free HBM */
-    int32_t reserved[8];
+    int32_t phase_timing;           /* 1: time each phase with CUDA events (no graph replay) into the result */
+    int32_t reserved[7];
 } gs_pf_opts;
 
 /* Fill `o` with the reference defaults (PowerFlowOptions()) plus precision = FP64. */
@@ -171,6 +172,15 @@ typedef struct gs_n1_result {
     double device_ms;
     int32_t n_singular_pivot;  /* systems whose static pivot failed */
     int32_t n_batches;
+    /* work and phase timing of the screen (phase times only with gs_pf_opts.phase_timing) */
+    int64_t kernel_launches;   /* kernels this call launched */
+    int32_t newton_iterations; /* Newton iterations of the largest batch (device loop trips) */
+    int32_t reserved1;
+    double factor_ms;          /* fused factorisation + forward substitution */
+    double solve_ms;           /* backward substitution (+ the refinement solves in mixed precision) */
+    double mismatch_ms;        /* mismatch + Jacobian fill (+ residual) */
+    double other_ms;           /* status, max |dx|, update */
+    double factor_bytes;       /* algorithmic bytes of the factor phase (J read + L,U written), whole call */
 } gs_n1_result;
 
 /* ---- context -------------------------------------------------------------------------------- */
@@ -205,6 +215,10 @@ typedef struct gs_grid_info {
 } gs_grid_info;
 int gs_grid_info_get(gs_grid *grid, gs_grid_info *info);
 
+/* Host-only: run the symbolic analysis of gs_grid_create without a device and report its sizes.
+ * For planning batch sizes and for tests on machines without a GPU. */
+int gs_analyze_host(const gs_grid_desc *desc, gs_grid_info *info);
+
 /* ---- solves --------------------------------------------------------------------------------- */
 
 /* IPowerFlowSolver.Solve on the intact grid (SparseNewtonRaphsonPowerFlow.Solve :48-54). */
@@ -218,9 +232,9 @@ int gs_pf_solve_batch(gs_grid *grid, int32_t count, const double *load_scale, co
                       double *vm, double *va_deg);
 
 /* ContingencyAnalysis.ScreenBranches / ScreenBranchesParallel / ScreenBranchesBatched: one full
- * Newton solve per outaged branch (indices into the branch arrays; each must be in service), then
- * the ScreenStateCore classification (ContingencyAnalysis.cs:1105-1238) on the device. Results are
- * in the order of `branch_idx`. */
+ * Newton solve per outaged branch (indices into the branch arrays; each must be in service; -1 is
+ * the intact grid, ScreenBaseCase), then the ScreenStateCore classification
+ * (ContingencyAnalysis.cs:1105-1238) on the device. Results are in the order of `branch_idx`. */
 int gs_n1_screen(gs_grid *grid, int32_t n_out, const int32_t *branch_idx, const gs_pf_opts *opts,
                  gs_n1_result *res);
 
