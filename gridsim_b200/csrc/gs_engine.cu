@@ -1503,3 +1503,130 @@ int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts*
 }
 
 }  // extern "C"
+
+// =============================================================================================
+// Allocation-free mismatch evaluation.
+//
+// For callers that may not allocate device memory at the point where they need a mismatch check: a
+// host loop that owns all device memory through its own pool, or code running while a CUDA stream is being
+// captured into a graph (cudaMalloc / cudaFree are not allowed there). They hand in device arrays they
+// already own; the only scratch this entry point needs (one max-norm accumulator and one flag word per
+// system) lives in the file-scope array below, which every GPU that loads this library holds until the
+// process exits. Calls that overlap on the GPU share it and race: issue them one after another.
+namespace gs {
+
+constexpr int kNoAllocMaxSystems = 65536;
+
+// [0, max): max |f| accumulators (bits of a non-negative double); [max, 2 max): non-finite flags (as words)
+static __device__ __align__(256) unsigned long long gNoAllocScratch[2 * kNoAllocMaxSystems];
+
+// Variant of k_mismatch_jac without the Jacobian fill: per (bus, system) the FP64 injections and the
+// mismatch of this bus's equations, reduced to a per-system max |f| in the static scratch. Inputs are
+// system-major ([count][n]); Va in radians; outage[s] removes one branch (or -1).
+__global__ void __launch_bounds__(256) k_mismatch_noalloc(DevGrid g, int count, const double* __restrict__ vm,
+                                                          const double* __restrict__ va, const int* __restrict__ outage,
+                                                          unsigned long long* acc, unsigned long long* bad) {
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int s = blockIdx.y * 32 + lane;
+    const int i = blockIdx.x * 8 + w;
+    double localMax = 0.0;
+    int nonFinite = 0;
+    if (i < g.n && s < count) {
+        const size_t row = (size_t)s * g.n;
+        int o = outage ? outage[s] : -1;
+        if (o >= g.nbr) { o = -1; nonFinite = 1; }  // not a branch of this grid: the result is NaN
+        int c0 = -1, c1 = -1, c2 = -1, c3 = -1;
+        if (o >= 0) { c0 = g.brCell[4 * o]; c1 = g.brCell[4 * o + 1]; c2 = g.brCell[4 * o + 2]; c3 = g.brCell[4 * o + 3]; }
+        const double vmi = vm[row + i], vai = va[row + i];
+        double pi = 0.0, qi = 0.0;
+        for (int p = g.yRowPtr[i]; p < g.yRowPtr[i + 1]; p++) {
+            const int j = g.yCol[p];
+            double G = g.yG[p], Bv = g.yB[p];
+            if (p == c0) { G = g.brRed[8 * o + 0]; Bv = g.brRed[8 * o + 1]; }
+            else if (p == c1) { G = g.brRed[8 * o + 2]; Bv = g.brRed[8 * o + 3]; }
+            else if (p == c2) { G = g.brRed[8 * o + 4]; Bv = g.brRed[8 * o + 5]; }
+            else if (p == c3) { G = g.brRed[8 * o + 6]; Bv = g.brRed[8 * o + 7]; }
+            double sn, cs;
+            sincos(vai - va[row + j], &sn, &cs);
+            const double vmj = vm[row + j];
+            pi += vmj * (G * cs + Bv * sn);
+            qi += vmj * (G * sn - Bv * cs);
+        }
+        const double P = vmi * pi, Q = vmi * qi;
+        if (g.busP[i] >= 0) {
+            const double f = (g.pgen[i] - g.pload[i]) - P;
+            localMax = fmax(localMax, fabs(f));
+            nonFinite |= isfinite(f) ? 0 : 1;
+        }
+        if (g.busQ[i] >= 0) {
+            const double f = (g.qgen[i] - g.qload[i]) - Q;
+            localMax = fmax(localMax, fabs(f));
+            nonFinite |= isfinite(f) ? 0 : 1;
+        }
+    }
+    __shared__ double red[8][32];
+    __shared__ int redBad[8][32];
+    red[w][lane] = localMax;
+    redBad[w][lane] = nonFinite;
+    __syncthreads();
+    if (w == 0 && s < count) {
+        double mx = red[0][lane];
+        int anyBad = redBad[0][lane];
+        for (int q = 1; q < 8; q++) { mx = fmax(mx, red[q][lane]); anyBad |= redBad[q][lane]; }
+        if (mx > 0.0) atomicMaxNonNeg(&acc[s], mx);
+        if (anyBad) atomicOr(&bad[s], 1ull);
+    }
+}
+
+__global__ void k_noalloc_clear(int count, unsigned long long* acc, unsigned long long* bad) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < count) { acc[s] = 0ull; bad[s] = 0ull; }
+}
+
+__global__ void k_noalloc_finish(int count, const unsigned long long* acc, const unsigned long long* bad, double* out) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < count) out[s] = bad[s] ? NAN : __longlong_as_double((long long)acc[s]);
+}
+
+namespace {
+std::mutex gNoAllocMu;
+unsigned long long* gNoAllocPtr[64] = {nullptr};  // device address of gNoAllocScratch, per device ordinal
+}  // namespace
+
+}  // namespace gs
+
+extern "C" int gs_pf_mismatch_noalloc(gs_grid* G, int32_t count, const double* d_vm, const double* d_va,
+                                      const int32_t* d_outage, double* d_max_mismatch) {
+    using namespace gs;
+    if (!G || count < 0 || (count > 0 && (!d_vm || !d_va || !d_max_mismatch))) return GS_ERR_INVALID_ARG;
+    gs_ctx* ctx = G->ctx;
+    if (count > kNoAllocMaxSystems)
+        return SetErr(ctx, GS_ERR_CAPACITY, "gs_pf_mismatch_noalloc: " + std::to_string(count) +
+                                              " systems requested, at most " + std::to_string(kNoAllocMaxSystems));
+    if (count == 0) return GS_OK;
+    if (ctx->device < 0 || ctx->device >= 64) return SetErr(ctx, GS_ERR_INVALID_ARG, "device ordinal out of range");
+    GS_CUDA(cudaSetDevice(ctx->device));
+    unsigned long long* scratch = nullptr;
+    {
+        // once per device, with that device current: the device address of the static scratch array
+        std::lock_guard<std::mutex> lock(gNoAllocMu);
+        if (!gNoAllocPtr[ctx->device]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, gNoAllocScratch);
+            if (e != cudaSuccess)
+                return SetErr(ctx, GS_ERR_CUDA, std::string("cudaGetSymbolAddress(gNoAllocScratch): ") + cudaGetErrorString(e));
+            gNoAllocPtr[ctx->device] = static_cast<unsigned long long*>(p);
+        }
+        scratch = gNoAllocPtr[ctx->device];
+    }
+    unsigned long long* acc = scratch;
+    unsigned long long* bad = scratch + kNoAllocMaxSystems;
+    cudaStream_t st = ctx->stream;
+    k_noalloc_clear<<<(count + 255) / 256, 256, 0, st>>>(count, acc, bad);
+    k_mismatch_noalloc<<<dim3((G->sym.n + 7) / 8, (count + 31) / 32), dim3(32, 8), 0, st>>>(G->view, count, d_vm, d_va,
+                                                                                           d_outage, acc, bad);
+    k_noalloc_finish<<<(count + 255) / 256, 256, 0, st>>>(count, acc, bad, d_max_mismatch);
+    GS_CUDA(cudaGetLastError());
+    GS_CUDA(cudaStreamSynchronize(st));
+    return GS_OK;
+}

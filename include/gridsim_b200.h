@@ -238,6 +238,21 @@ int gs_pf_solve_batch(gs_grid *grid, int32_t count, const double *load_scale, co
 int gs_n1_screen(gs_grid *grid, int32_t n_out, const int32_t *branch_idx, const gs_pf_opts *opts,
                  gs_n1_result *res);
 
+/* ---- allocation-free mismatch check (no counterpart in the reference) ---------------------
+ * For callers that cannot allocate device memory where they need the check: a loop whose device memory all
+ * comes from its own pool, or code running while a stream is captured into a CUDA graph, where cudaMalloc
+ * is not allowed. Computes, for `count` states of the grid, the FP64 max |mismatch| (the quantity the Newton
+ * iteration tests against its tolerance) into d_max_mismatch[count] (NaN for a non-finite mismatch).
+ * d_vm / d_va are the caller's DEVICE arrays, system-major [count][n_bus], angles in radians; d_outage
+ * (device, [count], -1 = none) may be NULL. No device memory is allocated or freed: the only scratch is a
+ * file-scope device array sized for GS_NOALLOC_MAX_SYSTEMS systems (768 KiB, held by every GPU that loads the
+ * library). More systems than that are refused with GS_ERR_CAPACITY. The first call on a device looks up
+ * that array's device address, so make it once before any stream capture. Calls share the array: calls
+ * that overlap on the GPU race, so issue them one after another. Synchronous on the context's stream. */
+#define GS_NOALLOC_MAX_SYSTEMS 65536
+int gs_pf_mismatch_noalloc(gs_grid *grid, int32_t count, const double *d_vm, const double *d_va,
+                           const int32_t *d_outage, double *d_max_mismatch);
+
 #ifdef __cplusplus
 }
 #endif
