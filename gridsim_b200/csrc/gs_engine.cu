@@ -502,6 +502,111 @@ __global__ void __launch_bounds__(256) k_residual(DevGrid g, DevBatch b) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// Few active systems (the last iterations of a batch, when almost every system has converged): one CTA per
+// active system walks the levels itself, its threads taking the entries (nodes) of each level side by side,
+// one dependent round of loads per level and phase. The system's LU is ~1 MB and stays in L2 across the
+// levels; the per-level launches and their warps for 32-system groups are not needed here.
+constexpr int kTailThreads = 1024;
+constexpr int kTailMaxSystems = 128;
+
+__global__ void k_collect_active(DevBatch b) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < b.count && b.active[s]) b.activeList[atomicAdd(b.activeCount, 1)] = s;
+}
+
+// one system, the whole warp: lanes take pairs q0 + lane, q0 + lane + 32, ...; fixed butterfly sum
+template <typename T>
+__device__ __forceinline__ T dotWarp1(const T* __restrict__ lu, const T* __restrict__ rhs, const int2* __restrict__ pr,
+                                      int64_t q0, int64_t q1, size_t B, int s) {
+    T acc = T(0);
+    for (int64_t q = q0 + (threadIdx.x & 31); q < q1; q += 32) {
+        const int2 a = __ldg(pr + q);
+        acc += lu[a.x * B + s] * rhs[a.y * B + s];
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    return acc;
+}
+
+// The few-systems path's wide pieces: one system, one warp.
+template <typename T>
+__device__ __forceinline__ void factorEntryWarp1(const DevGrid& g, const DevBatch& b, int e, int s) {
+    const size_t B = (size_t)b.B;
+    T* lu = (T*)b.lu;
+    T* y = (T*)b.y;
+    const int kind = g.entKind[e], slot = g.entSlot[e], node = g.entNode[e];
+    const T dot = dotWarp1<T>(lu, kind == kFwd ? y : lu, g.pairs, g.entPairPtr[e], g.entPairPtr[e + 1], B, s);
+    if ((threadIdx.x & 31) != 0) return;
+    if (kind == kFwd) { y[slot * B + s] -= dot; return; }
+    const T a = g.entHasA[e] ? lu[slot * B + s] : T(0);
+    T v = a - dot;
+    if (kind == kDiag) {
+        const T fl = pivotFloor<T>() * (fabs(a) > T(1) ? fabs(a) : T(1));
+        if (!(fabs(v) > fl)) { atomicOr(&b.flags[s], kFlagPivotPerturbed); v = (v < T(0)) ? -fl : fl; }
+        ((T*)b.piv)[node * B + s] = v;
+        return;
+    }
+    if (kind == kLower) v = v / ((const T*)b.piv)[node * B + s];
+    lu[slot * B + s] = v;
+}
+
+template <typename T>
+__device__ __forceinline__ void backwardNodeWarp1(const DevGrid& g, const DevBatch& b, T* y, int q, int s) {
+    const size_t B = (size_t)b.B;
+    const T* lu = (const T*)b.lu;
+    const int k = g.levelNodes[q];
+    const int64_t base = g.luBase[k];
+    const int c = g.luCnt[k];
+    const int* rows = g.pRows + g.pRowPtr[k];
+    T acc = T(0);
+    for (int t = threadIdx.x & 31; t < c; t += 32) acc += lu[(base + 1 + t) * B + s] * y[__ldg(rows + t) * B + s];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) y[k * B + s] = (y[k * B + s] - acc) / ((const T*)b.piv)[k * B + s];
+}
+
+template <typename T>
+__device__ __forceinline__ void forwardEntryWarp1(const DevGrid& g, const DevBatch& b, T* v, int e, int s) {
+    const size_t B = (size_t)b.B;
+    const int k = g.entNode[e];
+    const T dot = dotWarp1<T>((const T*)b.lu, v, g.pairs, g.entPairPtr[e], g.entPairPtr[e + 1], B, s);
+    if ((threadIdx.x & 31) == 0) v[k * B + s] -= dot;
+}
+
+template <typename T, int W>
+__global__ void __launch_bounds__(kTailThreads) k_tail(DevGrid g, DevBatch b, T* vec) {
+    const int s = b.activeList[blockIdx.x];
+    if (W != kWorkFactor && vec != (T*)b.y && !b.refine[s]) return;  // uniform across the block
+    const int* ptr = W == kWorkFactor ? g.fWorkPtr : (W == kWorkBackward ? g.bWorkPtr : g.vWorkPtr);
+    const int* work = W == kWorkFactor ? g.fWork : (W == kWorkBackward ? g.bWork : g.vWork);
+    const int* wide = W == kWorkFactor ? g.fWide : (W == kWorkBackward ? g.bWide : g.vWide);
+    const int phases = W == kWorkFactor ? 2 : 1;
+    const int warp = threadIdx.x >> 5;
+    for (int step = 0; step < b.nLevels; step++) {
+        const int l = W == kWorkBackward ? b.nLevels - 1 - step : step;
+        for (int ph = 0; ph < phases; ph++) {
+            const int i = phases * l + ph;
+            const int w0 = ptr[i], w1 = ptr[i + 1], nw = wide[i];
+            // wide pieces (the first nw of the range): a warp each
+            for (int w = w0 + warp; w < w0 + nw; w += kTailThreads / 32) {
+                const int x = __ldg(work + w);
+                if (W == kWorkFactor) factorEntryWarp1<T>(g, b, x, s);
+                else if (W == kWorkBackward) backwardNodeWarp1<T>(g, b, vec, x, s);
+                else forwardEntryWarp1<T>(g, b, vec, x, s);
+            }
+            // short pieces: a thread each
+            for (int w = w0 + nw + threadIdx.x; w < w1; w += kTailThreads) {
+                const int x = __ldg(work + w);
+                if (W == kWorkFactor) factorEntry<T>(g, b, x, s, true, false);
+                else if (W == kWorkBackward) backwardNode<T>(g, b, vec, x, s, false);
+                else forwardEntry<T>(g, b, vec, x, s, false);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // 5. max |dx| per system, then the damped update.
 template <typename T>
 __global__ void __launch_bounds__(256) k_dxmax(DevGrid g, DevBatch b, int rowsPerBlock, int refine) {
@@ -738,6 +843,7 @@ struct DevBuf {
 struct Workspace {
     int B = 0;
     int precision = -1;
+    DevBuf activeList;
     DevBuf vm, va, lu, piv, y, z, rhs64, refine, maxMis, maxDx, startMis, finalMis, status, iters, convIters, convAt, active, flags, outage,
         loadScale, activeCount;
     DevBuf code, value, maxLoad, minVmNeg, maxVmB, chunkCount, chunkOffset, outKind, outElem, outVal, pq;
@@ -828,9 +934,11 @@ int UploadGrid(gs_grid* G) {
     UP(s.factor.work, fWork); UP(s.factor.items, fItems); UP(s.factor.levelItemPtr, fLevelPtr);
     UP(s.backward.work, bWork); UP(s.backward.items, bItems); UP(s.backward.levelItemPtr, bLevelPtr);
     UP(s.forward.work, vWork); UP(s.forward.items, vItems); UP(s.forward.levelItemPtr, vLevelPtr);
+    UP(s.factor.levelWorkPtr, fWorkPtr); UP(s.backward.levelWorkPtr, bWorkPtr); UP(s.forward.levelWorkPtr, vWorkPtr);
+    UP(s.factor.levelWide, fWide); UP(s.backward.levelWide, bWide); UP(s.forward.levelWide, vWide);
 #undef UP
     // the persistent kernels take every level from the first one whose items (and those of all levels above
-    // it) fit twice in a CTA's warps in each phase
+    // it) fit twice in a CTA's warps in each phase; the wide levels below run one launch per level and phase
     G->split = s.nLevels;
     for (int l = s.nLevels - 1; l >= 0; l--) {
         const auto& fp = s.factor.levelItemPtr;
@@ -869,6 +977,7 @@ int EnsureWorkspace(gs_grid* G, int B, int precision, bool classify, bool loadSc
     GS_CUDA(w.status.alloc(Bz * 4)); GS_CUDA(w.iters.alloc(Bz * 4)); GS_CUDA(w.active.alloc(Bz * 4));
     GS_CUDA(w.convIters.alloc(Bz * 4)); GS_CUDA(w.convAt.alloc(Bz * 4));
     GS_CUDA(w.flags.alloc(Bz * 4)); GS_CUDA(w.outage.alloc(Bz * 4)); GS_CUDA(w.activeCount.alloc(16));
+    GS_CUDA(w.activeList.alloc(Bz * 4));
     GS_CUDA(w.startVm.alloc(s.n * 8)); GS_CUDA(w.startVa.alloc(s.n * 8));
     if (loadScale) GS_CUDA(w.loadScale.alloc(s.n * Bz * 8));
     if (classify) {
@@ -898,6 +1007,8 @@ DevBatch MakeBatch(gs_grid* G, int count, bool useScale) {
     b.flags = w.flags.as<int>(); b.outage = w.outage.as<int>();
     b.loadScale = useScale ? w.loadScale.as<double>() : nullptr;
     b.activeCount = w.activeCount.as<int>();
+    b.activeList = w.activeList.as<int>();
+    b.nLevels = G->sym.nLevels;
     return b;
 }
 
@@ -1017,6 +1128,40 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
         if (timed) { float t; cudaEventElapsedTime(&t, ev[0], ev[1]); mMs += t; }
         if (*ctx->pinnedCount == 0) break;
         iterations++;
+        const int nActive = *ctx->pinnedCount;
+        if (nActive <= kTailMaxSystems) {
+            // few systems left: one CTA per active system (k_tail), no per-level launches
+            if (timed) cudaEventRecord(ev[1], st);
+            cudaMemsetAsync(b.activeCount, 0, sizeof(int), st);
+            k_collect_active<<<(count + 255) / 256, 256, 0, st>>>(b);
+            k_tail<T, kWorkFactor><<<nActive, kTailThreads, 0, st>>>(g, b, (T*)b.y);
+            if (timed) cudaEventRecord(ev[2], st);
+            k_tail<T, kWorkBackward><<<nActive, kTailThreads, 0, st>>>(g, b, (T*)b.y);
+            launches += 4;
+            if (refine) {
+                k_residual<T><<<dim3((s.n + 7) / 8, groups), blk8, 0, st>>>(g, b);
+                k_tail<T, kWorkForward><<<nActive, kTailThreads, 0, st>>>(g, b, (T*)b.z);
+                k_tail<T, kWorkBackward><<<nActive, kTailThreads, 0, st>>>(g, b, (T*)b.z);
+                launches += 3;
+            }
+            if (timed) cudaEventRecord(ev[3], st);
+            updatePhase();
+            launches += 2;
+            if (timed) {
+                cudaEventRecord(ev[4], st);
+                ce = cudaEventSynchronize(ev[4]);
+                if (ce != cudaSuccess) { rc = SetErr(ctx, GS_ERR_CUDA, std::string("newton: ") + cudaGetErrorString(ce)); break; }
+                float t1, t2, t3;
+                cudaEventElapsedTime(&t1, ev[1], ev[2]);
+                cudaEventElapsedTime(&t2, ev[2], ev[3]);
+                cudaEventElapsedTime(&t3, ev[3], ev[4]);
+                fMs += t1; sMs += t2; oMs += t3;
+                if (traceIters)
+                    std::fprintf(stderr, "gs: iteration %d active %d (few-systems path) factor %.3f ms solve %.3f ms update %.3f ms\n",
+                                 iter, nActive, t1, t2, t3);
+            }
+            continue;
+        }
         if (!timed) {
             ce = cudaGraphLaunch(exec, st);
             launches += launchesPerStep;

@@ -77,6 +77,8 @@ struct Symbolic {
         std::vector<int32_t> work;
         std::vector<int32_t> items;        // 2 per item
         std::vector<int32_t> levelItemPtr;
+        std::vector<int32_t> levelWorkPtr; // the work of a level (phase) is work[levelWorkPtr[i] .. [i+1])
+        std::vector<int32_t> levelWide;    // how many of a level (phase)'s first items are wide (one piece each)
     };
     Schedule factor, backward, forward;
 };

@@ -62,6 +62,12 @@ struct DevGrid {
     const int* vWork;
     const int* vItems;
     const int* vLevelPtr;
+    const int* fWorkPtr;  // per level (and phase for the factorisation): work range
+    const int* bWorkPtr;
+    const int* vWorkPtr;
+    const int* fWide;     // per level (phase): leading wide items
+    const int* bWide;
+    const int* vWide;
     const int64_t* luBase;
     const int* luCnt;
     const int* pRowPtr;
@@ -71,6 +77,7 @@ struct DevGrid {
 struct DevBatch {
     int B;                  // interleave stride (multiple of 32)
     int count;              // live systems
+    int nLevels;            // elimination-tree levels of the grid
     double* vm;             // [n][B]
     double* va;             // [n][B]
     void* lu;               // [nnzLU][B] of the LU type (diagonal slots keep A(k, k))
@@ -92,6 +99,7 @@ struct DevBatch {
     const int* outage;      // [B] branch index or -1
     const double* loadScale;  // [n][B] or null
     int* activeCount;       // [1]
+    int* activeList;        // [B] systems still stepping (filled for the few-systems path)
 };
 
 }  // namespace gs

@@ -363,11 +363,13 @@ std::string Analyze(const HostGrid& g, Symbolic& s) {
     const int kShort = 32, kPack = 8;
     auto pack = [&](Symbolic::Schedule& sc, const std::vector<int32_t>& list, const std::vector<int64_t>& len) {
         std::vector<int32_t> shortOnes;
+        int wide = 0;
         for (size_t q = 0; q < list.size(); q++) {
             if (len[q] > kShort) {
                 sc.work.push_back(list[q]);
                 sc.items.push_back((int32_t)sc.work.size() - 1);
                 sc.items.push_back(-1);
+                wide++;
             } else {
                 shortOnes.push_back(list[q]);
             }
@@ -379,10 +381,13 @@ std::string Analyze(const HostGrid& g, Symbolic& s) {
             for (int t = 0; t < cnt; t++) sc.work.push_back(shortOnes[q + t]);
         }
         sc.levelItemPtr.push_back((int32_t)sc.items.size() / 2);
+        sc.levelWorkPtr.push_back((int32_t)sc.work.size());
+        sc.levelWide.push_back(wide);
     };
-    s.factor.levelItemPtr.assign(1, 0);
-    s.backward.levelItemPtr.assign(1, 0);
-    s.forward.levelItemPtr.assign(1, 0);
+    for (Symbolic::Schedule* sc : {&s.factor, &s.backward, &s.forward}) {
+        sc->levelItemPtr.assign(1, 0);
+        sc->levelWorkPtr.assign(1, 0);
+    }
     for (int l = 0; l < s.nLevels; l++) {
         std::vector<int32_t> phaseA, phaseB, bwd, fwd;
         std::vector<int64_t> lenA, lenB, lenBwd, lenFwd;
