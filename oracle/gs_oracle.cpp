@@ -1006,8 +1006,9 @@ int gso_n1_screen(const gs_grid_desc* d, int32_t nOut, const int32_t* idx, const
                   gs_n1_result* res) {
     if (!d || !res || !OptionsSupported(opt) || nOut < 0) return GS_ERR_INVALID_ARG;
     Model m = FromDesc(d);
-    for (int k = 0; k < nOut; k++)
-        if (idx[k] < 0 || idx[k] >= (int)m.br.size() || !m.br[idx[k]].inService) return GS_ERR_INVALID_ARG;
+    for (int k = 0; k < nOut; k++)  // -1 is the intact grid (ScreenBaseCase)
+        if (idx[k] < -1 || idx[k] >= (int)m.br.size() || (idx[k] >= 0 && !m.br[idx[k]].inService))
+            return GS_ERR_INVALID_ARG;
     std::vector<double> vm0, va0;
     res->base_status = GS_PF_NOT_RUN;
     res->base_iterations = 0;

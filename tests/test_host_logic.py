@@ -1,0 +1,75 @@
+"""Host-side logic on CPU: netting against the base case, violation texts, option mapping, sharding."""
+import numpy as np
+
+import oracle
+from gridsim_b200 import _abi, synthetic
+from gridsim_b200.engine import ContingencyAnalysis, PowerFlowOptions
+from gridsim_b200.parallel import merge, shard
+from tests.conftest import golden_model
+
+
+def _study():
+    o = _abi.default_opts()
+    o.max_iterations = 100
+    o.enforce_q_limits = 1
+    return o
+
+
+def test_case14_netting_pins():
+    """ContingencyCorrectnessTests.cs:209-237: base overvoltage 1.090 on buses 6, 7, 8; netted 16 / 3 / 1."""
+    m, _ = golden_model("case14")
+    o = _study()
+    base = ContingencyAnalysis._results(m, [-1], oracle.screen(m, np.array([-1], np.int32), o))[0]
+    assert base.violations == ["overvoltage 1.090 p.u."]
+    assert [d.element for d in base.details] == [6, 7, 8]
+    assert abs(base.details[0].value - 1.07) < 1e-12
+    idx = m.in_service_branches()
+    raw = ContingencyAnalysis._results(m, idx, oracle.screen(m, idx, o))
+    net = [ContingencyAnalysis.net_against_base(m, r, base) for r in raw]
+    assert sum(r.secure for r in net) == 16
+    assert sum(r.converged and not r.secure for r in net) == 3
+    assert sum(not r.converged for r in net) == 1
+    for r in net:
+        if r.converged:
+            assert "overvoltage 1.090 p.u." in r.pre_existing_violations
+
+
+def test_violation_texts_follow_the_reference_format():
+    from gridsim_b200.engine import ContingencyViolation, _violation_texts
+    m, _ = golden_model("case14")
+    det = [ContingencyViolation(_abi.VIOL_BRANCH_OVERLOAD, 0, 104.4, "1-2"),
+           ContingencyViolation(_abi.VIOL_UNDERVOLTAGE, 5, 0.93412, ""),
+           ContingencyViolation(_abi.VIOL_UNDERVOLTAGE, 6, 0.9312, ""),
+           ContingencyViolation(_abi.VIOL_OVERVOLTAGE, 8, 1.0901, "")]
+    assert _violation_texts(m, det) == ["branch 1-2 104%", "undervoltage 0.931 p.u.", "overvoltage 1.090 p.u."]
+
+
+def test_options_map_onto_the_c_struct():
+    c = PowerFlowOptions(tolerance=1e-9, max_iterations=7, precision="mixed", warm_start_from_base=True,
+                         per_bus_voltage_limits=True, batch_width=64).to_c()
+    assert (c.tolerance, c.max_iterations, c.precision, c.warm_start_from_base, c.per_bus_voltage_limits,
+            c.batch_width) == (1e-9, 7, _abi.PREC_MIXED, 1, 1, 64)
+
+
+def test_shards_cover_every_outage_once():
+    for n in (0, 1, 7, 100, 101):
+        for world in (1, 2, 3, 8):
+            covered = []
+            for r in range(world):
+                covered.extend(range(n)[shard(n, r, world)])
+            assert covered == list(range(n))
+
+
+def test_merged_shards_equal_one_screen():
+    m = synthetic.config_grid(0, 0)
+    idx = synthetic.outage_set(m, None, 0)[:30]
+    o = _abi.default_opts()
+    o.max_iterations = 20
+    o.per_bus_voltage_limits = 1
+    o.warm_start_from_base = 1
+    whole = oracle.screen(m, idx, o)
+    parts = [oracle.screen(m, idx[shard(len(idx), r, 3)], o) for r in range(3)]
+    got = merge(parts)
+    for k in ("status", "iterations", "viol_ptr", "viol_kind", "viol_element"):
+        assert np.array_equal(got[k], whole[k]), k
+    assert np.array_equal(got["viol_value"], whole["viol_value"])
