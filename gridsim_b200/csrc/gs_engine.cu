@@ -46,17 +46,25 @@ __device__ __forceinline__ void atomicMaxNonNeg(unsigned long long* a, double v)
     atomicMax(a, (unsigned long long)__double_as_longlong(v));
 }
 
+// The system of batch position `idx`: the position itself, or (few-systems path) the idx-th listed system;
+// -1 past the end of the list.
+__device__ __forceinline__ int sysAt(int idx, const int* list, int nList) {
+    if (!list) return idx;
+    return idx < nList ? list[idx] : -1;
+}
+
 // ---------------------------------------------------------------------------------------------
 // 1. mismatch + Jacobian fill. Block (32, 8): lane = system, y = bus within the block.
 template <typename T>
-__global__ void __launch_bounds__(256) k_mismatch_jac(DevGrid g, DevBatch b, int fillJac, double* pOut, double* qOut) {
+__global__ void __launch_bounds__(256) k_mismatch_jac(DevGrid g, DevBatch b, int fillJac, double* pOut, double* qOut,
+                                                      const int* list, int nList) {
     const int lane = threadIdx.x, w = threadIdx.y;
-    const int s = blockIdx.y * 32 + lane;
+    const int s = sysAt(blockIdx.y * 32 + lane, list, nList);
     const int i = blockIdx.x * 8 + w;
     const size_t B = (size_t)b.B;
     double localMax = 0.0;
     int bad = 0;  // 1: mismatch not finite, 2: Jacobian not finite
-    const bool live = i < g.n && s < b.count && b.active[s];
+    const bool live = i < g.n && s >= 0 && s < b.count && b.active[s];
     if (live) {
         const int o = b.outage[s];
         int c0 = -1, c1 = -1, c2 = -1, c3 = -1;
@@ -136,7 +144,7 @@ __global__ void __launch_bounds__(256) k_mismatch_jac(DevGrid g, DevBatch b, int
     red[w][lane] = localMax;
     redBad[w][lane] = bad;
     __syncthreads();
-    if (w == 0 && s < b.count) {
+    if (w == 0 && s >= 0 && s < b.count) {
         double mx = red[0][lane];
         int anyBad = redBad[0][lane];
         for (int q = 1; q < 8; q++) { mx = fmax(mx, red[q][lane]); anyBad |= redBad[q][lane]; }
@@ -433,11 +441,11 @@ __global__ void __launch_bounds__(32 * kPersistWarps) k_persistent(DevGrid g, De
 // (the same H/N/M/L expressions as the fill). The correction solve of r with the same FP32 factors makes the
 // step accurate to ~(kappa * 2^-24)^2, so the Newton path follows the FP64 path and stops where it stops.
 template <typename T>
-__global__ void __launch_bounds__(256) k_residual(DevGrid g, DevBatch b) {
+__global__ void __launch_bounds__(256) k_residual(DevGrid g, DevBatch b, const int* list, int nList) {
     const int lane = threadIdx.x, w = threadIdx.y;
-    const int s = blockIdx.y * 32 + lane;
+    const int s = sysAt(blockIdx.y * 32 + lane, list, nList);
     const int i = blockIdx.x * 8 + w;
-    if (i >= g.n || s >= b.count || !b.active[s]) return;
+    if (i >= g.n || s < 0 || s >= b.count || !b.active[s]) return;
     const size_t B = (size_t)b.B;
     const int kp = g.busP[i], kq = g.busQ[i];
     if (kp < 0 && kq < 0) return;
@@ -609,16 +617,17 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(DevGrid g, DevBatch b, T*
 // ---------------------------------------------------------------------------------------------
 // 5. max |dx| per system, then the damped update.
 template <typename T>
-__global__ void __launch_bounds__(256) k_dxmax(DevGrid g, DevBatch b, int rowsPerBlock, int refine) {
+__global__ void __launch_bounds__(256) k_dxmax(DevGrid g, DevBatch b, int rowsPerBlock, int refine, const int* list,
+                                               int nList) {
     const int lane = threadIdx.x, w = threadIdx.y;
-    const int s = blockIdx.y * 32 + lane;
+    const int s = sysAt(blockIdx.y * 32 + lane, list, nList);
     const size_t B = (size_t)b.B;
     const T* y = (const T*)b.y;
     const T* z = (const T*)b.z;
     const int r0 = blockIdx.x * rowsPerBlock, r1 = min(g.m, r0 + rowsPerBlock);
     double mx = 0.0;
     bool bad = false;
-    if (s < b.count && b.active[s]) {
+    if (s >= 0 && s < b.count && b.active[s]) {
         for (int k = r0 + w; k < r1; k += 8) {
             const double v = (double)y[k * B + s] + (refine && b.refine[s] ? (double)z[k * B + s] : 0.0);
             bad |= !isfinite(v);
@@ -630,7 +639,7 @@ __global__ void __launch_bounds__(256) k_dxmax(DevGrid g, DevBatch b, int rowsPe
     red[w][lane] = mx;
     redBad[w][lane] = bad;
     __syncthreads();
-    if (w == 0 && s < b.count) {
+    if (w == 0 && s >= 0 && s < b.count) {
         double m = red[0][lane];
         int anyBad = redBad[0][lane];
         for (int q = 1; q < 8; q++) { m = fmax(m, red[q][lane]); anyBad |= redBad[q][lane]; }
@@ -640,11 +649,11 @@ __global__ void __launch_bounds__(256) k_dxmax(DevGrid g, DevBatch b, int rowsPe
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_update(DevGrid g, DevBatch b, int refine) {
+__global__ void __launch_bounds__(256) k_update(DevGrid g, DevBatch b, int refine, const int* list, int nList) {
     const int lane = threadIdx.x;
-    const int s = blockIdx.y * 32 + lane;
+    const int s = sysAt(blockIdx.y * 32 + lane, list, nList);
     const int i = blockIdx.x * 8 + threadIdx.y;
-    if (i >= g.n || s >= b.count || !b.active[s]) return;
+    if (i >= g.n || s < 0 || s >= b.count || !b.active[s]) return;
     if (b.flags[s] & kFlagStepBad) return;
     const size_t B = (size_t)b.B;
     const T* y = (const T*)b.y;
@@ -1076,7 +1085,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
     auto solvePhase = [&]() {
         backward((T*)b.y);
         if (refine) {
-            k_residual<T><<<dim3((s.n + 7) / 8, groups), blk8, 0, st>>>(g, b);
+            k_residual<T><<<dim3((s.n + 7) / 8, groups), blk8, 0, st>>>(g, b, nullptr, 0);
             stepLaunches++;
             for (int l = 0; l < split; l++) launchLevel(k_level<T, kWorkForward>, (T*)b.z, vp[l], vp[l + 1]);
             if (split < s.nLevels) {
@@ -1087,9 +1096,10 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
         }
     };
     const int rowsPerBlock = 512;
-    auto updatePhase = [&]() {
-        k_dxmax<T><<<dim3((s.m + rowsPerBlock - 1) / rowsPerBlock, groups), blk8, 0, st>>>(g, b, rowsPerBlock, refine);
-        k_update<T><<<dim3((s.n + 7) / 8, groups), blk8, 0, st>>>(g, b, refine);
+    auto updatePhase = [&](const int* list, int nList) {
+        const int grp = list ? (nList + 31) / 32 : groups;
+        k_dxmax<T><<<dim3((s.m + rowsPerBlock - 1) / rowsPerBlock, grp), blk8, 0, st>>>(g, b, rowsPerBlock, refine, list, nList);
+        k_update<T><<<dim3((s.n + 7) / 8, grp), blk8, 0, st>>>(g, b, refine, list, nList);
         stepLaunches += 2;
     };
     cudaGraph_t graph;
@@ -1099,7 +1109,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
         GS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         factorPhase();
         solvePhase();
-        updatePhase();
+        updatePhase(nullptr, 0);
         ce = cudaStreamEndCapture(st, &graph);
         if (ce != cudaSuccess) return SetErr(ctx, GS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
         ce = cudaGraphInstantiate(&exec, graph, 0);
@@ -1115,9 +1125,14 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
     int iterations = 0;
     double fMs = 0, sMs = 0, mMs = 0, oMs = 0;
     int rc = GS_OK;
+    int listCount = 0;  // > 0: b.activeList holds the systems of the previous few-systems iteration
     for (int iter = 0; iter <= o.max_iterations + 4; iter++) {
         if (timed) cudaEventRecord(ev[0], st);
-        k_mismatch_jac<T><<<dim3((s.n + 7) / 8, groups), blk8, 0, st>>>(g, b, 1, nullptr, nullptr);
+        if (listCount > 0)
+            k_mismatch_jac<T><<<dim3((s.n + 7) / 8, (listCount + 31) / 32), blk8, 0, st>>>(g, b, 1, nullptr, nullptr,
+                                                                                         b.activeList, listCount);
+        else
+            k_mismatch_jac<T><<<dim3((s.n + 7) / 8, groups), blk8, 0, st>>>(g, b, 1, nullptr, nullptr, nullptr, 0);
         if (timed) cudaEventRecord(ev[1], st);
         cudaMemsetAsync(b.activeCount, 0, sizeof(int), st);
         k_status<<<(count + 255) / 256, 256, 0, st>>>(b, iter, o.tolerance, o.diverge_limit_pu, o.max_iterations, 0);
@@ -1139,13 +1154,14 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             k_tail<T, kWorkBackward><<<nActive, kTailThreads, 0, st>>>(g, b, (T*)b.y);
             launches += 4;
             if (refine) {
-                k_residual<T><<<dim3((s.n + 7) / 8, groups), blk8, 0, st>>>(g, b);
+                k_residual<T><<<dim3((s.n + 7) / 8, (nActive + 31) / 32), blk8, 0, st>>>(g, b, b.activeList, nActive);
                 k_tail<T, kWorkForward><<<nActive, kTailThreads, 0, st>>>(g, b, (T*)b.z);
                 k_tail<T, kWorkBackward><<<nActive, kTailThreads, 0, st>>>(g, b, (T*)b.z);
                 launches += 3;
             }
             if (timed) cudaEventRecord(ev[3], st);
-            updatePhase();
+            updatePhase(b.activeList, nActive);
+            listCount = nActive;
             launches += 2;
             if (timed) {
                 cudaEventRecord(ev[4], st);
@@ -1173,7 +1189,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             cudaEventRecord(ev[2], st);
             solvePhase();
             cudaEventRecord(ev[3], st);
-            updatePhase();
+            updatePhase(nullptr, 0);
             cudaEventRecord(ev[4], st);
             launches += stepLaunches;
             ce = cudaEventSynchronize(ev[4]);
@@ -1393,9 +1409,9 @@ int gs_pf_solve(gs_grid* G, const gs_pf_opts* opts, gs_pf_result* res) {
         double* P = G->ws.pq.as<double>();
         double* Q = P + (size_t)n * B;
         if (o.precision == GS_PREC_MIXED)
-            k_mismatch_jac<float><<<dim3((n + 7) / 8, B / 32), dim3(32, 8), 0, ctx->stream>>>(G->view, b, 0, P, Q);
+            k_mismatch_jac<float><<<dim3((n + 7) / 8, B / 32), dim3(32, 8), 0, ctx->stream>>>(G->view, b, 0, P, Q, nullptr, 0);
         else
-            k_mismatch_jac<double><<<dim3((n + 7) / 8, B / 32), dim3(32, 8), 0, ctx->stream>>>(G->view, b, 0, P, Q);
+            k_mismatch_jac<double><<<dim3((n + 7) / 8, B / 32), dim3(32, 8), 0, ctx->stream>>>(G->view, b, 0, P, Q, nullptr, 0);
         GS_CUDA(cudaStreamSynchronize(ctx->stream));
         std::vector<double> p(n), q(n);
         GS_CUDA(cudaMemcpy2D(p.data(), 8, P, B * 8, 8, n, cudaMemcpyDeviceToHost));
