@@ -203,7 +203,11 @@ __global__ void k_status(DevBatch b, int iter, double tol, double divLimit, int 
     if (fl & kFlagJacBad) { b.status[s] = GS_PF_MAX_ITERATIONS; b.active[s] = 0; return; }  // SolveStep refuses it
     // Mixed precision refines the FP32 step with the FP64 residual once the mismatch is small: far from the
     // root the Newton step is self-correcting and an FP32 step error of ~kappa * 2^-24 changes nothing.
-    if (b.refine) b.refine[s] = mis < kRefineBelowPu ? 1 : 0;
+    if (b.refine) {
+        const int r = mis < kRefineBelowPu ? 1 : 0;
+        b.refine[s] = r;
+        if (r) atomicAdd(b.activeCount + 1, 1);
+    }
     atomicAdd(b.activeCount, 1);
 }
 
@@ -515,21 +519,72 @@ __global__ void __launch_bounds__(256) k_residual(DevGrid g, DevBatch b, const i
 // one dependent round of loads per level and phase. The system's LU is ~1 MB and stays in L2 across the
 // levels; the per-level launches and their warps for 32-system groups are not needed here.
 constexpr int kTailThreads = 1024;
-constexpr int kTailMaxSystems = 128;
+constexpr int kTailMaxSystems = 148;  // one wave of k_tail CTAs (one 1024-thread CTA per SM)
+constexpr int kCompactCap = 160;      // systems the compact workspace holds (kTailMaxSystems rounded up to 32)
 
 __global__ void k_collect_active(DevBatch b) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < b.count && b.active[s]) b.activeList[atomicAdd(b.activeCount, 1)] = s;
 }
 
-// one system, the whole warp: lanes take pairs q0 + lane, q0 + lane + 32, ...; fixed butterfly sum
+// Compaction of the few systems still stepping. Their state (voltages, load scalings, Newton control) moves
+// into a workspace whose interleave stride is the number of systems rounded up to 32, so that a system's
+// LU, right-hand sides and voltages span tens of MB instead of GB: the dependent loads of the level walk
+// then hit L2. Everything else a step needs (Jacobian, LU, right-hand sides) is rebuilt from the state
+// each iteration. Grid (ceil(n / 8), ceil(count / 32)), block (32, 8); position c of the compact batch
+// holds system origin[c] of the full batch.
+__device__ __forceinline__ void moveSystem(const DevBatch& from, int sf, const DevBatch& to, int st, int i, int n) {
+    const size_t Bf = (size_t)from.B, Bt = (size_t)to.B;
+    to.vm[i * Bt + st] = from.vm[i * Bf + sf];
+    to.va[i * Bt + st] = from.va[i * Bf + sf];
+    if (from.loadScale && to.loadScale) const_cast<double*>(to.loadScale)[i * Bt + st] = from.loadScale[i * Bf + sf];
+    if (i != 0) return;
+    to.maxMis[st] = from.maxMis[sf];
+    to.maxDx[st] = from.maxDx[sf];
+    to.startMis[st] = from.startMis[sf];
+    to.finalMis[st] = from.finalMis[sf];
+    to.status[st] = from.status[sf];
+    to.iters[st] = from.iters[sf];
+    to.convIters[st] = from.convIters[sf];
+    to.convAt[st] = from.convAt[sf];
+    to.active[st] = from.active[sf];
+    to.flags[st] = from.flags[sf];
+    const_cast<int*>(to.outage)[st] = from.outage[sf];
+    if (from.refine && to.refine) to.refine[st] = from.refine[sf];
+}
+
+__global__ void k_gather(DevBatch full, DevBatch compact, const int* origin, int n) {
+    const int c = blockIdx.y * 32 + threadIdx.x, i = blockIdx.x * 8 + threadIdx.y;
+    if (c >= compact.count || i >= n) return;
+    moveSystem(full, origin[c], compact, c, i, n);
+}
+
+__global__ void k_scatter(DevBatch compact, DevBatch full, const int* origin, int n) {
+    const int c = blockIdx.y * 32 + threadIdx.x, i = blockIdx.x * 8 + threadIdx.y;
+    if (c >= compact.count || i >= n) return;
+    moveSystem(compact, c, full, origin[c], i, n);
+}
+
+// one system, the whole warp: lanes take pairs q0 + lane, q0 + lane + 32, ...; four pairs per lane are
+// in flight at once (their index loads, then their eight value loads), then a fixed butterfly sum
 template <typename T>
 __device__ __forceinline__ T dotWarp1(const T* __restrict__ lu, const T* __restrict__ rhs, const int2* __restrict__ pr,
                                       int64_t q0, int64_t q1, size_t B, int s) {
+    constexpr int U = 4;
     T acc = T(0);
-    for (int64_t q = q0 + (threadIdx.x & 31); q < q1; q += 32) {
-        const int2 a = __ldg(pr + q);
-        acc += lu[a.x * B + s] * rhs[a.y * B + s];
+    for (int64_t q = q0 + (threadIdx.x & 31); q < q1; q += 32 * U) {
+        int2 a[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) a[u] = q + 32 * u < q1 ? __ldg(pr + q + 32 * u) : make_int2(-1, -1);
+        T l[U], r[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const bool ok = a[u].x >= 0;
+            l[u] = ok ? lu[a[u].x * B + s] : T(0);
+            r[u] = ok ? rhs[a[u].y * B + s] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) acc += l[u] * r[u];
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
@@ -566,8 +621,22 @@ __device__ __forceinline__ void backwardNodeWarp1(const DevGrid& g, const DevBat
     const int64_t base = g.luBase[k];
     const int c = g.luCnt[k];
     const int* rows = g.pRows + g.pRowPtr[k];
+    constexpr int U = 4;
     T acc = T(0);
-    for (int t = threadIdx.x & 31; t < c; t += 32) acc += lu[(base + 1 + t) * B + s] * y[__ldg(rows + t) * B + s];
+    for (int t = threadIdx.x & 31; t < c; t += 32 * U) {
+        int r[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) r[u] = t + 32 * u < c ? __ldg(rows + t + 32 * u) : -1;
+        T uu[U], x[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const bool ok = r[u] >= 0;
+            uu[u] = ok ? lu[(base + 1 + t + 32 * u) * B + s] : T(0);
+            x[u] = ok ? y[r[u] * B + s] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) acc += uu[u] * x[u];
+    }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
     if ((threadIdx.x & 31) == 0) y[k * B + s] = (y[k * B + s] - acc) / ((const T*)b.piv)[k * B + s];
@@ -852,7 +921,7 @@ struct DevBuf {
 struct Workspace {
     int B = 0;
     int precision = -1;
-    DevBuf activeList;
+    DevBuf activeList, origin;  // origin: a compact batch position -> the system of the full batch
     DevBuf vm, va, lu, piv, y, z, rhs64, refine, maxMis, maxDx, startMis, finalMis, status, iters, convIters, convAt, active, flags, outage,
         loadScale, activeCount;
     DevBuf code, value, maxLoad, minVmNeg, maxVmB, chunkCount, chunkOffset, outKind, outElem, outVal, pq;
@@ -877,6 +946,7 @@ struct gs_grid {
     gs::DevGrid view{};
     std::vector<double> pgen, qgen, pload, qload;
     gs::Workspace ws;
+    gs::Workspace tws;  // compact copy of the few systems still stepping
     int split = 0;  // first level run by the persistent kernels
 };
 
@@ -965,10 +1035,7 @@ size_t PerSystemBytes(const Symbolic& s, int precision) {
     return (size_t)s.nnzLU * t + 2 * (size_t)s.m * t + refine + (size_t)s.n * 16 + (size_t)(s.nbr + s.n) * 9 + 256;
 }
 
-int EnsureWorkspace(gs_grid* G, int B, int precision, bool classify, bool loadScale) {
-    gs_ctx* ctx = G->ctx;
-    Workspace& w = G->ws;
-    const Symbolic& s = G->sym;
+int EnsureWs(gs_ctx* ctx, const Symbolic& s, Workspace& w, int B, int precision, bool classify, bool loadScale) {
     size_t t = precision == GS_PREC_MIXED ? 4 : 8;
     size_t Bz = (size_t)B;
     GS_CUDA(w.vm.alloc(s.n * Bz * 8));
@@ -987,6 +1054,7 @@ int EnsureWorkspace(gs_grid* G, int B, int precision, bool classify, bool loadSc
     GS_CUDA(w.convIters.alloc(Bz * 4)); GS_CUDA(w.convAt.alloc(Bz * 4));
     GS_CUDA(w.flags.alloc(Bz * 4)); GS_CUDA(w.outage.alloc(Bz * 4)); GS_CUDA(w.activeCount.alloc(16));
     GS_CUDA(w.activeList.alloc(Bz * 4));
+    GS_CUDA(w.origin.alloc(Bz * 4));
     GS_CUDA(w.startVm.alloc(s.n * 8)); GS_CUDA(w.startVa.alloc(s.n * 8));
     if (loadScale) GS_CUDA(w.loadScale.alloc(s.n * Bz * 8));
     if (classify) {
@@ -1000,10 +1068,18 @@ int EnsureWorkspace(gs_grid* G, int B, int precision, bool classify, bool loadSc
     return GS_OK;
 }
 
-DevBatch MakeBatch(gs_grid* G, int count, bool useScale) {
-    Workspace& w = G->ws;
+int EnsureWorkspace(gs_grid* G, int B, int precision, bool classify, bool loadScale) {
+    // the compact workspace of the few-systems path (its interleave stride is set per compaction)
+    const int cap = std::min(B, kCompactCap);
+    int rc = EnsureWs(G->ctx, G->sym, G->tws, cap, precision, false, loadScale);
+    if (rc != GS_OK) return rc;
+    return EnsureWs(G->ctx, G->sym, G->ws, B, precision, classify, loadScale);
+}
+
+// A batch view of workspace `w` with interleave stride B (at most the stride it was sized for).
+DevBatch MakeBatchWs(const Workspace& w, int nLevels, int B, int count, bool useScale) {
     DevBatch b{};
-    b.B = w.B; b.count = count;
+    b.B = B; b.count = count;
     b.vm = w.vm.as<double>(); b.va = w.va.as<double>(); b.lu = w.lu.p; b.y = w.y.p; b.piv = w.piv.p;
     const bool mixed = w.precision == GS_PREC_MIXED;
     b.z = mixed ? w.z.p : nullptr;
@@ -1017,8 +1093,12 @@ DevBatch MakeBatch(gs_grid* G, int count, bool useScale) {
     b.loadScale = useScale ? w.loadScale.as<double>() : nullptr;
     b.activeCount = w.activeCount.as<int>();
     b.activeList = w.activeList.as<int>();
-    b.nLevels = G->sym.nLevels;
+    b.nLevels = nLevels;
     return b;
+}
+
+DevBatch MakeBatch(gs_grid* G, int count, bool useScale) {
+    return MakeBatchWs(G->ws, G->sym.nLevels, G->ws.B, count, useScale);
 }
 
 // Run the Newton iteration of `count` systems already placed in the workspace (outage, loadScale).
@@ -1082,9 +1162,9 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
         }
         for (int l = split - 1; l >= 0; l--) launchLevel(k_level<T, kWorkBackward>, vec, bp[l], bp[l + 1]);
     };
-    auto solvePhase = [&]() {
+    auto solvePhase = [&](bool doRefine) {
         backward((T*)b.y);
-        if (refine) {
+        if (doRefine) {
             k_residual<T><<<dim3((s.n + 7) / 8, groups), blk8, 0, st>>>(g, b, nullptr, 0);
             stepLaunches++;
             for (int l = 0; l < split; l++) launchLevel(k_level<T, kWorkForward>, (T*)b.z, vp[l], vp[l + 1]);
@@ -1096,73 +1176,111 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
         }
     };
     const int rowsPerBlock = 512;
-    auto updatePhase = [&](const int* list, int nList) {
-        const int grp = list ? (nList + 31) / 32 : groups;
-        k_dxmax<T><<<dim3((s.m + rowsPerBlock - 1) / rowsPerBlock, grp), blk8, 0, st>>>(g, b, rowsPerBlock, refine, list, nList);
-        k_update<T><<<dim3((s.n + 7) / 8, grp), blk8, 0, st>>>(g, b, refine, list, nList);
+    auto updatePhase = [&](bool doRefine) {
+        k_dxmax<T><<<dim3((s.m + rowsPerBlock - 1) / rowsPerBlock, groups), blk8, 0, st>>>(g, b, rowsPerBlock, doRefine, nullptr, 0);
+        k_update<T><<<dim3((s.n + 7) / 8, groups), blk8, 0, st>>>(g, b, doRefine, nullptr, 0);
         stepLaunches += 2;
     };
-    cudaGraph_t graph;
-    cudaGraphExec_t exec = nullptr;
+    // The full-batch step as a graph; mixed precision keeps a second graph with the refinement solve, launched
+    // only in iterations where some system refines (k_status counts them).
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    int64_t launchesPerStep[2] = {0, 0};
     cudaError_t ce;
     if (!timed) {
-        GS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        factorPhase();
-        solvePhase();
-        updatePhase(nullptr, 0);
-        ce = cudaStreamEndCapture(st, &graph);
-        if (ce != cudaSuccess) return SetErr(ctx, GS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
-        ce = cudaGraphInstantiate(&exec, graph, 0);
-        cudaGraphDestroy(graph);
-        if (ce != cudaSuccess) return SetErr(ctx, GS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
-    } else {
-        stepLaunches = 0;
+        for (int r = 0; r <= refine; r++) {
+            cudaGraph_t graph;
+            stepLaunches = 0;
+            GS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            factorPhase();
+            solvePhase(r != 0);
+            updatePhase(r != 0);
+            ce = cudaStreamEndCapture(st, &graph);
+            if (ce == cudaSuccess) {
+                ce = cudaGraphInstantiate(&exec[r], graph, 0);
+                cudaGraphDestroy(graph);
+            }
+            if (ce != cudaSuccess) {
+                for (auto& x : exec) if (x) cudaGraphExecDestroy(x);
+                return SetErr(ctx, GS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+            }
+            launchesPerStep[r] = stepLaunches;
+        }
     }
-    const int64_t launchesPerStep = stepLaunches;
     const char* traceEnv = std::getenv("GS_TRACE_ITERATIONS");  // per-iteration phase times (with phase_timing)
     const bool traceIters = traceEnv && traceEnv[0] == '1';
     int64_t launches = 1;
     int iterations = 0;
+    int64_t sysIters = 0;  // systems stepped, summed over the iterations
     double fMs = 0, sMs = 0, mMs = 0, oMs = 0;
     int rc = GS_OK;
-    int listCount = 0;  // > 0: b.activeList holds the systems of the previous few-systems iteration
+    int listCount = 0;  // > 0: cur.activeList holds the systems of the previous few-systems iteration
+    // The batch being stepped: the full one, or (few-systems path) a compact copy of its last systems.
+    DevBatch cur = b;
+    bool compacted = false;
+    const dim3 nodeBlocks((s.n + 7) / 8);
     for (int iter = 0; iter <= o.max_iterations + 4; iter++) {
         if (timed) cudaEventRecord(ev[0], st);
         if (listCount > 0)
-            k_mismatch_jac<T><<<dim3((s.n + 7) / 8, (listCount + 31) / 32), blk8, 0, st>>>(g, b, 1, nullptr, nullptr,
-                                                                                         b.activeList, listCount);
+            k_mismatch_jac<T><<<dim3(nodeBlocks.x, (listCount + 31) / 32), blk8, 0, st>>>(g, cur, 1, nullptr, nullptr,
+                                                                                       cur.activeList, listCount);
         else
-            k_mismatch_jac<T><<<dim3((s.n + 7) / 8, groups), blk8, 0, st>>>(g, b, 1, nullptr, nullptr, nullptr, 0);
+            k_mismatch_jac<T><<<dim3(nodeBlocks.x, cur.B / 32), blk8, 0, st>>>(g, cur, 1, nullptr, nullptr, nullptr, 0);
         if (timed) cudaEventRecord(ev[1], st);
-        cudaMemsetAsync(b.activeCount, 0, sizeof(int), st);
-        k_status<<<(count + 255) / 256, 256, 0, st>>>(b, iter, o.tolerance, o.diverge_limit_pu, o.max_iterations, 0);
+        cudaMemsetAsync(cur.activeCount, 0, 2 * sizeof(int), st);
+        k_status<<<(cur.count + 255) / 256, 256, 0, st>>>(cur, iter, o.tolerance, o.diverge_limit_pu, o.max_iterations, 0);
         launches += 2;
-        cudaMemcpyAsync(ctx->pinnedCount, b.activeCount, sizeof(int), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(ctx->pinnedCount, cur.activeCount, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
         ce = cudaStreamSynchronize(st);
         if (ce != cudaSuccess) { rc = SetErr(ctx, GS_ERR_CUDA, std::string("newton: ") + cudaGetErrorString(ce)); break; }
         if (timed) { float t; cudaEventElapsedTime(&t, ev[0], ev[1]); mMs += t; }
         if (*ctx->pinnedCount == 0) break;
         iterations++;
-        const int nActive = *ctx->pinnedCount;
+        const int nActive = ctx->pinnedCount[0];
+        const int anyRefine = refine && ctx->pinnedCount[1] > 0 ? 1 : 0;
+        sysIters += nActive;
         if (nActive <= kTailMaxSystems) {
-            // few systems left: one CTA per active system (k_tail), no per-level launches
             if (timed) cudaEventRecord(ev[1], st);
-            cudaMemsetAsync(b.activeCount, 0, sizeof(int), st);
-            k_collect_active<<<(count + 255) / 256, 256, 0, st>>>(b);
-            k_tail<T, kWorkFactor><<<nActive, kTailThreads, 0, st>>>(g, b, (T*)b.y);
+            const int stride = (nActive + 31) / 32 * 32;
+            if (!compacted || 2 * stride <= cur.B) {
+                // (re)compact: the full batch takes back the compact systems, then the active ones move out
+                if (compacted) {
+                    k_scatter<<<dim3(nodeBlocks.x, cur.B / 32), blk8, 0, st>>>(cur, b, G->tws.origin.as<int>(), s.n);
+                    launches++;
+                }
+                cudaMemsetAsync(b.activeCount, 0, sizeof(int), st);
+                k_collect_active<<<(count + 255) / 256, 256, 0, st>>>(b);
+                cudaMemcpyAsync(G->tws.origin.p, b.activeList, nActive * sizeof(int), cudaMemcpyDeviceToDevice, st);
+                cur = MakeBatchWs(G->tws, s.nLevels, stride, nActive, useScale);
+                k_gather<<<dim3(nodeBlocks.x, stride / 32), blk8, 0, st>>>(b, cur, G->tws.origin.as<int>(), s.n);
+                // this iteration's Jacobian and right-hand side, rebuilt in the compact workspace; the mismatch
+                // maximum it records was already taken by k_status
+                k_mismatch_jac<T><<<dim3(nodeBlocks.x, stride / 32), blk8, 0, st>>>(g, cur, 1, nullptr, nullptr, nullptr, 0);
+                cudaMemsetAsync(cur.maxMis, 0, (size_t)nActive * sizeof(unsigned long long), st);
+                launches += 3;
+                compacted = true;
+            }
+            // few systems left: one CTA per active system (k_tail), no per-level launches
+            cudaMemsetAsync(cur.activeCount, 0, sizeof(int), st);
+            k_collect_active<<<(cur.count + 255) / 256, 256, 0, st>>>(cur);
+            k_tail<T, kWorkFactor><<<nActive, kTailThreads, 0, st>>>(g, cur, (T*)cur.y);
             if (timed) cudaEventRecord(ev[2], st);
-            k_tail<T, kWorkBackward><<<nActive, kTailThreads, 0, st>>>(g, b, (T*)b.y);
-            launches += 4;
+            k_tail<T, kWorkBackward><<<nActive, kTailThreads, 0, st>>>(g, cur, (T*)cur.y);
+            launches += 3;
             if (refine) {
-                k_residual<T><<<dim3((s.n + 7) / 8, (nActive + 31) / 32), blk8, 0, st>>>(g, b, b.activeList, nActive);
-                k_tail<T, kWorkForward><<<nActive, kTailThreads, 0, st>>>(g, b, (T*)b.z);
-                k_tail<T, kWorkBackward><<<nActive, kTailThreads, 0, st>>>(g, b, (T*)b.z);
+                k_residual<T><<<dim3(nodeBlocks.x, (nActive + 31) / 32), blk8, 0, st>>>(g, cur, cur.activeList, nActive);
+                k_tail<T, kWorkForward><<<nActive, kTailThreads, 0, st>>>(g, cur, (T*)cur.z);
+                k_tail<T, kWorkBackward><<<nActive, kTailThreads, 0, st>>>(g, cur, (T*)cur.z);
                 launches += 3;
             }
             if (timed) cudaEventRecord(ev[3], st);
-            updatePhase(b.activeList, nActive);
+            {
+                const int grp = (nActive + 31) / 32;
+                k_dxmax<T><<<dim3((s.m + rowsPerBlock - 1) / rowsPerBlock, grp), blk8, 0, st>>>(g, cur, rowsPerBlock, refine,
+                                                                                               cur.activeList, nActive);
+                k_update<T><<<dim3(nodeBlocks.x, grp), blk8, 0, st>>>(g, cur, refine, cur.activeList, nActive);
+                launches += 2;
+            }
             listCount = nActive;
-            launches += 2;
             if (timed) {
                 cudaEventRecord(ev[4], st);
                 ce = cudaEventSynchronize(ev[4]);
@@ -1179,17 +1297,17 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             continue;
         }
         if (!timed) {
-            ce = cudaGraphLaunch(exec, st);
-            launches += launchesPerStep;
+            ce = cudaGraphLaunch(exec[anyRefine], st);
+            launches += launchesPerStep[anyRefine];
             if (ce != cudaSuccess) { rc = SetErr(ctx, GS_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(ce)); break; }
         } else {
             stepLaunches = 0;
             cudaEventRecord(ev[1], st);
             factorPhase();
             cudaEventRecord(ev[2], st);
-            solvePhase();
+            solvePhase(anyRefine != 0);
             cudaEventRecord(ev[3], st);
-            updatePhase(nullptr, 0);
+            updatePhase(anyRefine != 0);
             cudaEventRecord(ev[4], st);
             launches += stepLaunches;
             ce = cudaEventSynchronize(ev[4]);
@@ -1204,15 +1322,19 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
                              *ctx->pinnedCount, t1, t2, t3);
         }
     }
+    if (compacted && rc == GS_OK) {
+        k_scatter<<<dim3(nodeBlocks.x, cur.B / 32), blk8, 0, st>>>(cur, b, G->tws.origin.as<int>(), s.n);
+        launches++;
+    }
     if (timed) for (auto& e : ev) cudaEventDestroy(e);
     if (stats) {
         stats->launches += launches;
         stats->iterations = std::max(stats->iterations, iterations);
         stats->factorMs += fMs; stats->solveMs += sMs; stats->mismatchMs += mMs; stats->otherMs += oMs;
         // algorithmic bytes of one factorisation per system: read J (nnzJ) + write L and U (nnzLU)
-        stats->factorBytes += (double)iterations * (double)count * (double)sizeof(T) * ((double)s.nnzJ + (double)s.nnzLU);
+        stats->factorBytes += (double)sysIters * (double)sizeof(T) * ((double)s.nnzJ + (double)s.nnzLU);
     }
-    if (exec) cudaGraphExecDestroy(exec);
+    for (auto& x : exec) if (x) cudaGraphExecDestroy(x);
     cudaEventRecord(e1, st);
     cudaEventSynchronize(e1);
     if (ms) cudaEventElapsedTime(ms, e0, e1);
@@ -1323,7 +1445,7 @@ int gs_ctx_create(int device, const gs_ctx_opts* opts, gs_ctx** out) {
     gs_ctx* c = new gs_ctx();
     c->device = device;
     c->stream = probe->stream;
-    if (cudaMallocHost(&c->pinnedCount, sizeof(int)) != cudaSuccess) { delete c; return GS_ERR_CUDA; }
+    if (cudaMallocHost(&c->pinnedCount, 4 * sizeof(int)) != cudaSuccess) { delete c; return GS_ERR_CUDA; }
     *out = c;
     return GS_OK;
 }

@@ -98,7 +98,7 @@ struct DevBatch {
     int* flags;             // [B]
     const int* outage;      // [B] branch index or -1
     const double* loadScale;  // [n][B] or null
-    int* activeCount;       // [1]
+    int* activeCount;       // [2]: systems still stepping, of which refine their step (mixed precision)
     int* activeList;        // [B] systems still stepping (filled for the few-systems path)
 };
 
