@@ -65,6 +65,7 @@ class N1Result(ctypes.Structure):
         ("base_status", c_i32), ("base_iterations", c_i32), ("device_ms", c_f64), ("n_singular_pivot", c_i32),
         ("n_batches", c_i32), ("kernel_launches", ctypes.c_int64), ("newton_iterations", c_i32), ("reserved1", c_i32),
         ("factor_ms", c_f64), ("solve_ms", c_f64), ("mismatch_ms", c_f64), ("other_ms", c_f64), ("factor_bytes", c_f64),
+        ("level_factor_ms", c_f64), ("level_factor_bytes", c_f64), ("tail_ms", c_f64),
     ]
 
 

@@ -1108,6 +1108,7 @@ struct NewtonStats {
     int iterations = 0;
     double factorMs = 0, solveMs = 0, mismatchMs = 0, otherMs = 0;
     double factorBytes = 0;
+    double levelFactorMs = 0, levelFactorBytes = 0, tailMs = 0;
 };
 
 template <typename T>
@@ -1211,7 +1212,8 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
     int64_t launches = 1;
     int iterations = 0;
     int64_t sysIters = 0;  // systems stepped, summed over the iterations
-    double fMs = 0, sMs = 0, mMs = 0, oMs = 0;
+    int64_t levelSys = 0;  // the same over full-batch iterations
+    double fMs = 0, sMs = 0, mMs = 0, oMs = 0, lfMs = 0, tMs = 0;
     int rc = GS_OK;
     int listCount = 0;  // > 0: cur.activeList holds the systems of the previous few-systems iteration
     // The batch being stepped: the full one, or (few-systems path) a compact copy of its last systems.
@@ -1289,7 +1291,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
                 cudaEventElapsedTime(&t1, ev[1], ev[2]);
                 cudaEventElapsedTime(&t2, ev[2], ev[3]);
                 cudaEventElapsedTime(&t3, ev[3], ev[4]);
-                fMs += t1; sMs += t2; oMs += t3;
+                fMs += t1; sMs += t2; oMs += t3; tMs += t1 + t2 + t3;
                 if (traceIters)
                     std::fprintf(stderr, "gs: iteration %d active %d (few-systems path) factor %.3f ms solve %.3f ms update %.3f ms\n",
                                  iter, nActive, t1, t2, t3);
@@ -1316,7 +1318,8 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             cudaEventElapsedTime(&t1, ev[1], ev[2]);
             cudaEventElapsedTime(&t2, ev[2], ev[3]);
             cudaEventElapsedTime(&t3, ev[3], ev[4]);
-            fMs += t1; sMs += t2; oMs += t3;
+            fMs += t1; sMs += t2; oMs += t3; lfMs += t1;
+            levelSys += nActive;
             if (traceIters)
                 std::fprintf(stderr, "gs: iteration %d active %d factor %.3f ms solve %.3f ms update %.3f ms\n", iter,
                              *ctx->pinnedCount, t1, t2, t3);
@@ -1333,6 +1336,9 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
         stats->factorMs += fMs; stats->solveMs += sMs; stats->mismatchMs += mMs; stats->otherMs += oMs;
         // algorithmic bytes of one factorisation per system: read J (nnzJ) + write L and U (nnzLU)
         stats->factorBytes += (double)sysIters * (double)sizeof(T) * ((double)s.nnzJ + (double)s.nnzLU);
+        stats->levelFactorMs += lfMs;
+        stats->levelFactorBytes += (double)levelSys * (double)sizeof(T) * ((double)s.nnzJ + (double)s.nnzLU);
+        stats->tailMs += tMs;
     }
     for (auto& x : exec) if (x) cudaGraphExecDestroy(x);
     cudaEventRecord(e1, st);
@@ -1782,6 +1788,9 @@ int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts*
     res->mismatch_ms = stats.mismatchMs;
     res->other_ms = stats.otherMs;
     res->factor_bytes = stats.factorBytes;
+    res->level_factor_ms = stats.levelFactorMs;
+    res->level_factor_bytes = stats.levelFactorBytes;
+    res->tail_ms = stats.tailMs;
     return capacityOk ? GS_OK : GS_ERR_CAPACITY;
 }
 

@@ -333,7 +333,8 @@ class ContingencyAnalysis:
         out.update(base_status=r.base_status, base_iterations=r.base_iterations, device_ms=r.device_ms,
                    n_singular_pivot=r.n_singular_pivot, n_batches=r.n_batches, kernel_launches=r.kernel_launches,
                    newton_iterations=r.newton_iterations, factor_ms=r.factor_ms, solve_ms=r.solve_ms,
-                   mismatch_ms=r.mismatch_ms, other_ms=r.other_ms, factor_bytes=r.factor_bytes)
+                   mismatch_ms=r.mismatch_ms, other_ms=r.other_ms, factor_bytes=r.factor_bytes,
+                   level_factor_ms=r.level_factor_ms, level_factor_bytes=r.level_factor_bytes, tail_ms=r.tail_ms)
         return out
 
     @classmethod

@@ -181,6 +181,10 @@ typedef struct gs_n1_result {
     double mismatch_ms;        /* mismatch + Jacobian fill (+ residual) */
     double other_ms;           /* status, max |dx|, update */
     double factor_bytes;       /* algorithmic bytes of the factor phase (J read + L,U written), whole call */
+    /* the factorisations of full-batch iterations alone (per-level launches + the narrow-top kernel) */
+    double level_factor_ms;
+    double level_factor_bytes;
+    double tail_ms;            /* iterations on the few-systems path, all phases */
 } gs_n1_result;
 
 /* ---- context -------------------------------------------------------------------------------- */
