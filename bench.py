@@ -116,6 +116,128 @@ def cpu_sample(m, idx, threads, target_s=12.0):
     return conv / dt, k, dt
 
 
+# ---------------------------------------------------------------------------------------------
+# Serving: Poisson arrivals of load-flow requests over the uneven grid population (64 synthetic grids, bus
+# counts log-uniform in 100-25,000; each request the base case or one random non-islanding branch outage of a
+# random grid, 50/50), answered by the request loop (gs_serve_*, mixed precision). Latency runs from the
+# request's scheduled arrival to its result on the host.
+SERVE_RATES = (100, 1000, 5000, 20000)
+SERVE_HEADLINE_RATE = 1000
+SERVE_SECONDS = 2.0
+
+
+def serve_population(workers):
+    from gridsim_b200 import synthetic
+    grids = synthetic.uneven_population(64, 0, 100, 25000, workers=workers)
+    outs = [synthetic.outage_set(m, None, 0) for m in grids]
+    return grids, outs
+
+
+def request_stream(outs, count, seed):
+    from gridsim_b200.serving import REQUEST_DTYPE
+    rng = np.random.default_rng(seed)
+    arr = np.zeros(count, REQUEST_DTYPE)
+    g = rng.integers(0, len(outs), count)
+    lens = np.array([len(o) for o in outs])
+    pick = (rng.random(count) * lens[g]).astype(np.int64)
+    base = rng.random(count) < 0.5
+    arr["grid"] = g
+    arr["outage"] = [(-1 if base[k] or lens[g[k]] == 0 else int(outs[g[k]][pick[k]])) for k in range(count)]
+    arr["tag"] = np.arange(count)
+    return arr
+
+
+def poisson_run(srv, reqs, rate, seed, drain_s=180.0):
+    rng = np.random.default_rng(seed)
+    n = len(reqs)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+    lat = np.full(n, np.nan)
+    status = np.full(n, -1)
+    iters = np.zeros(n)
+    delay = np.zeros(n)
+    k = got = 0
+    t0 = time.perf_counter()
+    t_last = 0.0
+    while got < n:
+        now = time.perf_counter() - t0
+        j = int(np.searchsorted(arrivals, now, side="right"))
+        if j > k:
+            delay[k:j] = (time.perf_counter() - t0) - arrivals[k:j]
+            srv.submit(reqs[k:j])
+            k = j
+        res = srv.poll(timeout_ms=0)
+        if res:
+            t_last = time.perf_counter() - t0
+            for r in res:
+                lat[r.tag] = r.latency_ms + delay[r.tag] * 1e3
+                status[r.tag] = r.status
+                iters[r.tag] = r.iterations
+            got += len(res)
+        else:
+            time.sleep(50e-6)
+        if now > arrivals[-1] + drain_s:
+            raise RuntimeError(f"serving at {rate} req/s: {n - got} requests unanswered")
+    return {"rate_rps": rate, "requests": n, "offered_s": float(arrivals[-1]),
+            "throughput_rps": n / max(t_last, 1e-9), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "p999_ms": float(np.percentile(lat, 99.9)),
+            "mean_ms": float(np.mean(lat)), "converged": float(np.mean(status == 0)),
+            "mean_iterations": float(np.mean(iters))}
+
+
+def batched_rps(ctx, grids, reqs, precision):
+    """The same requests through the batched API, grouped by grid: outages as one N-1 screen per grid (warm
+    start), base cases as one batch solve per grid. Wall time after one untimed pass."""
+    from gridsim_b200.engine import ContingencyAnalysis, SparseNewtonRaphsonPowerFlow
+    solvers = [SparseNewtonRaphsonPowerFlow(precision, ctx) for _ in grids]
+    opt = options(precision)
+    groups = []
+    for g in range(len(grids)):
+        sel = reqs[reqs["grid"] == g]["outage"]
+        groups.append((np.ascontiguousarray(sel[sel >= 0], np.int32), int(np.sum(sel < 0))))
+
+    def one_pass():
+        for g, (m, (outs, nbase)) in enumerate(zip(grids, groups)):
+            if len(outs):
+                ContingencyAnalysis.screen_raw(m, outs, solvers[g], opt)
+            if nbase:
+                solvers[g].solve_batch(m, outage=np.full(nbase, -1, np.int32), options=opt)
+    one_pass()
+    t = time.perf_counter()
+    one_pass()
+    return len(reqs) / (time.perf_counter() - t)
+
+
+def run_serving(ctx, workers):
+    from gridsim_b200.serving import LoadFlowServer, drain
+    t = time.perf_counter()
+    grids, outs = serve_population(workers)
+    gen_s = time.perf_counter() - t
+    srv = LoadFlowServer(options("mixed"), ctx)
+    for m in grids:
+        srv.add_grid(m)
+    srv.start()
+    try:
+        warm = request_stream(outs, 2000, 99)
+        srv.submit(warm)
+        drain(srv, len(warm))
+        runs = []
+        for i, rate in enumerate(SERVE_RATES):
+            reqs = request_stream(outs, int(max(200, rate * SERVE_SECONDS)), 1000 + i)
+            runs.append(poisson_run(srv, reqs, rate, 2000 + i))
+        st = srv.stats()
+    finally:
+        srv.close()
+    ref_reqs = request_stream(outs, 20000, 77)
+    out = {"population": f"64 synthetic grids, bus counts log-uniform 100-25,000 "
+                         f"({sum(m.n_bus for m in grids):,} buses), built in {gen_s:.0f} s",
+           "requests": "base case or one random non-islanding branch outage of a random grid (50/50)",
+           "precision": "mixed", "slots_per_grid": 128, "slot_gb": st["slot_bytes"] / 1e9, "runs": runs,
+           "batched_fp64_rps": batched_rps(ctx, grids, ref_reqs, "fp64"),
+           "batched_mixed_rps": batched_rps(ctx, grids, ref_reqs, "mixed")}
+    head = next(r for r in runs if r["rate_rps"] == SERVE_HEADLINE_RATE)
+    return out, head
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -234,6 +356,9 @@ def run_ours(args):
                "max_dva_rad": float(np.max(np.abs(np.radians(g["va_deg"][cv] - o["va_deg"][cv])))),
                "violations_identical": bool(np.array_equal(g["viol_element"], o["viol_element"]) and
                                             np.array_equal(g["viol_kind"], o["viol_kind"]))}
+    serving, head = None, None
+    if rank == 0 and not args.no_serve:
+        serving, head = run_serving(ctx, os.cpu_count() or 1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, k, dt = cpu_sample(m, idx, os.cpu_count() or 1)
@@ -266,7 +391,9 @@ def run_ours(args):
                          "other": prof["other_ms"], "few_systems_path": prof["tail_ms"],
                          "full_batch_factor": prof["level_factor_ms"]},
             "cpu_baseline": cpu, "clocks": mx["clocks"], "gpu_launches": mx["launches"], "accuracy_vs_oracle": acc,
-            "serve_p99_ms": None,
+            "serve_p99_ms": head["p99_ms"] if head else None,
+            "serve_rate_rps": SERVE_HEADLINE_RATE if head else None,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if dist:
@@ -282,6 +409,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -77,6 +77,29 @@ class GridInfo(ctypes.Structure):
     ]
 
 
+class ServeOpts(ctypes.Structure):
+    _fields_ = [("pf", PfOpts), ("slots_per_grid", c_i32), ("state_slots", c_i32), ("hbm_fraction", c_f64),
+                ("reserved", c_i32 * 8)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("grid", c_i32), ("outage", c_i32), ("want_state", c_i32), ("reserved", c_i32), ("tag", ctypes.c_uint64)]
+
+
+class Response(ctypes.Structure):
+    _fields_ = [("ticket", ctypes.c_uint64), ("tag", ctypes.c_uint64), ("grid", c_i32), ("outage", c_i32),
+                ("status", c_i32), ("iterations", c_i32), ("max_mismatch", c_f64), ("queue_ms", c_f64),
+                ("latency_ms", c_f64), ("state_offset", ctypes.c_int64)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("ticks", ctypes.c_int64),
+                ("system_steps", ctypes.c_int64), ("grids", c_i32), ("slots_total", c_i32), ("in_flight", c_i32),
+                ("queued", c_i32), ("slot_bytes", c_f64), ("failed", c_i32), ("reserved", c_i32 * 7)]
+
+
+GS_SERVE_MAX_SLOTS = 128
+
 # Every entry point the header declares, with its ctypes signature.
 EXPORTS = {
     "gs_abi_version": (c_i32, []),
@@ -93,6 +116,14 @@ EXPORTS = {
     "gs_n1_screen": (c_i32, [c_vp, c_i32, c_vp, ctypes.POINTER(PfOpts), ctypes.POINTER(N1Result)]),
     "gs_analyze_host": (c_i32, [ctypes.POINTER(GridDesc), ctypes.POINTER(GridInfo)]),
     "gs_pf_mismatch_noalloc": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp]),
+    "gs_serve_create": (c_i32, [c_vp, ctypes.POINTER(ServeOpts), ctypes.POINTER(c_vp)]),
+    "gs_serve_add_grid": (c_i32, [c_vp, c_vp, ctypes.POINTER(c_i32)]),
+    "gs_serve_start": (c_i32, [c_vp]),
+    "gs_serve_submit": (c_i32, [c_vp, c_i32, c_vp, c_vp]),
+    "gs_serve_poll": (c_i32, [c_vp, c_i32, c_i32, c_vp, c_vp, ctypes.c_int64, ctypes.POINTER(c_i32)]),
+    "gs_serve_stats_get": (c_i32, [c_vp, ctypes.POINTER(ServeStats)]),
+    "gs_serve_stop": (c_i32, [c_vp, c_i32]),
+    "gs_serve_destroy": (c_i32, [c_vp]),
 }
 
 _lib = None

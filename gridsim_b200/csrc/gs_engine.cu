@@ -155,52 +155,36 @@ __global__ void __launch_bounds__(256) k_mismatch_jac(DevGrid g, DevBatch b, int
 }
 
 // ---------------------------------------------------------------------------------------------
-// 2. per-system Newton control (RunNewton :218-238). With `polish` > 0 (mixed precision), a system that
-//    has met the tolerance keeps its Converged status and takes at most `polish` more steps while its
-//    mismatch is above tol * 1e-3: the FP32 step converges linearly, so the first state under the
-//    tolerance can sit ~||J^-1|| * tol from the root; the extra steps bring it to the root the FP64
-//    iteration reaches. The status (and so every convergence flag) is decided at the first crossing.
-__global__ void k_status(DevBatch b, int iter, double tol, double divLimit, int maxIter, int polish) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= b.count || !b.active[s]) return;
+// 2. per-system Newton control (RunNewton :218-238): the tests in the reference's order. `iter` is the
+//    system's step count so far. Returns whether the system takes another step; `activeCount[0]` counts
+//    those, `activeCount[1]` those of them that refine their step (mixed precision).
+__device__ __forceinline__ bool statusStep(const DevBatch& b, int s, int iter, double tol, double divLimit, int maxIter) {
     const double mis = __longlong_as_double((long long)b.maxMis[s]);
     b.maxMis[s] = 0ull;
     b.maxDx[s] = 0ull;
     const int fl = b.flags[s];
-    if (b.convAt[s] >= 0) {  // polishing a converged state
-        const bool ok = !(fl & (kFlagNonFinite | kFlagStepBad | kFlagJacBad)) && mis < tol;
-        if (ok) b.finalMis[s] = mis;
-        if (!ok || mis < tol * 1e-3 || iter - b.convAt[s] >= polish) { b.active[s] = 0; return; }
-        atomicAdd(b.activeCount, 1);
-        return;
-    }
     if (fl & kFlagNonFinite) {  // a NaN mismatch never converges; the non-finite step then stops the run
         b.finalMis[s] = NAN;
         b.status[s] = GS_PF_NON_FINITE;
         b.active[s] = 0;
-        return;
+        return false;
     }
     if (fl & kFlagStepBad) {  // the previous step was refused: the run stops, state unchanged
         b.status[s] = GS_PF_MAX_ITERATIONS;
         b.active[s] = 0;
-        return;
+        return false;
     }
     b.finalMis[s] = mis;
     if (iter == 0) b.startMis[s] = mis;
     if (mis < tol) {
         b.status[s] = GS_PF_CONVERGED;
         b.convIters[s] = b.iters[s];
-        if (polish > 0 && mis >= tol * 1e-3 && !(fl & kFlagJacBad)) {
-            b.convAt[s] = iter;
-            atomicAdd(b.activeCount, 1);
-        } else {
-            b.active[s] = 0;
-        }
-        return;
+        b.active[s] = 0;
+        return false;
     }
-    if (mis > fmax(divLimit, b.startMis[s])) { b.status[s] = GS_PF_DIVERGED; b.active[s] = 0; return; }
-    if (iter >= maxIter) { b.status[s] = GS_PF_MAX_ITERATIONS; b.active[s] = 0; return; }
-    if (fl & kFlagJacBad) { b.status[s] = GS_PF_MAX_ITERATIONS; b.active[s] = 0; return; }  // SolveStep refuses it
+    if (mis > fmax(divLimit, b.startMis[s])) { b.status[s] = GS_PF_DIVERGED; b.active[s] = 0; return false; }
+    if (iter >= maxIter) { b.status[s] = GS_PF_MAX_ITERATIONS; b.active[s] = 0; return false; }
+    if (fl & kFlagJacBad) { b.status[s] = GS_PF_MAX_ITERATIONS; b.active[s] = 0; return false; }  // SolveStep refuses it
     // Mixed precision refines the FP32 step with the FP64 residual once the mismatch is small: far from the
     // root the Newton step is self-correcting and an FP32 step error of ~kappa * 2^-24 changes nothing.
     if (b.refine) {
@@ -209,6 +193,22 @@ __global__ void k_status(DevBatch b, int iter, double tol, double divLimit, int 
         if (r) atomicAdd(b.activeCount + 1, 1);
     }
     atomicAdd(b.activeCount, 1);
+    return true;
+}
+
+// A batch in lock step: every active system has taken `iter` steps.
+__global__ void k_status(DevBatch b, int iter, double tol, double divLimit, int maxIter) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= b.count || !b.active[s]) return;
+    statusStep(b, s, iter, tol, divLimit, maxIter);
+}
+
+// Systems admitted at different times (the request loop): each at its own step count. Systems that stop
+// here are listed in done[1 ..], done[0] their number.
+__global__ void k_status_each(DevBatch b, double tol, double divLimit, int maxIter, int* done) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= b.count || !b.active[s]) return;
+    if (!statusStep(b, s, b.iters[s], tol, divLimit, maxIter)) done[1 + atomicAdd(done, 1)] = s;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -546,7 +546,6 @@ __device__ __forceinline__ void moveSystem(const DevBatch& from, int sf, const D
     to.status[st] = from.status[sf];
     to.iters[st] = from.iters[sf];
     to.convIters[st] = from.convIters[sf];
-    to.convAt[st] = from.convAt[sf];
     to.active[st] = from.active[sf];
     to.flags[st] = from.flags[sf];
     const_cast<int*>(to.outage)[st] = from.outage[sf];
@@ -763,7 +762,6 @@ __global__ void k_init(DevGrid g, DevBatch b, const double* vmStart, const doubl
         b.status[s] = s < b.count ? GS_PF_MAX_ITERATIONS : GS_PF_NOT_RUN;
         b.iters[s] = 0;
         b.convIters[s] = 0;
-        b.convAt[s] = -1;
         if (b.refine) b.refine[s] = 0;
         b.active[s] = s < b.count ? 1 : 0;
         b.flags[s] = 0;
@@ -922,7 +920,7 @@ struct Workspace {
     int B = 0;
     int precision = -1;
     DevBuf activeList, origin;  // origin: a compact batch position -> the system of the full batch
-    DevBuf vm, va, lu, piv, y, z, rhs64, refine, maxMis, maxDx, startMis, finalMis, status, iters, convIters, convAt, active, flags, outage,
+    DevBuf vm, va, lu, piv, y, z, rhs64, refine, maxMis, maxDx, startMis, finalMis, status, iters, convIters, active, flags, outage,
         loadScale, activeCount;
     DevBuf code, value, maxLoad, minVmNeg, maxVmB, chunkCount, chunkOffset, outKind, outElem, outVal, pq;
     DevBuf startVm, startVa;
@@ -1051,7 +1049,7 @@ int EnsureWs(gs_ctx* ctx, const Symbolic& s, Workspace& w, int B, int precision,
     GS_CUDA(w.maxMis.alloc(Bz * 8)); GS_CUDA(w.maxDx.alloc(Bz * 8));
     GS_CUDA(w.startMis.alloc(Bz * 8)); GS_CUDA(w.finalMis.alloc(Bz * 8));
     GS_CUDA(w.status.alloc(Bz * 4)); GS_CUDA(w.iters.alloc(Bz * 4)); GS_CUDA(w.active.alloc(Bz * 4));
-    GS_CUDA(w.convIters.alloc(Bz * 4)); GS_CUDA(w.convAt.alloc(Bz * 4));
+    GS_CUDA(w.convIters.alloc(Bz * 4));
     GS_CUDA(w.flags.alloc(Bz * 4)); GS_CUDA(w.outage.alloc(Bz * 4)); GS_CUDA(w.activeCount.alloc(16));
     GS_CUDA(w.activeList.alloc(Bz * 4));
     GS_CUDA(w.origin.alloc(Bz * 4));
@@ -1088,7 +1086,7 @@ DevBatch MakeBatchWs(const Workspace& w, int nLevels, int B, int count, bool use
     b.maxMis = w.maxMis.as<unsigned long long>(); b.maxDx = w.maxDx.as<unsigned long long>();
     b.startMis = w.startMis.as<double>(); b.finalMis = w.finalMis.as<double>();
     b.status = w.status.as<int>(); b.iters = w.iters.as<int>(); b.active = w.active.as<int>();
-    b.convIters = w.convIters.as<int>(); b.convAt = w.convAt.as<int>();
+    b.convIters = w.convIters.as<int>();
     b.flags = w.flags.as<int>(); b.outage = w.outage.as<int>();
     b.loadScale = useScale ? w.loadScale.as<double>() : nullptr;
     b.activeCount = w.activeCount.as<int>();
@@ -1229,7 +1227,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             k_mismatch_jac<T><<<dim3(nodeBlocks.x, cur.B / 32), blk8, 0, st>>>(g, cur, 1, nullptr, nullptr, nullptr, 0);
         if (timed) cudaEventRecord(ev[1], st);
         cudaMemsetAsync(cur.activeCount, 0, 2 * sizeof(int), st);
-        k_status<<<(cur.count + 255) / 256, 256, 0, st>>>(cur, iter, o.tolerance, o.diverge_limit_pu, o.max_iterations, 0);
+        k_status<<<(cur.count + 255) / 256, 256, 0, st>>>(cur, iter, o.tolerance, o.diverge_limit_pu, o.max_iterations);
         launches += 2;
         cudaMemcpyAsync(ctx->pinnedCount, cur.activeCount, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
         ce = cudaStreamSynchronize(st);
@@ -1922,3 +1920,6 @@ extern "C" int gs_pf_mismatch_noalloc(gs_grid* G, int32_t count, const double* d
     GS_CUDA(cudaStreamSynchronize(st));
     return GS_OK;
 }
+
+// The request loop (gs_serve_*): uses the kernels and host helpers above.
+#include "gs_serve.cuh"

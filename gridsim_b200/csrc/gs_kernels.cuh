@@ -93,7 +93,6 @@ struct DevBatch {
     int* status;            // [B]
     int* iters;             // [B] steps taken
     int* convIters;         // [B] steps taken when the tolerance was first met
-    int* convAt;            // [B] iteration of the first crossing, -1 before
     int* active;            // [B]
     int* flags;             // [B]
     const int* outage;      // [B] branch index or -1

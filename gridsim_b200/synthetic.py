@@ -448,13 +448,31 @@ def load_scalings(m: GridModel, count: int, seed: int) -> np.ndarray:
     return g * np.exp(0.05 * rng.standard_normal((count, m.n_bus)))
 
 
-def uneven_population(n_grids: int = 64, seed: int = 0, lo: int = 100, hi: int = 25000):
-    """Grids with bus counts log-uniform in [lo, hi], b ~ U(1.35, 1.4) n, n_pv = 0.12 n."""
+def population_specs(n_grids: int = 64, seed: int = 0, lo: int = 100, hi: int = 25000):
+    """(n_bus, n_branch, n_pv, seed, name) of the uneven population: bus counts log-uniform in [lo, hi],
+    b ~ U(1.35, 1.4) n, n_pv = 0.12 n."""
     rng = np.random.Generator(np.random.PCG64(seed + 32452843))
     sizes = np.exp(rng.uniform(math.log(lo), math.log(hi), size=n_grids)).astype(int)
     out = []
     for g, n in enumerate(sizes):
         b = int(round(n * rng.uniform(1.35, 1.4)))
-        out.append(make_grid(int(n), b, max(1, int(round(0.12 * n))), seed * 1000 + g,
-                             name=f"synthetic-uneven-{g}-{n}bus"))
+        out.append((int(n), b, max(1, int(round(0.12 * n))), seed * 1000 + g, f"synthetic-uneven-{g}-{n}bus"))
     return out
+
+
+def _make_from_spec(spec):
+    n, b, npv, sd, name = spec
+    return make_grid(n, b, npv, sd, name=name)
+
+
+def uneven_population(n_grids: int = 64, seed: int = 0, lo: int = 100, hi: int = 25000, workers: int = 0):
+    """The uneven-size population (population_specs), built on `workers` spawned processes (0: in this one)."""
+    specs = population_specs(n_grids, seed, lo, hi)
+    if workers <= 1:
+        return [_make_from_spec(s) for s in specs]
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    order = sorted(range(len(specs)), key=lambda k: -specs[k][0])  # largest first: the pool finishes together
+    with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        built = dict(zip(order, ex.map(_make_from_spec, [specs[k] for k in order])))
+    return [built[k] for k in range(len(specs))]

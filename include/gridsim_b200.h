@@ -242,6 +242,78 @@ int gs_pf_solve_batch(gs_grid *grid, int32_t count, const double *load_scale, co
 int gs_n1_screen(gs_grid *grid, int32_t n_out, const int32_t *branch_idx, const gs_pf_opts *opts,
                  gs_n1_result *res);
 
+/* ---- request loop (serving) ---------------------------------------------------------------------
+ * The reference's nearest counterpart is its sequential `gridsim rpc` host (src/GridSim.Cli/RpcCommand.cs:11-50):
+ * one JSON request at a time, `solve` running the `pf` solver on a case held by handle. Here one native
+ * scheduler thread keeps every registered grid resident on the device (symbolic data, base solution and a
+ * batch of request slots) and steps the occupied slots of each grid one Newton iteration at a time on that
+ * grid's own stream (continuous batching): a request joins a free slot of its grid at the next iteration
+ * boundary and leaves as soon as its system stops, so requests that arrive while others are on the GPU
+ * overlap with them, and grids step concurrently. Slot counts are sized from free device memory when a grid
+ * is added (admission by free HBM); a request waits on the host until its grid has a free slot. A system's
+ * arithmetic does not depend on its slot or on the other requests: a request's result is the same alone
+ * and in any mix. Outage requests start from the grid's solved base case when pf.warm_start_from_base is
+ * set; base-case requests (outage -1) start from the case's stored voltages, as gs_pf_solve does. */
+typedef struct gs_server gs_server;
+
+#define GS_SERVE_MAX_SLOTS 128
+
+typedef struct gs_serve_opts {
+    gs_pf_opts pf;             /* options of every request (precision, tolerance, iteration cap, warm start) */
+    int32_t slots_per_grid;    /* concurrent systems per grid, a multiple of 32, at most GS_SERVE_MAX_SLOTS; 0 = 128 */
+    int32_t state_slots;       /* solved states returned per grid and iteration; 0 = 16 */
+    double hbm_fraction;       /* share of the free device memory the slot batches may take; 0 = 0.5 */
+    int32_t reserved[8];
+} gs_serve_opts;
+
+typedef struct gs_request {
+    int32_t grid;              /* index from gs_serve_add_grid */
+    int32_t outage;            /* in-service branch index, -1 = the intact grid */
+    int32_t want_state;        /* return the solved Vm and Va */
+    int32_t reserved;
+    uint64_t tag;              /* the caller's, returned unchanged */
+} gs_request;
+
+typedef struct gs_response {
+    uint64_t ticket;           /* from gs_serve_submit */
+    uint64_t tag;
+    int32_t grid, outage;
+    int32_t status;            /* enum gs_pf_status */
+    int32_t iterations;
+    double max_mismatch;       /* pu */
+    double queue_ms;           /* submit -> admitted into a slot (host clock) */
+    double latency_ms;         /* submit -> result on the host */
+    int64_t state_offset;      /* Vm at state[state_offset + i], Va (degrees) at state[state_offset + n_bus + i]; -1 none */
+} gs_response;
+
+typedef struct gs_serve_stats {
+    int64_t submitted, completed, ticks;  /* ticks: Newton iterations stepped, over all grids */
+    int64_t system_steps;                 /* systems stepped, summed over ticks */
+    int32_t grids, slots_total, in_flight, queued;
+    double slot_bytes;                    /* device memory of the slot batches */
+    int32_t failed;                       /* a CUDA error stopped the loop (gs_last_error has it) */
+    int32_t reserved[7];
+} gs_serve_stats;
+
+int gs_serve_create(gs_ctx *ctx, const gs_serve_opts *opts, gs_server **out);
+/* Register a grid (before gs_serve_start): solves its base case when warm starts are on, sizes its slot
+ * batch from the memory budget (GS_ERR_OOM when not even 32 slots fit). The grid must outlive the server. */
+int gs_serve_add_grid(gs_server *srv, gs_grid *grid, int32_t *grid_index);
+int gs_serve_start(gs_server *srv);
+/* Queue n requests; tickets[n] (may be NULL) receives their tickets. The whole call is refused
+ * (GS_ERR_INVALID_ARG) if any request names an unknown grid or a branch that is not in service. */
+int gs_serve_submit(gs_server *srv, int32_t n, const gs_request *req, uint64_t *tickets);
+/* Take up to `max` finished requests, waiting up to timeout_ms for the first. States of requests that
+ * asked for them are copied into `state` (capacity in doubles); a response whose state does not fit stays
+ * queued for the next poll. */
+int gs_serve_poll(gs_server *srv, int32_t max, int32_t timeout_ms, gs_response *out, double *state,
+                  int64_t state_capacity, int32_t *got);
+int gs_serve_stats_get(gs_server *srv, gs_serve_stats *stats);
+/* Finish every queued and running request (their responses stay pollable), then stop the loop;
+ * GS_ERR_TIMEOUT if that takes longer than timeout_ms (the loop is stopped anyway). */
+int gs_serve_stop(gs_server *srv, int32_t timeout_ms);
+int gs_serve_destroy(gs_server *srv);
+
 /* ---- allocation-free mismatch check (no counterpart in the reference) ---------------------
  * For callers that cannot allocate device memory where they need the check: a loop whose device memory all
  * comes from its own pool, or code running while a stream is captured into a CUDA graph, where cudaMalloc
