@@ -207,11 +207,50 @@ def batched_rps(ctx, grids, reqs, precision):
     return len(reqs) / (time.perf_counter() - t)
 
 
-def run_serving(ctx, workers):
+def run_uneven(ctx, grids, steps=3):
+    """4,096 independent load flows (64 load scalings of each of the 64 grids: a global U(0.7, 1.3) times per-bus
+    lognormal sigma 0.05), FP32 factor with FP64 mismatch, in one persistent graph-captured launch
+    (gs_pf_solve_multi, CTA shape autotuned on the first call); beside it the same cases through the per-grid
+    batched path (one gs_pf_solve_batch per grid) in both precisions."""
+    from gridsim_b200 import synthetic
+    from gridsim_b200.engine import PowerFlowOptions, SparseNewtonRaphsonPowerFlow, UnevenBatch
+    scales = [synthetic.load_scalings(m, 64, k) for k, m in enumerate(grids)]
+    counts = [64] * len(grids)
+    out = {"workload": "4,096 load flows: 64 load scalings of each of 64 synthetic grids (100-25,000 buses)"}
+    batch = UnevenBatch(grids, ctx)
+    try:
+        for prec in ("mixed", "fp64"):
+            opt = PowerFlowOptions(precision=prec, max_iterations=20)
+            r = batch.solve(counts, scales, None, opt)  # autotunes on this first call
+            tune = dict(batch.stats)
+            dev, wall = [], []
+            for _ in range(steps):
+                t = time.perf_counter()
+                r = batch.solve(counts, scales, None, opt)
+                wall.append(time.perf_counter() - t)
+                dev.append(batch.stats["device_ms"])
+            conv = int(sum(int((s == 0).sum()) for s in r["status"]))
+            out[prec] = {"load_flows_per_s": conv / (float(np.median(dev)) / 1e3), "device_ms": float(np.median(dev)),
+                         "e2e_load_flows_per_s": conv / float(np.median(wall)), "converged": conv,
+                         "threads_per_cta": tune["threads_per_cta"], "ctas": tune["ctas"], "tune_ms": tune["tune_ms"],
+                         "newton_steps": batch.stats["system_steps"]}
+    finally:
+        batch.close()
+    for prec in ("mixed", "fp64"):
+        opt = PowerFlowOptions(precision=prec, max_iterations=20)
+        solvers = [SparseNewtonRaphsonPowerFlow(prec, ctx) for _ in grids]
+        for g, m in enumerate(grids):
+            solvers[g].solve_batch(m, load_scale=scales[g], options=opt)
+        t = time.perf_counter()
+        conv = 0
+        for g, m in enumerate(grids):
+            conv += int((solvers[g].solve_batch(m, load_scale=scales[g], options=opt)["status"] == 0).sum())
+        out[f"per_grid_batched_{prec}_load_flows_per_s"] = conv / (time.perf_counter() - t)
+    return out
+
+
+def run_serving(ctx, grids, outs, gen_s):
     from gridsim_b200.serving import LoadFlowServer, drain
-    t = time.perf_counter()
-    grids, outs = serve_population(workers)
-    gen_s = time.perf_counter() - t
     srv = LoadFlowServer(options("mixed"), ctx)
     for m in grids:
         srv.add_grid(m)
@@ -356,9 +395,13 @@ def run_ours(args):
                "max_dva_rad": float(np.max(np.abs(np.radians(g["va_deg"][cv] - o["va_deg"][cv])))),
                "violations_identical": bool(np.array_equal(g["viol_element"], o["viol_element"]) and
                                             np.array_equal(g["viol_kind"], o["viol_kind"]))}
-    serving, head = None, None
+    serving, head, uneven = None, None, None
     if rank == 0 and not args.no_serve:
-        serving, head = run_serving(ctx, os.cpu_count() or 1)
+        t = time.perf_counter()
+        grids, outs = serve_population(os.cpu_count() or 1)
+        gen_s = time.perf_counter() - t
+        uneven = run_uneven(ctx, grids)
+        serving, head = run_serving(ctx, grids, outs, gen_s)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, k, dt = cpu_sample(m, idx, os.cpu_count() or 1)
@@ -394,6 +437,7 @@ def run_ours(args):
             "serve_p99_ms": head["p99_ms"] if head else None,
             "serve_rate_rps": SERVE_HEADLINE_RATE if head else None,
             "serving": serving,
+            "uneven_batch": uneven,
         }
         print(json.dumps(line), flush=True)
     if dist:

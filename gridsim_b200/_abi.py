@@ -77,6 +77,12 @@ class GridInfo(ctypes.Structure):
     ]
 
 
+class MultiStats(ctypes.Structure):
+    _fields_ = [("device_ms", c_f64), ("tune_ms", c_f64), ("threads_per_cta", c_i32), ("ctas", c_i32),
+                ("items", c_i32), ("tuned_now", c_i32), ("system_steps", ctypes.c_int64), ("shared_top", c_i32),
+                ("reserved", c_i32 * 7)]
+
+
 class ServeOpts(ctypes.Structure):
     _fields_ = [("pf", PfOpts), ("slots_per_grid", c_i32), ("state_slots", c_i32), ("hbm_fraction", c_f64),
                 ("reserved", c_i32 * 8)]
@@ -116,6 +122,8 @@ EXPORTS = {
     "gs_n1_screen": (c_i32, [c_vp, c_i32, c_vp, ctypes.POINTER(PfOpts), ctypes.POINTER(N1Result)]),
     "gs_analyze_host": (c_i32, [ctypes.POINTER(GridDesc), ctypes.POINTER(GridInfo)]),
     "gs_pf_mismatch_noalloc": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp]),
+    "gs_pf_solve_multi": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(PfOpts), c_vp, c_vp, c_vp, c_vp,
+                                  c_vp, ctypes.POINTER(MultiStats)]),
     "gs_serve_create": (c_i32, [c_vp, ctypes.POINTER(ServeOpts), ctypes.POINTER(c_vp)]),
     "gs_serve_add_grid": (c_i32, [c_vp, c_vp, ctypes.POINTER(c_i32)]),
     "gs_serve_start": (c_i32, [c_vp]),

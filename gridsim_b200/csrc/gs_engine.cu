@@ -27,6 +27,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -54,24 +55,56 @@ __device__ __forceinline__ int sysAt(int idx, const int* list, int nList) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// 1. mismatch + Jacobian fill. Block (32, 8): lane = system, y = bus within the block.
+// 1. mismatch + Jacobian fill of bus i of system s: injections over row i of Y (the outaged branch's four cells
+//    replaced by their reduced values), the mismatch into the right-hand side (and its FP64 copy in mixed
+//    precision), the Jacobian blocks of row i into their LU slots; folds |mismatch| into localMax and sets bad
+//    (1: mismatch not finite, 2: Jacobian not finite).
 template <typename T>
-__global__ void __launch_bounds__(256) k_mismatch_jac(DevGrid g, DevBatch b, int fillJac, double* pOut, double* qOut,
-                                                      const int* list, int nList) {
-    const int lane = threadIdx.x, w = threadIdx.y;
-    const int s = sysAt(blockIdx.y * 32 + lane, list, nList);
-    const int i = blockIdx.x * 8 + w;
+__device__ __forceinline__ void busMismatchJac(const DevGrid& g, const DevBatch& b, int i, int s, int fillJac, double* pOut,
+                                               double* qOut, double& localMax, int& bad) {
     const size_t B = (size_t)b.B;
-    double localMax = 0.0;
-    int bad = 0;  // 1: mismatch not finite, 2: Jacobian not finite
-    const bool live = i < g.n && s >= 0 && s < b.count && b.active[s];
-    if (live) {
-        const int o = b.outage[s];
-        int c0 = -1, c1 = -1, c2 = -1, c3 = -1;
-        if (o >= 0) { c0 = g.brCell[4 * o]; c1 = g.brCell[4 * o + 1]; c2 = g.brCell[4 * o + 2]; c3 = g.brCell[4 * o + 3]; }
-        const double vmi = b.vm[i * B + s], vai = b.va[i * B + s];
-        double pi = 0.0, qi = 0.0;
-        const int p0 = g.yRowPtr[i], p1 = g.yRowPtr[i + 1];
+    const int o = b.outage[s];
+    int c0 = -1, c1 = -1, c2 = -1, c3 = -1;
+    if (o >= 0) { c0 = g.brCell[4 * o]; c1 = g.brCell[4 * o + 1]; c2 = g.brCell[4 * o + 2]; c3 = g.brCell[4 * o + 3]; }
+    const double vmi = b.vm[i * B + s], vai = b.va[i * B + s];
+    double pi = 0.0, qi = 0.0;
+    const int p0 = g.yRowPtr[i], p1 = g.yRowPtr[i + 1];
+    for (int p = p0; p < p1; p++) {
+        const int j = g.yCol[p];
+        double G = g.yG[p], Bv = g.yB[p];
+        if (p == c0) { G = g.brRed[8 * o + 0]; Bv = g.brRed[8 * o + 1]; }
+        else if (p == c1) { G = g.brRed[8 * o + 2]; Bv = g.brRed[8 * o + 3]; }
+        else if (p == c2) { G = g.brRed[8 * o + 4]; Bv = g.brRed[8 * o + 5]; }
+        else if (p == c3) { G = g.brRed[8 * o + 6]; Bv = g.brRed[8 * o + 7]; }
+        double sn, cs;
+        sincos(vai - b.va[j * B + s], &sn, &cs);
+        const double vmj = b.vm[j * B + s];
+        pi += vmj * (G * cs + Bv * sn);
+        qi += vmj * (G * sn - Bv * cs);
+    }
+    const double P = vmi * pi, Q = vmi * qi;
+    if (pOut) { pOut[i * B + s] = P; qOut[i * B + s] = Q; }
+    double sc = b.loadScale ? b.loadScale[i * B + s] : 1.0;
+    const double pspec = b.loadScale ? g.pgen[i] - sc * g.pload[i] : g.pgen[i] - g.pload[i];
+    const double qspec = b.loadScale ? g.qgen[i] - sc * g.qload[i] : g.qgen[i] - g.qload[i];
+    T* y = (T*)b.y;
+    const int kp = g.busP[i], kq = g.busQ[i];
+    if (kp >= 0) {
+        const double f = pspec - P;
+        y[kp * B + s] = (T)f;
+        if (b.rhs64) b.rhs64[kp * B + s] = f;
+        localMax = fmax(localMax, fabs(f));
+        bad |= isfinite(f) ? 0 : 1;
+    }
+    if (kq >= 0) {
+        const double f = qspec - Q;
+        y[kq * B + s] = (T)f;
+        if (b.rhs64) b.rhs64[kq * B + s] = f;
+        localMax = fmax(localMax, fabs(f));
+        bad |= isfinite(f) ? 0 : 1;
+    }
+    if (fillJac && (kp >= 0 || kq >= 0)) {
+        T* lu = (T*)b.lu;
         for (int p = p0; p < p1; p++) {
             const int j = g.yCol[p];
             double G = g.yG[p], Bv = g.yB[p];
@@ -79,65 +112,43 @@ __global__ void __launch_bounds__(256) k_mismatch_jac(DevGrid g, DevBatch b, int
             else if (p == c1) { G = g.brRed[8 * o + 2]; Bv = g.brRed[8 * o + 3]; }
             else if (p == c2) { G = g.brRed[8 * o + 4]; Bv = g.brRed[8 * o + 5]; }
             else if (p == c3) { G = g.brRed[8 * o + 6]; Bv = g.brRed[8 * o + 7]; }
-            double sn, cs;
-            sincos(vai - b.va[j * B + s], &sn, &cs);
-            const double vmj = b.vm[j * B + s];
-            pi += vmj * (G * cs + Bv * sn);
-            qi += vmj * (G * sn - Bv * cs);
-        }
-        const double P = vmi * pi, Q = vmi * qi;
-        if (pOut) { pOut[i * B + s] = P; qOut[i * B + s] = Q; }
-        double sc = b.loadScale ? b.loadScale[i * B + s] : 1.0;
-        const double pspec = b.loadScale ? g.pgen[i] - sc * g.pload[i] : g.pgen[i] - g.pload[i];
-        const double qspec = b.loadScale ? g.qgen[i] - sc * g.qload[i] : g.qgen[i] - g.qload[i];
-        T* y = (T*)b.y;
-        const int kp = g.busP[i], kq = g.busQ[i];
-        if (kp >= 0) {
-            const double f = pspec - P;
-            y[kp * B + s] = (T)f;
-            if (b.rhs64) b.rhs64[kp * B + s] = f;
-            localMax = fmax(localMax, fabs(f));
-            bad |= isfinite(f) ? 0 : 1;
-        }
-        if (kq >= 0) {
-            const double f = qspec - Q;
-            y[kq * B + s] = (T)f;
-            if (b.rhs64) b.rhs64[kq * B + s] = f;
-            localMax = fmax(localMax, fabs(f));
-            bad |= isfinite(f) ? 0 : 1;
-        }
-        if (fillJac && (kp >= 0 || kq >= 0)) {
-            T* lu = (T*)b.lu;
-            for (int p = p0; p < p1; p++) {
-                const int j = g.yCol[p];
-                double G = g.yG[p], Bv = g.yB[p];
-                if (p == c0) { G = g.brRed[8 * o + 0]; Bv = g.brRed[8 * o + 1]; }
-                else if (p == c1) { G = g.brRed[8 * o + 2]; Bv = g.brRed[8 * o + 3]; }
-                else if (p == c2) { G = g.brRed[8 * o + 4]; Bv = g.brRed[8 * o + 5]; }
-                else if (p == c3) { G = g.brRed[8 * o + 6]; Bv = g.brRed[8 * o + 7]; }
-                double H, N, M, L;
-                if (i == j) {
-                    H = -Q - Bv * vmi * vmi;
-                    N = P / vmi + G * vmi;
-                    M = P - G * vmi * vmi;
-                    L = Q / vmi - Bv * vmi;
-                } else {
-                    double sn, cs;
-                    sincos(vai - b.va[j * B + s], &sn, &cs);
-                    const double vmj = b.vm[j * B + s];
-                    H = vmi * vmj * (G * sn - Bv * cs);
-                    N = vmi * (G * cs + Bv * sn);
-                    M = -vmi * vmj * (G * cs + Bv * sn);
-                    L = vmi * (G * sn - Bv * cs);
-                }
-                const int4 sl = *reinterpret_cast<const int4*>(g.ySlot + 4 * p);
-                if (sl.x >= 0) lu[sl.x * B + s] = (T)H;
-                if (sl.y >= 0) lu[sl.y * B + s] = (T)N;
-                if (sl.z >= 0) lu[sl.z * B + s] = (T)M;
-                if (sl.w >= 0) lu[sl.w * B + s] = (T)L;
-                bad |= (isfinite(H) && isfinite(N) && isfinite(M) && isfinite(L)) ? 0 : 2;
+            double H, N, M, L;
+            if (i == j) {
+                H = -Q - Bv * vmi * vmi;
+                N = P / vmi + G * vmi;
+                M = P - G * vmi * vmi;
+                L = Q / vmi - Bv * vmi;
+            } else {
+                double sn, cs;
+                sincos(vai - b.va[j * B + s], &sn, &cs);
+                const double vmj = b.vm[j * B + s];
+                H = vmi * vmj * (G * sn - Bv * cs);
+                N = vmi * (G * cs + Bv * sn);
+                M = -vmi * vmj * (G * cs + Bv * sn);
+                L = vmi * (G * sn - Bv * cs);
             }
+            const int4 sl = *reinterpret_cast<const int4*>(g.ySlot + 4 * p);
+            if (sl.x >= 0) lu[sl.x * B + s] = (T)H;
+            if (sl.y >= 0) lu[sl.y * B + s] = (T)N;
+            if (sl.z >= 0) lu[sl.z * B + s] = (T)M;
+            if (sl.w >= 0) lu[sl.w * B + s] = (T)L;
+            bad |= (isfinite(H) && isfinite(N) && isfinite(M) && isfinite(L)) ? 0 : 2;
         }
+    }
+}
+
+// The batched kernel. Block (32, 8): lane = system, y = bus within the block.
+template <typename T>
+__global__ void __launch_bounds__(256) k_mismatch_jac(DevGrid g, DevBatch b, int fillJac, double* pOut, double* qOut,
+                                                      const int* list, int nList) {
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int s = sysAt(blockIdx.y * 32 + lane, list, nList);
+    const int i = blockIdx.x * 8 + w;
+    double localMax = 0.0;
+    int bad = 0;  // 1: mismatch not finite, 2: Jacobian not finite
+    const bool live = i < g.n && s >= 0 && s < b.count && b.active[s];
+    if (live) {
+        busMismatchJac<T>(g, b, i, s, fillJac, pOut, qOut, localMax, bad);
     }
     __shared__ double red[8][32];
     __shared__ int redBad[8][32];
@@ -285,18 +296,26 @@ __device__ __forceinline__ T dotSerial(const T* __restrict__ lu, const T* __rest
     return acc;
 }
 
+// Work descriptors (one int4 per schedule position, so that a piece of work costs one 16-byte load before its
+// pairs): an entry of the factorisation or the forward substitution is {slot (or y index), first pair, end of
+// pairs, kind | hasA << 2 | node << 3}; a node of the backward substitution is {node, LU base, |U row|, first
+// row index}.
+__device__ __forceinline__ int descKind(const int4& d) { return d.w & 3; }
+__device__ __forceinline__ bool descHasA(const int4& d) { return (d.w >> 2) & 1; }
+__device__ __forceinline__ int descNode(const int4& d) { return d.w >> 3; }
+
 // One entry of the fused factorisation: A - sum(left * right), divided by the node's pivot for lower entries;
 // the diagonal's result is the pivot (kept in its own array: the diagonal slot keeps A(k, k)). `wide`: the
 // whole warp computes this entry (pair lanes + butterfly), else this lane group alone.
 template <typename T>
-__device__ __forceinline__ void factorEntry(const DevGrid& g, const DevBatch& b, int e, int s, bool act, bool wide) {
+__device__ __forceinline__ void factorEntry(const DevGrid& g, const DevBatch& b, const int4 d, int s, bool act, bool wide) {
     const size_t B = (size_t)b.B;
     T* lu = (T*)b.lu;
     T* y = (T*)b.y;
-    const int kind = g.entKind[e];
-    const int slot = g.entSlot[e];
-    const int node = g.entNode[e];
-    const int64_t q0 = g.entPairPtr[e], q1 = g.entPairPtr[e + 1];
+    const int kind = descKind(d);
+    const int slot = d.x;
+    const int node = descNode(d);
+    const int64_t q0 = d.y, q1 = d.z;
     const T* rhs = kind == kFwd ? y : lu;
     const T dot = wide ? dotSP<T>(lu, rhs, g.pairs, q0, q1, B, s) : dotSerial<T>(lu, rhs, g.pairs, q0, q1, B, s);
     const bool writer = !wide || (threadIdx.x & 31) < Lay<T>::S;
@@ -305,7 +324,7 @@ __device__ __forceinline__ void factorEntry(const DevGrid& g, const DevBatch& b,
         if (writer) y[slot * B + s] = v;
         return;
     }
-    const T a = g.entHasA[e] ? lu[slot * B + s] : T(0);
+    const T a = descHasA(d) ? lu[slot * B + s] : T(0);
     T v = a - dot;
     if (kind == kDiag) {
         const T fl = pivotFloor<T>() * (fabs(a) > T(1) ? fabs(a) : T(1));
@@ -320,16 +339,16 @@ __device__ __forceinline__ void factorEntry(const DevGrid& g, const DevBatch& b,
     if (writer) lu[slot * B + s] = v;
 }
 
-// backward substitution of node levelNodes[q]: x(k) = (y(k) - sum U(k, r) x(r)) / U(k, k), in place
+// backward substitution of a node: x(k) = (y(k) - sum U(k, r) x(r)) / U(k, k), in place
 template <typename T>
-__device__ __forceinline__ void backwardNode(const DevGrid& g, const DevBatch& b, T* y, int q, int s, bool wide) {
+__device__ __forceinline__ void backwardNode(const DevGrid& g, const DevBatch& b, T* y, const int4 d, int s, bool wide) {
     constexpr int S = Lay<T>::S, P = Lay<T>::P;
     const size_t B = (size_t)b.B;
     const T* lu = (const T*)b.lu;
-    const int k = g.levelNodes[q];
-    const int64_t base = g.luBase[k];
-    const int c = g.luCnt[k];
-    const int* rows = g.pRows + g.pRowPtr[k];
+    const int k = d.x;
+    const int64_t base = d.y;
+    const int c = d.z;
+    const int* rows = g.pRows + d.w;
     T acc = T(0);
     if (wide) {
         const int lane = threadIdx.x & 31;
@@ -367,10 +386,10 @@ __device__ __forceinline__ void backwardNode(const DevGrid& g, const DevBatch& b
 
 // forward substitution of a second right-hand side v: v(k) -= sum L(k, j) v(j), with node k's forward entry
 template <typename T>
-__device__ __forceinline__ void forwardEntry(const DevGrid& g, const DevBatch& b, T* v, int e, int s, bool wide) {
+__device__ __forceinline__ void forwardEntry(const DevGrid& g, const DevBatch& b, T* v, const int4 d, int s, bool wide) {
     const size_t B = (size_t)b.B;
-    const int k = g.entNode[e];
-    const int64_t q0 = g.entPairPtr[e], q1 = g.entPairPtr[e + 1];
+    const int k = descNode(d);
+    const int64_t q0 = d.y, q1 = d.z;
     const T* lu = (const T*)b.lu;
     const T dot = wide ? dotSP<T>(lu, v, g.pairs, q0, q1, B, s) : dotSerial<T>(lu, v, g.pairs, q0, q1, B, s);
     const T r = v[k * B + s] - dot;
@@ -383,12 +402,12 @@ __device__ __forceinline__ int laneSystem(int grp) { return grp * Lay<T>::S + ((
 
 // Run one work item: a wide piece by the whole warp, or up to `count` short pieces over the lane groups.
 template <typename T, typename F>
-__device__ __forceinline__ void runItem(const int* __restrict__ work, const int* __restrict__ items, int it, F&& f) {
+__device__ __forceinline__ void runItem(const int4* __restrict__ desc, const int* __restrict__ items, int it, F&& f) {
     const int start = __ldg(items + 2 * it), count = __ldg(items + 2 * it + 1);
     if (count < 0) {
-        f(__ldg(work + start), true);
+        f(__ldg(desc + start), true);
     } else {
-        for (int p = (threadIdx.x & 31) / Lay<T>::S; p < count; p += Lay<T>::P) f(__ldg(work + start + p), false);
+        for (int p = (threadIdx.x & 31) / Lay<T>::S; p < count; p += Lay<T>::P) f(__ldg(desc + start + p), false);
     }
 }
 
@@ -397,11 +416,11 @@ enum WhichWork { kWorkFactor = 0, kWorkBackward = 1, kWorkForward = 2 };
 template <typename T, int W>
 __device__ __forceinline__ void doItem(const DevGrid& g, const DevBatch& b, T* vec, int it, int s, bool act) {
     if (W == kWorkFactor)
-        runItem<T>(g.fWork, g.fItems, it, [&](int e, bool wide) { factorEntry<T>(g, b, e, s, act, wide); });
+        runItem<T>(g.fDesc, g.fItems, it, [&](const int4 d, bool wide) { factorEntry<T>(g, b, d, s, act, wide); });
     else if (W == kWorkBackward)
-        runItem<T>(g.bWork, g.bItems, it, [&](int q, bool wide) { backwardNode<T>(g, b, vec, q, s, wide); });
+        runItem<T>(g.bDesc, g.bItems, it, [&](const int4 d, bool wide) { backwardNode<T>(g, b, vec, d, s, wide); });
     else
-        runItem<T>(g.vWork, g.vItems, it, [&](int e, bool wide) { forwardEntry<T>(g, b, vec, e, s, wide); });
+        runItem<T>(g.vDesc, g.vItems, it, [&](const int4 d, bool wide) { forwardEntry<T>(g, b, vec, d, s, wide); });
 }
 
 // One level (or phase) of a schedule, items [i0, i1): block (32, 4), a warp per item, S systems per warp.
@@ -445,11 +464,7 @@ __global__ void __launch_bounds__(32 * kPersistWarps) k_persistent(DevGrid g, De
 // (the same H/N/M/L expressions as the fill). The correction solve of r with the same FP32 factors makes the
 // step accurate to ~(kappa * 2^-24)^2, so the Newton path follows the FP64 path and stops where it stops.
 template <typename T>
-__global__ void __launch_bounds__(256) k_residual(DevGrid g, DevBatch b, const int* list, int nList) {
-    const int lane = threadIdx.x, w = threadIdx.y;
-    const int s = sysAt(blockIdx.y * 32 + lane, list, nList);
-    const int i = blockIdx.x * 8 + w;
-    if (i >= g.n || s < 0 || s >= b.count || !b.active[s]) return;
+__device__ __forceinline__ void busResidual(const DevGrid& g, const DevBatch& b, int i, int s) {
     const size_t B = (size_t)b.B;
     const int kp = g.busP[i], kq = g.busQ[i];
     if (kp < 0 && kq < 0) return;
@@ -511,6 +526,15 @@ __global__ void __launch_bounds__(256) k_residual(DevGrid g, DevBatch b, const i
     }
     if (kp >= 0) z[kp * B + s] = (T)(b.rhs64[kp * B + s] - jp);
     if (kq >= 0) z[kq * B + s] = (T)(b.rhs64[kq * B + s] - jq);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_residual(DevGrid g, DevBatch b, const int* list, int nList) {
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int s = sysAt(blockIdx.y * 32 + lane, list, nList);
+    const int i = blockIdx.x * 8 + w;
+    if (i >= g.n || s < 0 || s >= b.count || !b.active[s]) return;
+    busResidual<T>(g, b, i, s);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -592,15 +616,15 @@ __device__ __forceinline__ T dotWarp1(const T* __restrict__ lu, const T* __restr
 
 // The few-systems path's wide pieces: one system, one warp.
 template <typename T>
-__device__ __forceinline__ void factorEntryWarp1(const DevGrid& g, const DevBatch& b, int e, int s) {
+__device__ __forceinline__ void factorEntryWarp1(const DevGrid& g, const DevBatch& b, const int4 d, int s) {
     const size_t B = (size_t)b.B;
     T* lu = (T*)b.lu;
     T* y = (T*)b.y;
-    const int kind = g.entKind[e], slot = g.entSlot[e], node = g.entNode[e];
-    const T dot = dotWarp1<T>(lu, kind == kFwd ? y : lu, g.pairs, g.entPairPtr[e], g.entPairPtr[e + 1], B, s);
+    const int kind = descKind(d), slot = d.x, node = descNode(d);
+    const T dot = dotWarp1<T>(lu, kind == kFwd ? y : lu, g.pairs, d.y, d.z, B, s);
     if ((threadIdx.x & 31) != 0) return;
     if (kind == kFwd) { y[slot * B + s] -= dot; return; }
-    const T a = g.entHasA[e] ? lu[slot * B + s] : T(0);
+    const T a = descHasA(d) ? lu[slot * B + s] : T(0);
     T v = a - dot;
     if (kind == kDiag) {
         const T fl = pivotFloor<T>() * (fabs(a) > T(1) ? fabs(a) : T(1));
@@ -613,13 +637,13 @@ __device__ __forceinline__ void factorEntryWarp1(const DevGrid& g, const DevBatc
 }
 
 template <typename T>
-__device__ __forceinline__ void backwardNodeWarp1(const DevGrid& g, const DevBatch& b, T* y, int q, int s) {
+__device__ __forceinline__ void backwardNodeWarp1(const DevGrid& g, const DevBatch& b, T* y, const int4 d, int s) {
     const size_t B = (size_t)b.B;
     const T* lu = (const T*)b.lu;
-    const int k = g.levelNodes[q];
-    const int64_t base = g.luBase[k];
-    const int c = g.luCnt[k];
-    const int* rows = g.pRows + g.pRowPtr[k];
+    const int k = d.x;
+    const int64_t base = d.y;
+    const int c = d.z;
+    const int* rows = g.pRows + d.w;
     constexpr int U = 4;
     T acc = T(0);
     for (int t = threadIdx.x & 31; t < c; t += 32 * U) {
@@ -642,37 +666,37 @@ __device__ __forceinline__ void backwardNodeWarp1(const DevGrid& g, const DevBat
 }
 
 template <typename T>
-__device__ __forceinline__ void forwardEntryWarp1(const DevGrid& g, const DevBatch& b, T* v, int e, int s) {
+__device__ __forceinline__ void forwardEntryWarp1(const DevGrid& g, const DevBatch& b, T* v, const int4 d, int s) {
     const size_t B = (size_t)b.B;
-    const int k = g.entNode[e];
-    const T dot = dotWarp1<T>((const T*)b.lu, v, g.pairs, g.entPairPtr[e], g.entPairPtr[e + 1], B, s);
+    const int k = descNode(d);
+    const T dot = dotWarp1<T>((const T*)b.lu, v, g.pairs, d.y, d.z, B, s);
     if ((threadIdx.x & 31) == 0) v[k * B + s] -= dot;
 }
 
+// One system, the whole block: every level (top down for the backward substitution) and phase of a schedule,
+// the wide pieces a warp each, the short pieces a thread each, a block barrier between levels and phases.
 template <typename T, int W>
-__global__ void __launch_bounds__(kTailThreads) k_tail(DevGrid g, DevBatch b, T* vec) {
-    const int s = b.activeList[blockIdx.x];
-    if (W != kWorkFactor && vec != (T*)b.y && !b.refine[s]) return;  // uniform across the block
+__device__ __forceinline__ void walkLevels(const DevGrid& g, const DevBatch& b, T* vec, int s, int l0, int l1) {
     const int* ptr = W == kWorkFactor ? g.fWorkPtr : (W == kWorkBackward ? g.bWorkPtr : g.vWorkPtr);
-    const int* work = W == kWorkFactor ? g.fWork : (W == kWorkBackward ? g.bWork : g.vWork);
+    const int4* desc = W == kWorkFactor ? g.fDesc : (W == kWorkBackward ? g.bDesc : g.vDesc);
     const int* wide = W == kWorkFactor ? g.fWide : (W == kWorkBackward ? g.bWide : g.vWide);
     const int phases = W == kWorkFactor ? 2 : 1;
     const int warp = threadIdx.x >> 5;
-    for (int step = 0; step < b.nLevels; step++) {
-        const int l = W == kWorkBackward ? b.nLevels - 1 - step : step;
+    for (int step = 0; step < l1 - l0; step++) {
+        const int l = W == kWorkBackward ? l1 - 1 - step : l0 + step;
         for (int ph = 0; ph < phases; ph++) {
             const int i = phases * l + ph;
             const int w0 = ptr[i], w1 = ptr[i + 1], nw = wide[i];
             // wide pieces (the first nw of the range): a warp each
-            for (int w = w0 + warp; w < w0 + nw; w += kTailThreads / 32) {
-                const int x = __ldg(work + w);
+            for (int w = w0 + warp; w < w0 + nw; w += (int)(blockDim.x >> 5)) {
+                const int4 x = __ldg(desc + w);
                 if (W == kWorkFactor) factorEntryWarp1<T>(g, b, x, s);
                 else if (W == kWorkBackward) backwardNodeWarp1<T>(g, b, vec, x, s);
                 else forwardEntryWarp1<T>(g, b, vec, x, s);
             }
             // short pieces: a thread each
-            for (int w = w0 + nw + threadIdx.x; w < w1; w += kTailThreads) {
-                const int x = __ldg(work + w);
+            for (int w = w0 + nw + (int)threadIdx.x; w < w1; w += (int)blockDim.x) {
+                const int4 x = __ldg(desc + w);
                 if (W == kWorkFactor) factorEntry<T>(g, b, x, s, true, false);
                 else if (W == kWorkBackward) backwardNode<T>(g, b, vec, x, s, false);
                 else forwardEntry<T>(g, b, vec, x, s, false);
@@ -680,6 +704,218 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(DevGrid g, DevBatch b, T*
             __syncthreads();
         }
     }
+}
+
+// ---- the top of the elimination tree in shared memory (levels >= L0 of the element size's DevTop) ----
+template <typename T>
+__device__ __forceinline__ const DevTop& topOf(const DevGrid& g) { return g.top[sizeof(T) == 4 ? 1 : 0]; }
+
+// sum over pairs [q0, q1) of sm[x] * sm[y], both operands in shared memory: one warp (fixed butterfly), or one thread
+template <typename T>
+__device__ __forceinline__ T smDotWarp(const T* sm, const int2* __restrict__ pr, int q0, int q1) {
+    T acc = T(0);
+    for (int q = q0 + (int)(threadIdx.x & 31); q < q1; q += 32) {
+        const int2 p = __ldg(pr + q);
+        acc += sm[p.x] * sm[p.y];
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    return acc;
+}
+
+template <typename T>
+__device__ __forceinline__ T smDotSerial(const T* sm, const int2* __restrict__ pr, int q0, int q1) {
+    T acc = T(0);
+    int q = q0;
+    for (; q + 4 <= q1; q += 4) {
+        const int2 a0 = __ldg(pr + q), a1 = __ldg(pr + q + 1), a2 = __ldg(pr + q + 2), a3 = __ldg(pr + q + 3);
+        acc += sm[a0.x] * sm[a0.y];
+        acc += sm[a1.x] * sm[a1.y];
+        acc += sm[a2.x] * sm[a2.y];
+        acc += sm[a3.x] * sm[a3.y];
+    }
+    for (; q < q1; q++) {
+        const int2 a = __ldg(pr + q);
+        acc += sm[a.x] * sm[a.y];
+    }
+    return acc;
+}
+
+// Top entries of `list` (the first nWide a warp each, the rest a thread each) start in shared memory from their
+// value (the right-hand side `rhs` for a forward entry, else A or 0) minus their external pairs, read from global.
+template <typename T>
+__device__ __forceinline__ void topLoad(const DevGrid& g, const DevBatch& b, const DevTop& t, T* sm, const T* rhs, int s,
+                                        const int* list, int nWide, int n) {
+    const size_t B = (size_t)b.B;
+    const T* lu = (const T*)b.lu;
+    const int warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5;
+    for (int q = warp; q < nWide; q += nWarps) {
+        const int ti = __ldg(list + q);
+        const int e = __ldg(t.ent + ti);
+        const bool fwd = g.entKind[e] == kFwd;
+        const T ext = dotWarp1<T>(lu, fwd ? rhs : lu, t.extPairs, __ldg(t.extPtr + ti), __ldg(t.extPtr + ti + 1), B, s);
+        if ((threadIdx.x & 31) == 0) {
+            const T base = fwd ? rhs[(size_t)g.entNode[e] * B + s] : (g.entHasA[e] ? lu[(size_t)g.entSlot[e] * B + s] : T(0));
+            sm[__ldg(t.entSm + ti)] = base - ext;
+        }
+    }
+    for (int q = nWide + (int)threadIdx.x; q < n; q += (int)blockDim.x) {
+        const int ti = __ldg(list + q);
+        const int e = __ldg(t.ent + ti);
+        const bool fwd = g.entKind[e] == kFwd;
+        const T ext = dotSerial<T>(lu, fwd ? rhs : lu, t.extPairs, __ldg(t.extPtr + ti), __ldg(t.extPtr + ti + 1), B, s);
+        const T base = fwd ? rhs[(size_t)g.entNode[e] * B + s] : (g.entHasA[e] ? lu[(size_t)g.entSlot[e] * B + s] : T(0));
+        sm[__ldg(t.entSm + ti)] = base - ext;
+    }
+}
+
+// the last step of a top entry of the factorisation: its value minus its internal dot; the pivot of a diagonal
+// (perturbed to the floor of |A(k, k)| when it collapses), a lower entry divided by its node's pivot
+template <typename T>
+__device__ __forceinline__ void topFinish(const DevGrid& g, const DevBatch& b, const DevTop& t, T* sm, int ti, T dot, int s) {
+    const int e = __ldg(t.ent + ti);
+    const int kind = g.entKind[e];
+    const int idx = __ldg(t.entSm + ti);
+    T v = sm[idx] - dot;
+    if (kind == kDiag) {
+        const T a = g.entHasA[e] ? ((const T*)b.lu)[(size_t)g.entSlot[e] * b.B + s] : T(0);
+        const T fl = pivotFloor<T>() * (fabs(a) > T(1) ? fabs(a) : T(1));
+        if (!(fabs(v) > fl)) {
+            atomicOr(&b.flags[s], kFlagPivotPerturbed);
+            v = (v < T(0)) ? -fl : fl;
+        }
+    } else if (kind == kLower) {
+        v = v / sm[__ldg(t.smemBase + g.entNode[e])];
+    }
+    sm[idx] = v;
+}
+
+// One system, the whole block: the fused factorisation + forward substitution. Levels below L0 walk global
+// memory; the top is loaded into shared memory `sm` (external pairs applied on the way), walked there, and
+// written back (U and L to the LU, pivots to piv, the forward-substituted right-hand side to y).
+template <typename T>
+__device__ void factorSystem(const DevGrid& g, const DevBatch& b, int s, T* sm, bool useTop) {
+    const DevTop& t = topOf<T>(g);
+    walkLevels<T, kWorkFactor>(g, b, (T*)b.y, s, 0, useTop ? t.L0 : g.nLevels);
+    if (!useTop || t.L0 >= g.nLevels) return;
+    const size_t B = (size_t)b.B;
+    T* lu = (T*)b.lu;
+    T* y = (T*)b.y;
+    T* piv = (T*)b.piv;
+    const int warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5, lane = threadIdx.x & 31;
+    topLoad<T>(g, b, t, sm, y, s, t.loadList, t.loadWide, t.nLoad);
+    __syncthreads();
+    const int nTop = g.nLevels - t.L0;
+    for (int i = 0; i < 2 * nTop; i++) {
+        const int w0 = __ldg(t.fWalkPtr + i), w1 = __ldg(t.fWalkPtr + i + 1), nw = __ldg(t.fWalkWide + i);
+        for (int w = w0 + warp; w < w0 + nw; w += nWarps) {
+            const int ti = __ldg(t.fWalk + w);
+            const T dot = smDotWarp<T>(sm, t.intPairs, __ldg(t.intPtr + ti), __ldg(t.intPtr + ti + 1));
+            if (lane == 0) topFinish<T>(g, b, t, sm, ti, dot, s);
+        }
+        for (int w = w0 + nw + (int)threadIdx.x; w < w1; w += (int)blockDim.x) {
+            const int ti = __ldg(t.fWalk + w);
+            topFinish<T>(g, b, t, sm, ti, smDotSerial<T>(sm, t.intPairs, __ldg(t.intPtr + ti), __ldg(t.intPtr + ti + 1)), s);
+        }
+        __syncthreads();
+    }
+    for (int q = threadIdx.x; q < t.nSlots; q += blockDim.x) {
+        const int node = __ldg(t.slotDiagNode + q);
+        if (node >= 0) piv[(size_t)node * B + s] = sm[q];
+        else lu[(size_t)__ldg(t.slotGlobal + q) * B + s] = sm[q];
+    }
+    for (int i = threadIdx.x; i < t.nNodes; i += blockDim.x) y[(size_t)__ldg(t.nodes + i) * B + s] = sm[t.nSlots + i];
+    __syncthreads();
+}
+
+// One system, the whole block: backward substitution of `vec` in place, the top in shared memory first.
+template <typename T>
+__device__ void backwardSystem(const DevGrid& g, const DevBatch& b, T* vec, int s, T* sm, bool useTop) {
+    const DevTop& t = topOf<T>(g);
+    const int L0 = useTop ? t.L0 : g.nLevels;
+    if (L0 < g.nLevels) {
+        const size_t B = (size_t)b.B;
+        const T* lu = (const T*)b.lu;
+        const T* piv = (const T*)b.piv;
+        const int warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5, lane = threadIdx.x & 31;
+        for (int q = threadIdx.x; q < t.nSlots; q += blockDim.x) {
+            const int node = __ldg(t.slotDiagNode + q);
+            sm[q] = node >= 0 ? piv[(size_t)node * B + s] : lu[(size_t)__ldg(t.slotGlobal + q) * B + s];
+        }
+        for (int i = threadIdx.x; i < t.nNodes; i += blockDim.x) sm[t.nSlots + i] = vec[(size_t)__ldg(t.nodes + i) * B + s];
+        __syncthreads();
+        const int nTop = g.nLevels - t.L0;
+        for (int lt = nTop - 1; lt >= 0; lt--) {
+            const int w0 = __ldg(t.bWalkPtr + lt), w1 = __ldg(t.bWalkPtr + lt + 1), nw = __ldg(t.bWalkWide + lt);
+            for (int w = w0 + warp; w < w0 + nw; w += nWarps) {
+                const int ni = __ldg(t.bWalk + w);
+                const int k = __ldg(t.nodes + ni), base = __ldg(t.smemBase + k), c = g.luCnt[k];
+                const int* rows = t.bRowSm + __ldg(t.bRowPtr + ni);
+                T acc = T(0);
+                for (int u = lane; u < c; u += 32) acc += sm[base + 1 + u] * sm[__ldg(rows + u)];
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+                if (lane == 0) sm[t.nSlots + ni] = (sm[t.nSlots + ni] - acc) / sm[base];
+            }
+            for (int w = w0 + nw + (int)threadIdx.x; w < w1; w += (int)blockDim.x) {
+                const int ni = __ldg(t.bWalk + w);
+                const int k = __ldg(t.nodes + ni), base = __ldg(t.smemBase + k), c = g.luCnt[k];
+                const int* rows = t.bRowSm + __ldg(t.bRowPtr + ni);
+                T acc = T(0);
+                for (int u = 0; u < c; u++) acc += sm[base + 1 + u] * sm[__ldg(rows + u)];
+                sm[t.nSlots + ni] = (sm[t.nSlots + ni] - acc) / sm[base];
+            }
+            __syncthreads();
+        }
+        for (int i = threadIdx.x; i < t.nNodes; i += blockDim.x) vec[(size_t)__ldg(t.nodes + i) * B + s] = sm[t.nSlots + i];
+        __syncthreads();
+    }
+    walkLevels<T, kWorkBackward>(g, b, vec, s, 0, L0);
+}
+
+// One system, the whole block: forward substitution of a second right-hand side `vec` in place.
+template <typename T>
+__device__ void forwardSystem(const DevGrid& g, const DevBatch& b, T* vec, int s, T* sm, bool useTop) {
+    const DevTop& t = topOf<T>(g);
+    walkLevels<T, kWorkForward>(g, b, vec, s, 0, useTop ? t.L0 : g.nLevels);
+    if (!useTop || t.L0 >= g.nLevels) return;
+    const size_t B = (size_t)b.B;
+    const T* lu = (const T*)b.lu;
+    const int warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5, lane = threadIdx.x & 31;
+    for (int q = threadIdx.x; q < t.nSlots; q += blockDim.x) sm[q] = lu[(size_t)__ldg(t.slotGlobal + q) * B + s];
+    topLoad<T>(g, b, t, sm, vec, s, t.fwdLoadList, t.fwdLoadWide, t.nFwdLoad);
+    __syncthreads();
+    const int nTop = g.nLevels - t.L0;
+    for (int lt = 0; lt < nTop; lt++) {
+        const int w0 = __ldg(t.vWalkPtr + lt), w1 = __ldg(t.vWalkPtr + lt + 1), nw = __ldg(t.vWalkWide + lt);
+        for (int w = w0 + warp; w < w0 + nw; w += nWarps) {
+            const int ti = __ldg(t.vWalk + w);
+            const T dot = smDotWarp<T>(sm, t.intPairs, __ldg(t.intPtr + ti), __ldg(t.intPtr + ti + 1));
+            if (lane == 0) sm[__ldg(t.entSm + ti)] -= dot;
+        }
+        for (int w = w0 + nw + (int)threadIdx.x; w < w1; w += (int)blockDim.x) {
+            const int ti = __ldg(t.vWalk + w);
+            sm[__ldg(t.entSm + ti)] -= smDotSerial<T>(sm, t.intPairs, __ldg(t.intPtr + ti), __ldg(t.intPtr + ti + 1));
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < t.nNodes; i += blockDim.x) vec[(size_t)__ldg(t.nodes + i) * B + s] = sm[t.nSlots + i];
+    __syncthreads();
+}
+
+// Dynamic shared memory of the one-system kernels (the top part of the grid's schedule).
+extern __shared__ __align__(16) unsigned char gsTopSmem[];
+
+// useTop: the top part in shared memory (launched with its bytes of dynamic shared memory), else every level in
+// global memory (the larger L1 then keeps more of the system's LU close).
+template <typename T, int W>
+__global__ void __launch_bounds__(kTailThreads) k_tail(DevGrid g, DevBatch b, T* vec, int useTop) {
+    const int s = b.activeList[blockIdx.x];
+    if (W != kWorkFactor && vec != (T*)b.y && !b.refine[s]) return;  // uniform across the block
+    T* sm = reinterpret_cast<T*>(gsTopSmem);
+    if (W == kWorkFactor) factorSystem<T>(g, b, s, sm, useTop != 0);
+    else if (W == kWorkBackward) backwardSystem<T>(g, b, vec, s, sm, useTop != 0);
+    else forwardSystem<T>(g, b, vec, s, sm, useTop != 0);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -716,13 +952,9 @@ __global__ void __launch_bounds__(256) k_dxmax(DevGrid g, DevBatch b, int rowsPe
     }
 }
 
+// the damped update of bus i of system s (the system's max |dx| is in maxDx); bus 0 counts the step
 template <typename T>
-__global__ void __launch_bounds__(256) k_update(DevGrid g, DevBatch b, int refine, const int* list, int nList) {
-    const int lane = threadIdx.x;
-    const int s = sysAt(blockIdx.y * 32 + lane, list, nList);
-    const int i = blockIdx.x * 8 + threadIdx.y;
-    if (i >= g.n || s < 0 || s >= b.count || !b.active[s]) return;
-    if (b.flags[s] & kFlagStepBad) return;
+__device__ __forceinline__ void busUpdate(const DevGrid& g, const DevBatch& b, int i, int s, int refine) {
     const size_t B = (size_t)b.B;
     const T* y = (const T*)b.y;
     const T* z = (const T*)b.z;
@@ -737,6 +969,16 @@ __global__ void __launch_bounds__(256) k_update(DevGrid g, DevBatch b, int refin
         b.vm[i * B + s] = v;
     }
     if (i == 0) b.iters[s] += 1;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_update(DevGrid g, DevBatch b, int refine, const int* list, int nList) {
+    const int lane = threadIdx.x;
+    const int s = sysAt(blockIdx.y * 32 + lane, list, nList);
+    const int i = blockIdx.x * 8 + threadIdx.y;
+    if (i >= g.n || s < 0 || s >= b.count || !b.active[s]) return;
+    if (b.flags[s] & kFlagStepBad) return;
+    busUpdate<T>(g, b, i, s, refine);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -934,6 +1176,7 @@ struct gs_ctx {
     std::mutex mu;
     cudaStream_t stream = nullptr;
     int* pinnedCount = nullptr;
+    std::map<std::string, int> multiTune;  // the multi-grid batch's CTA shape per set of grids (autotuned)
 };
 
 struct gs_grid {
@@ -980,7 +1223,7 @@ int UploadGrid(gs_grid* G) {
     const HostGrid& h = G->host;
     const Symbolic& s = G->sym;
     DevGrid& v = G->view;
-    v.n = s.n; v.m = s.m; v.nnzY = s.nnzY; v.nbr = s.nbr; v.nnzLU = s.nnzLU;
+    v.n = s.n; v.m = s.m; v.nnzY = s.nnzY; v.nbr = s.nbr; v.nnzLU = s.nnzLU; v.nLevels = s.nLevels;
     const int n = h.n;
     G->pgen.assign(n, 0.0); G->qgen.assign(n, 0.0);
     for (int k = 0; k < h.ngen; k++) {
@@ -1008,11 +1251,45 @@ int UploadGrid(gs_grid* G) {
     UP(s.entPairPtr, entPairPtr); UP(pairs, pairs); UP(s.diagPairNode, diagEnt); UP(s.levelNodes, levelNodes);
     UP(s.luBase, luBase); UP(s.luCnt, luCnt); UP(s.pRowPtr, pRowPtr); UP(s.pRows, pRows);
     UP(s.levelNodePtr, levelNodePtr); UP(s.entNode, entNode);
+    {
+        // work descriptors, one per schedule position
+        auto entDesc = [&](int e) {
+            return make_int4(s.entSlot[e], (int)s.entPairPtr[e], (int)s.entPairPtr[e + 1],
+                             s.entKind[e] | (s.entHasA[e] << 2) | (s.entNode[e] << 3));
+        };
+        std::vector<int4> fd, vd, bd;
+        for (int e : s.factor.work) fd.push_back(entDesc(e));
+        for (int e : s.forward.work) vd.push_back(entDesc(e));
+        for (int q : s.backward.work) {
+            const int k = s.levelNodes[q];
+            bd.push_back(make_int4(k, (int)s.luBase[k], s.luCnt[k], s.pRowPtr[k]));
+        }
+        UP(fd, fDesc); UP(vd, vDesc); UP(bd, bDesc);
+    }
     UP(s.factor.work, fWork); UP(s.factor.items, fItems); UP(s.factor.levelItemPtr, fLevelPtr);
     UP(s.backward.work, bWork); UP(s.backward.items, bItems); UP(s.backward.levelItemPtr, bLevelPtr);
     UP(s.forward.work, vWork); UP(s.forward.items, vItems); UP(s.forward.levelItemPtr, vLevelPtr);
     UP(s.factor.levelWorkPtr, fWorkPtr); UP(s.backward.levelWorkPtr, bWorkPtr); UP(s.forward.levelWorkPtr, vWorkPtr);
     UP(s.factor.levelWide, fWide); UP(s.backward.levelWide, bWide); UP(s.forward.levelWide, vWide);
+    for (int w = 0; w < 2; w++) {
+        const Symbolic::TopPart& t = s.top[w];
+        DevTop& d = v.top[w];
+        d.L0 = t.L0; d.nSlots = t.nSlots; d.nNodes = t.nNodes; d.nEnt = (int)t.ent.size();
+        d.loadWide = t.loadWide; d.nLoad = (int)t.loadList.size();
+        d.fwdLoadWide = t.fwdLoadWide; d.nFwdLoad = (int)t.fwdLoadList.size();
+        std::vector<int2> ip(t.intPairs.size() / 2), ep(t.extPairs.size() / 2);
+        for (size_t q = 0; q < ip.size(); q++) ip[q] = make_int2(t.intPairs[2 * q], t.intPairs[2 * q + 1]);
+        for (size_t q = 0; q < ep.size(); q++) ep[q] = make_int2(t.extPairs[2 * q], t.extPairs[2 * q + 1]);
+#define UPT(vec, field) if ((rc = Upload(G, vec, &d.field)) != GS_OK) return rc
+        UPT(t.slotGlobal, slotGlobal); UPT(t.slotDiagNode, slotDiagNode); UPT(t.nodes, nodes); UPT(t.smemBase, smemBase);
+        UPT(t.ent, ent); UPT(t.entSm, entSm); UPT(t.intPtr, intPtr); UPT(t.extPtr, extPtr);
+        UPT(ip, intPairs); UPT(ep, extPairs); UPT(t.loadList, loadList); UPT(t.fwdLoadList, fwdLoadList);
+        UPT(t.fWalk, fWalk); UPT(t.fWalkPtr, fWalkPtr); UPT(t.fWalkWide, fWalkWide);
+        UPT(t.vWalk, vWalk); UPT(t.vWalkPtr, vWalkPtr); UPT(t.vWalkWide, vWalkWide);
+        UPT(t.bWalk, bWalk); UPT(t.bWalkPtr, bWalkPtr); UPT(t.bWalkWide, bWalkWide);
+        UPT(t.bRowPtr, bRowPtr); UPT(t.bRowSm, bRowSm);
+#undef UPT
+    }
 #undef UP
     // the persistent kernels take every level from the first one whose items (and those of all levels above
     // it) fit twice in a CTA's warps in each phase; the wide levels below run one launch per level and phase
@@ -1262,14 +1539,14 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             // few systems left: one CTA per active system (k_tail), no per-level launches
             cudaMemsetAsync(cur.activeCount, 0, sizeof(int), st);
             k_collect_active<<<(cur.count + 255) / 256, 256, 0, st>>>(cur);
-            k_tail<T, kWorkFactor><<<nActive, kTailThreads, 0, st>>>(g, cur, (T*)cur.y);
+            k_tail<T, kWorkFactor><<<nActive, kTailThreads, 0, st>>>(g, cur, (T*)cur.y, 0);
             if (timed) cudaEventRecord(ev[2], st);
-            k_tail<T, kWorkBackward><<<nActive, kTailThreads, 0, st>>>(g, cur, (T*)cur.y);
+            k_tail<T, kWorkBackward><<<nActive, kTailThreads, 0, st>>>(g, cur, (T*)cur.y, 0);
             launches += 3;
             if (refine) {
                 k_residual<T><<<dim3(nodeBlocks.x, (nActive + 31) / 32), blk8, 0, st>>>(g, cur, cur.activeList, nActive);
-                k_tail<T, kWorkForward><<<nActive, kTailThreads, 0, st>>>(g, cur, (T*)cur.z);
-                k_tail<T, kWorkBackward><<<nActive, kTailThreads, 0, st>>>(g, cur, (T*)cur.z);
+                k_tail<T, kWorkForward><<<nActive, kTailThreads, 0, st>>>(g, cur, (T*)cur.z, 0);
+                k_tail<T, kWorkBackward><<<nActive, kTailThreads, 0, st>>>(g, cur, (T*)cur.z, 0);
                 launches += 3;
             }
             if (timed) cudaEventRecord(ev[3], st);
@@ -1407,6 +1684,10 @@ using namespace gs;
 
 extern "C" {
 
+namespace gs {
+cudaError_t SetKernelAttributes();  // defined after the multi-grid kernels
+}
+
 int gs_ctx_create(int device, const gs_ctx_opts* opts, gs_ctx** out) {
     if (!out) return GS_ERR_INVALID_ARG;
     *out = nullptr;
@@ -1449,6 +1730,7 @@ int gs_ctx_create(int device, const gs_ctx_opts* opts, gs_ctx** out) {
     gs_ctx* c = new gs_ctx();
     c->device = device;
     c->stream = probe->stream;
+    if (cudaSetDevice(device) != cudaSuccess || gs::SetKernelAttributes() != cudaSuccess) { delete c; return GS_ERR_CUDA; }
     if (cudaMallocHost(&c->pinnedCount, 4 * sizeof(int)) != cudaSuccess) { delete c; return GS_ERR_CUDA; }
     *out = c;
     return GS_OK;
@@ -1921,5 +2203,27 @@ extern "C" int gs_pf_mismatch_noalloc(gs_grid* G, int32_t count, const double* d
     return GS_OK;
 }
 
-// The request loop (gs_serve_*): uses the kernels and host helpers above.
+// The uneven multi-grid batch (gs_pf_solve_multi) and the request loop (gs_serve_*): they use the kernels and
+// host helpers above.
+#include "gs_multi.cuh"
 #include "gs_serve.cuh"
+
+namespace gs {
+// the one-system kernels hold the top of the elimination tree in up to 200 KB of dynamic shared memory
+cudaError_t SetKernelAttributes() {
+    const int bytes = 210 * 1024;  // the 200 KB budget of the top part, with room to spare
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void* f) {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    };
+    set((const void*)k_tail<float, kWorkFactor>);
+    set((const void*)k_tail<float, kWorkBackward>);
+    set((const void*)k_tail<float, kWorkForward>);
+    set((const void*)k_tail<double, kWorkFactor>);
+    set((const void*)k_tail<double, kWorkBackward>);
+    set((const void*)k_tail<double, kWorkForward>);
+    set((const void*)k_newton<float>);
+    set((const void*)k_newton<double>);
+    return e;
+}
+}  // namespace gs

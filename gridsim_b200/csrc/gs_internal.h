@@ -81,7 +81,41 @@ struct Symbolic {
         std::vector<int32_t> levelWide;    // how many of a level (phase)'s first items are wide (one piece each)
     };
     Schedule factor, backward, forward;
+
+    // The top of the elimination tree (levels >= L0) held in shared memory by the one-system walks: the LU
+    // values of its nodes (node k's [diag, U..., L...] from smemBase[k]) and then their right-hand-side values
+    // (smem index yIdx[k]). Every pair of a top entry is internal (its node j is a top node: both operands in
+    // shared memory, smem indices) or external (j below L0: global indices, applied in one parallel pass before
+    // the top walk, as their operands are final by then). L0 is the lowest level whose top fits the budget;
+    // built once per element size (FP64 / FP32).
+    struct TopPart {
+        int L0 = 0;                   // nLevels: no top part
+        int nSlots = 0, nNodes = 0;   // smem LU values, then smem right-hand-side values
+        std::vector<int32_t> smemBase, yIdx;   // per node (-1 below L0)
+        std::vector<int32_t> slotGlobal;       // per smem LU value: its global LU slot
+        std::vector<int32_t> slotDiagNode;     // per smem LU value: the node whose diagonal it is, else -1
+        std::vector<int32_t> nodes;            // top nodes, smem right-hand-side order
+        // all entries of the top nodes: the global entry, its smem index, internal and external pairs
+        std::vector<int32_t> ent, entSm;
+        std::vector<int32_t> intPtr, extPtr;   // [nEnt + 1]
+        std::vector<int32_t> intPairs, extPairs;
+        // load + external pass of the factorisation: all top entries (wide first); of the forward
+        // substitution of a second right-hand side: the forward entries (wide first). Indices into ent.
+        std::vector<int32_t> loadList, fwdLoadList;
+        int loadWide = 0, fwdLoadWide = 0;
+        // walks: per (level - L0) and phase, indices into ent, wide first; the forward entries per level;
+        // the backward nodes per level (indices into nodes) with their U rows as smem right-hand-side indices
+        std::vector<int32_t> fWalk, fWalkPtr, fWalkWide;   // ptr [2 * nTop + 1], wide [2 * nTop]
+        std::vector<int32_t> vWalk, vWalkPtr, vWalkWide;   // ptr [nTop + 1]
+        std::vector<int32_t> bWalk, bWalkPtr, bWalkWide;   // ptr [nTop + 1]
+        std::vector<int32_t> bRowPtr, bRowSm;              // per top node (nodes order): smem indices of x(P_k)
+        size_t bytes(size_t elem) const { return (size_t)(nSlots + nNodes) * elem; }
+    };
+    TopPart top[2];  // [0] FP64, [1] FP32
 };
+
+// Build s.top[which] for values of `elem` bytes within `budget` bytes of shared memory.
+void BuildTopPart(Symbolic& s, int which, size_t elem, size_t budget);
 
 // Build the symbolic analysis; returns an empty string on success, else the reason.
 std::string Analyze(const HostGrid& g, Symbolic& s);

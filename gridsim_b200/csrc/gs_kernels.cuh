@@ -19,9 +19,38 @@ enum : int32_t {
     kFlagJacBad = 8,          // the Jacobian held a NaN / Inf (the step is refused)
 };
 
+// Symbolic::TopPart on the device (one per element size).
+struct DevTop {
+    int L0, nSlots, nNodes, nEnt, loadWide, nLoad, fwdLoadWide, nFwdLoad;
+    const int* slotGlobal;
+    const int* slotDiagNode;
+    const int* nodes;
+    const int* smemBase;
+    const int* ent;
+    const int* entSm;
+    const int* intPtr;
+    const int* extPtr;
+    const int2* intPairs;
+    const int2* extPairs;
+    const int* loadList;
+    const int* fwdLoadList;
+    const int* fWalk;
+    const int* fWalkPtr;
+    const int* fWalkWide;
+    const int* vWalk;
+    const int* vWalkPtr;
+    const int* vWalkWide;
+    const int* bWalk;
+    const int* bWalkPtr;
+    const int* bWalkWide;
+    const int* bRowPtr;
+    const int* bRowSm;
+};
+
 struct DevGrid {
     int n, m, nnzY, nbr;
     int64_t nnzLU;
+    int nLevels;          // elimination-tree levels of the schedules
     const int* yRowPtr;
     const int* yCol;
     const double* yG;
@@ -65,6 +94,9 @@ struct DevGrid {
     const int* fWorkPtr;  // per level (and phase for the factorisation): work range
     const int* bWorkPtr;
     const int* vWorkPtr;
+    const int4* fDesc;    // per schedule position: the work descriptor (see gs_engine.cu)
+    const int4* bDesc;
+    const int4* vDesc;
     const int* fWide;     // per level (phase): leading wide items
     const int* bWide;
     const int* vWide;
@@ -72,6 +104,7 @@ struct DevGrid {
     const int* luCnt;
     const int* pRowPtr;
     const int* pRows;
+    DevTop top[2];        // [0] FP64, [1] FP32
 };
 
 struct DevBatch {

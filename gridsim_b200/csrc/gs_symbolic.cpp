@@ -24,6 +24,9 @@
 #include "gs_internal.h"
 
 namespace gs {
+
+// Shared memory a one-system walk may hold the top of the elimination tree in.
+constexpr size_t kTopBudgetBytes = 200 * 1024;
 namespace {
 
 using cplx = std::complex<double>;
@@ -411,7 +414,127 @@ std::string Analyze(const HostGrid& g, Symbolic& s) {
         pack(s.backward, bwd, lenBwd);
         pack(s.forward, fwd, lenFwd);
     }
+    BuildTopPart(s, 0, sizeof(double), kTopBudgetBytes);
+    BuildTopPart(s, 1, sizeof(float), kTopBudgetBytes);
     return "";
+}
+
+void BuildTopPart(Symbolic& s, int which, size_t elem, size_t budget) {
+    Symbolic::TopPart& t = s.top[which];
+    t = Symbolic::TopPart();
+    const int m = s.m, L = s.nLevels;
+    // values (LU + right-hand side) of the top from each level up
+    std::vector<int64_t> vals(L + 1, 0);
+    for (int l = L - 1; l >= 0; l--) {
+        int64_t v = 0;
+        for (int q = s.levelNodePtr[l]; q < s.levelNodePtr[l + 1]; q++) v += 2 * (int64_t)s.luCnt[s.levelNodes[q]] + 2;
+        vals[l] = vals[l + 1] + v;
+    }
+    int L0 = L;
+    while (L0 > 0 && (size_t)vals[L0 - 1] * elem <= budget) L0--;
+    t.L0 = L0;
+    if (L0 >= L) return;
+    const int nTop = L - L0;
+    t.smemBase.assign(m, -1);
+    t.yIdx.assign(m, -1);
+    for (int l = L0; l < L; l++)
+        for (int q = s.levelNodePtr[l]; q < s.levelNodePtr[l + 1]; q++) {
+            const int k = s.levelNodes[q];
+            t.smemBase[k] = t.nSlots;
+            for (int x = 0; x < 2 * s.luCnt[k] + 1; x++) {
+                t.slotGlobal.push_back((int32_t)(s.luBase[k] + x));
+                t.slotDiagNode.push_back(x == 0 ? k : -1);
+            }
+            t.nSlots += 2 * s.luCnt[k] + 1;
+            t.nodes.push_back(k);
+        }
+    t.nNodes = (int)t.nodes.size();
+    for (int i = 0; i < t.nNodes; i++) t.yIdx[t.nodes[i]] = t.nSlots + i;
+    std::vector<int> slotNode(s.nnzLU);
+    for (int k = 0; k < m; k++)
+        for (int64_t x = s.luBase[k]; x < s.luBase[k] + 2 * s.luCnt[k] + 1; x++) slotNode[x] = k;
+    // entries of the top nodes and their pairs split into internal (smem) and external (global) ones
+    constexpr int kWideTop = 32, kWideExt = 16;
+    std::vector<int32_t> nInt, nExt, kindOf;
+    t.intPtr.assign(1, 0);
+    t.extPtr.assign(1, 0);
+    std::vector<int32_t> firstEnt(m, -1);
+    for (int k : t.nodes) {
+        firstEnt[k] = (int32_t)t.ent.size();
+        const int e0 = s.diagPairNode[k];
+        for (int e = e0; e < e0 + 2 * s.luCnt[k] + 2; e++) {
+            const int kind = s.entKind[e];
+            t.ent.push_back(e);
+            t.entSm.push_back(kind == kFwd ? t.yIdx[k] : t.smemBase[k] + (int32_t)(s.entSlot[e] - s.luBase[k]));
+            int ni = 0, nx = 0;
+            for (int64_t q = s.entPairPtr[e]; q < s.entPairPtr[e + 1]; q++) {
+                const int left = s.pairs[2 * q], right = s.pairs[2 * q + 1];
+                const int j = slotNode[left];
+                if (s.level[j] >= L0) {
+                    t.intPairs.push_back(t.smemBase[j] + (int32_t)(left - s.luBase[j]));
+                    t.intPairs.push_back(kind == kFwd ? t.yIdx[right] : t.smemBase[j] + (int32_t)(right - s.luBase[j]));
+                    ni++;
+                } else {
+                    t.extPairs.push_back(left);
+                    t.extPairs.push_back(right);
+                    nx++;
+                }
+            }
+            t.intPtr.push_back((int32_t)(t.intPairs.size() / 2));
+            t.extPtr.push_back((int32_t)(t.extPairs.size() / 2));
+            nInt.push_back(ni);
+            nExt.push_back(nx);
+            kindOf.push_back(kind);
+        }
+    }
+    const int nEnt = (int)t.ent.size();
+    for (int ti = 0; ti < nEnt; ti++) if (nExt[ti] > kWideExt) t.loadList.push_back(ti);
+    t.loadWide = (int)t.loadList.size();
+    for (int ti = 0; ti < nEnt; ti++) if (nExt[ti] <= kWideExt) t.loadList.push_back(ti);
+    for (int ti = 0; ti < nEnt; ti++) if (kindOf[ti] == kFwd && nExt[ti] > kWideExt) t.fwdLoadList.push_back(ti);
+    t.fwdLoadWide = (int)t.fwdLoadList.size();
+    for (int ti = 0; ti < nEnt; ti++) if (kindOf[ti] == kFwd && nExt[ti] <= kWideExt) t.fwdLoadList.push_back(ti);
+    // walks per top level
+    auto addWide = [&](std::vector<int32_t>& walk, std::vector<int32_t>& wideCnt, std::vector<int32_t>& ptr,
+                       const std::vector<int32_t>& list, const std::vector<int32_t>& len, int wideAt) {
+        int w = 0;
+        for (size_t q = 0; q < list.size(); q++) if (len[q] > wideAt) { walk.push_back(list[q]); w++; }
+        for (size_t q = 0; q < list.size(); q++) if (len[q] <= wideAt) walk.push_back(list[q]);
+        wideCnt.push_back(w);
+        ptr.push_back((int32_t)walk.size());
+    };
+    t.fWalkPtr.assign(1, 0);
+    t.vWalkPtr.assign(1, 0);
+    t.bWalkPtr.assign(1, 0);
+    std::vector<int32_t> nodeIndex(m, -1);
+    for (int i = 0; i < t.nNodes; i++) nodeIndex[t.nodes[i]] = i;
+    for (int lt = 0; lt < nTop; lt++) {
+        const int l = L0 + lt;
+        std::vector<int32_t> pa, pb, pf, la, lb, lf, bn, lbn;
+        for (int q = s.levelNodePtr[l]; q < s.levelNodePtr[l + 1]; q++) {
+            const int k = s.levelNodes[q];
+            const int c = s.luCnt[k];
+            for (int ti = firstEnt[k]; ti < firstEnt[k] + 2 * c + 2; ti++) {
+                const int kind = kindOf[ti];
+                // after the load an upper or forward entry without internal pairs holds its final value
+                if (kind == kLower) { pb.push_back(ti); lb.push_back(nInt[ti]); }
+                else if (kind == kDiag || nInt[ti] > 0) { pa.push_back(ti); la.push_back(nInt[ti]); }
+                if (kind == kFwd && nInt[ti] > 0) { pf.push_back(ti); lf.push_back(nInt[ti]); }
+            }
+            bn.push_back(nodeIndex[k]);
+            lbn.push_back(c);
+        }
+        addWide(t.fWalk, t.fWalkWide, t.fWalkPtr, pa, la, kWideTop);
+        addWide(t.fWalk, t.fWalkWide, t.fWalkPtr, pb, lb, kWideTop);
+        addWide(t.vWalk, t.vWalkWide, t.vWalkPtr, pf, lf, kWideTop);
+        addWide(t.bWalk, t.bWalkWide, t.bWalkPtr, bn, lbn, kWideTop);
+    }
+    t.bRowPtr.assign(1, 0);
+    for (int i = 0; i < t.nNodes; i++) {
+        const int k = t.nodes[i];
+        for (int q = s.pRowPtr[k]; q < s.pRowPtr[k + 1]; q++) t.bRowSm.push_back(t.yIdx[s.pRows[q]]);
+        t.bRowPtr.push_back((int32_t)t.bRowSm.size());
+    }
 }
 
 }  // namespace gs

@@ -232,6 +232,69 @@ class SparseNewtonRaphsonPowerFlow:
 
 
 # ---------------------------------------------------------------------------------------------
+class UnevenBatch:
+    """Independent load flows of several grids of any sizes in one persistent launch (``gs_pf_solve_multi``).
+
+    The grids are uploaded once; every :meth:`solve` runs ``counts[k]`` cases of grid k, each from its case's
+    stored voltages, optionally with per-bus load multipliers and a branch outage. The CTA shape is autotuned on
+    the first call for this set of grids and reused afterwards."""
+
+    def __init__(self, models: Sequence[GridModel], ctx: Optional[CudaContext] = None):
+        self.ctx = ctx or CudaContext.default()
+        self.models = list(models)
+        self.grids = [CudaGrid(m, self.ctx) for m in self.models]
+        self.stats = None
+
+    def solve(self, counts: Sequence[int], load_scale: Optional[Sequence[np.ndarray]] = None,
+              outage: Optional[Sequence[np.ndarray]] = None, options: Optional[PowerFlowOptions] = None,
+              keep_states: bool = False) -> dict:
+        """load_scale[k]: [counts[k], n_bus(k)] multipliers of Pd and Qd; outage[k]: [counts[k]] branch indices.
+        Returns per-grid lists of status, iterations, max_mismatch (and vm, va_deg [counts[k], n_bus(k)])."""
+        opt = options or PowerFlowOptions()
+        counts = np.ascontiguousarray(counts, np.int32)
+        k = len(self.models)
+        n = [m.n_bus for m in self.models]
+        total = int(counts.sum())
+        states = int(sum(int(c) * nb for c, nb in zip(counts, n)))
+        ls = None if load_scale is None else np.ascontiguousarray(
+            np.concatenate([np.asarray(load_scale[g], np.float64).reshape(-1) for g in range(k)]))
+        og = None if outage is None else np.ascontiguousarray(
+            np.concatenate([np.asarray(outage[g], np.int32).reshape(-1) for g in range(k)]))
+        if ls is not None and ls.shape[0] != states:
+            raise ValueError("load_scale: counts[k] x n_bus(k) values per grid")
+        if og is not None and og.shape[0] != total:
+            raise ValueError("outage: counts[k] values per grid")
+        st, it, mis = np.zeros(total, np.int32), np.zeros(total, np.int32), np.zeros(total)
+        vm = np.zeros(states) if keep_states else None
+        va = np.zeros(states) if keep_states else None
+        handles = (ctypes.c_void_p * max(k, 1))(*[g.handle.value for g in self.grids])
+        c = opt.to_c()
+        stats = _abi.MultiStats()
+        self.ctx.check(self.ctx.lib.gs_pf_solve_multi(self.ctx.handle, k, handles, _p(counts), _p(ls), _p(og),
+                                                      ctypes.byref(c), _p(st), _p(it), _p(mis), _p(vm), _p(va),
+                                                      ctypes.byref(stats)), "gs_pf_solve_multi")
+        self.stats = {f: getattr(stats, f) for f, _ in _abi.MultiStats._fields_ if f != "reserved"}
+        out = {"status": [], "iterations": [], "max_mismatch": [], "vm": [], "va_deg": []}
+        c0 = s0 = 0
+        for g in range(k):
+            cnt = int(counts[g])
+            out["status"].append(st[c0:c0 + cnt])
+            out["iterations"].append(it[c0:c0 + cnt])
+            out["max_mismatch"].append(mis[c0:c0 + cnt])
+            if keep_states:
+                out["vm"].append(vm[s0:s0 + cnt * n[g]].reshape(cnt, n[g]))
+                out["va_deg"].append(va[s0:s0 + cnt * n[g]].reshape(cnt, n[g]))
+            c0 += cnt
+            s0 += cnt * n[g]
+        return out
+
+    def close(self) -> None:
+        for g in self.grids:
+            g.close()
+        self.grids = []
+
+
+# ---------------------------------------------------------------------------------------------
 @dataclass
 class ContingencyViolation:
     """ContingencyViolation (ContingencyAnalysis.cs:156-163)."""

@@ -242,6 +242,35 @@ int gs_pf_solve_batch(gs_grid *grid, int32_t count, const double *load_scale, co
 int gs_n1_screen(gs_grid *grid, int32_t n_out, const int32_t *branch_idx, const gs_pf_opts *opts,
                  gs_n1_result *res);
 
+/* ---- uneven multi-grid batch -------------------------------------------------------------------
+ * counts[k] independent load flows of grid k (k < n_grids; grids of any sizes, one context) in ONE
+ * persistent kernel launch, captured in a CUDA graph: every CTA takes the next (grid, case) item from a
+ * device counter, largest grids first, and runs that case's whole Newton iteration itself (mismatch and
+ * Jacobian, status test, level-scheduled LU, triangular solves, FP64 refinement in mixed precision, damped
+ * update) with no host round trip. The CTA size and the shared-memory use of the level walk are picked by a
+ * built-in autotuner on the first call for a set of grids (timed trial launches on a sample of the items),
+ * and kept for later calls with the same set.
+ * Many SparseNewtonRaphsonPowerFlow.Solve calls (src/GridSim.Core/PowerFlow/SparseNewtonRaphsonPowerFlow.cs:48-54)
+ * on different grids, each case from its case's stored voltages.
+ * Per-case arrays are concatenated grid after grid, case after case: load_scale (NULL = 1) and the states
+ * vm / va_deg (may be NULL) hold counts[k] * n_bus(k) values for grid k; outage, status, iterations and
+ * max_mismatch hold one value per case (outage NULL or -1 = none). */
+typedef struct gs_multi_stats {
+    double device_ms;          /* the graph launch (CUDA events) */
+    double tune_ms;            /* autotuning trials of this call (0 when the choice was cached) */
+    int32_t threads_per_cta;   /* the autotuner's choice */
+    int32_t ctas;              /* persistent CTAs launched */
+    int32_t items;             /* load flows */
+    int32_t tuned_now;         /* 1: this call ran the autotuner */
+    int64_t system_steps;      /* Newton steps taken, summed over the cases */
+    int32_t shared_top;        /* the autotuner's choice: 1 = the top of the elimination tree in shared memory */
+    int32_t reserved[7];
+} gs_multi_stats;
+
+int gs_pf_solve_multi(gs_ctx *ctx, int32_t n_grids, gs_grid *const *grids, const int32_t *counts,
+                      const double *load_scale, const int32_t *outage, const gs_pf_opts *opts, int32_t *status,
+                      int32_t *iterations, double *max_mismatch, double *vm, double *va_deg, gs_multi_stats *stats);
+
 /* ---- request loop (serving) ---------------------------------------------------------------------
  * The reference's nearest counterpart is its sequential `gridsim rpc` host (src/GridSim.Cli/RpcCommand.cs:11-50):
  * one JSON request at a time, `solve` running the `pf` solver on a case held by handle. Here one native
