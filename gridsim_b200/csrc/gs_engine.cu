@@ -673,12 +673,104 @@ __device__ __forceinline__ void forwardEntryWarp1(const DevGrid& g, const DevBat
     if ((threadIdx.x & 31) == 0) v[k * B + s] -= dot;
 }
 
+// One system, a group of G lanes of a warp (mask: the group's lanes): lane j of the group takes pairs q0 + j,
+// q0 + j + G, ..., four at a time in flight; a fixed butterfly over the group completes the sum in every lane.
+template <typename T, int G>
+__device__ __forceinline__ T dotGroup(const T* __restrict__ lu, const T* __restrict__ rhs, const int2* __restrict__ pr,
+                                      int q0, int q1, size_t B, int s, unsigned mask) {
+    const int j = threadIdx.x & (G - 1);
+    T acc = T(0);
+    for (int q = q0 + j; q < q1; q += 4 * G) {
+        int2 a[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) a[u] = q + u * G < q1 ? __ldg(pr + q + u * G) : make_int2(-1, -1);
+        T l[4], r[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const bool ok = a[u].x >= 0;
+            l[u] = ok ? lu[a[u].x * B + s] : T(0);
+            r[u] = ok ? rhs[a[u].y * B + s] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) acc += l[u] * r[u];
+    }
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(mask, acc, off);
+    return acc;
+}
+
+// the rest of a factorisation entry once its dot is known (by the one lane that writes it)
+template <typename T>
+__device__ __forceinline__ void factorFinish(const DevBatch& b, const int4 d, int s, T dot) {
+    const size_t B = (size_t)b.B;
+    T* lu = (T*)b.lu;
+    const int kind = descKind(d), slot = d.x, node = descNode(d);
+    if (kind == kFwd) {
+        T* y = (T*)b.y;
+        y[slot * B + s] -= dot;
+        return;
+    }
+    const T a = descHasA(d) ? lu[slot * B + s] : T(0);
+    T v = a - dot;
+    if (kind == kDiag) {
+        const T fl = pivotFloor<T>() * (fabs(a) > T(1) ? fabs(a) : T(1));
+        if (!(fabs(v) > fl)) { atomicOr(&b.flags[s], kFlagPivotPerturbed); v = (v < T(0)) ? -fl : fl; }
+        ((T*)b.piv)[node * B + s] = v;
+        return;
+    }
+    if (kind == kLower) v = v / ((const T*)b.piv)[node * B + s];
+    lu[slot * B + s] = v;
+}
+
+// a mid-length piece of a one-system walk by a group of G lanes
+template <typename T, int W, int G>
+__device__ __forceinline__ void groupPiece(const DevGrid& g, const DevBatch& b, T* vec, const int4 d, int s, unsigned mask) {
+    const size_t B = (size_t)b.B;
+    const bool lead = (threadIdx.x & (G - 1)) == 0;
+    if (W == kWorkFactor) {
+        const T* lu = (const T*)b.lu;
+        const T dot = dotGroup<T, G>(lu, descKind(d) == kFwd ? (const T*)b.y : lu, g.pairs, d.y, d.z, B, s, mask);
+        if (lead) factorFinish<T>(b, d, s, dot);
+    } else if (W == kWorkForward) {
+        const T dot = dotGroup<T, G>((const T*)b.lu, vec, g.pairs, d.y, d.z, B, s, mask);
+        if (lead) vec[(size_t)descNode(d) * B + s] -= dot;
+    } else {
+        const T* lu = (const T*)b.lu;
+        const int k = d.x, c = d.z;
+        const int64_t base = d.y;
+        const int* rows = g.pRows + d.w;
+        const int j = threadIdx.x & (G - 1);
+        T acc = T(0);
+        for (int t = j; t < c; t += 4 * G) {
+            int r[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) r[u] = t + u * G < c ? __ldg(rows + t + u * G) : -1;
+            T uu[4], x[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const bool ok = r[u] >= 0;
+                uu[u] = ok ? lu[(base + 1 + t + u * G) * B + s] : T(0);
+                x[u] = ok ? vec[r[u] * B + s] : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) acc += uu[u] * x[u];
+        }
+#pragma unroll
+        for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(mask, acc, off);
+        if (lead) vec[k * B + s] = (vec[k * B + s] - acc) / ((const T*)b.piv)[k * B + s];
+    }
+}
+
 // One system, the whole block: every level (top down for the backward substitution) and phase of a schedule,
-// the wide pieces a warp each, the short pieces a thread each, a block barrier between levels and phases.
+// the wide pieces a warp each, the short ones of more than 8 pairs a group of 8 lanes each, the rest a thread each,
+// a block barrier between levels and phases.
 template <typename T, int W>
 __device__ __forceinline__ void walkLevels(const DevGrid& g, const DevBatch& b, T* vec, int s, int l0, int l1) {
     const int* ptr = W == kWorkFactor ? g.fWorkPtr : (W == kWorkBackward ? g.bWorkPtr : g.vWorkPtr);
     const int4* desc = W == kWorkFactor ? g.fDesc : (W == kWorkBackward ? g.bDesc : g.vDesc);
+    const int* midCnt = W == kWorkFactor ? g.fMid : (W == kWorkBackward ? g.bMid : g.vMid);
+    constexpr int G = 8;  // lanes per mid-length piece
+    const unsigned gmask = 0xFFu << (threadIdx.x & 24);
     const int* wide = W == kWorkFactor ? g.fWide : (W == kWorkBackward ? g.bWide : g.vWide);
     const int phases = W == kWorkFactor ? 2 : 1;
     const int warp = threadIdx.x >> 5;
@@ -694,8 +786,12 @@ __device__ __forceinline__ void walkLevels(const DevGrid& g, const DevBatch& b, 
                 else if (W == kWorkBackward) backwardNodeWarp1<T>(g, b, vec, x, s);
                 else forwardEntryWarp1<T>(g, b, vec, x, s);
             }
-            // short pieces: a thread each
-            for (int w = w0 + nw + (int)threadIdx.x; w < w1; w += (int)blockDim.x) {
+            // mid-length short pieces: a group of G lanes each (longest first)
+            const int nm = midCnt[i];
+            for (int w = w0 + nw + (int)(threadIdx.x / G); w < w0 + nw + nm; w += (int)(blockDim.x / G))
+                groupPiece<T, W, G>(g, b, vec, __ldg(desc + w), s, gmask);
+            // the rest: a thread each
+            for (int w = w0 + nw + nm + (int)threadIdx.x; w < w1; w += (int)blockDim.x) {
                 const int4 x = __ldg(desc + w);
                 if (W == kWorkFactor) factorEntry<T>(g, b, x, s, true, false);
                 else if (W == kWorkBackward) backwardNode<T>(g, b, vec, x, s, false);
@@ -906,16 +1002,52 @@ __device__ void forwardSystem(const DevGrid& g, const DevBatch& b, T* vec, int s
 // Dynamic shared memory of the one-system kernels (the top part of the grid's schedule).
 extern __shared__ __align__(16) unsigned char gsTopSmem[];
 
-// useTop: the top part in shared memory (launched with its bytes of dynamic shared memory), else every level in
-// global memory (the larger L1 then keeps more of the system's LU close).
+// Levels [l0, l1) of a schedule for the listed systems, one CTA each (the wide levels below l0 run as per-level
+// launches over the same batch).
 template <typename T, int W>
-__global__ void __launch_bounds__(kTailThreads) k_tail(DevGrid g, DevBatch b, T* vec, int useTop) {
+__global__ void __launch_bounds__(kTailThreads) k_tail(DevGrid g, DevBatch b, T* vec, int l0, int l1) {
     const int s = b.activeList[blockIdx.x];
     if (W != kWorkFactor && vec != (T*)b.y && !b.refine[s]) return;  // uniform across the block
-    T* sm = reinterpret_cast<T*>(gsTopSmem);
-    if (W == kWorkFactor) factorSystem<T>(g, b, s, sm, useTop != 0);
-    else if (W == kWorkBackward) backwardSystem<T>(g, b, vec, s, sm, useTop != 0);
-    else forwardSystem<T>(g, b, vec, s, sm, useTop != 0);
+    walkLevels<T, W>(g, b, vec, s, l0, l1);
+}
+
+// One step of the few systems of a batch (their list in b.activeList): factorisation, backward substitution and,
+// in mixed precision, the FP64-residual refinement. Levels below `lt` (many entries each) run as per-level launches
+// over the batch, the levels above as one CTA per system.
+template <typename T>
+int64_t FewSystemsSolve(const DevGrid& g, const DevBatch& b, const Symbolic& s, int nActive, int lt, bool refine,
+                        cudaStream_t st, cudaEvent_t afterFactor) {
+    int64_t launches = 0;
+    const int groups = b.B / Lay<T>::S;
+    const dim3 blk4(32, 4), blk8(32, 8);
+    auto level = [&](auto kernel, T* vec, int i0, int i1) {
+        if (i1 > i0) { kernel<<<dim3((i1 - i0 + 3) / 4, groups), blk4, 0, st>>>(g, b, vec, i0, i1); launches++; }
+    };
+    const auto& fp = s.factor.levelItemPtr;
+    const auto& bp = s.backward.levelItemPtr;
+    const auto& vp = s.forward.levelItemPtr;
+    const int L = s.nLevels;
+    auto backward = [&](T* vec) {
+        k_tail<T, kWorkBackward><<<nActive, kTailThreads, 0, st>>>(g, b, vec, lt, L);
+        launches++;
+        for (int l = lt - 1; l >= 0; l--) level(k_level<T, kWorkBackward>, vec, bp[l], bp[l + 1]);
+    };
+    for (int l = 0; l < lt; l++) {
+        level(k_level<T, kWorkFactor>, (T*)b.y, fp[2 * l], fp[2 * l + 1]);
+        level(k_level<T, kWorkFactor>, (T*)b.y, fp[2 * l + 1], fp[2 * l + 2]);
+    }
+    k_tail<T, kWorkFactor><<<nActive, kTailThreads, 0, st>>>(g, b, (T*)b.y, lt, L);
+    launches++;
+    if (afterFactor) cudaEventRecord(afterFactor, st);
+    backward((T*)b.y);
+    if (refine) {
+        k_residual<T><<<dim3((s.n + 7) / 8, (nActive + 31) / 32), blk8, 0, st>>>(g, b, b.activeList, nActive);
+        for (int l = 0; l < lt; l++) level(k_level<T, kWorkForward>, (T*)b.z, vp[l], vp[l + 1]);
+        k_tail<T, kWorkForward><<<nActive, kTailThreads, 0, st>>>(g, b, (T*)b.z, lt, L);
+        launches += 2;
+        backward((T*)b.z);
+    }
+    return launches;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1188,7 +1320,8 @@ struct gs_grid {
     std::vector<double> pgen, qgen, pload, qload;
     gs::Workspace ws;
     gs::Workspace tws;  // compact copy of the few systems still stepping
-    int split = 0;  // first level run by the persistent kernels
+    int split = 0;      // first level run by the persistent kernels
+    int tailSplit = 0;  // first level the few-systems path runs as one CTA per system
 };
 
 namespace gs {
@@ -1271,6 +1404,7 @@ int UploadGrid(gs_grid* G) {
     UP(s.forward.work, vWork); UP(s.forward.items, vItems); UP(s.forward.levelItemPtr, vLevelPtr);
     UP(s.factor.levelWorkPtr, fWorkPtr); UP(s.backward.levelWorkPtr, bWorkPtr); UP(s.forward.levelWorkPtr, vWorkPtr);
     UP(s.factor.levelWide, fWide); UP(s.backward.levelWide, bWide); UP(s.forward.levelWide, vWide);
+    UP(s.factor.levelMid, fMid); UP(s.backward.levelMid, bMid); UP(s.forward.levelMid, vMid);
     for (int w = 0; w < 2; w++) {
         const Symbolic::TopPart& t = s.top[w];
         DevTop& d = v.top[w];
@@ -1293,6 +1427,19 @@ int UploadGrid(gs_grid* G) {
 #undef UP
     // the persistent kernels take every level from the first one whose items (and those of all levels above
     // it) fit twice in a CTA's warps in each phase; the wide levels below run one launch per level and phase
+    // the few-systems path runs the lowest levels as per-level launches while a phase of them holds more short
+    // pieces than one CTA's threads (more than one round of a one-system walk)
+    G->tailSplit = 0;
+    for (int l = 0; l < s.nLevels; l++) {
+        bool wideLevel = false;
+        for (int ph = 0; ph < 2; ph++) {
+            const int i = 2 * l + ph;
+            if (s.factor.levelWorkPtr[i + 1] - s.factor.levelWorkPtr[i] - s.factor.levelWide[i] > kTailThreads) wideLevel = true;
+        }
+        if (s.backward.levelWorkPtr[l + 1] - s.backward.levelWorkPtr[l] - s.backward.levelWide[l] > kTailThreads) wideLevel = true;
+        if (!wideLevel) break;
+        G->tailSplit = l + 1;
+    }
     G->split = s.nLevels;
     for (int l = s.nLevels - 1; l >= 0; l--) {
         const auto& fp = s.factor.levelItemPtr;
@@ -1536,19 +1683,11 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
                 launches += 3;
                 compacted = true;
             }
-            // few systems left: one CTA per active system (k_tail), no per-level launches
+            // few systems left: the wide bottom levels as per-level launches over the compact batch, the rest as
+            // one CTA per active system (k_tail)
             cudaMemsetAsync(cur.activeCount, 0, sizeof(int), st);
             k_collect_active<<<(cur.count + 255) / 256, 256, 0, st>>>(cur);
-            k_tail<T, kWorkFactor><<<nActive, kTailThreads, 0, st>>>(g, cur, (T*)cur.y, 0);
-            if (timed) cudaEventRecord(ev[2], st);
-            k_tail<T, kWorkBackward><<<nActive, kTailThreads, 0, st>>>(g, cur, (T*)cur.y, 0);
-            launches += 3;
-            if (refine) {
-                k_residual<T><<<dim3(nodeBlocks.x, (nActive + 31) / 32), blk8, 0, st>>>(g, cur, cur.activeList, nActive);
-                k_tail<T, kWorkForward><<<nActive, kTailThreads, 0, st>>>(g, cur, (T*)cur.z, 0);
-                k_tail<T, kWorkBackward><<<nActive, kTailThreads, 0, st>>>(g, cur, (T*)cur.z, 0);
-                launches += 3;
-            }
+            launches += 1 + FewSystemsSolve<T>(g, cur, s, nActive, G->tailSplit, anyRefine != 0, st, timed ? ev[2] : nullptr);
             if (timed) cudaEventRecord(ev[3], st);
             {
                 const int grp = (nActive + 31) / 32;

@@ -79,6 +79,7 @@ struct Symbolic {
         std::vector<int32_t> levelItemPtr;
         std::vector<int32_t> levelWorkPtr; // the work of a level (phase) is work[levelWorkPtr[i] .. [i+1])
         std::vector<int32_t> levelWide;    // how many of a level (phase)'s first items are wide (one piece each)
+        std::vector<int32_t> levelMid;     // how many of the short pieces after them are longer than 8 pairs
     };
     Schedule factor, backward, forward;
 

@@ -97,6 +97,9 @@ struct DevGrid {
     const int4* fDesc;    // per schedule position: the work descriptor (see gs_engine.cu)
     const int4* bDesc;
     const int4* vDesc;
+    const int* fMid;      // per level (phase): the mid-length short pieces after the wide ones
+    const int* bMid;
+    const int* vMid;
     const int* fWide;     // per level (phase): leading wide items
     const int* bWide;
     const int* vWide;

@@ -238,13 +238,7 @@ cudaError_t LaunchB(gs_server* S, Lane& L) {
     if (na > 0) {
         cudaMemsetAsync(b.activeCount, 0, sizeof(int), L.st);
         k_collect_active<<<(L.C + 255) / 256, 256, 0, L.st>>>(b);
-        k_tail<T, kWorkFactor><<<na, kTailThreads, 0, L.st>>>(g, b, (T*)b.y, 0);
-        k_tail<T, kWorkBackward><<<na, kTailThreads, 0, L.st>>>(g, b, (T*)b.y, 0);
-        if (refine) {
-            k_residual<T><<<dim3((n + 7) / 8, (na + 31) / 32), blk8, 0, L.st>>>(g, b, b.activeList, na);
-            k_tail<T, kWorkForward><<<na, kTailThreads, 0, L.st>>>(g, b, (T*)b.z, 0);
-            k_tail<T, kWorkBackward><<<na, kTailThreads, 0, L.st>>>(g, b, (T*)b.z, 0);
-        }
+        FewSystemsSolve<T>(g, b, L.G->sym, na, L.G->tailSplit, refine != 0, L.st, nullptr);
         constexpr int rowsPerBlock = 512;
         k_dxmax<T><<<dim3((m + rowsPerBlock - 1) / rowsPerBlock, (na + 31) / 32), blk8, 0, L.st>>>(g, b, rowsPerBlock, refine,
                                                                                                 b.activeList, na);

@@ -364,8 +364,11 @@ std::string Analyze(const HostGrid& g, Symbolic& s) {
     // Short pieces (at most kShort pairs) are packed kPack to an item (the most lane groups a warp has:
     // 4 for FP32, 8 for FP64 -- the kernels take the first `count`); longer ones get a warp each.
     const int kShort = 32, kPack = 8;
+    // The short pieces of a level are ordered longest first; the one-system walks give those with more than kMid
+    // pairs a group of lanes each (levelMid counts them).
+    const int kMid = 8;
     auto pack = [&](Symbolic::Schedule& sc, const std::vector<int32_t>& list, const std::vector<int64_t>& len) {
-        std::vector<int32_t> shortOnes;
+        std::vector<std::pair<int64_t, int32_t>> shortLen;
         int wide = 0;
         for (size_t q = 0; q < list.size(); q++) {
             if (len[q] > kShort) {
@@ -374,9 +377,18 @@ std::string Analyze(const HostGrid& g, Symbolic& s) {
                 sc.items.push_back(-1);
                 wide++;
             } else {
-                shortOnes.push_back(list[q]);
+                shortLen.push_back({len[q], list[q]});
             }
         }
+        std::stable_sort(shortLen.begin(), shortLen.end(),
+                         [](const std::pair<int64_t, int32_t>& a, const std::pair<int64_t, int32_t>& b) { return a.first > b.first; });
+        std::vector<int32_t> shortOnes;
+        int mid = 0;
+        for (auto& pr : shortLen) {
+            shortOnes.push_back(pr.second);
+            if (pr.first > kMid) mid++;
+        }
+        sc.levelMid.push_back(mid);
         for (size_t q = 0; q < shortOnes.size(); q += kPack) {
             int cnt = (int)std::min<size_t>(kPack, shortOnes.size() - q);
             sc.items.push_back((int32_t)sc.work.size());
