@@ -765,37 +765,56 @@ __device__ __forceinline__ void groupPiece(const DevGrid& g, const DevBatch& b, 
 // the wide pieces a warp each, the short ones of more than 8 pairs a group of 8 lanes each, the rest a thread each,
 // a block barrier between levels and phases.
 template <typename T, int W>
-__device__ __forceinline__ void walkLevels(const DevGrid& g, const DevBatch& b, T* vec, int s, int l0, int l1) {
+__device__ __forceinline__ void walkLevels(const DevGrid& g, const DevBatch& b, T* vec, int s, int l0, int l1, int* queue) {
     const int* ptr = W == kWorkFactor ? g.fWorkPtr : (W == kWorkBackward ? g.bWorkPtr : g.vWorkPtr);
     const int4* desc = W == kWorkFactor ? g.fDesc : (W == kWorkBackward ? g.bDesc : g.vDesc);
     const int* midCnt = W == kWorkFactor ? g.fMid : (W == kWorkBackward ? g.bMid : g.vMid);
-    constexpr int G = 8;  // lanes per mid-length piece
-    const unsigned gmask = 0xFFu << (threadIdx.x & 24);
     const int* wide = W == kWorkFactor ? g.fWide : (W == kWorkBackward ? g.bWide : g.vWide);
+    constexpr int G = 8;  // lanes per mid-length piece
+    const int lane = threadIdx.x & 31, glead = lane & 24;
+    const unsigned gmask = 0xFFu << glead;
     const int phases = W == kWorkFactor ? 2 : 1;
-    const int warp = threadIdx.x >> 5;
+    // three shared counters per level and phase (wide, mid, rest), zeroed once per walk
+    const int nq = 3 * phases * (l1 - l0);
+    for (int k = threadIdx.x; k < nq; k += blockDim.x) queue[k] = 0;
+    __syncthreads();
     for (int step = 0; step < l1 - l0; step++) {
         const int l = W == kWorkBackward ? l1 - 1 - step : l0 + step;
         for (int ph = 0; ph < phases; ph++) {
             const int i = phases * l + ph;
-            const int w0 = ptr[i], w1 = ptr[i + 1], nw = wide[i];
-            // wide pieces (the first nw of the range): a warp each
-            for (int w = w0 + warp; w < w0 + nw; w += (int)(blockDim.x >> 5)) {
-                const int4 x = __ldg(desc + w);
+            int* q = queue + 3 * (phases * (l - l0) + ph);
+            const int w0 = __ldg(ptr + i), w1 = __ldg(ptr + i + 1), nw = __ldg(wide + i), nm = __ldg(midCnt + i);
+            // pieces are taken from the counters as warps, groups and threads come free: wide ones a warp each,
+            // mid-length ones (longest first) a group of G lanes each, the rest a thread each, 32 per warp grab
+            for (;;) {
+                int w = 0;
+                if (lane == 0) w = atomicAdd(q, 1);
+                w = __shfl_sync(0xffffffffu, w, 0);
+                if (w >= nw) break;
+                const int4 x = __ldg(desc + w0 + w);
                 if (W == kWorkFactor) factorEntryWarp1<T>(g, b, x, s);
                 else if (W == kWorkBackward) backwardNodeWarp1<T>(g, b, vec, x, s);
                 else forwardEntryWarp1<T>(g, b, vec, x, s);
             }
-            // mid-length short pieces: a group of G lanes each (longest first)
-            const int nm = midCnt[i];
-            for (int w = w0 + nw + (int)(threadIdx.x / G); w < w0 + nw + nm; w += (int)(blockDim.x / G))
-                groupPiece<T, W, G>(g, b, vec, __ldg(desc + w), s, gmask);
-            // the rest: a thread each
-            for (int w = w0 + nw + nm + (int)threadIdx.x; w < w1; w += (int)blockDim.x) {
-                const int4 x = __ldg(desc + w);
-                if (W == kWorkFactor) factorEntry<T>(g, b, x, s, true, false);
-                else if (W == kWorkBackward) backwardNode<T>(g, b, vec, x, s, false);
-                else forwardEntry<T>(g, b, vec, x, s, false);
+            for (;;) {
+                int w = 0;
+                if (lane == glead) w = atomicAdd(q + 1, 1);
+                w = __shfl_sync(gmask, w, glead);
+                if (w >= nm) break;
+                groupPiece<T, W, G>(g, b, vec, __ldg(desc + w0 + nw + w), s, gmask);
+            }
+            const int nr = w1 - w0 - nw - nm;
+            for (;;) {
+                int w = 0;
+                if (lane == 0) w = atomicAdd(q + 2, 32);
+                w = __shfl_sync(0xffffffffu, w, 0);
+                if (w >= nr) break;
+                if (w + lane < nr) {
+                    const int4 x = __ldg(desc + w0 + nw + nm + w + lane);
+                    if (W == kWorkFactor) factorEntry<T>(g, b, x, s, true, false);
+                    else if (W == kWorkBackward) backwardNode<T>(g, b, vec, x, s, false);
+                    else forwardEntry<T>(g, b, vec, x, s, false);
+                }
             }
             __syncthreads();
         }
@@ -890,9 +909,9 @@ __device__ __forceinline__ void topFinish(const DevGrid& g, const DevBatch& b, c
 // memory; the top is loaded into shared memory `sm` (external pairs applied on the way), walked there, and
 // written back (U and L to the LU, pivots to piv, the forward-substituted right-hand side to y).
 template <typename T>
-__device__ void factorSystem(const DevGrid& g, const DevBatch& b, int s, T* sm, bool useTop) {
+__device__ void factorSystem(const DevGrid& g, const DevBatch& b, int s, T* sm, bool useTop, int* queue) {
     const DevTop& t = topOf<T>(g);
-    walkLevels<T, kWorkFactor>(g, b, (T*)b.y, s, 0, useTop ? t.L0 : g.nLevels);
+    walkLevels<T, kWorkFactor>(g, b, (T*)b.y, s, 0, useTop ? t.L0 : g.nLevels, queue);
     if (!useTop || t.L0 >= g.nLevels) return;
     const size_t B = (size_t)b.B;
     T* lu = (T*)b.lu;
@@ -926,7 +945,7 @@ __device__ void factorSystem(const DevGrid& g, const DevBatch& b, int s, T* sm, 
 
 // One system, the whole block: backward substitution of `vec` in place, the top in shared memory first.
 template <typename T>
-__device__ void backwardSystem(const DevGrid& g, const DevBatch& b, T* vec, int s, T* sm, bool useTop) {
+__device__ void backwardSystem(const DevGrid& g, const DevBatch& b, T* vec, int s, T* sm, bool useTop, int* queue) {
     const DevTop& t = topOf<T>(g);
     const int L0 = useTop ? t.L0 : g.nLevels;
     if (L0 < g.nLevels) {
@@ -966,14 +985,14 @@ __device__ void backwardSystem(const DevGrid& g, const DevBatch& b, T* vec, int 
         for (int i = threadIdx.x; i < t.nNodes; i += blockDim.x) vec[(size_t)__ldg(t.nodes + i) * B + s] = sm[t.nSlots + i];
         __syncthreads();
     }
-    walkLevels<T, kWorkBackward>(g, b, vec, s, 0, L0);
+    walkLevels<T, kWorkBackward>(g, b, vec, s, 0, L0, queue);
 }
 
 // One system, the whole block: forward substitution of a second right-hand side `vec` in place.
 template <typename T>
-__device__ void forwardSystem(const DevGrid& g, const DevBatch& b, T* vec, int s, T* sm, bool useTop) {
+__device__ void forwardSystem(const DevGrid& g, const DevBatch& b, T* vec, int s, T* sm, bool useTop, int* queue) {
     const DevTop& t = topOf<T>(g);
-    walkLevels<T, kWorkForward>(g, b, vec, s, 0, useTop ? t.L0 : g.nLevels);
+    walkLevels<T, kWorkForward>(g, b, vec, s, 0, useTop ? t.L0 : g.nLevels, queue);
     if (!useTop || t.L0 >= g.nLevels) return;
     const size_t B = (size_t)b.B;
     const T* lu = (const T*)b.lu;
@@ -999,17 +1018,21 @@ __device__ void forwardSystem(const DevGrid& g, const DevBatch& b, T* vec, int s
     __syncthreads();
 }
 
-// Dynamic shared memory of the one-system kernels (the top part of the grid's schedule).
+// Dynamic shared memory of the one-system kernels: the top part of the grid's schedule (when used), then the piece
+// counters of the level walks.
 extern __shared__ __align__(16) unsigned char gsTopSmem[];
 
 // Levels [l0, l1) of a schedule for the listed systems, one CTA each (the wide levels below l0 run as per-level
-// launches over the same batch).
+// launches over the same batch). Dynamic shared memory: the walk's piece counters (QueueBytes).
 template <typename T, int W>
 __global__ void __launch_bounds__(kTailThreads) k_tail(DevGrid g, DevBatch b, T* vec, int l0, int l1) {
     const int s = b.activeList[blockIdx.x];
     if (W != kWorkFactor && vec != (T*)b.y && !b.refine[s]) return;  // uniform across the block
-    walkLevels<T, W>(g, b, vec, s, l0, l1);
+    walkLevels<T, W>(g, b, vec, s, l0, l1, reinterpret_cast<int*>(gsTopSmem));
 }
+
+// shared memory of the piece counters of a walk over every level of a grid
+inline size_t QueueBytes(int nLevels) { return (size_t)6 * nLevels * sizeof(int); }
 
 // One step of the few systems of a batch (their list in b.activeList): factorisation, backward substitution and,
 // in mixed precision, the FP64-residual refinement. Levels below `lt` (many entries each) run as per-level launches
@@ -1027,8 +1050,9 @@ int64_t FewSystemsSolve(const DevGrid& g, const DevBatch& b, const Symbolic& s, 
     const auto& bp = s.backward.levelItemPtr;
     const auto& vp = s.forward.levelItemPtr;
     const int L = s.nLevels;
+    const size_t qb = QueueBytes(L);
     auto backward = [&](T* vec) {
-        k_tail<T, kWorkBackward><<<nActive, kTailThreads, 0, st>>>(g, b, vec, lt, L);
+        k_tail<T, kWorkBackward><<<nActive, kTailThreads, qb, st>>>(g, b, vec, lt, L);
         launches++;
         for (int l = lt - 1; l >= 0; l--) level(k_level<T, kWorkBackward>, vec, bp[l], bp[l + 1]);
     };
@@ -1036,14 +1060,14 @@ int64_t FewSystemsSolve(const DevGrid& g, const DevBatch& b, const Symbolic& s, 
         level(k_level<T, kWorkFactor>, (T*)b.y, fp[2 * l], fp[2 * l + 1]);
         level(k_level<T, kWorkFactor>, (T*)b.y, fp[2 * l + 1], fp[2 * l + 2]);
     }
-    k_tail<T, kWorkFactor><<<nActive, kTailThreads, 0, st>>>(g, b, (T*)b.y, lt, L);
+    k_tail<T, kWorkFactor><<<nActive, kTailThreads, qb, st>>>(g, b, (T*)b.y, lt, L);
     launches++;
     if (afterFactor) cudaEventRecord(afterFactor, st);
     backward((T*)b.y);
     if (refine) {
         k_residual<T><<<dim3((s.n + 7) / 8, (nActive + 31) / 32), blk8, 0, st>>>(g, b, b.activeList, nActive);
         for (int l = 0; l < lt; l++) level(k_level<T, kWorkForward>, (T*)b.z, vp[l], vp[l + 1]);
-        k_tail<T, kWorkForward><<<nActive, kTailThreads, 0, st>>>(g, b, (T*)b.z, lt, L);
+        k_tail<T, kWorkForward><<<nActive, kTailThreads, qb, st>>>(g, b, (T*)b.z, lt, L);
         launches += 2;
         backward((T*)b.z);
     }
@@ -2350,7 +2374,7 @@ extern "C" int gs_pf_mismatch_noalloc(gs_grid* G, int32_t count, const double* d
 namespace gs {
 // the one-system kernels hold the top of the elimination tree in up to 200 KB of dynamic shared memory
 cudaError_t SetKernelAttributes() {
-    const int bytes = 210 * 1024;  // the 200 KB budget of the top part, with room to spare
+    const int bytes = 220 * 1024;  // the 200 KB budget of the top part plus the walk counters
     cudaError_t e = cudaSuccess;
     auto set = [&](const void* f) {
         if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);

@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(1024) k_newton(const DevGrid* grids, const Mul
                                                  SlotArena arena, const double* loadScale, const int* outage,
                                                  int* outStatus, int* outIters, double* outMis, double* outVm,
                                                  double* outVa, double tol, double divLimit, int maxIter,
-                                                 unsigned long long* steps, int useTopFlag) {
+                                                 unsigned long long* steps, int useTopFlag, int queueOffset) {
     __shared__ DevGrid sg;
     __shared__ int sItem, sGo;
     __shared__ double redD[32];
@@ -75,6 +75,7 @@ __global__ void __launch_bounds__(1024) k_newton(const DevGrid* grids, const Mul
     const bool mixed = sizeof(T) < sizeof(double);
     T* sm = reinterpret_cast<T*>(gsTopSmem);  // the top part of the current item's grid
     const bool useTop = useTopFlag != 0;
+    int* queue = reinterpret_cast<int*>(gsTopSmem + queueOffset);  // the level walks' piece counters
     for (;;) {
         if (tid == 0) sItem = atomicAdd(next, 1);
         __syncthreads();
@@ -148,14 +149,14 @@ __global__ void __launch_bounds__(1024) k_newton(const DevGrid* grids, const Mul
             }
             __syncthreads();
             if (!sGo) break;
-            factorSystem<T>(g, b, 0, sm, useTop);
-            backwardSystem<T>(g, b, (T*)b.y, 0, sm, useTop);
+            factorSystem<T>(g, b, 0, sm, useTop, queue);
+            backwardSystem<T>(g, b, (T*)b.y, 0, sm, useTop, queue);
             const int refine = mixed ? sc->refine : 0;
             if (refine) {
                 for (int i = tid; i < n; i += bd) busResidual<T>(g, b, i, 0);
                 __syncthreads();
-                forwardSystem<T>(g, b, (T*)b.z, 0, sm, useTop);
-                backwardSystem<T>(g, b, (T*)b.z, 0, sm, useTop);
+                forwardSystem<T>(g, b, (T*)b.z, 0, sm, useTop, queue);
+                backwardSystem<T>(g, b, (T*)b.z, 0, sm, useTop, queue);
             }
             const T* y = (const T*)b.y;
             const T* z = (const T*)b.z;
@@ -272,12 +273,18 @@ extern "C" int gs_pf_solve_multi(gs_ctx* ctx, int32_t nGrids, gs_grid* const* gr
     const int candThreads[kCand] = {1024, 512, 256, 1024, 512, 256};
     const int candTop[kCand] = {0, 0, 0, 1, 1, 1};
     size_t topBytes = 16;
+    int maxLevels = 1;
     for (int k = 0; k < nGrids; k++)
-        if (counts[k] > 0) topBytes = std::max(topBytes, grids[k]->sym.top[mixed ? 1 : 0].bytes(t));
+        if (counts[k] > 0) {
+            topBytes = std::max(topBytes, grids[k]->sym.top[mixed ? 1 : 0].bytes(t));
+            maxLevels = std::max(maxLevels, grids[k]->sym.nLevels);
+        }
+    topBytes = (topBytes + 15) / 16 * 16;
+    const size_t queueBytes = QueueBytes(maxLevels);
     int ctasOf[kCand];
     for (int q = 0; q < kCand; q++) {
         int occ = 0;
-        const size_t sm = candTop[q] ? topBytes : 0;
+        const size_t sm = (candTop[q] ? topBytes : 0) + queueBytes;
         cudaError_t e = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_newton<float>, candThreads[q], sm)
                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_newton<double>, candThreads[q], sm);
         if (e != cudaSuccess) return SetErr(ctx, GS_ERR_CUDA, std::string("occupancy: ") + cudaGetErrorString(e));
@@ -315,17 +322,18 @@ extern "C" int gs_pf_solve_multi(gs_ctx* ctx, int32_t nGrids, gs_grid* const* gr
     if (vmOut) GS_CUDA(dVm.alloc((size_t)nStates * 8));
     if (vaOut) GS_CUDA(dVa.alloc((size_t)nStates * 8));
     auto launch = [&](int q, const MultiItem* its, int nIts) {
-        const size_t sm = candTop[q] ? topBytes : 0;
+        const size_t sm = (candTop[q] ? topBytes : 0) + queueBytes;
+        const int qOff = candTop[q] ? (int)topBytes : 0;
         if (mixed)
             k_newton<float><<<ctasOf[q], candThreads[q], sm, st>>>(
                 dViews.as<DevGrid>(), its, nIts, dNext.as<int>(), arena, dScale.as<double>(), dOut.as<int>(),
                 dStatus.as<int>(), dIters.as<int>(), dMis.as<double>(), dVm.as<double>(), dVa.as<double>(), o.tolerance,
-                o.diverge_limit_pu, o.max_iterations, dSteps.as<unsigned long long>(), candTop[q]);
+                o.diverge_limit_pu, o.max_iterations, dSteps.as<unsigned long long>(), candTop[q], qOff);
         else
             k_newton<double><<<ctasOf[q], candThreads[q], sm, st>>>(
                 dViews.as<DevGrid>(), its, nIts, dNext.as<int>(), arena, dScale.as<double>(), dOut.as<int>(),
                 dStatus.as<int>(), dIters.as<int>(), dMis.as<double>(), dVm.as<double>(), dVa.as<double>(), o.tolerance,
-                o.diverge_limit_pu, o.max_iterations, dSteps.as<unsigned long long>(), candTop[q]);
+                o.diverge_limit_pu, o.max_iterations, dSteps.as<unsigned long long>(), candTop[q], qOff);
     };
     // autotuner: the CTA shape per set of grids (and precision), from timed trials on a sample of the items
     std::string key = mixed ? "m" : "d";
