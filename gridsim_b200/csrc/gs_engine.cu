@@ -86,7 +86,15 @@ __device__ __forceinline__ void busMismatchJac(const DevGrid& g, const DevBatch&
     if (pOut) { pOut[i * B + s] = P; qOut[i * B + s] = Q; }
     double sc = b.loadScale ? b.loadScale[i * B + s] : 1.0;
     const double pspec = b.loadScale ? g.pgen[i] - sc * g.pload[i] : g.pgen[i] - g.pload[i];
-    const double qspec = b.loadScale ? g.qgen[i] - sc * g.qload[i] : g.qgen[i] - g.qload[i];
+    double qspec = b.loadScale ? g.qgen[i] - sc * g.qload[i] : g.qgen[i] - g.qload[i];
+    // Q limits: a bus that starts PV keeps an identity Q row while it is PV (its Vm step is 0, its Q mismatch
+    // is not an equation); once switched to PQ its Q is held at the limit
+    const bool startsPV = g.qlim && g.busType[i] == 2;
+    const bool pvNow = startsPV && b.effType[i * B + s] == 2;
+    if (startsPV) {
+        b.qinj[i * B + s] = Q;
+        if (!pvNow) qspec = b.qspecSys[i * B + s];
+    }
     T* y = (T*)b.y;
     const int kp = g.busP[i], kq = g.busQ[i];
     if (kp >= 0) {
@@ -96,7 +104,10 @@ __device__ __forceinline__ void busMismatchJac(const DevGrid& g, const DevBatch&
         localMax = fmax(localMax, fabs(f));
         bad |= isfinite(f) ? 0 : 1;
     }
-    if (kq >= 0) {
+    if (kq >= 0 && pvNow) {
+        y[kq * B + s] = T(0);
+        if (b.rhs64) b.rhs64[kq * B + s] = 0.0;
+    } else if (kq >= 0) {
         const double f = qspec - Q;
         y[kq * B + s] = (T)f;
         if (b.rhs64) b.rhs64[kq * B + s] = f;
@@ -126,6 +137,10 @@ __device__ __forceinline__ void busMismatchJac(const DevGrid& g, const DevBatch&
                 N = vmi * (G * cs + Bv * sn);
                 M = -vmi * vmj * (G * cs + Bv * sn);
                 L = vmi * (G * sn - Bv * cs);
+            }
+            if (pvNow) {  // the identity Q row of a bus that is PV now
+                M = 0.0;
+                L = i == j ? 1.0 : 0.0;
             }
             const int4 sl = *reinterpret_cast<const int4*>(g.ySlot + 4 * p);
             if (sl.x >= 0) lu[sl.x * B + s] = (T)H;
@@ -212,6 +227,107 @@ __global__ void k_status(DevBatch b, int iter, double tol, double divLimit, int 
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= b.count || !b.active[s]) return;
     statusStep(b, s, iter, tol, divLimit, maxIter);
+}
+
+// ---- Q-limit enforcement (SparseNewtonRaphsonPowerFlow.Solve's Q-limit passes, SparseNewtonRaphsonPowerFlow.cs:118-160;
+//      NewtonShell.ApplyQLimits :519-558, RevertBrokenPins :593-603, TryRevertPin :563-576). Every pass is a Newton run
+//      of its own (its first mismatch is the divergence reference, the iteration cap counts its steps). When a pass
+//      converges, PV buses whose generator Q is beyond the aggregate limits (by more than 1e-3 MVAr) become PQ with
+//      Q held at the limit; if none does, pinned buses whose voltage crossed the set point (by 1e-4 pu) revert to
+//      PV once each. Any change starts the next pass from the present state (up to 100 passes, then one last run
+//      whose end is not a convergence); no change ends the solve converged.
+constexpr double kQLimitTolMva = 1e-3;      // NewtonShell.cs:26
+constexpr double kRevertVoltTolPu = 1e-4;   // NewtonShell.cs:31
+constexpr int kMaxQPasses = 100;            // PowerFlowOptions.MaxQLimitPasses default
+enum : int32_t { kQReverted = 16 };
+
+__global__ void k_status_q(DevBatch b, double tol, double divLimit, int maxIter) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= b.count || !b.active[s]) return;
+    b.qState[s] &= ~kQSkipStep;
+    const int iter = b.passIter[s];
+    const double mis = __longlong_as_double((long long)b.maxMis[s]);
+    b.maxMis[s] = 0ull;
+    b.maxDx[s] = 0ull;
+    const int fl = b.flags[s];
+    if (fl & kFlagNonFinite) { b.finalMis[s] = NAN; b.status[s] = GS_PF_NON_FINITE; b.active[s] = 0; return; }
+    if (fl & kFlagStepBad) { b.status[s] = GS_PF_MAX_ITERATIONS; b.active[s] = 0; return; }
+    b.finalMis[s] = mis;
+    if (iter == 0) b.startMis[s] = mis;
+    if (mis < tol) {
+        if (b.qState[s] & kQFinalPass) { b.status[s] = GS_PF_MAX_ITERATIONS; b.active[s] = 0; return; }
+        b.qState[s] |= kQPending;  // the Q limits decide (k_qapply, k_qrevert, k_qfinish)
+        return;
+    }
+    if (mis > fmax(divLimit, b.startMis[s])) { b.status[s] = GS_PF_DIVERGED; b.active[s] = 0; return; }
+    if (iter >= maxIter) { b.status[s] = GS_PF_MAX_ITERATIONS; b.active[s] = 0; return; }
+    if (fl & kFlagJacBad) { b.status[s] = GS_PF_MAX_ITERATIONS; b.active[s] = 0; return; }
+    if (b.refine) {
+        const int r = mis < kRefineBelowPu ? 1 : 0;
+        b.refine[s] = r;
+        if (r) atomicAdd(b.activeCount + 1, 1);
+    }
+    atomicAdd(b.activeCount, 1);
+}
+
+// ApplyQLimits on the systems whose pass converged: grid (ceil(n / 8), B / 32), block (32, 8).
+__global__ void k_qapply(DevGrid g, DevBatch b) {
+    const int s = blockIdx.y * 32 + threadIdx.x, i = blockIdx.x * 8 + threadIdx.y;
+    if (i >= g.n || s >= b.count || !b.active[s] || !(b.qState[s] & kQPending) || g.busType[i] != 2) return;
+    const size_t idx = (size_t)i * b.B + s;
+    if (b.effType[idx] != 2) return;
+    const double qd = (b.loadScale ? b.loadScale[idx] : 1.0) * g.qload[i];  // the bus's load, pu
+    const double qGen = (b.qinj[idx] + qd) * g.baseMva;
+    const bool fixed = g.qminMvar[i] == g.qmaxMvar[i];
+    if (qGen > g.qmaxMvar[i] + kQLimitTolMva) {
+        b.effType[idx] = 1;
+        b.qspecSys[idx] = g.qmaxPu[i] - qd;
+        b.pinned[idx] = fixed ? 2 : 1;
+        atomicOr(&b.qState[s], kQChanged);
+    } else if (qGen < g.qminMvar[i] - kQLimitTolMva) {
+        b.effType[idx] = 1;
+        b.qspecSys[idx] = g.qminPu[i] - qd;
+        b.pinned[idx] = fixed ? 2 : -1;
+        atomicOr(&b.qState[s], kQChanged);
+    }
+}
+
+// RevertBrokenPins on the systems whose pass converged without a switch.
+__global__ void k_qrevert(DevGrid g, DevBatch b) {
+    const int s = blockIdx.y * 32 + threadIdx.x, i = blockIdx.x * 8 + threadIdx.y;
+    if (i >= g.n || s >= b.count || !b.active[s] || g.busType[i] != 2) return;
+    const int st = b.qState[s];
+    if (!(st & kQPending) || (st & kQChanged)) return;
+    const size_t idx = (size_t)i * b.B + s;
+    const int pin = b.pinned[idx];
+    if (b.effType[idx] != 1 || (pin != 1 && pin != -1) || b.reverted[idx] >= 1) return;
+    const double vm = b.vm[idx], vg = g.vm0[i];
+    if ((pin == 1 && vm > vg + kRevertVoltTolPu) || (pin == -1 && vm < vg - kRevertVoltTolPu)) {
+        b.effType[idx] = 2;
+        b.vm[idx] = vg;
+        b.pinned[idx] = 0;
+        b.reverted[idx] += 1;
+        atomicOr(&b.qState[s], kQReverted);
+    }
+}
+
+// The end of a converged pass: a switch starts the next pass (this iteration's step is not taken), else converged.
+__global__ void k_qfinish(DevBatch b) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= b.count || !b.active[s]) return;
+    const int st = b.qState[s];
+    if (!(st & kQPending)) return;
+    if (st & (kQChanged | kQReverted)) {
+        b.qPass[s] += 1;
+        b.passIter[s] = 0;
+        b.qState[s] = kQSkipStep | (b.qPass[s] >= kMaxQPasses ? kQFinalPass : 0);
+        atomicAdd(b.activeCount, 1);
+    } else {
+        b.status[s] = GS_PF_CONVERGED;
+        b.convIters[s] = b.iters[s];
+        b.active[s] = 0;
+        b.qState[s] = 0;
+    }
 }
 
 // Systems admitted at different times (the request loop): each at its own step count. Systems that stop
@@ -466,6 +582,7 @@ __global__ void __launch_bounds__(32 * kPersistWarps) k_persistent(DevGrid g, De
 template <typename T>
 __device__ __forceinline__ void busResidual(const DevGrid& g, const DevBatch& b, int i, int s) {
     const size_t B = (size_t)b.B;
+    const bool pvNow = g.qlim && g.busType[i] == 2 && b.effType[i * B + s] == 2;
     const int kp = g.busP[i], kq = g.busQ[i];
     if (kp < 0 && kq < 0) return;
     const T* dx = (const T*)b.y;
@@ -525,7 +642,7 @@ __device__ __forceinline__ void busResidual(const DevGrid& g, const DevBatch& b,
         jq += M * dth + L * dv;
     }
     if (kp >= 0) z[kp * B + s] = (T)(b.rhs64[kp * B + s] - jp);
-    if (kq >= 0) z[kq * B + s] = (T)(b.rhs64[kq * B + s] - jq);
+    if (kq >= 0) z[kq * B + s] = pvNow ? T(0) : (T)(b.rhs64[kq * B + s] - jq);
 }
 
 template <typename T>
@@ -562,6 +679,17 @@ __device__ __forceinline__ void moveSystem(const DevBatch& from, int sf, const D
     to.vm[i * Bt + st] = from.vm[i * Bf + sf];
     to.va[i * Bt + st] = from.va[i * Bf + sf];
     if (from.loadScale && to.loadScale) const_cast<double*>(to.loadScale)[i * Bt + st] = from.loadScale[i * Bf + sf];
+    if (from.qState && to.qState) {
+        to.effType[i * Bt + st] = from.effType[i * Bf + sf];
+        to.qspecSys[i * Bt + st] = from.qspecSys[i * Bf + sf];
+        to.pinned[i * Bt + st] = from.pinned[i * Bf + sf];
+        to.reverted[i * Bt + st] = from.reverted[i * Bf + sf];
+        if (i == 0) {
+            to.passIter[st] = from.passIter[sf];
+            to.qPass[st] = from.qPass[sf];
+            to.qState[st] = from.qState[sf];
+        }
+    }
     if (i != 0) return;
     to.maxMis[st] = from.maxMis[sf];
     to.maxDx[st] = from.maxDx[sf];
@@ -1124,7 +1252,10 @@ __device__ __forceinline__ void busUpdate(const DevGrid& g, const DevBatch& b, i
         if (v < kVmFloorPu) v = kVmFloorPu;
         b.vm[i * B + s] = v;
     }
-    if (i == 0) b.iters[s] += 1;
+    if (i == 0) {
+        b.iters[s] += 1;
+        if (b.passIter) b.passIter[s] += 1;
+    }
 }
 
 template <typename T>
@@ -1134,6 +1265,7 @@ __global__ void __launch_bounds__(256) k_update(DevGrid g, DevBatch b, int refin
     const int i = blockIdx.x * 8 + threadIdx.y;
     if (i >= g.n || s < 0 || s >= b.count || !b.active[s]) return;
     if (b.flags[s] & kFlagStepBad) return;
+    if (b.qState && (b.qState[s] & kQSkipStep)) return;  // a new Q-limit pass starts from this state
     busUpdate<T>(g, b, i, s, refine);
 }
 
@@ -1152,6 +1284,13 @@ __global__ void k_init(DevGrid g, DevBatch b, const double* vmStart, const doubl
     if (g.busType[i] == 3) va = g.va0[i];
     b.vm[i * B + s] = vm;
     b.va[i * B + s] = va;
+    if (b.qState) {
+        b.effType[i * B + s] = g.busType[i];
+        b.qspecSys[i * B + s] = 0.0;
+        b.pinned[i * B + s] = 0;
+        b.reverted[i * B + s] = 0;
+        if (i == 0) { b.passIter[s] = 0; b.qPass[s] = 0; b.qState[s] = 0; }
+    }
     if (i == 0) {
         b.maxMis[s] = 0ull;
         b.maxDx[s] = 0ull;
@@ -1318,6 +1457,7 @@ struct Workspace {
     int B = 0;
     int precision = -1;
     DevBuf activeList, origin;  // origin: a compact batch position -> the system of the full batch
+    DevBuf effType, qspecSys, pinned, reverted, qinj, passIter, qPass, qState;  // Q-limit enforcement
     DevBuf vm, va, lu, piv, y, z, rhs64, refine, maxMis, maxDx, startMis, finalMis, status, iters, convIters, active, flags, outage,
         loadScale, activeCount;
     DevBuf code, value, maxLoad, minVmNeg, maxVmB, chunkCount, chunkOffset, outKind, outElem, outVal, pq;
@@ -1344,6 +1484,7 @@ struct gs_grid {
     std::vector<double> pgen, qgen, pload, qload;
     gs::Workspace ws;
     gs::Workspace tws;  // compact copy of the few systems still stepping
+    std::unique_ptr<gs_grid> qgrid;  // the same grid analysed for Q-limit enforcement (built on first use)
     int split = 0;      // first level run by the persistent kernels
     int tailSplit = 0;  // first level the few-systems path runs as one CTA per system
 };
@@ -1381,6 +1522,8 @@ int UploadGrid(gs_grid* G) {
     const Symbolic& s = G->sym;
     DevGrid& v = G->view;
     v.n = s.n; v.m = s.m; v.nnzY = s.nnzY; v.nbr = s.nbr; v.nnzLU = s.nnzLU; v.nLevels = s.nLevels;
+    v.qlim = s.qlim ? 1 : 0;
+    v.baseMva = h.base;
     const int n = h.n;
     G->pgen.assign(n, 0.0); G->qgen.assign(n, 0.0);
     for (int k = 0; k < h.ngen; k++) {
@@ -1403,6 +1546,11 @@ int UploadGrid(gs_grid* G) {
     UP(s.brCell, brCell); UP(s.brRed, brRed); UP(s.brStamp, brStamp);
     UP(h.brF, brF); UP(h.brT, brT); UP(rate, rateA); UP(h.brOn, brOn);
     UP(G->pgen, pgen); UP(G->qgen, qgen); UP(G->pload, pload); UP(G->qload, qload);
+    {
+        std::vector<double> qminPu(n), qmaxPu(n);
+        for (int i = 0; i < n; i++) { qminPu[i] = s.qminMvar[i] / h.base; qmaxPu[i] = s.qmaxMvar[i] / h.base; }
+        UP(qminPu, qminPu); UP(qmaxPu, qmaxPu); UP(s.qminMvar, qminMvar); UP(s.qmaxMvar, qmaxMvar);
+    }
     UP(s.vm0, vm0); UP(s.va0, va0); UP(s.type0, busType); UP(s.busP, busP); UP(s.busQ, busQ); UP(s.ySlot, ySlot);
     UP(s.entSlot, entSlot); UP(s.entKind, entKind); UP(s.entHasA, entHasA);
     UP(s.entPairPtr, entPairPtr); UP(pairs, pairs); UP(s.diagPairNode, diagEnt); UP(s.levelNodes, levelNodes);
@@ -1482,6 +1630,12 @@ size_t PerSystemBytes(const Symbolic& s, int precision) {
 }
 
 int EnsureWs(gs_ctx* ctx, const Symbolic& s, Workspace& w, int B, int precision, bool classify, bool loadScale) {
+    if (s.qlim) {
+        const size_t nb = (size_t)s.n * B;
+        GS_CUDA(w.effType.alloc(nb * 4)); GS_CUDA(w.qspecSys.alloc(nb * 8)); GS_CUDA(w.pinned.alloc(nb * 4));
+        GS_CUDA(w.reverted.alloc(nb * 4)); GS_CUDA(w.qinj.alloc(nb * 8));
+        GS_CUDA(w.passIter.alloc((size_t)B * 4)); GS_CUDA(w.qPass.alloc((size_t)B * 4)); GS_CUDA(w.qState.alloc((size_t)B * 4));
+    }
     size_t t = precision == GS_PREC_MIXED ? 4 : 8;
     size_t Bz = (size_t)B;
     GS_CUDA(w.vm.alloc(s.n * Bz * 8));
@@ -1540,6 +1694,11 @@ DevBatch MakeBatchWs(const Workspace& w, int nLevels, int B, int count, bool use
     b.activeCount = w.activeCount.as<int>();
     b.activeList = w.activeList.as<int>();
     b.nLevels = nLevels;
+    if (w.qState.p) {
+        b.effType = w.effType.as<int>(); b.qspecSys = w.qspecSys.as<double>(); b.pinned = w.pinned.as<int>();
+        b.reverted = w.reverted.as<int>(); b.qinj = w.qinj.as<double>(); b.passIter = w.passIter.as<int>();
+        b.qPass = w.qPass.as<int>(); b.qState = w.qState.as<int>();
+    }
     return b;
 }
 
@@ -1666,7 +1825,9 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
     DevBatch cur = b;
     bool compacted = false;
     const dim3 nodeBlocks((s.n + 7) / 8);
-    for (int iter = 0; iter <= o.max_iterations + 4; iter++) {
+    // with Q limits every pass may take up to max_iterations steps (plus the step-less pass switches)
+    const int maxLoop = g.qlim ? (o.max_iterations + 2) * (kMaxQPasses + 2) : o.max_iterations + 4;
+    for (int iter = 0; iter <= maxLoop; iter++) {
         if (timed) cudaEventRecord(ev[0], st);
         if (listCount > 0)
             k_mismatch_jac<T><<<dim3(nodeBlocks.x, (listCount + 31) / 32), blk8, 0, st>>>(g, cur, 1, nullptr, nullptr,
@@ -1675,7 +1836,15 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             k_mismatch_jac<T><<<dim3(nodeBlocks.x, cur.B / 32), blk8, 0, st>>>(g, cur, 1, nullptr, nullptr, nullptr, 0);
         if (timed) cudaEventRecord(ev[1], st);
         cudaMemsetAsync(cur.activeCount, 0, 2 * sizeof(int), st);
-        k_status<<<(cur.count + 255) / 256, 256, 0, st>>>(cur, iter, o.tolerance, o.diverge_limit_pu, o.max_iterations);
+        if (g.qlim) {
+            k_status_q<<<(cur.count + 255) / 256, 256, 0, st>>>(cur, o.tolerance, o.diverge_limit_pu, o.max_iterations);
+            k_qapply<<<dim3(nodeBlocks.x, cur.B / 32), blk8, 0, st>>>(g, cur);
+            k_qrevert<<<dim3(nodeBlocks.x, cur.B / 32), blk8, 0, st>>>(g, cur);
+            k_qfinish<<<(cur.count + 255) / 256, 256, 0, st>>>(cur);
+            launches += 3;
+        } else {
+            k_status<<<(cur.count + 255) / 256, 256, 0, st>>>(cur, iter, o.tolerance, o.diverge_limit_pu, o.max_iterations);
+        }
         launches += 2;
         cudaMemcpyAsync(ctx->pinnedCount, cur.activeCount, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
         ce = cudaStreamSynchronize(st);
@@ -1795,8 +1964,6 @@ int NewtonDispatch(gs_grid* G, int count, bool useScale, bool startFromWs, const
 
 int CheckOpts(gs_ctx* ctx, const gs_pf_opts* o) {
     if (!o) return SetErr(ctx, GS_ERR_INVALID_ARG, "null options");
-    if (o->enforce_q_limits)
-        return SetErr(ctx, GS_ERR_UNSUPPORTED, "enforce_q_limits: the PV->PQ switching loop is not built yet");
     if (o->retry_from_dc_start)
         return SetErr(ctx, GS_ERR_UNSUPPORTED, "retry_from_dc_start: the DC-angle retry is not built yet");
     if (!(o->tolerance > 0) || o->tolerance > 1e-2) return SetErr(ctx, GS_ERR_INVALID_ARG, "tolerance must be in (0, 1e-2]");
@@ -1821,6 +1988,23 @@ int ChooseB(gs_grid* G, int want, const gs_pf_opts& o) {
 }
 
 // Solve the intact grid once in system 0 of the workspace (B = 32) and keep its state in startVm/Va.
+// The grid analysed for Q-limit enforcement (the same host data; every PV bus has a Q equation in its pattern),
+// built on the first call that enforces Q limits.
+int QGridOf(gs_grid* G, gs_grid** out) {
+    if (!G->qgrid) {
+        auto Q = std::make_unique<gs_grid>();
+        Q->ctx = G->ctx;
+        Q->host = G->host;
+        std::string err = Analyze(Q->host, Q->sym, true);
+        if (!err.empty()) return SetErr(G->ctx, GS_ERR_INVALID_ARG, err);
+        int rc = UploadGrid(Q.get());
+        if (rc) return rc;
+        G->qgrid = std::move(Q);
+    }
+    *out = G->qgrid.get();
+    return GS_OK;
+}
+
 int SolveBase(gs_grid* G, const gs_pf_opts& o, int* status, int* iters, double* mis, float* ms) {
     gs_ctx* ctx = G->ctx;
     int rc = EnsureWorkspace(G, 32, o.precision, false, false);
@@ -1954,6 +2138,7 @@ int gs_pf_solve(gs_grid* G, const gs_pf_opts* opts, gs_pf_result* res) {
     gs_pf_opts o = *opts;
     if (o.flat_start) return SetErr(ctx, GS_ERR_UNSUPPORTED, "flat_start: pass a flat start in the descriptor");
     GS_CUDA(cudaSetDevice(ctx->device));
+    if (o.enforce_q_limits && (rc = QGridOf(G, &G)) != GS_OK) return rc;
     int st = 0, it = 0;
     double mis = 0;
     float ms = 0;
@@ -2020,6 +2205,10 @@ int gs_pf_solve_batch(gs_grid* G, int32_t count, const double* loadScale, const 
     if (rc) return rc;
     gs_pf_opts o = *opts;
     if (o.flat_start) return SetErr(ctx, GS_ERR_UNSUPPORTED, "flat_start: pass a flat start in the descriptor");
+    if (o.enforce_q_limits) {
+        GS_CUDA(cudaSetDevice(ctx->device));
+        if ((rc = QGridOf(G, &G)) != GS_OK) return rc;
+    }
     const Symbolic& s = G->sym;
     if (outage)
         for (int k = 0; k < count; k++)
@@ -2078,6 +2267,10 @@ int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts*
     if (rc) return rc;
     gs_pf_opts o = *opts;
     if (o.flat_start) return SetErr(ctx, GS_ERR_UNSUPPORTED, "flat_start: pass a flat start in the descriptor");
+    if (o.enforce_q_limits) {
+        GS_CUDA(cudaSetDevice(ctx->device));
+        if ((rc = QGridOf(G, &G)) != GS_OK) return rc;
+    }
     const Symbolic& s = G->sym;
     const HostGrid& h = G->host;
     for (int k = 0; k < nOut; k++)  // AN-02: an out-of-service branch is refused (ContingencyAnalysis.cs:290-300)

@@ -43,6 +43,9 @@ struct Symbolic {
     std::vector<int> type0, pPos, qPos;
     int m = 0, npv = 0, npq = 0;
     std::vector<double> pspec, qspec, vm0, va0;  // va0 radians
+    // Q-limit enforcement (qlim): the Q equation of every PV bus is in the pattern; per-bus aggregate limits
+    bool qlim = false;
+    std::vector<double> qminMvar, qmaxMvar;
     // ---- Jacobian superset pattern and the minimum-degree order ----
     int nnzJ = 0;
     std::vector<int> jRowPtr, jCol;
@@ -119,7 +122,7 @@ struct Symbolic {
 void BuildTopPart(Symbolic& s, int which, size_t elem, size_t budget);
 
 // Build the symbolic analysis; returns an empty string on success, else the reason.
-std::string Analyze(const HostGrid& g, Symbolic& s);
+std::string Analyze(const HostGrid& g, Symbolic& s, bool qlim = false);
 
 // Minimum-degree order of a structurally symmetric pattern (pivot step -> index).
 std::vector<int> MinimumDegreeOrder(int n, const std::vector<int>& rowPtr, const std::vector<int>& col);

@@ -51,6 +51,12 @@ struct DevGrid {
     int n, m, nnzY, nbr;
     int64_t nnzLU;
     int nLevels;          // elimination-tree levels of the schedules
+    int qlim;             // Q-limit enforcement: PV buses have a Q equation (an identity row while PV)
+    double baseMva;
+    const double* qminPu; // aggregate reactive limits per bus (pu)
+    const double* qmaxPu;
+    const double* qminMvar;
+    const double* qmaxMvar;
     const int* yRowPtr;
     const int* yCol;
     const double* yG;
@@ -135,6 +141,18 @@ struct DevBatch {
     const double* loadScale;  // [n][B] or null
     int* activeCount;       // [2]: systems still stepping, of which refine their step (mixed precision)
     int* activeList;        // [B] systems still stepping (filled for the few-systems path)
+    // Q-limit enforcement (grids with qlim), else null
+    int* effType;           // [n][B] the bus's type now (2 PV, 1 switched to PQ), for buses that start PV
+    double* qspecSys;       // [n][B] Q specification of a switched bus (pu)
+    int* pinned;            // [n][B] 0 none, 1 at Qmax, -1 at Qmin, 2 fixed (Qmin == Qmax)
+    int* reverted;          // [n][B] reverts to PV so far
+    double* qinj;           // [n][B] Q injection at the last mismatch (pu)
+    int* passIter;          // [B] steps of the current Q-limit pass
+    int* qPass;             // [B] passes completed
+    int* qState;            // [B] kQ* bits
 };
+
+// qState bits
+enum : int32_t { kQPending = 1, kQChanged = 2, kQSkipStep = 4, kQFinalPass = 8 };
 
 }  // namespace gs

@@ -97,11 +97,12 @@ std::vector<int> MinimumDegreeOrder(int n, const std::vector<int>& rowPtr, const
     return order;
 }
 
-std::string Analyze(const HostGrid& g, Symbolic& s) {
+std::string Analyze(const HostGrid& g, Symbolic& s, bool qlim) {
     const int n = g.n;
     s = Symbolic();
     s.n = n;
     s.nbr = g.nbr;
+    s.qlim = qlim;
 
     // ---------------- Y-bus (stamping order: in-service branches in order, then bus shunts) ----------------
     struct Contribution { int row, col, owner; double gv, bv; };  // owner: branch index or -1 (shunt)
@@ -169,11 +170,15 @@ std::string Analyze(const HostGrid& g, Symbolic& s) {
     // ---------------- bus specification and equation numbering ----------------
     std::vector<double> pgB(n, 0), qgB(n, 0), vgB(n, 0);
     std::vector<char> hasGen(n, 0);
+    s.qminMvar.assign(n, 0.0);
+    s.qmaxMvar.assign(n, 0.0);
     for (int k = 0; k < g.ngen; k++) {
         if (!g.genOn[k]) continue;
         int i = g.genBus[k];
         pgB[i] += g.pg[k];
         qgB[i] += g.qg[k];
+        s.qminMvar[i] += g.qmin[k];  // the bus's aggregate reactive limits (NewtonShell.BuildBusSpec)
+        s.qmaxMvar[i] += g.qmax[k];
         vgB[i] = g.vg[k];  // the last unit at the bus sets the voltage
         hasGen[i] = 1;
     }
@@ -191,7 +196,9 @@ std::string Analyze(const HostGrid& g, Symbolic& s) {
     s.qPos.assign(n, -1);
     int m = 0;
     for (int i = 0; i < n; i++) if (s.type0[i] != 3) s.pPos[i] = m++;
-    for (int i = 0; i < n; i++) if (s.type0[i] == 1) { s.qPos[i] = m++; s.npq++; }
+    // with Q limits every PV bus may become PQ: its Q equation is in the pattern (an identity row while PV)
+    for (int i = 0; i < n; i++)
+        if (s.type0[i] == 1 || (qlim && s.type0[i] == 2)) { s.qPos[i] = m++; if (s.type0[i] == 1) s.npq++; }
     for (int i = 0; i < n; i++) if (s.type0[i] == 2) s.npv++;
     s.m = m;
     if (m == 0) return "the grid has no unknowns";

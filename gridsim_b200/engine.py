@@ -26,8 +26,10 @@ from .model import GridModel
 
 @dataclass
 class PowerFlowOptions:
-    """PowerFlowOptions (``PowerFlow/PowerFlowOptions.cs``). Q-limit enforcement and the DC-angle retry are
-    reference features this engine does not run yet: they default to off here and are refused when set."""
+    """PowerFlowOptions (``PowerFlow/PowerFlowOptions.cs``). Q-limit enforcement (PV -> PQ switching passes,
+    up to 100, with the reference's reverts) runs on the device for single solves, batch solves and screens; the
+    DC-angle retry is not built and is refused when set. Both default to off here (the reference defaults them on,
+    ``PowerFlowOptions.cs:98,121``) because the benchmark workloads run without them."""
     tolerance: float = 1e-8
     max_iterations: int = 30
     diverge_limit_pu: float = 10.0
@@ -56,9 +58,13 @@ class PowerFlowOptions:
         return o
 
 
-# ContingencyAnalysis.StudyOptions (ContingencyAnalysis.cs:263-268) is 100 iterations with Q limits on; the
-# Q-limit loop is not built yet, so the study set here keeps only the iteration cap.
+# ContingencyAnalysis.StudyOptions (ContingencyAnalysis.cs:263-268): 100 iterations with Q limits on.
 STUDY_MAX_ITERATIONS = 100
+
+
+def study_options(precision: str = "fp64") -> "PowerFlowOptions":
+    """ContingencyAnalysis.StudyOptions: the options every contingency study of the reference solves with."""
+    return PowerFlowOptions(max_iterations=STUDY_MAX_ITERATIONS, enforce_q_limits=True, precision=precision)
 
 
 @dataclass

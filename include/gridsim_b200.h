@@ -117,7 +117,9 @@ typedef struct gs_pf_opts {
     double diverge_limit_pu;        /* default 10; +inf turns the stop off */
     int32_t max_iterations;         /* default 30 (StudyOptions 100) */
     int32_t flat_start;             /* default 0 */
-    int32_t enforce_q_limits;       /* must be 0 in this build (GS_ERR_UNSUPPORTED otherwise) */
+    int32_t enforce_q_limits;       /* PV->PQ switching passes (SparseNewtonRaphsonPowerFlow.cs:118-160); default 0
+                                       here (the reference's default is on); refused by the multi-grid batch and
+                                       the request loop */
     int32_t retry_from_dc_start;    /* must be 0 in this build */
     int32_t per_bus_voltage_limits; /* judge buses against their own vmin/vmax (VoltageLimits.cs:55-67) */
     int32_t precision;              /* enum gs_precision */
