@@ -376,11 +376,13 @@ def run_ours(args):
     # the narrow-top k_persistent<float, 0>), its algorithmic bytes (J read + L, U written per system stepped)
     fb, fms = prof["level_factor_bytes"], prof["level_factor_ms"]
     achieved = fb / (fms / 1e3) / 1e9 if fms > 0 else None
+    # measured DRAM bytes of one factorisation per system (ncu, committed under profiles/), against the same
+    # unit as `achieved`'s numerator: bytes per system and full-batch factorisation
     traffic = None
-    tf = os.path.join(ROOT, "profiles", "factor_traffic_per_launch.json")
+    tf = os.path.join(ROOT, "profiles", "factor_traffic_per_system.json")
     if os.path.exists(tf):
         with open(tf) as fh:
-            traffic = json.load(fh).get("bytes_per_launch")
+            traffic = json.load(fh).get("bytes_per_system")
     # accuracy against the oracle on a small sample (untimed)
     acc = None
     if rank == 0 and not args.no_check:
@@ -429,6 +431,8 @@ def run_ours(args):
                          "kernel": "k_level<float,0> + k_persistent<float,0>: fused static-pivot LU + forward "
                                    "substitution of full-batch iterations",
                          "bytes_per_system": 4 * (info.nnz_j + info.nnz_lu),
+                         "traffic_unit": "DRAM bytes per system and full-batch factorisation (ncu), beside "
+                                         "bytes_per_system (algorithmic)",
                          "peak_source": peak_kind},
             "phase_ms": {"factor": prof["factor_ms"], "solve": prof["solve_ms"], "mismatch": prof["mismatch_ms"],
                          "other": prof["other_ms"], "few_systems_path": prof["tail_ms"],
