@@ -360,9 +360,12 @@ __device__ __forceinline__ T dotSP(const T* __restrict__ lu, const T* __restrict
     const int lane = threadIdx.x & 31;
     const int pl = lane / S;
     T acc = T(0);
+    // the next batch's index pairs are loaded while this batch's operands are in flight
+    int2 next = q0 + lane < q1 ? __ldg(pr + q0 + lane) : make_int2(0, 0);
     for (int64_t base = q0; base < q1; base += 32) {
         const int cnt = (int)min((int64_t)32, q1 - base);
-        const int2 mine = lane < cnt ? __ldg(pr + base + lane) : make_int2(0, 0);
+        const int2 mine = next;
+        if (base + 32 < q1) next = base + 32 + lane < q1 ? __ldg(pr + base + 32 + lane) : make_int2(0, 0);
         T l[S], r[S];
 #pragma unroll
         for (int u = 0; u < S; u++) {
@@ -569,7 +572,7 @@ __global__ void __launch_bounds__(32 * kPersistWarps) k_persistent(DevGrid g, De
         const int l = W == kWorkBackward ? l1 - 1 - step : l0 + step;
         for (int ph = 0; ph < phases; ph++) {
             const int i0 = ptr[phases * l + ph], i1 = ptr[phases * l + ph + 1];
-            for (int it = i0 + threadIdx.y; it < i1; it += kPersistWarps) doItem<T, W>(g, b, vec, it, s, act);
+            for (int it = i0 + threadIdx.y; it < i1; it += blockDim.y) doItem<T, W>(g, b, vec, it, s, act);
             __syncthreads();
         }
     }
@@ -723,10 +726,21 @@ __device__ __forceinline__ T dotWarp1(const T* __restrict__ lu, const T* __restr
                                       int64_t q0, int64_t q1, size_t B, int s) {
     constexpr int U = 4;
     T acc = T(0);
+    // the next round's index pairs are loaded while this round's operands are in flight
+    int2 an[U];
+    {
+        const int64_t q = q0 + (threadIdx.x & 31);
+#pragma unroll
+        for (int u = 0; u < U; u++) an[u] = q + 32 * u < q1 ? __ldg(pr + q + 32 * u) : make_int2(-1, -1);
+    }
     for (int64_t q = q0 + (threadIdx.x & 31); q < q1; q += 32 * U) {
         int2 a[U];
 #pragma unroll
-        for (int u = 0; u < U; u++) a[u] = q + 32 * u < q1 ? __ldg(pr + q + 32 * u) : make_int2(-1, -1);
+        for (int u = 0; u < U; u++) a[u] = an[u];
+        if (q + 32 * U < q1) {
+#pragma unroll
+            for (int u = 0; u < U; u++) an[u] = q + 32 * (U + u) < q1 ? __ldg(pr + q + 32 * (U + u)) : make_int2(-1, -1);
+        }
         T l[U], r[U];
 #pragma unroll
         for (int u = 0; u < U; u++) {
@@ -1744,6 +1758,19 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
     // one persistent launch per phase (narrow: a few tasks per level, latency-bound)
     const int split = G->split;
     const int persistThreads = 32;
+    // warps per persistent CTA: as many as let every system group's CTA be resident at once (one wave), at most
+    // kPersistWarps (a second partial wave would double the launch)
+    int persistWarps = kPersistWarps;
+    {
+        int sms = 0, occ = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+        for (int wpc = kPersistWarps; wpc >= 4; wpc--) {
+            persistWarps = wpc;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_persistent<T, kWorkFactor>, 32 * wpc, 0) == cudaSuccess &&
+                (int64_t)occ * sms >= w.B / Lay<T>::S)
+                break;
+        }
+    }
     const int luGroups = w.B / Lay<T>::S;  // warps of the LU kernels cover S systems each
     auto launchLevel = [&](auto kernel, T* vec, int i0, int i1) {
         if (i1 > i0) { kernel<<<dim3((i1 - i0 + 3) / 4, luGroups), blk4, 0, st>>>(g, b, vec, i0, i1); stepLaunches++; }
@@ -1757,13 +1784,13 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             launchLevel(k_level<T, kWorkFactor>, (T*)b.y, fp[2 * l + 1], fp[2 * l + 2]);
         }
         if (split < s.nLevels) {
-            k_persistent<T, kWorkFactor><<<luGroups, dim3(persistThreads, kPersistWarps), 0, st>>>(g, b, (T*)b.y, split, s.nLevels);
+            k_persistent<T, kWorkFactor><<<luGroups, dim3(persistThreads, persistWarps), 0, st>>>(g, b, (T*)b.y, split, s.nLevels);
             stepLaunches++;
         }
     };
     auto backward = [&](T* vec) {
         if (split < s.nLevels) {
-            k_persistent<T, kWorkBackward><<<luGroups, dim3(persistThreads, kPersistWarps), 0, st>>>(g, b, vec, split, s.nLevels);
+            k_persistent<T, kWorkBackward><<<luGroups, dim3(persistThreads, persistWarps), 0, st>>>(g, b, vec, split, s.nLevels);
             stepLaunches++;
         }
         for (int l = split - 1; l >= 0; l--) launchLevel(k_level<T, kWorkBackward>, vec, bp[l], bp[l + 1]);
@@ -1775,7 +1802,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             stepLaunches++;
             for (int l = 0; l < split; l++) launchLevel(k_level<T, kWorkForward>, (T*)b.z, vp[l], vp[l + 1]);
             if (split < s.nLevels) {
-                k_persistent<T, kWorkForward><<<luGroups, dim3(persistThreads, kPersistWarps), 0, st>>>(g, b, (T*)b.z, split, s.nLevels);
+                k_persistent<T, kWorkForward><<<luGroups, dim3(persistThreads, persistWarps), 0, st>>>(g, b, (T*)b.z, split, s.nLevels);
                 stepLaunches++;
             }
             backward((T*)b.z);
