@@ -544,7 +544,7 @@ __device__ __forceinline__ void doItem(const DevGrid& g, const DevBatch& b, T* v
 
 // One level (or phase) of a schedule, items [i0, i1): block (32, 4), a warp per item, S systems per warp.
 template <typename T, int W>
-__global__ void __launch_bounds__(128) k_level(DevGrid g, DevBatch b, T* vec, int i0, int i1) {
+__global__ void __launch_bounds__(128, 10) k_level(DevGrid g, DevBatch b, T* vec, int i0, int i1) {
     const int it = i0 + blockIdx.x * 4 + threadIdx.y;
     const int s = laneSystem<T>(blockIdx.y);
     if (it >= i1) return;
@@ -1485,6 +1485,7 @@ struct gs_ctx {
     std::string lastError;
     std::mutex mu;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;  // the second half of a batch's level sequences
     int* pinnedCount = nullptr;
     std::map<std::string, int> multiTune;  // the multi-grid batch's CTA shape per set of grids (autotuned)
 };
@@ -1720,6 +1721,26 @@ DevBatch MakeBatch(gs_grid* G, int count, bool useScale) {
     return MakeBatchWs(G->ws, G->sym.nLevels, G->ws.B, count, useScale);
 }
 
+// The systems [off, off + n) of batch b as a batch of their own (same interleave stride).
+template <typename T>
+DevBatch HalfView(const DevBatch& b, int off, int n) {
+    DevBatch h = b;
+    h.count = std::max(0, n);
+    auto sh = [&](auto* p) { return p ? p + off : p; };
+    h.vm = sh(b.vm); h.va = sh(b.va);
+    h.lu = b.lu ? (void*)((T*)b.lu + off) : nullptr;
+    h.piv = b.piv ? (void*)((T*)b.piv + off) : nullptr;
+    h.y = b.y ? (void*)((T*)b.y + off) : nullptr;
+    h.z = b.z ? (void*)((T*)b.z + off) : nullptr;
+    h.rhs64 = sh(b.rhs64); h.refine = sh(b.refine); h.maxMis = sh(b.maxMis); h.maxDx = sh(b.maxDx);
+    h.startMis = sh(b.startMis); h.finalMis = sh(b.finalMis); h.status = sh(b.status); h.iters = sh(b.iters);
+    h.convIters = sh(b.convIters); h.active = sh(b.active); h.flags = sh(b.flags); h.outage = sh(b.outage);
+    h.loadScale = sh(b.loadScale);
+    h.effType = sh(b.effType); h.qspecSys = sh(b.qspecSys); h.pinned = sh(b.pinned); h.reverted = sh(b.reverted);
+    h.qinj = sh(b.qinj); h.passIter = sh(b.passIter); h.qPass = sh(b.qPass); h.qState = sh(b.qState);
+    return h;
+}
+
 // Run the Newton iteration of `count` systems already placed in the workspace (outage, loadScale).
 // `startFromWs`: start every system from ws.startVm / startVa (a solved base), else from the grid start.
 struct NewtonStats {
@@ -1771,42 +1792,68 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
                 break;
         }
     }
-    const int luGroups = w.B / Lay<T>::S;  // warps of the LU kernels cover S systems each
-    auto launchLevel = [&](auto kernel, T* vec, int i0, int i1) {
-        if (i1 > i0) { kernel<<<dim3((i1 - i0 + 3) / 4, luGroups), blk4, 0, st>>>(g, b, vec, i0, i1); stepLaunches++; }
+    // The batch's level sequences run as two halves on two streams (parallel branches of the step's graph), so
+    // that one half's dependent-load latency and wave tails overlap the other's; small batches run as one.
+    const int halves = (w.B / Lay<T>::S >= 2 * 148 && count > w.B / 2) ? 2 : 1;
+    DevBatch hb[2] = {b, b};
+    if (halves == 2) {
+        const int bh = w.B / 2;
+        hb[0].count = bh;
+        hb[1] = HalfView<T>(b, bh, count - bh);
+    }
+    cudaStream_t st2 = ctx->stream2;
+    cudaEvent_t evFork, evJoin;
+    GS_CUDA(cudaEventCreateWithFlags(&evFork, cudaEventDisableTiming));
+    GS_CUDA(cudaEventCreateWithFlags(&evJoin, cudaEventDisableTiming));
+    auto launchLevel = [&](const DevBatch& bb, cudaStream_t ss, auto kernel, T* vec, int i0, int i1) {
+        const int grp = (bb.count + Lay<T>::S - 1) / Lay<T>::S;
+        if (i1 > i0 && grp > 0) { kernel<<<dim3((i1 - i0 + 3) / 4, grp), blk4, 0, ss>>>(g, bb, vec, i0, i1); stepLaunches++; }
     };
     const auto& fp = s.factor.levelItemPtr;
     const auto& bp = s.backward.levelItemPtr;
     const auto& vp = s.forward.levelItemPtr;
-    auto factorPhase = [&]() {
+    auto factorPhase = [&](const DevBatch& bb, cudaStream_t ss) {
         for (int l = 0; l < split; l++) {
-            launchLevel(k_level<T, kWorkFactor>, (T*)b.y, fp[2 * l], fp[2 * l + 1]);
-            launchLevel(k_level<T, kWorkFactor>, (T*)b.y, fp[2 * l + 1], fp[2 * l + 2]);
+            launchLevel(bb, ss, k_level<T, kWorkFactor>, (T*)bb.y, fp[2 * l], fp[2 * l + 1]);
+            launchLevel(bb, ss, k_level<T, kWorkFactor>, (T*)bb.y, fp[2 * l + 1], fp[2 * l + 2]);
         }
         if (split < s.nLevels) {
-            k_persistent<T, kWorkFactor><<<luGroups, dim3(persistThreads, persistWarps), 0, st>>>(g, b, (T*)b.y, split, s.nLevels);
+            k_persistent<T, kWorkFactor><<<(bb.count + Lay<T>::S - 1) / Lay<T>::S, dim3(persistThreads, persistWarps), 0, ss>>>(
+                g, bb, (T*)bb.y, split, s.nLevels);
             stepLaunches++;
         }
     };
-    auto backward = [&](T* vec) {
+    auto backward = [&](const DevBatch& bb, cudaStream_t ss, T* vec) {
         if (split < s.nLevels) {
-            k_persistent<T, kWorkBackward><<<luGroups, dim3(persistThreads, persistWarps), 0, st>>>(g, b, vec, split, s.nLevels);
+            k_persistent<T, kWorkBackward><<<(bb.count + Lay<T>::S - 1) / Lay<T>::S, dim3(persistThreads, persistWarps), 0, ss>>>(
+                g, bb, vec, split, s.nLevels);
             stepLaunches++;
         }
-        for (int l = split - 1; l >= 0; l--) launchLevel(k_level<T, kWorkBackward>, vec, bp[l], bp[l + 1]);
+        for (int l = split - 1; l >= 0; l--) launchLevel(bb, ss, k_level<T, kWorkBackward>, vec, bp[l], bp[l + 1]);
     };
-    auto solvePhase = [&](bool doRefine) {
-        backward((T*)b.y);
+    auto solvePhase = [&](const DevBatch& bb, cudaStream_t ss, bool doRefine) {
+        backward(bb, ss, (T*)bb.y);
         if (doRefine) {
-            k_residual<T><<<dim3((s.n + 7) / 8, groups), blk8, 0, st>>>(g, b, nullptr, 0);
+            k_residual<T><<<dim3((s.n + 7) / 8, (bb.count + 31) / 32), blk8, 0, ss>>>(g, bb, nullptr, 0);
             stepLaunches++;
-            for (int l = 0; l < split; l++) launchLevel(k_level<T, kWorkForward>, (T*)b.z, vp[l], vp[l + 1]);
+            for (int l = 0; l < split; l++) launchLevel(bb, ss, k_level<T, kWorkForward>, (T*)bb.z, vp[l], vp[l + 1]);
             if (split < s.nLevels) {
-                k_persistent<T, kWorkForward><<<luGroups, dim3(persistThreads, persistWarps), 0, st>>>(g, b, (T*)b.z, split, s.nLevels);
+                k_persistent<T, kWorkForward><<<(bb.count + Lay<T>::S - 1) / Lay<T>::S, dim3(persistThreads, persistWarps), 0, ss>>>(
+                    g, bb, (T*)bb.z, split, s.nLevels);
                 stepLaunches++;
             }
-            backward((T*)b.z);
+            backward(bb, ss, (T*)bb.z);
         }
+    };
+    // a phase over both halves: the second half on st2, forked from and joined back into st
+    auto bothHalves = [&](auto&& phase) {
+        if (halves == 1) { phase(hb[0], st); return; }
+        cudaEventRecord(evFork, st);
+        cudaStreamWaitEvent(st2, evFork, 0);
+        phase(hb[1], st2);
+        phase(hb[0], st);
+        cudaEventRecord(evJoin, st2);
+        cudaStreamWaitEvent(st, evJoin, 0);
     };
     const int rowsPerBlock = 512;
     auto updatePhase = [&](bool doRefine) {
@@ -1824,8 +1871,10 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             cudaGraph_t graph;
             stepLaunches = 0;
             GS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            factorPhase();
-            solvePhase(r != 0);
+            bothHalves([&](const DevBatch& bb, cudaStream_t ss) {
+                factorPhase(bb, ss);
+                solvePhase(bb, ss, r != 0);
+            });
             updatePhase(r != 0);
             ce = cudaStreamEndCapture(st, &graph);
             if (ce == cudaSuccess) {
@@ -1834,6 +1883,8 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             }
             if (ce != cudaSuccess) {
                 for (auto& x : exec) if (x) cudaGraphExecDestroy(x);
+                cudaEventDestroy(evFork);
+                cudaEventDestroy(evJoin);
                 return SetErr(ctx, GS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
             }
             launchesPerStep[r] = stepLaunches;
@@ -1939,9 +1990,9 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
         } else {
             stepLaunches = 0;
             cudaEventRecord(ev[1], st);
-            factorPhase();
+            bothHalves([&](const DevBatch& bb, cudaStream_t ss) { factorPhase(bb, ss); });
             cudaEventRecord(ev[2], st);
-            solvePhase(anyRefine != 0);
+            bothHalves([&](const DevBatch& bb, cudaStream_t ss) { solvePhase(bb, ss, anyRefine != 0); });
             cudaEventRecord(ev[3], st);
             updatePhase(anyRefine != 0);
             cudaEventRecord(ev[4], st);
@@ -1975,6 +2026,8 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
         stats->tailMs += tMs;
     }
     for (auto& x : exec) if (x) cudaGraphExecDestroy(x);
+    cudaEventDestroy(evFork);
+    cudaEventDestroy(evJoin);
     cudaEventRecord(e1, st);
     cudaEventSynchronize(e1);
     if (ms) cudaEventElapsedTime(ms, e0, e1);
@@ -2104,7 +2157,8 @@ int gs_ctx_create(int device, const gs_ctx_opts* opts, gs_ctx** out) {
     gs_ctx* c = new gs_ctx();
     c->device = device;
     c->stream = probe->stream;
-    if (cudaSetDevice(device) != cudaSuccess || gs::SetKernelAttributes() != cudaSuccess) { delete c; return GS_ERR_CUDA; }
+    if (cudaSetDevice(device) != cudaSuccess || gs::SetKernelAttributes() != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess) { delete c; return GS_ERR_CUDA; }
     if (cudaMallocHost(&c->pinnedCount, 4 * sizeof(int)) != cudaSuccess) { delete c; return GS_ERR_CUDA; }
     *out = c;
     return GS_OK;
@@ -2115,6 +2169,7 @@ int gs_ctx_destroy(gs_ctx* c) {
     cudaSetDevice(c->device);
     if (c->pinnedCount) cudaFreeHost(c->pinnedCount);
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->stream2) cudaStreamDestroy(c->stream2);
     delete c;
     return GS_OK;
 }
