@@ -1485,7 +1485,7 @@ struct gs_ctx {
     std::string lastError;
     std::mutex mu;
     cudaStream_t stream = nullptr;
-    cudaStream_t stream2 = nullptr;  // the second half of a batch's level sequences
+    cudaStream_t partStream[2] = {nullptr, nullptr};  // part 1 of a batch's level sequences (part 0 runs on `stream`)
     int* pinnedCount = nullptr;
     std::map<std::string, int> multiTune;  // the multi-grid batch's CTA shape per set of grids (autotuned)
 };
@@ -1686,7 +1686,10 @@ int EnsureWs(gs_ctx* ctx, const Symbolic& s, Workspace& w, int B, int precision,
 int EnsureWorkspace(gs_grid* G, int B, int precision, bool classify, bool loadScale) {
     // the compact workspace of the few-systems path (its interleave stride is set per compaction)
     const int cap = std::min(B, kCompactCap);
-    int rc = EnsureWs(G->ctx, G->sym, G->tws, cap, precision, false, loadScale);
+    // FP64 whatever the batch's precision: the few-systems path is latency-bound, so FP32 factors save nothing there
+    // and would need the refinement solve
+    (void)precision;
+    int rc = EnsureWs(G->ctx, G->sym, G->tws, cap, GS_PREC_FP64, false, loadScale);
     if (rc != GS_OK) return rc;
     return EnsureWs(G->ctx, G->sym, G->ws, B, precision, classify, loadScale);
 }
@@ -1720,6 +1723,9 @@ DevBatch MakeBatchWs(const Workspace& w, int nLevels, int B, int count, bool use
 DevBatch MakeBatch(gs_grid* G, int count, bool useScale) {
     return MakeBatchWs(G->ws, G->sym.nLevels, G->ws.B, count, useScale);
 }
+
+// Parts of a full batch whose level sequences run side by side (parallel branches of the step graph).
+constexpr int kParts = 2;  // measured on the 10,000-bus screen: 2 parts beat 1, 3 and 4 in mixed precision
 
 // The systems [off, off + n) of batch b as a batch of their own (same interleave stride).
 template <typename T>
@@ -1794,17 +1800,24 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
     }
     // The batch's level sequences run as two halves on two streams (parallel branches of the step's graph), so
     // that one half's dependent-load latency and wave tails overlap the other's; small batches run as one.
-    const int halves = (w.B / Lay<T>::S >= 2 * 148 && count > w.B / 2) ? 2 : 1;
-    DevBatch hb[2] = {b, b};
-    if (halves == 2) {
-        const int bh = w.B / 2;
-        hb[0].count = bh;
-        hb[1] = HalfView<T>(b, bh, count - bh);
+    // parts: as many as keep each part at 148 or more system groups and at least one system, at most kParts
+    int parts = 1;
+    {
+        const int groupsAll = w.B / Lay<T>::S;
+        while (parts < kParts && groupsAll / (parts + 1) >= 148 && count > (w.B / (parts + 1)) * parts) parts++;
     }
-    cudaStream_t st2 = ctx->stream2;
-    cudaEvent_t evFork, evJoin;
+    DevBatch hb[kParts];
+    {
+        const int per = (w.B / parts) / 32 * 32;
+        for (int q = 0; q < parts; q++) {
+            const int off = q * per, n = q == parts - 1 ? count - off : std::min(per, count - off);
+            hb[q] = q == 0 ? b : HalfView<T>(b, off, n);
+            if (q == 0) hb[0].count = std::min(count, parts == 1 ? count : per);
+        }
+    }
+    cudaEvent_t evFork, evJoin[kParts];
     GS_CUDA(cudaEventCreateWithFlags(&evFork, cudaEventDisableTiming));
-    GS_CUDA(cudaEventCreateWithFlags(&evJoin, cudaEventDisableTiming));
+    for (auto& e : evJoin) GS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     auto launchLevel = [&](const DevBatch& bb, cudaStream_t ss, auto kernel, T* vec, int i0, int i1) {
         const int grp = (bb.count + Lay<T>::S - 1) / Lay<T>::S;
         if (i1 > i0 && grp > 0) { kernel<<<dim3((i1 - i0 + 3) / 4, grp), blk4, 0, ss>>>(g, bb, vec, i0, i1); stepLaunches++; }
@@ -1845,15 +1858,19 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             backward(bb, ss, (T*)bb.z);
         }
     };
-    // a phase over both halves: the second half on st2, forked from and joined back into st
+    // a phase over every part: parts 1.. on their own streams, forked from and joined back into st
     auto bothHalves = [&](auto&& phase) {
-        if (halves == 1) { phase(hb[0], st); return; }
+        if (parts == 1) { phase(hb[0], st); return; }
         cudaEventRecord(evFork, st);
-        cudaStreamWaitEvent(st2, evFork, 0);
-        phase(hb[1], st2);
+        for (int q = 1; q < parts; q++) {
+            cudaStreamWaitEvent(ctx->partStream[q], evFork, 0);
+            phase(hb[q], ctx->partStream[q]);
+        }
         phase(hb[0], st);
-        cudaEventRecord(evJoin, st2);
-        cudaStreamWaitEvent(st, evJoin, 0);
+        for (int q = 1; q < parts; q++) {
+            cudaEventRecord(evJoin[q], ctx->partStream[q]);
+            cudaStreamWaitEvent(st, evJoin[q], 0);
+        }
     };
     const int rowsPerBlock = 512;
     auto updatePhase = [&](bool doRefine) {
@@ -1884,7 +1901,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             if (ce != cudaSuccess) {
                 for (auto& x : exec) if (x) cudaGraphExecDestroy(x);
                 cudaEventDestroy(evFork);
-                cudaEventDestroy(evJoin);
+                for (auto& e : evJoin) cudaEventDestroy(e);
                 return SetErr(ctx, GS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
             }
             launchesPerStep[r] = stepLaunches;
@@ -1908,7 +1925,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
     for (int iter = 0; iter <= maxLoop; iter++) {
         if (timed) cudaEventRecord(ev[0], st);
         if (listCount > 0)
-            k_mismatch_jac<T><<<dim3(nodeBlocks.x, (listCount + 31) / 32), blk8, 0, st>>>(g, cur, 1, nullptr, nullptr,
+            k_mismatch_jac<double><<<dim3(nodeBlocks.x, (listCount + 31) / 32), blk8, 0, st>>>(g, cur, 1, nullptr, nullptr,
                                                                                        cur.activeList, listCount);
         else
             k_mismatch_jac<T><<<dim3(nodeBlocks.x, cur.B / 32), blk8, 0, st>>>(g, cur, 1, nullptr, nullptr, nullptr, 0);
@@ -1949,22 +1966,22 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
                 k_gather<<<dim3(nodeBlocks.x, stride / 32), blk8, 0, st>>>(b, cur, G->tws.origin.as<int>(), s.n);
                 // this iteration's Jacobian and right-hand side, rebuilt in the compact workspace; the mismatch
                 // maximum it records was already taken by k_status
-                k_mismatch_jac<T><<<dim3(nodeBlocks.x, stride / 32), blk8, 0, st>>>(g, cur, 1, nullptr, nullptr, nullptr, 0);
+                k_mismatch_jac<double><<<dim3(nodeBlocks.x, stride / 32), blk8, 0, st>>>(g, cur, 1, nullptr, nullptr, nullptr, 0);
                 cudaMemsetAsync(cur.maxMis, 0, (size_t)nActive * sizeof(unsigned long long), st);
                 launches += 3;
                 compacted = true;
             }
             // few systems left: the wide bottom levels as per-level launches over the compact batch, the rest as
-            // one CTA per active system (k_tail)
+            // one CTA per active system (k_tail), in FP64 (the compact workspace's precision)
             cudaMemsetAsync(cur.activeCount, 0, sizeof(int), st);
             k_collect_active<<<(cur.count + 255) / 256, 256, 0, st>>>(cur);
-            launches += 1 + FewSystemsSolve<T>(g, cur, s, nActive, G->tailSplit, anyRefine != 0, st, timed ? ev[2] : nullptr);
+            launches += 1 + FewSystemsSolve<double>(g, cur, s, nActive, G->tailSplit, false, st, timed ? ev[2] : nullptr);
             if (timed) cudaEventRecord(ev[3], st);
             {
                 const int grp = (nActive + 31) / 32;
-                k_dxmax<T><<<dim3((s.m + rowsPerBlock - 1) / rowsPerBlock, grp), blk8, 0, st>>>(g, cur, rowsPerBlock, refine,
+                k_dxmax<double><<<dim3((s.m + rowsPerBlock - 1) / rowsPerBlock, grp), blk8, 0, st>>>(g, cur, rowsPerBlock, 0,
                                                                                                cur.activeList, nActive);
-                k_update<T><<<dim3(nodeBlocks.x, grp), blk8, 0, st>>>(g, cur, refine, cur.activeList, nActive);
+                k_update<double><<<dim3(nodeBlocks.x, grp), blk8, 0, st>>>(g, cur, 0, cur.activeList, nActive);
                 launches += 2;
             }
             listCount = nActive;
@@ -2027,7 +2044,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
     }
     for (auto& x : exec) if (x) cudaGraphExecDestroy(x);
     cudaEventDestroy(evFork);
-    cudaEventDestroy(evJoin);
+    for (auto& e : evJoin) cudaEventDestroy(e);
     cudaEventRecord(e1, st);
     cudaEventSynchronize(e1);
     if (ms) cudaEventElapsedTime(ms, e0, e1);
@@ -2158,7 +2175,7 @@ int gs_ctx_create(int device, const gs_ctx_opts* opts, gs_ctx** out) {
     c->device = device;
     c->stream = probe->stream;
     if (cudaSetDevice(device) != cudaSuccess || gs::SetKernelAttributes() != cudaSuccess ||
-        cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess) { delete c; return GS_ERR_CUDA; }
+        cudaStreamCreateWithFlags(&c->partStream[1], cudaStreamNonBlocking) != cudaSuccess) { delete c; return GS_ERR_CUDA; }
     if (cudaMallocHost(&c->pinnedCount, 4 * sizeof(int)) != cudaSuccess) { delete c; return GS_ERR_CUDA; }
     *out = c;
     return GS_OK;
@@ -2169,7 +2186,7 @@ int gs_ctx_destroy(gs_ctx* c) {
     cudaSetDevice(c->device);
     if (c->pinnedCount) cudaFreeHost(c->pinnedCount);
     if (c->stream) cudaStreamDestroy(c->stream);
-    if (c->stream2) cudaStreamDestroy(c->stream2);
+    for (auto& ps : c->partStream) if (ps) cudaStreamDestroy(ps);
     delete c;
     return GS_OK;
 }
