@@ -218,6 +218,7 @@ __device__ __forceinline__ bool statusStep(const DevBatch& b, int s, int iter, d
         b.refine[s] = r;
         if (r) atomicAdd(b.activeCount + 1, 1);
     }
+    if (b.beforeLast) b.beforeLast[s] = mis;
     atomicAdd(b.activeCount, 1);
     return true;
 }
@@ -255,7 +256,12 @@ __global__ void k_status_q(DevBatch b, double tol, double divLimit, int maxIter)
     b.finalMis[s] = mis;
     if (iter == 0) b.startMis[s] = mis;
     if (mis < tol) {
-        if (b.qState[s] & kQFinalPass) { b.status[s] = GS_PF_MAX_ITERATIONS; b.active[s] = 0; return; }
+        if (b.qState[s] & kQFinalPass) {  // the last run converged, but the pass cap ends the solve unconverged
+            b.status[s] = GS_PF_MAX_ITERATIONS;
+            b.qState[s] |= kQFinalConverged;
+            b.active[s] = 0;
+            return;
+        }
         b.qState[s] |= kQPending;  // the Q limits decide (k_qapply, k_qrevert, k_qfinish)
         return;
     }
@@ -267,6 +273,7 @@ __global__ void k_status_q(DevBatch b, double tol, double divLimit, int maxIter)
         b.refine[s] = r;
         if (r) atomicAdd(b.activeCount + 1, 1);
     }
+    if (b.beforeLast) b.beforeLast[s] = mis;
     atomicAdd(b.activeCount, 1);
 }
 
@@ -697,6 +704,7 @@ __device__ __forceinline__ void moveSystem(const DevBatch& from, int sf, const D
     to.maxMis[st] = from.maxMis[sf];
     to.maxDx[st] = from.maxDx[sf];
     to.startMis[st] = from.startMis[sf];
+    if (from.beforeLast && to.beforeLast) to.beforeLast[st] = from.beforeLast[sf];
     to.finalMis[st] = from.finalMis[sf];
     to.status[st] = from.status[sf];
     to.iters[st] = from.iters[sf];
@@ -711,6 +719,14 @@ __global__ void k_gather(DevBatch full, DevBatch compact, const int* origin, int
     const int c = blockIdx.y * 32 + threadIdx.x, i = blockIdx.x * 8 + threadIdx.y;
     if (c >= compact.count || i >= n) return;
     moveSystem(full, origin[c], compact, c, i, n);
+}
+
+// pairs[c] = (position in `from`, position in `to`): grid (ceil(n / 8), ceil(nPairs / 32)), block (32, 8).
+__global__ void k_move_listed(DevBatch from, DevBatch to, const int2* pairs, int nPairs, int n) {
+    const int c = blockIdx.y * 32 + threadIdx.x, i = blockIdx.x * 8 + threadIdx.y;
+    if (c >= nPairs || i >= n) return;
+    const int2 p = pairs[c];
+    moveSystem(from, p.x, to, p.y, i, n);
 }
 
 __global__ void k_scatter(DevBatch compact, DevBatch full, const int* origin, int n) {
@@ -1285,14 +1301,16 @@ __global__ void __launch_bounds__(256) k_update(DevGrid g, DevBatch b, int refin
 
 // ---------------------------------------------------------------------------------------------
 // start state: every system from the shared start (vm0/va0) or from a base state of one system.
-__global__ void k_init(DevGrid g, DevBatch b, const double* vmStart, const double* vaStart) {
+// vmSys / vaSys ([n][B], may be null): a start state per system (the DC retry), else vmStart / vaStart for all.
+__global__ void k_init(DevGrid g, DevBatch b, const double* vmStart, const double* vaStart, const double* vmSys,
+                       const double* vaSys) {
     const int lane = threadIdx.x;
     const int s = blockIdx.y * 32 + lane;
     const int i = blockIdx.x * 8 + threadIdx.y;
     if (i >= g.n || s >= b.B) return;
     const size_t B = (size_t)b.B;
-    double vm = vmStart ? vmStart[i] : g.vm0[i];
-    double va = vaStart ? vaStart[i] : g.va0[i];
+    double vm = vmSys ? vmSys[i * B + s] : (vmStart ? vmStart[i] : g.vm0[i]);
+    double va = vaSys ? vaSys[i * B + s] : (vaStart ? vaStart[i] : g.va0[i]);
     // PV and slack magnitudes are set points whatever the start (NewtonShell.BuildBusSpec :467-469)
     if (g.busType[i] != 1) vm = g.vm0[i];
     if (g.busType[i] == 3) va = g.va0[i];
@@ -1309,6 +1327,7 @@ __global__ void k_init(DevGrid g, DevBatch b, const double* vmStart, const doubl
         b.maxMis[s] = 0ull;
         b.maxDx[s] = 0ull;
         b.startMis[s] = 0.0;
+        if (b.beforeLast) b.beforeLast[s] = NAN;
         b.finalMis[s] = NAN;
         b.status[s] = s < b.count ? GS_PF_MAX_ITERATIONS : GS_PF_NOT_RUN;
         b.iters[s] = 0;
@@ -1472,6 +1491,7 @@ struct Workspace {
     int precision = -1;
     DevBuf activeList, origin;  // origin: a compact batch position -> the system of the full batch
     DevBuf effType, qspecSys, pinned, reverted, qinj, passIter, qPass, qState;  // Q-limit enforcement
+    DevBuf beforeLast;
     DevBuf vm, va, lu, piv, y, z, rhs64, refine, maxMis, maxDx, startMis, finalMis, status, iters, convIters, active, flags, outage,
         loadScale, activeCount;
     DevBuf code, value, maxLoad, minVmNeg, maxVmB, chunkCount, chunkOffset, outKind, outElem, outVal, pq;
@@ -1500,6 +1520,7 @@ struct gs_grid {
     gs::Workspace ws;
     gs::Workspace tws;  // compact copy of the few systems still stepping
     std::unique_ptr<gs_grid> qgrid;  // the same grid analysed for Q-limit enforcement (built on first use)
+    std::unique_ptr<gs_grid> rgrid;  // a twin with its own workspace for the DC-angle retries (built on first use)
     int split = 0;      // first level run by the persistent kernels
     int tailSplit = 0;  // first level the few-systems path runs as one CTA per system
 };
@@ -1664,7 +1685,7 @@ int EnsureWs(gs_ctx* ctx, const Symbolic& s, Workspace& w, int B, int precision,
         GS_CUDA(w.refine.alloc(Bz * 4));
     }
     GS_CUDA(w.maxMis.alloc(Bz * 8)); GS_CUDA(w.maxDx.alloc(Bz * 8));
-    GS_CUDA(w.startMis.alloc(Bz * 8)); GS_CUDA(w.finalMis.alloc(Bz * 8));
+    GS_CUDA(w.startMis.alloc(Bz * 8)); GS_CUDA(w.finalMis.alloc(Bz * 8)); GS_CUDA(w.beforeLast.alloc(Bz * 8));
     GS_CUDA(w.status.alloc(Bz * 4)); GS_CUDA(w.iters.alloc(Bz * 4)); GS_CUDA(w.active.alloc(Bz * 4));
     GS_CUDA(w.convIters.alloc(Bz * 4));
     GS_CUDA(w.flags.alloc(Bz * 4)); GS_CUDA(w.outage.alloc(Bz * 4)); GS_CUDA(w.activeCount.alloc(16));
@@ -1704,7 +1725,7 @@ DevBatch MakeBatchWs(const Workspace& w, int nLevels, int B, int count, bool use
     b.rhs64 = mixed ? w.rhs64.as<double>() : nullptr;
     b.refine = mixed ? w.refine.as<int>() : nullptr;
     b.maxMis = w.maxMis.as<unsigned long long>(); b.maxDx = w.maxDx.as<unsigned long long>();
-    b.startMis = w.startMis.as<double>(); b.finalMis = w.finalMis.as<double>();
+    b.startMis = w.startMis.as<double>(); b.finalMis = w.finalMis.as<double>(); b.beforeLast = w.beforeLast.as<double>();
     b.status = w.status.as<int>(); b.iters = w.iters.as<int>(); b.active = w.active.as<int>();
     b.convIters = w.convIters.as<int>();
     b.flags = w.flags.as<int>(); b.outage = w.outage.as<int>();
@@ -1740,6 +1761,7 @@ DevBatch HalfView(const DevBatch& b, int off, int n) {
     h.z = b.z ? (void*)((T*)b.z + off) : nullptr;
     h.rhs64 = sh(b.rhs64); h.refine = sh(b.refine); h.maxMis = sh(b.maxMis); h.maxDx = sh(b.maxDx);
     h.startMis = sh(b.startMis); h.finalMis = sh(b.finalMis); h.status = sh(b.status); h.iters = sh(b.iters);
+    h.beforeLast = sh(b.beforeLast);
     h.convIters = sh(b.convIters); h.active = sh(b.active); h.flags = sh(b.flags); h.outage = sh(b.outage);
     h.loadScale = sh(b.loadScale);
     h.effType = sh(b.effType); h.qspecSys = sh(b.qspecSys); h.pinned = sh(b.pinned); h.reverted = sh(b.reverted);
@@ -1759,7 +1781,7 @@ struct NewtonStats {
 
 template <typename T>
 int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_opts& o, float* ms,
-           NewtonStats* stats = nullptr) {
+           NewtonStats* stats = nullptr, const double* vmSys = nullptr, const double* vaSys = nullptr) {
     gs_ctx* ctx = G->ctx;
     const Symbolic& s = G->sym;
     Workspace& w = G->ws;
@@ -1773,7 +1795,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
     GS_CUDA(cudaEventRecord(e0, st));
     dim3 blk8(32, 8), blk4(32, 4);
     k_init<<<dim3((s.n + 7) / 8, groups), blk8, 0, st>>>(g, b, startFromWs ? w.startVm.as<double>() : nullptr,
-                                                          startFromWs ? w.startVa.as<double>() : nullptr);
+                                                          startFromWs ? w.startVa.as<double>() : nullptr, vmSys, vaSys);
     GS_CUDA(cudaGetLastError());
     // the step (factor levels, backward levels, refinement, max |dx|, update) as one graph
     const int refine = sizeof(T) < sizeof(double) ? 1 : 0;
@@ -2054,15 +2076,165 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
 }
 
 int NewtonDispatch(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_opts& o, float* ms,
-                   NewtonStats* stats = nullptr) {
-    if (o.precision == GS_PREC_MIXED) return Newton<float>(G, count, useScale, startFromWs, o, ms, stats);
-    return Newton<double>(G, count, useScale, startFromWs, o, ms, stats);
+                   NewtonStats* stats = nullptr, const double* vmSys = nullptr, const double* vaSys = nullptr) {
+    if (o.precision == GS_PREC_MIXED) return Newton<float>(G, count, useScale, startFromWs, o, ms, stats, vmSys, vaSys);
+    return Newton<double>(G, count, useScale, startFromWs, o, ms, stats, vmSys, vaSys);
+}
+
+// ---- the DC-angle retry (NewtonShell.SolveWithRetry, NewtonShell.cs:227-268) ----
+constexpr double kRetryStallFactor = 1e-3;        // NewtonShell.cs:146
+constexpr double kRetryLastStepFactor = 0.5;      // NewtonShell.cs:167
+constexpr double kMaxRetryBranchAngleDeg = 90.0;  // NewtonShell.cs:142
+
+int UploadGrid(gs_grid* G);
+
+int RetryGridOf(gs_grid* G, gs_grid** out) {
+    if (!G->rgrid) {
+        auto R = std::make_unique<gs_grid>();
+        R->ctx = G->ctx;
+        R->host = G->host;
+        std::string err = Analyze(R->host, R->sym, G->sym.qlim);
+        if (!err.empty()) return SetErr(G->ctx, GS_ERR_INVALID_ARG, err);
+        int rc = UploadGrid(R.get());
+        if (rc) return rc;
+        G->rgrid = std::move(R);
+    }
+    *out = G->rgrid.get();
+    return GS_OK;
+}
+
+// The largest angle across an in-service branch (the outaged one excluded), net of its phase shift, in [-180, 180]
+// degrees (NewtonShell.MaxBranchAngleDeg).
+double MaxBranchAngleDeg(const HostGrid& h, int skip, const double* vaRad, size_t stride) {
+    double mx = 0.0;
+    for (int k = 0; k < h.nbr; k++) {
+        if (!h.brOn[k] || k == skip) continue;
+        const double a = (vaRad[h.brF[k] * stride] - vaRad[h.brT[k] * stride]) * 180.0 / 3.14159265358979323846 - h.shift[k];
+        mx = std::max(mx, std::fabs(std::remainder(a, 360.0)));
+    }
+    return mx;
+}
+
+// After the Newton run of `count` systems in G's workspace (system s with outage[s], load scaling loadScale[s * n]
+// when given, started warm from ws.startVm/startVa when `warm`): systems whose last Newton run failed to converge and
+// stalled (NewtonShell.Stalled, :162 and :200-206) are solved again from DC power-flow angles (the magnitudes of the
+// ordinary start), in a twin grid's workspace; a retry that converges with every branch angle within 90 degrees
+// replaces the system's result (state, status, iterations, mismatch), any other keeps the first result.
+int RetryStalled(gs_grid* G, int count, const int* outage, const double* loadScale, bool warm, const gs_pf_opts& o,
+                 float* msOut, NewtonStats* stats) {
+    if (!o.retry_from_dc_start || o.max_iterations <= 1 || count <= 0) return GS_OK;
+    gs_ctx* ctx = G->ctx;
+    const Symbolic& s = G->sym;
+    const HostGrid& h = G->host;
+    Workspace& w = G->ws;
+    const bool qlim = s.qlim;
+    std::vector<int> st(count), it(count), pass(qlim ? count : 0), qs(qlim ? count : 0);
+    std::vector<double> fin(count), start(count), before(count);
+    GS_CUDA(cudaMemcpy(st.data(), w.status.p, count * 4, cudaMemcpyDeviceToHost));
+    GS_CUDA(cudaMemcpy(it.data(), w.iters.p, count * 4, cudaMemcpyDeviceToHost));
+    GS_CUDA(cudaMemcpy(fin.data(), w.finalMis.p, count * 8, cudaMemcpyDeviceToHost));
+    GS_CUDA(cudaMemcpy(start.data(), w.startMis.p, count * 8, cudaMemcpyDeviceToHost));
+    GS_CUDA(cudaMemcpy(before.data(), w.beforeLast.p, count * 8, cudaMemcpyDeviceToHost));
+    if (qlim) {
+        GS_CUDA(cudaMemcpy(pass.data(), w.passIter.p, count * 4, cudaMemcpyDeviceToHost));
+        GS_CUDA(cudaMemcpy(qs.data(), w.qState.p, count * 4, cudaMemcpyDeviceToHost));
+    }
+    int slack = -1, slacks = 0;
+    for (int i = 0; i < s.n; i++) if (s.type0[i] == 3) { slack = i; slacks++; }
+    if (slacks != 1) return GS_OK;  // TrySeedDcAngles needs exactly one slack
+    std::vector<int> cand;
+    for (int k = 0; k < count; k++) {
+        if (st[k] == GS_PF_CONVERGED) continue;
+        if (qlim && (qs[k] & kQFinalConverged)) continue;  // the last run converged: the pass cap, not Newton, failed
+        const int steps = qlim ? pass[k] : it[k];
+        const bool diverged = st[k] == GS_PF_DIVERGED;
+        const bool capReached = !diverged && st[k] != GS_PF_NON_FINITE && steps >= o.max_iterations;
+        if (capReached && steps == 0) continue;
+        if (fin[k] <= kRetryStallFactor * start[k]) continue;  // still converging (a NaN counts as stalled)
+        if (capReached && steps >= 2 && fin[k] <= kRetryLastStepFactor * before[k]) continue;
+        cand.push_back(k);
+    }
+    if (cand.empty()) return GS_OK;
+    const int n = s.n;
+    // ordinary start magnitudes, DC angles
+    std::vector<double> vmBase(n), vaBase(n);
+    if (warm) {
+        GS_CUDA(cudaMemcpy(vmBase.data(), w.startVm.p, n * 8, cudaMemcpyDeviceToHost));
+        GS_CUDA(cudaMemcpy(vaBase.data(), w.startVa.p, n * 8, cudaMemcpyDeviceToHost));
+    } else {
+        vmBase = s.vm0;
+        vaBase = s.va0;
+    }
+    std::vector<int> ok, okOut;
+    std::vector<std::vector<double>> seeds;
+    for (int k : cand) {
+        std::vector<double> th;
+        const double* sc = loadScale ? loadScale + (size_t)k * n : nullptr;
+        if (!DcAngles(h, s, outage ? outage[k] : -1, slack, sc, th)) continue;
+        std::vector<double> va(n);
+        for (int i = 0; i < n; i++)
+            va[i] = i == slack ? vaBase[slack] : vaBase[slack] + std::remainder(th[i], 360.0) * 3.14159265358979323846 / 180.0;
+        seeds.push_back(std::move(va));
+        ok.push_back(k);
+        okOut.push_back(outage ? outage[k] : -1);
+    }
+    if (ok.empty()) return GS_OK;
+    gs_grid* R = nullptr;
+    int rc = RetryGridOf(G, &R);
+    if (rc) return rc;
+    const int nc = (int)ok.size();
+    const int B = std::max(32, (nc + 31) / 32 * 32);
+    rc = EnsureWorkspace(R, B, o.precision, false, loadScale != nullptr);
+    if (rc) return rc;
+    Workspace& rw = R->ws;
+    std::vector<int> outs(B, -1);
+    for (int c = 0; c < nc; c++) outs[c] = okOut[c];
+    GS_CUDA(cudaMemcpy(rw.outage.p, outs.data(), B * 4, cudaMemcpyHostToDevice));
+    if (loadScale) {
+        std::vector<double> scl((size_t)n * B, 1.0);
+        for (int c = 0; c < nc; c++)
+            for (int i = 0; i < n; i++) scl[(size_t)i * B + c] = loadScale[(size_t)ok[c] * n + i];
+        GS_CUDA(cudaMemcpy(rw.loadScale.p, scl.data(), scl.size() * 8, cudaMemcpyHostToDevice));
+    }
+    std::vector<double> vmS((size_t)n * B, 1.0), vaS((size_t)n * B, 0.0);
+    for (int c = 0; c < nc; c++)
+        for (int i = 0; i < n; i++) {
+            vmS[(size_t)i * B + c] = vmBase[i];
+            vaS[(size_t)i * B + c] = seeds[c][i];
+        }
+    DevBuf dvm, dva;
+    GS_CUDA(dvm.alloc(vmS.size() * 8));
+    GS_CUDA(dva.alloc(vaS.size() * 8));
+    GS_CUDA(cudaMemcpy(dvm.p, vmS.data(), vmS.size() * 8, cudaMemcpyHostToDevice));
+    GS_CUDA(cudaMemcpy(dva.p, vaS.data(), vaS.size() * 8, cudaMemcpyHostToDevice));
+    float ms = 0;
+    rc = NewtonDispatch(R, nc, loadScale != nullptr, false, o, &ms, stats, dvm.as<double>(), dva.as<double>());
+    if (rc) return rc;
+    if (msOut) *msOut += ms;
+    // keep the retries that converged within the branch-angle bound
+    std::vector<int> rst(nc);
+    std::vector<double> rva((size_t)n * B);
+    GS_CUDA(cudaMemcpy(rst.data(), rw.status.p, nc * 4, cudaMemcpyDeviceToHost));
+    GS_CUDA(cudaMemcpy(rva.data(), rw.va.p, rva.size() * 8, cudaMemcpyDeviceToHost));
+    std::vector<int2> pairs;
+    for (int c = 0; c < nc; c++)
+        if (rst[c] == GS_PF_CONVERGED && MaxBranchAngleDeg(h, okOut[c], rva.data() + c, (size_t)B) <= kMaxRetryBranchAngleDeg)
+            pairs.push_back(make_int2(c, ok[c]));
+    if (pairs.empty()) return GS_OK;
+    DevBuf dp;
+    GS_CUDA(dp.alloc(pairs.size() * sizeof(int2)));
+    GS_CUDA(cudaMemcpy(dp.p, pairs.data(), pairs.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    const DevBatch from = MakeBatchWs(rw, R->sym.nLevels, rw.B, nc, loadScale != nullptr);
+    const DevBatch to = MakeBatch(G, count, loadScale != nullptr);
+    k_move_listed<<<dim3((n + 7) / 8, ((int)pairs.size() + 31) / 32), dim3(32, 8), 0, ctx->stream>>>(
+        from, to, dp.as<int2>(), (int)pairs.size(), n);
+    GS_CUDA(cudaGetLastError());
+    GS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return GS_OK;
 }
 
 int CheckOpts(gs_ctx* ctx, const gs_pf_opts* o) {
     if (!o) return SetErr(ctx, GS_ERR_INVALID_ARG, "null options");
-    if (o->retry_from_dc_start)
-        return SetErr(ctx, GS_ERR_UNSUPPORTED, "retry_from_dc_start: the DC-angle retry is not built yet");
     if (!(o->tolerance > 0) || o->tolerance > 1e-2) return SetErr(ctx, GS_ERR_INVALID_ARG, "tolerance must be in (0, 1e-2]");
     if (o->max_iterations < 0) return SetErr(ctx, GS_ERR_INVALID_ARG, "max_iterations must be 0 or more");
     if (!(o->diverge_limit_pu > 0)) return SetErr(ctx, GS_ERR_INVALID_ARG, "diverge_limit_pu must be above 0");
@@ -2109,6 +2281,9 @@ int SolveBase(gs_grid* G, const gs_pf_opts& o, int* status, int* iters, double* 
     std::vector<int> outage(G->ws.B, -1);
     GS_CUDA(cudaMemcpy(G->ws.outage.p, outage.data(), outage.size() * 4, cudaMemcpyHostToDevice));
     rc = NewtonDispatch(G, 1, false, false, o, ms);
+    if (rc) return rc;
+    const int none = -1;
+    rc = RetryStalled(G, 1, &none, nullptr, false, o, ms, nullptr);
     if (rc) return rc;
     const size_t B = G->ws.B;
     const int n = G->sym.n;
@@ -2333,6 +2508,8 @@ int gs_pf_solve_batch(gs_grid* G, int32_t count, const double* loadScale, const 
         float ms = 0;
         rc = NewtonDispatch(G, cnt, loadScale != nullptr, false, o, &ms);
         if (rc) return rc;
+        rc = RetryStalled(G, cnt, out.data(), loadScale ? loadScale + (size_t)done * n : nullptr, false, o, &ms, nullptr);
+        if (rc) return rc;
         std::vector<int> st(cnt), it(cnt);
         std::vector<double> mis(cnt);
         GS_CUDA(cudaMemcpy(st.data(), G->ws.status.p, cnt * 4, cudaMemcpyDeviceToHost));
@@ -2427,6 +2604,8 @@ int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts*
         GS_CUDA(cudaMemcpy(w.outage.p, out.data(), B * 4, cudaMemcpyHostToDevice));
         float ms = 0;
         rc = NewtonDispatch(G, cnt, false, warm, o, &ms, &stats);
+        if (rc) return rc;
+        rc = RetryStalled(G, cnt, out.data(), nullptr, warm, o, &ms, &stats);
         if (rc) return rc;
         totalMs += ms;
         res->n_batches++;

@@ -124,6 +124,11 @@ void BuildTopPart(Symbolic& s, int which, size_t elem, size_t budget);
 // Build the symbolic analysis; returns an empty string on success, else the reason.
 std::string Analyze(const HostGrid& g, Symbolic& s, bool qlim = false);
 
+// DC power-flow angles (degrees) of the grid with branch `skip` out (-1 none), referenced at bus `slack`, with the
+// loads scaled by loadScale[i] (may be null); false unless the DC model is one island (gs_dc.cpp).
+bool DcAngles(const HostGrid& h, const Symbolic& s, int skip, int slack, const double* loadScale,
+              std::vector<double>& thetaDeg);
+
 // Minimum-degree order of a structurally symmetric pattern (pivot step -> index).
 std::vector<int> MinimumDegreeOrder(int n, const std::vector<int>& rowPtr, const std::vector<int>& col);
 

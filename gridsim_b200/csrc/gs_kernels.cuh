@@ -130,7 +130,8 @@ struct DevBatch {
     int* refine;            // [B] refine this step (mixed precision), or null
     unsigned long long* maxMis;  // [B] bit pattern of a non-negative double
     unsigned long long* maxDx;
-    double* startMis;       // [B]
+    double* startMis;       // [B] mismatch at the start of the current Newton run
+    double* beforeLast;     // [B] mismatch the last step was taken from (the DC retry's stall test)
     double* finalMis;       // [B]
     int* status;            // [B]
     int* iters;             // [B] steps taken
@@ -153,6 +154,6 @@ struct DevBatch {
 };
 
 // qState bits
-enum : int32_t { kQPending = 1, kQChanged = 2, kQSkipStep = 4, kQFinalPass = 8 };
+enum : int32_t { kQPending = 1, kQChanged = 2, kQSkipStep = 4, kQFinalPass = 8, kQFinalConverged = 32 };
 
 }  // namespace gs

@@ -205,6 +205,7 @@ extern "C" int gs_pf_solve_multi(gs_ctx* ctx, int32_t nGrids, gs_grid* const* gr
     const gs_pf_opts o = *opts;
     if (o.flat_start) return SetErr(ctx, GS_ERR_UNSUPPORTED, "flat_start: pass a flat start in the descriptor");
     if (o.enforce_q_limits) return SetErr(ctx, GS_ERR_UNSUPPORTED, "enforce_q_limits: not in the multi-grid batch");
+    if (o.retry_from_dc_start) return SetErr(ctx, GS_ERR_UNSUPPORTED, "retry_from_dc_start: not in the multi-grid batch");
     // cases, their offsets and the sizes of the largest grid
     int64_t nCases = 0, nStates = 0;
     int maxN = 1, maxM = 1;

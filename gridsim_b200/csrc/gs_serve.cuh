@@ -375,6 +375,7 @@ int gs_serve_create(gs_ctx* ctx, const gs_serve_opts* opts, gs_server** out) {
     if (rc) return rc;
     if (opts->pf.flat_start) return SetErr(ctx, GS_ERR_UNSUPPORTED, "flat_start: pass a flat start in the descriptor");
     if (opts->pf.enforce_q_limits) return SetErr(ctx, GS_ERR_UNSUPPORTED, "enforce_q_limits: not in the request loop");
+    if (opts->pf.retry_from_dc_start) return SetErr(ctx, GS_ERR_UNSUPPORTED, "retry_from_dc_start: not in the request loop");
     const int slots = opts->slots_per_grid ? opts->slots_per_grid : GS_SERVE_MAX_SLOTS;
     if (slots < 32 || slots > GS_SERVE_MAX_SLOTS || slots % 32)
         return SetErr(ctx, GS_ERR_INVALID_ARG, "slots_per_grid must be a multiple of 32 in [32, 128]");

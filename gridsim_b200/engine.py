@@ -27,9 +27,9 @@ from .model import GridModel
 @dataclass
 class PowerFlowOptions:
     """PowerFlowOptions (``PowerFlow/PowerFlowOptions.cs``). Q-limit enforcement (PV -> PQ switching passes,
-    up to 100, with the reference's reverts) runs on the device for single solves, batch solves and screens; the
-    DC-angle retry is not built and is refused when set. Both default to off here (the reference defaults them on,
-    ``PowerFlowOptions.cs:98,121``) because the benchmark workloads run without them."""
+    up to 100, with the reference's reverts) and the DC-angle retry of stalled solves run for single solves, batch
+    solves and screens. Both default to off here (the reference defaults them on, ``PowerFlowOptions.cs:98,121``)
+    because the benchmark workloads run without them."""
     tolerance: float = 1e-8
     max_iterations: int = 30
     diverge_limit_pu: float = 10.0

@@ -120,7 +120,9 @@ typedef struct gs_pf_opts {
     int32_t enforce_q_limits;       /* PV->PQ switching passes (SparseNewtonRaphsonPowerFlow.cs:118-160); default 0
                                        here (the reference's default is on); refused by the multi-grid batch and
                                        the request loop */
-    int32_t retry_from_dc_start;    /* must be 0 in this build */
+    int32_t retry_from_dc_start;    /* solve a stalled case again from DC power-flow angles (NewtonShell.SolveWithRetry,
+                                       NewtonShell.cs:227-268); default 0 here (the reference's default is on);
+                                       refused by the multi-grid batch and the request loop */
     int32_t per_bus_voltage_limits; /* judge buses against their own vmin/vmax (VoltageLimits.cs:55-67) */
     int32_t precision;              /* enum gs_precision */
     int32_t warm_start_from_base;   /* screens: solve the intact grid first and start every outage from

@@ -10,7 +10,8 @@
 //     target (1e-8) does not need cross-OS bit identity.
 //   * ContingencyAnalysis.ProvablyUnsolvablePart (:1700-1830) is not restated: it only short-cuts states
 //     the Newton solve reports non-converged anyway, with the same result.
-//   * the DC-angle retry (NewtonShell.cs:227-268) is not restated; options with it set are refused.
+//   * the DC power flow of the DC-angle retry assumes the reference bus of a single-island DC model is the
+//     case's slack (DistributionFactors picks it as the AC island pre-pass does); other cases get no retry.
 #include "../include/gridsim_b200.h"
 
 #include <algorithm>
@@ -19,7 +20,9 @@
 #include <complex>
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <limits>
+#include <map>
 #include <numeric>
 #include <string>
 #include <thread>
@@ -688,7 +691,13 @@ constexpr double kVmFloorPu = 0.01;       // NewtonShell.cs:48
 constexpr double kQLimitTolMva = 1e-3;    // NewtonShell.cs:26
 constexpr double kRevertVoltTolPu = 1e-4; // NewtonShell.cs:31
 
-struct RunEnd { bool converged = false, diverged = false; int iters = 0; double maxMis = INFINITY; };
+// How a Newton run ended (NewtonShell.NewtonRunEnd, NewtonShell.cs:170-174): its start mismatch, the mismatch it
+// took its last step from, its steps and whether the iteration cap stopped it.
+struct RunEnd {
+    bool converged = false, diverged = false, capReached = false;
+    int iters = 0;
+    double maxMis = INFINITY, startMis = NAN, beforeLast = NAN;
+};
 
 // RunNewton (:168-265) with NewtonShell.SolveStep (:74-120) and ApplyStep (:128-136).
 RunEnd RunNewton(CpuSparseLuSolver& solver, const ComplexCsr& y, const std::vector<int>& type, std::vector<double>& Vm,
@@ -737,6 +746,7 @@ RunEnd RunNewton(CpuSparseLuSolver& solver, const ComplexCsr& y, const std::vect
             maxAbs = std::max(maxAbs, std::fabs(sol[k]));
         }
         if (!ok) break;
+        r.beforeLast = maxMis;  // the retry's stall test only (SparseNewtonRaphsonPowerFlow.cs:259)
         dx = sol;
         double damp = maxAbs > kMaxUndampedStep ? kMaxUndampedStep / maxAbs : 1.0;
         for (int i = 0; i < n; i++) {
@@ -745,6 +755,8 @@ RunEnd RunNewton(CpuSparseLuSolver& solver, const ComplexCsr& y, const std::vect
         }
     }
     r.iters = iter;
+    r.startMis = startMis;
+    r.capReached = !r.converged && !r.diverged && iter >= opt.max_iterations;
     return r;
 }
 
@@ -807,11 +819,100 @@ struct SolveOut {
     int iterations = 0;
     double maxMis = NAN;
     std::vector<double> vm, va, p, q;  // va in radians; p, q in pu
+    bool available = true;    // false: the DC-angle start could not be formed (nothing was solved)
+    bool newtonFailed = false;  // the last Newton run did not converge (the retry's trigger)
+    RunEnd runEnd;            // how that run ended
 };
+
+// DcPowerFlow.Solve on DcDemand.LegacyView (Analysis/DcPowerFlow.cs:40-51, DcDemand.cs:36-50): every tap 1, no
+// phase shift, no Gs; B' from b = 1/x of the in-service branches with non-zero reactance (the outaged one removed);
+// injections sum(Pg) - Pd; the slack is the single island's reference. Returns false (no angles) unless the DC
+// model is one island, or when B' is singular.
+bool DcAngles(const Model& m, int skip, int slack, std::vector<double>& thetaDeg) {
+    const int n = m.n;
+    std::vector<int> parent(n);
+    std::iota(parent.begin(), parent.end(), 0);
+    std::function<int(int)> find = [&](int a) { return parent[a] == a ? a : parent[a] = find(parent[a]); };
+    std::vector<std::pair<int, int>> cells;
+    std::vector<double> vals;
+    std::vector<int> red(n, -1);
+    int nr = 0;
+    for (int i = 0; i < n; i++) if (i != slack) red[i] = nr++;
+    std::map<std::pair<int, int>, double> acc;
+    for (int k = 0; k < (int)m.br.size(); k++) {
+        const Br& br = m.br[k];
+        if (!br.inService || k == skip || br.x == 0.0) continue;
+        parent[find(br.f)] = find(br.t);
+        const double b = 1.0 / br.x;
+        const int f = red[br.f], t = red[br.t];
+        if (f >= 0) acc[{f, f}] += b;
+        if (t >= 0) acc[{t, t}] += b;
+        if (f >= 0 && t >= 0) { acc[{f, t}] -= b; acc[{t, f}] -= b; }
+    }
+    int islands = 0;
+    for (int i = 0; i < n; i++) if (find(i) == i) islands++;
+    if (islands != 1 || nr == 0) return false;
+    Csr a;
+    a.n = nr;
+    a.rowPtr.assign(nr + 1, 0);
+    for (auto& kv : acc) a.rowPtr[kv.first.first + 1]++;
+    for (int r = 0; r < nr; r++) a.rowPtr[r + 1] += a.rowPtr[r];
+    for (auto& kv : acc) { a.colIdx.push_back(kv.first.second); a.val.push_back(kv.second); }  // map order: row-major
+    std::vector<double> pinj(n, 0.0), rhs(nr), th;
+    for (const Gen& g : m.gens) pinj[g.bus] += g.pg;
+    for (int i = 0; i < n; i++) if (red[i] >= 0) rhs[red[i]] = (pinj[i] - m.pd[i]) / m.base;
+    CpuSparseLuSolver solver;
+    if (!solver.Solve(a, rhs, th)) return false;
+    thetaDeg.assign(n, 0.0);
+    for (int i = 0; i < n; i++) if (red[i] >= 0) thetaDeg[i] = th[red[i]] * 180.0 / kPi;
+    return true;
+}
+
+// NewtonShell.TrySeedDcAngles (:282-299): every non-slack start angle from the DC power flow, reduced to
+// [-180, 180] degrees, offset by the slack's own start angle; magnitudes unchanged. False: no single slack, or no
+// single-island DC model.
+bool TrySeedDcAngles(const Model& m, int skip, BusSpec& s) {
+    int slack = -1, slacks = 0;
+    for (int i = 0; i < m.n; i++) if (s.type0[i] == 3) { slack = i; slacks++; }
+    if (slacks != 1) return false;
+    std::vector<double> th;
+    if (!DcAngles(m, skip, slack, th)) return false;
+    const double va0 = s.va[slack];
+    for (int i = 0; i < m.n; i++)
+        if (i != slack) s.va[i] = va0 + std::remainder(th[i], 360.0) * kPi / 180.0;
+    return true;
+}
+
+constexpr double kRetryStallFactor = 1e-3;        // NewtonShell.cs:146
+constexpr double kRetryLastStepFactor = 0.5;      // NewtonShell.cs:167
+constexpr double kMaxRetryBranchAngleDeg = 90.0;  // NewtonShell.cs:142
+
+// NewtonShell.Stalled (:162, :200-206): a run that did not converge stalled (or diverged) rather than being cut off
+// by the iteration cap while still converging.
+bool Stalled(const RunEnd& r, double finalMis) {
+    if (r.capReached && r.iters == 0) return false;
+    if (finalMis <= kRetryStallFactor * r.startMis) return false;  // a NaN on either side counts as stalled
+    if (r.capReached && r.iters >= 2 && finalMis <= kRetryLastStepFactor * r.beforeLast) return false;
+    return true;
+}
+
+// NewtonShell.MaxBranchAngleDeg: the largest angle across an in-service branch, net of its phase shift, wrapped
+// to [-180, 180] degrees.
+double MaxBranchAngleDeg(const Model& m, int skip, const std::vector<double>& vaRad) {
+    double mx = 0.0;
+    for (int k = 0; k < (int)m.br.size(); k++) {
+        const Br& br = m.br[k];
+        if (!br.inService || k == skip) continue;
+        const double a = std::fabs(std::remainder((vaRad[br.f] - vaRad[br.t]) * 180.0 / kPi - br.shift, 360.0));
+        mx = std::max(mx, a);
+    }
+    return mx;
+}
 
 // SparseNewtonRaphsonPowerFlow.SolveAcAttempt (:69-166) + NewtonShell.AssembleResult status (:649-693).
 // `vmStart/vaStart` (radians) replace the model's stored start when given (warm start, GridScenario.cs:35-52).
-SolveOut SolveModel(const Model& m, int skip, const gs_pf_opts& opt, const double* vmStart, const double* vaStartRad) {
+SolveOut SolveModel(const Model& m, int skip, const gs_pf_opts& opt, const double* vmStart, const double* vaStartRad,
+                    bool dcStart = false) {
     int n = m.n;
     ComplexCsr y = BuildY(m, skip);
     Model mm;  // only the start values can differ
@@ -825,6 +926,11 @@ SolveOut SolveModel(const Model& m, int skip, const gs_pf_opts& opt, const doubl
     if (vmStart) {  // keep the radian start exactly (the degree round trip is not needed)
         for (int i = 0; i < n; i++)
             if (src->type[i] != 3 && !opt.flat_start) s.va[i] = vaStartRad[i];
+    }
+    if (dcStart && !TrySeedDcAngles(m, skip, s)) {
+        SolveOut none;
+        none.available = false;
+        return none;
     }
     std::vector<int> eff = s.type0, pinned(n, kPinNone), revertCount(n, 0);
     std::vector<double> Vm = s.vm, Va = s.va, P(n), Q(n), qspec = s.qspec;
@@ -851,6 +957,7 @@ SolveOut SolveModel(const Model& m, int skip, const gs_pf_opts& opt, const doubl
         total += re.iters;
         converged = false;
     }
+    const bool newtonFailed = !re.converged;
     ComputeInjections(y, Vm, Va, P, Q);
     SolveOut o;
     bool finite = std::isfinite(re.maxMis);
@@ -863,8 +970,24 @@ SolveOut SolveModel(const Model& m, int skip, const gs_pf_opts& opt, const doubl
              : GS_PF_MAX_ITERATIONS;
     o.iterations = total;
     o.maxMis = re.maxMis;
+    o.newtonFailed = newtonFailed;
+    o.runEnd = re;
     o.vm = Vm; o.va = Va; o.p = P; o.q = Q;
     return o;
+}
+
+// NewtonShell.SolveWithRetry (:227-268): the ordinary solve; when its last Newton run failed to converge and stalled
+// (and the option is on, with a cap above 1), the solve again from DC power-flow angles, kept only if it converges
+// with every branch angle within 90 degrees.
+SolveOut SolveWithRetry(const Model& m, int skip, const gs_pf_opts& opt, const double* vmStart, const double* vaStartRad) {
+    SolveOut first = SolveModel(m, skip, opt, vmStart, vaStartRad, false);
+    if (first.status == GS_PF_CONVERGED || !first.newtonFailed || !opt.retry_from_dc_start || opt.max_iterations <= 1 ||
+        !Stalled(first.runEnd, first.maxMis))
+        return first;
+    SolveOut retry = SolveModel(m, skip, opt, vmStart, vaStartRad, true);
+    if (!retry.available) return first;
+    if (retry.status == GS_PF_CONVERGED && MaxBranchAngleDeg(m, skip, retry.va) <= kMaxRetryBranchAngleDeg) return retry;
+    return first;
 }
 
 // NewtonShell.ComputeLineFlows (:699-734): per-branch complex flows (MVA) and loading %.
@@ -923,7 +1046,7 @@ void Classify(const Model& m, int skip, const std::vector<double>& vm, const std
     }
 }
 
-bool OptionsSupported(const gs_pf_opts* o) { return o && !o->retry_from_dc_start; }
+bool OptionsSupported(const gs_pf_opts* o) { return o != nullptr; }
 
 }  // namespace
 
@@ -934,7 +1057,7 @@ extern "C" {
 int gso_pf_solve(const gs_grid_desc* d, const gs_pf_opts* opt, gs_pf_result* res) {
     if (!d || !res || !OptionsSupported(opt)) return GS_ERR_INVALID_ARG;
     Model m = FromDesc(d);
-    SolveOut o = SolveModel(m, -1, *opt, nullptr, nullptr);
+    SolveOut o = SolveWithRetry(m, -1, *opt, nullptr, nullptr);
     res->status = o.status;
     res->iterations = o.iterations;
     res->max_mismatch = o.maxMis;
@@ -1013,7 +1136,7 @@ int gso_n1_screen(const gs_grid_desc* d, int32_t nOut, const int32_t* idx, const
     res->base_status = GS_PF_NOT_RUN;
     res->base_iterations = 0;
     if (opt->warm_start_from_base) {
-        SolveOut b = SolveModel(m, -1, *opt, nullptr, nullptr);
+        SolveOut b = SolveWithRetry(m, -1, *opt, nullptr, nullptr);
         res->base_status = b.status;
         res->base_iterations = b.iterations;
         vm0 = b.vm;
@@ -1027,8 +1150,8 @@ int gso_n1_screen(const gs_grid_desc* d, int32_t nOut, const int32_t* idx, const
         for (;;) {
             int k = cursor.fetch_add(1);
             if (k >= nOut) return;
-            outs[k] = SolveModel(m, idx[k], *opt, vm0.empty() ? nullptr : vm0.data(),
-                                 va0.empty() ? nullptr : va0.data());
+            outs[k] = SolveWithRetry(m, idx[k], *opt, vm0.empty() ? nullptr : vm0.data(),
+                                     va0.empty() ? nullptr : va0.data());
             if (outs[k].status == GS_PF_CONVERGED)
                 Classify(m, idx[k], outs[k].vm, outs[k].va, opt->per_bus_voltage_limits != 0, maxLoad[k], minVm[k],
                          maxVm[k], viol[k]);
