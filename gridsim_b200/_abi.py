@@ -17,8 +17,11 @@ c_i32, c_f64, c_u8, c_vp = ctypes.c_int32, ctypes.c_double, ctypes.c_uint8, ctyp
 GS_OK, GS_ERR_INVALID_ARG, GS_ERR_CUDA, GS_ERR_OOM, GS_ERR_NO_DEVICE = 0, 1, 2, 3, 4
 GS_ERR_TIMEOUT, GS_ERR_STATE, GS_ERR_UNSUPPORTED, GS_ERR_INTERNAL, GS_ERR_CAPACITY = 5, 6, 7, 8, 9
 
-PF_CONVERGED, PF_MAX_ITERATIONS, PF_NON_FINITE, PF_DIVERGED, PF_SINGULAR_PIVOT, PF_TIMEOUT, PF_NOT_RUN = range(7)
-PF_STATUS_NAMES = ["Converged", "MaxIterations", "NonFinite", "Diverged", "SingularPivot", "Timeout", "NotRun"]
+(PF_CONVERGED, PF_MAX_ITERATIONS, PF_NON_FINITE, PF_DIVERGED, PF_SINGULAR_PIVOT, PF_TIMEOUT, PF_NOT_RUN,
+ PF_UNSOLVABLE_PART) = range(8)
+PF_STATUS_NAMES = ["Converged", "MaxIterations", "NonFinite", "Diverged", "SingularPivot", "Timeout", "NotRun",
+                   "UnsolvablePart"]
+RATE_A, RATE_B, RATE_C = 0, 1, 2
 
 PREC_FP64, PREC_MIXED = 0, 1
 VIOL_BRANCH_OVERLOAD, VIOL_BOUNDARY_OVERLOAD, VIOL_UNDERVOLTAGE, VIOL_OVERVOLTAGE = 0, 1, 2, 3
@@ -36,7 +39,9 @@ class GridDesc(ctypes.Structure):
         ("gen_bus", c_vp), ("pg", c_vp), ("qg", c_vp), ("vg", c_vp), ("qmin", c_vp), ("qmax", c_vp),
         ("gen_in_service", c_vp),
         ("br_from", c_vp), ("br_to", c_vp), ("r", c_vp), ("x", c_vp), ("b", c_vp), ("tap", c_vp),
-        ("shift_deg", c_vp), ("rate_a", c_vp), ("br_in_service", c_vp),
+        ("shift_deg", c_vp), ("rate_a", c_vp), ("br_in_service", c_vp), ("rate_b", c_vp), ("rate_c", c_vp),
+        ("n_boundary", c_i32), ("reserved1", c_i32), ("bnd_ptr", c_vp), ("bnd_branch", c_vp), ("bnd_dir", c_vp),
+        ("bnd_limit_mw", c_vp),
     ]
 
 
@@ -45,7 +50,7 @@ class PfOpts(ctypes.Structure):
         ("tolerance", c_f64), ("diverge_limit_pu", c_f64), ("max_iterations", c_i32), ("flat_start", c_i32),
         ("enforce_q_limits", c_i32), ("retry_from_dc_start", c_i32), ("per_bus_voltage_limits", c_i32),
         ("precision", c_i32), ("warm_start_from_base", c_i32), ("batch_width", c_i32), ("phase_timing", c_i32),
-        ("reserved", c_i32 * 7),
+        ("post_fault_rating", c_i32), ("reserved", c_i32 * 6),
     ]
 
 
@@ -65,7 +70,8 @@ class N1Result(ctypes.Structure):
         ("base_status", c_i32), ("base_iterations", c_i32), ("device_ms", c_f64), ("n_singular_pivot", c_i32),
         ("n_batches", c_i32), ("kernel_launches", ctypes.c_int64), ("newton_iterations", c_i32), ("reserved1", c_i32),
         ("factor_ms", c_f64), ("solve_ms", c_f64), ("mismatch_ms", c_f64), ("other_ms", c_f64), ("factor_bytes", c_f64),
-        ("level_factor_ms", c_f64), ("level_factor_bytes", c_f64), ("tail_ms", c_f64),
+        ("level_factor_ms", c_f64), ("level_factor_bytes", c_f64), ("tail_ms", c_f64), ("islanded", c_vp),
+        ("worst_boundary_pct", c_vp),
     ]
 
 
@@ -121,6 +127,7 @@ EXPORTS = {
     "gs_pf_solve_batch": (c_i32, [c_vp, c_i32, c_vp, c_vp, ctypes.POINTER(PfOpts), c_vp, c_vp, c_vp, c_vp, c_vp]),
     "gs_n1_screen": (c_i32, [c_vp, c_i32, c_vp, ctypes.POINTER(PfOpts), ctypes.POINTER(N1Result)]),
     "gs_analyze_host": (c_i32, [ctypes.POINTER(GridDesc), ctypes.POINTER(GridInfo)]),
+    "gs_outage_topology": (c_i32, [ctypes.POINTER(GridDesc), c_f64, c_i32, c_vp, c_vp, c_vp]),
     "gs_pf_mismatch_noalloc": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp]),
     "gs_pf_solve_multi": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(PfOpts), c_vp, c_vp, c_vp, c_vp,
                                   c_vp, ctypes.POINTER(MultiStats)]),

@@ -67,7 +67,17 @@ __device__ __forceinline__ void busMismatchJac(const DevGrid& g, const DevBatch&
     int c0 = -1, c1 = -1, c2 = -1, c3 = -1;
     if (o >= 0) { c0 = g.brCell[4 * o]; c1 = g.brCell[4 * o + 1]; c2 = g.brCell[4 * o + 2]; c3 = g.brCell[4 * o + 3]; }
     const double vmi = b.vm[i * B + s], vai = b.va[i * B + s];
-    double pi = 0.0, qi = 0.0;
+    // Q limits: a bus that starts PV keeps an identity Q row while it is PV (its Vm step is 0, its Q mismatch
+    // is not an equation); once switched to PQ its Q is held at the limit
+    const bool startsPV = g.qlim && g.busType[i] == 2;
+    const bool pvNow = startsPV && b.effType[i * B + s] == 2;
+    const int kp = g.busP[i], kq = g.busQ[i];
+    const bool fill = fillJac && (kp >= 0 || kq >= 0);
+    T* lu = (T*)b.lu;
+    // one pass over row i: the injections, and the off-diagonal Jacobian blocks from the same sin/cos (they do not
+    // need P, Q); the diagonal blocks follow from the sums
+    double pi = 0.0, qi = 0.0, Gd = 0.0, Bd = 0.0;
+    int pd = -1;
     const int p0 = g.yRowPtr[i], p1 = g.yRowPtr[i + 1];
     for (int p = p0; p < p1; p++) {
         const int j = g.yCol[p];
@@ -81,22 +91,41 @@ __device__ __forceinline__ void busMismatchJac(const DevGrid& g, const DevBatch&
         const double vmj = b.vm[j * B + s];
         pi += vmj * (G * cs + Bv * sn);
         qi += vmj * (G * sn - Bv * cs);
+        if (j == i) { pd = p; Gd = G; Bd = Bv; continue; }
+        if (!fill) continue;
+        const double H = vmi * vmj * (G * sn - Bv * cs);
+        const double N = vmi * (G * cs + Bv * sn);
+        const double M = pvNow ? 0.0 : -vmi * vmj * (G * cs + Bv * sn);  // the identity Q row of a bus that is PV now
+        const double L = pvNow ? 0.0 : vmi * (G * sn - Bv * cs);
+        const int4 sl = *reinterpret_cast<const int4*>(g.ySlot + 4 * p);
+        if (sl.x >= 0) lu[sl.x * B + s] = (T)H;
+        if (sl.y >= 0) lu[sl.y * B + s] = (T)N;
+        if (sl.z >= 0) lu[sl.z * B + s] = (T)M;
+        if (sl.w >= 0) lu[sl.w * B + s] = (T)L;
+        bad |= (isfinite(H) && isfinite(N) && isfinite(M) && isfinite(L)) ? 0 : 2;
     }
     const double P = vmi * pi, Q = vmi * qi;
+    if (fill && pd >= 0) {
+        const double H = -Q - Bd * vmi * vmi;
+        const double N = P / vmi + Gd * vmi;
+        const double M = pvNow ? 0.0 : P - Gd * vmi * vmi;
+        const double L = pvNow ? 1.0 : Q / vmi - Bd * vmi;
+        const int4 sl = *reinterpret_cast<const int4*>(g.ySlot + 4 * pd);
+        if (sl.x >= 0) lu[sl.x * B + s] = (T)H;
+        if (sl.y >= 0) lu[sl.y * B + s] = (T)N;
+        if (sl.z >= 0) lu[sl.z * B + s] = (T)M;
+        if (sl.w >= 0) lu[sl.w * B + s] = (T)L;
+        bad |= (isfinite(H) && isfinite(N) && isfinite(M) && isfinite(L)) ? 0 : 2;
+    }
     if (pOut) { pOut[i * B + s] = P; qOut[i * B + s] = Q; }
     double sc = b.loadScale ? b.loadScale[i * B + s] : 1.0;
     const double pspec = b.loadScale ? g.pgen[i] - sc * g.pload[i] : g.pgen[i] - g.pload[i];
     double qspec = b.loadScale ? g.qgen[i] - sc * g.qload[i] : g.qgen[i] - g.qload[i];
-    // Q limits: a bus that starts PV keeps an identity Q row while it is PV (its Vm step is 0, its Q mismatch
-    // is not an equation); once switched to PQ its Q is held at the limit
-    const bool startsPV = g.qlim && g.busType[i] == 2;
-    const bool pvNow = startsPV && b.effType[i * B + s] == 2;
     if (startsPV) {
         b.qinj[i * B + s] = Q;
         if (!pvNow) qspec = b.qspecSys[i * B + s];
     }
     T* y = (T*)b.y;
-    const int kp = g.busP[i], kq = g.busQ[i];
     if (kp >= 0) {
         const double f = pspec - P;
         y[kp * B + s] = (T)f;
@@ -113,42 +142,6 @@ __device__ __forceinline__ void busMismatchJac(const DevGrid& g, const DevBatch&
         if (b.rhs64) b.rhs64[kq * B + s] = f;
         localMax = fmax(localMax, fabs(f));
         bad |= isfinite(f) ? 0 : 1;
-    }
-    if (fillJac && (kp >= 0 || kq >= 0)) {
-        T* lu = (T*)b.lu;
-        for (int p = p0; p < p1; p++) {
-            const int j = g.yCol[p];
-            double G = g.yG[p], Bv = g.yB[p];
-            if (p == c0) { G = g.brRed[8 * o + 0]; Bv = g.brRed[8 * o + 1]; }
-            else if (p == c1) { G = g.brRed[8 * o + 2]; Bv = g.brRed[8 * o + 3]; }
-            else if (p == c2) { G = g.brRed[8 * o + 4]; Bv = g.brRed[8 * o + 5]; }
-            else if (p == c3) { G = g.brRed[8 * o + 6]; Bv = g.brRed[8 * o + 7]; }
-            double H, N, M, L;
-            if (i == j) {
-                H = -Q - Bv * vmi * vmi;
-                N = P / vmi + G * vmi;
-                M = P - G * vmi * vmi;
-                L = Q / vmi - Bv * vmi;
-            } else {
-                double sn, cs;
-                sincos(vai - b.va[j * B + s], &sn, &cs);
-                const double vmj = b.vm[j * B + s];
-                H = vmi * vmj * (G * sn - Bv * cs);
-                N = vmi * (G * cs + Bv * sn);
-                M = -vmi * vmj * (G * cs + Bv * sn);
-                L = vmi * (G * sn - Bv * cs);
-            }
-            if (pvNow) {  // the identity Q row of a bus that is PV now
-                M = 0.0;
-                L = i == j ? 1.0 : 0.0;
-            }
-            const int4 sl = *reinterpret_cast<const int4*>(g.ySlot + 4 * p);
-            if (sl.x >= 0) lu[sl.x * B + s] = (T)H;
-            if (sl.y >= 0) lu[sl.y * B + s] = (T)N;
-            if (sl.z >= 0) lu[sl.z * B + s] = (T)M;
-            if (sl.w >= 0) lu[sl.w * B + s] = (T)L;
-            bad |= (isfinite(H) && isfinite(N) && isfinite(M) && isfinite(L)) ? 0 : 2;
-        }
     }
 }
 
@@ -1346,52 +1339,86 @@ __global__ void k_init(DevGrid g, DevBatch b, const double* vmStart, const doubl
 struct Classify {
     const double* lo;  // [n] effective lower limit
     const double* hi;
-    uint8_t* code;     // [items][B]: 0 none, 1 overload, 2 under, 3 over
+    uint8_t* code;     // [items][B]: 0 none, 1 overload, 2 under, 3 over, 4 boundary overload
     double* value;     // [items][B]
     unsigned long long* maxLoad;  // [B]
     unsigned long long* minVmNeg; // [B] max of (-Vm) stored as bits of (100 - Vm) (positive)
     unsigned long long* maxVm;    // [B]
+    unsigned long long* worstBnd; // [B]
     int* chunkCount;   // [nChunks][B]
     int chunk;
+    int postRating;    // enum gs_post_fault_rating: the rating of outage states
 };
 
+// From-end and to-end complex power of branch k in system s, pu (NewtonShell.ComputeLineFlows :699-734).
+__device__ __forceinline__ void branchPower(const DevGrid& g, const DevBatch& b, int k, int s, double& sFr,
+                                            double& sFi, double& sTr, double& sTi) {
+    const size_t B = (size_t)b.B;
+    const int f = g.brF[k], t = g.brT[k];
+    double sf, cf, st, ct;
+    sincos(b.va[f * B + s], &sf, &cf);
+    sincos(b.va[t * B + s], &st, &ct);
+    const double vfr = b.vm[f * B + s] * cf, vfi = b.vm[f * B + s] * sf;
+    const double vtr = b.vm[t * B + s] * ct, vti = b.vm[t * B + s] * st;
+    const double* y = g.brStamp + 8 * k;
+    // iF = yff vf + yft vt ; iT = ytf vf + ytt vt
+    const double ifr = y[0] * vfr - y[1] * vfi + y[4] * vtr - y[5] * vti;
+    const double ifi = y[0] * vfi + y[1] * vfr + y[4] * vti + y[5] * vtr;
+    const double itr = y[6] * vfr - y[7] * vfi + y[2] * vtr - y[3] * vti;
+    const double iti = y[6] * vfi + y[7] * vfr + y[2] * vti + y[3] * vtr;
+    // S = V conj(I)
+    sFr = vfr * ifr + vfi * ifi; sFi = vfi * ifr - vfr * ifi;
+    sTr = vtr * itr + vti * iti; sTi = vti * itr - vtr * iti;
+}
+
+// Items per system: the branches (thermal), the boundaries, then the buses (voltage), in the order the reference
+// lists the violations (ScreenStateCore :1150-1235).
 __global__ void k_classify(DevGrid g, DevBatch b, Classify c) {
     const int lane = threadIdx.x;
     const int s = blockIdx.y * 32 + lane;
     const int item = blockIdx.x * 8 + threadIdx.y;
-    const int nItems = g.nbr + g.n;
+    const int nItems = g.nbr + g.nBnd + g.n;
     if (item >= nItems || s >= b.count) return;
     const size_t B = (size_t)b.B;
     uint8_t code = 0;
     double val = 0.0;
     if (b.status[s] == GS_PF_CONVERGED) {
+        const int o = b.outage[s];
         if (item < g.nbr) {
             const int k = item;
-            if (g.brOn[k] && k != b.outage[s]) {
-                const int f = g.brF[k], t = g.brT[k];
-                double sf, cf, st, ct;
-                sincos(b.va[f * B + s], &sf, &cf);
-                sincos(b.va[t * B + s], &st, &ct);
-                const double vfr = b.vm[f * B + s] * cf, vfi = b.vm[f * B + s] * sf;
-                const double vtr = b.vm[t * B + s] * ct, vti = b.vm[t * B + s] * st;
-                const double* y = g.brStamp + 8 * k;
-                // iF = yff vf + yft vt ; iT = ytf vf + ytt vt
-                const double ifr = y[0] * vfr - y[1] * vfi + y[4] * vtr - y[5] * vti;
-                const double ifi = y[0] * vfi + y[1] * vfr + y[4] * vti + y[5] * vtr;
-                const double itr = y[6] * vfr - y[7] * vfi + y[2] * vtr - y[3] * vti;
-                const double iti = y[6] * vfi + y[7] * vfr + y[2] * vti + y[3] * vtr;
-                // S = V conj(I) * base
-                const double sFr = vfr * ifr + vfi * ifi, sFi = vfi * ifr - vfr * ifi;
-                const double sTr = vtr * itr + vti * iti, sTi = vti * itr - vtr * iti;
-                // base_mva folded into rateA (the host passes rateA / base)
+            if (g.brOn[k] && k != o) {
+                double sFr, sFi, sTr, sTi;
+                branchPower(g, b, k, s, sFr, sFi, sTr, sTi);
                 const double mva = fmax(hypot(sFr, sFi), hypot(sTr, sTi));
-                const double r = g.rateA[k];
+                // base_mva folded into the ratings (the host passes rating / base); an outage state may be judged
+                // against RateB / RateC, falling back to RateA where that rating is 0 (:1273-1284)
+                double r = g.rateA[k];
+                if (c.postRating != GS_RATE_A && o >= 0) {
+                    const double rx = c.postRating == GS_RATE_B ? g.rateB[k] : g.rateC[k];
+                    if (rx > 0) r = rx;
+                }
                 val = r > 0 ? mva / r * 100.0 : 0.0;
                 if (val > 0.0) atomicMaxNonNeg(&c.maxLoad[s], val);
                 if (val > 100.0) code = 1;
             }
+        } else if (item < g.nbr + g.nBnd) {
+            // BoundaryAnalysis.EvaluateAfterOutage (Analysis/BoundaryAnalysis.cs:43-68): the signed sum of the members'
+            // from-end MW; the outaged branch is not in the reduced model, an out-of-service one carries nothing
+            const int q = item - g.nbr;
+            double flow = 0.0;
+            for (int e = g.bndPtr[q]; e < g.bndPtr[q + 1]; e++) {
+                const int k = g.bndBranch[e];
+                if (!g.brOn[k] || k == o) continue;
+                double sFr, sFi, sTr, sTi;
+                branchPower(g, b, k, s, sFr, sFi, sTr, sTi);
+                flow += g.bndDir[e] * (sFr * g.baseMva);
+            }
+            const double lim = g.bndLimit[q];
+            val = lim > 0 ? fabs(flow) / lim * 100.0 : 0.0;
+            if (val > 0.0) atomicMaxNonNeg(&c.worstBnd[s], val);
+            if (lim > 0 && fabs(flow) > lim) code = 4;
         } else {
-            const int i = item - g.nbr;
+            const int i = item - g.nbr - g.nBnd;
             val = b.vm[i * B + s];
             if (val < c.lo[i]) code = 2;
             else if (val > c.hi[i]) code = 3;
@@ -1410,7 +1437,7 @@ __global__ void k_compact(DevGrid g, DevBatch b, Classify c, const int* chunkOff
     const int lane = threadIdx.x;
     const int s = blockIdx.y * 32 + lane;
     const int ch = blockIdx.x * 4 + threadIdx.y;
-    const int nItems = g.nbr + g.n;
+    const int nItems = g.nbr + g.nBnd + g.n;
     const int nChunks = (nItems + c.chunk - 1) / c.chunk;
     if (ch >= nChunks || s >= b.count) return;
     const size_t B = (size_t)b.B;
@@ -1419,8 +1446,10 @@ __global__ void k_compact(DevGrid g, DevBatch b, Classify c, const int* chunkOff
     for (int item = ch * c.chunk; item < e; item++) {
         const uint8_t code = c.code[(size_t)item * B + s];
         if (!code) continue;
-        outKind[w] = code == 1 ? GS_VIOL_BRANCH_OVERLOAD : (code == 2 ? GS_VIOL_UNDERVOLTAGE : GS_VIOL_OVERVOLTAGE);
-        outElem[w] = code == 1 ? item : busId[item - g.nbr];
+        outKind[w] = code == 1 ? GS_VIOL_BRANCH_OVERLOAD
+                   : code == 4 ? GS_VIOL_BOUNDARY_OVERLOAD
+                   : (code == 2 ? GS_VIOL_UNDERVOLTAGE : GS_VIOL_OVERVOLTAGE);
+        outElem[w] = code == 1 ? item : code == 4 ? item - g.nbr : busId[item - g.nbr - g.nBnd];
         outVal[w] = c.value[(size_t)item * B + s];
         w++;
     }
@@ -1494,7 +1523,7 @@ struct Workspace {
     DevBuf beforeLast;
     DevBuf vm, va, lu, piv, y, z, rhs64, refine, maxMis, maxDx, startMis, finalMis, status, iters, convIters, active, flags, outage,
         loadScale, activeCount;
-    DevBuf code, value, maxLoad, minVmNeg, maxVmB, chunkCount, chunkOffset, outKind, outElem, outVal, pq;
+    DevBuf code, value, maxLoad, minVmNeg, maxVmB, worstBnd, chunkCount, chunkOffset, outKind, outElem, outVal, pq;
     DevBuf startVm, startVa;
 };
 
@@ -1572,15 +1601,21 @@ int UploadGrid(gs_grid* G) {
         G->pgen[i] /= h.base; G->qgen[i] /= h.base;
         G->pload[i] = h.pd[i] / h.base; G->qload[i] = h.qd[i] / h.base;
     }
-    std::vector<double> rate(h.nbr);
-    for (int k = 0; k < h.nbr; k++) rate[k] = h.rateA[k] / h.base;
+    std::vector<double> rate(h.nbr), rateB(h.nbr), rateC(h.nbr);
+    for (int k = 0; k < h.nbr; k++) {
+        rate[k] = h.rateA[k] / h.base;
+        rateB[k] = h.rateB[k] / h.base;
+        rateC[k] = h.rateC[k] / h.base;
+    }
+    v.nBnd = h.nBnd;
     std::vector<int2> pairs(s.pairs.size() / 2);
     for (size_t q = 0; q < pairs.size(); q++) pairs[q] = make_int2(s.pairs[2 * q], s.pairs[2 * q + 1]);
     int rc;
 #define UP(vec, field) if ((rc = Upload(G, vec, &v.field)) != GS_OK) return rc
     UP(s.yRowPtr, yRowPtr); UP(s.yCol, yCol); UP(s.yG, yG); UP(s.yB, yB);
     UP(s.brCell, brCell); UP(s.brRed, brRed); UP(s.brStamp, brStamp);
-    UP(h.brF, brF); UP(h.brT, brT); UP(rate, rateA); UP(h.brOn, brOn);
+    UP(h.brF, brF); UP(h.brT, brT); UP(rate, rateA); UP(rateB, rateB); UP(rateC, rateC); UP(h.brOn, brOn);
+    UP(h.bndPtr, bndPtr); UP(h.bndBranch, bndBranch); UP(h.bndDir, bndDir); UP(h.bndLimit, bndLimit);
     UP(G->pgen, pgen); UP(G->qgen, qgen); UP(G->pload, pload); UP(G->qload, qload);
     {
         std::vector<double> qminPu(n), qmaxPu(n);
@@ -1665,7 +1700,8 @@ size_t PerSystemBytes(const Symbolic& s, int precision) {
     return (size_t)s.nnzLU * t + 2 * (size_t)s.m * t + refine + (size_t)s.n * 16 + (size_t)(s.nbr + s.n) * 9 + 256;
 }
 
-int EnsureWs(gs_ctx* ctx, const Symbolic& s, Workspace& w, int B, int precision, bool classify, bool loadScale) {
+// classifyItems: items per system of the screen's classification (branches + boundaries + buses), 0 = none
+int EnsureWs(gs_ctx* ctx, const Symbolic& s, Workspace& w, int B, int precision, int classifyItems, bool loadScale) {
     if (s.qlim) {
         const size_t nb = (size_t)s.n * B;
         GS_CUDA(w.effType.alloc(nb * 4)); GS_CUDA(w.qspecSys.alloc(nb * 8)); GS_CUDA(w.pinned.alloc(nb * 4));
@@ -1693,11 +1729,12 @@ int EnsureWs(gs_ctx* ctx, const Symbolic& s, Workspace& w, int B, int precision,
     GS_CUDA(w.origin.alloc(Bz * 4));
     GS_CUDA(w.startVm.alloc(s.n * 8)); GS_CUDA(w.startVa.alloc(s.n * 8));
     if (loadScale) GS_CUDA(w.loadScale.alloc(s.n * Bz * 8));
-    if (classify) {
-        const int nItems = s.nbr + s.n;
+    if (classifyItems > 0) {
+        const int nItems = classifyItems;
         GS_CUDA(w.code.alloc((size_t)nItems * Bz));
         GS_CUDA(w.value.alloc((size_t)nItems * Bz * 8));
         GS_CUDA(w.maxLoad.alloc(Bz * 8)); GS_CUDA(w.minVmNeg.alloc(Bz * 8)); GS_CUDA(w.maxVmB.alloc(Bz * 8));
+        GS_CUDA(w.worstBnd.alloc(Bz * 8));
     }
     w.B = B;
     w.precision = precision;
@@ -1710,9 +1747,10 @@ int EnsureWorkspace(gs_grid* G, int B, int precision, bool classify, bool loadSc
     // FP64 whatever the batch's precision: the few-systems path is latency-bound, so FP32 factors save nothing there
     // and would need the refinement solve
     (void)precision;
-    int rc = EnsureWs(G->ctx, G->sym, G->tws, cap, GS_PREC_FP64, false, loadScale);
+    int rc = EnsureWs(G->ctx, G->sym, G->tws, cap, GS_PREC_FP64, 0, loadScale);
     if (rc != GS_OK) return rc;
-    return EnsureWs(G->ctx, G->sym, G->ws, B, precision, classify, loadScale);
+    return EnsureWs(G->ctx, G->sym, G->ws, B, precision, classify ? G->sym.nbr + G->host.nBnd + G->sym.n : 0,
+                    loadScale);
 }
 
 // A batch view of workspace `w` with interleave stride B (at most the stride it was sized for).
@@ -2553,7 +2591,30 @@ int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts*
         if (idx[k] < -1 || idx[k] >= s.nbr || (idx[k] >= 0 && !h.brOn[idx[k]]))
             return SetErr(ctx, GS_ERR_INVALID_ARG, "branch " + std::to_string(idx[k]) + " is not an in-service branch");
     GS_CUDA(cudaSetDevice(ctx->device));
-    const int n = s.n, nItems = s.nbr + s.n;
+    const int n = s.n, nItems = s.nbr + h.nBnd + s.n;
+    // the topology pass (ScreenStateCore :1118-1127): provably unsolvable states are reported without a solve,
+    // and a state that does not converge says whether the outage split the network (:1661-1665)
+    std::vector<uint8_t> splits(nOut), unsolv(nOut);
+    {
+        const std::string terr = OutageTopology(h, o.tolerance, nOut, idx, splits.data(), unsolv.data());
+        if (!terr.empty()) return SetErr(ctx, GS_ERR_INVALID_ARG, terr);
+    }
+    std::vector<int> solvePos;
+    solvePos.reserve(nOut);
+    for (int j = 0; j < nOut; j++) {
+        if (!unsolv[j]) { solvePos.push_back(j); continue; }
+        if (res->status) res->status[j] = GS_PF_UNSOLVABLE_PART;
+        if (res->iterations) res->iterations[j] = 0;
+        if (res->max_mismatch) res->max_mismatch[j] = 0.0;
+        if (res->max_loading_pct) res->max_loading_pct[j] = 0.0;
+        if (res->worst_boundary_pct) res->worst_boundary_pct[j] = 0.0;
+        if (res->min_vm) res->min_vm[j] = 0.0;
+        if (res->max_vm) res->max_vm[j] = 0.0;
+        if (res->islanded) res->islanded[j] = splits[j];
+        if (res->vm) std::fill(res->vm + (size_t)j * n, res->vm + (size_t)(j + 1) * n, 0.0);
+        if (res->va_deg) std::fill(res->va_deg + (size_t)j * n, res->va_deg + (size_t)(j + 1) * n, 0.0);
+    }
+    const int nSolve = (int)solvePos.size();
     res->base_status = GS_PF_NOT_RUN;
     res->base_iterations = 0;
     res->n_singular_pivot = 0;
@@ -2592,15 +2653,15 @@ int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts*
     int written = 0;
     bool capacityOk = true;
     int done = 0;
-    while (done < nOut) {
-        int B = ChooseB(G, nOut - done, o);
+    while (done < nSolve) {
+        int B = ChooseB(G, nSolve - done, o);
         rc = EnsureWorkspace(G, B, o.precision, true, false);
         if (rc) return rc;
         Workspace& w = G->ws;
         const size_t Bz = (size_t)B;
-        const int cnt = std::min(B, nOut - done);
+        const int cnt = std::min(B, nSolve - done);
         std::vector<int> out(B, -1);
-        for (int k = 0; k < cnt; k++) out[k] = idx[done + k];
+        for (int k = 0; k < cnt; k++) out[k] = idx[solvePos[done + k]];
         GS_CUDA(cudaMemcpy(w.outage.p, out.data(), B * 4, cudaMemcpyHostToDevice));
         float ms = 0;
         rc = NewtonDispatch(G, cnt, false, warm, o, &ms, &stats);
@@ -2617,9 +2678,11 @@ int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts*
         GS_CUDA(cudaMemsetAsync(w.maxLoad.p, 0, Bz * 8, ctx->stream));
         GS_CUDA(cudaMemsetAsync(w.minVmNeg.p, 0, Bz * 8, ctx->stream));
         GS_CUDA(cudaMemsetAsync(w.maxVmB.p, 0, Bz * 8, ctx->stream));
+        GS_CUDA(cudaMemsetAsync(w.worstBnd.p, 0, Bz * 8, ctx->stream));
         Classify c{dlo.as<double>(), dhi.as<double>(), w.code.as<uint8_t>(), w.value.as<double>(),
                    w.maxLoad.as<unsigned long long>(), w.minVmNeg.as<unsigned long long>(),
-                   w.maxVmB.as<unsigned long long>(), w.chunkCount.as<int>(), chunk};
+                   w.maxVmB.as<unsigned long long>(), w.worstBnd.as<unsigned long long>(), w.chunkCount.as<int>(),
+                   chunk, o.post_fault_rating};
         DevBatch b = MakeBatch(G, cnt, false);
         k_classify<<<dim3((nItems + 7) / 8, B / 32), dim3(32, 8), 0, ctx->stream>>>(G->view, b, c);
         GS_CUDA(cudaGetLastError());
@@ -2627,7 +2690,7 @@ int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts*
         GS_CUDA(cudaMemcpyAsync(cc.data(), w.chunkCount.p, cc.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
         std::vector<int> st(cnt), it(cnt), fl(cnt);
         std::vector<double> mis(cnt);
-        std::vector<unsigned long long> mxl(cnt), mnv(cnt), mxv(cnt);
+        std::vector<unsigned long long> mxl(cnt), mnv(cnt), mxv(cnt), wbd(cnt);
         GS_CUDA(cudaMemcpyAsync(st.data(), w.status.p, cnt * 4, cudaMemcpyDeviceToHost, ctx->stream));
         GS_CUDA(cudaMemcpyAsync(it.data(), w.iters.p, cnt * 4, cudaMemcpyDeviceToHost, ctx->stream));
         std::vector<int> itc(cnt);
@@ -2637,6 +2700,7 @@ int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts*
         GS_CUDA(cudaMemcpyAsync(mxl.data(), w.maxLoad.p, cnt * 8, cudaMemcpyDeviceToHost, ctx->stream));
         GS_CUDA(cudaMemcpyAsync(mnv.data(), w.minVmNeg.p, cnt * 8, cudaMemcpyDeviceToHost, ctx->stream));
         GS_CUDA(cudaMemcpyAsync(mxv.data(), w.maxVmB.p, cnt * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        GS_CUDA(cudaMemcpyAsync(wbd.data(), w.worstBnd.p, cnt * 8, cudaMemcpyDeviceToHost, ctx->stream));
         GS_CUDA(cudaStreamSynchronize(ctx->stream));
         int batchTotal = 0;
         std::vector<int> sysStart(cnt);
@@ -2650,7 +2714,7 @@ int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts*
             batchTotal = acc;
         }
         for (int k = 0; k < cnt; k++) {
-            const int g = done + k;
+            const int g = solvePos[done + k];
             auto asD = [](unsigned long long u) { double d; std::memcpy(&d, &u, 8); return d; };
             const bool conv = st[k] == GS_PF_CONVERGED;
             if (res->status) res->status[g] = st[k];
@@ -2659,6 +2723,8 @@ int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts*
             if (res->max_loading_pct) res->max_loading_pct[g] = conv ? asD(mxl[k]) : 0.0;
             if (res->min_vm) res->min_vm[g] = conv ? 100.0 - asD(mnv[k]) : 0.0;
             if (res->max_vm) res->max_vm[g] = conv ? asD(mxv[k]) : 0.0;
+            if (res->worst_boundary_pct) res->worst_boundary_pct[g] = conv ? asD(wbd[k]) : 0.0;
+            if (res->islanded) res->islanded[g] = !conv && splits[g];
             if (res->viol_ptr) res->viol_ptr[g] = written + sysStart[k];
             if (fl[k] & kFlagPivotPerturbed) res->n_singular_pivot++;
         }
@@ -2687,12 +2753,16 @@ int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts*
                 GS_CUDA(cudaMemcpy(v.data(), pass == 0 ? w.vm.p : w.va.p, v.size() * 8, cudaMemcpyDeviceToHost));
                 const double f = pass == 0 ? 1.0 : 180.0 / 3.14159265358979323846;
                 for (int k = 0; k < cnt; k++)
-                    for (int i = 0; i < n; i++) dst[(size_t)(done + k) * n + i] = v[(size_t)i * Bz + k] * f;
+                    for (int i = 0; i < n; i++) dst[(size_t)solvePos[done + k] * n + i] = v[(size_t)i * Bz + k] * f;
             }
         }
         done += cnt;
     }
-    if (res->viol_ptr) res->viol_ptr[nOut] = written;
+    if (res->viol_ptr) {  // a state reported without a solve has no entries: it starts where the next one does
+        res->viol_ptr[nOut] = written;
+        for (int j = nOut - 1; j >= 0; j--)
+            if (unsolv[j]) res->viol_ptr[j] = res->viol_ptr[j + 1];
+    }
     res->viol_count = written;
     res->device_ms = totalMs;
     res->kernel_launches = stats.launches;

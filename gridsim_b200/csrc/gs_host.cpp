@@ -51,14 +51,44 @@ std::string CopyGrid(const gs_grid_desc* d, HostGrid& g) {
         g.tap.assign(d->tap, d->tap + nb); g.shift.assign(d->shift_deg, d->shift_deg + nb);
         g.rateA.assign(d->rate_a, d->rate_a + nb);
     }
+    g.rateB.assign(nb, 0.0);
+    g.rateC.assign(nb, 0.0);
+    if (d->rate_b && nb > 0) g.rateB.assign(d->rate_b, d->rate_b + nb);
+    if (d->rate_c && nb > 0) g.rateC.assign(d->rate_c, d->rate_c + nb);
     g.brOn.assign(nb, 1);
     if (d->br_in_service && nb > 0) g.brOn.assign(d->br_in_service, d->br_in_service + nb);
     for (int k = 0; k < nb; k++) {
         if (g.brF[k] < 0 || g.brF[k] >= n || g.brT[k] < 0 || g.brT[k] >= n) return "branch end out of range";
         if (g.brF[k] == g.brT[k]) return "a branch joins a bus to itself";
         if (g.tap[k] < 0 || std::isnan(g.tap[k])) return "a tap ratio must be 0 (a line) or above";  // AdmittanceStamp.cs:63-66
-        if (std::isnan(g.rateA[k])) return "a rating must be 0 (unrated) or a number above 0";
+        // ScreenStateCore refuses a NaN rating A/B/C by name (ContingencyAnalysis.cs:1160-1168)
+        if (std::isnan(g.rateA[k]) || std::isnan(g.rateB[k]) || std::isnan(g.rateC[k]))
+            return "a rating must be 0 (unrated) or a number above 0";
         if (g.r[k] == 0 && g.x[k] == 0) return "a branch has zero impedance";
+    }
+    // boundaries (Model/Model.cs:516-560; the limit rule of BoundaryAnalysis.EvaluateAfterOutage :60-62, the
+    // direction rule of JsonGridLoader.cs:219-223)
+    if (d->n_boundary < 0) return "n_boundary must be 0 or more";
+    g.nBnd = d->n_boundary;
+    g.bndPtr.assign(1, 0);
+    if (g.nBnd > 0) {
+        if (!d->bnd_ptr || !d->bnd_limit_mw) return "a required boundary array is null";
+        if (d->bnd_ptr[0] != 0) return "bnd_ptr[0] must be 0";
+        for (int q = 0; q < g.nBnd; q++)
+            if (d->bnd_ptr[q + 1] < d->bnd_ptr[q]) return "bnd_ptr must not decrease";
+        const int nm = d->bnd_ptr[g.nBnd];
+        if (nm > 0 && (!d->bnd_branch || !d->bnd_dir)) return "a required boundary array is null";
+        g.bndPtr.assign(d->bnd_ptr, d->bnd_ptr + g.nBnd + 1);
+        g.bndBranch.assign(d->bnd_branch, d->bnd_branch + nm);
+        g.bndDir.assign(d->bnd_dir, d->bnd_dir + nm);
+        g.bndLimit.assign(d->bnd_limit_mw, d->bnd_limit_mw + g.nBnd);
+        for (int e = 0; e < nm; e++) {
+            if (g.bndBranch[e] < 0 || g.bndBranch[e] >= nb) return "a boundary names a branch out of range";
+            if (g.bndDir[e] != 1 && g.bndDir[e] != -1) return "a boundary branch direction must be 1 or -1";
+        }
+        for (int q = 0; q < g.nBnd; q++)
+            if (!std::isfinite(g.bndLimit[q]) || g.bndLimit[q] < 0)
+                return "a boundary transfer limit must be a finite non-negative MW value (0 = no limit set)";
     }
     return "";
 }

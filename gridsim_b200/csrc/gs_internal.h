@@ -19,8 +19,12 @@ struct HostGrid {
     std::vector<double> pg, qg, vg, qmin, qmax;
     std::vector<uint8_t> genOn;
     std::vector<int> brF, brT;
-    std::vector<double> r, x, b, tap, shift, rateA;
+    std::vector<double> r, x, b, tap, shift, rateA, rateB, rateC;
     std::vector<uint8_t> brOn;
+    // boundaries: members bndPtr[q] .. bndPtr[q+1]-1 (branch position, direction), limit in MW (0 = none)
+    int nBnd = 0;
+    std::vector<int> bndPtr, bndBranch, bndDir;
+    std::vector<double> bndLimit;
 };
 
 // Entry kinds of the fused factor + forward-substitution schedule.

@@ -66,8 +66,15 @@ struct DevGrid {
     const double* brStamp;
     const int* brF;
     const int* brT;
-    const double* rateA;
+    const double* rateA;  // ratings / base (0 = unrated or not given)
+    const double* rateB;
+    const double* rateC;
     const uint8_t* brOn;
+    int nBnd;             // boundaries: members bndPtr[q] .. bndPtr[q+1]-1 (branch, direction), limit MW
+    const int* bndPtr;
+    const int* bndBranch;
+    const int* bndDir;
+    const double* bndLimit;
     const double* pgen;   // generation per bus (pu)
     const double* qgen;
     const double* pload;  // load per bus (pu)

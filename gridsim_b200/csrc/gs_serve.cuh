@@ -427,7 +427,7 @@ int gs_serve_add_grid(gs_server* S, gs_grid* G, int32_t* index) {
         GS_CUDA(cudaMemcpy(L->baseVm.p, G->ws.startVm.p, (size_t)s.n * 8, cudaMemcpyDeviceToDevice));
         GS_CUDA(cudaMemcpy(L->baseVa.p, G->ws.startVa.p, (size_t)s.n * 8, cudaMemcpyDeviceToDevice));
     }
-    int rc = EnsureWs(ctx, s, L->ws, C, o.precision, false, false);
+    int rc = EnsureWs(ctx, s, L->ws, C, o.precision, 0, false);
     if (rc) return rc;
     GS_CUDA(cudaMemset(L->ws.active.p, 0, (size_t)C * sizeof(int)));
     GS_CUDA(L->admitD.alloc((size_t)2 * C * sizeof(int)));

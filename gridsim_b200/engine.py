@@ -41,6 +41,7 @@ class PowerFlowOptions:
     warm_start_from_base: bool = False
     batch_width: int = 0
     phase_timing: bool = False
+    post_fault_rating: str = "A"     # "A", "B" or "C": the rating outage states are judged against (screens)
 
     def to_c(self) -> _abi.PfOpts:
         o = _abi.default_opts()
@@ -55,6 +56,7 @@ class PowerFlowOptions:
         o.warm_start_from_base = int(self.warm_start_from_base)
         o.batch_width = int(self.batch_width)
         o.phase_timing = int(self.phase_timing)
+        o.post_fault_rating = {"A": _abi.RATE_A, "B": _abi.RATE_B, "C": _abi.RATE_C}[self.post_fault_rating.upper()]
         return o
 
 
@@ -63,8 +65,10 @@ STUDY_MAX_ITERATIONS = 100
 
 
 def study_options(precision: str = "fp64") -> "PowerFlowOptions":
-    """ContingencyAnalysis.StudyOptions: the options every contingency study of the reference solves with."""
-    return PowerFlowOptions(max_iterations=STUDY_MAX_ITERATIONS, enforce_q_limits=True, precision=precision)
+    """ContingencyAnalysis.StudyOptions: the options every contingency study of the reference solves with (100
+    iterations, Q limits on, and the reference's default DC-angle retry, ``PowerFlowOptions.cs:121``)."""
+    return PowerFlowOptions(max_iterations=STUDY_MAX_ITERATIONS, enforce_q_limits=True, retry_from_dc_start=True,
+                            precision=precision)
 
 
 @dataclass
@@ -327,6 +331,7 @@ class ContingencyResult:
     netted_against_base: bool = False
     pre_existing_violations: list = field(default_factory=list)
     worsened_pre_existing_violations: list = field(default_factory=list)
+    islanded: bool = False  # not converged, and the outage split the network (:1661-1665)
 
     @property
     def secure(self) -> bool:
@@ -334,14 +339,21 @@ class ContingencyResult:
 
 
 def _branch_label(model: GridModel, k: int) -> str:
-    """ContingencyAnalysis.Label (:1832-1833): the name (none here: "from-to" bus ids) plus " (tx)"."""
-    lab = f"{int(model.bus_id[model.br_from[k]])}-{int(model.bus_id[model.br_to[k]])}"
+    """ContingencyAnalysis.Label (:1832-1833): the name (else "from-to" bus ids) plus " (tx)"."""
+    nm = model.br_name[k] if model.br_name is not None else ""
+    lab = nm if nm else f"{int(model.bus_id[model.br_from[k]])}-{int(model.bus_id[model.br_to[k]])}"
     return lab + (" (tx)" if model.is_transformer[k] else "")
 
 
 def _violation_texts(model: GridModel, details: Sequence[ContingencyViolation]) -> list:
-    """ContingencyAnalysis.ViolationTexts (:1050-1067)."""
-    texts = [f"branch {d.name} {d.value:.0f}%" for d in details if d.kind == _abi.VIOL_BRANCH_OVERLOAD]
+    """ContingencyAnalysis.ViolationTexts (:1050-1067): branch and boundary lines in detail order, then one
+    undervoltage and one overvoltage line."""
+    texts = []
+    for d in details:
+        if d.kind == _abi.VIOL_BRANCH_OVERLOAD:
+            texts.append(f"branch {d.name} {d.value:.0f}%")
+        elif d.kind == _abi.VIOL_BOUNDARY_OVERLOAD:
+            texts.append(f"boundary {d.name} {d.value:.0f}%")
     under = [d.value for d in details if d.kind == _abi.VIOL_UNDERVOLTAGE]
     over = [d.value for d in details if d.kind == _abi.VIOL_OVERVOLTAGE]
     if under:
@@ -352,7 +364,8 @@ def _violation_texts(model: GridModel, details: Sequence[ContingencyViolation]) 
 
 
 def _branch_name(model: GridModel, k: int) -> str:
-    return f"{int(model.bus_id[model.br_from[k]])}-{int(model.bus_id[model.br_to[k]])}"
+    """The name a branch violation carries: the branch's name, else "from-to" (:1168-1172)."""
+    return model.branch_label(k)
 
 
 class ContingencyAnalysis:
@@ -376,6 +389,7 @@ class ContingencyAnalysis:
         while True:
             out = dict(status=np.zeros(k, np.int32), iterations=np.zeros(k, np.int32), max_mismatch=np.zeros(k),
                        min_vm=np.zeros(k), max_vm=np.zeros(k), max_loading_pct=np.zeros(k),
+                       worst_boundary_pct=np.zeros(k), islanded=np.zeros(k, np.uint8),
                        viol_ptr=np.zeros(k + 1, np.int32), viol_kind=np.zeros(cap, np.int32),
                        viol_element=np.zeros(cap, np.int32), viol_value=np.zeros(cap))
             if keep_states:
@@ -406,24 +420,43 @@ class ContingencyAnalysis:
                    level_factor_ms=r.level_factor_ms, level_factor_bytes=r.level_factor_bytes, tail_ms=r.tail_ms)
         return out
 
+    @staticmethod
+    def outage_topology(model: GridModel, branch_indices: Sequence[int], tolerance: float = 1e-8):
+        """Per outage (-1 = the intact grid): (splits, unsolvable) — ContingencyAnalysis.Splits (:1665) and whether
+        ProvablyUnsolvablePart (:1750-1830) rejects the grid without the branch. Host only (no device needed); the
+        screen runs the same pass before it solves."""
+        lib = _abi.load_library()
+        idx = np.ascontiguousarray(branch_indices, dtype=np.int32)
+        sp = np.zeros(idx.shape[0], np.uint8)
+        un = np.zeros(idx.shape[0], np.uint8)
+        d = model.desc()
+        rc = lib.gs_outage_topology(ctypes.byref(d), float(tolerance), idx.shape[0], _p(idx), _p(sp), _p(un))
+        if rc != _abi.GS_OK:
+            raise EngineError(f"gs_outage_topology: {_abi.load_library().gs_status_str(rc).decode()}")
+        return sp.astype(bool), un.astype(bool)
+
     @classmethod
     def _results(cls, model: GridModel, idx: Sequence[int], raw: dict) -> list:
         res = []
         for j, k in enumerate(idx):
             st = int(raw["status"][j])
             label = _branch_label(model, int(k)) if k >= 0 else cls.BASE_CASE_LABEL
-            if st != _abi.PF_CONVERGED:  # NonConverged (:1661-1662); islanding is not screened here
-                res.append(ContingencyResult(label, False, 0.0, 0.0, 0.0, 0.0, ["no solution"], [], st,
-                                             int(raw["iterations"][j]), float(raw["max_mismatch"][j])))
+            if st != _abi.PF_CONVERGED:  # NonConverged (:1661-1662)
+                isl = bool(raw["islanded"][j])
+                res.append(ContingencyResult(label, False, 0.0, 0.0, 0.0, 0.0, ["islanded" if isl else "no solution"],
+                                             [], st, int(raw["iterations"][j]), float(raw["max_mismatch"][j]),
+                                             islanded=isl))
                 continue
             a, b = raw["viol_ptr"][j], raw["viol_ptr"][j + 1]
             det = []
             for q in range(a, b):
                 kind = int(raw["viol_kind"][q])
                 el = int(raw["viol_element"][q])
-                det.append(ContingencyViolation(kind, el, float(raw["viol_value"][q]),
-                                                _branch_name(model, el) if kind == _abi.VIOL_BRANCH_OVERLOAD else ""))
-            res.append(ContingencyResult(label, True, float(raw["max_loading_pct"][j]), 0.0, float(raw["min_vm"][j]),
+                name = (_branch_name(model, el) if kind == _abi.VIOL_BRANCH_OVERLOAD
+                        else model.boundaries[el][0] if kind == _abi.VIOL_BOUNDARY_OVERLOAD else "")
+                det.append(ContingencyViolation(kind, el, float(raw["viol_value"][q]), name))
+            res.append(ContingencyResult(label, True, float(raw["max_loading_pct"][j]),
+                                         float(raw["worst_boundary_pct"][j]), float(raw["min_vm"][j]),
                                          float(raw["max_vm"][j]), _violation_texts(model, det), det, st,
                                          int(raw["iterations"][j]), float(raw["max_mismatch"][j])))
         return res

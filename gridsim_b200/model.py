@@ -13,7 +13,7 @@ Loaders:
   as PQ, VMAX/VMIN become the bus's own limits, TAP 0 means a line (ratio 1).
 * :func:`load_case_dir` / :func:`save_case_dir` — GridSim's v1 JSON case directory
   (``IO/Json/JsonGridLoader.cs:55-255``): ``system.json``, ``buses.json``, ``generation.json``,
-  ``demand.json``, ``transmission.json``. Only the keys this path needs are read; ``"dispatch": false``
+  ``demand.json``, ``transmission.json``, ``transformer.json``, ``boundaries.json``. Only the keys this path needs are read; ``"dispatch": false``
   keeps the written generator outputs (``:254``), which is what every case written here uses.
 """
 from __future__ import annotations
@@ -24,6 +24,7 @@ import math
 import os
 import re
 from dataclasses import dataclass, field
+from typing import List, Optional, Tuple
 
 import numpy as np
 
@@ -65,6 +66,11 @@ class GridModel:
     rate_a: np.ndarray
     br_in_service: np.ndarray
     is_transformer: np.ndarray
+    rate_b: Optional[np.ndarray] = None  # short-term / emergency MVA (0 = not given); None = all 0
+    rate_c: Optional[np.ndarray] = None
+    br_name: Optional[List[str]] = None  # branch names ("" = unnamed); None = every branch unnamed
+    # transmission boundaries (Boundary, Model/Model.cs:516-560): (name, limit MW, [(branch name, direction)])
+    boundaries: List[Tuple[str, float, List[Tuple[str, int]]]] = field(default_factory=list)
     meta: dict = field(default_factory=dict)
     _keep: list = field(default_factory=list, repr=False)
 
@@ -81,9 +87,42 @@ class GridModel:
         return int(self.gen_bus.shape[0])
 
     def copy(self) -> "GridModel":
-        kw = {k: (v.copy() if isinstance(v, (np.ndarray, dict)) else v) for k, v in self.__dict__.items()
+        kw = {k: (v.copy() if isinstance(v, (np.ndarray, dict, list)) else v) for k, v in self.__dict__.items()
               if k != "_keep"}
         return GridModel(**kw)
+
+    def branch_label(self, k: int) -> str:
+        """A branch's name, or its end buses "from-to" when it has none (ContingencyAnalysis.cs:1168-1172)."""
+        nm = self.br_name[k] if self.br_name is not None else ""
+        return nm if nm and nm.strip() else f"{int(self.bus_id[self.br_from[k]])}-{int(self.bus_id[self.br_to[k]])}"
+
+    def boundary_members(self):
+        """Boundary members resolved to branch positions: (ptr, branch, direction, limit MW), CSR. Every member name
+        must name exactly one branch, and every direction must be 1 or -1 (Boundary.BranchNameProblems,
+        Model/Model.cs:535-551; JsonGridLoader.cs:219-223); otherwise ValueError lists the problems."""
+        names = self.br_name if self.br_name is not None else [""] * self.n_branch
+        where = {}
+        for k, nm in enumerate(names):
+            if nm:
+                where.setdefault(nm, []).append(k)
+        ptr, br, dr, lim, bad = [0], [], [], [], []
+        for name, limit, members in self.boundaries:
+            for bn, d in members:
+                ks = where.get(bn, [])
+                if len(ks) != 1:
+                    bad.append(f"boundary '{name}' names branch '{bn}', which "
+                               + ("matches no branch of the case" if not ks else f"{len(ks)} branches share"))
+                    continue
+                if d not in (1, -1):
+                    bad.append(f"boundary '{name}': branch '{bn}' has direction {d}; it must be 1 or -1")
+                    continue
+                br.append(ks[0])
+                dr.append(int(d))
+            ptr.append(len(br))
+            lim.append(float(limit))
+        if bad:
+            raise ValueError("; ".join(bad[:20]))
+        return (np.array(ptr, np.int32), np.array(br, np.int32), np.array(dr, np.int32), np.array(lim, np.float64))
 
     def with_voltages(self, vm: np.ndarray, va_deg: np.ndarray) -> "GridModel":
         """Warm start: every bus starts at the given state (GridScenario.WithSolvedVoltages,
@@ -124,6 +163,15 @@ class GridModel:
         d.tap, d.shift_deg = arr(self.tap, np.float64), arr(self.shift_deg, np.float64)
         d.rate_a = arr(self.rate_a, np.float64)
         d.br_in_service = arr(self.br_in_service, np.uint8)
+        if self.rate_b is not None:
+            d.rate_b = arr(self.rate_b, np.float64)
+        if self.rate_c is not None:
+            d.rate_c = arr(self.rate_c, np.float64)
+        if self.boundaries:
+            ptr, br, dr, lim = self.boundary_members()
+            d.n_boundary = len(self.boundaries)
+            d.bnd_ptr, d.bnd_branch = arr(ptr, np.int32), arr(br, np.int32)
+            d.bnd_dir, d.bnd_limit_mw = arr(dr, np.int32), arr(lim, np.float64)
         return d
 
     # ---- JSON round trip of the whole model (golden fixtures) -------------------------------------
@@ -132,6 +180,10 @@ class GridModel:
         for k, v in self.__dict__.items():
             if isinstance(v, np.ndarray):
                 out[k] = [None if (isinstance(t, float) and math.isnan(t)) else t for t in v.tolist()]
+        if self.br_name is not None:
+            out["br_name"] = list(self.br_name)
+        if self.boundaries:
+            out["boundaries"] = [[nm, lim, [list(x) for x in mem]] for nm, lim, mem in self.boundaries]
         return out
 
     @staticmethod
@@ -146,7 +198,10 @@ class GridModel:
             base_kv=f64("base_kv"), gen_bus=i32("gen_bus"), pg=f64("pg"), qg=f64("qg"), vg=f64("vg"),
             qmin=f64("qmin"), qmax=f64("qmax"), gen_in_service=u8("gen_in_service"), br_from=i32("br_from"),
             br_to=i32("br_to"), r=f64("r"), x=f64("x"), b=f64("b"), tap=f64("tap"), shift_deg=f64("shift_deg"),
-            rate_a=f64("rate_a"), br_in_service=u8("br_in_service"), is_transformer=u8("is_transformer"))
+            rate_a=f64("rate_a"), br_in_service=u8("br_in_service"), is_transformer=u8("is_transformer"),
+            rate_b=f64("rate_b") if "rate_b" in d else None, rate_c=f64("rate_c") if "rate_c" in d else None,
+            br_name=list(d["br_name"]) if "br_name" in d else None,
+            boundaries=[(nm, float(lim), [(str(b), int(x)) for b, x in mem]) for nm, lim, mem in d.get("boundaries", [])])
 
 
 # =============================================================================================
@@ -206,7 +261,8 @@ def parse_matpower(text: str, name: str = "matpower") -> GridModel:
         br_to=np.array([pos[int(r[1])] for r in brs], np.int32),
         r=g(brs, 2), x=g(brs, 3), b=g(brs, 4), tap=np.where(tap_raw != 0.0, tap_raw, 1.0), shift_deg=g(brs, 9),
         rate_a=g(brs, 5), br_in_service=np.ones(len(brs), np.uint8),
-        is_transformer=(tap_raw != 0.0).astype(np.uint8))
+        is_transformer=(tap_raw != 0.0).astype(np.uint8),
+        rate_b=g(brs, 6), rate_c=g(brs, 7))  # RATE_B / RATE_C (MatpowerParser.cs:384-385)
 
 
 def load_matpower(path: str) -> GridModel:
@@ -250,11 +306,20 @@ def save_case_dir(m: GridModel, path: str) -> None:
                          for i in range(m.n_bus) if m.pd[i] != 0 or m.qd[i] != 0])
     lines = []
     for k in range(m.n_branch):
-        lines.append({"name": f"L{k}", "from": int(m.bus_id[m.br_from[k]]), "to": int(m.bus_id[m.br_to[k]]),
-                      "rPu": float(m.r[k]), "xPu": float(m.x[k]), "bPu": float(m.b[k]),
-                      "ratingMva": float(m.rate_a[k]), "tapRatio": float(m.tap[k]),
-                      "phaseShiftDeg": float(m.shift_deg[k]), "isTransformer": bool(m.is_transformer[k])})
+        ln = {"name": m.br_name[k] if m.br_name is not None and m.br_name[k] else f"L{k}",
+              "from": int(m.bus_id[m.br_from[k]]), "to": int(m.bus_id[m.br_to[k]]),
+              "rPu": float(m.r[k]), "xPu": float(m.x[k]), "bPu": float(m.b[k]),
+              "ratingMva": float(m.rate_a[k]), "tapRatio": float(m.tap[k]),
+              "phaseShiftDeg": float(m.shift_deg[k]), "isTransformer": bool(m.is_transformer[k])}
+        for key, arr in (("ratingBMva", m.rate_b), ("ratingCMva", m.rate_c)):
+            if arr is not None and arr[k] != 0:
+                ln[key] = float(arr[k])
+        lines.append(ln)
     dump("transmission.json", lines)
+    if m.boundaries:
+        dump("boundaries.json", [{"name": nm, "limitMw": lim,
+                                  "branches": [{"branch": b, "direction": d} for b, d in mem]}
+                                 for nm, lim, mem in m.boundaries])
 
 
 def load_case_dir(path: str) -> GridModel:
@@ -270,6 +335,8 @@ def load_case_dir(path: str) -> GridModel:
     gens = read("generation.json", [])
     dem = read("demand.json", [])
     lines = read("transmission.json", [])
+    txs = read("transformer.json", [])
+    bnds = read("boundaries.json", [])
     if not buses:
         raise ValueError("buses.json is empty or missing")
     if sysd.get("dispatch", True):
@@ -295,7 +362,13 @@ def load_case_dir(path: str) -> GridModel:
     f = lambda rows, k, dflt=0.0: np.array([float(r.get(k, dflt)) if r.get(k) is not None else dflt  # noqa: E731
                                            for r in rows], np.float64)
     circ = np.array([int(l.get("circuits", 1)) for l in lines], np.float64)
+    if (circ < 1).any():
+        raise ValueError("a line has circuits below 1")
     cap = f(gens, "capacityMva")
+    # transformers follow the lines as branches (JsonGridLoader.cs:189-196): no charging, ratings per unit
+    ntx = len(txs)
+    cat = lambda a, b: np.concatenate([a, b])  # noqa: E731
+    one = np.ones(ntx)
     return GridModel(
         name=sysd.get("name", os.path.basename(os.path.normpath(path))), base_mva=float(sysd.get("baseMva", 100.0)),
         bus_id=np.array([int(b["id"]) for b in buses], np.int32), bus_type=btype, pd=pd, qd=qd,
@@ -306,9 +379,17 @@ def load_case_dir(path: str) -> GridModel:
         qmin=np.array([g["qMinMvar"] if g.get("qMinMvar") is not None else -c for g, c in zip(gens, cap)], np.float64),
         qmax=np.array([g["qMaxMvar"] if g.get("qMaxMvar") is not None else c for g, c in zip(gens, cap)], np.float64),
         gen_in_service=np.array([1 if g.get("inService", True) else 0 for g in gens], np.uint8),
-        br_from=np.array([pos[int(l["from"])] for l in lines], np.int32),
-        br_to=np.array([pos[int(l["to"])] for l in lines], np.int32),
-        r=f(lines, "rPu") / circ, x=f(lines, "xPu") / circ, b=f(lines, "bPu") * circ, tap=f(lines, "tapRatio", 1.0),
-        shift_deg=f(lines, "phaseShiftDeg"), rate_a=f(lines, "ratingMva") * circ,
-        br_in_service=np.ones(len(lines), np.uint8),
-        is_transformer=np.array([1 if l.get("isTransformer", False) else 0 for l in lines], np.uint8))
+        br_from=np.array([pos[int(l["from"])] for l in lines + txs], np.int32),
+        br_to=np.array([pos[int(l["to"])] for l in lines + txs], np.int32),
+        r=cat(f(lines, "rPu") / circ, f(txs, "rPu")), x=cat(f(lines, "xPu") / circ, f(txs, "xPu")),
+        b=cat(f(lines, "bPu") * circ, np.zeros(ntx)), tap=cat(f(lines, "tapRatio", 1.0), f(txs, "tapRatio", 1.0)),
+        shift_deg=cat(f(lines, "phaseShiftDeg"), f(txs, "phaseShiftDeg")),
+        rate_a=cat(f(lines, "ratingMva") * circ, f(txs, "ratingMva")),
+        br_in_service=np.ones(len(lines) + ntx, np.uint8),
+        is_transformer=np.array([1 if l.get("isTransformer", False) else 0 for l in lines] + [1] * ntx, np.uint8),
+        rate_b=cat(f(lines, "ratingBMva") * circ, f(txs, "ratingBMva") * one),
+        rate_c=cat(f(lines, "ratingCMva") * circ, f(txs, "ratingCMva") * one),
+        br_name=[l.get("name") or "" for l in lines + txs],
+        boundaries=[(b.get("name", ""), float(b.get("limitMw", 0.0)),
+                     [(x.get("branch", ""), int(x.get("direction", 1))) for x in (b.get("branches") or [])])
+                    for b in bnds])

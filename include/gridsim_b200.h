@@ -56,8 +56,16 @@ enum gs_pf_status {
     GS_PF_SINGULAR_PIVOT = 4, /* a static pivot collapsed below its floor: the step could not be taken
                                  (the reference reports this state as MaxIterations, NewtonShell.cs:74-120) */
     GS_PF_TIMEOUT = 5,
-    GS_PF_NOT_RUN = 6
+    GS_PF_NOT_RUN = 6,
+    GS_PF_UNSOLVABLE_PART = 7 /* not solved: the outage leaves a connected part with no reference bus whose
+                                 real-power balance no state can meet, so the solve could only end non-converged
+                                 (ContingencyAnalysis.ProvablyUnsolvablePart, Analysis/ContingencyAnalysis.cs:1750-1830) */
 };
+
+/* Rating an outage state's branch loadings are judged against (PostFaultRating,
+ * src/GridSim.Core/PowerFlow/PowerFlowOptions.cs:162-170): the base case always uses RateA; a branch whose
+ * RateB / RateC is 0 falls back to RateA (ContingencyAnalysis.PostFaultLoadingPercent, :1273-1284). */
+enum gs_post_fault_rating { GS_RATE_A = 0, GS_RATE_B = 1, GS_RATE_C = 2 };
 
 /* Arithmetic of the linear step (Jacobian values, LU, triangular solves). Mismatch, update and
  * convergence test are always FP64. */
@@ -109,6 +117,16 @@ typedef struct gs_grid_desc {
     const double *shift_deg;
     const double *rate_a;           /* MVA, 0 = unrated */
     const uint8_t *br_in_service;   /* NULL = all in service */
+    const double *rate_b, *rate_c;  /* short-term / emergency MVA, 0 = not given; each array may be NULL */
+    /* transmission boundaries (Boundary, Model/Model.cs:516-560), CSR: members bnd_ptr[q] .. bnd_ptr[q+1]-1 of
+       boundary q are branch positions (the one branch each member's name resolves to) with direction +1 / -1;
+       limit 0 = no limit authored (flow reported, never overloaded) */
+    int32_t n_boundary;
+    int32_t reserved1;
+    const int32_t *bnd_ptr;         /* [n_boundary+1] */
+    const int32_t *bnd_branch;      /* [bnd_ptr[n_boundary]] */
+    const int32_t *bnd_dir;
+    const double *bnd_limit_mw;     /* [n_boundary] */
 } gs_grid_desc;
 
 /* ---- options: PowerFlowOptions (src/GridSim.Core/PowerFlow/PowerFlowOptions.cs:15-158) ---- */
@@ -129,7 +147,8 @@ typedef struct gs_pf_opts {
                                        its solution (GridScenario.WithSolvedVoltages, Simulation/GridScenario.cs:35-52) */
     int32_t batch_width;            /* systems per device batch; 0 = choose from free HBM */
     int32_t phase_timing;           /* 1: time each phase with CUDA events (no graph replay) into the result */
-    int32_t reserved[7];
+    int32_t post_fault_rating;      /* enum gs_post_fault_rating, screens only; default GS_RATE_A */
+    int32_t reserved[6];
 } gs_pf_opts;
 
 /* Fill `o` with the reference defaults (PowerFlowOptions()) plus precision = FP64. */
@@ -189,6 +208,10 @@ typedef struct gs_n1_result {
     double level_factor_ms;
     double level_factor_bytes;
     double tail_ms;            /* iterations on the few-systems path, all phases */
+    /* per outage, each may be NULL */
+    uint8_t *islanded;         /* 1 when the state did not converge and the outage split the network into more
+                                  connected parts than the grid has (ContingencyAnalysis.Splits, :1665-1687) */
+    double *worst_boundary_pct;/* highest boundary loading, 0 when not converged or no boundary is limited */
 } gs_n1_result;
 
 /* ---- context -------------------------------------------------------------------------------- */
@@ -242,9 +265,21 @@ int gs_pf_solve_batch(gs_grid *grid, int32_t count, const double *load_scale, co
 /* ContingencyAnalysis.ScreenBranches / ScreenBranchesParallel / ScreenBranchesBatched: one full
  * Newton solve per outaged branch (indices into the branch arrays; each must be in service; -1 is
  * the intact grid, ScreenBaseCase), then the ScreenStateCore classification
- * (ContingencyAnalysis.cs:1105-1238) on the device. Results are in the order of `branch_idx`. */
+ * (ContingencyAnalysis.cs:1105-1238) on the device. Results are in the order of `branch_idx`.
+ * Before any solve, a topology pass on the host finds the outages that leave a provably unsolvable part
+ * (ScreenStateCore :1118-1127): those are reported GS_PF_UNSOLVABLE_PART and never reach the device.
+ * With opts->post_fault_rating an outage state's loadings use RateB / RateC; limited boundaries add
+ * GS_VIOL_BOUNDARY_OVERLOAD entries (element = boundary position) between the branch and voltage entries. */
 int gs_n1_screen(gs_grid *grid, int32_t n_out, const int32_t *branch_idx, const gs_pf_opts *opts,
                  gs_n1_result *res);
+
+/* The topology verdicts of a set of single-branch outages (host only, no device needed): splits[k] = 1 when
+ * removing branch_idx[k] leaves more connected parts than the grid has (ContingencyAnalysis.Splits, :1665);
+ * unsolvable[k] = 1 when the grid without it has a part that ProvablyUnsolvablePart (:1750-1830) rejects at
+ * `tolerance`. -1 is the intact grid. Bridges and per-side sums come from one depth-first pass, so the cost
+ * is O(buses + branches) plus the buses of each slack-less side. Either output may be NULL. */
+int gs_outage_topology(const gs_grid_desc *desc, double tolerance, int32_t n_out, const int32_t *branch_idx,
+                       uint8_t *splits, uint8_t *unsolvable);
 
 /* ---- uneven multi-grid batch -------------------------------------------------------------------
  * counts[k] independent load flows of grid k (k < n_grids; grids of any sizes, one context) in ONE

@@ -40,6 +40,7 @@ def _load():
                                       ctypes.POINTER(_abi.N1Result)]
         lib.gso_jacobian.argtypes = [ctypes.POINTER(_abi.GridDesc), vp, vp, vp, vp, vp, i32, vp, i32]
         lib.gso_md_order.argtypes = [i32, vp, vp, vp]
+        lib.gso_outage_topology.argtypes = [ctypes.POINTER(_abi.GridDesc), ctypes.c_double, i32, vp, vp, vp]
         lib.gso_sparse_solve.argtypes = [i32, vp, vp, vp, vp, vp]
         _lib = lib
     return _lib
@@ -80,6 +81,7 @@ def screen(model, branch_idx, opts=None, threads: int = 0, keep_states: bool = F
     while True:
         out = dict(status=np.zeros(k, np.int32), iterations=np.zeros(k, np.int32), max_mismatch=np.zeros(k),
                    min_vm=np.zeros(k), max_vm=np.zeros(k), max_loading_pct=np.zeros(k),
+                   worst_boundary_pct=np.zeros(k), islanded=np.zeros(k, np.uint8),
                    viol_ptr=np.zeros(k + 1, np.int32), viol_kind=np.zeros(cap, np.int32),
                    viol_element=np.zeros(cap, np.int32), viol_value=np.zeros(cap))
         if keep_states:
@@ -106,6 +108,20 @@ def screen(model, branch_idx, opts=None, threads: int = 0, keep_states: bool = F
     out["base_status"] = r.base_status
     out["base_iterations"] = r.base_iterations
     return out
+
+
+def outage_topology(model, branch_idx, tolerance=1e-8):
+    """Per outage: (splits, unsolvable) — ContingencyAnalysis.Splits and ProvablyUnsolvablePart of the grid
+    without the branch, computed per reduced model as the reference does."""
+    lib = _load()
+    idx = np.ascontiguousarray(branch_idx, dtype=np.int32)
+    sp = np.zeros(idx.shape[0], np.uint8)
+    un = np.zeros(idx.shape[0], np.uint8)
+    d = model.desc()
+    rc = lib.gso_outage_topology(ctypes.byref(d), tolerance, idx.shape[0], _p(idx), _p(sp), _p(un))
+    if rc != 0:
+        raise RuntimeError(f"oracle topology failed: {rc}")
+    return sp.astype(bool), un.astype(bool)
 
 
 def jacobian(model):

@@ -8,8 +8,6 @@
 // Deliberate deviations (documented in the design notes):
 //   * sin/cos come from libm, not the reference's fdlibm port (Numerics/DetMath.cs:66-71); the parity
 //     target (1e-8) does not need cross-OS bit identity.
-//   * ContingencyAnalysis.ProvablyUnsolvablePart (:1700-1830) is not restated: it only short-cuts states
-//     the Newton solve reports non-converged anyway, with the same result.
 //   * the DC power flow of the DC-angle retry assumes the reference bus of a single-island DC model is the
 //     case's slack (DistributionFactors picks it as the AC island pre-pass does); other cases get no retry.
 #include "../include/gridsim_b200.h"
@@ -40,6 +38,12 @@ struct Br {
     int f, t;
     double r, x, b, tap, shift, rateA;
     bool inService;
+    double rateB, rateC;
+};
+// Boundary (Model/Model.cs:516-560) with its branch names resolved to positions.
+struct Bnd {
+    double limitMw;
+    std::vector<std::pair<int, int>> members;  // (branch position, direction)
 };
 struct Model {
     int n = 0;
@@ -48,6 +52,7 @@ struct Model {
     std::vector<double> pd, qd, gs, bs, vm, vaDeg, vmin, vmax;
     std::vector<Gen> gens;      // in-service units only (GridModel.Generators)
     std::vector<Br> br;         // GridModel.Branches order
+    std::vector<Bnd> bnd;
 };
 
 Model FromDesc(const gs_grid_desc* d) {
@@ -73,7 +78,13 @@ Model FromDesc(const gs_grid_desc* d) {
     }
     for (int k = 0; k < d->n_branch; k++) {
         m.br.push_back({d->br_from[k], d->br_to[k], d->r[k], d->x[k], d->b[k], d->tap[k], d->shift_deg[k],
-                        d->rate_a[k], d->br_in_service ? d->br_in_service[k] != 0 : true});
+                        d->rate_a[k], d->br_in_service ? d->br_in_service[k] != 0 : true,
+                        d->rate_b ? d->rate_b[k] : 0.0, d->rate_c ? d->rate_c[k] : 0.0});
+    }
+    for (int q = 0; q < d->n_boundary; q++) {
+        Bnd b{d->bnd_limit_mw[q], {}};
+        for (int e = d->bnd_ptr[q]; e < d->bnd_ptr[q + 1]; e++) b.members.push_back({d->bnd_branch[e], d->bnd_dir[e]});
+        m.bnd.push_back(b);
     }
     return m;
 }
@@ -1017,19 +1028,43 @@ void LineFlows(const Model& m, int skip, const std::vector<double>& vm, const st
 
 struct Violation { int kind, element; double value; };
 
-// ContingencyAnalysis.ScreenStateCore (:1105-1238), converged branch: thermal (:1156-1180, keyed by the
-// ORIGINAL branch index, threshold 100 %), voltage per-bus (:1196-1223) or the 0.94/1.06 band (:1226-1235,
-// VoltageLimits.cs:28-31). Boundaries do not exist in these grids.
+// ContingencyAnalysis.ScreenStateCore (:1105-1238), converged branch: thermal (:1150-1180, keyed by the
+// ORIGINAL branch index, threshold 100 %; an outage state judged against RateB / RateC when asked, falling back to
+// the RateA loading where that rating is 0, PostFaultLoadingPercent :1273-1284), boundaries
+// (BoundaryAnalysis.EvaluateAfterOutage, Analysis/BoundaryAnalysis.cs:43-68: the signed sum of the members' from-end
+// MW, a limit of 0 = none), then voltage per-bus (:1196-1223) or the 0.94/1.06 band (:1226-1235,
+// VoltageLimits.cs:28-31).
 void Classify(const Model& m, int skip, const std::vector<double>& vm, const std::vector<double>& va, bool perBus,
-              double& maxLoad, double& minVm, double& maxVm, std::vector<Violation>& out) {
-    std::vector<double> loading(m.br.size());
-    LineFlows(m, skip, vm, va, loading.data(), nullptr, nullptr);
+              int postRating, double& maxLoad, double& worstBnd, double& minVm, double& maxVm,
+              std::vector<Violation>& out) {
+    const int nb = (int)m.br.size();
+    std::vector<double> loading(nb), sf(2 * (size_t)nb), st(2 * (size_t)nb);
+    LineFlows(m, skip, vm, va, loading.data(), sf.data(), st.data());
+    const bool postFault = skip >= 0;  // ScreenOutageCore: postFault = indices.Count > 0 (:1096)
     maxLoad = 0;
-    for (int k = 0; k < (int)m.br.size(); k++) {
+    for (int k = 0; k < nb; k++) {
         if (k == skip) continue;  // the reduced model has no such branch
         double l = loading[k];
+        if (postFault && postRating != GS_RATE_A) {
+            const double rating = postRating == GS_RATE_B ? m.br[k].rateB : m.br[k].rateC;
+            if (rating > 0) {
+                const double mva = std::max(std::abs(cplx(sf[2 * k], sf[2 * k + 1])), std::abs(cplx(st[2 * k], st[2 * k + 1])));
+                l = mva / rating * 100.0;
+            }
+        }
         if (l > maxLoad) maxLoad = l;
         if (l > 100.0) out.push_back({GS_VIOL_BRANCH_OVERLOAD, k, l});
+    }
+    worstBnd = 0;
+    for (int q = 0; q < (int)m.bnd.size(); q++) {
+        const Bnd& b = m.bnd[q];
+        double flow = 0;
+        for (const auto& mem : b.members)
+            if (mem.first != skip) flow += mem.second * sf[2 * mem.first];  // an out-of-service branch carries 0
+        const bool limited = b.limitMw > 0;
+        const double l = limited ? std::fabs(flow) / b.limitMw * 100.0 : 0.0;
+        if (l > worstBnd) worstBnd = l;
+        if (limited && std::fabs(flow) > b.limitMw) out.push_back({GS_VIOL_BOUNDARY_OVERLOAD, q, l});
     }
     minVm = INFINITY; maxVm = -INFINITY;
     for (int i = 0; i < m.n; i++) { minVm = std::min(minVm, vm[i]); maxVm = std::max(maxVm, vm[i]); }
@@ -1044,6 +1079,72 @@ void Classify(const Model& m, int skip, const std::vector<double>& vm, const std
         if (vm[i] < lo) out.push_back({GS_VIOL_UNDERVOLTAGE, m.id[i], vm[i]});
         else if (vm[i] > hi) out.push_back({GS_VIOL_OVERVOLTAGE, m.id[i], vm[i]});
     }
+}
+
+// ContingencyAnalysis.ConnectedParts (:1671-1687) of the model without branch `skip`: buses joined by in-service
+// branches (union-find).
+int ConnectedParts(const Model& m, int skip) {
+    std::vector<int> parent(m.n);
+    std::iota(parent.begin(), parent.end(), 0);
+    auto find = [&](int x) { while (parent[x] != x) { parent[x] = parent[parent[x]]; x = parent[x]; } return x; };
+    int parts = m.n;
+    for (int k = 0; k < (int)m.br.size(); k++) {
+        if (k == skip || !m.br[k].inService) continue;
+        int a = find(m.br[k].f), c = find(m.br[k].t);
+        if (a != c) { parent[a] = c; parts--; }
+    }
+    return parts;
+}
+
+// ContingencyAnalysis.ProvablyUnsolvablePart (:1750-1830) of the model without branch `skip`: true when a connected
+// part has no reference bus, no negative R or Gs, and either its demand exceeds its generation by more than
+// count * tol + 1e-6 pu, or it is lossless (every R and Gs zero) and unbalanced by at least that much.
+bool ProvablyUnsolvablePart(const Model& m, int skip, double tol) {
+    if (!(tol > 0.0) || !std::isfinite(tol)) return false;
+    if (!(m.base > 0.0) || !std::isfinite(m.base)) return false;
+    {
+        std::vector<int> ids(m.id);
+        std::sort(ids.begin(), ids.end());
+        if (std::adjacent_find(ids.begin(), ids.end()) != ids.end()) return false;
+    }
+    const int n = m.n;
+    std::vector<int> parent(n);
+    std::iota(parent.begin(), parent.end(), 0);
+    auto find = [&](int x) { while (parent[x] != x) { parent[x] = parent[parent[x]]; x = parent[x]; } return x; };
+    for (int k = 0; k < (int)m.br.size(); k++) {
+        if (k == skip || !m.br[k].inService) continue;
+        int a = find(m.br[k].f), c = find(m.br[k].t);
+        if (a != c) parent[a] = c;
+    }
+    std::vector<double> pgByBus(n, 0.0);
+    for (const Gen& g : m.gens) pgByBus[g.bus] += g.pg;
+    std::vector<int> order, count(n, 0);
+    std::vector<char> hasSlack(n, 0), anyNeg(n, 0), anyLoss(n, 0);
+    std::vector<double> net(n, 0.0);
+    for (int i = 0; i < n; i++) {
+        int r = find(i);
+        if (count[r] == 0) order.push_back(r);
+        count[r]++;
+        if (m.type[i] == 3) hasSlack[r] = 1;
+        if (!std::isfinite(m.gs[i]) || !std::isfinite(m.pd[i]) || !std::isfinite(pgByBus[i])) return false;
+        if (m.gs[i] < 0.0) anyNeg[r] = 1;
+        if (m.gs[i] != 0.0) anyLoss[r] = 1;
+        net[r] += (pgByBus[i] - m.pd[i]) / m.base;
+    }
+    for (int k = 0; k < (int)m.br.size(); k++) {
+        if (k == skip || !m.br[k].inService) continue;
+        int r = find(m.br[k].f);
+        if (!std::isfinite(m.br[k].r)) return false;
+        if (m.br[k].r < 0.0) anyNeg[r] = 1;
+        if (m.br[k].r != 0.0) anyLoss[r] = 1;
+    }
+    for (int r : order) {
+        if (hasSlack[r] || anyNeg[r]) continue;
+        double slack = count[r] * tol + 1e-6;  // UnsolvableMarginPu (:1700-1705)
+        if (net[r] <= -slack) return true;
+        if (!anyLoss[r] && std::fabs(net[r]) >= slack) return true;
+    }
+    return false;
 }
 
 bool OptionsSupported(const gs_pf_opts* o) { return o != nullptr; }
@@ -1144,17 +1245,30 @@ int gso_n1_screen(const gs_grid_desc* d, int32_t nOut, const int32_t* idx, const
     }
     std::vector<SolveOut> outs(nOut);
     std::vector<std::vector<Violation>> viol(nOut);
-    std::vector<double> maxLoad(nOut, 0), minVm(nOut, 0), maxVm(nOut, 0);
+    std::vector<double> maxLoad(nOut, 0), worstBnd(nOut, 0), minVm(nOut, 0), maxVm(nOut, 0);
+    std::vector<uint8_t> islanded(nOut, 0);
+    const int partsBefore = ConnectedParts(m, -1);
     std::atomic<int> cursor{0};
     auto work = [&]() {
         for (;;) {
             int k = cursor.fetch_add(1);
             if (k >= nOut) return;
-            outs[k] = SolveWithRetry(m, idx[k], *opt, vm0.empty() ? nullptr : vm0.data(),
-                                     va0.empty() ? nullptr : va0.data());
+            // ScreenStateCore (:1118-1127): a provably unsolvable state is reported without a solve
+            if (ProvablyUnsolvablePart(m, idx[k], opt->tolerance)) {
+                outs[k].status = GS_PF_UNSOLVABLE_PART;
+                outs[k].iterations = 0;
+                outs[k].maxMis = 0;
+                outs[k].vm.assign(m.n, 0.0);
+                outs[k].va.assign(m.n, 0.0);
+            } else {
+                outs[k] = SolveWithRetry(m, idx[k], *opt, vm0.empty() ? nullptr : vm0.data(),
+                                         va0.empty() ? nullptr : va0.data());
+            }
             if (outs[k].status == GS_PF_CONVERGED)
-                Classify(m, idx[k], outs[k].vm, outs[k].va, opt->per_bus_voltage_limits != 0, maxLoad[k], minVm[k],
-                         maxVm[k], viol[k]);
+                Classify(m, idx[k], outs[k].vm, outs[k].va, opt->per_bus_voltage_limits != 0, opt->post_fault_rating,
+                         maxLoad[k], worstBnd[k], minVm[k], maxVm[k], viol[k]);
+            else  // NonConverged(label, Splits(before, reduced)) (:1661-1665)
+                islanded[k] = ConnectedParts(m, idx[k]) > partsBefore;
         }
     };
     int nt = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
@@ -1176,6 +1290,8 @@ int gso_n1_screen(const gs_grid_desc* d, int32_t nOut, const int32_t* idx, const
         if (res->min_vm) res->min_vm[k] = minVm[k];
         if (res->max_vm) res->max_vm[k] = maxVm[k];
         if (res->max_loading_pct) res->max_loading_pct[k] = maxLoad[k];
+        if (res->worst_boundary_pct) res->worst_boundary_pct[k] = worstBnd[k];
+        if (res->islanded) res->islanded[k] = islanded[k];
         if (res->viol_ptr) res->viol_ptr[k] = w;
         for (const Violation& v : viol[k]) {
             if (fits && res->viol_kind) {
@@ -1192,6 +1308,21 @@ int gso_n1_screen(const gs_grid_desc* d, int32_t nOut, const int32_t* idx, const
     }
     if (res->viol_ptr) res->viol_ptr[nOut] = w;
     return fits ? GS_OK : GS_ERR_CAPACITY;
+}
+
+// The topology verdicts of single-branch outages (the product's gs_outage_topology), the reference's way: per outage,
+// ConnectedParts of the reduced model against the intact one and ProvablyUnsolvablePart of the reduced model.
+int gso_outage_topology(const gs_grid_desc* d, double tol, int32_t nOut, const int32_t* idx, uint8_t* splits,
+                        uint8_t* unsolvable) {
+    if (!d || nOut < 0) return GS_ERR_INVALID_ARG;
+    Model m = FromDesc(d);
+    const int before = ConnectedParts(m, -1);
+    for (int k = 0; k < nOut; k++) {
+        if (idx[k] < -1 || idx[k] >= (int)m.br.size()) return GS_ERR_INVALID_ARG;
+        if (splits) splits[k] = ConnectedParts(m, idx[k]) > before;
+        if (unsolvable) unsolvable[k] = ProvablyUnsolvablePart(m, idx[k], tol);
+    }
+    return GS_OK;
 }
 
 }  // extern "C"

@@ -25,9 +25,11 @@ def golden_model(name):
 
 @pytest.fixture
 def study_opts():
-    """ContingencyAnalysis.StudyOptions (ContingencyAnalysis.cs:263-268): 100 iterations, Q limits on."""
+    """ContingencyAnalysis.StudyOptions (ContingencyAnalysis.cs:263-268): 100 iterations, Q limits on, and the
+    default DC-angle retry (PowerFlowOptions.cs:121)."""
     from gridsim_b200 import _abi
     o = _abi.default_opts()
     o.max_iterations = 100
     o.enforce_q_limits = 1
+    o.retry_from_dc_start = 1
     return o

@@ -8,6 +8,10 @@ tests pin:
 * case9: ``tests/GridSim.Tests/PowerFlowTests.cs:11-15`` (ExpectedVm / ExpectedVaDeg, tolerances :38-46);
 * case14/57/118/300: ``tests/GridSim.Tests/IeeeCasesTests.cs:16-24`` arrays, tolerances :91-95.
 
+It also turns the reference's captured ``gridsim nminus1`` outputs
+(``tests/GridSim.Tests/fixtures/cli-stdout/nminus1-*.txt``: every outage's status, maximum loading, worst boundary
+loading and voltage extremes, after netting against the base case) into ``cli_nminus1.json``.
+
 The fixtures are what the tests read; the tests never read the reference tree.
 """
 import json
@@ -47,5 +51,51 @@ def main(ref_root):
         print(name, m.n_bus, "buses", m.n_branch, "branches", m.n_gen, "gens")
 
 
+def parse_cli_screen(text):
+    """One captured N-1 table: the base-case line, each outage row, and the 'makes ... worse' notes."""
+    lines = text.replace("\r\n", "\n").split("\n")
+    out = {"base": None, "rows": [], "worsened": {}}
+    in_table = False
+    for ln in lines:
+        if ln.startswith("Base case: secure"):
+            out["base"] = []
+        elif ln.startswith("Base case:"):
+            out["base"] = [t.strip() for t in ln.split("any outage:", 1)[1].split(";")]
+        elif ln.startswith("Outage "):
+            in_table = True
+        elif ln.startswith("-----"):
+            if in_table and out["rows"]:
+                in_table = False
+        elif in_table and ln.strip():
+            label, rest = ln[:30].strip(), ln[32:]
+            status, tail = rest[:12].strip(), rest[14:].strip()
+            m = re.match(r"(\d+)%\s+(\d+)%\s+([0-9.]+)\s+([0-9.]+)$", tail)
+            row = {"outage": label, "status": status}
+            if m:
+                row.update(max_load=int(m.group(1)), worst_bnd=int(m.group(2)), vmin=m.group(3), vmax=m.group(4))
+            else:
+                row["text"] = tail
+            out["rows"].append(row)
+        elif ln.startswith("  ") and ": makes base-case violation(s) worse: " in ln:
+            who, what = ln.strip().split(": makes base-case violation(s) worse: ")
+            out["worsened"][who] = [t.strip() for t in what.split(";")]
+    return out
+
+
+def cli_screens(ref_root):
+    fx = os.path.join(ref_root, "tests", "GridSim.Tests", "fixtures", "cli-stdout")
+    doc = {}
+    for name, case, per_bus in (("nminus1-case9", "case9", True), ("nminus1-case9-global-vlimits", "case9", False),
+                                ("nminus1-case14", "case14", True)):
+        d = parse_cli_screen(open(os.path.join(fx, name + ".txt")).read())
+        d.update(case=case, per_bus_voltage_limits=per_bus, source=f"tests/GridSim.Tests/fixtures/cli-stdout/{name}.txt")
+        doc[name] = d
+        print(name, len(d["rows"]), "rows")
+    with open(os.path.join(HERE, "cli_nminus1.json"), "w") as fh:
+        json.dump(doc, fh, indent=1)
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    main(root)
+    cli_screens(root)
