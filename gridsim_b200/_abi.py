@@ -126,6 +126,7 @@ EXPORTS = {
     "gs_pf_solve": (c_i32, [c_vp, ctypes.POINTER(PfOpts), ctypes.POINTER(PfResult)]),
     "gs_pf_solve_batch": (c_i32, [c_vp, c_i32, c_vp, c_vp, ctypes.POINTER(PfOpts), c_vp, c_vp, c_vp, c_vp, c_vp]),
     "gs_n1_screen": (c_i32, [c_vp, c_i32, c_vp, ctypes.POINTER(PfOpts), ctypes.POINTER(N1Result)]),
+    "gs_nk_screen": (c_i32, [c_vp, c_i32, c_i32, c_vp, ctypes.POINTER(PfOpts), ctypes.POINTER(N1Result)]),
     "gs_analyze_host": (c_i32, [ctypes.POINTER(GridDesc), ctypes.POINTER(GridInfo)]),
     "gs_outage_topology": (c_i32, [ctypes.POINTER(GridDesc), c_f64, c_i32, c_vp, c_vp, c_vp]),
     "gs_pf_mismatch_noalloc": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp]),

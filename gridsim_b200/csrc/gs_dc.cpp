@@ -16,7 +16,7 @@
 
 namespace gs {
 
-bool DcAngles(const HostGrid& h, const Symbolic& s, int skip, int slack, const double* loadScale,
+bool DcAngles(const HostGrid& h, const Symbolic& s, const std::vector<int>& skip, int slack, const double* loadScale,
               std::vector<double>& thetaDeg) {
     const int n = h.n;
     std::vector<int> parent(n);
@@ -30,7 +30,7 @@ bool DcAngles(const HostGrid& h, const Symbolic& s, int skip, int slack, const d
     for (int i = 0; i < n; i++) if (i != slack) red[i] = nr++;
     std::vector<std::map<int, double>> rows(nr);
     for (int k = 0; k < h.nbr; k++) {
-        if (!h.brOn[k] || k == skip || h.x[k] == 0.0) continue;
+        if (!h.brOn[k] || h.x[k] == 0.0 || std::find(skip.begin(), skip.end(), k) != skip.end()) continue;
         parent[find(h.brF[k])] = find(h.brT[k]);
         const double b = 1.0 / h.x[k];
         const int f = red[h.brF[k]], t = red[h.brT[k]];

@@ -63,9 +63,6 @@ template <typename T>
 __device__ __forceinline__ void busMismatchJac(const DevGrid& g, const DevBatch& b, int i, int s, int fillJac, double* pOut,
                                                double* qOut, double& localMax, int& bad) {
     const size_t B = (size_t)b.B;
-    const int o = b.outage[s];
-    int c0 = -1, c1 = -1, c2 = -1, c3 = -1;
-    if (o >= 0) { c0 = g.brCell[4 * o]; c1 = g.brCell[4 * o + 1]; c2 = g.brCell[4 * o + 2]; c3 = g.brCell[4 * o + 3]; }
     const double vmi = b.vm[i * B + s], vai = b.va[i * B + s];
     // Q limits: a bus that starts PV keeps an identity Q row while it is PV (its Vm step is 0, its Q mismatch
     // is not an equation); once switched to PQ its Q is held at the limit
@@ -79,13 +76,11 @@ __device__ __forceinline__ void busMismatchJac(const DevGrid& g, const DevBatch&
     double pi = 0.0, qi = 0.0, Gd = 0.0, Bd = 0.0;
     int pd = -1;
     const int p0 = g.yRowPtr[i], p1 = g.yRowPtr[i + 1];
+    CellOverride ovr(g, b.outage[s], p0);
     for (int p = p0; p < p1; p++) {
         const int j = g.yCol[p];
         double G = g.yG[p], Bv = g.yB[p];
-        if (p == c0) { G = g.brRed[8 * o + 0]; Bv = g.brRed[8 * o + 1]; }
-        else if (p == c1) { G = g.brRed[8 * o + 2]; Bv = g.brRed[8 * o + 3]; }
-        else if (p == c2) { G = g.brRed[8 * o + 4]; Bv = g.brRed[8 * o + 5]; }
-        else if (p == c3) { G = g.brRed[8 * o + 6]; Bv = g.brRed[8 * o + 7]; }
+        ovr.at(g, p, G, Bv);
         double sn, cs;
         sincos(vai - b.va[j * B + s], &sn, &cs);
         const double vmj = b.vm[j * B + s];
@@ -595,52 +590,40 @@ __device__ __forceinline__ void busResidual(const DevGrid& g, const DevBatch& b,
         if (kq >= 0) z[kq * B + s] = T(0);
         return;
     }
-    const int o = b.outage[s];
-    int c0 = -1, c1 = -1, c2 = -1, c3 = -1;
-    if (o >= 0) { c0 = g.brCell[4 * o]; c1 = g.brCell[4 * o + 1]; c2 = g.brCell[4 * o + 2]; c3 = g.brCell[4 * o + 3]; }
     const double vmi = b.vm[i * B + s], vai = b.va[i * B + s];
     const int p0 = g.yRowPtr[i], p1 = g.yRowPtr[i + 1];
-    double pi = 0.0, qi = 0.0;
+    // one pass: the injections, and the off-diagonal blocks applied to dx from the same sin/cos; the diagonal
+    // blocks need P, Q and follow the loop
+    CellOverride ovr(g, b.outage[s], p0);
+    double pi = 0.0, qi = 0.0, jp = 0.0, jq = 0.0, Gd = 0.0, Bd = 0.0;
     for (int p = p0; p < p1; p++) {
         const int j = g.yCol[p];
         double G = g.yG[p], Bv = g.yB[p];
-        if (p == c0) { G = g.brRed[8 * o + 0]; Bv = g.brRed[8 * o + 1]; }
-        else if (p == c1) { G = g.brRed[8 * o + 2]; Bv = g.brRed[8 * o + 3]; }
-        else if (p == c2) { G = g.brRed[8 * o + 4]; Bv = g.brRed[8 * o + 5]; }
-        else if (p == c3) { G = g.brRed[8 * o + 6]; Bv = g.brRed[8 * o + 7]; }
+        ovr.at(g, p, G, Bv);
         double sn, cs;
         sincos(vai - b.va[j * B + s], &sn, &cs);
         const double vmj = b.vm[j * B + s];
         pi += vmj * (G * cs + Bv * sn);
         qi += vmj * (G * sn - Bv * cs);
-    }
-    const double P = vmi * pi, Q = vmi * qi;
-    double jp = 0.0, jq = 0.0;
-    for (int p = p0; p < p1; p++) {
-        const int j = g.yCol[p];
-        double G = g.yG[p], Bv = g.yB[p];
-        if (p == c0) { G = g.brRed[8 * o + 0]; Bv = g.brRed[8 * o + 1]; }
-        else if (p == c1) { G = g.brRed[8 * o + 2]; Bv = g.brRed[8 * o + 3]; }
-        else if (p == c2) { G = g.brRed[8 * o + 4]; Bv = g.brRed[8 * o + 5]; }
-        else if (p == c3) { G = g.brRed[8 * o + 6]; Bv = g.brRed[8 * o + 7]; }
-        double H, N, M, L;
-        if (i == j) {
-            H = -Q - Bv * vmi * vmi;
-            N = P / vmi + G * vmi;
-            M = P - G * vmi * vmi;
-            L = Q / vmi - Bv * vmi;
-        } else {
-            double sn, cs;
-            sincos(vai - b.va[j * B + s], &sn, &cs);
-            const double vmj = b.vm[j * B + s];
-            H = vmi * vmj * (G * sn - Bv * cs);
-            N = vmi * (G * cs + Bv * sn);
-            M = -vmi * vmj * (G * cs + Bv * sn);
-            L = vmi * (G * sn - Bv * cs);
-        }
+        if (j == i) { Gd = G; Bd = Bv; continue; }
+        const double H = vmi * vmj * (G * sn - Bv * cs);
+        const double N = vmi * (G * cs + Bv * sn);
+        const double M = -vmi * vmj * (G * cs + Bv * sn);
+        const double L = vmi * (G * sn - Bv * cs);
         const int jP = g.busP[j], jQ = g.busQ[j];
         const double dth = jP >= 0 ? (double)dx[jP * B + s] : 0.0;
         const double dv = jQ >= 0 ? (double)dx[jQ * B + s] : 0.0;
+        jp += H * dth + N * dv;
+        jq += M * dth + L * dv;
+    }
+    {
+        const double P = vmi * pi, Q = vmi * qi;
+        const double H = -Q - Bd * vmi * vmi;
+        const double N = P / vmi + Gd * vmi;
+        const double M = P - Gd * vmi * vmi;
+        const double L = Q / vmi - Bd * vmi;
+        const double dth = kp >= 0 ? (double)dx[kp * B + s] : 0.0;
+        const double dv = kq >= 0 ? (double)dx[kq * B + s] : 0.0;
         jp += H * dth + N * dv;
         jq += M * dth + L * dv;
     }
@@ -1386,7 +1369,7 @@ __global__ void k_classify(DevGrid g, DevBatch b, Classify c) {
         const int o = b.outage[s];
         if (item < g.nbr) {
             const int k = item;
-            if (g.brOn[k] && k != o) {
+            if (g.brOn[k] && !branchOut(g, o, k)) {
                 double sFr, sFi, sTr, sTi;
                 branchPower(g, b, k, s, sFr, sFi, sTr, sTi);
                 const double mva = fmax(hypot(sFr, sFi), hypot(sTr, sTi));
@@ -1408,7 +1391,7 @@ __global__ void k_classify(DevGrid g, DevBatch b, Classify c) {
             double flow = 0.0;
             for (int e = g.bndPtr[q]; e < g.bndPtr[q + 1]; e++) {
                 const int k = g.bndBranch[e];
-                if (!g.brOn[k] || k == o) continue;
+                if (!g.brOn[k] || branchOut(g, o, k)) continue;
                 double sFr, sFi, sTr, sTi;
                 branchPower(g, b, k, s, sFr, sFi, sTr, sTi);
                 flow += g.bndDir[e] * (sFr * g.baseMva);
@@ -1550,6 +1533,8 @@ struct gs_grid {
     gs::Workspace tws;  // compact copy of the few systems still stepping
     std::unique_ptr<gs_grid> qgrid;  // the same grid analysed for Q-limit enforcement (built on first use)
     std::unique_ptr<gs_grid> rgrid;  // a twin with its own workspace for the DC-angle retries (built on first use)
+    gs::OutageSetTable sets;         // multi-branch outages of the current call (view.nSet > 0 while installed)
+    gs::DevBuf setBrBuf, setCellBuf, setRedBuf;
     int split = 0;      // first level run by the persistent kernels
     int tailSplit = 0;  // first level the few-systems path runs as one CTA per system
 };
@@ -2141,12 +2126,47 @@ int RetryGridOf(gs_grid* G, gs_grid** out) {
     return GS_OK;
 }
 
-// The largest angle across an in-service branch (the outaged one excluded), net of its phase shift, in [-180, 180]
-// degrees (NewtonShell.MaxBranchAngleDeg).
-double MaxBranchAngleDeg(const HostGrid& h, int skip, const double* vaRad, size_t stride) {
+// The branches outage id `id` takes out: none (-1), one branch (id < nbr), or the set id - nbr of the installed table.
+std::vector<int> OutageBranches(const gs_grid* G, int id) {
+    if (id < 0) return {};
+    if (id < G->sym.nbr) return {id};
+    std::vector<int> b;
+    const int* p = &G->sets.br[(size_t)(id - G->sym.nbr) * kSetBranches];
+    for (int j = 0; j < kSetBranches; j++)
+        if (p[j] >= 0) b.push_back(p[j]);
+    return b;
+}
+
+// Install a call's outage sets on G: the kernels read them through G->view until UninstallSets.
+int InstallSets(gs_grid* G, const OutageSetTable& t) {
+    gs_ctx* ctx = G->ctx;
+    G->sets = t;
+    G->view.nSet = t.n;
+    if (t.n == 0) return GS_OK;
+    GS_CUDA(G->setBrBuf.alloc(t.br.size() * 4));
+    GS_CUDA(G->setCellBuf.alloc(t.cell.size() * 4));
+    GS_CUDA(G->setRedBuf.alloc(t.red.size() * 8));
+    GS_CUDA(cudaMemcpy(G->setBrBuf.p, t.br.data(), t.br.size() * 4, cudaMemcpyHostToDevice));
+    GS_CUDA(cudaMemcpy(G->setCellBuf.p, t.cell.data(), t.cell.size() * 4, cudaMemcpyHostToDevice));
+    GS_CUDA(cudaMemcpy(G->setRedBuf.p, t.red.data(), t.red.size() * 8, cudaMemcpyHostToDevice));
+    G->view.setBr = G->setBrBuf.as<int>();
+    G->view.setCell = G->setCellBuf.as<int>();
+    G->view.setRed = G->setRedBuf.as<double>();
+    return GS_OK;
+}
+
+void UninstallSets(gs_grid* G) {
+    G->sets = OutageSetTable();
+    G->view.nSet = 0;
+    if (G->rgrid) { G->rgrid->sets = OutageSetTable(); G->rgrid->view.nSet = 0; }
+}
+
+// The largest angle across an in-service branch (the outaged ones excluded), net of its phase shift, in
+// [-180, 180] degrees (NewtonShell.MaxBranchAngleDeg).
+double MaxBranchAngleDeg(const HostGrid& h, const std::vector<int>& skip, const double* vaRad, size_t stride) {
     double mx = 0.0;
     for (int k = 0; k < h.nbr; k++) {
-        if (!h.brOn[k] || k == skip) continue;
+        if (!h.brOn[k] || std::find(skip.begin(), skip.end(), k) != skip.end()) continue;
         const double a = (vaRad[h.brF[k] * stride] - vaRad[h.brT[k] * stride]) * 180.0 / 3.14159265358979323846 - h.shift[k];
         mx = std::max(mx, std::fabs(std::remainder(a, 360.0)));
     }
@@ -2208,7 +2228,7 @@ int RetryStalled(gs_grid* G, int count, const int* outage, const double* loadSca
     for (int k : cand) {
         std::vector<double> th;
         const double* sc = loadScale ? loadScale + (size_t)k * n : nullptr;
-        if (!DcAngles(h, s, outage ? outage[k] : -1, slack, sc, th)) continue;
+        if (!DcAngles(h, s, OutageBranches(G, outage ? outage[k] : -1), slack, sc, th)) continue;
         std::vector<double> va(n);
         for (int i = 0; i < n; i++)
             va[i] = i == slack ? vaBase[slack] : vaBase[slack] + std::remainder(th[i], 360.0) * 3.14159265358979323846 / 180.0;
@@ -2220,6 +2240,7 @@ int RetryStalled(gs_grid* G, int count, const int* outage, const double* loadSca
     gs_grid* R = nullptr;
     int rc = RetryGridOf(G, &R);
     if (rc) return rc;
+    if (G->view.nSet > 0 && (rc = InstallSets(R, G->sets)) != GS_OK) return rc;  // the same outage ids
     const int nc = (int)ok.size();
     const int B = std::max(32, (nc + 31) / 32 * 32);
     rc = EnsureWorkspace(R, B, o.precision, false, loadScale != nullptr);
@@ -2256,7 +2277,8 @@ int RetryStalled(gs_grid* G, int count, const int* outage, const double* loadSca
     GS_CUDA(cudaMemcpy(rva.data(), rw.va.p, rva.size() * 8, cudaMemcpyDeviceToHost));
     std::vector<int2> pairs;
     for (int c = 0; c < nc; c++)
-        if (rst[c] == GS_PF_CONVERGED && MaxBranchAngleDeg(h, okOut[c], rva.data() + c, (size_t)B) <= kMaxRetryBranchAngleDeg)
+        if (rst[c] == GS_PF_CONVERGED &&
+            MaxBranchAngleDeg(h, OutageBranches(G, okOut[c]), rva.data() + c, (size_t)B) <= kMaxRetryBranchAngleDeg)
             pairs.push_back(make_int2(c, ok[c]));
     if (pairs.empty()) return GS_OK;
     DevBuf dp;
@@ -2574,8 +2596,16 @@ int gs_pf_solve_batch(gs_grid* G, int32_t count, const double* loadScale, const 
     return GS_OK;
 }
 
-int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts* opts, gs_n1_result* res) {
-    if (!G || !res || nOut < 0 || (nOut > 0 && !idx)) return GS_ERR_INVALID_ARG;
+}  // extern "C"
+
+namespace gs {
+namespace {
+
+// The screen of a list of outages, each a list of branches taken out together (empty: the intact grid, ScreenBaseCase;
+// one branch: ScreenBranches; several: ScreenOutageCore over several indices, ContingencyAnalysis.cs:1087-1097).
+int ScreenOutageLists(gs_grid* G, int nOut, const std::vector<std::vector<int>>& lists, const gs_pf_opts* opts,
+                      gs_n1_result* res) {
+    if (!G || !res || nOut < 0) return GS_ERR_INVALID_ARG;
     gs_ctx* ctx = G->ctx;
     int rc = CheckOpts(ctx, opts);
     if (rc) return rc;
@@ -2587,16 +2617,42 @@ int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts*
     }
     const Symbolic& s = G->sym;
     const HostGrid& h = G->host;
-    for (int k = 0; k < nOut; k++)  // AN-02: an out-of-service branch is refused (ContingencyAnalysis.cs:290-300)
-        if (idx[k] < -1 || idx[k] >= s.nbr || (idx[k] >= 0 && !h.brOn[idx[k]]))
-            return SetErr(ctx, GS_ERR_INVALID_ARG, "branch " + std::to_string(idx[k]) + " is not an in-service branch");
+    // outage ids: -1, a branch, or nbr + the position of a multi-branch set in this call's table
+    std::vector<int> ids(nOut, -1);
+    OutageSetTable table;
+    for (int k = 0; k < nOut; k++) {
+        const std::vector<int>& b = lists[k];
+        if ((int)b.size() > kSetBranches)
+            return SetErr(ctx, GS_ERR_UNSUPPORTED, "an outage takes at most " + std::to_string(kSetBranches) + " branches");
+        for (size_t j = 0; j < b.size(); j++) {
+            // AN-02: an out-of-service branch is refused (ContingencyAnalysis.cs:290-300)
+            if (b[j] < 0 || b[j] >= s.nbr || !h.brOn[b[j]])
+                return SetErr(ctx, GS_ERR_INVALID_ARG, "branch " + std::to_string(b[j]) + " is not an in-service branch");
+            for (size_t q = 0; q < j; q++)
+                if (b[q] == b[j])
+                    return SetErr(ctx, GS_ERR_INVALID_ARG, "branch " + std::to_string(b[j]) + " appears twice in one outage");
+        }
+        ids[k] = b.empty() ? -1 : b.size() == 1 ? b[0] : s.nbr + AddOutageSet(s, b, table);
+    }
+    const int* idx = ids.data();
     GS_CUDA(cudaSetDevice(ctx->device));
+    if ((rc = InstallSets(G, table)) != GS_OK) return rc;
+    struct Uninstall { gs_grid* g; ~Uninstall() { UninstallSets(g); } } uninstall{G};
     const int n = s.n, nItems = s.nbr + h.nBnd + s.n;
     // the topology pass (ScreenStateCore :1118-1127): provably unsolvable states are reported without a solve,
     // and a state that does not converge says whether the outage split the network (:1661-1665)
     std::vector<uint8_t> splits(nOut), unsolv(nOut);
     {
-        const std::string terr = OutageTopology(h, o.tolerance, nOut, idx, splits.data(), unsolv.data());
+        std::vector<int> single(nOut);
+        for (int k = 0; k < nOut; k++) single[k] = idx[k] < s.nbr ? idx[k] : -1;
+        std::string terr = OutageTopology(h, o.tolerance, nOut, single.data(), splits.data(), unsolv.data());
+        for (int k = 0; k < nOut && terr.empty(); k++) {
+            if (idx[k] < s.nbr) continue;
+            bool sp = false, un = false;
+            terr = OutageSetTopology(h, o.tolerance, lists[k], sp, un);
+            splits[k] = sp;
+            unsolv[k] = un;
+        }
         if (!terr.empty()) return SetErr(ctx, GS_ERR_INVALID_ARG, terr);
     }
     std::vector<int> solvePos;
@@ -2776,6 +2832,35 @@ int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts*
     res->level_factor_bytes = stats.levelFactorBytes;
     res->tail_ms = stats.tailMs;
     return capacityOk ? GS_OK : GS_ERR_CAPACITY;
+}
+
+}  // namespace
+}  // namespace gs
+
+extern "C" {
+
+int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts* opts, gs_n1_result* res) {
+    if (!G || !res || nOut < 0 || (nOut > 0 && !idx)) return GS_ERR_INVALID_ARG;
+    std::vector<std::vector<int>> lists(nOut);
+    for (int k = 0; k < nOut; k++) {
+        if (idx[k] < -1)
+            return SetErr(G->ctx, GS_ERR_INVALID_ARG, "branch " + std::to_string(idx[k]) + " is not an in-service branch");
+        if (idx[k] >= 0) lists[k].push_back(idx[k]);
+    }
+    return ScreenOutageLists(G, nOut, lists, opts, res);
+}
+
+int gs_nk_screen(gs_grid* G, int32_t nOut, int32_t k, const int32_t* sets, const gs_pf_opts* opts, gs_n1_result* res) {
+    if (!G || !res || nOut < 0 || k < 1 || (nOut > 0 && !sets)) return GS_ERR_INVALID_ARG;
+    std::vector<std::vector<int>> lists(nOut);
+    for (int j = 0; j < nOut; j++)
+        for (int q = 0; q < k; q++) {
+            const int b = sets[(size_t)j * k + q];
+            if (b < -1)
+                return SetErr(G->ctx, GS_ERR_INVALID_ARG, "branch " + std::to_string(b) + " is not an in-service branch");
+            if (b >= 0) lists[j].push_back(b);
+        }
+    return ScreenOutageLists(G, nOut, lists, opts, res);
 }
 
 }  // extern "C"

@@ -13,4 +13,7 @@ void FillInfo(const HostGrid& g, const Symbolic& s, gs_grid_info* info);
 // Either output may be null; empty string on success.
 std::string OutageTopology(const HostGrid& h, double tol, int nOut, const int* idx, uint8_t* splits,
                            uint8_t* unsolvable);
+// The same verdicts for one multi-branch outage (every branch in `removed` out at once).
+std::string OutageSetTopology(const HostGrid& h, double tol, const std::vector<int>& removed, bool& splits,
+                              bool& unsolvable);
 }  // namespace gs

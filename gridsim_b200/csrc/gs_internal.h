@@ -43,6 +43,10 @@ struct Symbolic {
     std::vector<int> brCell;      // [4*nbr]
     std::vector<double> brRed;    // [8*nbr]
     std::vector<double> brStamp;  // [8*nbr] yff, ytt, yft, ytf (re, im) for line flows
+    // per Y cell, its stamps in stamping order (owner branch, or -1 for a bus shunt, and the value): what a Y
+    // rebuilt without a set of branches sums, cell by cell
+    std::vector<int> ccPtr, ccOwner;
+    std::vector<double> ccG, ccB;
     // ---- bus specification ----
     std::vector<int> type0, pPos, qPos;
     int m = 0, npv = 0, npq = 0;
@@ -128,10 +132,25 @@ void BuildTopPart(Symbolic& s, int which, size_t elem, size_t budget);
 // Build the symbolic analysis; returns an empty string on success, else the reason.
 std::string Analyze(const HostGrid& g, Symbolic& s, bool qlim = false);
 
-// DC power-flow angles (degrees) of the grid with branch `skip` out (-1 none), referenced at bus `slack`, with the
+// DC power-flow angles (degrees) of the grid with the branches `skip` out, referenced at bus `slack`, with the
 // loads scaled by loadScale[i] (may be null); false unless the DC model is one island (gs_dc.cpp).
-bool DcAngles(const HostGrid& h, const Symbolic& s, int skip, int slack, const double* loadScale,
+bool DcAngles(const HostGrid& h, const Symbolic& s, const std::vector<int>& skip, int slack, const double* loadScale,
               std::vector<double>& thetaDeg);
+
+// Multi-branch outages (ContingencyAnalysis.ScreenOutageCore over several indices, :1087-1097). A set's outage id
+// is nbr + its position in the table; one branch keeps its own index (the N-1 path). Per set: its branches (-1
+// padded), the distinct Y cells they touch in ascending order (an INT_MAX sentinel after the last), and each cell's
+// value summed without every branch of the set, in stamping order.
+constexpr int kSetBranches = 4;
+constexpr int kSetStride = 4 * kSetBranches + 1;
+struct OutageSetTable {
+    int n = 0;
+    std::vector<int> br;      // [n * kSetBranches]
+    std::vector<int> cell;    // [n * kSetStride]
+    std::vector<double> red;  // [n * 2 * kSetStride] (G, B) per cell
+};
+// Append the set of in-service branches `b` (2..kSetBranches distinct indices); returns its position.
+int AddOutageSet(const Symbolic& s, const std::vector<int>& b, OutageSetTable& t);
 
 // Minimum-degree order of a structurally symmetric pattern (pivot step -> index).
 std::vector<int> MinimumDegreeOrder(int n, const std::vector<int>& rowPtr, const std::vector<int>& col);

@@ -70,6 +70,10 @@ struct DevGrid {
     const double* rateB;
     const double* rateC;
     const uint8_t* brOn;
+    int nSet;             // multi-branch outage sets of the current call (OutageSetTable; ids nbr .. nbr+nSet-1)
+    const int* setBr;
+    const int* setCell;
+    const double* setRed;
     int nBnd;             // boundaries: members bndPtr[q] .. bndPtr[q+1]-1 (branch, direction), limit MW
     const int* bndPtr;
     const int* bndBranch;
@@ -162,5 +166,42 @@ struct DevBatch {
 
 // qState bits
 enum : int32_t { kQPending = 1, kQChanged = 2, kQSkipStep = 4, kQFinalPass = 8, kQFinalConverged = 32 };
+
+// The Y cells a system's outage changes, walked in step with a row's cells: one branch (its four cells and their
+// values without it, brCell / brRed) or an outage set (its distinct cells in ascending order and their values without
+// every branch of the set). Construct with the row's first cell; call at() for each cell of the row in order.
+struct CellOverride {
+    int o, c0, c1, c2, c3, ov;
+    const int* sc;
+    const double* sr;
+    __device__ __forceinline__ CellOverride(const DevGrid& g, int outage, int p0)
+        : o(outage), c0(-1), c1(-1), c2(-1), c3(-1), ov(0), sc(nullptr), sr(nullptr) {
+        if (o >= g.nbr) {
+            const int q = o - g.nbr;
+            sc = g.setCell + (size_t)kSetStride * q;
+            sr = g.setRed + (size_t)2 * kSetStride * q;
+            while (sc[ov] < p0) ov++;  // stops at the sentinel
+        } else if (o >= 0) {
+            c0 = g.brCell[4 * o]; c1 = g.brCell[4 * o + 1]; c2 = g.brCell[4 * o + 2]; c3 = g.brCell[4 * o + 3];
+        }
+    }
+    __device__ __forceinline__ void at(const DevGrid& g, int p, double& G, double& Bv) {
+        if (p == c0) { G = g.brRed[8 * o + 0]; Bv = g.brRed[8 * o + 1]; }
+        else if (p == c1) { G = g.brRed[8 * o + 2]; Bv = g.brRed[8 * o + 3]; }
+        else if (p == c2) { G = g.brRed[8 * o + 4]; Bv = g.brRed[8 * o + 5]; }
+        else if (p == c3) { G = g.brRed[8 * o + 6]; Bv = g.brRed[8 * o + 7]; }
+        else if (sc && p == sc[ov]) { G = sr[2 * ov]; Bv = sr[2 * ov + 1]; ov++; }
+    }
+};
+
+// True when branch k is out in a system whose outage id is o.
+__device__ __forceinline__ bool branchOut(const DevGrid& g, int o, int k) {
+    if (o < g.nbr) return o == k;
+    const int* br = g.setBr + (size_t)kSetBranches * (o - g.nbr);
+#pragma unroll
+    for (int j = 0; j < kSetBranches; j++)
+        if (br[j] == k) return true;
+    return false;
+}
 
 }  // namespace gs

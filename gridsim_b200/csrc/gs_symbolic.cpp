@@ -16,6 +16,7 @@
 //     with forward substitution: every L/U entry is its own sparse dot product over the row subtree of
 //     its node, with the index pairs precomputed here.
 #include <algorithm>
+#include <limits>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -151,6 +152,18 @@ std::string Analyze(const HostGrid& g, Symbolic& s, bool qlim) {
         s.yG[p] = gv;
         s.yB[p] = bv;
     }
+    s.ccPtr.assign(s.nnzY + 1, 0);
+    for (int p = 0; p < s.nnzY; p++) s.ccPtr[p + 1] = s.ccPtr[p] + (int)cellContrib[p].size();
+    s.ccOwner.resize(s.ccPtr[s.nnzY]);
+    s.ccG.resize(s.ccPtr[s.nnzY]);
+    s.ccB.resize(s.ccPtr[s.nnzY]);
+    for (int p = 0; p < s.nnzY; p++)
+        for (size_t q = 0; q < cellContrib[p].size(); q++) {
+            const Contribution& c = contrib[cellContrib[p][q]];
+            s.ccOwner[s.ccPtr[p] + q] = c.owner;
+            s.ccG[s.ccPtr[p] + q] = c.gv;
+            s.ccB[s.ccPtr[p] + q] = c.bv;
+        }
     s.brCell.assign(4 * (size_t)g.nbr, -1);
     s.brRed.assign(8 * (size_t)g.nbr, 0.0);
     for (int k = 0; k < g.nbr; k++) {
@@ -554,6 +567,29 @@ void BuildTopPart(Symbolic& s, int which, size_t elem, size_t budget) {
         for (int q = s.pRowPtr[k]; q < s.pRowPtr[k + 1]; q++) t.bRowSm.push_back(t.yIdx[s.pRows[q]]);
         t.bRowPtr.push_back((int32_t)t.bRowSm.size());
     }
+}
+
+int AddOutageSet(const Symbolic& s, const std::vector<int>& b, OutageSetTable& t) {
+    std::vector<int> cells;
+    for (int k : b)
+        for (int q = 0; q < 4; q++) cells.push_back(s.brCell[4 * (size_t)k + q]);
+    std::sort(cells.begin(), cells.end());
+    cells.erase(std::unique(cells.begin(), cells.end()), cells.end());
+    const int q = t.n++;
+    t.br.resize((size_t)t.n * kSetBranches, -1);
+    t.cell.resize((size_t)t.n * kSetStride, std::numeric_limits<int>::max());
+    t.red.resize((size_t)t.n * 2 * kSetStride, 0.0);
+    for (size_t j = 0; j < b.size(); j++) t.br[(size_t)q * kSetBranches + j] = b[j];
+    for (size_t c = 0; c < cells.size(); c++) {
+        const int p = cells[c];
+        double gv = 0.0, bv = 0.0;  // the cell's stamps in stamping order, the set's own left out
+        for (int e = s.ccPtr[p]; e < s.ccPtr[p + 1]; e++)
+            if (std::find(b.begin(), b.end(), s.ccOwner[e]) == b.end()) { gv += s.ccG[e]; bv += s.ccB[e]; }
+        t.cell[(size_t)q * kSetStride + c] = p;
+        t.red[(size_t)q * 2 * kSetStride + 2 * c] = gv;
+        t.red[(size_t)q * 2 * kSetStride + 2 * c + 1] = bv;
+    }
+    return q;
 }
 
 }  // namespace gs

@@ -12,6 +12,7 @@ succeeds but the first solve raises (there is no CPU path).
 from __future__ import annotations
 
 import ctypes
+import itertools
 import math
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
@@ -368,6 +369,15 @@ def _branch_name(model: GridModel, k: int) -> str:
     return model.branch_label(k)
 
 
+@dataclass
+class NkScreenReport:
+    """NkScreenReport (``ContingencyAnalysis.cs:174-186``): the screened combinations worst first, the single
+    outages left out of the pairing because they already fail at N-1, and why nothing was screened (or None)."""
+    results: list
+    excluded_single_outages: list
+    note: Optional[str] = None
+
+
 class ContingencyAnalysis:
     """The N-1 branch screen of ``Analysis/ContingencyAnalysis.cs`` on the B200 engine."""
 
@@ -379,8 +389,22 @@ class ContingencyAnalysis:
     def screen_raw(model: GridModel, branch_indices: Sequence[int], solver: SparseNewtonRaphsonPowerFlow,
                    options: PowerFlowOptions, keep_states: bool = False) -> dict:
         """One ``gs_n1_screen`` call; returns the raw arrays (status, iterations, violation CSR, ...)."""
-        g = solver.grid_for(model)
         idx = np.ascontiguousarray(branch_indices, dtype=np.int32)
+        return ContingencyAnalysis._screen_call(model, idx, None, solver, options, keep_states)
+
+    @staticmethod
+    def screen_sets_raw(model: GridModel, branch_sets, solver: SparseNewtonRaphsonPowerFlow,
+                        options: PowerFlowOptions, keep_states: bool = False) -> dict:
+        """One ``gs_nk_screen`` call: row j of `branch_sets` ([n_out, k], -1 = none) lists the branches outage j
+        takes out together (ScreenOutageCore over several indices, ``ContingencyAnalysis.cs:1087-1097``)."""
+        sets = np.ascontiguousarray(branch_sets, dtype=np.int32)
+        if sets.ndim != 2:
+            raise ValueError("branch_sets must be [n_out, k]")
+        return ContingencyAnalysis._screen_call(model, sets, sets.shape[1], solver, options, keep_states)
+
+    @staticmethod
+    def _screen_call(model, idx, width, solver, options, keep_states):
+        g = solver.grid_for(model)
         k = idx.shape[0]
         n = model.n_bus
         # violation capacity: remembered per grid (a too small buffer makes the engine report the size
@@ -400,12 +424,15 @@ class ContingencyAnalysis:
                 setattr(r, key, _p(v))
             r.viol_capacity = cap
             c = options.to_c()
-            rc = g.ctx.lib.gs_n1_screen(g.handle, k, _p(idx), ctypes.byref(c), ctypes.byref(r))
+            if width is None:
+                rc = g.ctx.lib.gs_n1_screen(g.handle, k, _p(idx), ctypes.byref(c), ctypes.byref(r))
+            else:
+                rc = g.ctx.lib.gs_nk_screen(g.handle, k, width, _p(idx), ctypes.byref(c), ctypes.byref(r))
             if rc == _abi.GS_ERR_CAPACITY:
                 cap = r.viol_count + 64
                 g.viol_per_outage = max(getattr(g, "viol_per_outage", 0), r.viol_count / max(k, 1))
                 continue
-            g.ctx.check(rc, "gs_n1_screen")
+            g.ctx.check(rc, "gs_n1_screen" if width is None else "gs_nk_screen")
             break
         nv = r.viol_count
         for key in ("viol_kind", "viol_element", "viol_value"):
@@ -436,11 +463,14 @@ class ContingencyAnalysis:
         return sp.astype(bool), un.astype(bool)
 
     @classmethod
-    def _results(cls, model: GridModel, idx: Sequence[int], raw: dict) -> list:
+    def _results(cls, model: GridModel, idx, raw: dict) -> list:
+        """ContingencyResult per outage; `idx` holds a branch per outage (-1 = the intact grid) or, for the
+        multi-branch screen, a row of branches (-1 = none) labelled "A + B" (LabelMany, :1836-1837)."""
         res = []
         for j, k in enumerate(idx):
             st = int(raw["status"][j])
-            label = _branch_label(model, int(k)) if k >= 0 else cls.BASE_CASE_LABEL
+            br = [int(x) for x in np.atleast_1d(k) if x >= 0]
+            label = " + ".join(_branch_label(model, b) for b in br) if br else cls.BASE_CASE_LABEL
             if st != _abi.PF_CONVERGED:  # NonConverged (:1661-1662)
                 isl = bool(raw["islanded"][j])
                 res.append(ContingencyResult(label, False, 0.0, 0.0, 0.0, 0.0, ["islanded" if isl else "no solution"],
@@ -483,6 +513,98 @@ class ContingencyAnalysis:
         options = options or PowerFlowOptions(precision=solver.precision)
         raw = cls.screen_raw(model, np.array([-1], np.int32), solver, options)
         return cls._results(model, [-1], raw)[0]
+
+    @classmethod
+    def screen_outage(cls, model: GridModel, indices: Sequence[int],
+                      solver: Optional[SparseNewtonRaphsonPowerFlow] = None,
+                      options: Optional[PowerFlowOptions] = None) -> ContingencyResult:
+        """ScreenOutage (:1087-1097 via ScreenOutageCore): the given branches out together, solved and classified."""
+        solver = solver or SparseNewtonRaphsonPowerFlow()
+        options = options or PowerFlowOptions(precision=solver.precision)
+        row = np.array([list(indices) or [-1]], np.int32)
+        raw = cls.screen_sets_raw(model, row, solver, options)
+        return cls._results(model, row, raw)[0]
+
+    STRESS_VOLTAGE_WEIGHT_PER_PU = 1000.0   # :239
+    DEFAULT_CANDIDATE_COUNT = 20            # :245
+    MAX_COMBINATIONS = 20_000_000           # ANA-18
+
+    @classmethod
+    def stress_score(cls, c: ContingencyResult) -> float:
+        """StressScore (:1077-1084): branch plus boundary loading plus 1000 x the voltage excursion beyond the
+        0.94-1.06 band; a state that did not converge is +inf."""
+        if not c.converged:
+            return math.inf
+        s = c.max_branch_loading_percent + c.worst_boundary_loading_percent
+        s += max(0.0, 0.94 - c.min_vm) * cls.STRESS_VOLTAGE_WEIGHT_PER_PU
+        s += max(0.0, c.max_vm - 1.06) * cls.STRESS_VOLTAGE_WEIGHT_PER_PU
+        return s
+
+    @classmethod
+    def screen_n_minus_k_report(cls, model: GridModel, k: int, solver: Optional[SparseNewtonRaphsonPowerFlow] = None,
+                                options: Optional[PowerFlowOptions] = None, candidate_count: int = 20,
+                                exhaustive: bool = False) -> "NkScreenReport":
+        """ScreenNMinusKReport (:378-426): the N-1 screen first (unless exhaustive), the single outages that solve
+        ranked by stress_score (stable, ties in branch order) and the top max(candidate_count, k) kept (RankCandidates
+        :438-451), every k-subset of the candidates in lexicographic order (Combinations :1851-1866) screened on the
+        device in one call, results worst first (stable)."""
+        solver = solver or SparseNewtonRaphsonPowerFlow()
+        options = options or PowerFlowOptions(precision=solver.precision)
+        return cls._nk_report(model, k, lambda idx: cls.screen_raw(model, idx, solver, options),
+                              lambda sets: cls.screen_sets_raw(model, sets, solver, options), candidate_count,
+                              exhaustive)
+
+    @classmethod
+    def _nk_report(cls, model: GridModel, k: int, screen_single, screen_sets, candidate_count: int,
+                   exhaustive: bool) -> "NkScreenReport":
+        """The N-k pipeline over two raw screens (a branch list, and a [n_out, k] set array)."""
+        if k < 1:
+            raise ValueError("contingency depth k must be >= 1")
+        live = model.in_service_branches()
+        n = live.shape[0]
+        if k > n:
+            return NkScreenReport([], [], f"the model has {n} branch(es), fewer than the depth k = {k}, so no "
+                                          f"{k}-outage combination exists; nothing was screened.")
+        if k == 1:
+            return NkScreenReport(cls._results(model, live, screen_single(live)), [])
+        excluded = []
+        if exhaustive:
+            cand = live
+        else:
+            single = cls._results(model, live, screen_single(live))
+            solvable = [i for i, c in enumerate(single) if c.converged]
+            excluded = [c for c in single if not c.converged]
+            take = min(max(candidate_count, k), len(solvable))
+            ranked = sorted(solvable, key=lambda i: -cls.stress_score(single[i]))[:take]
+            cand = live[np.array(ranked, dtype=np.int64)] if ranked else live[:0]
+        count = math.comb(len(cand), k) if len(cand) >= k else 0
+        if count > cls.MAX_COMBINATIONS:
+            raise ValueError(f"N-{k}: {len(cand)} candidate branches give about {count:.4g} outage combinations, "
+                             f"more than the {cls.MAX_COMBINATIONS} one screen takes; screen fewer candidates (a "
+                             f"candidate count) or a smaller k.")
+        note = None
+        if len(cand) < k:
+            note = (f"only {len(cand)} single outage(s) solve ({len(excluded)} do not), fewer than the depth k = {k}, "
+                    f"so no {k}-outage combination could be formed; nothing was screened.")
+            return NkScreenReport([], excluded, note)
+        combos = np.array(list(itertools.combinations([int(c) for c in cand], k)), np.int32).reshape(-1, k)
+        results = cls._results(model, combos, screen_sets(combos))
+        order = sorted(range(len(results)), key=lambda i: -cls.stress_score(results[i]))
+        return NkScreenReport([results[i] for i in order], excluded, note)
+
+    @classmethod
+    def screen_n_minus_k(cls, model: GridModel, k: int, solver: Optional[SparseNewtonRaphsonPowerFlow] = None,
+                         options: Optional[PowerFlowOptions] = None, candidate_count: int = 20,
+                         exhaustive: bool = False) -> list:
+        """ScreenNMinusK (:370-373): the results of screen_n_minus_k_report."""
+        return cls.screen_n_minus_k_report(model, k, solver, options, candidate_count, exhaustive).results
+
+    @classmethod
+    def screen_n_minus_2(cls, model: GridModel, solver: Optional[SparseNewtonRaphsonPowerFlow] = None,
+                         options: Optional[PowerFlowOptions] = None, candidate_count: int = 20,
+                         exhaustive: bool = False) -> list:
+        """ScreenNMinus2 (:356-360)."""
+        return cls.screen_n_minus_k(model, 2, solver, options, candidate_count, exhaustive)
 
     @classmethod
     def net_against_base(cls, model: GridModel, outage: ContingencyResult, base: ContingencyResult,

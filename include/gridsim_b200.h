@@ -273,6 +273,14 @@ int gs_pf_solve_batch(gs_grid *grid, int32_t count, const double *load_scale, co
 int gs_n1_screen(gs_grid *grid, int32_t n_out, const int32_t *branch_idx, const gs_pf_opts *opts,
                  gs_n1_result *res);
 
+/* Multi-branch outages (ScreenOutageCore over several indices, Analysis/ContingencyAnalysis.cs:1087-1097; the
+ * N-k screens ScreenNMinusK :378-426 enumerate them): outage j takes out every branch branch_sets[j*k .. j*k+k-1]
+ * that is not -1 (at most 4, distinct, in service; none = the intact grid). The Y cells each set touches get their
+ * values without every branch of the set, summed in stamping order; everything else (topology pass, Newton solve,
+ * retry, classification, result layout) is gs_n1_screen's, which is the k = 1 case. */
+int gs_nk_screen(gs_grid *grid, int32_t n_out, int32_t k, const int32_t *branch_sets, const gs_pf_opts *opts,
+                 gs_n1_result *res);
+
 /* The topology verdicts of a set of single-branch outages (host only, no device needed): splits[k] = 1 when
  * removing branch_idx[k] leaves more connected parts than the grid has (ContingencyAnalysis.Splits, :1665);
  * unsolvable[k] = 1 when the grid without it has a part that ProvablyUnsolvablePart (:1750-1830) rejects at

@@ -40,6 +40,8 @@ def _load():
                                       ctypes.POINTER(_abi.N1Result)]
         lib.gso_jacobian.argtypes = [ctypes.POINTER(_abi.GridDesc), vp, vp, vp, vp, vp, i32, vp, i32]
         lib.gso_md_order.argtypes = [i32, vp, vp, vp]
+        lib.gso_nk_screen.argtypes = [ctypes.POINTER(_abi.GridDesc), i32, i32, vp, ctypes.POINTER(_abi.PfOpts), i32,
+                                      ctypes.POINTER(_abi.N1Result)]
         lib.gso_outage_topology.argtypes = [ctypes.POINTER(_abi.GridDesc), ctypes.c_double, i32, vp, vp, vp]
         lib.gso_sparse_solve.argtypes = [i32, vp, vp, vp, vp, vp]
         _lib = lib
@@ -72,9 +74,18 @@ def solve(model, opts=None) -> dict:
 
 def screen(model, branch_idx, opts=None, threads: int = 0, keep_states: bool = False) -> dict:
     """ScreenBranchesParallel on `threads` host threads (0 = all)."""
+    return _screen(model, np.ascontiguousarray(branch_idx, dtype=np.int32), None, opts, threads, keep_states)
+
+
+def screen_sets(model, sets, opts=None, threads: int = 0, keep_states: bool = False) -> dict:
+    """ScreenOutageCore over several branches per outage: `sets` is [n_out, k] (-1 = none)."""
+    sets = np.ascontiguousarray(sets, dtype=np.int32)
+    return _screen(model, sets, sets.shape[1], opts, threads, keep_states)
+
+
+def _screen(model, idx, width, opts, threads, keep_states):
     lib = _load()
     o = opts or _abi.default_opts()
-    idx = np.ascontiguousarray(branch_idx, dtype=np.int32)
     k = idx.shape[0]
     n = model.n_bus
     cap = max(64, k * 8)
@@ -92,7 +103,10 @@ def screen(model, branch_idx, opts=None, threads: int = 0, keep_states: bool = F
             setattr(r, key, _p(v))
         r.viol_capacity = cap
         d = model.desc()
-        rc = lib.gso_n1_screen(ctypes.byref(d), k, _p(idx), ctypes.byref(o), threads, ctypes.byref(r))
+        if width is None:
+            rc = lib.gso_n1_screen(ctypes.byref(d), k, _p(idx), ctypes.byref(o), threads, ctypes.byref(r))
+        else:
+            rc = lib.gso_nk_screen(ctypes.byref(d), k, width, _p(idx), ctypes.byref(o), threads, ctypes.byref(r))
         if rc == _abi.GS_ERR_CAPACITY:
             cap = r.viol_count + 16
             continue

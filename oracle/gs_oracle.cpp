@@ -1034,13 +1034,12 @@ struct Violation { int kind, element; double value; };
 // (BoundaryAnalysis.EvaluateAfterOutage, Analysis/BoundaryAnalysis.cs:43-68: the signed sum of the members' from-end
 // MW, a limit of 0 = none), then voltage per-bus (:1196-1223) or the 0.94/1.06 band (:1226-1235,
 // VoltageLimits.cs:28-31).
-void Classify(const Model& m, int skip, const std::vector<double>& vm, const std::vector<double>& va, bool perBus,
-              int postRating, double& maxLoad, double& worstBnd, double& minVm, double& maxVm,
+void Classify(const Model& m, int skip, bool postFault, const std::vector<double>& vm, const std::vector<double>& va,
+              bool perBus, int postRating, double& maxLoad, double& worstBnd, double& minVm, double& maxVm,
               std::vector<Violation>& out) {
     const int nb = (int)m.br.size();
     std::vector<double> loading(nb), sf(2 * (size_t)nb), st(2 * (size_t)nb);
     LineFlows(m, skip, vm, va, loading.data(), sf.data(), st.data());
-    const bool postFault = skip >= 0;  // ScreenOutageCore: postFault = indices.Count > 0 (:1096)
     maxLoad = 0;
     for (int k = 0; k < nb; k++) {
         if (k == skip) continue;  // the reduced model has no such branch
@@ -1223,16 +1222,18 @@ int gso_sparse_solve(int32_t n, const int32_t* rowPtr, const int32_t* colIdx, co
     return GS_OK;
 }
 
-// ScreenBranchesParallel (ContingencyAnalysis.cs:323-344): one outage per task on `threads` host threads
-// (0 = all). Output layout is gs_n1_result's. With warm_start_from_base the intact grid is solved first
-// and its state starts every outage (GridScenario.WithSolvedVoltages).
-int gso_n1_screen(const gs_grid_desc* d, int32_t nOut, const int32_t* idx, const gs_pf_opts* opt, int32_t threads,
-                  gs_n1_result* res) {
-    if (!d || !res || !OptionsSupported(opt) || nOut < 0) return GS_ERR_INVALID_ARG;
-    Model m = FromDesc(d);
-    for (int k = 0; k < nOut; k++)  // -1 is the intact grid (ScreenBaseCase)
-        if (idx[k] < -1 || idx[k] >= (int)m.br.size() || (idx[k] >= 0 && !m.br[idx[k]].inService))
-            return GS_ERR_INVALID_ARG;
+}  // extern "C"
+
+namespace {
+
+// The screen of outages given as lists of branches taken out together (ScreenOutageCore, :1087-1097): one branch is
+// the N-1 path (the branch skipped in the Y build), several are taken out of a copy of the model.
+int ScreenLists(const Model& m, const std::vector<std::vector<int>>& lists, const gs_pf_opts* opt, int threads,
+                gs_n1_result* res) {
+    const int nOut = (int)lists.size();
+    for (const auto& l : lists)
+        for (int k : l)
+            if (k < 0 || k >= (int)m.br.size() || !m.br[k].inService) return GS_ERR_INVALID_ARG;
     std::vector<double> vm0, va0;
     res->base_status = GS_PF_NOT_RUN;
     res->base_iterations = 0;
@@ -1253,22 +1254,31 @@ int gso_n1_screen(const gs_grid_desc* d, int32_t nOut, const int32_t* idx, const
         for (;;) {
             int k = cursor.fetch_add(1);
             if (k >= nOut) return;
+            const std::vector<int>& l = lists[k];
+            Model reduced;
+            const Model* mk = &m;
+            int skip = l.size() == 1 ? l[0] : -1;
+            if (l.size() > 1) {
+                reduced = m;
+                for (int b : l) reduced.br[b].inService = false;
+                mk = &reduced;
+            }
             // ScreenStateCore (:1118-1127): a provably unsolvable state is reported without a solve
-            if (ProvablyUnsolvablePart(m, idx[k], opt->tolerance)) {
+            if (ProvablyUnsolvablePart(*mk, skip, opt->tolerance)) {
                 outs[k].status = GS_PF_UNSOLVABLE_PART;
                 outs[k].iterations = 0;
                 outs[k].maxMis = 0;
                 outs[k].vm.assign(m.n, 0.0);
                 outs[k].va.assign(m.n, 0.0);
             } else {
-                outs[k] = SolveWithRetry(m, idx[k], *opt, vm0.empty() ? nullptr : vm0.data(),
+                outs[k] = SolveWithRetry(*mk, skip, *opt, vm0.empty() ? nullptr : vm0.data(),
                                          va0.empty() ? nullptr : va0.data());
             }
             if (outs[k].status == GS_PF_CONVERGED)
-                Classify(m, idx[k], outs[k].vm, outs[k].va, opt->per_bus_voltage_limits != 0, opt->post_fault_rating,
-                         maxLoad[k], worstBnd[k], minVm[k], maxVm[k], viol[k]);
+                Classify(*mk, skip, !l.empty(), outs[k].vm, outs[k].va, opt->per_bus_voltage_limits != 0,
+                         opt->post_fault_rating, maxLoad[k], worstBnd[k], minVm[k], maxVm[k], viol[k]);
             else  // NonConverged(label, Splits(before, reduced)) (:1661-1665)
-                islanded[k] = ConnectedParts(m, idx[k]) > partsBefore;
+                islanded[k] = ConnectedParts(*mk, skip) > partsBefore;
         }
     };
     int nt = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
@@ -1308,6 +1318,41 @@ int gso_n1_screen(const gs_grid_desc* d, int32_t nOut, const int32_t* idx, const
     }
     if (res->viol_ptr) res->viol_ptr[nOut] = w;
     return fits ? GS_OK : GS_ERR_CAPACITY;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ScreenBranchesParallel (ContingencyAnalysis.cs:323-344): one outage per task on `threads` host threads
+// (0 = all). Output layout is gs_n1_result's; -1 is the intact grid (ScreenBaseCase). With warm_start_from_base the
+// intact grid is solved first and its state starts every outage (GridScenario.WithSolvedVoltages).
+int gso_n1_screen(const gs_grid_desc* d, int32_t nOut, const int32_t* idx, const gs_pf_opts* opt, int32_t threads,
+                  gs_n1_result* res) {
+    if (!d || !res || !OptionsSupported(opt) || nOut < 0) return GS_ERR_INVALID_ARG;
+    Model m = FromDesc(d);
+    std::vector<std::vector<int>> lists(nOut);
+    for (int k = 0; k < nOut; k++) {
+        if (idx[k] < -1) return GS_ERR_INVALID_ARG;
+        if (idx[k] >= 0) lists[k].push_back(idx[k]);
+    }
+    return ScreenLists(m, lists, opt, threads, res);
+}
+
+// ScreenOutageCore over several indices per outage (the N-k screens' unit of work): outage j takes out every branch
+// sets[j*k .. j*k+k-1] that is not -1.
+int gso_nk_screen(const gs_grid_desc* d, int32_t nOut, int32_t k, const int32_t* sets, const gs_pf_opts* opt,
+                  int32_t threads, gs_n1_result* res) {
+    if (!d || !res || !OptionsSupported(opt) || nOut < 0 || k < 1) return GS_ERR_INVALID_ARG;
+    Model m = FromDesc(d);
+    std::vector<std::vector<int>> lists(nOut);
+    for (int j = 0; j < nOut; j++)
+        for (int q = 0; q < k; q++) {
+            const int b = sets[(size_t)j * k + q];
+            if (b < -1) return GS_ERR_INVALID_ARG;
+            if (b >= 0) lists[j].push_back(b);
+        }
+    return ScreenLists(m, lists, opt, threads, res);
 }
 
 // The topology verdicts of single-branch outages (the product's gs_outage_topology), the reference's way: per outage,

@@ -10,7 +10,8 @@ tests pin:
 
 It also turns the reference's captured ``gridsim nminus1`` outputs
 (``tests/GridSim.Tests/fixtures/cli-stdout/nminus1-*.txt``: every outage's status, maximum loading, worst boundary
-loading and voltage extremes, after netting against the base case) into ``cli_nminus1.json``.
+loading and voltage extremes, after netting against the base case) and ``gridsim nminus2`` outputs (``nminus2-*.txt``:
+the worst pairs, the count line and the single outages left out of the pairing) into ``cli_nminus1.json``.
 
 The fixtures are what the tests read; the tests never read the reference tree.
 """
@@ -91,6 +92,19 @@ def cli_screens(ref_root):
         d.update(case=case, per_bus_voltage_limits=per_bus, source=f"tests/GridSim.Tests/fixtures/cli-stdout/{name}.txt")
         doc[name] = d
         print(name, len(d["rows"]), "rows")
+    for name, case, per_bus in (("nminus2-case9", "case9", True), ("nminus2-case9-global-vlimits", "case9", False)):
+        text = open(os.path.join(fx, name + ".txt")).read()
+        d = parse_cli_screen(text)
+        m = re.search(r"\(showing worst (\d+) of (\d+)\)", text)
+        d["screened"] = int(m.group(2)) if m else len(d["rows"])
+        m = re.search(r"(\d+) outages screened\s+(\d+) secure\s+(\d+) with violations\s+(\d+) islanded", text)
+        d["counts"] = [int(m.group(i)) for i in range(1, 5)]
+        d["excluded"] = [[ln[:32].strip(), ln[32:].strip()] for ln in text.split("\n")[text.split("\n").index(
+            next(ln for ln in text.split("\n") if "left out of the pairing" in ln)) + 1:] if ln.startswith("  ")]
+        d.update(case=case, per_bus_voltage_limits=per_bus, k=2, candidate_count=20,
+                 source=f"tests/GridSim.Tests/fixtures/cli-stdout/{name}.txt")
+        doc[name] = d
+        print(name, d["screened"], "combinations")
     with open(os.path.join(HERE, "cli_nminus1.json"), "w") as fh:
         json.dump(doc, fh, indent=1)
 
