@@ -22,6 +22,7 @@ GS_ERR_TIMEOUT, GS_ERR_STATE, GS_ERR_UNSUPPORTED, GS_ERR_INTERNAL, GS_ERR_CAPACI
 PF_STATUS_NAMES = ["Converged", "MaxIterations", "NonFinite", "Diverged", "SingularPivot", "Timeout", "NotRun",
                    "UnsolvablePart"]
 RATE_A, RATE_B, RATE_C = 0, 1, 2
+LS_OK, LS_SINGULAR, LS_NON_FINITE_INPUT, LS_MALFORMED = 0, 1, 2, 3
 
 PREC_FP64, PREC_MIXED = 0, 1
 VIOL_BRANCH_OVERLOAD, VIOL_BOUNDARY_OVERLOAD, VIOL_UNDERVOLTAGE, VIOL_OVERVOLTAGE = 0, 1, 2, 3
@@ -129,6 +130,7 @@ EXPORTS = {
     "gs_nk_screen": (c_i32, [c_vp, c_i32, c_i32, c_vp, ctypes.POINTER(PfOpts), ctypes.POINTER(N1Result)]),
     "gs_analyze_host": (c_i32, [ctypes.POINTER(GridDesc), ctypes.POINTER(GridInfo)]),
     "gs_outage_topology": (c_i32, [ctypes.POINTER(GridDesc), c_f64, c_i32, c_vp, c_vp, c_vp]),
+    "gs_sparse_solve_batch": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "gs_pf_mismatch_noalloc": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp]),
     "gs_pf_solve_multi": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(PfOpts), c_vp, c_vp, c_vp, c_vp,
                                   c_vp, ctypes.POINTER(MultiStats)]),

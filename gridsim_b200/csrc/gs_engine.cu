@@ -691,6 +691,21 @@ __device__ __forceinline__ void moveSystem(const DevBatch& from, int sf, const D
     if (from.refine && to.refine) to.refine[st] = from.refine[sf];
 }
 
+// The batched linear solve's inputs into the workspace: A's stored entries into their LU slots, b into the
+// right-hand side in pivot order. vals / rhs are system-major ([cnt][nnz], [cnt][n]); grid (ceil(max(nnz, n) / 8),
+// B / 32), block (32, 8).
+__global__ void k_load_matrix(DevBatch b, int cnt, int nnz, int n, const int* __restrict__ aSlot,
+                              const int* __restrict__ pinv, const double* __restrict__ vals,
+                              const double* __restrict__ rhs) {
+    const int s = blockIdx.y * 32 + threadIdx.x, q = blockIdx.x * 8 + threadIdx.y;
+    if (s >= b.B) return;
+    const size_t B = (size_t)b.B;
+    if (q == 0) { b.active[s] = s < cnt; b.flags[s] = 0; }
+    if (s >= cnt) return;
+    if (q < nnz) ((double*)b.lu)[(size_t)aSlot[q] * B + s] = vals[(size_t)s * nnz + q];
+    if (q < n) ((double*)b.y)[(size_t)pinv[q] * B + s] = rhs[(size_t)s * n + q];
+}
+
 __global__ void k_gather(DevBatch full, DevBatch compact, const int* origin, int n) {
     const int c = blockIdx.y * 32 + threadIdx.x, i = blockIdx.x * 8 + threadIdx.y;
     if (c >= compact.count || i >= n) return;
@@ -1512,6 +1527,8 @@ struct Workspace {
 
 }  // namespace gs
 
+struct MatrixPattern;  // an analysed sparse-matrix pattern of the batched linear solve (kept per context)
+
 struct gs_ctx {
     int device = 0;
     std::string lastError;
@@ -1520,6 +1537,8 @@ struct gs_ctx {
     cudaStream_t partStream[2] = {nullptr, nullptr};  // part 1 of a batch's level sequences (part 0 runs on `stream`)
     int* pinnedCount = nullptr;
     std::map<std::string, int> multiTune;  // the multi-grid batch's CTA shape per set of grids (autotuned)
+    std::vector<std::unique_ptr<MatrixPattern>> patterns;  // most recently used last
+    ~gs_ctx();
 };
 
 struct gs_grid {
@@ -1538,6 +1557,16 @@ struct gs_grid {
     int split = 0;      // first level run by the persistent kernels
     int tailSplit = 0;  // first level the few-systems path runs as one CTA per system
 };
+
+struct MatrixPattern {
+    uint64_t hash = 0;
+    int n = 0;
+    std::vector<int> rowPtr, colIdx, aSlot;
+    std::unique_ptr<gs_grid> grid;  // the pattern's symbolic analysis, schedules and workspace (no Y, no buses)
+    gs::DevBuf dSlot, dPinv;
+};
+
+gs_ctx::~gs_ctx() = default;
 
 namespace gs {
 namespace {
@@ -2861,6 +2890,196 @@ int gs_nk_screen(gs_grid* G, int32_t nOut, int32_t k, const int32_t* sets, const
             if (b >= 0) lists[j].push_back(b);
         }
     return ScreenOutageLists(G, nOut, lists, opts, res);
+}
+
+}  // extern "C"
+
+namespace gs {
+namespace {
+
+constexpr int kMaxPatterns = 8;  // analysed patterns kept per context
+
+uint64_t PatternHash(int n, const int* rp, const int* ci) {  // FNV-1a over the pattern's integers
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](int v) {
+        for (int q = 0; q < 4; q++) { h ^= (uint8_t)((uint32_t)v >> (8 * q)); h *= 1099511628211ull; }
+    };
+    mix(n);
+    for (int i = 0; i <= n; i++) mix(rp[i]);
+    for (int p = 0; p < rp[n]; p++) mix(ci[p]);
+    return h;
+}
+
+// The analysed pattern of a (validated) CSR matrix: from the context's cache, or analysed and uploaded now.
+int PatternOf(gs_ctx* ctx, int n, const int* rp, const int* ci, MatrixPattern** out) {
+    const uint64_t h = PatternHash(n, rp, ci);
+    auto& v = ctx->patterns;
+    for (size_t i = 0; i < v.size(); i++) {
+        const MatrixPattern& P = *v[i];
+        if (P.hash == h && P.n == n && std::equal(P.rowPtr.begin(), P.rowPtr.end(), rp) &&
+            std::equal(P.colIdx.begin(), P.colIdx.end(), ci)) {
+            std::rotate(v.begin() + i, v.begin() + i + 1, v.end());
+            *out = v.back().get();
+            return GS_OK;
+        }
+    }
+    auto P = std::make_unique<MatrixPattern>();
+    P->hash = h;
+    P->n = n;
+    P->rowPtr.assign(rp, rp + n + 1);
+    P->colIdx.assign(ci, ci + rp[n]);
+    P->grid = std::make_unique<gs_grid>();
+    P->grid->ctx = ctx;
+    const std::string err = AnalyzeMatrix(n, rp, ci, P->grid->sym, P->aSlot);
+    if (!err.empty()) return SetErr(ctx, GS_ERR_INVALID_ARG, err);
+    int rc = UploadGrid(P->grid.get());
+    if (rc) return rc;
+    const std::vector<int>& pinv = P->grid->sym.pinv;
+    GS_CUDA(P->dSlot.alloc(std::max<size_t>(4, P->aSlot.size() * 4)));
+    GS_CUDA(P->dPinv.alloc(pinv.size() * 4));
+    if (!P->aSlot.empty()) GS_CUDA(cudaMemcpy(P->dSlot.p, P->aSlot.data(), P->aSlot.size() * 4, cudaMemcpyHostToDevice));
+    GS_CUDA(cudaMemcpy(P->dPinv.p, pinv.data(), pinv.size() * 4, cudaMemcpyHostToDevice));
+    if ((int)v.size() >= kMaxPatterns) v.erase(v.begin());
+    v.push_back(std::move(P));
+    *out = v.back().get();
+    return GS_OK;
+}
+
+// Factorise and solve the `cnt` systems loaded into G's workspace (FP64): the fused factorisation + forward
+// substitution level by level, then the backward substitution; the solution is left in y (pivot order).
+int LinearSolve(gs_grid* G, int cnt) {
+    using T = double;
+    gs_ctx* ctx = G->ctx;
+    const Symbolic& s = G->sym;
+    const DevBatch b = MakeBatch(G, cnt, false);
+    const DevGrid& g = G->view;
+    cudaStream_t st = ctx->stream;
+    const int grp = (cnt + Lay<T>::S - 1) / Lay<T>::S;
+    const dim3 blk4(32, 4), blkP(32, kPersistWarps);
+    auto level = [&](auto kernel, int i0, int i1) {
+        if (i1 > i0) kernel<<<dim3((i1 - i0 + 3) / 4, grp), blk4, 0, st>>>(g, b, (T*)b.y, i0, i1);
+    };
+    const auto& fp = s.factor.levelItemPtr;
+    const auto& bp = s.backward.levelItemPtr;
+    const int split = G->split;
+    for (int l = 0; l < split; l++) {
+        level(k_level<T, kWorkFactor>, fp[2 * l], fp[2 * l + 1]);
+        level(k_level<T, kWorkFactor>, fp[2 * l + 1], fp[2 * l + 2]);
+    }
+    if (split < s.nLevels) {
+        k_persistent<T, kWorkFactor><<<grp, blkP, 0, st>>>(g, b, (T*)b.y, split, s.nLevels);
+        k_persistent<T, kWorkBackward><<<grp, blkP, 0, st>>>(g, b, (T*)b.y, split, s.nLevels);
+    }
+    for (int l = split - 1; l >= 0; l--) level(k_level<T, kWorkBackward>, bp[l], bp[l + 1]);
+    GS_CUDA(cudaGetLastError());
+    return GS_OK;
+}
+
+}  // namespace
+}  // namespace gs
+
+extern "C" {
+
+int gs_sparse_solve_batch(gs_ctx* ctx, int32_t count, const int32_t* n, const int32_t* rowPtr, const int32_t* colIdx,
+                          const double* values, const double* rhs, double* x, int32_t* status) {
+    if (!ctx || count < 0) return GS_ERR_INVALID_ARG;
+    if (count == 0) return GS_OK;
+    if (!n || !rowPtr || !colIdx || !values || !rhs || !x || !status) return GS_ERR_INVALID_ARG;
+    // each system's blocks; a block whose size cannot be read makes the call malformed
+    std::vector<int64_t> rpOff(count), nzOff(count), vOff(count);
+    int64_t a = 0, z = 0, v = 0;
+    for (int q = 0; q < count; q++) {
+        if (n[q] <= 0) return SetErr(ctx, GS_ERR_INVALID_ARG, "system " + std::to_string(q) + " has no rows");
+        rpOff[q] = a; nzOff[q] = z; vOff[q] = v;
+        const int nnz = rowPtr[a + n[q]];
+        if (nnz < 0) return SetErr(ctx, GS_ERR_INVALID_ARG, "system " + std::to_string(q) + " has a negative entry count");
+        a += n[q] + 1; z += nnz; v += n[q];
+    }
+    GS_CUDA(cudaSetDevice(ctx->device));
+    // per-system checks (ArgumentException per system in the reference), then systems grouped by pattern
+    std::map<uint64_t, std::vector<int>> groups;
+    for (int q = 0; q < count; q++) {
+        const int nq = n[q];
+        const int* rp = rowPtr + rpOff[q];
+        const int* ci = colIdx + nzOff[q];
+        bool ok = rp[0] == 0;
+        for (int i = 0; i < nq && ok; i++) ok = rp[i + 1] >= rp[i];
+        for (int i = 0; i < nq && ok; i++) {
+            std::vector<int> row(ci + rp[i], ci + rp[i + 1]);
+            std::sort(row.begin(), row.end());
+            ok = (row.empty() || (row.front() >= 0 && row.back() < nq)) &&
+                 std::adjacent_find(row.begin(), row.end()) == row.end();
+        }
+        if (!ok) { status[q] = GS_LS_MALFORMED; continue; }
+        bool finite = true;
+        for (int p = 0; p < rp[nq] && finite; p++) finite = std::isfinite(values[nzOff[q] + p]);
+        for (int i = 0; i < nq && finite; i++) finite = std::isfinite(rhs[vOff[q] + i]);
+        if (!finite) { status[q] = GS_LS_NON_FINITE_INPUT; continue; }
+        status[q] = GS_LS_OK;
+        groups[PatternHash(nq, rp, ci)].push_back(q);
+    }
+    gs_pf_opts o;
+    gs_pf_opts_default(&o);
+    for (auto& kv : groups) {
+        // one hash may hold several patterns: split the list by exact pattern
+        std::vector<int> todo = kv.second;
+        while (!todo.empty()) {
+            const int q0 = todo.front();
+            const int nq = n[q0];
+            const int* rp0 = rowPtr + rpOff[q0];
+            const int* ci0 = colIdx + nzOff[q0];
+            const int nnz = rp0[nq];
+            std::vector<int> same, rest;
+            for (int q : todo) {
+                const bool eq = n[q] == nq && std::equal(rp0, rp0 + nq + 1, rowPtr + rpOff[q]) &&
+                                std::equal(ci0, ci0 + nnz, colIdx + nzOff[q]);
+                (eq ? same : rest).push_back(q);
+            }
+            todo.swap(rest);
+            MatrixPattern* P = nullptr;
+            int rc = PatternOf(ctx, nq, rp0, ci0, &P);
+            if (rc) return rc;
+            gs_grid* G = P->grid.get();
+            int done = 0;
+            while (done < (int)same.size()) {
+                const int want = (int)same.size() - done;
+                const int B = ChooseB(G, want, o);
+                if ((rc = EnsureWorkspace(G, B, GS_PREC_FP64, false, false)) != GS_OK) return rc;
+                const int cnt = std::min(B, want);
+                std::vector<double> hv((size_t)cnt * nnz), hb((size_t)cnt * nq);
+                for (int c = 0; c < cnt; c++) {
+                    const int q = same[done + c];
+                    std::copy(values + nzOff[q], values + nzOff[q] + nnz, hv.begin() + (size_t)c * nnz);
+                    std::copy(rhs + vOff[q], rhs + vOff[q] + nq, hb.begin() + (size_t)c * nq);
+                }
+                DevBuf dv, db;
+                GS_CUDA(dv.alloc(std::max<size_t>(8, hv.size() * 8)));
+                GS_CUDA(db.alloc(hb.size() * 8));
+                if (!hv.empty()) GS_CUDA(cudaMemcpy(dv.p, hv.data(), hv.size() * 8, cudaMemcpyHostToDevice));
+                GS_CUDA(cudaMemcpy(db.p, hb.data(), hb.size() * 8, cudaMemcpyHostToDevice));
+                const DevBatch b = MakeBatch(G, cnt, false);
+                k_load_matrix<<<dim3((std::max(nnz, nq) + 7) / 8, B / 32), dim3(32, 8), 0, ctx->stream>>>(
+                    b, cnt, nnz, nq, P->dSlot.as<int>(), P->dPinv.as<int>(), dv.as<double>(), db.as<double>());
+                GS_CUDA(cudaGetLastError());
+                if ((rc = LinearSolve(G, cnt)) != GS_OK) return rc;
+                std::vector<double> y((size_t)nq * B);
+                std::vector<int> fl(cnt);
+                GS_CUDA(cudaMemcpyAsync(y.data(), G->ws.y.p, y.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+                GS_CUDA(cudaMemcpyAsync(fl.data(), G->ws.flags.p, cnt * 4, cudaMemcpyDeviceToHost, ctx->stream));
+                GS_CUDA(cudaStreamSynchronize(ctx->stream));
+                const std::vector<int>& pinv = G->sym.pinv;
+                for (int c = 0; c < cnt; c++) {
+                    const int q = same[done + c];
+                    bool good = !(fl[c] & kFlagPivotPerturbed);
+                    for (int i = 0; i < nq && good; i++) good = std::isfinite(y[(size_t)pinv[i] * B + c]);
+                    if (!good) { status[q] = GS_LS_SINGULAR; continue; }
+                    for (int i = 0; i < nq; i++) x[vOff[q] + i] = y[(size_t)pinv[i] * B + c];
+                }
+                done += cnt;
+            }
+        }
+    }
+    return GS_OK;
 }
 
 }  // extern "C"

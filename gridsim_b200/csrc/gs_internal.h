@@ -3,6 +3,7 @@
 
 #include <cstdint>
 #include <string>
+#include <functional>
 #include <vector>
 
 #include "../../include/gridsim_b200.h"
@@ -131,6 +132,17 @@ void BuildTopPart(Symbolic& s, int which, size_t elem, size_t budget);
 
 // Build the symbolic analysis; returns an empty string on success, else the reason.
 std::string Analyze(const HostGrid& g, Symbolic& s, bool qlim = false);
+
+// The static-pivot LU symbolic of s.m and the structurally symmetric pattern s.jRowPtr / s.jCol (diagonal present):
+// minimum-degree order, LU pattern, levels, Crout entries and their index pairs, work schedules, top parts. mapA gets
+// slotOf(k, l) (the LU slot of permuted cell (k, l), -1 outside the pattern) to record the caller's value maps, and
+// marks the slots that receive a value of A (the rest are fill and start from zero).
+std::string FactorSymbolic(Symbolic& s, const std::function<void(const std::function<int64_t(int, int)>&,
+                                                                 std::vector<char>&)>& mapA);
+
+// The symbolic analysis of a general square sparse matrix (CSR, n x n): the pattern of A + A^T with the diagonal,
+// then FactorSymbolic. aSlot[q] is the LU slot of A's q-th stored entry (CSR order). Empty string on success.
+std::string AnalyzeMatrix(int n, const int* rowPtr, const int* colIdx, Symbolic& s, std::vector<int>& aSlot);
 
 // DC power-flow angles (degrees) of the grid with the branches `skip` out, referenced at bus `slack`, with the
 // loads scaled by loadScale[i] (may be null); false unless the DC model is one island (gs_dc.cpp).

@@ -16,6 +16,7 @@
 //     with forward substitution: every L/U entry is its own sparse dot product over the row subtree of
 //     its node, with the index pairs precomputed here.
 #include <algorithm>
+#include <functional>
 #include <limits>
 #include <cmath>
 #include <complex>
@@ -240,6 +241,34 @@ std::string Analyze(const HostGrid& g, Symbolic& s, bool qlim) {
     s.jCol.resize(s.nnzJ);
     for (int a = 0; a < m; a++) std::copy(jr[a].begin(), jr[a].end(), s.jCol.begin() + s.jRowPtr[a]);
 
+    return FactorSymbolic(s, [&](const std::function<int64_t(int, int)>& slotOf, std::vector<char>& hasA) {
+        // Y cell -> the four Jacobian blocks' LU slots
+        s.ySlot.assign(4 * (size_t)s.nnzY, -1);
+        for (int i = 0; i < n; i++) {
+            int pi = s.pPos[i], qi = s.qPos[i];
+            for (int p = s.yRowPtr[i]; p < s.yRowPtr[i + 1]; p++) {
+                int j = s.yCol[p], pj = s.pPos[j], qj = s.qPos[j];
+                int* o = &s.ySlot[4 * (size_t)p];
+                if (pi >= 0 && pj >= 0) o[0] = (int)slotOf(s.pinv[pi], s.pinv[pj]);
+                if (pi >= 0 && qj >= 0) o[1] = (int)slotOf(s.pinv[pi], s.pinv[qj]);
+                if (qi >= 0 && pj >= 0) o[2] = (int)slotOf(s.pinv[qi], s.pinv[pj]);
+                if (qi >= 0 && qj >= 0) o[3] = (int)slotOf(s.pinv[qi], s.pinv[qj]);
+            }
+        }
+        s.busP.assign(n, -1);
+        s.busQ.assign(n, -1);
+        for (int i = 0; i < n; i++) {
+            if (s.pPos[i] >= 0) s.busP[i] = s.pinv[s.pPos[i]];
+            if (s.qPos[i] >= 0) s.busQ[i] = s.pinv[s.qPos[i]];
+        }
+        // which LU slots hold a Jacobian value (the rest are fill, which start from zero)
+        for (int v : s.ySlot) if (v >= 0) hasA[v] = 1;
+    });
+}
+
+std::string FactorSymbolic(Symbolic& s, const std::function<void(const std::function<int64_t(int, int)>&,
+                                                                 std::vector<char>&)>& mapA) {
+    const int m = s.m;
     // ---------------- ordering and static-pivot LU pattern ----------------
     s.perm = MinimumDegreeOrder(m, s.jRowPtr, s.jCol);
     s.pinv.assign(m, -1);
@@ -289,28 +318,8 @@ std::string Analyze(const HostGrid& g, Symbolic& s, bool qlim) {
         int t = posIn(l, k);
         return t < 0 ? -1 : s.luBase[l] + 1 + s.luCnt[l] + t;
     };
-    // Y cell -> the four Jacobian blocks' LU slots
-    s.ySlot.assign(4 * (size_t)s.nnzY, -1);
-    for (int i = 0; i < n; i++) {
-        int pi = s.pPos[i], qi = s.qPos[i];
-        for (int p = s.yRowPtr[i]; p < s.yRowPtr[i + 1]; p++) {
-            int j = s.yCol[p], pj = s.pPos[j], qj = s.qPos[j];
-            int* o = &s.ySlot[4 * (size_t)p];
-            if (pi >= 0 && pj >= 0) o[0] = (int)slotOf(s.pinv[pi], s.pinv[pj]);
-            if (pi >= 0 && qj >= 0) o[1] = (int)slotOf(s.pinv[pi], s.pinv[qj]);
-            if (qi >= 0 && pj >= 0) o[2] = (int)slotOf(s.pinv[qi], s.pinv[pj]);
-            if (qi >= 0 && qj >= 0) o[3] = (int)slotOf(s.pinv[qi], s.pinv[qj]);
-        }
-    }
-    s.busP.assign(n, -1);
-    s.busQ.assign(n, -1);
-    for (int i = 0; i < n; i++) {
-        if (s.pPos[i] >= 0) s.busP[i] = s.pinv[s.pPos[i]];
-        if (s.qPos[i] >= 0) s.busQ[i] = s.pinv[s.qPos[i]];
-    }
-    // which LU slots hold a Jacobian value (the rest are fill, which start from zero)
     std::vector<char> hasA(s.nnzLU, 0);
-    for (int v : s.ySlot) if (v >= 0) hasA[v] = 1;
+    mapA(slotOf, hasA);
 
     // ---------------- levels ----------------
     s.level.assign(m, 0);
@@ -449,6 +458,52 @@ std::string Analyze(const HostGrid& g, Symbolic& s, bool qlim) {
     BuildTopPart(s, 0, sizeof(double), kTopBudgetBytes);
     BuildTopPart(s, 1, sizeof(float), kTopBudgetBytes);
     return "";
+}
+
+std::string AnalyzeMatrix(int n, const int* rowPtr, const int* colIdx, Symbolic& s, std::vector<int>& aSlot) {
+    s = Symbolic();
+    if (n <= 0) return "the matrix has no rows";
+    if (rowPtr[0] != 0) return "row_ptr[0] must be 0";
+    for (int i = 0; i < n; i++)
+        if (rowPtr[i + 1] < rowPtr[i]) return "row_ptr must not decrease";
+    const int nnz = rowPtr[n];
+    std::vector<std::vector<int>> jr(n);
+    for (int i = 0; i < n; i++) {
+        for (int p = rowPtr[i]; p < rowPtr[i + 1]; p++) {
+            const int j = colIdx[p];
+            if (j < 0 || j >= n) return "a column index is out of range";
+            jr[i].push_back(j);
+            jr[j].push_back(i);
+        }
+        jr[i].push_back(i);
+    }
+    for (int i = 0; i < n; i++) {  // a column twice in one row is malformed (CsrMatrix holds each cell once)
+        std::vector<int> row(colIdx + rowPtr[i], colIdx + rowPtr[i + 1]);
+        std::sort(row.begin(), row.end());
+        if (std::adjacent_find(row.begin(), row.end()) != row.end()) return "a row names a column twice";
+    }
+    s.n = n;
+    s.m = n;
+    s.jRowPtr.assign(n + 1, 0);
+    for (int a = 0; a < n; a++) {
+        std::sort(jr[a].begin(), jr[a].end());
+        jr[a].erase(std::unique(jr[a].begin(), jr[a].end()), jr[a].end());
+        s.jRowPtr[a + 1] = s.jRowPtr[a] + (int)jr[a].size();
+    }
+    s.nnzJ = s.jRowPtr[n];
+    s.jCol.resize(s.nnzJ);
+    for (int a = 0; a < n; a++) std::copy(jr[a].begin(), jr[a].end(), s.jCol.begin() + s.jRowPtr[a]);
+    s.yRowPtr.assign(n + 1, 0);  // no Y: the value kernels of the load flow are not used on a bare matrix
+    s.busP.assign(n, -1);
+    s.busQ.assign(n, -1);
+    return FactorSymbolic(s, [&](const std::function<int64_t(int, int)>& slotOf, std::vector<char>& hasA) {
+        aSlot.assign(nnz, -1);
+        for (int i = 0; i < n; i++)
+            for (int p = rowPtr[i]; p < rowPtr[i + 1]; p++) {
+                aSlot[p] = (int)slotOf(s.pinv[i], s.pinv[colIdx[p]]);
+                hasA[aSlot[p]] = 1;
+            }
+    });
 }
 
 void BuildTopPart(Symbolic& s, int which, size_t elem, size_t budget) {

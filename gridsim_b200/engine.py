@@ -243,6 +243,69 @@ class SparseNewtonRaphsonPowerFlow:
 
 
 # ---------------------------------------------------------------------------------------------
+class CudaSparseLinearSolver:
+    """ISparseLinearSolver (``Abstractions/ISparseLinearSolver.cs:12-17``) and IBatchedSparseLinearSolver
+    (``Abstractions/IBatchedSparseLinearSolver.cs:19-37``) on the device: ``gs_sparse_solve_batch``.
+
+    A matrix is a SciPy CSR matrix or a tuple ``(indptr, indices, data)`` of a square n x n matrix. ``solve`` returns
+    x, or None when the matrix is singular, and raises ValueError on non-finite input or a malformed matrix (the
+    reference's ArgumentException). ``solve_batch`` takes systems of any sizes and patterns; a failed system's entry is
+    None and its exception goes into ``errors``; the inputs are never modified."""
+
+    def __init__(self, ctx: Optional[CudaContext] = None):
+        self.ctx = ctx or CudaContext.default()
+
+    @staticmethod
+    def _csr(a):
+        if hasattr(a, "indptr"):
+            return (np.asarray(a.indptr), np.asarray(a.indices), np.asarray(a.data), a.shape[0])
+        indptr, indices, data = a
+        return (np.asarray(indptr), np.asarray(indices), np.asarray(data), len(indptr) - 1)
+
+    def solve(self, a, b) -> Optional[np.ndarray]:
+        errors = [None]
+        (x,) = self.solve_batch([a], [b], errors)
+        if errors[0] is not None:
+            raise errors[0]
+        return x
+
+    def solve_batch(self, matrices: Sequence, rhs: Sequence, errors: Optional[list] = None) -> list:
+        if len(matrices) != len(rhs):
+            raise ValueError(f"{len(matrices)} matrices but {len(rhs)} right-hand sides")
+        k = len(matrices)
+        if errors is not None and len(errors) != k:
+            raise ValueError("errors must hold one slot per system")
+        parts = [self._csr(a) for a in matrices]
+        for (indptr, _, _, n), b in zip(parts, rhs):
+            if len(indptr) != n + 1 or np.asarray(b).shape != (n,):
+                raise ValueError("a matrix is not square or its right-hand side has the wrong length")
+        n = np.array([p[3] for p in parts], np.int32)
+        rp = np.concatenate([np.asarray(p[0], np.int32) for p in parts]) if k else np.zeros(0, np.int32)
+        ci = np.concatenate([np.asarray(p[1], np.int32) for p in parts]) if k else np.zeros(0, np.int32)
+        va = np.concatenate([np.asarray(p[2], np.float64) for p in parts]) if k else np.zeros(0)
+        bb = np.concatenate([np.asarray(b, np.float64) for b in rhs]) if k else np.zeros(0)
+        x = np.zeros(bb.shape[0])
+        st = np.zeros(k, np.int32)
+        rc = self.ctx.lib.gs_sparse_solve_batch(self.ctx.handle, k, _p(n), _p(rp), _p(ci), _p(va), _p(bb), _p(x), _p(st))
+        self.ctx.check(rc, "gs_sparse_solve_batch")
+        out, off = [], 0
+        for j in range(k):
+            nj = int(n[j])
+            err = None
+            if st[j] == _abi.LS_OK:
+                out.append(x[off:off + nj].copy())
+            else:
+                out.append(None)
+                if st[j] == _abi.LS_NON_FINITE_INPUT:
+                    err = ValueError(f"system {j}: a value or right-hand side is not finite")
+                elif st[j] == _abi.LS_MALFORMED:
+                    err = ValueError(f"system {j}: the CSR matrix is malformed")
+            if errors is not None:
+                errors[j] = err
+            off += nj
+        return out
+
+
 class UnevenBatch:
     """Independent load flows of several grids of any sizes in one persistent launch (``gs_pf_solve_multi``).
 

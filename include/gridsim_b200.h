@@ -281,6 +281,26 @@ int gs_n1_screen(gs_grid *grid, int32_t n_out, const int32_t *branch_idx, const 
 int gs_nk_screen(gs_grid *grid, int32_t n_out, int32_t k, const int32_t *branch_sets, const gs_pf_opts *opts,
                  gs_n1_result *res);
 
+/* ---- batched sparse linear solve: ISparseLinearSolver.Solve (Abstractions/ISparseLinearSolver.cs:12-17) and
+ *      IBatchedSparseLinearSolver.SolveBatch (Abstractions/IBatchedSparseLinearSolver.cs:19-37) ----------------
+ * `count` square systems A_s x_s = b_s in FP64, of any sizes and patterns, in CSR, concatenated system after
+ * system: n[s] rows; row_ptr holds n[s]+1 offsets per system (each block starting at 0); col_idx and values hold
+ * row_ptr[n[s]] entries per system; rhs and x hold n[s] values per system. Systems that share a pattern are
+ * factorised together on the device: static diagonal pivots on a minimum-degree order of A + A^T (the reference
+ * orders the same pattern, SparseLuFactorization.cs:69-195, but pivots by rows); the analysis of a pattern is kept
+ * on the context for later calls, as CpuSparseLuSolver caches its ordering (CpuSparseLuSolver.cs:22-48). The inputs
+ * are not modified. A system that fails reports it in status[s] and leaves its x untouched (the null result and the
+ * errors[s] entry of SolveBatch); a malformed call (null arrays, count < 0) returns GS_ERR_INVALID_ARG. */
+enum gs_ls_status {
+    GS_LS_OK = 0,
+    GS_LS_SINGULAR = 1,        /* a pivot fell below 1e-12 x max(1, |A(k,k)|), or x is not finite: no result */
+    GS_LS_NON_FINITE_INPUT = 2,/* a value or right-hand side is not finite (the reference's ArgumentException) */
+    GS_LS_MALFORMED = 3        /* this system's CSR is malformed (offsets, a column out of range or twice) */
+};
+int gs_sparse_solve_batch(gs_ctx *ctx, int32_t count, const int32_t *n, const int32_t *row_ptr,
+                          const int32_t *col_idx, const double *values, const double *rhs, double *x,
+                          int32_t *status);
+
 /* The topology verdicts of a set of single-branch outages (host only, no device needed): splits[k] = 1 when
  * removing branch_idx[k] leaves more connected parts than the grid has (ContingencyAnalysis.Splits, :1665);
  * unsolvable[k] = 1 when the grid without it has a part that ProvablyUnsolvablePart (:1750-1830) rejects at

@@ -1,0 +1,111 @@
+"""The batched sparse linear solve (gs_sparse_solve_batch: ISparseLinearSolver.Solve and
+IBatchedSparseLinearSolver.SolveBatch, Abstractions/ISparseLinearSolver.cs:12-17, IBatchedSparseLinearSolver.cs:19-37).
+
+CPU: the oracle's restatement of the reference's solver (CpuSparseLuSolver over the Gilbert-Peierls LU with partial
+pivoting) against dense numpy solves, which pins it on arbitrary matrices. GPU: systems of different sizes and
+patterns in one call (the reference's Jacobians of the golden cases at their start points, random nonsymmetric
+diagonally dominant matrices) against the oracle, within REL_TOL of the solution's norm (FP64 with a different
+pivot order: the results agree to rounding); singular systems give no result, non-finite and malformed systems an
+error for that system alone, and the inputs are left as they were.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from gridsim_b200 import synthetic
+from tests.conftest import golden_model
+
+REL_TOL = 1e-9
+
+
+def _random_csr(n, seed, density=0.08):
+    rng = np.random.default_rng(seed)
+    a = np.where(rng.random((n, n)) < density, rng.normal(size=(n, n)), 0.0)
+    a += np.diag(np.abs(a).sum(axis=1) + 1.0 + rng.random(n))  # diagonally dominant: the diagonal pivots hold
+    rows, cols = np.nonzero(a)
+    indptr = np.searchsorted(rows, np.arange(n + 1)).astype(np.int32)
+    return (indptr, cols.astype(np.int32), a[rows, cols]), a
+
+
+def test_oracle_solver_matches_dense_solves():
+    for seed in range(20):
+        (rp, ci, v), a = _random_csr(int(5 + 7 * seed), seed)
+        b = np.random.default_rng(seed + 99).normal(size=a.shape[0])
+        x = oracle.sparse_solve(rp, ci, v, b)
+        ref = np.linalg.solve(a, b)
+        assert np.max(np.abs(x - ref)) <= 1e-12 * max(1.0, np.max(np.abs(ref)))
+
+
+def test_oracle_solver_reports_singular():
+    (rp, ci, v), a = _random_csr(12, 3)
+    v = v.copy()
+    v[rp[4]:rp[5]] = 0.0  # a zero row
+    assert oracle.sparse_solve(rp, ci, v, np.ones(12)) is None
+
+
+def _jacobians():
+    out = []
+    for name in ("case9", "case14", "case57", "case118", "case300"):
+        m, _ = golden_model(name)
+        rp, ci, v, mis = oracle.jacobian(m)
+        out.append(((rp, ci, v), mis))
+    m = synthetic.config_grid(1, 0)
+    rp, ci, v, mis = oracle.jacobian(m)
+    out.append(((rp, ci, v), mis))
+    return out
+
+
+@pytest.mark.gpu
+def test_mixed_batch_matches_the_oracle():
+    from gridsim_b200.engine import CudaSparseLinearSolver
+    systems = []
+    for (csr, mis) in _jacobians():
+        rng = np.random.default_rng(len(systems))
+        for c in range(3):  # the same pattern three times, values perturbed
+            v = csr[2] * (1.0 + 0.01 * c * rng.standard_normal(csr[2].shape[0]))
+            systems.append(((csr[0], csr[1], v), mis))
+    for seed in range(40):
+        (csr, a) = _random_csr(int(20 + 5 * seed), 1000 + seed)
+        systems.append((csr, np.random.default_rng(seed).normal(size=a.shape[0])))
+    mats = [s[0] for s in systems]
+    rhs = [s[1] for s in systems]
+    copies = [(m[0].copy(), m[1].copy(), m[2].copy()) for m in mats], [r.copy() for r in rhs]
+    solver = CudaSparseLinearSolver()
+    errors = [None] * len(mats)
+    xs = solver.solve_batch(mats, rhs, errors)
+    assert all(e is None for e in errors)
+    for (rp, ci, v), b, x in zip(mats, rhs, xs):
+        ref = oracle.sparse_solve(rp, ci, v, b)
+        assert ref is not None and x is not None
+        assert np.max(np.abs(x - ref)) <= REL_TOL * max(1.0, np.max(np.abs(ref)))
+    for m, c in zip(mats, copies[0]):  # inputs unmodified
+        assert all(np.array_equal(p, q) for p, q in zip(m, c))
+    assert all(np.array_equal(r, c) for r, c in zip(rhs, copies[1]))
+    again = solver.solve_batch(mats, rhs)  # the analysed patterns are reused: same results bit for bit
+    assert all(np.array_equal(a, b) for a, b in zip(xs, again))
+
+
+@pytest.mark.gpu
+def test_failures_stay_with_their_system():
+    from gridsim_b200.engine import CudaSparseLinearSolver
+    (rp, ci, v), a = _random_csr(30, 7)
+    b = np.ones(30)
+    sing = v.copy()
+    sing[rp[3]:rp[4]] = 0.0  # a zero row: singular
+    nan = v.copy()
+    nan[0] = np.nan
+    bad_ci = ci.copy()
+    bad_ci[0] = 30  # a column out of range
+    solver = CudaSparseLinearSolver()
+    errors = [None] * 5
+    xs = solver.solve_batch([(rp, ci, v), (rp, ci, sing), (rp, ci, nan), (rp, bad_ci, v), (rp, ci, v)],
+                            [b, b, b, b, b], errors)
+    ref = np.linalg.solve(a, b)
+    assert np.max(np.abs(xs[0] - ref)) <= REL_TOL * np.max(np.abs(ref))
+    assert xs[1] is None and errors[1] is None  # singular: no result, no exception (ISparseLinearSolver returns null)
+    assert xs[2] is None and isinstance(errors[2], ValueError)
+    assert xs[3] is None and isinstance(errors[3], ValueError)
+    assert np.array_equal(xs[4], xs[0])
+    with pytest.raises(ValueError):
+        solver.solve((rp, ci, nan), b)
+    assert solver.solve((rp, ci, sing), b) is None
