@@ -23,6 +23,7 @@ PF_STATUS_NAMES = ["Converged", "MaxIterations", "NonFinite", "Diverged", "Singu
                    "UnsolvablePart"]
 RATE_A, RATE_B, RATE_C = 0, 1, 2
 LS_OK, LS_SINGULAR, LS_NON_FINITE_INPUT, LS_MALFORMED = 0, 1, 2, 3
+OUTAGE_BRANCH, OUTAGE_GENERATOR, OUTAGE_BUS = 0, 1, 2
 
 PREC_FP64, PREC_MIXED = 0, 1
 VIOL_BRANCH_OVERLOAD, VIOL_BOUNDARY_OVERLOAD, VIOL_UNDERVOLTAGE, VIOL_OVERVOLTAGE = 0, 1, 2, 3
@@ -128,6 +129,7 @@ EXPORTS = {
     "gs_pf_solve_batch": (c_i32, [c_vp, c_i32, c_vp, c_vp, ctypes.POINTER(PfOpts), c_vp, c_vp, c_vp, c_vp, c_vp]),
     "gs_n1_screen": (c_i32, [c_vp, c_i32, c_vp, ctypes.POINTER(PfOpts), ctypes.POINTER(N1Result)]),
     "gs_nk_screen": (c_i32, [c_vp, c_i32, c_i32, c_vp, ctypes.POINTER(PfOpts), ctypes.POINTER(N1Result)]),
+    "gs_element_screen": (c_i32, [c_vp, c_i32, c_vp, c_vp, ctypes.POINTER(PfOpts), ctypes.POINTER(N1Result)]),
     "gs_analyze_host": (c_i32, [ctypes.POINTER(GridDesc), ctypes.POINTER(GridInfo)]),
     "gs_outage_topology": (c_i32, [ctypes.POINTER(GridDesc), c_f64, c_i32, c_vp, c_vp, c_vp]),
     "gs_sparse_solve_batch": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),

@@ -17,7 +17,7 @@
 namespace gs {
 
 bool DcAngles(const HostGrid& h, const Symbolic& s, const std::vector<int>& skip, int slack, const double* loadScale,
-              std::vector<double>& thetaDeg) {
+              std::vector<double>& thetaDeg, int deadBus, int specBus, double specDpPu) {
     const int n = h.n;
     std::vector<int> parent(n);
     std::iota(parent.begin(), parent.end(), 0);
@@ -27,7 +27,7 @@ bool DcAngles(const HostGrid& h, const Symbolic& s, const std::vector<int>& skip
     };
     std::vector<int> red(n, -1);
     int nr = 0;
-    for (int i = 0; i < n; i++) if (i != slack) red[i] = nr++;
+    for (int i = 0; i < n; i++) if (i != slack && i != deadBus) red[i] = nr++;
     std::vector<std::map<int, double>> rows(nr);
     for (int k = 0; k < h.nbr; k++) {
         if (!h.brOn[k] || h.x[k] == 0.0 || std::find(skip.begin(), skip.end(), k) != skip.end()) continue;
@@ -39,7 +39,7 @@ bool DcAngles(const HostGrid& h, const Symbolic& s, const std::vector<int>& skip
         if (f >= 0 && t >= 0) { rows[f][t] -= b; rows[t][f] -= b; }
     }
     int islands = 0;
-    for (int i = 0; i < n; i++) if (find(i) == i) islands++;
+    for (int i = 0; i < n; i++) if (i != deadBus && find(i) == i) islands++;  // a removed bus is not in the model
     if (islands != 1 || nr == 0) return false;
     // minimum-degree order of the pattern
     std::vector<int> rowPtr(nr + 1, 0), col;
@@ -56,7 +56,8 @@ bool DcAngles(const HostGrid& h, const Symbolic& s, const std::vector<int>& skip
     std::vector<double> rhs(nr, 0.0);
     for (int i = 0; i < n; i++)
         if (red[i] >= 0)  // injections sum(Pg) - Pd (pu), the load scaled as the case's
-            rhs[pinv[red[i]]] = loadScale ? s.pspec[i] - (loadScale[i] - 1.0) * h.pd[i] / h.base : s.pspec[i];
+            rhs[pinv[red[i]]] = (loadScale ? s.pspec[i] - (loadScale[i] - 1.0) * h.pd[i] / h.base : s.pspec[i]) -
+                                (i == specBus ? specDpPu : 0.0);
     // elimination (rows keep their upper parts; the pattern is symmetric, so row k's upper columns are the rows
     // that hold column k)
     for (int k = 0; k < nr; k++) {

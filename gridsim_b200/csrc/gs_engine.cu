@@ -64,10 +64,14 @@ __device__ __forceinline__ void busMismatchJac(const DevGrid& g, const DevBatch&
                                                double* qOut, double& localMax, int& bad) {
     const size_t B = (size_t)b.B;
     const double vmi = b.vm[i * B + s], vai = b.va[i * B + s];
-    // Q limits: a bus that starts PV keeps an identity Q row while it is PV (its Vm step is 0, its Q mismatch
-    // is not an equation); once switched to PQ its Q is held at the limit
-    const bool startsPV = g.qlim && g.busType[i] == 2;
-    const bool pvNow = startsPV && b.effType[i * B + s] == 2;
+    // Grids analysed with every bus's P and Q rows (qlim): the bus's type in this system (3 reference, 2 PV, 1 PQ,
+    // 0 removed) decides which rows are equations. A reference or removed bus keeps identity P and Q rows, a PV bus
+    // an identity Q row (their steps are 0, their mismatches are not equations); a bus that starts PV or reference
+    // and is PQ now (switched at a Q limit, or left without units) holds Q at qspecSys.
+    const int gt = g.busType[i];
+    const int et = g.qlim ? b.effType[i * B + s] : gt;
+    const bool pId = g.qlim && (et == 3 || et == 0);
+    const bool qId = g.qlim && et != 1;
     const int kp = g.busP[i], kq = g.busQ[i];
     const bool fill = fillJac && (kp >= 0 || kq >= 0);
     T* lu = (T*)b.lu;
@@ -88,10 +92,10 @@ __device__ __forceinline__ void busMismatchJac(const DevGrid& g, const DevBatch&
         qi += vmj * (G * sn - Bv * cs);
         if (j == i) { pd = p; Gd = G; Bd = Bv; continue; }
         if (!fill) continue;
-        const double H = vmi * vmj * (G * sn - Bv * cs);
-        const double N = vmi * (G * cs + Bv * sn);
-        const double M = pvNow ? 0.0 : -vmi * vmj * (G * cs + Bv * sn);  // the identity Q row of a bus that is PV now
-        const double L = pvNow ? 0.0 : vmi * (G * sn - Bv * cs);
+        const double H = pId ? 0.0 : vmi * vmj * (G * sn - Bv * cs);
+        const double N = pId ? 0.0 : vmi * (G * cs + Bv * sn);
+        const double M = qId ? 0.0 : -vmi * vmj * (G * cs + Bv * sn);
+        const double L = qId ? 0.0 : vmi * (G * sn - Bv * cs);
         const int4 sl = *reinterpret_cast<const int4*>(g.ySlot + 4 * p);
         if (sl.x >= 0) lu[sl.x * B + s] = (T)H;
         if (sl.y >= 0) lu[sl.y * B + s] = (T)N;
@@ -101,10 +105,10 @@ __device__ __forceinline__ void busMismatchJac(const DevGrid& g, const DevBatch&
     }
     const double P = vmi * pi, Q = vmi * qi;
     if (fill && pd >= 0) {
-        const double H = -Q - Bd * vmi * vmi;
-        const double N = P / vmi + Gd * vmi;
-        const double M = pvNow ? 0.0 : P - Gd * vmi * vmi;
-        const double L = pvNow ? 1.0 : Q / vmi - Bd * vmi;
+        const double H = pId ? 1.0 : -Q - Bd * vmi * vmi;
+        const double N = pId ? 0.0 : P / vmi + Gd * vmi;
+        const double M = qId ? 0.0 : P - Gd * vmi * vmi;
+        const double L = qId ? 1.0 : Q / vmi - Bd * vmi;
         const int4 sl = *reinterpret_cast<const int4*>(g.ySlot + 4 * pd);
         if (sl.x >= 0) lu[sl.x * B + s] = (T)H;
         if (sl.y >= 0) lu[sl.y * B + s] = (T)N;
@@ -114,21 +118,28 @@ __device__ __forceinline__ void busMismatchJac(const DevGrid& g, const DevBatch&
     }
     if (pOut) { pOut[i * B + s] = P; qOut[i * B + s] = Q; }
     double sc = b.loadScale ? b.loadScale[i * B + s] : 1.0;
-    const double pspec = b.loadScale ? g.pgen[i] - sc * g.pload[i] : g.pgen[i] - g.pload[i];
+    double pspec = b.loadScale ? g.pgen[i] - sc * g.pload[i] : g.pgen[i] - g.pload[i];
     double qspec = b.loadScale ? g.qgen[i] - sc * g.qload[i] : g.qgen[i] - g.qload[i];
-    if (startsPV) {
-        b.qinj[i * B + s] = Q;
-        if (!pvNow) qspec = b.qspecSys[i * B + s];
+    if (b.specBus && b.specBus[s] == i) {  // a generator outage: the bus loses the unit's output
+        pspec = (g.pgen[i] - b.specDp[s]) - sc * g.pload[i];
+        qspec = (g.qgen[i] - b.specDq[s]) - sc * g.qload[i];
+    }
+    if (g.qlim) {
+        if (gt == 2) b.qinj[i * B + s] = Q;
+        if (et == 1 && gt != 1) qspec = b.qspecSys[i * B + s];
     }
     T* y = (T*)b.y;
-    if (kp >= 0) {
+    if (kp >= 0 && pId) {
+        y[kp * B + s] = T(0);
+        if (b.rhs64) b.rhs64[kp * B + s] = 0.0;
+    } else if (kp >= 0) {
         const double f = pspec - P;
         y[kp * B + s] = (T)f;
         if (b.rhs64) b.rhs64[kp * B + s] = f;
         localMax = fmax(localMax, fabs(f));
         bad |= isfinite(f) ? 0 : 1;
     }
-    if (kq >= 0 && pvNow) {
+    if (kq >= 0 && qId) {
         y[kq * B + s] = T(0);
         if (b.rhs64) b.rhs64[kq * B + s] = 0.0;
     } else if (kq >= 0) {
@@ -268,20 +279,23 @@ __global__ void k_status_q(DevBatch b, double tol, double divLimit, int maxIter)
 // ApplyQLimits on the systems whose pass converged: grid (ceil(n / 8), B / 32), block (32, 8).
 __global__ void k_qapply(DevGrid g, DevBatch b) {
     const int s = blockIdx.y * 32 + threadIdx.x, i = blockIdx.x * 8 + threadIdx.y;
-    if (i >= g.n || s >= b.count || !b.active[s] || !(b.qState[s] & kQPending) || g.busType[i] != 2) return;
+    if (!g.qlimOn || i >= g.n || s >= b.count || !b.active[s] || !(b.qState[s] & kQPending) || g.busType[i] != 2) return;
     const size_t idx = (size_t)i * b.B + s;
     if (b.effType[idx] != 2) return;
     const double qd = (b.loadScale ? b.loadScale[idx] : 1.0) * g.qload[i];  // the bus's load, pu
     const double qGen = (b.qinj[idx] + qd) * g.baseMva;
-    const bool fixed = g.qminMvar[i] == g.qmaxMvar[i];
-    if (qGen > g.qmaxMvar[i] + kQLimitTolMva) {
+    // the aggregate limits of the bus's units (those left after a generator outage)
+    const bool spec = b.specBus && b.specBus[s] == i;
+    const double qmin = spec ? b.specQmin[s] : g.qminMvar[i], qmax = spec ? b.specQmax[s] : g.qmaxMvar[i];
+    const bool fixed = qmin == qmax;
+    if (qGen > qmax + kQLimitTolMva) {
         b.effType[idx] = 1;
-        b.qspecSys[idx] = g.qmaxPu[i] - qd;
+        b.qspecSys[idx] = (spec ? qmax / g.baseMva : g.qmaxPu[i]) - qd;
         b.pinned[idx] = fixed ? 2 : 1;
         atomicOr(&b.qState[s], kQChanged);
-    } else if (qGen < g.qminMvar[i] - kQLimitTolMva) {
+    } else if (qGen < qmin - kQLimitTolMva) {
         b.effType[idx] = 1;
-        b.qspecSys[idx] = g.qminPu[i] - qd;
+        b.qspecSys[idx] = (spec ? qmin / g.baseMva : g.qminPu[i]) - qd;
         b.pinned[idx] = fixed ? 2 : -1;
         atomicOr(&b.qState[s], kQChanged);
     }
@@ -296,7 +310,10 @@ __global__ void k_qrevert(DevGrid g, DevBatch b) {
     const size_t idx = (size_t)i * b.B + s;
     const int pin = b.pinned[idx];
     if (b.effType[idx] != 1 || (pin != 1 && pin != -1) || b.reverted[idx] >= 1) return;
-    const double vm = b.vm[idx], vg = g.vm0[i];
+    double vg = g.vm0[i];  // the set point (of the units left, after a generator outage)
+    if (b.ovBus && b.ovBus[2 * s] == i && !isnan(b.ovVm[2 * s])) vg = b.ovVm[2 * s];
+    else if (b.ovBus && b.ovBus[2 * s + 1] == i && !isnan(b.ovVm[2 * s + 1])) vg = b.ovVm[2 * s + 1];
+    const double vm = b.vm[idx];
     if ((pin == 1 && vm > vg + kRevertVoltTolPu) || (pin == -1 && vm < vg - kRevertVoltTolPu)) {
         b.effType[idx] = 2;
         b.vm[idx] = vg;
@@ -580,7 +597,8 @@ __global__ void __launch_bounds__(32 * kPersistWarps) k_persistent(DevGrid g, De
 template <typename T>
 __device__ __forceinline__ void busResidual(const DevGrid& g, const DevBatch& b, int i, int s) {
     const size_t B = (size_t)b.B;
-    const bool pvNow = g.qlim && g.busType[i] == 2 && b.effType[i * B + s] == 2;
+    const int et = g.qlim ? b.effType[i * B + s] : g.busType[i];
+    const bool pId = g.qlim && (et == 3 || et == 0), qId = g.qlim && et != 1;  // identity rows (busMismatchJac)
     const int kp = g.busP[i], kq = g.busQ[i];
     if (kp < 0 && kq < 0) return;
     const T* dx = (const T*)b.y;
@@ -627,8 +645,8 @@ __device__ __forceinline__ void busResidual(const DevGrid& g, const DevBatch& b,
         jp += H * dth + N * dv;
         jq += M * dth + L * dv;
     }
-    if (kp >= 0) z[kp * B + s] = (T)(b.rhs64[kp * B + s] - jp);
-    if (kq >= 0) z[kq * B + s] = pvNow ? T(0) : (T)(b.rhs64[kq * B + s] - jq);
+    if (kp >= 0) z[kp * B + s] = pId ? T(0) : (T)(b.rhs64[kp * B + s] - jp);
+    if (kq >= 0) z[kq * B + s] = qId ? T(0) : (T)(b.rhs64[kq * B + s] - jq);
 }
 
 template <typename T>
@@ -689,6 +707,18 @@ __device__ __forceinline__ void moveSystem(const DevBatch& from, int sf, const D
     to.flags[st] = from.flags[sf];
     const_cast<int*>(to.outage)[st] = from.outage[sf];
     if (from.refine && to.refine) to.refine[st] = from.refine[sf];
+    if (from.ovBus && to.ovBus) {
+        for (int q = 0; q < 2; q++) {
+            const_cast<int*>(to.ovBus)[2 * st + q] = from.ovBus[2 * sf + q];
+            const_cast<int*>(to.ovType)[2 * st + q] = from.ovType[2 * sf + q];
+            const_cast<double*>(to.ovVm)[2 * st + q] = from.ovVm[2 * sf + q];
+        }
+        const_cast<int*>(to.specBus)[st] = from.specBus[sf];
+        const_cast<double*>(to.specDp)[st] = from.specDp[sf];
+        const_cast<double*>(to.specDq)[st] = from.specDq[sf];
+        const_cast<double*>(to.specQmin)[st] = from.specQmin[sf];
+        const_cast<double*>(to.specQmax)[st] = from.specQmax[sf];
+    }
 }
 
 // The batched linear solve's inputs into the workspace: A's stored entries into their LU slots, b into the
@@ -1302,14 +1332,28 @@ __global__ void k_init(DevGrid g, DevBatch b, const double* vmStart, const doubl
     const size_t B = (size_t)b.B;
     double vm = vmSys ? vmSys[i * B + s] : (vmStart ? vmStart[i] : g.vm0[i]);
     double va = vaSys ? vaSys[i * B + s] : (vaStart ? vaStart[i] : g.va0[i]);
-    // PV and slack magnitudes are set points whatever the start (NewtonShell.BuildBusSpec :467-469)
-    if (g.busType[i] != 1) vm = g.vm0[i];
-    if (g.busType[i] == 3) va = g.va0[i];
+    // an element outage may change this bus's type in this system, and its set point or stored magnitude
+    const int gt = g.busType[i];
+    int et = gt;
+    double ov = NAN;
+    if (b.ovBus && s < b.count) {
+        if (b.ovBus[2 * s] == i) { et = b.ovType[2 * s]; ov = b.ovVm[2 * s]; }
+        else if (b.ovBus[2 * s + 1] == i) { et = b.ovType[2 * s + 1]; ov = b.ovVm[2 * s + 1]; }
+    }
+    // PV and reference magnitudes are set points whatever the start (NewtonShell.BuildBusSpec :467-469)
+    if (et == 2 || et == 3) vm = isnan(ov) ? g.vm0[i] : ov;
+    else if (!isnan(ov) && !vmSys && !vmStart) vm = ov;  // a bus that starts PQ here: its stored magnitude
+    if (gt == 3 && et == 3) va = g.va0[i];
     b.vm[i * B + s] = vm;
     b.va[i * B + s] = va;
     if (b.qState) {
-        b.effType[i * B + s] = g.busType[i];
-        b.qspecSys[i * B + s] = 0.0;
+        b.effType[i * B + s] = et;
+        double qs = 0.0;
+        if (et == 1 && gt != 1) {  // left without units: Q is what the units left give, less the load
+            const double qd = (b.loadScale ? b.loadScale[i * B + s] : 1.0) * g.qload[i];
+            qs = ((b.specBus && b.specBus[s] == i) ? g.qgen[i] - b.specDq[s] : g.qgen[i]) - qd;
+        }
+        b.qspecSys[i * B + s] = qs;
         b.pinned[i * B + s] = 0;
         b.reverted[i * B + s] = 0;
         if (i == 0) { b.passIter[s] = 0; b.qPass[s] = 0; b.qState[s] = 0; }
@@ -1417,11 +1461,13 @@ __global__ void k_classify(DevGrid g, DevBatch b, Classify c) {
             if (lim > 0 && fabs(flow) > lim) code = 4;
         } else {
             const int i = item - g.nbr - g.nBnd;
-            val = b.vm[i * B + s];
-            if (val < c.lo[i]) code = 2;
-            else if (val > c.hi[i]) code = 3;
-            atomicMaxNonNeg(&c.maxVm[s], val);
-            atomicMaxNonNeg(&c.minVmNeg[s], 100.0 - val);
+            if (!(g.qlim && b.effType[i * B + s] == 0)) {  // a removed bus is not in the reduced model
+                val = b.vm[i * B + s];
+                if (val < c.lo[i]) code = 2;
+                else if (val > c.hi[i]) code = 3;
+                atomicMaxNonNeg(&c.maxVm[s], val);
+                atomicMaxNonNeg(&c.minVmNeg[s], 100.0 - val);
+            }
         }
     }
     c.code[(size_t)item * B + s] = code;
@@ -1518,6 +1564,8 @@ struct Workspace {
     int precision = -1;
     DevBuf activeList, origin;  // origin: a compact batch position -> the system of the full batch
     DevBuf effType, qspecSys, pinned, reverted, qinj, passIter, qPass, qState;  // Q-limit enforcement
+    DevBuf ovBus, ovType, ovVm, specBus, specDp, specDq, specQmin, specQmax;    // element outages
+    bool ovOn = false;  // the element-outage arrays hold this call's systems
     DevBuf beforeLast;
     DevBuf vm, va, lu, piv, y, z, rhs64, refine, maxMis, maxDx, startMis, finalMis, status, iters, convIters, active, flags, outage,
         loadScale, activeCount;
@@ -1553,6 +1601,7 @@ struct gs_grid {
     std::unique_ptr<gs_grid> qgrid;  // the same grid analysed for Q-limit enforcement (built on first use)
     std::unique_ptr<gs_grid> rgrid;  // a twin with its own workspace for the DC-angle retries (built on first use)
     gs::OutageSetTable sets;         // multi-branch outages of the current call (view.nSet > 0 while installed)
+    std::vector<gs::ElemSys> elemBatch;  // element outages of the systems in the workspace (empty: none)
     gs::DevBuf setBrBuf, setCellBuf, setRedBuf;
     int split = 0;      // first level run by the persistent kernels
     int tailSplit = 0;  // first level the few-systems path runs as one CTA per system
@@ -1602,6 +1651,7 @@ int UploadGrid(gs_grid* G) {
     DevGrid& v = G->view;
     v.n = s.n; v.m = s.m; v.nnzY = s.nnzY; v.nbr = s.nbr; v.nnzLU = s.nnzLU; v.nLevels = s.nLevels;
     v.qlim = s.qlim ? 1 : 0;
+    v.qlimOn = v.qlim;
     v.baseMva = h.base;
     const int n = h.n;
     G->pgen.assign(n, 0.0); G->qgen.assign(n, 0.0);
@@ -1721,6 +1771,9 @@ int EnsureWs(gs_ctx* ctx, const Symbolic& s, Workspace& w, int B, int precision,
         GS_CUDA(w.effType.alloc(nb * 4)); GS_CUDA(w.qspecSys.alloc(nb * 8)); GS_CUDA(w.pinned.alloc(nb * 4));
         GS_CUDA(w.reverted.alloc(nb * 4)); GS_CUDA(w.qinj.alloc(nb * 8));
         GS_CUDA(w.passIter.alloc((size_t)B * 4)); GS_CUDA(w.qPass.alloc((size_t)B * 4)); GS_CUDA(w.qState.alloc((size_t)B * 4));
+        GS_CUDA(w.ovBus.alloc((size_t)B * 8)); GS_CUDA(w.ovType.alloc((size_t)B * 8)); GS_CUDA(w.ovVm.alloc((size_t)B * 16));
+        GS_CUDA(w.specBus.alloc((size_t)B * 4)); GS_CUDA(w.specDp.alloc((size_t)B * 8)); GS_CUDA(w.specDq.alloc((size_t)B * 8));
+        GS_CUDA(w.specQmin.alloc((size_t)B * 8)); GS_CUDA(w.specQmax.alloc((size_t)B * 8));
     }
     size_t t = precision == GS_PREC_MIXED ? 4 : 8;
     size_t Bz = (size_t)B;
@@ -1789,6 +1842,11 @@ DevBatch MakeBatchWs(const Workspace& w, int nLevels, int B, int count, bool use
         b.effType = w.effType.as<int>(); b.qspecSys = w.qspecSys.as<double>(); b.pinned = w.pinned.as<int>();
         b.reverted = w.reverted.as<int>(); b.qinj = w.qinj.as<double>(); b.passIter = w.passIter.as<int>();
         b.qPass = w.qPass.as<int>(); b.qState = w.qState.as<int>();
+        if (w.ovOn) {
+            b.ovBus = w.ovBus.as<int>(); b.ovType = w.ovType.as<int>(); b.ovVm = w.ovVm.as<double>();
+            b.specBus = w.specBus.as<int>(); b.specDp = w.specDp.as<double>(); b.specDq = w.specDq.as<double>();
+            b.specQmin = w.specQmin.as<double>(); b.specQmax = w.specQmax.as<double>();
+        }
     }
     return b;
 }
@@ -1818,6 +1876,10 @@ DevBatch HalfView(const DevBatch& b, int off, int n) {
     h.loadScale = sh(b.loadScale);
     h.effType = sh(b.effType); h.qspecSys = sh(b.qspecSys); h.pinned = sh(b.pinned); h.reverted = sh(b.reverted);
     h.qinj = sh(b.qinj); h.passIter = sh(b.passIter); h.qPass = sh(b.qPass); h.qState = sh(b.qState);
+    auto sh2 = [&](auto* p) { return p ? p + 2 * off : p; };  // two entries per system
+    h.ovBus = sh2(b.ovBus); h.ovType = sh2(b.ovType); h.ovVm = sh2(b.ovVm);
+    h.specBus = sh(b.specBus); h.specDp = sh(b.specDp); h.specDq = sh(b.specDq);
+    h.specQmin = sh(b.specQmin); h.specQmax = sh(b.specQmax);
     return h;
 }
 
@@ -2155,6 +2217,27 @@ int RetryGridOf(gs_grid* G, gs_grid** out) {
     return GS_OK;
 }
 
+// The element-outage arrays of workspace w for systems 0 .. e.size()-1 (the rest: no change).
+int UploadElements(gs_grid* G, Workspace& w, const std::vector<ElemSys>& e) {
+    gs_ctx* ctx = G->ctx;
+    const int B = w.B;
+    std::vector<int> ob(2 * (size_t)B, -1), ot(2 * (size_t)B, 0), sb(B, -1);
+    std::vector<double> ov(2 * (size_t)B, NAN), dp(B, 0.0), dq(B, 0.0), qn(B, 0.0), qx(B, 0.0);
+    for (size_t k = 0; k < e.size(); k++) {
+        for (int q = 0; q < 2; q++) { ob[2 * k + q] = e[k].ovBus[q]; ot[2 * k + q] = e[k].ovType[q]; ov[2 * k + q] = e[k].ovVm[q]; }
+        sb[k] = e[k].specBus; dp[k] = e[k].dp; dq[k] = e[k].dq; qn[k] = e[k].qmin; qx[k] = e[k].qmax;
+    }
+    GS_CUDA(cudaMemcpy(w.ovBus.p, ob.data(), ob.size() * 4, cudaMemcpyHostToDevice));
+    GS_CUDA(cudaMemcpy(w.ovType.p, ot.data(), ot.size() * 4, cudaMemcpyHostToDevice));
+    GS_CUDA(cudaMemcpy(w.ovVm.p, ov.data(), ov.size() * 8, cudaMemcpyHostToDevice));
+    GS_CUDA(cudaMemcpy(w.specBus.p, sb.data(), sb.size() * 4, cudaMemcpyHostToDevice));
+    GS_CUDA(cudaMemcpy(w.specDp.p, dp.data(), dp.size() * 8, cudaMemcpyHostToDevice));
+    GS_CUDA(cudaMemcpy(w.specDq.p, dq.data(), dq.size() * 8, cudaMemcpyHostToDevice));
+    GS_CUDA(cudaMemcpy(w.specQmin.p, qn.data(), qn.size() * 8, cudaMemcpyHostToDevice));
+    GS_CUDA(cudaMemcpy(w.specQmax.p, qx.data(), qx.size() * 8, cudaMemcpyHostToDevice));
+    return GS_OK;
+}
+
 // The branches outage id `id` takes out: none (-1), one branch (id < nbr), or the set id - nbr of the installed table.
 std::vector<int> OutageBranches(const gs_grid* G, int id) {
     if (id < 0) return {};
@@ -2226,9 +2309,16 @@ int RetryStalled(gs_grid* G, int count, const int* outage, const double* loadSca
         GS_CUDA(cudaMemcpy(pass.data(), w.passIter.p, count * 4, cudaMemcpyDeviceToHost));
         GS_CUDA(cudaMemcpy(qs.data(), w.qState.p, count * 4, cudaMemcpyDeviceToHost));
     }
-    int slack = -1, slacks = 0;
-    for (int i = 0; i < s.n; i++) if (s.type0[i] == 3) { slack = i; slacks++; }
+    int gridSlack = -1, slacks = 0;
+    for (int i = 0; i < s.n; i++) if (s.type0[i] == 3) { gridSlack = i; slacks++; }
     if (slacks != 1) return GS_OK;  // TrySeedDcAngles needs exactly one slack
+    const bool elems = !G->elemBatch.empty();
+    auto slackOf = [&](int k) {  // an element outage may have moved the reference
+        if (elems)
+            for (int q = 0; q < 2; q++)
+                if (G->elemBatch[k].ovBus[q] >= 0 && G->elemBatch[k].ovType[q] == 3) return G->elemBatch[k].ovBus[q];
+        return gridSlack;
+    };
     std::vector<int> cand;
     for (int k = 0; k < count; k++) {
         if (st[k] == GS_PF_CONVERGED) continue;
@@ -2257,7 +2347,16 @@ int RetryStalled(gs_grid* G, int count, const int* outage, const double* loadSca
     for (int k : cand) {
         std::vector<double> th;
         const double* sc = loadScale ? loadScale + (size_t)k * n : nullptr;
-        if (!DcAngles(h, s, OutageBranches(G, outage ? outage[k] : -1), slack, sc, th)) continue;
+        const int slack = slackOf(k);
+        int dead = -1, specBus = -1;
+        double dp = 0.0;
+        if (elems) {
+            const ElemSys& e = G->elemBatch[k];
+            for (int q = 0; q < 2; q++) if (e.ovBus[q] >= 0 && e.ovType[q] == 0) dead = e.ovBus[q];
+            specBus = e.specBus;
+            dp = e.dp;
+        }
+        if (!DcAngles(h, s, OutageBranches(G, outage ? outage[k] : -1), slack, sc, th, dead, specBus, dp)) continue;
         std::vector<double> va(n);
         for (int i = 0; i < n; i++)
             va[i] = i == slack ? vaBase[slack] : vaBase[slack] + std::remainder(th[i], 360.0) * 3.14159265358979323846 / 180.0;
@@ -2278,6 +2377,14 @@ int RetryStalled(gs_grid* G, int count, const int* outage, const double* loadSca
     std::vector<int> outs(B, -1);
     for (int c = 0; c < nc; c++) outs[c] = okOut[c];
     GS_CUDA(cudaMemcpy(rw.outage.p, outs.data(), B * 4, cudaMemcpyHostToDevice));
+    R->view.qlimOn = G->view.qlimOn;
+    struct RetryOvOff { gs_grid* r; ~RetryOvOff() { r->ws.ovOn = r->tws.ovOn = false; r->elemBatch.clear(); } } retryOvOff{R};
+    if (elems) {  // the retried systems keep their element outages
+        R->elemBatch.clear();
+        for (int c = 0; c < nc; c++) R->elemBatch.push_back(G->elemBatch[ok[c]]);
+        if ((rc = UploadElements(R, rw, R->elemBatch)) != GS_OK) return rc;
+        rw.ovOn = R->tws.ovOn = true;
+    }
     if (loadScale) {
         std::vector<double> scl((size_t)n * B, 1.0);
         for (int c = 0; c < nc; c++)
@@ -2285,11 +2392,17 @@ int RetryStalled(gs_grid* G, int count, const int* outage, const double* loadSca
         GS_CUDA(cudaMemcpy(rw.loadScale.p, scl.data(), scl.size() * 8, cudaMemcpyHostToDevice));
     }
     std::vector<double> vmS((size_t)n * B, 1.0), vaS((size_t)n * B, 0.0);
-    for (int c = 0; c < nc; c++)
+    for (int c = 0; c < nc; c++) {
         for (int i = 0; i < n; i++) {
             vmS[(size_t)i * B + c] = vmBase[i];
             vaS[(size_t)i * B + c] = seeds[c][i];
         }
+        if (elems && !warm)  // a bus that starts PQ in this outage starts from its stored magnitude
+            for (int q = 0; q < 2; q++) {
+                const ElemSys& e = G->elemBatch[ok[c]];
+                if (e.ovBus[q] >= 0 && e.ovType[q] == 1 && !std::isnan(e.ovVm[q])) vmS[(size_t)e.ovBus[q] * B + c] = e.ovVm[q];
+            }
+    }
     DevBuf dvm, dva;
     GS_CUDA(dvm.alloc(vmS.size() * 8));
     GS_CUDA(dva.alloc(vaS.size() * 8));
@@ -2630,9 +2743,48 @@ int gs_pf_solve_batch(gs_grid* G, int32_t count, const double* loadScale, const 
 namespace gs {
 namespace {
 
-// The screen of a list of outages, each a list of branches taken out together (empty: the intact grid, ScreenBaseCase;
-// one branch: ScreenBranches; several: ScreenOutageCore over several indices, ContingencyAnalysis.cs:1087-1097).
-int ScreenOutageLists(gs_grid* G, int nOut, const std::vector<std::vector<int>>& lists, const gs_pf_opts* opts,
+// One outage of a screen: branches taken out together, and for an element outage (ScreenElementOutage,
+// ContingencyAnalysis.cs:1355-1437) a generator or a bus (whose branches are listed too).
+struct Element {
+    std::vector<int> branches;
+    int gen = -1;
+    int bus = -1;
+};
+
+// The bus with the largest remaining unit by |Pg| (first in model order among ties) among the buses reachable from
+// `seeds` over in-service branches not in `gone`, never through `removedBus`; -1 when none (ReelectReference
+// :1440-1488).
+int ReelectReference(const HostGrid& h, const std::vector<int>& seeds, const std::vector<uint8_t>& gone, int removedBus,
+                     int removedGen) {
+    std::vector<std::vector<int>> adj(h.n);
+    for (int k = 0; k < h.nbr; k++)
+        if (h.brOn[k] && !gone[k]) { adj[h.brF[k]].push_back(h.brT[k]); adj[h.brT[k]].push_back(h.brF[k]); }
+    std::vector<uint8_t> reach(h.n, 0);
+    std::vector<int> queue;
+    for (int x : seeds) if (x != removedBus && !reach[x]) { reach[x] = 1; queue.push_back(x); }
+    for (size_t q = 0; q < queue.size(); q++)
+        for (int v : adj[queue[q]])
+            if (v != removedBus && !reach[v]) { reach[v] = 1; queue.push_back(v); }
+    int best = -1;
+    for (int g = 0; g < h.ngen; g++) {
+        if (!h.genOn[g] || g == removedGen || h.genBus[g] == removedBus || !reach[h.genBus[g]]) continue;
+        if (best < 0 || std::fabs(h.pg[g]) > std::fabs(h.pg[best])) best = g;
+    }
+    return best < 0 ? -1 : h.genBus[best];
+}
+
+// The set point of bus i from its in-service units other than `removedGen` (the last one in model order sets it,
+// NewtonShell.BuildBusSpec); NaN when none is left.
+double SetPointOf(const HostGrid& h, int i, int removedGen) {
+    double vg = NAN;
+    for (int g = 0; g < h.ngen; g++)
+        if (h.genOn[g] && g != removedGen && h.genBus[g] == i) vg = h.vg[g];
+    return vg;
+}
+
+// The screen of a list of outages (empty: the intact grid, ScreenBaseCase; one branch: ScreenBranches; several:
+// ScreenOutageCore over several indices, ContingencyAnalysis.cs:1087-1097; a generator or a bus: ScreenElementOutage).
+int ScreenOutageLists(gs_grid* G, int nOut, const std::vector<Element>& els, const gs_pf_opts* opts,
                       gs_n1_result* res) {
     if (!G || !res || nOut < 0) return GS_ERR_INVALID_ARG;
     gs_ctx* ctx = G->ctx;
@@ -2640,15 +2792,22 @@ int ScreenOutageLists(gs_grid* G, int nOut, const std::vector<std::vector<int>>&
     if (rc) return rc;
     gs_pf_opts o = *opts;
     if (o.flat_start) return SetErr(ctx, GS_ERR_UNSUPPORTED, "flat_start: pass a flat start in the descriptor");
-    if (o.enforce_q_limits) {
+    bool anyElement = false;
+    for (const Element& e : els) anyElement = anyElement || e.gen >= 0 || e.bus >= 0;
+    // generator and bus outages change bus types: they run on the grid analysed with every bus's P and Q rows
+    if (o.enforce_q_limits || anyElement) {
         GS_CUDA(cudaSetDevice(ctx->device));
         if ((rc = QGridOf(G, &G)) != GS_OK) return rc;
     }
+    G->view.qlimOn = o.enforce_q_limits ? 1 : 0;
+    struct QlimRestore { gs_grid* g; ~QlimRestore() { g->view.qlimOn = g->view.qlim; } } qlimRestore{G};
     const Symbolic& s = G->sym;
     const HostGrid& h = G->host;
     // outage ids: -1, a branch, or nbr + the position of a multi-branch set in this call's table
     std::vector<int> ids(nOut, -1);
     OutageSetTable table;
+    std::vector<std::vector<int>> lists(nOut);
+    for (int k = 0; k < nOut; k++) lists[k] = els[k].branches;
     for (int k = 0; k < nOut; k++) {
         const std::vector<int>& b = lists[k];
         if ((int)b.size() > kSetBranches)
@@ -2664,9 +2823,62 @@ int ScreenOutageLists(gs_grid* G, int nOut, const std::vector<std::vector<int>>&
         ids[k] = b.empty() ? -1 : b.size() == 1 ? b[0] : s.nbr + AddOutageSet(s, b, table);
     }
     const int* idx = ids.data();
+    // element outages: bus type changes, lost output, a reference moved when its last unit goes (ReelectReference)
+    std::vector<ElemSys> elem(anyElement ? nOut : 0);
+    std::vector<ElementCut> cuts(anyElement ? nOut : 0);
+    std::vector<uint8_t> noReference(nOut, 0);
+    for (int k = 0; k < nOut && anyElement; k++) {
+        const Element& e = els[k];
+        ElemSys& x = elem[k];
+        ElementCut& c = cuts[k];
+        c.branches = e.branches;
+        c.gen = e.gen;
+        c.bus = e.bus;
+        const bool warmStart = o.warm_start_from_base != 0;
+        if (e.gen >= 0) {
+            if (e.gen >= h.ngen || !h.genOn[e.gen])
+                return SetErr(ctx, GS_ERR_INVALID_ARG, "generator " + std::to_string(e.gen) + " is not an in-service unit");
+            const int i = h.genBus[e.gen];
+            x.specBus = i;
+            x.dp = h.pg[e.gen] / h.base;
+            x.dq = h.qg[e.gen] / h.base;
+            int left = 0;
+            for (int g = 0; g < h.ngen; g++)
+                if (h.genOn[g] && g != e.gen && h.genBus[g] == i) { left++; x.qmin += h.qmin[g]; x.qmax += h.qmax[g]; }
+            const double vg = SetPointOf(h, i, e.gen);
+            if (s.type0[i] == 3 && left == 0) {  // the reference's last unit: the reference moves
+                const int j = ReelectReference(h, {i}, std::vector<uint8_t>(h.nbr, 0), -1, e.gen);
+                if (j < 0) { noReference[k] = 1; continue; }
+                x.ovBus[0] = i; x.ovType[0] = 1; x.ovVm[0] = warmStart ? NAN : h.vm[i];
+                x.ovBus[1] = j; x.ovType[1] = 3; x.ovVm[1] = SetPointOf(h, j, e.gen);
+                c.slackFrom = i;
+                c.slackTo = j;
+            } else if (s.type0[i] == 2 && left == 0) {  // a PV bus left with no unit is solved as PQ
+                x.ovBus[0] = i; x.ovType[0] = 1; x.ovVm[0] = warmStart ? NAN : h.vm[i];
+            } else if ((s.type0[i] == 2 || s.type0[i] == 3) && vg != s.vm0[i]) {  // the set point of the units left
+                x.ovBus[0] = i; x.ovType[0] = s.type0[i]; x.ovVm[0] = vg;
+            }
+        } else if (e.bus >= 0) {
+            x.ovBus[0] = e.bus; x.ovType[0] = 0;
+            if (s.type0[e.bus] == 3) {  // the reference bus itself: the reference moves, seen from its neighbours
+                std::vector<uint8_t> gone(h.nbr, 0);
+                std::vector<int> seeds;
+                for (int b : e.branches) {
+                    gone[b] = 1;
+                    seeds.push_back(h.brF[b] == e.bus ? h.brT[b] : h.brF[b]);
+                }
+                const int j = ReelectReference(h, seeds, gone, e.bus, -1);
+                if (j < 0) { noReference[k] = 1; continue; }
+                x.ovBus[1] = j; x.ovType[1] = 3; x.ovVm[1] = SetPointOf(h, j, -1);
+                c.slackFrom = e.bus;
+                c.slackTo = j;
+            }
+        }
+    }
     GS_CUDA(cudaSetDevice(ctx->device));
     if ((rc = InstallSets(G, table)) != GS_OK) return rc;
     struct Uninstall { gs_grid* g; ~Uninstall() { UninstallSets(g); } } uninstall{G};
+    struct OvOff { gs_grid* g; ~OvOff() { g->ws.ovOn = g->tws.ovOn = false; g->elemBatch.clear(); } } ovOff{G};
     const int n = s.n, nItems = s.nbr + h.nBnd + s.n;
     // the topology pass (ScreenStateCore :1118-1127): provably unsolvable states are reported without a solve,
     // and a state that does not converge says whether the outage split the network (:1661-1665)
@@ -2676,11 +2888,15 @@ int ScreenOutageLists(gs_grid* G, int nOut, const std::vector<std::vector<int>>&
         for (int k = 0; k < nOut; k++) single[k] = idx[k] < s.nbr ? idx[k] : -1;
         std::string terr = OutageTopology(h, o.tolerance, nOut, single.data(), splits.data(), unsolv.data());
         for (int k = 0; k < nOut && terr.empty(); k++) {
-            if (idx[k] < s.nbr) continue;
+            const bool isElement = anyElement && (els[k].gen >= 0 || els[k].bus >= 0);
+            if (idx[k] < s.nbr && !isElement) continue;
             bool sp = false, un = false;
-            terr = OutageSetTopology(h, o.tolerance, lists[k], sp, un);
+            ElementCut cut;
+            if (isElement) cut = cuts[k];
+            else cut.branches = lists[k];
+            terr = ElementTopology(h, o.tolerance, cut, sp, un);
             splits[k] = sp;
-            unsolv[k] = un;
+            unsolv[k] = un || noReference[k];  // no unit left to take the reference: not solved (:1370-1372)
         }
         if (!terr.empty()) return SetErr(ctx, GS_ERR_INVALID_ARG, terr);
     }
@@ -2748,6 +2964,12 @@ int ScreenOutageLists(gs_grid* G, int nOut, const std::vector<std::vector<int>>&
         std::vector<int> out(B, -1);
         for (int k = 0; k < cnt; k++) out[k] = idx[solvePos[done + k]];
         GS_CUDA(cudaMemcpy(w.outage.p, out.data(), B * 4, cudaMemcpyHostToDevice));
+        if (anyElement) {
+            G->elemBatch.assign(cnt, ElemSys());
+            for (int k = 0; k < cnt; k++) G->elemBatch[k] = elem[solvePos[done + k]];
+            if ((rc = UploadElements(G, G->ws, G->elemBatch)) != GS_OK) return rc;
+            G->ws.ovOn = G->tws.ovOn = true;
+        }
         float ms = 0;
         rc = NewtonDispatch(G, cnt, false, warm, o, &ms, &stats);
         if (rc) return rc;
@@ -2870,26 +3092,57 @@ extern "C" {
 
 int gs_n1_screen(gs_grid* G, int32_t nOut, const int32_t* idx, const gs_pf_opts* opts, gs_n1_result* res) {
     if (!G || !res || nOut < 0 || (nOut > 0 && !idx)) return GS_ERR_INVALID_ARG;
-    std::vector<std::vector<int>> lists(nOut);
+    std::vector<Element> lists(nOut);
     for (int k = 0; k < nOut; k++) {
         if (idx[k] < -1)
             return SetErr(G->ctx, GS_ERR_INVALID_ARG, "branch " + std::to_string(idx[k]) + " is not an in-service branch");
-        if (idx[k] >= 0) lists[k].push_back(idx[k]);
+        if (idx[k] >= 0) lists[k].branches.push_back(idx[k]);
     }
     return ScreenOutageLists(G, nOut, lists, opts, res);
 }
 
 int gs_nk_screen(gs_grid* G, int32_t nOut, int32_t k, const int32_t* sets, const gs_pf_opts* opts, gs_n1_result* res) {
     if (!G || !res || nOut < 0 || k < 1 || (nOut > 0 && !sets)) return GS_ERR_INVALID_ARG;
-    std::vector<std::vector<int>> lists(nOut);
+    std::vector<Element> lists(nOut);
     for (int j = 0; j < nOut; j++)
         for (int q = 0; q < k; q++) {
             const int b = sets[(size_t)j * k + q];
             if (b < -1)
                 return SetErr(G->ctx, GS_ERR_INVALID_ARG, "branch " + std::to_string(b) + " is not an in-service branch");
-            if (b >= 0) lists[j].push_back(b);
+            if (b >= 0) lists[j].branches.push_back(b);
         }
     return ScreenOutageLists(G, nOut, lists, opts, res);
+}
+
+int gs_element_screen(gs_grid* G, int32_t nOut, const int32_t* kind, const int32_t* index, const gs_pf_opts* opts,
+                      gs_n1_result* res) {
+    if (!G || !res || nOut < 0 || (nOut > 0 && (!kind || !index))) return GS_ERR_INVALID_ARG;
+    const HostGrid& h = G->host;
+    std::vector<Element> els(nOut);
+    for (int j = 0; j < nOut; j++) {
+        const int x = index[j];
+        switch (kind[j]) {
+            case GS_OUTAGE_BRANCH:
+                if (x < 0 || x >= h.nbr || !h.brOn[x])
+                    return SetErr(G->ctx, GS_ERR_INVALID_ARG, "branch " + std::to_string(x) + " is not an in-service branch");
+                els[j].branches.push_back(x);
+                break;
+            case GS_OUTAGE_GENERATOR:
+                if (x < 0 || x >= h.ngen || !h.genOn[x])
+                    return SetErr(G->ctx, GS_ERR_INVALID_ARG, "generator " + std::to_string(x) + " is not an in-service unit");
+                els[j].gen = x;
+                break;
+            case GS_OUTAGE_BUS:
+                if (x < 0 || x >= h.n) return SetErr(G->ctx, GS_ERR_INVALID_ARG, "bus position " + std::to_string(x) + " is out of range");
+                els[j].bus = x;
+                for (int k = 0; k < h.nbr; k++)  // the bus goes with every branch touching it (:1393-1399)
+                    if (h.brOn[k] && (h.brF[k] == x || h.brT[k] == x)) els[j].branches.push_back(k);
+                break;
+            default:
+                return SetErr(G->ctx, GS_ERR_INVALID_ARG, "unknown outage kind " + std::to_string(kind[j]));
+        }
+    }
+    return ScreenOutageLists(G, nOut, els, opts, res);
 }
 
 }  // extern "C"

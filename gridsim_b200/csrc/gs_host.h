@@ -13,7 +13,12 @@ void FillInfo(const HostGrid& g, const Symbolic& s, gs_grid_info* info);
 // Either output may be null; empty string on success.
 std::string OutageTopology(const HostGrid& h, double tol, int nOut, const int* idx, uint8_t* splits,
                            uint8_t* unsolvable);
-// The same verdicts for one multi-branch outage (every branch in `removed` out at once).
-std::string OutageSetTopology(const HostGrid& h, double tol, const std::vector<int>& removed, bool& splits,
-                              bool& unsolvable);
+// An element outage for the topology verdicts: branches out, a unit out (-1 none), a bus out (-1 none; its branches
+// listed too), and the reference moved from one bus to another (-1 none) when the outage took its last unit.
+struct ElementCut {
+    std::vector<int> branches;
+    int gen = -1, bus = -1, slackFrom = -1, slackTo = -1;
+};
+// The same verdicts for one element outage (several branches, a unit, a bus).
+std::string ElementTopology(const HostGrid& h, double tol, const ElementCut& e, bool& splits, bool& unsolvable);
 }  // namespace gs

@@ -1,6 +1,7 @@
 // gs_internal.h — host-side data of the gridsim_b200 engine (not part of the C ABI).
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <string>
 #include <functional>
@@ -146,14 +147,15 @@ std::string AnalyzeMatrix(int n, const int* rowPtr, const int* colIdx, Symbolic&
 
 // DC power-flow angles (degrees) of the grid with the branches `skip` out, referenced at bus `slack`, with the
 // loads scaled by loadScale[i] (may be null); false unless the DC model is one island (gs_dc.cpp).
+// For an element outage, `deadBus` is a removed bus (-1 none) and bus `specBus` (-1 none) loses specDpPu of generation.
 bool DcAngles(const HostGrid& h, const Symbolic& s, const std::vector<int>& skip, int slack, const double* loadScale,
-              std::vector<double>& thetaDeg);
+              std::vector<double>& thetaDeg, int deadBus = -1, int specBus = -1, double specDpPu = 0.0);
 
 // Multi-branch outages (ContingencyAnalysis.ScreenOutageCore over several indices, :1087-1097). A set's outage id
 // is nbr + its position in the table; one branch keeps its own index (the N-1 path). Per set: its branches (-1
 // padded), the distinct Y cells they touch in ascending order (an INT_MAX sentinel after the last), and each cell's
 // value summed without every branch of the set, in stamping order.
-constexpr int kSetBranches = 4;
+constexpr int kSetBranches = 16;  // a bus outage takes every branch at the bus
 constexpr int kSetStride = 4 * kSetBranches + 1;
 struct OutageSetTable {
     int n = 0;
@@ -161,6 +163,18 @@ struct OutageSetTable {
     std::vector<int> cell;    // [n * kSetStride]
     std::vector<double> red;  // [n * 2 * kSetStride] (G, B) per cell
 };
+// The per-system changes of an element outage (a generator or a bus, ScreenElementOutage,
+// Analysis/ContingencyAnalysis.cs:1355-1437): up to two buses whose type changes (3 reference, 2 PV, 1 PQ, 0 removed)
+// with the magnitude they hold or start from (NaN: as the grid), the bus that loses a unit with the lost output (pu)
+// and the Q limits of its remaining units (MVAr).
+struct ElemSys {
+    int ovBus[2] = {-1, -1};
+    int ovType[2] = {0, 0};
+    double ovVm[2] = {NAN, NAN};
+    int specBus = -1;
+    double dp = 0.0, dq = 0.0, qmin = 0.0, qmax = 0.0;
+};
+
 // Append the set of in-service branches `b` (2..kSetBranches distinct indices); returns its position.
 int AddOutageSet(const Symbolic& s, const std::vector<int>& b, OutageSetTable& t);
 

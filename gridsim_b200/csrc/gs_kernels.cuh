@@ -51,7 +51,8 @@ struct DevGrid {
     int n, m, nnzY, nbr;
     int64_t nnzLU;
     int nLevels;          // elimination-tree levels of the schedules
-    int qlim;             // Q-limit enforcement: PV buses have a Q equation (an identity row while PV)
+    int qlim;             // every bus has P and Q rows (identity rows where the bus is PV, reference or removed)
+    int qlimOn;           // with qlim: PV buses switch to PQ at their Q limits (Q-limit enforcement)
     double baseMva;
     const double* qminPu; // aggregate reactive limits per bus (pu)
     const double* qmaxPu;
@@ -162,6 +163,17 @@ struct DevBatch {
     int* passIter;          // [B] steps of the current Q-limit pass
     int* qPass;             // [B] passes completed
     int* qState;            // [B] kQ* bits
+    // element outages (grids with qlim: every bus has P and Q rows), else null: per system up to two buses whose
+    // type changes (3 reference, 2 PV, 1 PQ, 0 removed) with the magnitude they start from or hold (NaN: as the
+    // grid), and the bus that loses units with the generation it loses (pu) and its remaining Q limits (MVAr)
+    const int* ovBus;       // [2B] bus or -1
+    const int* ovType;      // [2B]
+    const double* ovVm;     // [2B]
+    const int* specBus;     // [B] bus or -1
+    const double* specDp;   // [B]
+    const double* specDq;   // [B]
+    const double* specQmin; // [B]
+    const double* specQmax; // [B]
 };
 
 // qState bits
@@ -198,8 +210,7 @@ struct CellOverride {
 __device__ __forceinline__ bool branchOut(const DevGrid& g, int o, int k) {
     if (o < g.nbr) return o == k;
     const int* br = g.setBr + (size_t)kSetBranches * (o - g.nbr);
-#pragma unroll
-    for (int j = 0; j < kSetBranches; j++)
+    for (int j = 0; j < kSetBranches && br[j] >= 0; j++)  // -1 after the last
         if (br[j] == k) return true;
     return false;
 }

@@ -209,10 +209,14 @@ std::string Analyze(const HostGrid& g, Symbolic& s, bool qlim) {
     s.pPos.assign(n, -1);
     s.qPos.assign(n, -1);
     int m = 0;
-    for (int i = 0; i < n; i++) if (s.type0[i] != 3) s.pPos[i] = m++;
-    // with Q limits every PV bus may become PQ: its Q equation is in the pattern (an identity row while PV)
-    for (int i = 0; i < n; i++)
-        if (s.type0[i] == 1 || (qlim && s.type0[i] == 2)) { s.qPos[i] = m++; if (s.type0[i] == 1) s.npq++; }
+    // with qlim every bus has both rows: a PV bus may become PQ (Q limits, a generator outage), a reference bus may
+    // lose its units and the reference move, a bus may be removed; a row that is not an equation in a system is an
+    // identity row there
+    for (int i = 0; i < n; i++) if (qlim || s.type0[i] != 3) s.pPos[i] = m++;
+    for (int i = 0; i < n; i++) {
+        if (s.type0[i] == 1) s.npq++;
+        if (qlim || s.type0[i] == 1) s.qPos[i] = m++;
+    }
     for (int i = 0; i < n; i++) if (s.type0[i] == 2) s.npv++;
     s.m = m;
     if (m == 0) return "the grid has no unknowns";

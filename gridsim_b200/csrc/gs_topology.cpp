@@ -208,24 +208,27 @@ std::string OutageTopology(const HostGrid& h, double tol, int nOut, const int* i
     return "";
 }
 
-// The same two verdicts for the grid without every branch in `removed` (a multi-branch outage), by one union-find
-// over the remaining in-service branches: O(buses + branches) per outage.
-std::string OutageSetTopology(const HostGrid& h, double tol, const std::vector<int>& removed, bool& splits,
-                              bool& unsolvable) {
+// The same two verdicts for an element outage (ScreenElementOutage, :1355-1437): the grid without the branches
+// e.branches, without unit e.gen (its output lost), without bus e.bus (its branches are among e.branches), and with
+// the reference moved from e.slackFrom to e.slackTo where the outage took the reference's last unit (ReelectReference
+// :1440-1488). One union-find over the remaining in-service branches: O(buses + branches) per outage.
+std::string ElementTopology(const HostGrid& h, double tol, const ElementCut& e, bool& splits, bool& unsolvable) {
     const int n = h.n, nb = h.nbr;
     splits = unsolvable = false;
     std::vector<uint8_t> gone(nb, 0);
-    for (int k : removed) {
+    for (int k : e.branches) {
         if (k < 0 || k >= nb) return "outage index out of range";
         gone[k] = 1;
     }
+    if (e.bus >= n || e.gen >= h.ngen) return "outage index out of range";
     std::vector<int> parent(n), partsAt(2, n);
     auto find = [&](int x) { while (parent[x] != x) { parent[x] = parent[parent[x]]; x = parent[x]; } return x; };
-    for (int pass = 0; pass < 2; pass++) {  // 0: the intact grid, 1: without the set
+    partsAt[1] = n - (e.bus >= 0 ? 1 : 0);  // a removed bus is not a part of the reduced model
+    for (int pass = 0; pass < 2; pass++) {  // 0: the intact grid, 1: the reduced one
         for (int i = 0; i < n; i++) parent[i] = i;
-        for (int e = 0; e < nb; e++) {
-            if (!h.brOn[e] || (pass == 1 && gone[e])) continue;
-            const int a = find(h.brF[e]), c = find(h.brT[e]);
+        for (int k = 0; k < nb; k++) {
+            if (!h.brOn[k] || (pass == 1 && gone[k])) continue;
+            const int a = find(h.brF[k]), c = find(h.brT[k]);
             if (a != c) { parent[a] = c; partsAt[pass]--; }
         }
     }
@@ -235,28 +238,30 @@ std::string OutageSetTopology(const HostGrid& h, double tol, const std::vector<i
     {
         std::unordered_set<int> ids;
         for (int i = 0; i < n; i++)
-            if (!ids.insert(h.busId[i]).second) return "";
+            if (i != e.bus && !ids.insert(h.busId[i]).second) return "";
     }
     std::vector<double> pgBus(n, 0.0);
     for (int g = 0; g < h.ngen; g++)
-        if (h.genOn[g]) pgBus[h.genBus[g]] += h.pg[g];
+        if (h.genOn[g] && g != e.gen && h.genBus[g] != e.bus) pgBus[h.genBus[g]] += h.pg[g];
     std::vector<int> count(n, 0), slack(n, 0), lossy(n, 0), neg(n, 0);
     std::vector<double> net(n, 0.0);
     for (int i = 0; i < n; i++) {
+        if (i == e.bus) continue;
         if (!std::isfinite(h.gsh[i]) || !std::isfinite(h.pd[i]) || !std::isfinite(pgBus[i])) return "";
         const int r = find(i);
+        const bool isSlack = (h.busType[i] == 3 && i != e.slackFrom) || i == e.slackTo;
         count[r]++;
-        slack[r] += h.busType[i] == 3;
+        slack[r] += isSlack;
         lossy[r] += h.gsh[i] != 0.0;
         neg[r] += h.gsh[i] < 0.0;
         net[r] += (pgBus[i] - h.pd[i]) / h.base;  // bus order within each part
     }
-    for (int e = 0; e < nb; e++) {
-        if (!h.brOn[e] || gone[e]) continue;
-        if (!std::isfinite(h.r[e])) return "";
-        const int r = find(h.brF[e]);
-        lossy[r] += h.r[e] != 0.0;
-        neg[r] += h.r[e] < 0.0;
+    for (int k = 0; k < nb; k++) {
+        if (!h.brOn[k] || gone[k]) continue;
+        if (!std::isfinite(h.r[k])) return "";
+        const int r = find(h.brF[k]);
+        lossy[r] += h.r[k] != 0.0;
+        neg[r] += h.r[k] < 0.0;
     }
     for (int r = 0; r < n && !unsolvable; r++) {
         if (count[r] == 0 || slack[r] > 0 || neg[r] > 0) continue;

@@ -396,6 +396,10 @@ class ContingencyResult:
     pre_existing_violations: list = field(default_factory=list)
     worsened_pre_existing_violations: list = field(default_factory=list)
     islanded: bool = False  # not converged, and the outage split the network (:1661-1665)
+    kind: int = 0           # OutageKind: 0 branch, 1 generator, 2 bus
+    lost_load_mw: float = 0.0
+    lost_generation_mw: float = 0.0
+    note: Optional[str] = None
 
     @property
     def secure(self) -> bool:
@@ -466,6 +470,16 @@ class ContingencyAnalysis:
         return ContingencyAnalysis._screen_call(model, sets, sets.shape[1], solver, options, keep_states)
 
     @staticmethod
+    def screen_elements_raw(model: GridModel, kinds: Sequence[int], indices: Sequence[int],
+                            solver: SparseNewtonRaphsonPowerFlow, options: PowerFlowOptions,
+                            keep_states: bool = False) -> dict:
+        """One ``gs_element_screen`` call: outage j is the branch / generator / bus indices[j] of kinds[j] (0, 1, 2);
+        generator indices are positions in the model's generator arrays, bus indices bus positions."""
+        k = np.ascontiguousarray(kinds, dtype=np.int32)
+        idx = np.ascontiguousarray(indices, dtype=np.int32)
+        return ContingencyAnalysis._screen_call(model, idx, ("elements", k), solver, options, keep_states)
+
+    @staticmethod
     def _screen_call(model, idx, width, solver, options, keep_states):
         g = solver.grid_for(model)
         k = idx.shape[0]
@@ -489,13 +503,16 @@ class ContingencyAnalysis:
             c = options.to_c()
             if width is None:
                 rc = g.ctx.lib.gs_n1_screen(g.handle, k, _p(idx), ctypes.byref(c), ctypes.byref(r))
+            elif isinstance(width, tuple):
+                rc = g.ctx.lib.gs_element_screen(g.handle, k, _p(width[1]), _p(idx), ctypes.byref(c), ctypes.byref(r))
             else:
                 rc = g.ctx.lib.gs_nk_screen(g.handle, k, width, _p(idx), ctypes.byref(c), ctypes.byref(r))
             if rc == _abi.GS_ERR_CAPACITY:
                 cap = r.viol_count + 64
                 g.viol_per_outage = max(getattr(g, "viol_per_outage", 0), r.viol_count / max(k, 1))
                 continue
-            g.ctx.check(rc, "gs_n1_screen" if width is None else "gs_nk_screen")
+            g.ctx.check(rc, "gs_n1_screen" if width is None else
+                        "gs_element_screen" if isinstance(width, tuple) else "gs_nk_screen")
             break
         nv = r.viol_count
         for key in ("viol_kind", "viol_element", "viol_value"):
@@ -668,6 +685,89 @@ class ContingencyAnalysis:
                          exhaustive: bool = False) -> list:
         """ScreenNMinus2 (:356-360)."""
         return cls.screen_n_minus_k(model, 2, solver, options, candidate_count, exhaustive)
+
+    @staticmethod
+    def single_outages(model: GridModel, branches: bool = True, generators: bool = False,
+                       buses: bool = False) -> list:
+        """SingleOutages (:1294-1302): (kind, index) for every branch (branch order), then every in-service generator
+        (model order; the index is its position among the in-service units, as GridModel.Generators), then every
+        bus (model order)."""
+        out = []
+        if branches:
+            out += [(0, k) for k in range(model.n_branch)]
+        if generators:
+            out += [(1, k) for k in range(int(np.sum(model.gen_in_service != 0)))]
+        if buses:
+            out += [(2, i) for i in range(model.n_bus)]
+        return out
+
+    @staticmethod
+    def _reelect(model: GridModel, removed_gen: int, removed_bus: int, affected: int):
+        """ReelectReference (:1440-1488) for the note: (new reference bus position or None, note text or None)."""
+        if model.bus_type[affected] != 3:
+            return None, None
+        on = np.nonzero(model.gen_in_service)[0]
+        units = [g for g in on if g != removed_gen and int(model.gen_bus[g]) != removed_bus]
+        if removed_bus < 0 and any(int(model.gen_bus[g]) == affected for g in units):
+            return None, None
+        adj = [[] for _ in range(model.n_bus)]
+        for k in np.nonzero(model.br_in_service)[0]:
+            f, t = int(model.br_from[k]), int(model.br_to[k])
+            if removed_bus in (f, t):
+                continue
+            adj[f].append(t)
+            adj[t].append(f)
+        if removed_bus < 0:
+            seeds = [affected]
+        else:
+            seeds = [int(model.br_to[k]) if int(model.br_from[k]) == removed_bus else int(model.br_from[k])
+                     for k in np.nonzero(model.br_in_service)[0] if removed_bus in (int(model.br_from[k]), int(model.br_to[k]))]
+        reach, queue = set(seeds), list(seeds)
+        while queue:
+            u = queue.pop(0)
+            for v in adj[u]:
+                if v != removed_bus and v not in reach:
+                    reach.add(v)
+                    queue.append(v)
+        best = None
+        for g in units:
+            if int(model.gen_bus[g]) in reach and (best is None or abs(model.pg[g]) > abs(model.pg[best])):
+                best = g
+        aid = int(model.bus_id[affected])
+        if best is None:
+            return None, f"no in-service unit is left to take over the reference of bus {aid}"
+        return int(model.gen_bus[best]), f"reference moved from bus {aid} to bus {int(model.bus_id[model.gen_bus[best]])}"
+
+    @classmethod
+    def screen_element_outages(cls, model: GridModel, outages: Sequence, solver: Optional[SparseNewtonRaphsonPowerFlow] = None,
+                               options: Optional[PowerFlowOptions] = None) -> list:
+        """ScreenElementOutages (:1309-1320) with the reference-bus dispatch: one device call for every (kind, index)
+        of `outages` (SingleOutages' indexing), results in order with the reference's labels ("gen 3 at bus 7",
+        "bus 7"), lost load and generation and the reference-move note."""
+        solver = solver or SparseNewtonRaphsonPowerFlow()
+        options = options or PowerFlowOptions(precision=solver.precision)
+        on = np.nonzero(model.gen_in_service)[0]
+        kinds = np.array([int(k) for k, _ in outages], np.int32)
+        idx = np.array([int(on[i]) if k == 1 else int(i) for k, i in outages], np.int32)
+        raw = cls.screen_elements_raw(model, kinds, idx, solver, options)
+        res = []
+        for j, (k, i) in enumerate(outages):
+            r = cls._results(model, [int(idx[j]) if k == 0 else -1], {key: (v[j:j + 1] if key in (
+                "status", "iterations", "max_mismatch", "max_loading_pct", "worst_boundary_pct", "min_vm", "max_vm",
+                "islanded") else v) for key, v in raw.items()} | {"viol_ptr": raw["viol_ptr"][j:j + 2]})[0]
+            if k == 1:
+                g = int(idx[j])
+                bus = int(model.gen_bus[g])
+                r.outage = f"gen {i} at bus {int(model.bus_id[bus])}"
+                r.kind, r.lost_generation_mw = 1, float(model.pg[g])
+                r.note = cls._reelect(model, g, -1, bus)[1]
+            elif k == 2:
+                r.outage = f"bus {int(model.bus_id[i])}"
+                r.kind, r.lost_load_mw = 2, float(model.pd[i])
+                r.lost_generation_mw = float(sum(model.pg[g] for g in on if int(model.gen_bus[g]) == i))
+                r.note = cls._reelect(model, -1, int(i), int(i))[1]
+            res.append(r)
+        return res
 
     @classmethod
     def net_against_base(cls, model: GridModel, outage: ContingencyResult, base: ContingencyResult,

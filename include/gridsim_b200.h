@@ -275,11 +275,26 @@ int gs_n1_screen(gs_grid *grid, int32_t n_out, const int32_t *branch_idx, const 
 
 /* Multi-branch outages (ScreenOutageCore over several indices, Analysis/ContingencyAnalysis.cs:1087-1097; the
  * N-k screens ScreenNMinusK :378-426 enumerate them): outage j takes out every branch branch_sets[j*k .. j*k+k-1]
- * that is not -1 (at most 4, distinct, in service; none = the intact grid). The Y cells each set touches get their
+ * that is not -1 (at most 16, distinct, in service; none = the intact grid). The Y cells each set touches get their
  * values without every branch of the set, summed in stamping order; everything else (topology pass, Newton solve,
  * retry, classification, result layout) is gs_n1_screen's, which is the k = 1 case. */
 int gs_nk_screen(gs_grid *grid, int32_t n_out, int32_t k, const int32_t *branch_sets, const gs_pf_opts *opts,
                  gs_n1_result *res);
+
+/* Single-element outages (ContingencyAnalysis.ScreenElementOutages / ScreenElementOutage,
+ * Analysis/ContingencyAnalysis.cs:1309-1437): outage j takes out the branch, the generator (a position in the
+ * generator arrays; the unit must be in service) or the bus (a position in the bus arrays) index[j] of kind[j].
+ * A generator outage loses the unit's output, picked up by the reference bus; a PV bus left with no unit is solved
+ * as PQ. A bus outage removes the bus with every branch touching it, its units and its load. When the outage takes
+ * the reference bus or its last unit, the reference moves to the bus of the largest remaining unit by |Pg| in the
+ * part the reference served (ReelectReference :1440-1488); with no unit there, the outage is reported
+ * GS_PF_UNSOLVABLE_PART. These run on the grid analysed with every bus's P and Q rows (identity rows where a bus is
+ * PV, the reference or removed in a system). Results as gs_n1_screen; a removed bus is left out of Vmin / Vmax and
+ * of the voltage violations, its vm / va_deg entries are the start values. Only the reference-bus dispatch
+ * (OutageDispatch.ReferenceBus, the default) is built. */
+enum gs_outage_kind { GS_OUTAGE_BRANCH = 0, GS_OUTAGE_GENERATOR = 1, GS_OUTAGE_BUS = 2 };
+int gs_element_screen(gs_grid *grid, int32_t n_out, const int32_t *kind, const int32_t *index, const gs_pf_opts *opts,
+                      gs_n1_result *res);
 
 /* ---- batched sparse linear solve: ISparseLinearSolver.Solve (Abstractions/ISparseLinearSolver.cs:12-17) and
  *      IBatchedSparseLinearSolver.SolveBatch (Abstractions/IBatchedSparseLinearSolver.cs:19-37) ----------------

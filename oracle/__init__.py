@@ -42,6 +42,8 @@ def _load():
         lib.gso_md_order.argtypes = [i32, vp, vp, vp]
         lib.gso_nk_screen.argtypes = [ctypes.POINTER(_abi.GridDesc), i32, i32, vp, ctypes.POINTER(_abi.PfOpts), i32,
                                       ctypes.POINTER(_abi.N1Result)]
+        lib.gso_element_screen.argtypes = [ctypes.POINTER(_abi.GridDesc), i32, vp, vp, ctypes.POINTER(_abi.PfOpts), i32,
+                                           ctypes.POINTER(_abi.N1Result)]
         lib.gso_outage_topology.argtypes = [ctypes.POINTER(_abi.GridDesc), ctypes.c_double, i32, vp, vp, vp]
         lib.gso_sparse_solve.argtypes = [i32, vp, vp, vp, vp, vp]
         _lib = lib
@@ -83,6 +85,12 @@ def screen_sets(model, sets, opts=None, threads: int = 0, keep_states: bool = Fa
     return _screen(model, sets, sets.shape[1], opts, threads, keep_states)
 
 
+def screen_elements(model, kinds, indices, opts=None, threads: int = 0, keep_states: bool = False) -> dict:
+    """ScreenElementOutages: outage j is the branch / generator / bus indices[j] of kinds[j] (0, 1, 2)."""
+    k = np.ascontiguousarray(kinds, dtype=np.int32)
+    return _screen(model, np.ascontiguousarray(indices, dtype=np.int32), ("elements", k), opts, threads, keep_states)
+
+
 def _screen(model, idx, width, opts, threads, keep_states):
     lib = _load()
     o = opts or _abi.default_opts()
@@ -105,6 +113,9 @@ def _screen(model, idx, width, opts, threads, keep_states):
         d = model.desc()
         if width is None:
             rc = lib.gso_n1_screen(ctypes.byref(d), k, _p(idx), ctypes.byref(o), threads, ctypes.byref(r))
+        elif isinstance(width, tuple):
+            rc = lib.gso_element_screen(ctypes.byref(d), k, _p(width[1]), _p(idx), ctypes.byref(o), threads,
+                                        ctypes.byref(r))
         else:
             rc = lib.gso_nk_screen(ctypes.byref(d), k, width, _p(idx), ctypes.byref(o), threads, ctypes.byref(r))
         if rc == _abi.GS_ERR_CAPACITY:

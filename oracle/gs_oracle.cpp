@@ -51,6 +51,7 @@ struct Model {
     std::vector<int> id, type;  // 1 PQ, 2 PV, 3 slack
     std::vector<double> pd, qd, gs, bs, vm, vaDeg, vmin, vmax;
     std::vector<Gen> gens;      // in-service units only (GridModel.Generators)
+    std::vector<int> genOfDesc; // descriptor unit -> position in gens (-1: out of service)
     std::vector<Br> br;         // GridModel.Branches order
     std::vector<Bnd> bnd;
 };
@@ -72,8 +73,10 @@ Model FromDesc(const gs_grid_desc* d) {
     m.vmax.assign(m.n, nan);
     if (d->vmin_pu) m.vmin.assign(d->vmin_pu, d->vmin_pu + m.n);
     if (d->vmax_pu) m.vmax.assign(d->vmax_pu, d->vmax_pu + m.n);
+    m.genOfDesc.assign(d->n_gen, -1);
     for (int g = 0; g < d->n_gen; g++) {
         if (d->gen_in_service && !d->gen_in_service[g]) continue;
+        m.genOfDesc[g] = (int)m.gens.size();
         m.gens.push_back({d->gen_bus[g], d->pg[g], d->qg[g], d->vg[g], d->qmin[g], d->qmax[g]});
     }
     for (int k = 0; k < d->n_branch; k++) {
@@ -1036,7 +1039,7 @@ struct Violation { int kind, element; double value; };
 // VoltageLimits.cs:28-31).
 void Classify(const Model& m, int skip, bool postFault, const std::vector<double>& vm, const std::vector<double>& va,
               bool perBus, int postRating, double& maxLoad, double& worstBnd, double& minVm, double& maxVm,
-              std::vector<Violation>& out) {
+              std::vector<Violation>& out, const std::vector<int>* original = nullptr) {
     const int nb = (int)m.br.size();
     std::vector<double> loading(nb), sf(2 * (size_t)nb), st(2 * (size_t)nb);
     LineFlows(m, skip, vm, va, loading.data(), sf.data(), st.data());
@@ -1052,7 +1055,8 @@ void Classify(const Model& m, int skip, bool postFault, const std::vector<double
             }
         }
         if (l > maxLoad) maxLoad = l;
-        if (l > 100.0) out.push_back({GS_VIOL_BRANCH_OVERLOAD, k, l});
+        if (l > 100.0) out.push_back({GS_VIOL_BRANCH_OVERLOAD, original ? (*original)[k] : k, l});  // keyed by the
+                                                                                                  // original index
     }
     worstBnd = 0;
     for (int q = 0; q < (int)m.bnd.size(); q++) {
@@ -1144,6 +1148,101 @@ bool ProvablyUnsolvablePart(const Model& m, int skip, double tol) {
         if (!anyLoss[r] && std::fabs(net[r]) >= slack) return true;
     }
     return false;
+}
+
+// ScreenElementOutage (ContingencyAnalysis.cs:1355-1437): the reduced model of one element outage, built as the
+// reference builds it. kind 1: the in-service unit `index` (a descriptor position) goes; kind 2: bus `index` goes with
+// every branch touching it, its units and its load (the buses after it move up one position). When the outage takes
+// a reference bus or its last unit, ReelectReference (:1440-1488) moves the reference to the bus of the largest
+// remaining unit by |Pg| (first in model order) in the part the reference served; `noReference` when none is left.
+// original[k] = the full model's index of the reduced model's branch k; busOf[i] = the reduced position of bus i
+// (-1: removed).
+struct Reduced {
+    Model m;
+    std::vector<int> original, busOf;
+    bool noReference = false;
+};
+
+Reduced ReduceForElement(const Model& m, int kind, int index) {
+    Reduced r;
+    r.m = m;
+    const int n = m.n;
+    r.busOf.resize(n);
+    std::iota(r.busOf.begin(), r.busOf.end(), 0);
+    r.original.resize(m.br.size());
+    std::iota(r.original.begin(), r.original.end(), 0);
+    int affected = -1, removedBus = -1;
+    if (kind == 1) {
+        const int gi = m.genOfDesc[index];
+        affected = m.gens[gi].bus;
+        r.m.gens.erase(r.m.gens.begin() + gi);
+    } else {
+        removedBus = affected = index;
+    }
+    // ReelectReference on the full model's buses (positions), before any renumbering
+    if (m.type[affected] == 3) {
+        bool left = false;
+        for (const Gen& g : r.m.gens) if (g.bus == affected && removedBus < 0) left = true;
+        if (!left) {
+            std::vector<std::vector<int>> adj(n);
+            for (size_t k = 0; k < m.br.size(); k++)
+                if (m.br[k].inService && m.br[k].f != removedBus && m.br[k].t != removedBus) {
+                    adj[m.br[k].f].push_back(m.br[k].t);
+                    adj[m.br[k].t].push_back(m.br[k].f);
+                }
+            std::vector<int> seeds;
+            if (removedBus < 0) seeds.push_back(affected);
+            else
+                for (const Br& b : m.br)
+                    if (b.inService && (b.f == removedBus || b.t == removedBus)) seeds.push_back(b.f == removedBus ? b.t : b.f);
+            std::vector<char> reach(n, 0);
+            std::vector<int> queue;
+            for (int x : seeds) if (!reach[x]) { reach[x] = 1; queue.push_back(x); }
+            for (size_t q = 0; q < queue.size(); q++)
+                for (int v : adj[queue[q]]) if (v != removedBus && !reach[v]) { reach[v] = 1; queue.push_back(v); }
+            const Gen* best = nullptr;
+            for (const Gen& g : r.m.gens)
+                if (g.bus != removedBus && reach[g.bus] && (!best || std::fabs(g.pg) > std::fabs(best->pg))) best = &g;
+            if (!best) { r.noReference = true; return r; }
+            if (removedBus < 0) r.m.type[affected] = 1;
+            if (r.m.type[best->bus] != 3) r.m.type[best->bus] = 3;
+        }
+    }
+    if (removedBus >= 0) {  // the bus, its branches and its units leave the model
+        Model red;
+        red.n = n - 1;
+        red.base = m.base;
+        for (int i = 0, j = 0; i < n; i++) {
+            if (i == removedBus) { r.busOf[i] = -1; continue; }
+            r.busOf[i] = j++;
+            red.id.push_back(r.m.id[i]); red.type.push_back(r.m.type[i]);
+            red.pd.push_back(m.pd[i]); red.qd.push_back(m.qd[i]); red.gs.push_back(m.gs[i]); red.bs.push_back(m.bs[i]);
+            red.vm.push_back(m.vm[i]); red.vaDeg.push_back(m.vaDeg[i]);
+            red.vmin.push_back(m.vmin[i]); red.vmax.push_back(m.vmax[i]);
+        }
+        for (const Gen& g : r.m.gens)
+            if (g.bus != removedBus) { Gen h = g; h.bus = r.busOf[g.bus]; red.gens.push_back(h); }
+        r.original.clear();
+        std::vector<int> newIndex(m.br.size(), -1);
+        for (size_t k = 0; k < m.br.size(); k++) {
+            const Br& b = m.br[k];
+            if (b.f == removedBus || b.t == removedBus) continue;
+            Br c = b;
+            c.f = r.busOf[b.f];
+            c.t = r.busOf[b.t];
+            newIndex[k] = (int)red.br.size();
+            red.br.push_back(c);
+            r.original.push_back((int)k);
+        }
+        for (const Bnd& b : m.bnd) {  // a boundary member that went with the bus contributes nothing
+            Bnd c{b.limitMw, {}};
+            for (const auto& mem : b.members)
+                if (newIndex[mem.first] >= 0) c.members.push_back({newIndex[mem.first], mem.second});
+            red.bnd.push_back(c);
+        }
+        r.m = std::move(red);
+    }
+    return r;
 }
 
 bool OptionsSupported(const gs_pf_opts* o) { return o != nullptr; }
@@ -1353,6 +1452,114 @@ int gso_nk_screen(const gs_grid_desc* d, int32_t nOut, int32_t k, const int32_t*
             if (b >= 0) lists[j].push_back(b);
         }
     return ScreenLists(m, lists, opt, threads, res);
+}
+
+// ScreenElementOutages (ContingencyAnalysis.cs:1309-1437) with the reference-bus dispatch: outage j is the branch,
+// unit or bus index[j] of kind[j] (0, 1, 2). Results in gs_n1_result's layout over the full model's buses; a removed
+// bus's state entries are 0 and it is in neither Vmin / Vmax nor the voltage violations.
+int gso_element_screen(const gs_grid_desc* d, int32_t nOut, const int32_t* kind, const int32_t* index,
+                       const gs_pf_opts* opt, int32_t threads, gs_n1_result* res) {
+    if (!d || !res || !OptionsSupported(opt) || nOut < 0) return GS_ERR_INVALID_ARG;
+    Model m = FromDesc(d);
+    for (int j = 0; j < nOut; j++) {
+        if (kind[j] == 0 && (index[j] < 0 || index[j] >= (int)m.br.size() || !m.br[index[j]].inService)) return GS_ERR_INVALID_ARG;
+        if (kind[j] == 1 && (index[j] < 0 || index[j] >= (int)m.genOfDesc.size() || m.genOfDesc[index[j]] < 0)) return GS_ERR_INVALID_ARG;
+        if (kind[j] == 2 && (index[j] < 0 || index[j] >= m.n)) return GS_ERR_INVALID_ARG;
+        if (kind[j] < 0 || kind[j] > 2) return GS_ERR_INVALID_ARG;
+    }
+    std::vector<double> vm0, va0;
+    res->base_status = GS_PF_NOT_RUN;
+    res->base_iterations = 0;
+    if (opt->warm_start_from_base) {
+        SolveOut b = SolveWithRetry(m, -1, *opt, nullptr, nullptr);
+        res->base_status = b.status;
+        res->base_iterations = b.iterations;
+        vm0 = b.vm;
+        va0 = b.va;
+    }
+    const int n = m.n;
+    std::vector<SolveOut> outs(nOut);
+    std::vector<std::vector<Violation>> viol(nOut);
+    std::vector<double> maxLoad(nOut, 0), worstBnd(nOut, 0), minVm(nOut, 0), maxVm(nOut, 0);
+    std::vector<uint8_t> islanded(nOut, 0);
+    std::vector<std::vector<int>> busOf(nOut);
+    const int partsBefore = ConnectedParts(m, -1);
+    std::atomic<int> cursor{0};
+    auto work = [&]() {
+        for (;;) {
+            const int j = cursor.fetch_add(1);
+            if (j >= nOut) return;
+            Reduced r;
+            int skip = -1;
+            if (kind[j] == 0) {
+                r.m = m;
+                r.busOf.resize(n);
+                std::iota(r.busOf.begin(), r.busOf.end(), 0);
+                skip = index[j];
+            } else {
+                r = ReduceForElement(m, kind[j], index[j]);
+            }
+            busOf[j] = r.busOf;
+            const Model& red = r.m;
+            const bool splits = ConnectedParts(red, skip) > partsBefore;
+            if (r.noReference || ProvablyUnsolvablePart(red, skip, opt->tolerance)) {
+                outs[j].status = GS_PF_UNSOLVABLE_PART;
+                outs[j].iterations = 0;
+                outs[j].maxMis = 0;
+                outs[j].vm.assign(red.n, 0.0);
+                outs[j].va.assign(red.n, 0.0);
+                islanded[j] = splits;
+                continue;
+            }
+            std::vector<double> v0, a0;
+            if (!vm0.empty())
+                for (int i = 0; i < n; i++)
+                    if (r.busOf[i] >= 0) { v0.push_back(vm0[i]); a0.push_back(va0[i]); }
+            outs[j] = SolveWithRetry(red, skip, *opt, v0.empty() ? nullptr : v0.data(), a0.empty() ? nullptr : a0.data());
+            if (outs[j].status == GS_PF_CONVERGED)
+                Classify(red, skip, true, outs[j].vm, outs[j].va, opt->per_bus_voltage_limits != 0, opt->post_fault_rating,
+                         maxLoad[j], worstBnd[j], minVm[j], maxVm[j], viol[j], kind[j] == 2 ? &r.original : nullptr);
+            else
+                islanded[j] = splits;
+        }
+    };
+    int nt = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    nt = std::max(1, std::min(nt, std::max(1, nOut)));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; t++) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+    int total = 0;
+    for (int j = 0; j < nOut; j++) total += (int)viol[j].size();
+    res->viol_count = total;
+    const bool fits = total <= res->viol_capacity;
+    int w = 0;
+    for (int j = 0; j < nOut; j++) {
+        if (res->status) res->status[j] = outs[j].status;
+        if (res->iterations) res->iterations[j] = outs[j].iterations;
+        if (res->max_mismatch) res->max_mismatch[j] = outs[j].maxMis;
+        if (res->min_vm) res->min_vm[j] = minVm[j];
+        if (res->max_vm) res->max_vm[j] = maxVm[j];
+        if (res->max_loading_pct) res->max_loading_pct[j] = maxLoad[j];
+        if (res->worst_boundary_pct) res->worst_boundary_pct[j] = worstBnd[j];
+        if (res->islanded) res->islanded[j] = islanded[j];
+        if (res->viol_ptr) res->viol_ptr[j] = w;
+        for (const Violation& v : viol[j]) {
+            if (fits && res->viol_kind) {
+                res->viol_kind[w] = v.kind;
+                res->viol_element[w] = v.element;
+                res->viol_value[w] = v.value;
+            }
+            w++;
+        }
+        for (int i = 0; i < n; i++) {
+            const int p = busOf[j][i];
+            if (res->vm) res->vm[(size_t)j * n + i] = p >= 0 ? outs[j].vm[p] : 0.0;
+            if (res->va_deg) res->va_deg[(size_t)j * n + i] = p >= 0 ? outs[j].va[p] * 180.0 / kPi : 0.0;
+        }
+    }
+    if (res->viol_ptr) res->viol_ptr[nOut] = w;
+    return fits ? GS_OK : GS_ERR_CAPACITY;
 }
 
 // The topology verdicts of single-branch outages (the product's gs_outage_topology), the reference's way: per outage,

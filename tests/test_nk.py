@@ -128,6 +128,6 @@ def test_bad_sets_are_refused():
     with pytest.raises(EngineError):
         ContingencyAnalysis.screen_sets_raw(m, np.array([[3, 3]], np.int32), solver, opt)   # a branch twice
     with pytest.raises(EngineError):
-        ContingencyAnalysis.screen_sets_raw(m, np.array([[0, 1, 2, 3, 4]], np.int32), solver, opt)  # five branches
+        ContingencyAnalysis.screen_sets_raw(m, np.arange(17, dtype=np.int32)[None, :], solver, opt)  # 17 branches
     with pytest.raises(EngineError):
         ContingencyAnalysis.screen_sets_raw(m, np.array([[0, m.n_branch]], np.int32), solver, opt)  # no such branch
