@@ -17,7 +17,7 @@ import oracle
 from gridsim_b200 import _abi
 from gridsim_b200.engine import ContingencyAnalysis, PowerFlowOptions, SparseNewtonRaphsonPowerFlow, study_options
 from gridsim_b200.model import PQ, PV, SLACK, GridModel
-from tests.conftest import golden_model
+from tests.conftest import assert_states_close, golden_model
 
 VM_TOL = 1e-8
 VA_TOL_RAD = 1e-8
@@ -77,14 +77,16 @@ def _compare(gpu, ref, m, kinds, idx):
     assert np.array_equal(gpu["viol_kind"], ref["viol_kind"])
     assert np.array_equal(gpu["viol_element"], ref["viol_element"])
     conv = ref["status"] == _abi.PF_CONVERGED
-    keep = np.ones(gpu["vm"].shape, bool)
-    for j in range(len(kinds)):
-        if kinds[j] == 2:
-            keep[j, idx[j]] = False  # a removed bus has no state in the reduced model
-    mask = conv[:, None] & keep
-    if mask.any():
-        assert np.max(np.abs(gpu["vm"][mask] - ref["vm"][mask])) <= VM_TOL
-        assert np.max(np.abs(np.radians(gpu["va_deg"][mask] - ref["va_deg"][mask]))) <= VA_TOL_RAD
+    for j in np.nonzero(conv)[0]:
+        if kinds[j] == 0:
+            removed, bus = [idx[j]], -1
+        elif kinds[j] == 2:  # a removed bus has no state in the reduced model
+            removed = [k for k in range(m.n_branch) if idx[j] in (m.br_from[k], m.br_to[k])]
+            bus = idx[j]
+        else:
+            removed, bus = [], -1
+        assert_states_close(m, removed, gpu["vm"][j], gpu["va_deg"][j], ref["vm"][j], ref["va_deg"][j], VM_TOL,
+                            VA_TOL_RAD, removed_bus=bus)
     assert np.max(np.abs(gpu["min_vm"][conv] - ref["min_vm"][conv]), initial=0) <= VM_TOL
 
 
