@@ -52,7 +52,8 @@ class PfOpts(ctypes.Structure):
         ("tolerance", c_f64), ("diverge_limit_pu", c_f64), ("max_iterations", c_i32), ("flat_start", c_i32),
         ("enforce_q_limits", c_i32), ("retry_from_dc_start", c_i32), ("per_bus_voltage_limits", c_i32),
         ("precision", c_i32), ("warm_start_from_base", c_i32), ("batch_width", c_i32), ("phase_timing", c_i32),
-        ("post_fault_rating", c_i32), ("reserved", c_i32 * 6),
+        ("post_fault_rating", c_i32), ("max_q_limit_passes", c_i32), ("revert_q_limits", c_i32),
+        ("reserved", c_i32 * 4),
     ]
 
 

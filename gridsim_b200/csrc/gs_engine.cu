@@ -238,7 +238,7 @@ __global__ void k_status(DevBatch b, int iter, double tol, double divLimit, int 
 //      whose end is not a convergence); no change ends the solve converged.
 constexpr double kQLimitTolMva = 1e-3;      // NewtonShell.cs:26
 constexpr double kRevertVoltTolPu = 1e-4;   // NewtonShell.cs:31
-constexpr int kMaxQPasses = 100;            // PowerFlowOptions.MaxQLimitPasses default
+constexpr int kMaxQPasses = 100;            // PowerFlowOptions.MaxQLimitPasses default (:101)
 enum : int32_t { kQReverted = 16 };
 
 __global__ void k_status_q(DevBatch b, double tol, double divLimit, int maxIter) {
@@ -276,12 +276,32 @@ __global__ void k_status_q(DevBatch b, double tol, double divLimit, int maxIter)
     atomicAdd(b.activeCount, 1);
 }
 
+// TryRevertPin (NewtonShell.cs:563-576): a bus pinned at a limit whose voltage crossed its set point (by 1e-4 pu, on
+// the side the limit pushes it) goes back to PV at the set point, once per solve.
+__device__ __forceinline__ bool tryRevertPin(const DevGrid& g, const DevBatch& b, int i, int s, size_t idx) {
+    const int pin = b.pinned[idx];
+    if (b.effType[idx] != 1 || (pin != 1 && pin != -1) || b.reverted[idx] >= 1) return false;
+    double vg = g.vm0[i];  // the set point (of the units left, after a generator outage)
+    if (b.ovBus && b.ovBus[2 * s] == i && !isnan(b.ovVm[2 * s])) vg = b.ovVm[2 * s];
+    else if (b.ovBus && b.ovBus[2 * s + 1] == i && !isnan(b.ovVm[2 * s + 1])) vg = b.ovVm[2 * s + 1];
+    const double vm = b.vm[idx];
+    if (!((pin == 1 && vm > vg + kRevertVoltTolPu) || (pin == -1 && vm < vg - kRevertVoltTolPu))) return false;
+    b.effType[idx] = 2;
+    b.vm[idx] = vg;
+    b.pinned[idx] = 0;
+    b.reverted[idx] += 1;
+    return true;
+}
+
 // ApplyQLimits on the systems whose pass converged: grid (ceil(n / 8), B / 32), block (32, 8).
 __global__ void k_qapply(DevGrid g, DevBatch b) {
     const int s = blockIdx.y * 32 + threadIdx.x, i = blockIdx.x * 8 + threadIdx.y;
     if (!g.qlimOn || i >= g.n || s >= b.count || !b.active[s] || !(b.qState[s] & kQPending) || g.busType[i] != 2) return;
     const size_t idx = (size_t)i * b.B + s;
-    if (b.effType[idx] != 2) return;
+    if (b.effType[idx] != 2) {  // with RevertQLimits a pinned bus may go back to PV in the same pass (:551-556)
+        if (g.qlimRevert && tryRevertPin(g, b, i, s, idx)) atomicOr(&b.qState[s], kQChanged);
+        return;
+    }
     const double qd = (b.loadScale ? b.loadScale[idx] : 1.0) * g.qload[i];  // the bus's load, pu
     const double qGen = (b.qinj[idx] + qd) * g.baseMva;
     // the aggregate limits of the bus's units (those left after a generator outage)
@@ -308,23 +328,11 @@ __global__ void k_qrevert(DevGrid g, DevBatch b) {
     const int st = b.qState[s];
     if (!(st & kQPending) || (st & kQChanged)) return;
     const size_t idx = (size_t)i * b.B + s;
-    const int pin = b.pinned[idx];
-    if (b.effType[idx] != 1 || (pin != 1 && pin != -1) || b.reverted[idx] >= 1) return;
-    double vg = g.vm0[i];  // the set point (of the units left, after a generator outage)
-    if (b.ovBus && b.ovBus[2 * s] == i && !isnan(b.ovVm[2 * s])) vg = b.ovVm[2 * s];
-    else if (b.ovBus && b.ovBus[2 * s + 1] == i && !isnan(b.ovVm[2 * s + 1])) vg = b.ovVm[2 * s + 1];
-    const double vm = b.vm[idx];
-    if ((pin == 1 && vm > vg + kRevertVoltTolPu) || (pin == -1 && vm < vg - kRevertVoltTolPu)) {
-        b.effType[idx] = 2;
-        b.vm[idx] = vg;
-        b.pinned[idx] = 0;
-        b.reverted[idx] += 1;
-        atomicOr(&b.qState[s], kQReverted);
-    }
+    if (tryRevertPin(g, b, i, s, idx)) atomicOr(&b.qState[s], kQReverted);
 }
 
 // The end of a converged pass: a switch starts the next pass (this iteration's step is not taken), else converged.
-__global__ void k_qfinish(DevBatch b) {
+__global__ void k_qfinish(DevBatch b, int maxPasses) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= b.count || !b.active[s]) return;
     const int st = b.qState[s];
@@ -332,7 +340,7 @@ __global__ void k_qfinish(DevBatch b) {
     if (st & (kQChanged | kQReverted)) {
         b.qPass[s] += 1;
         b.passIter[s] = 0;
-        b.qState[s] = kQSkipStep | (b.qPass[s] >= kMaxQPasses ? kQFinalPass : 0);
+        b.qState[s] = kQSkipStep | (b.qPass[s] >= maxPasses ? kQFinalPass : 0);
         atomicAdd(b.activeCount, 1);
     } else {
         b.status[s] = GS_PF_CONVERGED;
@@ -1652,6 +1660,7 @@ int UploadGrid(gs_grid* G) {
     v.n = s.n; v.m = s.m; v.nnzY = s.nnzY; v.nbr = s.nbr; v.nnzLU = s.nnzLU; v.nLevels = s.nLevels;
     v.qlim = s.qlim ? 1 : 0;
     v.qlimOn = v.qlim;
+    v.qlimMaxPasses = kMaxQPasses;
     v.baseMva = h.base;
     const int n = h.n;
     G->pgen.assign(n, 0.0); G->qgen.assign(n, 0.0);
@@ -2057,7 +2066,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
     bool compacted = false;
     const dim3 nodeBlocks((s.n + 7) / 8);
     // with Q limits every pass may take up to max_iterations steps (plus the step-less pass switches)
-    const int maxLoop = g.qlim ? (o.max_iterations + 2) * (kMaxQPasses + 2) : o.max_iterations + 4;
+    const int maxLoop = g.qlim ? (o.max_iterations + 2) * (g.qlimMaxPasses + 2) : o.max_iterations + 4;
     for (int iter = 0; iter <= maxLoop; iter++) {
         if (timed) cudaEventRecord(ev[0], st);
         if (listCount > 0)
@@ -2071,7 +2080,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             k_status_q<<<(cur.count + 255) / 256, 256, 0, st>>>(cur, o.tolerance, o.diverge_limit_pu, o.max_iterations);
             k_qapply<<<dim3(nodeBlocks.x, cur.B / 32), blk8, 0, st>>>(g, cur);
             k_qrevert<<<dim3(nodeBlocks.x, cur.B / 32), blk8, 0, st>>>(g, cur);
-            k_qfinish<<<(cur.count + 255) / 256, 256, 0, st>>>(cur);
+            k_qfinish<<<(cur.count + 255) / 256, 256, 0, st>>>(cur, g.qlimMaxPasses);
             launches += 3;
         } else {
             k_status<<<(cur.count + 255) / 256, 256, 0, st>>>(cur, iter, o.tolerance, o.diverge_limit_pu, o.max_iterations);
@@ -2191,6 +2200,8 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
 
 int NewtonDispatch(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_opts& o, float* ms,
                    NewtonStats* stats = nullptr, const double* vmSys = nullptr, const double* vaSys = nullptr) {
+    G->view.qlimRevert = o.revert_q_limits ? 1 : 0;  // the call's Q-limit options (PowerFlowOptions.cs:101, 110)
+    G->view.qlimMaxPasses = o.max_q_limit_passes > 0 ? o.max_q_limit_passes : kMaxQPasses;
     if (o.precision == GS_PREC_MIXED) return Newton<float>(G, count, useScale, startFromWs, o, ms, stats, vmSys, vaSys);
     return Newton<double>(G, count, useScale, startFromWs, o, ms, stats, vmSys, vaSys);
 }
@@ -2442,6 +2453,9 @@ int CheckOpts(gs_ctx* ctx, const gs_pf_opts* o) {
     if (!(o->diverge_limit_pu > 0)) return SetErr(ctx, GS_ERR_INVALID_ARG, "diverge_limit_pu must be above 0");
     if (o->precision != GS_PREC_FP64 && o->precision != GS_PREC_MIXED)
         return SetErr(ctx, GS_ERR_INVALID_ARG, "unknown precision");
+    if (o->max_q_limit_passes < 0) return SetErr(ctx, GS_ERR_INVALID_ARG, "max_q_limit_passes must be 0 (the default) or more");
+    if (o->post_fault_rating < GS_RATE_A || o->post_fault_rating > GS_RATE_C)
+        return SetErr(ctx, GS_ERR_INVALID_ARG, "unknown post_fault_rating");
     return GS_OK;
 }
 

@@ -53,6 +53,8 @@ struct DevGrid {
     int nLevels;          // elimination-tree levels of the schedules
     int qlim;             // every bus has P and Q rows (identity rows where the bus is PV, reference or removed)
     int qlimOn;           // with qlim: PV buses switch to PQ at their Q limits (Q-limit enforcement)
+    int qlimRevert;       // with qlimOn: a pinned bus may revert to PV in the pass that switches others
+    int qlimMaxPasses;    // cap on switching passes
     double baseMva;
     const double* qminPu; // aggregate reactive limits per bus (pu)
     const double* qmaxPu;

@@ -43,6 +43,8 @@ class PowerFlowOptions:
     batch_width: int = 0
     phase_timing: bool = False
     post_fault_rating: str = "A"     # "A", "B" or "C": the rating outage states are judged against (screens)
+    max_q_limit_passes: int = 100    # MaxQLimitPasses
+    revert_q_limits: bool = False    # RevertQLimits
 
     def to_c(self) -> _abi.PfOpts:
         o = _abi.default_opts()
@@ -58,6 +60,8 @@ class PowerFlowOptions:
         o.batch_width = int(self.batch_width)
         o.phase_timing = int(self.phase_timing)
         o.post_fault_rating = {"A": _abi.RATE_A, "B": _abi.RATE_B, "C": _abi.RATE_C}[self.post_fault_rating.upper()]
+        o.max_q_limit_passes = int(self.max_q_limit_passes)
+        o.revert_q_limits = int(self.revert_q_limits)
         return o
 
 

@@ -148,7 +148,9 @@ typedef struct gs_pf_opts {
     int32_t batch_width;            /* systems per device batch; 0 = choose from free HBM */
     int32_t phase_timing;           /* 1: time each phase with CUDA events (no graph replay) into the result */
     int32_t post_fault_rating;      /* enum gs_post_fault_rating, screens only; default GS_RATE_A */
-    int32_t reserved[6];
+    int32_t max_q_limit_passes;     /* cap on PV->PQ switching passes (MaxQLimitPasses); 0 = the default 100 */
+    int32_t revert_q_limits;        /* RevertQLimits: a pinned bus may go back to PV within a switching pass; 0 */
+    int32_t reserved[4];
 } gs_pf_opts;
 
 /* Fill `o` with the reference defaults (PowerFlowOptions()) plus precision = FP64. */

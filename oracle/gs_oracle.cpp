@@ -952,7 +952,8 @@ SolveOut SolveModel(const Model& m, int skip, const gs_pf_opts& opt, const doubl
     bool converged = false;
     int total = 0;
     RunEnd re;
-    int qPasses = opt.enforce_q_limits ? 100 : 1;  // PowerFlowOptions.MaxQLimitPasses default (:101)
+    // PowerFlowOptions.MaxQLimitPasses (:101, default 100) and RevertQLimits (:110, default off)
+    int qPasses = opt.enforce_q_limits ? (opt.max_q_limit_passes > 0 ? opt.max_q_limit_passes : 100) : 1;
     bool switchPending = false;
     for (int qp = 0; qp < qPasses; qp++) {
         switchPending = false;
@@ -961,7 +962,7 @@ SolveOut SolveModel(const Model& m, int skip, const gs_pf_opts& opt, const doubl
         total += re.iters;
         if (!opt.enforce_q_limits) break;
         if (!converged) break;
-        bool changed = ApplyQLimits(s, eff, Q, qspec, m.base, Vm, pinned, revertCount, false);
+        bool changed = ApplyQLimits(s, eff, Q, qspec, m.base, Vm, pinned, revertCount, opt.revert_q_limits != 0);
         if (!changed) changed = RevertBrokenPins(s, eff, Vm, pinned, revertCount);
         switchPending = changed;
         if (!changed) break;

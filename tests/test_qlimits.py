@@ -115,3 +115,22 @@ def test_q_limits_refused_where_not_built():
             b.solve([1], options=PowerFlowOptions(enforce_q_limits=True))
     finally:
         b.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("extra", [{"revert_q_limits": True}, {"max_q_limit_passes": 1}, {"max_q_limit_passes": 3}])
+def test_revert_and_pass_cap_options_match_the_oracle(tight_grid, precision, extra):
+    """RevertQLimits (a pinned bus may go back to PV in the pass that switches others, PowerFlowOptions.cs:103-110) and
+    MaxQLimitPasses (:100-101) on the tight-limits grid: both change the screen (checked on the oracle) and the device
+    follows the oracle."""
+    m = tight_grid
+    opt = PowerFlowOptions(max_iterations=30, enforce_q_limits=True, warm_start_from_base=True,
+                           per_bus_voltage_limits=True, precision=precision, **extra)
+    idx = synthetic.outage_set(m, None, 0)
+    gpu = ContingencyAnalysis.screen_raw(m, idx, SparseNewtonRaphsonPowerFlow(precision), opt, keep_states=True)
+    ref = oracle.screen(m, idx, opt.to_c(), keep_states=True)
+    _compare(gpu, ref)
+    assert np.array_equal(gpu["iterations"], ref["iterations"])
+    plain = oracle.screen(m, idx, PowerFlowOptions(max_iterations=30, enforce_q_limits=True, warm_start_from_base=True,
+                                                   per_bus_voltage_limits=True).to_c())
+    assert not np.array_equal(plain["iterations"], ref["iterations"])
