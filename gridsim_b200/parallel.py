@@ -13,6 +13,7 @@ from typing import Callable, Optional
 import numpy as np
 
 PER_OUTAGE = ("status", "iterations", "max_mismatch", "min_vm", "max_vm", "max_loading_pct")
+OPTIONAL = ("worst_boundary_pct", "islanded")  # merged when every part has them
 
 
 def shard(n_items: int, rank: int, world: int) -> slice:
@@ -25,6 +26,9 @@ def shard(n_items: int, rank: int, world: int) -> slice:
 def merge(parts: list) -> dict:
     """Concatenate per-rank raw screen results (rank order) into one, fixing the violation offsets."""
     out = {k: np.concatenate([p[k] for p in parts]) for k in PER_OUTAGE}
+    for k in OPTIONAL:
+        if all(k in p for p in parts):
+            out[k] = np.concatenate([p[k] for p in parts])
     ptr, kinds, elems, vals = [0], [], [], []
     for p in parts:
         base = ptr[-1]
@@ -51,10 +55,11 @@ def screen_sharded(model, branch_idx, screen: Callable, group=None, rank: Option
         world = dist.get_world_size(group) if dist.is_available() and dist.is_initialized() else 1
     if rank is None:
         rank = dist.get_rank(group) if world > 1 else 0
-    mine = screen(model, idx[shard(len(idx), rank, world)])
+    mine = screen(model, idx[shard(len(idx), rank, world)])  # rows: a branch, or a set of branches per outage
     if world == 1:
         return merge([mine])
-    part = {k: np.asarray(mine[k]) for k in PER_OUTAGE + ("viol_ptr", "viol_kind", "viol_element", "viol_value")}
+    keys = PER_OUTAGE + ("viol_ptr", "viol_kind", "viol_element", "viol_value") + tuple(k for k in OPTIONAL if k in mine)
+    part = {k: np.asarray(mine[k]) for k in keys}
     parts = [None] * world
     dist.all_gather_object(parts, part, group=group)
     return merge(parts)

@@ -13,6 +13,15 @@ def _free_port():
         return s.getsockname()[1]
 
 
+def _pairs(m):
+    """21 two-branch outages of the 120-bus grid, bridges among them (some split the grid)."""
+    from gridsim_b200 import synthetic
+    live = m.in_service_branches()
+    br = np.nonzero(synthetic.bridges(m))[0][:3]
+    rows = [[int(live[3 * k]), int(live[3 * k + 1])] for k in range(18)] + [[int(b), int(live[0])] for b in br]
+    return np.array(rows, np.int32)
+
+
 def _worker(rank, world, port, out_path):
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -31,8 +40,11 @@ def _worker(rank, world, port, out_path):
         o.max_iterations = 20
         o.warm_start_from_base = 1
         got = screen_sharded(m, idx, lambda mm, ii: oracle.screen(mm, ii, o, threads=1))
+        pairs = _pairs(m)
+        got2 = screen_sharded(m, pairs, lambda mm, ss: oracle.screen_sets(mm, ss, o, threads=1))
         if rank == 0:
             np.savez(out_path, **got)
+            np.savez(out_path + ".pairs.npz", **got2)
     finally:
         dist.destroy_process_group()
 
@@ -52,6 +64,12 @@ def test_two_rank_screen_equals_one_process(tmp_path):
     o.max_iterations = 20
     o.warm_start_from_base = 1
     whole = oracle.screen(m, idx, o)
-    for k in ("status", "iterations", "viol_ptr", "viol_kind", "viol_element", "viol_value", "max_loading_pct"):
+    for k in ("status", "iterations", "viol_ptr", "viol_kind", "viol_element", "viol_value", "max_loading_pct",
+              "islanded", "worst_boundary_pct"):
         assert np.array_equal(got[k], whole[k]), k
+    # multi-branch outages shard by rows the same way
+    got2 = np.load(out + ".pairs.npz")
+    whole2 = oracle.screen_sets(m, _pairs(m), o)
+    for k in ("status", "iterations", "viol_ptr", "viol_kind", "viol_element", "islanded"):
+        assert np.array_equal(got2[k], whole2[k]), k
     del torch
