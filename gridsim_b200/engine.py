@@ -3,8 +3,11 @@
 * :class:`SparseNewtonRaphsonPowerFlow` — ``IPowerFlowSolver.Solve(GridModel, PowerFlowOptions)``
   (``src/GridSim.Core/Abstractions/IPowerFlowSolver.cs:10-13``) on the B200 engine.
 * :class:`ContingencyAnalysis` — ``ScreenBranches`` / ``ScreenBranchesParallel`` / ``ScreenBaseCase`` /
-  ``NetAgainstBase`` (``src/GridSim.Core/Analysis/ContingencyAnalysis.cs:306-344, 958-1043``), with the
-  screen's Newton solves and ScreenStateCore classification running on the device.
+  ``NetAgainstBase`` (``src/GridSim.Core/Analysis/ContingencyAnalysis.cs:306-344, 958-1043``), ``ScreenOutage``
+  and the N-k screens (:356-426), ``ScreenElementOutages`` (:1309-1437), with the screen's Newton solves and
+  ScreenStateCore classification running on the device.
+* :class:`CudaSparseLinearSolver` — ``ISparseLinearSolver`` / ``IBatchedSparseLinearSolver``.
+* :class:`UnevenBatch` — many load flows of different grids in one persistent launch.
 
 Every call goes through ``libgridsim_b200.so``; if the library is missing the import of this module
 succeeds but the first solve raises (there is no CPU path).
@@ -547,14 +550,17 @@ class ContingencyAnalysis:
         return sp.astype(bool), un.astype(bool)
 
     @classmethod
-    def _results(cls, model: GridModel, idx, raw: dict) -> list:
+    def _results(cls, model: GridModel, idx, raw: dict, labels: Optional[Sequence[str]] = None) -> list:
         """ContingencyResult per outage; `idx` holds a branch per outage (-1 = the intact grid) or, for the
-        multi-branch screen, a row of branches (-1 = none) labelled "A + B" (LabelMany, :1836-1837)."""
+        multi-branch screen, a row of branches (-1 = none) labelled "A + B" (LabelMany, :1836-1837); `labels`
+        replaces those labels."""
         res = []
         for j, k in enumerate(idx):
             st = int(raw["status"][j])
             br = [int(x) for x in np.atleast_1d(k) if x >= 0]
             label = " + ".join(_branch_label(model, b) for b in br) if br else cls.BASE_CASE_LABEL
+            if labels is not None:
+                label = labels[j]
             if st != _abi.PF_CONVERGED:  # NonConverged (:1661-1662)
                 isl = bool(raw["islanded"][j])
                 res.append(ContingencyResult(label, False, 0.0, 0.0, 0.0, 0.0, ["islanded" if isl else "no solution"],
@@ -754,23 +760,26 @@ class ContingencyAnalysis:
         kinds = np.array([int(k) for k, _ in outages], np.int32)
         idx = np.array([int(on[i]) if k == 1 else int(i) for k, i in outages], np.int32)
         raw = cls.screen_elements_raw(model, kinds, idx, solver, options)
-        res = []
+        labels = []
         for j, (k, i) in enumerate(outages):
-            r = cls._results(model, [int(idx[j]) if k == 0 else -1], {key: (v[j:j + 1] if key in (
-                "status", "iterations", "max_mismatch", "max_loading_pct", "worst_boundary_pct", "min_vm", "max_vm",
-                "islanded") else v) for key, v in raw.items()} | {"viol_ptr": raw["viol_ptr"][j:j + 2]})[0]
+            if k == 0:
+                labels.append(_branch_label(model, int(idx[j])))
+            elif k == 1:  # "gen {index} at bus {id}" for a unit without a name (:1363)
+                labels.append(f"gen {i} at bus {int(model.bus_id[model.gen_bus[idx[j]]])}")
+            else:
+                labels.append(f"bus {int(model.bus_id[i])}")
+        res = cls._results(model, np.where(kinds == 0, idx, -1), raw, labels)
+        for j, (k, i) in enumerate(outages):
+            r = res[j]
+            r.kind = int(k)
             if k == 1:
                 g = int(idx[j])
-                bus = int(model.gen_bus[g])
-                r.outage = f"gen {i} at bus {int(model.bus_id[bus])}"
-                r.kind, r.lost_generation_mw = 1, float(model.pg[g])
-                r.note = cls._reelect(model, g, -1, bus)[1]
+                r.lost_generation_mw = float(model.pg[g])
+                r.note = cls._reelect(model, g, -1, int(model.gen_bus[g]))[1]
             elif k == 2:
-                r.outage = f"bus {int(model.bus_id[i])}"
-                r.kind, r.lost_load_mw = 2, float(model.pd[i])
+                r.lost_load_mw = float(model.pd[i])
                 r.lost_generation_mw = float(sum(model.pg[g] for g in on if int(model.gen_bus[g]) == i))
                 r.note = cls._reelect(model, -1, int(i), int(i))[1]
-            res.append(r)
         return res
 
     @classmethod
