@@ -1611,7 +1611,8 @@ struct gs_grid {
     gs::OutageSetTable sets;         // multi-branch outages of the current call (view.nSet > 0 while installed)
     std::vector<gs::ElemSys> elemBatch;  // element outages of the systems in the workspace (empty: none)
     gs::DevBuf setBrBuf, setCellBuf, setRedBuf;
-    int split = 0;      // first level run by the persistent kernels
+    int split = 0;      // first level run by the persistent kernels (factorisation)
+    int splitB = 0;     // first level run by the persistent kernels in the triangular solves
     int tailSplit = 0;  // first level the few-systems path runs as one CTA per system
 };
 
@@ -1764,6 +1765,16 @@ int UploadGrid(gs_grid* G) {
         if (std::max(std::max(a, bb), c) > 2 * kPersistWarps) break;
         G->split = l;
     }
+    // the solves have one item per level for a few nodes (short pieces packed), so their persistent walk can start
+    // lower in the tree than the factorisation's
+    G->splitB = s.nLevels;
+    for (int l = s.nLevels - 1; l >= 0; l--) {
+        const int c = s.backward.levelItemPtr[l + 1] - s.backward.levelItemPtr[l];
+        const int v = s.forward.levelItemPtr[l + 1] - s.forward.levelItemPtr[l];
+        if (std::max(c, v) > 2 * kPersistWarps) break;
+        G->splitB = l;
+    }
+    G->splitB = std::min(G->splitB, G->split);
     return GS_OK;
 }
 
@@ -1928,7 +1939,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
     int64_t stepLaunches = 0;
     // levels [0, split) run one launch per level (wide: thousands of tasks); levels [split, nLevels) run in
     // one persistent launch per phase (narrow: a few tasks per level, latency-bound)
-    const int split = G->split;
+    const int split = G->split, splitB = G->splitB;
     const int persistThreads = 32;
     // warps per persistent CTA: as many as let every system group's CTA be resident at once (one wave), at most
     // kPersistWarps (a second partial wave would double the launch)
@@ -1982,22 +1993,22 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
         }
     };
     auto backward = [&](const DevBatch& bb, cudaStream_t ss, T* vec) {
-        if (split < s.nLevels) {
+        if (splitB < s.nLevels) {
             k_persistent<T, kWorkBackward><<<(bb.count + Lay<T>::S - 1) / Lay<T>::S, dim3(persistThreads, persistWarps), 0, ss>>>(
-                g, bb, vec, split, s.nLevels);
+                g, bb, vec, splitB, s.nLevels);
             stepLaunches++;
         }
-        for (int l = split - 1; l >= 0; l--) launchLevel(bb, ss, k_level<T, kWorkBackward>, vec, bp[l], bp[l + 1]);
+        for (int l = splitB - 1; l >= 0; l--) launchLevel(bb, ss, k_level<T, kWorkBackward>, vec, bp[l], bp[l + 1]);
     };
     auto solvePhase = [&](const DevBatch& bb, cudaStream_t ss, bool doRefine) {
         backward(bb, ss, (T*)bb.y);
         if (doRefine) {
             k_residual<T><<<dim3((s.n + 7) / 8, (bb.count + 31) / 32), blk8, 0, ss>>>(g, bb, nullptr, 0);
             stepLaunches++;
-            for (int l = 0; l < split; l++) launchLevel(bb, ss, k_level<T, kWorkForward>, (T*)bb.z, vp[l], vp[l + 1]);
-            if (split < s.nLevels) {
+            for (int l = 0; l < splitB; l++) launchLevel(bb, ss, k_level<T, kWorkForward>, (T*)bb.z, vp[l], vp[l + 1]);
+            if (splitB < s.nLevels) {
                 k_persistent<T, kWorkForward><<<(bb.count + Lay<T>::S - 1) / Lay<T>::S, dim3(persistThreads, persistWarps), 0, ss>>>(
-                    g, bb, (T*)bb.z, split, s.nLevels);
+                    g, bb, (T*)bb.z, splitB, s.nLevels);
                 stepLaunches++;
             }
             backward(bb, ss, (T*)bb.z);
@@ -3228,16 +3239,14 @@ int LinearSolve(gs_grid* G, int cnt) {
     };
     const auto& fp = s.factor.levelItemPtr;
     const auto& bp = s.backward.levelItemPtr;
-    const int split = G->split;
+    const int split = G->split, splitB = G->splitB;
     for (int l = 0; l < split; l++) {
         level(k_level<T, kWorkFactor>, fp[2 * l], fp[2 * l + 1]);
         level(k_level<T, kWorkFactor>, fp[2 * l + 1], fp[2 * l + 2]);
     }
-    if (split < s.nLevels) {
-        k_persistent<T, kWorkFactor><<<grp, blkP, 0, st>>>(g, b, (T*)b.y, split, s.nLevels);
-        k_persistent<T, kWorkBackward><<<grp, blkP, 0, st>>>(g, b, (T*)b.y, split, s.nLevels);
-    }
-    for (int l = split - 1; l >= 0; l--) level(k_level<T, kWorkBackward>, bp[l], bp[l + 1]);
+    if (split < s.nLevels) k_persistent<T, kWorkFactor><<<grp, blkP, 0, st>>>(g, b, (T*)b.y, split, s.nLevels);
+    if (splitB < s.nLevels) k_persistent<T, kWorkBackward><<<grp, blkP, 0, st>>>(g, b, (T*)b.y, splitB, s.nLevels);
+    for (int l = splitB - 1; l >= 0; l--) level(k_level<T, kWorkBackward>, bp[l], bp[l + 1]);
     GS_CUDA(cudaGetLastError());
     return GS_OK;
 }
