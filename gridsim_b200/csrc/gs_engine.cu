@@ -672,8 +672,11 @@ __global__ void __launch_bounds__(256) k_residual(DevGrid g, DevBatch b, const i
 // one dependent round of loads per level and phase. The system's LU is ~1 MB and stays in L2 across the
 // levels; the per-level launches and their warps for 32-system groups are not needed here.
 constexpr int kTailThreads = 1024;
-constexpr int kTailMaxSystems = 148;  // one wave of k_tail CTAs (one 1024-thread CTA per SM)
-constexpr int kCompactCap = 160;      // systems the compact workspace holds (kTailMaxSystems rounded up to 32)
+// Two waves of k_tail CTAs (one 1024-thread CTA per SM). Measured on the 10,000-bus screen, where an iteration with
+// ~220 of 5,000 systems left costs ~15 ms as a full-batch step and ~7 ms on this path: 148 (one wave) 22,200,
+// 224 23,900, 296 24,200, 448 23,900 load flows/s in one run.
+constexpr int kTailMaxSystems = 296;
+constexpr int kCompactCap = 320;      // systems the compact workspace holds (kTailMaxSystems rounded up to 32)
 
 __global__ void k_collect_active(DevBatch b) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
