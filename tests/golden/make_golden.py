@@ -43,6 +43,11 @@ def main(ref_root):
         "case118": (ieee["Case118Vm"], ieee["Case118Va"], 0.03, 1.0),
         "case300": (ieee["Case300Vm"], ieee["Case300Va"], 0.02, 12.0),
     }
+    # case24_ieee_rts: the model only, for its RATE_B / RATE_C columns
+    # (tests/GridSim.Tests/ContingencyTypesAndRatingsTests.cs:43-51)
+    m24 = load_matpower(os.path.join(ref_root, "data", "matpower", "lib", "case24_ieee_rts.m"))
+    with open(os.path.join(HERE, "case24_ieee_rts.json"), "w") as fh:
+        json.dump({"source": "data/matpower/lib/case24_ieee_rts.m", "model": m24.to_dict(), "published": None}, fh)
     for name, (vm, va, vm_tol, va_tol) in published.items():
         m = load_matpower(os.path.join(ref_root, "data", "matpower", "lib", name + ".m"))
         doc = {"source": f"data/matpower/lib/{name}.m", "model": m.to_dict(),
