@@ -17,7 +17,7 @@ from __future__ import annotations
 import ctypes
 import itertools
 import math
-from dataclasses import dataclass, field
+from dataclasses import dataclass, field, replace
 from typing import Optional, Sequence
 
 import numpy as np
@@ -66,6 +66,15 @@ class PowerFlowOptions:
         o.max_q_limit_passes = int(self.max_q_limit_passes)
         o.revert_q_limits = int(self.revert_q_limits)
         return o
+
+    def device_model(self, model: GridModel) -> GridModel:
+        """The model whose descriptor the library solves with these options: the flat-start copy under
+        ``flat_start`` (the library takes a flat start through the descriptor's voltages), else `model`."""
+        return model.flat_started() if self.flat_start else model
+
+    def device_c(self) -> _abi.PfOpts:
+        """gs_pf_opts for a grid built from :meth:`device_model`: the flat start is already in its voltages."""
+        return replace(self, flat_start=False).to_c()
 
 
 # ContingencyAnalysis.StudyOptions (ContingencyAnalysis.cs:263-268): 100 iterations with Q limits on.
@@ -195,8 +204,16 @@ class SparseNewtonRaphsonPowerFlow:
         self.ctx = ctx
         self._grid: Optional[CudaGrid] = None
         self._model_key = None
+        self._flat_src: Optional[GridModel] = None
+        self._flat: Optional[GridModel] = None
 
-    def grid_for(self, model: GridModel) -> CudaGrid:
+    def grid_for(self, model: GridModel, options: Optional[PowerFlowOptions] = None) -> CudaGrid:
+        """The device grid of `model` (kept while the same model is solved again); with options that ask for a flat
+        start, the grid of its flat-start copy (:meth:`PowerFlowOptions.device_model`), kept likewise."""
+        if options is not None and options.flat_start:
+            if self._flat_src is not model:
+                self._flat_src, self._flat = model, options.device_model(model)
+            model = self._flat
         key = id(model)
         if self._grid is None or self._model_key != key or self._grid.model is not model:
             self._grid = CudaGrid(model, self.ctx)
@@ -205,7 +222,7 @@ class SparseNewtonRaphsonPowerFlow:
 
     def solve(self, model: GridModel, options: Optional[PowerFlowOptions] = None) -> PowerFlowResult:
         opt = options or PowerFlowOptions(precision=self.precision)
-        g = self.grid_for(model)
+        g = self.grid_for(model, opt)
         n, nb = model.n_bus, model.n_branch
         out = {k: np.zeros(n) for k in ("vm", "va_deg", "p_inj_mw", "q_inj_mvar")}
         out["loading_percent"] = np.zeros(nb)
@@ -214,7 +231,7 @@ class SparseNewtonRaphsonPowerFlow:
         r = _abi.PfResult()
         r.vm, r.va_deg, r.p_inj_mw, r.q_inj_mvar = (_p(out[k]) for k in ("vm", "va_deg", "p_inj_mw", "q_inj_mvar"))
         r.loading_pct, r.sf_mva, r.st_mva = _p(out["loading_percent"]), _p(out["sf"]), _p(out["st"])
-        c = opt.to_c()
+        c = opt.device_c()
         g.ctx.check(g.ctx.lib.gs_pf_solve(g.handle, ctypes.byref(c), ctypes.byref(r)), "gs_pf_solve")
         sf = out["sf"][: 2 * nb].reshape(-1, 2)
         st = out["st"][: 2 * nb].reshape(-1, 2)
@@ -229,7 +246,7 @@ class SparseNewtonRaphsonPowerFlow:
                     keep_states: bool = False) -> dict:
         """Many load flows of one grid in device batches (``gs_pf_solve_batch``)."""
         opt = options or PowerFlowOptions(precision=self.precision)
-        g = self.grid_for(model)
+        g = self.grid_for(model, opt)
         n = model.n_bus
         count = (load_scale.shape[0] if load_scale is not None else outage.shape[0])
         ls = None if load_scale is None else np.ascontiguousarray(load_scale, np.float64)
@@ -239,7 +256,7 @@ class SparseNewtonRaphsonPowerFlow:
         mis = np.zeros(count)
         vm = np.zeros(count * n) if keep_states else None
         va = np.zeros(count * n) if keep_states else None
-        c = opt.to_c()
+        c = opt.device_c()
         g.ctx.check(g.ctx.lib.gs_pf_solve_batch(g.handle, count, _p(ls), _p(og), ctypes.byref(c), _p(st), _p(it),
                                                 _p(mis), _p(vm), _p(va)), "gs_pf_solve_batch")
         out = {"status": st, "iterations": it, "max_mismatch": mis}
@@ -324,6 +341,7 @@ class UnevenBatch:
         self.ctx = ctx or CudaContext.default()
         self.models = list(models)
         self.grids = [CudaGrid(m, self.ctx) for m in self.models]
+        self._flat_grids: Optional[list] = None
         self.stats = None
 
     def solve(self, counts: Sequence[int], load_scale: Optional[Sequence[np.ndarray]] = None,
@@ -348,8 +366,13 @@ class UnevenBatch:
         st, it, mis = np.zeros(total, np.int32), np.zeros(total, np.int32), np.zeros(total)
         vm = np.zeros(states) if keep_states else None
         va = np.zeros(states) if keep_states else None
-        handles = (ctypes.c_void_p * max(k, 1))(*[g.handle.value for g in self.grids])
-        c = opt.to_c()
+        grids = self.grids
+        if opt.flat_start:   # the flat-start copies, uploaded on first use
+            if self._flat_grids is None:
+                self._flat_grids = [CudaGrid(opt.device_model(m), self.ctx) for m in self.models]
+            grids = self._flat_grids
+        handles = (ctypes.c_void_p * max(k, 1))(*[g.handle.value for g in grids])
+        c = opt.device_c()
         stats = _abi.MultiStats()
         self.ctx.check(self.ctx.lib.gs_pf_solve_multi(self.ctx.handle, k, handles, _p(counts), _p(ls), _p(og),
                                                       ctypes.byref(c), _p(st), _p(it), _p(mis), _p(vm), _p(va),
@@ -370,9 +393,10 @@ class UnevenBatch:
         return out
 
     def close(self) -> None:
-        for g in self.grids:
+        for g in self.grids + (self._flat_grids or []):
             g.close()
         self.grids = []
+        self._flat_grids = None
 
 
 # ---------------------------------------------------------------------------------------------
@@ -488,7 +512,7 @@ class ContingencyAnalysis:
 
     @staticmethod
     def _screen_call(model, idx, width, solver, options, keep_states):
-        g = solver.grid_for(model)
+        g = solver.grid_for(model, options)
         k = idx.shape[0]
         n = model.n_bus
         # violation capacity: remembered per grid (a too small buffer makes the engine report the size
@@ -507,7 +531,7 @@ class ContingencyAnalysis:
             for key, v in out.items():
                 setattr(r, key, _p(v))
             r.viol_capacity = cap
-            c = options.to_c()
+            c = options.device_c()
             if width is None:
                 rc = g.ctx.lib.gs_n1_screen(g.handle, k, _p(idx), ctypes.byref(c), ctypes.byref(r))
             elif isinstance(width, tuple):

@@ -132,6 +132,17 @@ class GridModel:
         m.va_deg = np.ascontiguousarray(va_deg, dtype=np.float64).copy()
         return m
 
+    def flat_started(self) -> "GridModel":
+        """The model whose stored voltages are the flat start of PowerFlowOptions.FlatStart: every bus that is not
+        a reference bus starts at 1 pu and 0 degrees, a reference bus keeps its stored Vm and angle, and a
+        voltage-controlled bus with units still starts at its units' set point (``NewtonShell.cs:463-474``). The
+        library takes a flat start this way, through the descriptor."""
+        m = self.copy()
+        free = m.bus_type != SLACK
+        m.vm[free] = 1.0
+        m.va_deg[free] = 0.0
+        return m
+
     def in_service_branches(self) -> np.ndarray:
         """ContingencyAnalysis.InServiceBranchIndices (``ContingencyAnalysis.cs:283-289``)."""
         return np.nonzero(self.br_in_service)[0].astype(np.int32)

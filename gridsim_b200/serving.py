@@ -65,7 +65,7 @@ class LoadFlowServer:
         self.lib = self.ctx.lib
         self.options = options or PowerFlowOptions()
         o = _abi.ServeOpts()
-        o.pf = self.options.to_c()
+        o.pf = self.options.device_c()
         o.slots_per_grid = slots_per_grid
         o.state_slots = state_slots
         o.hbm_fraction = hbm_fraction
@@ -78,7 +78,7 @@ class LoadFlowServer:
         self._state = np.zeros(0)
 
     def add_grid(self, model: GridModel) -> int:
-        g = CudaGrid(model, self.ctx)
+        g = CudaGrid(self.options.device_model(model), self.ctx)
         idx = ctypes.c_int32()
         self.ctx.check(self.lib.gs_serve_add_grid(self.handle, g.handle, ctypes.byref(idx)), "gs_serve_add_grid")
         self.grids.append(g)

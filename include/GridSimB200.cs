@@ -239,7 +239,9 @@ namespace GridSim.Core.PowerFlow.B200
 
         /// <summary>PowerFlowOptions (PowerFlow/PowerFlowOptions.cs:15-158) as gs_pf_opts. The reference's defaults
         /// are kept, Q limits and the DC retry included; <paramref name="precision"/> chooses the arithmetic of the
-        /// linear step. Trace is not filled by the device path; Cancellation is honoured before the call.</summary>
+        /// linear step. FlatStart is not a flag of the call: the library takes a flat start through the descriptor's
+        /// voltages (<see cref="GsGrid.For(GridModel, bool)"/>). Trace is not filled by the device path; Cancellation
+        /// is honoured before the call.</summary>
         public static PfOpts Options(PowerFlowOptions? options, int precision)
         {
             var o = new PfOpts();
@@ -249,7 +251,6 @@ namespace GridSim.Core.PowerFlow.B200
             o.Tolerance = options.Tolerance;
             o.DivergeLimitPu = options.DivergeLimitPu;
             o.MaxIterations = options.MaxIterations;
-            o.FlatStart = options.FlatStart ? 1 : 0;
             o.EnforceQLimits = options.EnforceQLimits ? 1 : 0;
             o.MaxQLimitPasses = options.MaxQLimitPasses;
             o.RevertQLimits = options.RevertQLimits ? 1 : 0;
@@ -303,24 +304,26 @@ namespace GridSim.Core.PowerFlow.B200
     public sealed class GsGrid
     {
         private static readonly ConditionalWeakTable<GridModel, GsGrid> Cache = new();
+        private static readonly ConditionalWeakTable<GridModel, GsGrid> FlatCache = new();
 
         public GridModel Model { get; }
         public Handle Native { get; }
         public IReadOnlyDictionary<int, int> PositionOfBus { get; }
         public object Sync { get; } = new();
 
-        /// <summary>The device grid of <paramref name="model"/>, built on first use and kept while the model lives.</summary>
-        public static GsGrid For(GridModel model)
+        /// <summary>The device grid of <paramref name="model"/>, built on first use and kept while the model lives;
+        /// with <paramref name="flatStart"/>, the grid whose start voltages are PowerFlowOptions.FlatStart's.</summary>
+        public static GsGrid For(GridModel model, bool flatStart = false)
         {
             ArgumentNullException.ThrowIfNull(model);
-            return Cache.GetValue(model, m => new GsGrid(m));
+            return flatStart ? FlatCache.GetValue(model, m => new GsGrid(m, true)) : Cache.GetValue(model, m => new GsGrid(m, false));
         }
 
-        private GsGrid(GridModel model)
+        private GsGrid(GridModel model, bool flatStart)
         {
             RequireSupported(model);
             Model = model;
-            using var desc = new PinnedDesc(model);
+            using var desc = new PinnedDesc(model, flatStart);
             PositionOfBus = desc.PositionOfBus;
             GsNative.GridDesc d = desc.Desc;
             GsNative.Check(GsNative.gs_grid_create(GsContext.Handle, ref d, out IntPtr g), GsContext.Handle, "gs_grid_create");
@@ -346,14 +349,16 @@ namespace GridSim.Core.PowerFlow.B200
         }
 
         /// <summary>A gs_grid_desc over pinned copies of a model's arrays; the library copies what it keeps during
-        /// the call, so the pins end when this is disposed.</summary>
+        /// the call, so the pins end when this is disposed. With <c>flatStart</c> every bus that is not a reference
+        /// bus starts at 1 pu and 0 degrees (a voltage-controlled bus with units still starts at their set point, a
+        /// reference bus at its stored values: NewtonShell.cs:463-474).</summary>
         public sealed class PinnedDesc : IDisposable
         {
             private readonly List<GCHandle> _pins = new();
             public GsNative.GridDesc Desc;
             public Dictionary<int, int> PositionOfBus { get; } = new();
 
-            public PinnedDesc(GridModel model)
+            public PinnedDesc(GridModel model, bool flatStart = false)
             {
                 IReadOnlyList<Bus> buses = model.Buses;
                 IReadOnlyList<Generator> gens = model.Generators;
@@ -371,7 +376,10 @@ namespace GridSim.Core.PowerFlow.B200
                     Bus b = buses[i];
                     busId[i] = b.Id;
                     busType[i] = b.Type switch { BusType.Slack => 3, BusType.Pv => 2, _ => 1 };
-                    pd[i] = b.Pd; qd[i] = b.Qd; gs[i] = b.Gs; bs[i] = b.Bs; vm[i] = b.Vm; va[i] = b.VaDeg;
+                    pd[i] = b.Pd; qd[i] = b.Qd; gs[i] = b.Gs; bs[i] = b.Bs;
+                    bool flat = flatStart && b.Type != BusType.Slack;
+                    vm[i] = flat ? 1.0 : b.Vm;
+                    va[i] = flat ? 0.0 : b.VaDeg;
                     vmin[i] = b.VminPu ?? double.NaN; vmax[i] = b.VmaxPu ?? double.NaN;
                 }
                 var genBus = new int[ng];
@@ -467,7 +475,7 @@ namespace GridSim.Core.PowerFlow.B200
 
         public unsafe PowerFlowResult Solve(GridModel model, PowerFlowOptions? options = null)
         {
-            GsGrid grid = GsGrid.For(model);
+            GsGrid grid = GsGrid.For(model, options?.FlatStart == true);
             GsNative.PfOpts o = GsNative.Options(options, (int)Precision);
             int n = model.Buses.Count, nb = model.Branches.Count;
             var vm = new double[n]; var va = new double[n]; var p = new double[n]; var q = new double[n];
@@ -740,7 +748,7 @@ namespace GridSim.Core.Analysis
             GsPrecision precision, string[] labels, int nOut, ScreenCall call, string name)
         {
             if (nOut == 0) return Array.Empty<ContingencyResult>();
-            GsGrid grid = GsGrid.For(model);
+            GsGrid grid = GsGrid.For(model, options?.FlatStart == true);
             GsNative.PfOpts o = GsNative.Options(options, (int)precision);
             var status = new int[nOut]; var iters = new int[nOut]; var mis = new double[nOut];
             var minVm = new double[nOut]; var maxVm = new double[nOut]; var maxLoad = new double[nOut];
