@@ -467,6 +467,201 @@ def _branch_name(model: GridModel, k: int) -> str:
     return model.branch_label(k)
 
 
+# ---- shared outage dispatch (OutageDispatch.GovernorDroop / Inertia) ---------------------------------------
+# ConverterPlant.Types (Model/Model.cs:207-215): plant types that are converter-interfaced ('_' read as '-')
+CONVERTER_TYPES = frozenset({"wind", "onshore", "offshore", "wind-onshore", "wind-offshore", "solar", "pv", "storage",
+                             "battery", "bess", "interconnector", "hvdc", "tidal"})
+
+
+def _synchronous(model: GridModel) -> np.ndarray:
+    """Per unit: a synchronous machine with a governor, neither power-flow-only nor converter plant
+    (Generator.IsConverterInterfaced, Model/Model.cs:147: the flag, else the type)."""
+    mc = model.machines()
+    out = np.zeros(model.n_gen, bool)
+    for g in range(model.n_gen):
+        conv = (bool(mc["converter"][g]) if mc["converter"][g] >= 0
+                else (mc["gen_type"][g] or "").strip().lower().replace("_", "-") in CONVERTER_TYPES)
+        out[g] = not mc["pf_only"][g] and not conv
+    return out
+
+
+def participation_weights(model: GridModel, units: Sequence[int], bus_type: np.ndarray, dispatch: str,
+                          island: Optional[Sequence[int]] = None, removed_bus: int = -1) -> np.ndarray:
+    """ParticipationWeights (ContingencyAnalysis.cs:1588-1645) over the network after an outage: `units` are the
+    units left (model positions, model order), `bus_type` the bus types after it, `removed_bus` a bus gone with its
+    branches (-1: none), `island` bus positions of the part that lost the power (None: everywhere). A unit takes
+    part when it is synchronous and its bus reaches a reference bus over in-service branches (inside that part);
+    its weight is its machine base (MBase, or the system base when MBase is 0 or less, MachineBase.EffectiveMva)
+    for droop and H times that for inertia. ValueError for a participant whose Pmin is above its Pmax."""
+    n = model.n_bus
+    adj = [[] for _ in range(n)]
+    for k in np.nonzero(model.br_in_service)[0]:
+        f, t = int(model.br_from[k]), int(model.br_to[k])
+        if removed_bus in (f, t):
+            continue
+        adj[f].append(t)
+        adj[t].append(f)
+
+    def flood(seeds):
+        seen = np.zeros(n, bool)
+        queue = [s for s in seeds]
+        seen[queue] = True
+        while queue:
+            u = queue.pop()
+            for v in adj[u]:
+                if not seen[v]:
+                    seen[v] = True
+                    queue.append(v)
+        return seen
+
+    reach = flood([i for i in range(n) if bus_type[i] == 3 and i != removed_bus])
+    if island is not None:
+        reach &= flood([int(i) for i in island])
+    mc = model.machines()
+    sync = _synchronous(model)
+    how = "governor droop" if dispatch == "droop" else "inertia"
+    w = np.zeros(len(units))
+    for p, g in enumerate(units):
+        if not sync[g] or not reach[int(model.gen_bus[g])]:
+            continue
+        mva = float(mc["mbase"][g]) if mc["mbase"][g] > 0.0 else float(model.base_mva)
+        x = mva if dispatch == "droop" else float(mc["inertia_h"][g]) * mva
+        if not (x > 0.0) or not math.isfinite(x):
+            continue
+        if mc["pmin"][g] > mc["pmax"][g]:
+            raise ValueError(f"Outage sharing by {how}: generator {p} at bus {int(model.bus_id[model.gen_bus[g]])} "
+                             f"has Pmin {mc['pmin'][g]:g} MW above Pmax {mc['pmax'][g]:g} MW, so it has no dispatch "
+                             "range to share within.")
+        w[p] = x
+    return w
+
+
+def share_lost_power(model: GridModel, units: Sequence[int], bus_type: np.ndarray, lost_mw: float, dispatch: str,
+                     island: Optional[Sequence[int]] = None, removed_bus: int = -1):
+    """ShareLostPower (ContingencyAnalysis.cs:1509-1579): the net lost MW (positive: generation lost) shared among
+    the participants of :func:`participation_weights` in proportion to their weights, each within [Pmin, Pmax]
+    from its scheduled output; a unit whose share exceeds its headroom is fixed at its limit and the rest shared
+    again among the others, until every share fits or no unit is left (what is left goes to the reference bus).
+    Returns (the new scheduled output of each unit of `units`, the note)."""
+    if dispatch not in ("droop", "inertia"):
+        raise ValueError("ShareLostPower shares among units; the reference-bus mode does not share.")
+    if not math.isfinite(lost_mw):
+        raise ValueError("The lost power must be a finite number of MW.")
+    how = "governor droop" if dispatch == "droop" else "inertia"
+    pg = np.array([float(model.pg[g]) for g in units])
+    if lost_mw == 0.0:
+        return pg, f"no net power lost, nothing to share by {how}"
+    weights = participation_weights(model, units, bus_type, dispatch, island, removed_bus)
+    mc = model.machines()
+    raise_ = lost_mw > 0.0
+    weight, room, delta, active = {}, {}, np.zeros(len(units)), []
+    for p, g in enumerate(units):
+        if not (weights[p] > 0.0):
+            continue
+        r = float(mc["pmax"][g]) - pg[p] if raise_ else pg[p] - float(mc["pmin"][g])
+        if not (r > 0.0):
+            continue
+        weight[p], room[p] = float(weights[p]), r
+        active.append(p)
+    remaining = abs(lost_mw)
+    at_limit = 0
+    participants = len(active)
+    while active and remaining > 0.0:
+        wsum = 0.0
+        for p in active:
+            wsum += weight[p]
+        capped = [p for p in active if remaining * weight[p] / wsum > room[p]]
+        if not capped:
+            for p in active:
+                delta[p] += remaining * weight[p] / wsum
+            remaining = 0.0
+            break
+        for p in capped:
+            delta[p] += room[p]
+            remaining -= room[p]
+            active.remove(p)
+            at_limit += 1
+        if remaining < 0.0:
+            remaining = 0.0
+    sign = 1.0 if raise_ else -1.0
+    for p in range(len(units)):
+        if delta[p] != 0.0:
+            pg[p] = pg[p] + sign * delta[p]
+    note = f"{'lost' if raise_ else 'surplus'} {abs(lost_mw):.1f} MW shared by {how} over {participants} unit(s)"
+    if at_limit > 0:
+        note += f", {at_limit} at a limit"
+    if remaining > 0.0:
+        note += f"; {remaining:.1f} MW beyond their headroom left to the reference"
+    return pg, note
+
+
+def _shared_outage(model: GridModel, kind: int, index: int, dispatch: str):
+    """The shared dispatch of one element outage, as ScreenElementOutage builds it (:1355-1421): None when nothing
+    is shared (a branch outage, or no unit left to take the reference); else (the model to solve the outage on, or
+    None when no power was lost, and the sharing note). The model keeps every element, so the device removes the
+    unit or bus as usual; its remaining units carry the shared output and its reference is already re-elected."""
+    if kind == 0:
+        return None
+    on = [int(g) for g in np.nonzero(model.gen_in_service)[0]]
+    types = model.bus_type.copy()
+    if kind == 1:
+        bus = int(model.gen_bus[index])
+        new_ref, moved_note = ContingencyAnalysis._reelect(model, index, -1, bus)
+        if new_ref is None and moved_note is not None:   # no unit left to take the reference: nothing is solved
+            return None
+        units = [g for g in on if g != index]
+        lost, island, removed = float(model.pg[index]), [bus], -1
+        affected = bus
+    else:
+        new_ref, moved_note = ContingencyAnalysis._reelect(model, -1, index, index)
+        if new_ref is None and moved_note is not None:
+            return None
+        units = [g for g in on if int(model.gen_bus[g]) != index]
+        lost_gen = 0.0
+        for g in on:
+            if int(model.gen_bus[g]) == index:
+                lost_gen += float(model.pg[g])
+        lost = lost_gen - float(model.pd[index])
+        island = []
+        for k in range(model.n_branch):
+            f, t = int(model.br_from[k]), int(model.br_to[k])
+            if model.br_in_service[k] and index in (f, t):
+                nb = t if f == index else f
+                if nb != index:
+                    island.append(nb)
+        removed = affected = index
+    if new_ref is not None:   # ReelectReference: the old reference (or the removed bus) PQ, the new one a reference
+        types[affected] = 1
+        types[new_ref] = 3
+    pg, note = share_lost_power(model, units, types, lost, dispatch, island, removed)
+    if lost == 0.0:
+        return None, note
+    moved = model.copy()
+    moved.bus_type = types
+    moved.pg[units] = pg
+    return moved, note
+
+
+def _merge_rows(raw: dict, subs: dict, keep_states: bool) -> None:
+    """Replace rows of a screen's raw result with single-outage results ({row: raw of one outage})."""
+    for key in ("status", "iterations", "max_mismatch", "min_vm", "max_vm", "max_loading_pct", "worst_boundary_pct",
+                "islanded"):
+        for j, s in subs.items():
+            raw[key][j] = s[key][0]
+    if keep_states:
+        for j, s in subs.items():
+            raw["vm"][j] = s["vm"][0]
+            raw["va_deg"][j] = s["va_deg"][0]
+    ptr = raw["viol_ptr"]
+    rows = []
+    for j in range(ptr.shape[0] - 1):
+        src, a, b = (subs[j], 0, subs[j]["viol_ptr"][1]) if j in subs else (raw, ptr[j], ptr[j + 1])
+        rows.append((src["viol_kind"][a:b], src["viol_element"][a:b], src["viol_value"][a:b]))
+    raw["viol_ptr"] = np.concatenate([[0], np.cumsum([len(r[0]) for r in rows])]).astype(np.int32)
+    for q, key in enumerate(("viol_kind", "viol_element", "viol_value")):
+        raw[key] = (np.concatenate([r[q] for r in rows]) if rows else raw[key][:0]).astype(raw[key].dtype)
+
+
 @dataclass
 class NkScreenReport:
     """NkScreenReport (``ContingencyAnalysis.cs:174-186``): the screened combinations worst first, the single
@@ -503,12 +698,45 @@ class ContingencyAnalysis:
     @staticmethod
     def screen_elements_raw(model: GridModel, kinds: Sequence[int], indices: Sequence[int],
                             solver: SparseNewtonRaphsonPowerFlow, options: PowerFlowOptions,
-                            keep_states: bool = False) -> dict:
-        """One ``gs_element_screen`` call: outage j is the branch / generator / bus indices[j] of kinds[j] (0, 1, 2);
-        generator indices are positions in the model's generator arrays, bus indices bus positions."""
+                            keep_states: bool = False, dispatch: str = "reference") -> dict:
+        """``gs_element_screen``: outage j is the branch / generator / bus indices[j] of kinds[j] (0, 1, 2);
+        generator indices are positions in the model's generator arrays, bus indices bus positions.
+
+        `dispatch` is OutageDispatch (ContingencyAnalysis.cs:120-129): "reference" (the reference bus picks up the
+        lost power; one device call for every outage), "droop" or "inertia" (ShareLostPower moves the remaining
+        units' scheduled output first, :1370-1374 and :1410-1421). A shared outage is solved as the element outage
+        of its own grid: the model with the units moved and the reference already re-elected (ReelectReference
+        works on the output before the sharing), so each costs a grid upload; "share_notes" holds the sharing notes
+        (None where nothing was shared: branch outages, and outages that leave no unit to take the reference)."""
         k = np.ascontiguousarray(kinds, dtype=np.int32)
         idx = np.ascontiguousarray(indices, dtype=np.int32)
-        return ContingencyAnalysis._screen_call(model, idx, ("elements", k), solver, options, keep_states)
+        raw = ContingencyAnalysis._screen_call(model, idx, ("elements", k), solver, options, keep_states)
+        if dispatch == "reference":
+            return raw
+        if dispatch not in ("droop", "inertia"):
+            raise ValueError(f"unknown outage dispatch {dispatch!r}: reference, droop or inertia")
+        if options.warm_start_from_base:
+            raise ValueError("a shared outage dispatch solves each outage from the model's stored voltages, as the "
+                             "reference does; warm_start_from_base is not offered with it")
+        notes = [None] * k.shape[0]
+        own = SparseNewtonRaphsonPowerFlow(solver.precision, solver.ctx)
+        subs = {}
+        for j in range(k.shape[0]):
+            plan = _shared_outage(model, int(k[j]), int(idx[j]), dispatch)
+            if plan is None:
+                continue
+            moved, notes[j] = plan
+            if moved is None:  # nothing to share: the reference-bus solve is the state
+                continue
+            subs[j] = ContingencyAnalysis._screen_call(moved, idx[j:j + 1], ("elements", k[j:j + 1]), own, options,
+                                                       keep_states)
+            if own._grid is not None:
+                own._grid.close()
+                own._grid = None
+        raw["share_notes"] = notes
+        if subs:
+            _merge_rows(raw, subs, keep_states)
+        return raw
 
     @staticmethod
     def _screen_call(model, idx, width, solver, options, keep_states):
@@ -774,16 +1002,17 @@ class ContingencyAnalysis:
 
     @classmethod
     def screen_element_outages(cls, model: GridModel, outages: Sequence, solver: Optional[SparseNewtonRaphsonPowerFlow] = None,
-                               options: Optional[PowerFlowOptions] = None) -> list:
-        """ScreenElementOutages (:1309-1320) with the reference-bus dispatch: one device call for every (kind, index)
-        of `outages` (SingleOutages' indexing), results in order with the reference's labels ("gen 3 at bus 7",
-        "bus 7"), lost load and generation and the reference-move note."""
+                               options: Optional[PowerFlowOptions] = None, dispatch: str = "reference") -> list:
+        """ScreenElementOutages (:1309-1320): every (kind, index) of `outages` (SingleOutages' indexing), results in
+        order with the reference's labels ("gen 3 at bus 7", "bus 7"), lost load and generation and the notes (the
+        reference move, then the sharing). `dispatch`: "reference" (one device call for every outage), "droop" or
+        "inertia" (:meth:`screen_elements_raw`)."""
         solver = solver or SparseNewtonRaphsonPowerFlow()
         options = options or PowerFlowOptions(precision=solver.precision)
         on = np.nonzero(model.gen_in_service)[0]
         kinds = np.array([int(k) for k, _ in outages], np.int32)
         idx = np.array([int(on[i]) if k == 1 else int(i) for k, i in outages], np.int32)
-        raw = cls.screen_elements_raw(model, kinds, idx, solver, options)
+        raw = cls.screen_elements_raw(model, kinds, idx, solver, options, dispatch=dispatch)
         labels = []
         for j, (k, i) in enumerate(outages):
             if k == 0:
@@ -804,6 +1033,9 @@ class ContingencyAnalysis:
                 r.lost_load_mw = float(model.pd[i])
                 r.lost_generation_mw = float(sum(model.pg[g] for g in on if int(model.gen_bus[g]) == i))
                 r.note = cls._reelect(model, -1, int(i), int(i))[1]
+            shared = raw.get("share_notes", [None] * len(res))[j]
+            if shared is not None:
+                r.note = shared if r.note is None else r.note + "; " + shared
         return res
 
     @classmethod

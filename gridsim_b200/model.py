@@ -71,6 +71,16 @@ class GridModel:
     br_name: Optional[List[str]] = None  # branch names ("" = unnamed); None = every branch unnamed
     # transmission boundaries (Boundary, Model/Model.cs:516-560): (name, limit MW, [(branch name, direction)])
     boundaries: List[Tuple[str, float, List[Tuple[str, int]]]] = field(default_factory=list)
+    # machine data of the units (Generator, Model/Model.cs:91-114), read only by the outage dispatch by governor
+    # droop or inertia: Pmin / Pmax (MW), MBase (MVA; 0 or less = the system base), H (s), the plant type, the
+    # power-flow-only flag and the converter flag (-1 = inferred from the type). None = the record's defaults.
+    pmin: Optional[np.ndarray] = None
+    pmax: Optional[np.ndarray] = None
+    mbase: Optional[np.ndarray] = None
+    inertia_h: Optional[np.ndarray] = None
+    gen_type: Optional[List[str]] = None
+    pf_only: Optional[np.ndarray] = None
+    converter: Optional[np.ndarray] = None
     meta: dict = field(default_factory=dict)
     _keep: list = field(default_factory=list, repr=False)
 
@@ -90,6 +100,16 @@ class GridModel:
         kw = {k: (v.copy() if isinstance(v, (np.ndarray, dict, list)) else v) for k, v in self.__dict__.items()
               if k != "_keep"}
         return GridModel(**kw)
+
+    def machines(self) -> dict:
+        """The units' machine data with the Generator record's defaults where the model gives none (Pmin 0,
+        Pmax +inf, MBase 100 MVA, H 0, type "", not power-flow-only, converter flag inferred from the type)."""
+        ng = self.n_gen
+        pick = lambda a, d, dt: np.full(ng, d, dt) if a is None else np.asarray(a, dt)  # noqa: E731
+        return {"pmin": pick(self.pmin, 0.0, np.float64), "pmax": pick(self.pmax, np.inf, np.float64),
+                "mbase": pick(self.mbase, 100.0, np.float64), "inertia_h": pick(self.inertia_h, 0.0, np.float64),
+                "gen_type": list(self.gen_type) if self.gen_type is not None else [""] * ng,
+                "pf_only": pick(self.pf_only, 0, np.uint8), "converter": pick(self.converter, -1, np.int8)}
 
     def branch_label(self, k: int) -> str:
         """A branch's name, or its end buses "from-to" when it has none (ContingencyAnalysis.cs:1168-1172)."""
@@ -195,6 +215,8 @@ class GridModel:
             out["br_name"] = list(self.br_name)
         if self.boundaries:
             out["boundaries"] = [[nm, lim, [list(x) for x in mem]] for nm, lim, mem in self.boundaries]
+        if self.gen_type is not None:
+            out["gen_type"] = list(self.gen_type)
         return out
 
     @staticmethod
@@ -212,7 +234,12 @@ class GridModel:
             rate_a=f64("rate_a"), br_in_service=u8("br_in_service"), is_transformer=u8("is_transformer"),
             rate_b=f64("rate_b") if "rate_b" in d else None, rate_c=f64("rate_c") if "rate_c" in d else None,
             br_name=list(d["br_name"]) if "br_name" in d else None,
-            boundaries=[(nm, float(lim), [(str(b), int(x)) for b, x in mem]) for nm, lim, mem in d.get("boundaries", [])])
+            boundaries=[(nm, float(lim), [(str(b), int(x)) for b, x in mem]) for nm, lim, mem in d.get("boundaries", [])],
+            pmin=f64("pmin") if "pmin" in d else None, pmax=f64("pmax") if "pmax" in d else None,
+            mbase=f64("mbase") if "mbase" in d else None, inertia_h=f64("inertia_h") if "inertia_h" in d else None,
+            gen_type=list(d["gen_type"]) if "gen_type" in d else None,
+            pf_only=u8("pf_only") if "pf_only" in d else None,
+            converter=np.array(d["converter"], np.int8) if "converter" in d else None)
 
 
 # =============================================================================================
@@ -273,7 +300,10 @@ def parse_matpower(text: str, name: str = "matpower") -> GridModel:
         r=g(brs, 2), x=g(brs, 3), b=g(brs, 4), tap=np.where(tap_raw != 0.0, tap_raw, 1.0), shift_deg=g(brs, 9),
         rate_a=g(brs, 5), br_in_service=np.ones(len(brs), np.uint8),
         is_transformer=(tap_raw != 0.0).astype(np.uint8),
-        rate_b=g(brs, 6), rate_c=g(brs, 7))  # RATE_B / RATE_C (MatpowerParser.cs:384-385)
+        rate_b=g(brs, 6), rate_c=g(brs, 7),  # RATE_B / RATE_C (MatpowerParser.cs:384-385)
+        # PMIN / PMAX / MBASE, a zero MBASE replaced by the system base, H 0 (MatpowerParser.cs:272-307)
+        pmin=g(gens, 9), pmax=g(gens, 8, np.inf), mbase=np.where(g(gens, 6) > 0, g(gens, 6), base),
+        inertia_h=np.zeros(len(gens)))
 
 
 def load_matpower(path: str) -> GridModel:
@@ -304,14 +334,24 @@ def save_case_dir(m: GridModel, path: str) -> None:
         buses.append(d)
     dump("buses.json", buses)
     gens = []
+    mach = m.machines()
     for k in range(m.n_gen):
         bi = int(m.gen_bus[k])
-        gens.append({"name": f"G{k}", "bus": int(m.bus_id[bi]),
-                     "role": "slack" if m.bus_type[bi] == SLACK else "pv",
-                     "capacityMva": float(max(abs(m.qmax[k]), abs(m.qmin[k]), abs(m.pg[k]), 1.0)),
-                     "outputMw": float(m.pg[k]), "qOutputMvar": float(m.qg[k]),
-                     "voltageSetpoint": float(m.vg[k]), "qMinMvar": float(m.qmin[k]), "qMaxMvar": float(m.qmax[k]),
-                     "inService": bool(m.gen_in_service[k])})
+        # capacityMva is the unit's MBase when the model has machine data (JsonGridLoader.cs:166)
+        cap = (float(mach["mbase"][k]) if m.mbase is not None and mach["mbase"][k] > 0
+               else float(max(abs(m.qmax[k]), abs(m.qmin[k]), abs(m.pg[k]), 1.0)))
+        g = {"name": f"G{k}", "bus": int(m.bus_id[bi]), "role": "slack" if m.bus_type[bi] == SLACK else "pv",
+             "capacityMva": cap, "outputMw": float(m.pg[k]), "qOutputMvar": float(m.qg[k]),
+             "voltageSetpoint": float(m.vg[k]), "qMinMvar": float(m.qmin[k]), "qMaxMvar": float(m.qmax[k]),
+             "inService": bool(m.gen_in_service[k]), "pMinMw": float(mach["pmin"][k]),
+             "pMaxMw": float(mach["pmax"][k]), "inertiaH": float(mach["inertia_h"][k])}
+        if mach["gen_type"][k]:
+            g["type"] = mach["gen_type"][k]
+        if mach["pf_only"][k]:
+            g["powerFlowOnly"] = True
+        if mach["converter"][k] >= 0:
+            g["converterInterfaced"] = bool(mach["converter"][k])
+        gens.append(g)
     dump("generation.json", gens)
     dump("demand.json", [{"name": f"D{i}", "bus": int(m.bus_id[i]), "pMw": float(m.pd[i]), "qMvar": float(m.qd[i])}
                          for i in range(m.n_bus) if m.pd[i] != 0 or m.qd[i] != 0])
@@ -401,6 +441,14 @@ def load_case_dir(path: str) -> GridModel:
         rate_b=cat(f(lines, "ratingBMva") * circ, f(txs, "ratingBMva") * one),
         rate_c=cat(f(lines, "ratingCMva") * circ, f(txs, "ratingCMva") * one),
         br_name=[l.get("name") or "" for l in lines + txs],
+        # machine data (JsonGridLoader.cs:158-170): Pmin 0 and Pmax capacityMva unless written, MBase capacityMva
+        pmin=f(gens, "pMinMw"), pmax=np.array([float(g["pMaxMw"]) if g.get("pMaxMw") is not None else c
+                                               for g, c in zip(gens, cap)], np.float64),
+        mbase=cap.copy(), inertia_h=f(gens, "inertiaH"),
+        gen_type=[g.get("type") if g.get("type") is not None else "ccgt" for g in gens],
+        pf_only=np.array([1 if g.get("powerFlowOnly", False) else 0 for g in gens], np.uint8),
+        converter=np.array([-1 if g.get("converterInterfaced") is None else int(bool(g["converterInterfaced"]))
+                            for g in gens], np.int8),
         boundaries=[(b.get("name", ""), float(b.get("limitMw", 0.0)),
                      [(x.get("branch", ""), int(x.get("direction", 1))) for x in (b.get("branches") or [])])
                     for b in bnds])

@@ -301,7 +301,7 @@ namespace GridSim.Core.PowerFlow.B200
     /// occurrence, as the solvers key buses; the in-service generators of <see cref="GridModel.Generators"/>, so a
     /// generator index of the screens is the reference's; boundary member names resolved to their one branch) and the
     /// grid handle. One caller at a time uses a grid (<see cref="Sync"/>).</summary>
-    public sealed class GsGrid
+    public sealed class GsGrid : IDisposable
     {
         private static readonly ConditionalWeakTable<GridModel, GsGrid> Cache = new();
         private static readonly ConditionalWeakTable<GridModel, GsGrid> FlatCache = new();
@@ -318,6 +318,16 @@ namespace GridSim.Core.PowerFlow.B200
             ArgumentNullException.ThrowIfNull(model);
             return flatStart ? FlatCache.GetValue(model, m => new GsGrid(m, true)) : Cache.GetValue(model, m => new GsGrid(m, false));
         }
+
+        /// <summary>A device grid of <paramref name="model"/> outside the cache, for a model used once: the caller
+        /// disposes it (its device memory is released at once, not when the collector runs).</summary>
+        public static GsGrid Uncached(GridModel model, bool flatStart = false)
+        {
+            ArgumentNullException.ThrowIfNull(model);
+            return new GsGrid(model, flatStart);
+        }
+
+        public void Dispose() => Native.Dispose();
 
         private GsGrid(GridModel model, bool flatStart)
         {
@@ -681,16 +691,15 @@ namespace GridSim.Core.Analysis
         }
 
         /// <summary>ScreenElementOutages (:1309-1320) with the reference-bus dispatch as one gs_element_screen: labels,
-        /// lost load and generation and the reference-move note as ScreenElementOutage gives them (:1343-1411). Another
-        /// dispatch (governor droop, inertia) runs the CPU screen with <paramref name="cpuSolver"/>.</summary>
+        /// lost load and generation and the notes as ScreenElementOutage gives them (:1343-1421). With governor droop or
+        /// inertia, ShareLostPower moves the remaining units first; each such outage is then solved as the element
+        /// outage of its own moved model (<see cref="MovedForSharing"/>), one device grid per outage.</summary>
         public static IReadOnlyList<ContingencyResult> ScreenElementOutagesCuda(GridModel model, IReadOnlyList<ElementOutage> outages,
             PowerFlowOptions? options = null, OutageDispatch dispatch = OutageDispatch.ReferenceBus,
-            GsPrecision precision = GsPrecision.Fp64, IPowerFlowSolver? cpuSolver = null)
+            GsPrecision precision = GsPrecision.Fp64)
         {
             ArgumentNullException.ThrowIfNull(model);
             ArgumentNullException.ThrowIfNull(outages);
-            if (dispatch != OutageDispatch.ReferenceBus)
-                return ScreenElementOutages(model, outages, cpuSolver, options, dispatch);
             Boundary.RequireResolvedBranchNames(model);
             int nOut = outages.Count;
             var kind = new int[nOut];
@@ -735,20 +744,97 @@ namespace GridSim.Core.Analysis
                     string? note = ReelectReference(model, kept, gens, removedBusId: bus.Id, bus.Id).Note;
                     row = row with { Kind = OutageKind.Bus, LostLoadMw = bus.Pd, LostGenerationMw = lostGen, Note = note };
                 }
+                if (dispatch != OutageDispatch.ReferenceBus && e.Kind != OutageKind.Branch)
+                {
+                    GridModel? moved = MovedForSharing(model, e, dispatch, out string? shareNote);
+                    if (moved is not null && !ReferenceEquals(moved, model))
+                    {
+                        using GsGrid own = GsGrid.Uncached(moved, options?.FlatStart == true);
+                        int[] k1 = { kind[j] }, i1 = { index[j] };
+                        ContingencyResult solved = RunScreen(model, options, precision, new[] { labels[j] }, 1,
+                            (IntPtr g, ref GsNative.PfOpts o, ref GsNative.N1Result r) => GsNative.gs_element_screen(g, 1, k1, i1, ref o, ref r),
+                            "gs_element_screen", own)[0];
+                        row = solved with { Kind = row.Kind, LostLoadMw = row.LostLoadMw, LostGenerationMw = row.LostGenerationMw, Note = row.Note };
+                    }
+                    if (shareNote is not null) row = row with { Note = row.Note is null ? shareNote : row.Note + "; " + shareNote };
+                }
                 results.Add(row);
             }
             return results;
         }
 
+        /// <summary>
+        /// The model a shared-dispatch element outage is solved on (ScreenElementOutage, :1355-1421): ReelectReference
+        /// and ShareLostPower, the reference's own, on the post-outage model, then written back into the full model, so
+        /// that the device removes the unit or bus as usual. Its remaining units carry their shared output, and its
+        /// reference is already re-elected (a removed reference bus is PQ), so the device does not re-elect it again by
+        /// the moved output. Null when nothing is shared (no unit is left to take the reference: the reference-bus row
+        /// stands); <paramref name="model"/> itself when no power was lost.
+        /// </summary>
+        private static GridModel? MovedForSharing(GridModel model, ElementOutage e, OutageDispatch dispatch, out string? shareNote)
+        {
+            shareNote = null;
+            IReadOnlyList<Generator> all = model.Generators;
+            var keep = new List<int>();   // positions in Generators of the units left
+            IReadOnlyList<Branch> branches = model.Branches;
+            double lost;
+            int affected;
+            int? removedBus = null;
+            var island = new List<int>();
+            if (e.Kind == OutageKind.Generator)
+            {
+                Generator gen = all[e.Index];
+                for (int i = 0; i < all.Count; i++) if (i != e.Index) keep.Add(i);
+                lost = gen.Pg;
+                affected = gen.Bus;
+                island.Add(gen.Bus);
+            }
+            else
+            {
+                Bus bus = model.Buses[e.Index];
+                double lostGen = 0.0;
+                for (int i = 0; i < all.Count; i++) { if (all[i].Bus == bus.Id) lostGen += all[i].Pg; else keep.Add(i); }
+                lost = lostGen - bus.Pd;
+                affected = bus.Id;
+                removedBus = bus.Id;
+                var kept = new List<Branch>(model.Branches.Count);
+                foreach (Branch b in model.Branches)
+                {
+                    if (b.From != bus.Id && b.To != bus.Id) { kept.Add(b); continue; }
+                    if (b.InService) island.Add(b.From == bus.Id ? b.To : b.From);
+                }
+                branches = kept;
+            }
+            var gens = new List<Generator>(keep.Count);
+            foreach (int i in keep) gens.Add(all[i]);
+            (IReadOnlyList<Bus>? buses, _, bool noUnitLeft) = ReelectReference(model, branches, gens, removedBusId: removedBus, affected);
+            if (noUnitLeft) return null;
+            IReadOnlyList<Bus> after = buses ?? model.Buses;
+            var reducedBuses = new List<Bus>(after.Count);
+            foreach (Bus b in after) if (removedBus is not int gone || b.Id != gone) reducedBuses.Add(b);
+            GridModel reduced = model.CopyWith(buses: reducedBuses, generators: gens, branches: branches);
+            (GridModel shared, string note) = ShareLostPower(reduced, lost, dispatch, island);
+            shareNote = note;
+            if (lost == 0.0) return model;
+            var movedGens = new Generator[all.Count];
+            for (int i = 0; i < all.Count; i++) movedGens[i] = all[i];
+            for (int p = 0; p < keep.Count; p++) movedGens[keep[p]] = shared.Generators[p];
+            var movedBuses = new List<Bus>(after.Count);
+            foreach (Bus b in after)
+                movedBuses.Add(removedBus is int r && b.Id == r && b.Type == BusType.Slack ? b with { Type = BusType.Pq } : b);
+            return model.CopyWith(buses: movedBuses, generators: movedGens);
+        }
+
         private delegate int ScreenCall(IntPtr grid, ref GsNative.PfOpts opts, ref GsNative.N1Result res);
 
         /// <summary>Run one screen call (again with a larger violation buffer when the library reports
-        /// GS_ERR_CAPACITY) and build its rows.</summary>
+        /// GS_ERR_CAPACITY) on <paramref name="grid"/> (default: the cached grid of <paramref name="model"/>) and build
+        /// its rows, named from <paramref name="model"/>.</summary>
         private static unsafe IReadOnlyList<ContingencyResult> RunScreen(GridModel model, PowerFlowOptions? options,
-            GsPrecision precision, string[] labels, int nOut, ScreenCall call, string name)
+            GsPrecision precision, string[] labels, int nOut, ScreenCall call, string name, GsGrid? grid = null)
         {
             if (nOut == 0) return Array.Empty<ContingencyResult>();
-            GsGrid grid = GsGrid.For(model, options?.FlatStart == true);
+            grid ??= GsGrid.For(model, options?.FlatStart == true);
             GsNative.PfOpts o = GsNative.Options(options, (int)precision);
             var status = new int[nOut]; var iters = new int[nOut]; var mis = new double[nOut];
             var minVm = new double[nOut]; var maxVm = new double[nOut]; var maxLoad = new double[nOut];

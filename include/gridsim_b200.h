@@ -292,8 +292,10 @@ int gs_nk_screen(gs_grid *grid, int32_t n_out, int32_t k, const int32_t *branch_
  * part the reference served (ReelectReference :1440-1488); with no unit there, the outage is reported
  * GS_PF_UNSOLVABLE_PART. These run on the grid analysed with every bus's P and Q rows (identity rows where a bus is
  * PV, the reference or removed in a system). Results as gs_n1_screen; a removed bus is left out of Vmin / Vmax and
- * of the voltage violations, its vm / va_deg entries are the start values. Only the reference-bus dispatch
- * (OutageDispatch.ReferenceBus, the default) is built. */
+ * of the voltage violations, its vm / va_deg entries are the start values. This call is the reference-bus dispatch
+ * (OutageDispatch.ReferenceBus, the default). The shared dispatches (GovernorDroop, Inertia: ShareLostPower
+ * :1509-1579) are the same call on a descriptor whose remaining units carry their shared output and whose reference
+ * is already re-elected (a removed reference bus given as PQ); the host builds it per outage. */
 enum gs_outage_kind { GS_OUTAGE_BRANCH = 0, GS_OUTAGE_GENERATOR = 1, GS_OUTAGE_BUS = 2 };
 int gs_element_screen(gs_grid *grid, int32_t n_out, const int32_t *kind, const int32_t *index, const gs_pf_opts *opts,
                       gs_n1_result *res);

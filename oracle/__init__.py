@@ -43,7 +43,9 @@ def _load():
         lib.gso_nk_screen.argtypes = [ctypes.POINTER(_abi.GridDesc), i32, i32, vp, ctypes.POINTER(_abi.PfOpts), i32,
                                       ctypes.POINTER(_abi.N1Result)]
         lib.gso_element_screen.argtypes = [ctypes.POINTER(_abi.GridDesc), i32, vp, vp, ctypes.POINTER(_abi.PfOpts), i32,
-                                           ctypes.POINTER(_abi.N1Result)]
+                                           ctypes.POINTER(_Machines), vp, ctypes.POINTER(_abi.N1Result)]
+        lib.gso_share_lost_power.argtypes = [ctypes.POINTER(_abi.GridDesc), ctypes.c_double, ctypes.POINTER(_Machines),
+                                             i32, vp, vp, vp]
         lib.gso_outage_topology.argtypes = [ctypes.POINTER(_abi.GridDesc), ctypes.c_double, i32, vp, vp, vp]
         lib.gso_sparse_solve.argtypes = [i32, vp, vp, vp, vp, vp]
         _lib = lib
@@ -52,6 +54,61 @@ def _load():
 
 def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class _Machines(ctypes.Structure):
+    _fields_ = [("dispatch", ctypes.c_int32), ("pmin", ctypes.c_void_p), ("pmax", ctypes.c_void_p),
+                ("mbase", ctypes.c_void_p), ("h", ctypes.c_void_p), ("sync", ctypes.c_void_p)]
+
+
+DISPATCH = {"reference": 0, "droop": 1, "inertia": 2}
+
+# ConverterPlant.Types (Model/Model.cs:207-215): converter-interfaced plant by type, case-insensitive, '_' as '-'
+CONVERTER_TYPES = {"wind", "onshore", "offshore", "wind-onshore", "wind-offshore", "solar", "pv", "storage", "battery",
+                   "bess", "interconnector", "hvdc", "tidal"}
+
+
+def _machines(model, dispatch):
+    """Per descriptor unit: Pmin, Pmax, MBase, H and whether it is a synchronous machine with a governor (not
+    power-flow-only; converter flag, else inferred from the type, Generator.IsConverterInterfaced :147)."""
+    mc = model.machines()
+    conv = [bool(c) if c >= 0 else (t or "").strip().lower().replace("_", "-") in CONVERTER_TYPES
+            for c, t in zip(mc["converter"], mc["gen_type"])]
+    sync = np.array([0 if (pf or cv) else 1 for pf, cv in zip(mc["pf_only"], conv)], np.uint8)
+    keep = [np.ascontiguousarray(mc[k], np.float64) for k in ("pmin", "pmax", "mbase", "inertia_h")] + [sync]
+    s = _Machines(DISPATCH[dispatch], *[_p(a) for a in keep])
+    return s, keep
+
+
+def share_note(stats, dispatch) -> str:
+    """The note ShareLostPower writes (ContingencyAnalysis.cs:1515-1578) from its figures (lost MW, participants,
+    units at a limit, MW left to the reference)."""
+    how = "governor droop" if dispatch == "droop" else "inertia"
+    lost, parts, at_limit, left = float(stats[0]), int(stats[1]), int(stats[2]), float(stats[3])
+    if lost == 0.0:
+        return f"no net power lost, nothing to share by {how}"
+    note = f"{'lost' if lost > 0 else 'surplus'} {abs(lost):.1f} MW shared by {how} over {parts} unit(s)"
+    if at_limit > 0:
+        note += f", {at_limit} at a limit"
+    if left > 0.0:
+        note += f"; {left:.1f} MW beyond their headroom left to the reference"
+    return note
+
+
+def share_lost_power(model, lost_mw, dispatch, island_buses=None):
+    """ShareLostPower on `model` itself: (every descriptor unit's Pg after the sharing, the note). `island_buses`:
+    bus positions of the part that lost the power (None: the whole network). ValueError where the reference throws."""
+    lib = _load()
+    mach, keep = _machines(model, dispatch)
+    isl = np.ascontiguousarray([] if island_buses is None else island_buses, np.int32)
+    pg = np.zeros(model.n_gen)
+    stats = np.zeros(4)
+    d = model.desc()
+    rc = lib.gso_share_lost_power(ctypes.byref(d), float(lost_mw), ctypes.byref(mach),
+                                  -1 if island_buses is None else isl.shape[0], _p(isl), _p(pg), _p(stats))
+    if rc != 0:
+        raise ValueError(f"ShareLostPower refused: lost {lost_mw} MW, dispatch {dispatch}")
+    return pg, share_note(stats, dispatch)
 
 
 def solve(model, opts=None) -> dict:
@@ -85,10 +142,15 @@ def screen_sets(model, sets, opts=None, threads: int = 0, keep_states: bool = Fa
     return _screen(model, sets, sets.shape[1], opts, threads, keep_states)
 
 
-def screen_elements(model, kinds, indices, opts=None, threads: int = 0, keep_states: bool = False) -> dict:
-    """ScreenElementOutages: outage j is the branch / generator / bus indices[j] of kinds[j] (0, 1, 2)."""
+def screen_elements(model, kinds, indices, opts=None, threads: int = 0, keep_states: bool = False,
+                    dispatch: str = "reference") -> dict:
+    """ScreenElementOutages: outage j is the branch / generator / bus indices[j] of kinds[j] (0, 1, 2), its lost
+    power picked up by the reference bus, or shared by governor droop or inertia (`dispatch`); with a shared
+    dispatch "share" holds each outage's (lost MW, participants, units at a limit, MW left), lost MW NaN where
+    nothing was shared, and "notes" the sharing notes (None there)."""
     k = np.ascontiguousarray(kinds, dtype=np.int32)
-    return _screen(model, np.ascontiguousarray(indices, dtype=np.int32), ("elements", k), opts, threads, keep_states)
+    return _screen(model, np.ascontiguousarray(indices, dtype=np.int32), ("elements", k, dispatch), opts, threads,
+                   keep_states)
 
 
 def _screen(model, idx, width, opts, threads, keep_states):
@@ -114,8 +176,11 @@ def _screen(model, idx, width, opts, threads, keep_states):
         if width is None:
             rc = lib.gso_n1_screen(ctypes.byref(d), k, _p(idx), ctypes.byref(o), threads, ctypes.byref(r))
         elif isinstance(width, tuple):
+            mach, keep = _machines(model, width[2])
+            share = np.zeros(4 * k)
             rc = lib.gso_element_screen(ctypes.byref(d), k, _p(width[1]), _p(idx), ctypes.byref(o), threads,
-                                        ctypes.byref(r))
+                                        ctypes.byref(mach), _p(share), ctypes.byref(r))
+            out["share"] = share.reshape(k, 4)
         else:
             rc = lib.gso_nk_screen(ctypes.byref(d), k, width, _p(idx), ctypes.byref(o), threads, ctypes.byref(r))
         if rc == _abi.GS_ERR_CAPACITY:
@@ -132,6 +197,8 @@ def _screen(model, idx, width, opts, threads, keep_states):
         out["va_deg"] = out["va_deg"].reshape(k, n)
     out["base_status"] = r.base_status
     out["base_iterations"] = r.base_iterations
+    if "share" in out:
+        out["notes"] = [None if np.isnan(s[0]) else share_note(s, width[2]) for s in out["share"]]
     return out
 
 

@@ -33,7 +33,13 @@ constexpr double kPi = 3.14159265358979323846;
 
 // ---------------------------------------------------------------------------------------------
 // Model: the GridModel fields the load flow reads (Model/Model.cs:20-35, 91-114, 253-275).
-struct Gen { int bus; double pg, qg, vg, qmin, qmax; };
+struct Gen {
+    int bus;
+    double pg, qg, vg, qmin, qmax;
+    // machine data, read only by the outage dispatch by governor droop or inertia (ShareLostPower)
+    double pmin = 0.0, pmax = std::numeric_limits<double>::infinity(), mbase = 100.0, h = 0.0;
+    bool sync = true;  // a synchronous machine with a governor: not power-flow-only, not converter plant
+};
 struct Br {
     int f, t;
     double r, x, b, tap, shift, rateA;
@@ -90,6 +96,26 @@ Model FromDesc(const gs_grid_desc* d) {
         m.bnd.push_back(b);
     }
     return m;
+}
+
+// Machine data per descriptor unit for the shared outage dispatch (0 reference bus, 1 governor droop, 2 inertia).
+struct GsoMachines {
+    int32_t dispatch;
+    const double *pmin, *pmax, *mbase, *h;
+    const uint8_t* sync;
+};
+
+void AttachMachines(Model& m, const GsoMachines* mc) {
+    for (size_t g = 0; g < m.genOfDesc.size(); g++) {
+        const int p = m.genOfDesc[g];
+        if (p < 0) continue;
+        Gen& u = m.gens[p];
+        u.pmin = mc->pmin[g];
+        u.pmax = mc->pmax[g];
+        u.mbase = mc->mbase[g];
+        u.h = mc->h[g];
+        u.sync = mc->sync[g] != 0;
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1246,6 +1272,97 @@ Reduced ReduceForElement(const Model& m, int kind, int index) {
     return r;
 }
 
+// ParticipationWeights (ContingencyAnalysis.cs:1588-1645): a unit takes part when it is a synchronous machine on a bus
+// that in-service branches connect to a reference bus (within the part `island` names, when given); its weight is
+// its effective machine base (MachineBase.EffectiveMva: MBase, or the system base when MBase is 0 or less) for
+// governor droop, H times that for inertia; a weight that is not a positive finite number takes no part. A
+// participant with Pmin above Pmax has no range to share within: false (the reference refuses it).
+bool ParticipationWeights(const Model& m, int dispatch, const std::vector<int>* island, std::vector<double>& w) {
+    std::vector<std::vector<int>> adj(m.n);
+    for (const Br& b : m.br)
+        if (b.inService) { adj[b.f].push_back(b.t); adj[b.t].push_back(b.f); }
+    auto flood = [&](std::vector<int> queue) {
+        std::vector<char> seen(m.n, 0);
+        for (int x : queue) seen[x] = 1;
+        for (size_t q = 0; q < queue.size(); q++)
+            for (int v : adj[queue[q]]) if (!seen[v]) { seen[v] = 1; queue.push_back(v); }
+        return seen;
+    };
+    std::vector<int> refs;
+    for (int i = 0; i < m.n; i++) if (m.type[i] == 3) refs.push_back(i);
+    std::vector<char> reach = flood(refs);
+    if (island) {
+        std::vector<char> part = flood(*island);
+        for (int i = 0; i < m.n; i++) reach[i] = reach[i] && part[i];
+    }
+    w.assign(m.gens.size(), 0.0);
+    for (size_t i = 0; i < m.gens.size(); i++) {
+        const Gen& g = m.gens[i];
+        if (!g.sync || !reach[g.bus]) continue;
+        const double mva = g.mbase > 0.0 ? g.mbase : m.base;
+        const double x = dispatch == 1 ? mva : g.h * mva;
+        if (!(x > 0.0) || !std::isfinite(x)) continue;
+        if (g.pmin > g.pmax) return false;
+        w[i] = x;
+    }
+    return true;
+}
+
+// ShareLostPower (ContingencyAnalysis.cs:1509-1579): the net lost MW (positive: generation lost) shared among the
+// participants in proportion to their weights, each within [Pmin, Pmax] from its scheduled Pg; a unit whose share
+// exceeds its headroom is fixed at its limit and the rest shared again (units visited in model order). `stats`:
+// lost MW, participants, units fixed at a limit, MW left to the reference. False for a lost MW that is not finite
+// or a participant with crossed limits.
+bool ShareLostPower(Model& m, double lostMw, int dispatch, const std::vector<int>* island, double stats[4]) {
+    if (!std::isfinite(lostMw)) return false;
+    stats[0] = lostMw; stats[1] = 0; stats[2] = 0; stats[3] = 0;
+    if (lostMw == 0.0) return true;
+    std::vector<double> weights;
+    if (!ParticipationWeights(m, dispatch, island, weights)) return false;
+    const size_t n = m.gens.size();
+    std::vector<double> weight(n, 0.0), room(n, 0.0), delta(n, 0.0);
+    std::vector<int> active;
+    const bool raise = lostMw > 0.0;
+    for (size_t i = 0; i < n; i++) {
+        const Gen& g = m.gens[i];
+        const double w = weights[i];
+        if (!(w > 0.0)) continue;
+        const double r = raise ? g.pmax - g.pg : g.pg - g.pmin;
+        if (!(r > 0.0)) continue;
+        weight[i] = w;
+        room[i] = r;
+        active.push_back((int)i);
+    }
+    double remaining = std::fabs(lostMw);
+    int fixedAtLimit = 0;
+    const int participants = (int)active.size();
+    while (!active.empty() && remaining > 0.0) {
+        double wsum = 0.0;
+        for (int i : active) wsum += weight[i];
+        std::vector<int> capped;
+        for (int i : active) if (remaining * weight[i] / wsum > room[i]) capped.push_back(i);
+        if (capped.empty()) {
+            for (int i : active) delta[i] += remaining * weight[i] / wsum;
+            remaining = 0.0;
+            break;
+        }
+        for (int i : capped) {
+            delta[i] += room[i];
+            remaining -= room[i];
+            active.erase(std::find(active.begin(), active.end(), i));
+            fixedAtLimit++;
+        }
+        if (remaining < 0.0) remaining = 0.0;
+    }
+    const double sign = raise ? 1.0 : -1.0;
+    for (size_t i = 0; i < n; i++)
+        if (delta[i] != 0.0) m.gens[i].pg = m.gens[i].pg + sign * delta[i];
+    stats[1] = participants;
+    stats[2] = fixedAtLimit;
+    stats[3] = remaining;
+    return true;
+}
+
 bool OptionsSupported(const gs_pf_opts* o) { return o != nullptr; }
 
 }  // namespace
@@ -1459,9 +1576,11 @@ int gso_nk_screen(const gs_grid_desc* d, int32_t nOut, int32_t k, const int32_t*
 // unit or bus index[j] of kind[j] (0, 1, 2). Results in gs_n1_result's layout over the full model's buses; a removed
 // bus's state entries are 0 and it is in neither Vmin / Vmax nor the voltage violations.
 int gso_element_screen(const gs_grid_desc* d, int32_t nOut, const int32_t* kind, const int32_t* index,
-                       const gs_pf_opts* opt, int32_t threads, gs_n1_result* res) {
+                       const gs_pf_opts* opt, int32_t threads, const GsoMachines* mach, double* share, gs_n1_result* res) {
     if (!d || !res || !OptionsSupported(opt) || nOut < 0) return GS_ERR_INVALID_ARG;
     Model m = FromDesc(d);
+    const int dispatch = mach ? mach->dispatch : 0;
+    if (mach) AttachMachines(m, mach);
     for (int j = 0; j < nOut; j++) {
         if (kind[j] == 0 && (index[j] < 0 || index[j] >= (int)m.br.size() || !m.br[index[j]].inService)) return GS_ERR_INVALID_ARG;
         if (kind[j] == 1 && (index[j] < 0 || index[j] >= (int)m.genOfDesc.size() || m.genOfDesc[index[j]] < 0)) return GS_ERR_INVALID_ARG;
@@ -1485,7 +1604,11 @@ int gso_element_screen(const gs_grid_desc* d, int32_t nOut, const int32_t* kind,
     std::vector<uint8_t> islanded(nOut, 0);
     std::vector<std::vector<int>> busOf(nOut);
     const int partsBefore = ConnectedParts(m, -1);
+    if (share)
+        for (int j = 0; j < nOut; j++)
+            for (int q = 0; q < 4; q++) share[4 * j + q] = q == 0 ? std::numeric_limits<double>::quiet_NaN() : 0.0;
     std::atomic<int> cursor{0};
+    std::atomic<int> refused{0};
     auto work = [&]() {
         for (;;) {
             const int j = cursor.fetch_add(1);
@@ -1499,6 +1622,29 @@ int gso_element_screen(const gs_grid_desc* d, int32_t nOut, const int32_t* kind,
                 skip = index[j];
             } else {
                 r = ReduceForElement(m, kind[j], index[j]);
+                // ScreenElementOutage (:1370-1374, :1410-1421): a shared dispatch moves the remaining units before
+                // the re-solve; the part that lost the power is the unit's bus, or the removed bus's neighbours
+                if (dispatch != 0 && !r.noReference) {
+                    double lost;
+                    std::vector<int> island;
+                    if (kind[j] == 1) {
+                        const Gen& g = m.gens[m.genOfDesc[index[j]]];
+                        lost = g.pg;
+                        island.push_back(g.bus);
+                    } else {
+                        double lostGen = 0.0;
+                        for (const Gen& g : m.gens) if (g.bus == index[j]) lostGen += g.pg;
+                        lost = lostGen - m.pd[index[j]];
+                        for (const Br& b : m.br)
+                            if (b.inService && (b.f == index[j] || b.t == index[j])) {
+                                const int nb = r.busOf[b.f == index[j] ? b.t : b.f];
+                                if (nb >= 0) island.push_back(nb);
+                            }
+                    }
+                    double st[4];
+                    if (!ShareLostPower(r.m, lost, dispatch, &island, st)) { refused = 1; busOf[j] = r.busOf; continue; }
+                    if (share) for (int q = 0; q < 4; q++) share[4 * j + q] = st[q];
+                }
             }
             busOf[j] = r.busOf;
             const Model& red = r.m;
@@ -1530,6 +1676,7 @@ int gso_element_screen(const gs_grid_desc* d, int32_t nOut, const int32_t* kind,
     for (int t = 1; t < nt; t++) pool.emplace_back(work);
     work();
     for (auto& th : pool) th.join();
+    if (refused) return GS_ERR_INVALID_ARG;
     int total = 0;
     for (int j = 0; j < nOut; j++) total += (int)viol[j].size();
     res->viol_count = total;
@@ -1565,6 +1712,23 @@ int gso_element_screen(const gs_grid_desc* d, int32_t nOut, const int32_t* kind,
 
 // The topology verdicts of single-branch outages (the product's gs_outage_topology), the reference's way: per outage,
 // ConnectedParts of the reduced model against the intact one and ProvablyUnsolvablePart of the reduced model.
+// ShareLostPower on the model of `d` (no outage taken): `lostMw` shared by mach->dispatch among its units, within the
+// part the island bus positions name (n_island < 0: the whole network). pg_out [n_gen] receives every descriptor
+// unit's scheduled output after the sharing; stats [4]: lost MW, participants, units fixed at a limit, MW left to
+// the reference. GS_ERR_INVALID_ARG for the reference-bus dispatch, a lost MW that is not finite, or a participant
+// with Pmin above Pmax (the reference refuses each).
+int gso_share_lost_power(const gs_grid_desc* d, double lostMw, const GsoMachines* mach, int32_t nIsland,
+                         const int32_t* island, double* pgOut, double* stats) {
+    if (!d || !mach || !pgOut || !stats || mach->dispatch < 1 || mach->dispatch > 2) return GS_ERR_INVALID_ARG;
+    Model m = FromDesc(d);
+    AttachMachines(m, mach);
+    std::vector<int> isl;
+    if (nIsland >= 0) isl.assign(island, island + nIsland);
+    if (!ShareLostPower(m, lostMw, mach->dispatch, nIsland >= 0 ? &isl : nullptr, stats)) return GS_ERR_INVALID_ARG;
+    for (int g = 0; g < d->n_gen; g++) pgOut[g] = m.genOfDesc[g] >= 0 ? m.gens[m.genOfDesc[g]].pg : d->pg[g];
+    return GS_OK;
+}
+
 int gso_outage_topology(const gs_grid_desc* d, double tol, int32_t nOut, const int32_t* idx, uint8_t* splits,
                         uint8_t* unsolvable) {
     if (!d || nOut < 0) return GS_ERR_INVALID_ARG;
