@@ -493,26 +493,17 @@ def participation_weights(model: GridModel, units: Sequence[int], bus_type: np.n
     part when it is synchronous and its bus reaches a reference bus over in-service branches (inside that part);
     its weight is its machine base (MBase, or the system base when MBase is 0 or less, MachineBase.EffectiveMva)
     for droop and H times that for inertia. ValueError for a participant whose Pmin is above its Pmax."""
-    n = model.n_bus
-    adj = [[] for _ in range(n)]
-    for k in np.nonzero(model.br_in_service)[0]:
-        f, t = int(model.br_from[k]), int(model.br_to[k])
-        if removed_bus in (f, t):
-            continue
-        adj[f].append(t)
-        adj[t].append(f)
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
 
-    def flood(seeds):
-        seen = np.zeros(n, bool)
-        queue = [s for s in seeds]
-        seen[queue] = True
-        while queue:
-            u = queue.pop()
-            for v in adj[u]:
-                if not seen[v]:
-                    seen[v] = True
-                    queue.append(v)
-        return seen
+    n = model.n_bus
+    on = (model.br_in_service != 0) & (model.br_from != removed_bus) & (model.br_to != removed_bus)
+    f, t = model.br_from[on], model.br_to[on]
+    graph = coo_matrix((np.ones(f.shape[0]), (f, t)), shape=(n, n))
+    _, part = connected_components(graph, directed=False)
+
+    def flood(seeds):   # the buses in-service branches connect to a seed: the seeds' connected parts
+        return np.isin(part, part[np.asarray(seeds, np.int64)]) if len(seeds) else np.zeros(n, bool)
 
     reach = flood([i for i in range(n) if bus_type[i] == 3 and i != removed_bus])
     if island is not None:
@@ -622,13 +613,9 @@ def _shared_outage(model: GridModel, kind: int, index: int, dispatch: str):
             if int(model.gen_bus[g]) == index:
                 lost_gen += float(model.pg[g])
         lost = lost_gen - float(model.pd[index])
-        island = []
-        for k in range(model.n_branch):
-            f, t = int(model.br_from[k]), int(model.br_to[k])
-            if model.br_in_service[k] and index in (f, t):
-                nb = t if f == index else f
-                if nb != index:
-                    island.append(nb)
+        touch = (model.br_in_service != 0) & ((model.br_from == index) | (model.br_to == index))
+        other = np.where(model.br_from[touch] == index, model.br_to[touch], model.br_from[touch])
+        island = [int(x) for x in other if x != index]
         removed = affected = index
     if new_ref is not None:   # ReelectReference: the old reference (or the removed bus) PQ, the new one a reference
         types[affected] = 1
