@@ -127,6 +127,7 @@ struct gs_server {
     std::deque<gs::serve::ServeTicket> incoming;
     std::deque<gs::serve::ServeResponse> done;
     uint64_t nextTicket = 1;
+    bool batch = false;  // Q limits or the DC retry: queued requests answered in batches (AdvanceBatch)
     bool started = false, stopping = false, abort = false, loopEnded = false, failed = false;
     int64_t submitted = 0, completed = 0;
     std::atomic<int64_t> ticks{0}, systemSteps{0};
@@ -286,6 +287,64 @@ bool Advance(gs_server* S, Lane& L, int laneIndex, cudaError_t* err) {
     return true;
 }
 
+// Batch mode (Q limits or the DC retry): a request's system changes between Newton passes (PV -> PQ switching, a
+// second solve from DC angles), so it is not stepped in a slot; every request queued for the lane is answered by one
+// gs_pf_solve_batch on the grid's own workspace, and requests that arrive meanwhile wait for the next batch. False
+// when the lane has nothing queued; *rc is the call's status (the requests stay queued on a failure).
+bool AdvanceBatch(gs_server* S, Lane& L, int laneIndex, int* rc) {
+    *rc = GS_OK;
+    if (L.pending.empty()) return false;
+    std::vector<ServeTicket> take(L.pending.begin(), L.pending.end());
+    L.pending.clear();
+    const int count = (int)take.size();
+    const size_t n = (size_t)L.G->sym.n;
+    bool anyState = false;
+    std::vector<int32_t> outage(count), status(count), iters(count);
+    std::vector<double> mis(count);
+    const auto admit = ServeClock::now();
+    for (int k = 0; k < count; k++) {
+        outage[k] = take[k].req.outage;
+        anyState = anyState || take[k].req.want_state != 0;
+        take[k].admit = admit;
+    }
+    std::vector<double> vm(anyState ? count * n : 0), va(anyState ? count * n : 0);
+    *rc = gs_pf_solve_batch(L.G, count, nullptr, outage.data(), &S->opts.pf, status.data(), iters.data(), mis.data(),
+                            anyState ? vm.data() : nullptr, anyState ? va.data() : nullptr);
+    if (*rc != GS_OK) {
+        L.pending.insert(L.pending.begin(), take.begin(), take.end());
+        return true;
+    }
+    S->ticks++;
+    S->systemSteps += count;
+    const auto now = ServeClock::now();
+    for (int k = 0; k < count; k++) {
+        const ServeTicket& t = take[k];
+        ServeResponse out;
+        out.r.ticket = t.ticket;
+        out.r.tag = t.req.tag;
+        out.r.grid = laneIndex;
+        out.r.outage = t.req.outage;
+        out.r.status = status[k];
+        out.r.iterations = iters[k];
+        out.r.max_mismatch = mis[k];
+        out.r.queue_ms = MsBetween(t.submit, t.admit);
+        out.r.latency_ms = MsBetween(t.submit, now);
+        out.r.state_offset = -1;
+        if (t.req.want_state) {
+            out.state.assign(vm.begin() + k * n, vm.begin() + (k + 1) * n);
+            out.state.insert(out.state.end(), va.begin() + k * n, va.begin() + (k + 1) * n);
+        }
+        {
+            std::lock_guard<std::mutex> l(S->mu);
+            S->done.push_back(std::move(out));
+            S->completed++;
+        }
+        S->inFlight--;
+    }
+    S->cvOut.notify_all();
+    return true;
+}
+
 // Answer everything still outstanding with GS_PF_NOT_RUN (after a CUDA error stopped the loop).
 void FailOutstanding(gs_server* S) {
     std::vector<ServeTicket> all;
@@ -339,10 +398,13 @@ void ServeLoop(gs_server* S) {
         }
         bool progress = false;
         cudaError_t err = cudaSuccess;
-        for (size_t k = 0; k < S->lanes.size() && err == cudaSuccess; k++)
-            progress |= mixed ? Advance<float>(S, *S->lanes[k], (int)k, &err) : Advance<double>(S, *S->lanes[k], (int)k, &err);
-        if (err != cudaSuccess) {
-            SetErr(S->ctx, GS_ERR_CUDA, std::string("request loop: ") + cudaGetErrorString(err));
+        int rc = GS_OK;
+        for (size_t k = 0; k < S->lanes.size() && err == cudaSuccess && rc == GS_OK; k++) {
+            if (S->batch) progress |= AdvanceBatch(S, *S->lanes[k], (int)k, &rc);
+            else progress |= mixed ? Advance<float>(S, *S->lanes[k], (int)k, &err) : Advance<double>(S, *S->lanes[k], (int)k, &err);
+        }
+        if (err != cudaSuccess || rc != GS_OK) {
+            if (err != cudaSuccess) SetErr(S->ctx, GS_ERR_CUDA, std::string("request loop: ") + cudaGetErrorString(err));
             {
                 std::lock_guard<std::mutex> l(S->mu);
                 S->failed = true;
@@ -374,8 +436,11 @@ int gs_serve_create(gs_ctx* ctx, const gs_serve_opts* opts, gs_server** out) {
     int rc = CheckOpts(ctx, &opts->pf);
     if (rc) return rc;
     if (opts->pf.flat_start) return SetErr(ctx, GS_ERR_UNSUPPORTED, "flat_start: pass a flat start in the descriptor");
-    if (opts->pf.enforce_q_limits) return SetErr(ctx, GS_ERR_UNSUPPORTED, "enforce_q_limits: not in the request loop");
-    if (opts->pf.retry_from_dc_start) return SetErr(ctx, GS_ERR_UNSUPPORTED, "retry_from_dc_start: not in the request loop");
+    // Q limits and the DC retry (the options of the reference's rpc solve, src/GridSim.Cli/RpcCommand.cs:675-676):
+    // answered in batches (AdvanceBatch), each request from the case's stored voltages as gs_pf_solve_batch starts them
+    const bool batch = opts->pf.enforce_q_limits || opts->pf.retry_from_dc_start;
+    if (batch && opts->pf.warm_start_from_base)
+        return SetErr(ctx, GS_ERR_UNSUPPORTED, "warm_start_from_base with Q limits or the DC retry: not in the request loop");
     const int slots = opts->slots_per_grid ? opts->slots_per_grid : GS_SERVE_MAX_SLOTS;
     if (slots < 32 || slots > GS_SERVE_MAX_SLOTS || slots % 32)
         return SetErr(ctx, GS_ERR_INVALID_ARG, "slots_per_grid must be a multiple of 32 in [32, 128]");
@@ -387,6 +452,7 @@ int gs_serve_create(gs_ctx* ctx, const gs_serve_opts* opts, gs_server** out) {
     auto* S = new gs_server();
     S->ctx = ctx;
     S->opts = *opts;
+    S->batch = batch;
     S->opts.slots_per_grid = slots;
     if (S->opts.state_slots == 0) S->opts.state_slots = 16;
     S->budget = (opts->hbm_fraction > 0 ? opts->hbm_fraction : 0.5) * (double)freeB;
@@ -406,6 +472,11 @@ int gs_serve_add_grid(gs_server* S, gs_grid* G, int32_t* index) {
     const Symbolic& s = G->sym;
     auto L = std::make_unique<Lane>();
     L->G = G;
+    if (S->batch) {  // answered through gs_pf_solve_batch on the grid's own workspace: no slot batch
+        *index = (int32_t)S->lanes.size();
+        S->lanes.push_back(std::move(L));
+        return GS_OK;
+    }
     L->stateSlots = std::min(S->opts.state_slots, S->opts.slots_per_grid);
     const double per = (double)PerSystemBytes(s, o.precision);
     const double fixed = (double)L->stateSlots * 2.0 * s.n * 8.0 + 2.0 * s.n * 8.0;

@@ -136,11 +136,11 @@ typedef struct gs_pf_opts {
     int32_t max_iterations;         /* default 30 (StudyOptions 100) */
     int32_t flat_start;             /* default 0 */
     int32_t enforce_q_limits;       /* PV->PQ switching passes (SparseNewtonRaphsonPowerFlow.cs:118-160); default 0
-                                       here (the reference's default is on); refused by the multi-grid batch and
-                                       the request loop */
+                                       here (the reference's default is on); refused by the multi-grid batch;
+                                       the request loop answers in batches with it */
     int32_t retry_from_dc_start;    /* solve a stalled case again from DC power-flow angles (NewtonShell.SolveWithRetry,
                                        NewtonShell.cs:227-268); default 0 here (the reference's default is on);
-                                       refused by the multi-grid batch and the request loop */
+                                       refused by the multi-grid batch; the request loop answers in batches */
     int32_t per_bus_voltage_limits; /* judge buses against their own vmin/vmax (VoltageLimits.cs:55-67) */
     int32_t precision;              /* enum gs_precision */
     int32_t warm_start_from_base;   /* screens: solve the intact grid first and start every outage from
@@ -368,7 +368,12 @@ int gs_pf_solve_multi(gs_ctx *ctx, int32_t n_grids, gs_grid *const *grids, const
  * is added (admission by free HBM); a request waits on the host until its grid has a free slot. A system's
  * arithmetic does not depend on its slot or on the other requests: a request's result is the same alone
  * and in any mix. Outage requests start from the grid's solved base case when pf.warm_start_from_base is
- * set; base-case requests (outage -1) start from the case's stored voltages, as gs_pf_solve does. */
+ * set; base-case requests (outage -1) start from the case's stored voltages, as gs_pf_solve does.
+ * With Q limits or the DC retry (the options of the reference's rpc solve, RpcCommand.cs:675-676) a request's system
+ * changes between Newton passes, so it is not stepped in a slot: the loop answers each grid's queued requests with
+ * one gs_pf_solve_batch (every request from the case's stored voltages; warm starts are refused with these options),
+ * and requests that arrive meanwhile wait for the next batch. That batch runs on the context's stream and the grid's
+ * own workspace: while such a loop runs, make no other solve call on its context. */
 typedef struct gs_server gs_server;
 
 #define GS_SERVE_MAX_SLOTS 128

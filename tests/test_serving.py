@@ -154,3 +154,50 @@ def test_bad_requests_are_refused(population):
             LoadFlowServer(_opts(), slots_per_grid=48)  # not a multiple of 32
     finally:
         srv.close()
+
+
+def test_requests_with_q_limits_and_the_retry_are_answered_in_batches():
+    """The reference's rpc solve options (100 iterations, Q limits on, the DC retry on: RpcCommand.cs:675-676): the
+    loop answers them through batch solves, held to the oracle like the slot-stepped requests."""
+    from gridsim_b200.engine import study_options
+    from tests.conftest import assert_states_close
+
+    m, _ = golden_model("case118")
+    opt = study_options()
+    idx = m.in_service_branches()[:30]
+    srv = LoadFlowServer(opt)
+    try:
+        g = srv.add_grid(m)
+        srv.start()
+        reqs = [(g, -1, 1)] * 3 + [(g, int(k), 1) for k in idx]
+        tickets = srv.submit(reqs)
+        got = {r.ticket: r for r in drain(srv, len(reqs))}
+        base = oracle.solve(m, opt.to_c())
+        ref = oracle.screen(m, idx, opt.to_c(), keep_states=True)
+        for j, (req, t) in enumerate(zip(reqs, tickets)):
+            r = got[int(t)]
+            if req[1] < 0:
+                assert r.status == base["status"] == _abi.PF_CONVERGED
+                assert np.max(np.abs(r.vm - base["vm"])) <= VM_TOL
+                assert np.max(np.abs(np.radians(r.va_deg - base["va_deg"]))) <= VA_TOL_RAD
+                continue
+            k = j - 3
+            if ref["status"][k] == _abi.PF_UNSOLVABLE_PART:
+                assert r.status != _abi.PF_CONVERGED
+                continue
+            assert r.status == ref["status"][k], req
+            if r.status == _abi.PF_CONVERGED:
+                assert_states_close(m, [req[1]], r.vm, r.va_deg, ref["vm"][k], ref["va_deg"][k], VM_TOL, VA_TOL_RAD)
+        st = srv.stats()
+        assert st["completed"] == st["submitted"] == len(reqs) and st["failed"] == 0
+    finally:
+        srv.close()
+
+
+def test_warm_starts_with_q_limits_are_refused():
+    from gridsim_b200.engine import study_options
+
+    opt = study_options()
+    opt.warm_start_from_base = True
+    with pytest.raises(EngineError):
+        LoadFlowServer(opt)
