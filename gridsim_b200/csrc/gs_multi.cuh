@@ -204,8 +204,6 @@ extern "C" int gs_pf_solve_multi(gs_ctx* ctx, int32_t nGrids, gs_grid* const* gr
     if (rc) return rc;
     const gs_pf_opts o = *opts;
     if (o.flat_start) return SetErr(ctx, GS_ERR_UNSUPPORTED, "flat_start: pass a flat start in the descriptor");
-    if (o.enforce_q_limits) return SetErr(ctx, GS_ERR_UNSUPPORTED, "enforce_q_limits: not in the multi-grid batch");
-    if (o.retry_from_dc_start) return SetErr(ctx, GS_ERR_UNSUPPORTED, "retry_from_dc_start: not in the multi-grid batch");
     // cases, their offsets and the sizes of the largest grid
     int64_t nCases = 0, nStates = 0;
     int maxN = 1, maxM = 1;
@@ -238,6 +236,36 @@ extern "C" int gs_pf_solve_multi(gs_ctx* ctx, int32_t nGrids, gs_grid* const* gr
     if (nCases == 0) return GS_OK;
     GS_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
+    // Q limits and the DC retry (ContingencyAnalysis.StudyOptions, ContingencyAnalysis.cs:263-268): a case's system
+    // changes between Newton passes, which the one-CTA-per-case solve does not carry; each grid's cases then run as
+    // one batch solve (the load scales, outages and states of a grid are contiguous in both layouts)
+    if (o.enforce_q_limits || o.retry_from_dc_start) {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        GS_CUDA(cudaEventCreate(&e0));
+        GS_CUDA(cudaEventCreate(&e1));
+        struct Events { cudaEvent_t a, b; ~Events() { cudaEventDestroy(a); cudaEventDestroy(b); } } evs{e0, e1};
+        GS_CUDA(cudaEventRecord(e0, st));
+        for (int k = 0; k < nGrids; k++) {
+            if (counts[k] == 0) continue;
+            const int64_t c0 = caseBase[k], s0 = stateBase[k];
+            rc = gs_pf_solve_batch(grids[k], counts[k], loadScale ? loadScale + s0 : nullptr, outage ? outage + c0 : nullptr,
+                                   &o, status ? status + c0 : nullptr, iterations ? iterations + c0 : nullptr,
+                                   maxMismatch ? maxMismatch + c0 : nullptr, vmOut ? vmOut + s0 : nullptr,
+                                   vaOut ? vaOut + s0 : nullptr);
+            if (rc) return rc;
+        }
+        GS_CUDA(cudaEventRecord(e1, st));
+        GS_CUDA(cudaEventSynchronize(e1));
+        if (stats) {
+            float ms = 0;
+            GS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            stats->device_ms = ms;
+            stats->items = (int32_t)nCases;
+            if (iterations)
+                for (int64_t c = 0; c < nCases; c++) stats->system_steps += iterations[c];
+        }
+        return GS_OK;
+    }
     // items, largest grid first (a grid's cases stay together, in case order)
     std::vector<int> order(nGrids);
     for (int k = 0; k < nGrids; k++) order[k] = k;

@@ -136,11 +136,11 @@ typedef struct gs_pf_opts {
     int32_t max_iterations;         /* default 30 (StudyOptions 100) */
     int32_t flat_start;             /* default 0 */
     int32_t enforce_q_limits;       /* PV->PQ switching passes (SparseNewtonRaphsonPowerFlow.cs:118-160); default 0
-                                       here (the reference's default is on); refused by the multi-grid batch;
-                                       the request loop answers in batches with it */
+                                       here (the reference's default is on); the multi-grid batch and the
+                                       request loop run it through batch solves */
     int32_t retry_from_dc_start;    /* solve a stalled case again from DC power-flow angles (NewtonShell.SolveWithRetry,
                                        NewtonShell.cs:227-268); default 0 here (the reference's default is on);
-                                       refused by the multi-grid batch; the request loop answers in batches */
+                                       the multi-grid batch and the request loop run it through batch solves */
     int32_t per_bus_voltage_limits; /* judge buses against their own vmin/vmax (VoltageLimits.cs:55-67) */
     int32_t precision;              /* enum gs_precision */
     int32_t warm_start_from_base;   /* screens: solve the intact grid first and start every outage from
@@ -340,7 +340,10 @@ int gs_outage_topology(const gs_grid_desc *desc, double tolerance, int32_t n_out
  * on different grids, each case from its case's stored voltages.
  * Per-case arrays are concatenated grid after grid, case after case: load_scale (NULL = 1) and the states
  * vm / va_deg (may be NULL) hold counts[k] * n_bus(k) values for grid k; outage, status, iterations and
- * max_mismatch hold one value per case (outage NULL or -1 = none). */
+ * max_mismatch hold one value per case (outage NULL or -1 = none).
+ * With Q limits or the DC retry (ContingencyAnalysis.StudyOptions) a case's system changes between Newton passes,
+ * which the one-CTA-per-case solve does not carry: each grid's cases then run as one gs_pf_solve_batch, and stats
+ * reports the CUDA-event time around them, the cases and the summed iterations (no CTA shape). */
 typedef struct gs_multi_stats {
     double device_ms;          /* the graph launch (CUDA events) */
     double tune_ms;            /* autotuning trials of this call (0 when the choice was cached) */

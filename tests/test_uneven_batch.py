@@ -78,3 +78,28 @@ def test_uneven_batch_counts_may_be_zero(population):
         assert (r["status"][1] == _abi.PF_CONVERGED).all()
     finally:
         batch.close()
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_uneven_batch_under_study_options(population, precision):
+    """ContingencyAnalysis.StudyOptions (100 iterations, Q limits, the DC retry): each grid's cases run as one batch
+    solve, held to the oracle like the persistent launch."""
+    from gridsim_b200.engine import study_options
+    from tests.conftest import assert_states_close
+
+    models, scales, outs = population
+    opt = study_options(precision)
+    batch = UnevenBatch(models)
+    try:
+        r = batch.solve([CASES] * len(models), scales, outs, opt, keep_states=True)
+        assert batch.stats["items"] == CASES * len(models)
+        for k, m in enumerate(models):
+            for c in range(CASES):
+                ref = _oracle_case(m, scales[k][c], int(outs[k][c]), opt.to_c())
+                assert r["status"][k][c] == ref["status"], (k, c)
+                if ref["status"] == _abi.PF_CONVERGED:
+                    assert r["max_mismatch"][k][c] < 1e-8
+                    assert_states_close(m, [int(outs[k][c])], r["vm"][k][c], r["va_deg"][k][c], ref["vm"], ref["va_deg"],
+                                        VM_TOL, VA_TOL_RAD)
+    finally:
+        batch.close()
