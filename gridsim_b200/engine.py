@@ -32,8 +32,9 @@ from .model import GridModel
 class PowerFlowOptions:
     """PowerFlowOptions (``PowerFlow/PowerFlowOptions.cs``). Q-limit enforcement (PV -> PQ switching passes,
     up to 100, with the reference's reverts) and the DC-angle retry of stalled solves run for single solves, batch
-    solves and screens. Both default to off here (the reference defaults them on, ``PowerFlowOptions.cs:98,121``)
-    because the benchmark workloads run without them."""
+    solves and screens, and through batch solves in the multi-grid batch and the request loop. Both default to off
+    here (the reference defaults them on, ``PowerFlowOptions.cs:98,121``) because the benchmark workloads run
+    without them. ``flat_start`` reaches the library as the flat-start copy of the model (:meth:`device_model`)."""
     tolerance: float = 1e-8
     max_iterations: int = 30
     diverge_limit_pu: float = 10.0
