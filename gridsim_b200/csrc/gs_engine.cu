@@ -3192,6 +3192,49 @@ uint64_t PatternHash(int n, const int* rp, const int* ci) {  // FNV-1a over the 
 }
 
 // The analysed pattern of a (validated) CSR matrix: from the context's cache, or analysed and uploaded now.
+// A row order whose diagonal is structurally zero-free: rowAt[c] = the row placed at position c. Empty when every row
+// holds its own diagonal entry (the order is the identity); else a maximum transversal grown from the rows that do,
+// by augmenting paths (depth first, iterative); {-1} when the pattern has none (structurally singular: the static
+// pivots then report every system of it singular). The reference pivots by rows instead (SparseLuFactorization.cs:
+// 69-195); with a zero-free diagonal the static diagonal pivots of the analysed order take the place of that choice.
+std::vector<int> RowTransversal(int n, const int* rp, const int* ci) {
+    std::vector<int> rowOfCol(n, -1), colOfRow(n, -1);
+    bool full = true;
+    for (int i = 0; i < n; i++) {
+        for (int p = rp[i]; p < rp[i + 1]; p++)
+            if (ci[p] == i) { rowOfCol[i] = i; colOfRow[i] = i; }
+        full = full && colOfRow[i] == i;
+    }
+    if (full) return {};
+    std::vector<int> mark(n, -1), via(n, -1), next(n, 0), path;
+    for (int r0 = 0; r0 < n; r0++) {
+        if (colOfRow[r0] >= 0) continue;
+        path.assign(1, r0);
+        next[r0] = rp[r0];
+        int found = -1;
+        while (!path.empty() && found < 0) {  // path: r0 and the rows reached from it through matched columns
+            const int u = path.back();
+            if (next[u] == rp[u + 1]) { path.pop_back(); continue; }
+            const int c = ci[next[u]++];
+            if (mark[c] == r0) continue;
+            mark[c] = r0;
+            if (rowOfCol[c] < 0) { found = c; break; }
+            const int w = rowOfCol[c];
+            via[w] = c;
+            next[w] = rp[w];
+            path.push_back(w);
+        }
+        if (found < 0) return {-1};
+        for (int k = (int)path.size() - 1, c = found; k >= 0; k--) {  // each row on the path takes the next column
+            const int u = path[k];
+            colOfRow[u] = c;
+            rowOfCol[c] = u;
+            c = k > 0 ? via[u] : -1;
+        }
+    }
+    return rowOfCol;
+}
+
 int PatternOf(gs_ctx* ctx, int n, const int* rp, const int* ci, MatrixPattern** out) {
     const uint64_t h = PatternHash(n, rp, ci);
     auto& v = ctx->patterns;
@@ -3211,11 +3254,34 @@ int PatternOf(gs_ctx* ctx, int n, const int* rp, const int* ci, MatrixPattern** 
     P->colIdx.assign(ci, ci + rp[n]);
     P->grid = std::make_unique<gs_grid>();
     P->grid->ctx = ctx;
-    const std::string err = AnalyzeMatrix(n, rp, ci, P->grid->sym, P->aSlot);
+    // rows reordered to a zero-free diagonal where needed: the analysis runs on that order; a stored entry keeps its
+    // slot through the map below and b's row i goes where row i went (the unknowns keep their order)
+    const std::vector<int> rowAt = RowTransversal(n, rp, ci);
+    const bool permuted = !rowAt.empty() && rowAt[0] >= 0;
+    std::vector<int> rp2, ci2, posOfRow;
+    if (permuted) {
+        rp2.assign(n + 1, 0);
+        posOfRow.assign(n, 0);
+        for (int c = 0; c < n; c++) {
+            const int r = rowAt[c];
+            posOfRow[r] = c;
+            rp2[c + 1] = rp2[c] + (rp[r + 1] - rp[r]);
+            ci2.insert(ci2.end(), ci + rp[r], ci + rp[r + 1]);
+        }
+    }
+    std::vector<int> slot2;
+    const std::string err = permuted ? AnalyzeMatrix(n, rp2.data(), ci2.data(), P->grid->sym, slot2)
+                                     : AnalyzeMatrix(n, rp, ci, P->grid->sym, P->aSlot);
     if (!err.empty()) return SetErr(ctx, GS_ERR_INVALID_ARG, err);
     int rc = UploadGrid(P->grid.get());
     if (rc) return rc;
-    const std::vector<int>& pinv = P->grid->sym.pinv;
+    std::vector<int> pinv = P->grid->sym.pinv;  // right-hand-side row -> pivot position
+    if (permuted) {
+        P->aSlot.assign(rp[n], 0);
+        for (int i = 0; i < n; i++)
+            for (int p = rp[i]; p < rp[i + 1]; p++) P->aSlot[p] = slot2[rp2[posOfRow[i]] + (p - rp[i])];
+        for (int i = 0; i < n; i++) pinv[i] = P->grid->sym.pinv[posOfRow[i]];
+    }
     GS_CUDA(P->dSlot.alloc(std::max<size_t>(4, P->aSlot.size() * 4)));
     GS_CUDA(P->dPinv.alloc(pinv.size() * 4));
     if (!P->aSlot.empty()) GS_CUDA(cudaMemcpy(P->dSlot.p, P->aSlot.data(), P->aSlot.size() * 4, cudaMemcpyHostToDevice));

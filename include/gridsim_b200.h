@@ -305,7 +305,8 @@ int gs_element_screen(gs_grid *grid, int32_t n_out, const int32_t *kind, const i
  * `count` square systems A_s x_s = b_s in FP64, of any sizes and patterns, in CSR, concatenated system after
  * system: n[s] rows; row_ptr holds n[s]+1 offsets per system (each block starting at 0); col_idx and values hold
  * row_ptr[n[s]] entries per system; rhs and x hold n[s] values per system. Systems that share a pattern are
- * factorised together on the device: static diagonal pivots on a minimum-degree order of A + A^T (the reference
+ * factorised together on the device: static diagonal pivots on a minimum-degree order of A + A^T, after a row order
+ * that makes the diagonal structurally zero-free where it is not (a maximum transversal; the reference
  * orders the same pattern, SparseLuFactorization.cs:69-195, but pivots by rows); the analysis of a pattern is kept
  * on the context for later calls, as CpuSparseLuSolver caches its ordering (CpuSparseLuSolver.cs:22-48). The inputs
  * are not modified. A system that fails reports it in status[s] and leaves its x untouched (the null result and the

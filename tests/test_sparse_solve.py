@@ -109,3 +109,56 @@ def test_failures_stay_with_their_system():
     with pytest.raises(ValueError):
         solver.solve((rp, ci, nan), b)
     assert solver.solve((rp, ci, sing), b) is None
+
+
+def _permuted_triangular(n, seed):
+    """A diagonally dominant lower-triangular matrix with its rows shuffled: a structurally zero diagonal whose one
+    zero-free row order is the triangle's (the reference's row pivoting finds it too)."""
+    rng = np.random.default_rng(seed)
+    low = np.tril(np.where(rng.random((n, n)) < 0.15, rng.normal(size=(n, n)), 0.0), -1)
+    low += np.diag(np.abs(low).sum(axis=1) + 1.0 + rng.random(n))
+    a = low[rng.permutation(n)]
+    rows, cols = np.nonzero(a)
+    indptr = np.searchsorted(rows, np.arange(n + 1)).astype(np.int32)
+    return (indptr, cols.astype(np.int32), a[rows, cols]), a
+
+
+def test_oracle_solver_handles_zero_diagonals():
+    for seed in range(10):
+        (rp, ci, v), a = _permuted_triangular(8 + 5 * seed, seed)
+        assert any(a[i, i] == 0 for i in range(a.shape[0]))
+        b = np.random.default_rng(seed).normal(size=a.shape[0])
+        x = oracle.sparse_solve(rp, ci, v, b)
+        ref = np.linalg.solve(a, b)
+        assert np.max(np.abs(x - ref)) <= 1e-12 * max(1.0, np.max(np.abs(ref)))
+
+
+@pytest.mark.gpu
+def test_zero_diagonals_are_solved_through_a_row_transversal():
+    """Patterns whose diagonal is structurally zero get a zero-free row order before the analysis."""
+    from gridsim_b200.engine import CudaSparseLinearSolver
+    mats, rhs, dense = [], [], []
+    for seed in range(12):
+        (csr, a) = _permuted_triangular(10 + 7 * seed, 500 + seed)
+        mats.append(csr)
+        dense.append(a)
+        rhs.append(np.random.default_rng(seed).normal(size=a.shape[0]))
+    perm = np.random.default_rng(3).permutation(9)   # a permutation matrix: x = P^T b
+    pm = np.zeros((9, 9))
+    pm[np.arange(9), perm] = 1.0
+    mats.append((np.arange(10, dtype=np.int32), perm.astype(np.int32), np.ones(9)))
+    dense.append(pm)
+    rhs.append(np.arange(1.0, 10.0))
+    solver = CudaSparseLinearSolver()
+    errors = [None] * len(mats)
+    xs = solver.solve_batch(mats, rhs, errors)
+    assert all(e is None for e in errors)
+    for (rp, ci, v), b, a, x in zip(mats, rhs, dense, xs):
+        ref = oracle.sparse_solve(rp, ci, v, b)
+        assert x is not None and ref is not None
+        assert np.max(np.abs(x - ref)) <= REL_TOL * max(1.0, np.max(np.abs(ref)))
+        assert np.max(np.abs(a @ x - b)) <= 1e-9 * max(1.0, np.max(np.abs(b)))
+    # no zero-free row order exists (column 0 is empty): singular, as the reference reports it
+    rp = np.array([0, 1, 2, 4], np.int32)
+    ci = np.array([1, 2, 1, 2], np.int32)
+    assert solver.solve((rp, ci, np.array([1.0, 2.0, 3.0, 4.0])), np.ones(3)) is None
