@@ -106,15 +106,20 @@ def test_tight_limits_n1_matches_oracle(tight_grid, precision):
     assert np.max(np.abs(free["vm"][both] - ref["vm"][both])) > 1e-4
 
 
-def test_q_limits_refused_where_not_built():
-    from gridsim_b200.engine import EngineError, UnevenBatch
+def test_multi_grid_batch_takes_q_limits_through_batch_solves():
+    """The uneven multi-grid batch runs Q-limit cases as each grid's batch solve: the same results bit for bit."""
+    from gridsim_b200.engine import UnevenBatch
     m = synthetic.config_grid(0, 0)
+    opt = PowerFlowOptions(enforce_q_limits=True)
     b = UnevenBatch([m])
     try:
-        with pytest.raises(EngineError):
-            b.solve([1], options=PowerFlowOptions(enforce_q_limits=True))
+        r = b.solve([2], options=opt, keep_states=True)
     finally:
         b.close()
+    ref = SparseNewtonRaphsonPowerFlow().solve_batch(m, outage=np.array([-1, -1], np.int32), options=opt,
+                                                     keep_states=True)
+    assert np.array_equal(r["status"][0], ref["status"]) and (ref["status"] == 0).all()
+    assert np.array_equal(r["vm"][0], ref["vm"]) and np.array_equal(r["va_deg"][0], ref["va_deg"])
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
