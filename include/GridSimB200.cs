@@ -283,6 +283,7 @@ namespace GridSim.Core.PowerFlow.B200
                 catch (DllNotFoundException) { return false; }
                 catch (EntryPointNotFoundException) { return false; }
                 catch (InvalidOperationException) { return false; }
+                catch (TimeoutException) { return false; }
             }
         }
 
@@ -548,8 +549,9 @@ namespace GridSim.Core.PowerFlow.B200
     /// <summary>
     /// ISparseLinearSolver and IBatchedSparseLinearSolver on gs_sparse_solve_batch: systems of any sizes and patterns
     /// in one call, those sharing a pattern factorised together; the analysis of a pattern is kept on the context.
-    /// Pivots are static on the diagonal of a minimum-degree order, so a system whose diagonal pivot collapses is
-    /// reported singular (null) where the reference's row pivoting might still have solved it.
+    /// Pivots are static on the diagonal of a minimum-degree order, after a row order that makes the diagonal
+    /// structurally zero-free where it is not; a system whose diagonal pivot still collapses is reported singular
+    /// (null) where the reference's row pivoting might have solved it.
     /// </summary>
     public sealed class CudaBatchedSparseLinearSolver : IBatchedSparseLinearSolver, ISparseLinearSolver
     {
