@@ -277,3 +277,42 @@ def test_device_shared_results_carry_the_notes():
     assert res[0].note.startswith("reference moved from bus 1 to bus 2; lost 40.0 MW shared by governor droop")
     assert res[1].note == "lost 60.0 MW shared by governor droop over 2 unit(s)"
     assert res[1].lost_generation_mw == 60.0 and res[1].converged
+
+
+# ---- host logic without a device -------------------------------------------------------------------------------
+def test_share_lost_power_edge_cases():
+    m = converters_model()
+    units = [0, 1, 2]
+    pg, note = share_lost_power(m, units, m.bus_type, 0.0, "inertia")
+    assert list(pg) == [30.0, 20.0, 10.0] and note == "no net power lost, nothing to share by inertia"
+    with pytest.raises(ValueError):
+        share_lost_power(m, units, m.bus_type, math.nan, "droop")
+    with pytest.raises(ValueError):
+        share_lost_power(m, units, m.bus_type, 5.0, "reference")
+    # a crossed Pmin / Pmax is refused only on a unit that takes part (ParticipationWeights, :1634-1641)
+    crossed = converters_model()
+    crossed.pmin[1], crossed.pmax[1] = 300.0, 200.0   # the wind plant: a converter, so it takes no part
+    pg, _ = share_lost_power(crossed, units, crossed.bus_type, 10.0, "droop")
+    assert pg[0] == 40.0
+    crossed.pmin[0] = 60.0                            # the synchronous unit: refused
+    with pytest.raises(ValueError, match="Pmin 60 MW above Pmax 50 MW"):
+        share_lost_power(crossed, units, crossed.bus_type, 10.0, "droop")
+
+
+def test_shared_rows_are_merged_in_outage_order():
+    from gridsim_b200.engine import _merge_rows
+    raw = dict(status=np.array([0, 0, 1], np.int32), iterations=np.array([3, 4, 20], np.int32),
+               max_mismatch=np.zeros(3), min_vm=np.array([0.97, 0.98, 0.0]), max_vm=np.array([1.02, 1.03, 0.0]),
+               max_loading_pct=np.array([90.0, 101.0, 0.0]), worst_boundary_pct=np.zeros(3),
+               islanded=np.zeros(3, np.uint8), viol_ptr=np.array([0, 0, 1, 1], np.int32),
+               viol_kind=np.array([0], np.int32), viol_element=np.array([7], np.int32), viol_value=np.array([101.0]))
+    sub = dict(status=np.array([0], np.int32), iterations=np.array([5], np.int32), max_mismatch=np.zeros(1),
+               min_vm=np.array([0.93]), max_vm=np.array([1.01]), max_loading_pct=np.array([120.0]),
+               worst_boundary_pct=np.zeros(1), islanded=np.zeros(1, np.uint8), viol_ptr=np.array([0, 2], np.int32),
+               viol_kind=np.array([0, 2], np.int32), viol_element=np.array([4, 11], np.int32),
+               viol_value=np.array([120.0, 0.93]))
+    _merge_rows(raw, {0: sub}, keep_states=False)
+    assert list(raw["status"]) == [0, 0, 1] and list(raw["iterations"]) == [5, 4, 20]
+    assert list(raw["viol_ptr"]) == [0, 2, 3, 3]
+    assert list(raw["viol_kind"]) == [0, 2, 0] and list(raw["viol_element"]) == [4, 11, 7]
+    assert list(raw["viol_value"]) == [120.0, 0.93, 101.0] and raw["viol_kind"].dtype == np.int32
