@@ -11,6 +11,7 @@
 //   CudaSparseNewtonPowerFlow      IPowerFlowSolver (Abstractions/IPowerFlowSolver.cs:10-13) on gs_pf_solve;
 //   CudaBatchedSparseLinearSolver  ISparseLinearSolver and IBatchedSparseLinearSolver (Abstractions/ISparseLinearSolver.cs:12-17,
 //                                  IBatchedSparseLinearSolver.cs:19-37) on gs_sparse_solve_batch;
+//   GsServer                       the request loop (gs_serve_*) for a resident host such as the rpc command's;
 //   ContingencyAnalysis (partial)  ScreenBranchesCuda, ScreenBaseCaseCuda, ScreenOutagesCuda and ScreenElementOutagesCuda:
 //                                  the screens of Analysis/ContingencyAnalysis.cs:306-344, :958-962, :944-950 and :1309-1437
 //                                  as one device call each, labelled by the reference's own Label / LabelMany and
@@ -623,6 +624,99 @@ namespace GridSim.Core.PowerFlow.B200
                 bo += n[s];
             }
             return result;
+        }
+    }
+
+    /// <summary>One answered request of <see cref="GsServer"/>: the caller's tag, the load flow's outcome and, when
+    /// asked for, the solved state (Vm in pu, Va in degrees, in the model's bus order).</summary>
+    public sealed record GsServedSolve(ulong Ticket, ulong Tag, int Grid, int Outage, PowerFlowStatus Status, int Iterations,
+        double MaxMismatch, double QueueMs, double LatencyMs, double[]? Vm, double[]? VaDeg);
+
+    /// <summary>
+    /// The request loop (gs_serve_*) for a resident host such as the rpc command's (src/GridSim.Cli/RpcCommand.cs:667-700,
+    /// which solves each held case with MaxIterations 100 and Q limits on): register the held cases, start, then submit
+    /// and poll from any thread. With Q limits or the DC retry the loop answers in batches; no other solve may then use
+    /// the process's device context while it runs.
+    /// </summary>
+    public sealed class GsServer : IDisposable
+    {
+        private IntPtr _server;
+        private readonly List<int> _nBus = new();
+        private readonly List<GsGrid> _grids = new();   // the grids must outlive the loop
+
+        public GsServer(PowerFlowOptions? options = null, GsPrecision precision = GsPrecision.Fp64, int slotsPerGrid = 0)
+        {
+            var o = new GsNative.ServeOpts { Pf = GsNative.Options(options, (int)precision), SlotsPerGrid = slotsPerGrid };
+            GsNative.Check(GsNative.gs_serve_create(GsContext.Handle, ref o, out _server), GsContext.Handle, "gs_serve_create");
+        }
+
+        /// <summary>Register a case (before <see cref="Start"/>); returns its grid index for requests.</summary>
+        public int AddGrid(GridModel model, bool flatStart = false)
+        {
+            GsGrid grid = GsGrid.For(model, flatStart);
+            GsNative.Check(GsNative.gs_serve_add_grid(_server, grid.Native.DangerousGetHandle(), out int index), GsContext.Handle,
+                           "gs_serve_add_grid");
+            _grids.Add(grid);
+            _nBus.Add(model.Buses.Count);
+            return index;
+        }
+
+        public void Start() => GsNative.Check(GsNative.gs_serve_start(_server), GsContext.Handle, "gs_serve_start");
+
+        /// <summary>Queue requests: (grid, in-service branch index or -1 for the intact case, whether to return the
+        /// state, the caller's tag). Returns their tickets.</summary>
+        public ulong[] Submit(IReadOnlyList<(int Grid, int Outage, bool WantState, ulong Tag)> requests)
+        {
+            var req = new GsNative.Request[requests.Count];
+            for (int k = 0; k < req.Length; k++)
+                req[k] = new GsNative.Request
+                {
+                    Grid = requests[k].Grid, Outage = requests[k].Outage, WantState = requests[k].WantState ? 1 : 0,
+                    Tag = requests[k].Tag,
+                };
+            var tickets = new ulong[req.Length];
+            if (req.Length > 0)
+                GsNative.Check(GsNative.gs_serve_submit(_server, req.Length, req, tickets), GsContext.Handle, "gs_serve_submit");
+            return tickets;
+        }
+
+        /// <summary>Take up to <paramref name="max"/> answers, waiting up to <paramref name="timeoutMs"/> for the first.</summary>
+        public IReadOnlyList<GsServedSolve> Poll(int max = 256, int timeoutMs = 0)
+        {
+            var resp = new GsNative.Response[max];
+            long capacity = 0;
+            foreach (int n in _nBus) capacity = Math.Max(capacity, 2L * n * max);
+            var state = new double[capacity];
+            GsNative.Check(GsNative.gs_serve_poll(_server, max, timeoutMs, resp, state, capacity, out int got), GsContext.Handle,
+                           "gs_serve_poll");
+            var answers = new List<GsServedSolve>(got);
+            for (int k = 0; k < got; k++)
+            {
+                GsNative.Response r = resp[k];
+                double[]? vm = null, va = null;
+                if (r.StateOffset >= 0)
+                {
+                    int n = _nBus[r.Grid];
+                    vm = new double[n];
+                    va = new double[n];
+                    Array.Copy(state, r.StateOffset, vm, 0, n);
+                    Array.Copy(state, r.StateOffset + n, va, 0, n);
+                }
+                answers.Add(new GsServedSolve(r.Ticket, r.Tag, r.Grid, r.Outage, CudaSparseNewtonPowerFlow.StatusOf(r.Status),
+                    r.Iterations, r.MaxMismatch, r.QueueMs, r.LatencyMs, vm, va));
+            }
+            return answers;
+        }
+
+        /// <summary>Finish every queued and running request, then stop the loop (their answers stay pollable).</summary>
+        public void Stop(int timeoutMs = 60000) =>
+            GsNative.Check(GsNative.gs_serve_stop(_server, timeoutMs), GsContext.Handle, "gs_serve_stop");
+
+        public void Dispose()
+        {
+            if (_server == IntPtr.Zero) return;
+            GsNative.gs_serve_destroy(_server);
+            _server = IntPtr.Zero;
         }
     }
 }
