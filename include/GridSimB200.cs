@@ -12,7 +12,8 @@
 //   CudaBatchedSparseLinearSolver  ISparseLinearSolver and IBatchedSparseLinearSolver (Abstractions/ISparseLinearSolver.cs:12-17,
 //                                  IBatchedSparseLinearSolver.cs:19-37) on gs_sparse_solve_batch;
 //   GsServer                       the request loop (gs_serve_*) for a resident host such as the rpc command's;
-//   ContingencyAnalysis (partial)  ScreenBranchesCuda, ScreenBaseCaseCuda, ScreenOutagesCuda and ScreenElementOutagesCuda:
+//   ContingencyAnalysis (partial)  ScreenBranchesCuda, ScreenBaseCaseCuda, ScreenOutagesCuda, ScreenNMinusKReportCuda and
+//                                  ScreenElementOutagesCuda:
 //                                  the screens of Analysis/ContingencyAnalysis.cs:306-344, :958-962, :944-950 and :1309-1437
 //                                  as one device call each, labelled by the reference's own Label / LabelMany and
 //                                  reported through its own NonConverged, so their rows read as the CPU screens' rows.
@@ -784,6 +785,42 @@ namespace GridSim.Core.Analysis
             return RunScreen(model, options, precision, labels, nOut,
                 (IntPtr g, ref GsNative.PfOpts o, ref GsNative.N1Result r) => GsNative.gs_nk_screen(g, nOut, k, rows, ref o, ref r),
                 "gs_nk_screen");
+        }
+
+        /// <summary>ScreenNMinusKReport (:378-426) on the device: the single outages screened and ranked by the reference's
+        /// own RankCandidates / StressScore (or every in-service branch when <paramref name="exhaustive"/>), its
+        /// Combinations of k of them screened in one gs_nk_screen, the results worst first.</summary>
+        public static NkScreenReport ScreenNMinusKReportCuda(GridModel model, int k, PowerFlowOptions? options = null,
+            int candidateCount = DefaultCandidateCount, bool exhaustive = false, GsPrecision precision = GsPrecision.Fp64)
+        {
+            ArgumentNullException.ThrowIfNull(model);
+            if (k < 1) throw new ArgumentOutOfRangeException(nameof(k), k, "contingency depth k must be >= 1");
+            int[] live = InServiceBranchIndices(model);
+            var none = Array.Empty<ContingencyResult>();
+            if (k > live.Length) return new NkScreenReport(none, none) { Note = NkScreenReport.TooFewBranches(live.Length, k) };
+            if (k == 1) return new NkScreenReport(ScreenBranchesCuda(model, options, null, precision), none);
+            int[] candidates;
+            IReadOnlyList<ContingencyResult> excluded = none;
+            if (exhaustive)
+            {
+                candidates = live;
+            }
+            else
+            {
+                IReadOnlyList<ContingencyResult> single = ScreenBranchesCuda(model, options, null, precision);
+                candidates = RankCandidates(single, candidateCount, k, out excluded).Select(i => live[i]).ToArray();
+            }
+            double comboCount = 1.0;
+            for (int c = 0; c < k; c++) comboCount = comboCount * (candidates.Length - c) / (c + 1);
+            if (comboCount > MaxCombinations)
+                throw new ArgumentException(FormattableString.Invariant(
+                    $"N-{k}: {candidates.Length} candidate branches give about {comboCount:G4} outage combinations, more than the {MaxCombinations} one screen takes; screen fewer candidates (a candidate count) or a smaller k."), nameof(k));
+            var combos = new List<int[]>();
+            Combinations(candidates, k, combos);
+            IReadOnlyList<ContingencyResult> results =
+                ScreenOutagesCuda(model, combos.Select(c => (IReadOnlyList<int>)c).ToList(), options, precision);
+            return new NkScreenReport(results.OrderByDescending(StressScore).ToList(), excluded)
+                { Note = NkScreenReport.TooFewCandidates(candidates.Length, excluded.Count, k) };
         }
 
         /// <summary>ScreenElementOutages (:1309-1320) with the reference-bus dispatch as one gs_element_screen: labels,
