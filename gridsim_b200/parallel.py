@@ -13,7 +13,7 @@ from typing import Callable, Optional
 import numpy as np
 
 PER_OUTAGE = ("status", "iterations", "max_mismatch", "min_vm", "max_vm", "max_loading_pct")
-OPTIONAL = ("worst_boundary_pct", "islanded")  # merged when every part has them
+OPTIONAL = ("worst_boundary_pct", "islanded", "share_notes")  # merged when every part has them
 
 
 def shard(n_items: int, rank: int, world: int) -> slice:
@@ -55,7 +55,8 @@ def screen_sharded(model, branch_idx, screen: Callable, group=None, rank: Option
         world = dist.get_world_size(group) if dist.is_available() and dist.is_initialized() else 1
     if rank is None:
         rank = dist.get_rank(group) if world > 1 else 0
-    mine = screen(model, idx[shard(len(idx), rank, world)])  # rows: a branch, or a set of branches per outage
+    # rows: a branch, a set of branches, or an element outage's (kind, index) per outage
+    mine = screen(model, idx[shard(len(idx), rank, world)])
     if world == 1:
         return merge([mine])
     keys = PER_OUTAGE + ("viol_ptr", "viol_kind", "viol_element", "viol_value") + tuple(k for k in OPTIONAL if k in mine)

@@ -22,6 +22,23 @@ def _pairs(m):
     return np.array(rows, np.int32)
 
 
+def _elements(m):
+    """(kind, index) rows: every in-service generator, then the first 15 buses."""
+    on = np.nonzero(m.gen_in_service)[0]
+    return np.array([[1, int(g)] for g in on] + [[2, i] for i in range(15)], np.int32)
+
+
+def _shared(m, rows):
+    """The element screen with governor-droop sharing; its notes under the engine's key."""
+    import oracle
+    from gridsim_b200 import _abi
+    o = _abi.default_opts()
+    o.max_iterations = 20
+    r = oracle.screen_elements(m, rows[:, 0], rows[:, 1], o, threads=1, dispatch="droop")
+    r["share_notes"] = r.pop("notes")
+    return r
+
+
 def _worker(rank, world, port, out_path):
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -42,9 +59,11 @@ def _worker(rank, world, port, out_path):
         got = screen_sharded(m, idx, lambda mm, ii: oracle.screen(mm, ii, o, threads=1))
         pairs = _pairs(m)
         got2 = screen_sharded(m, pairs, lambda mm, ss: oracle.screen_sets(mm, ss, o, threads=1))
+        got3 = screen_sharded(m, _elements(m), lambda mm, ee: _shared(mm, ee))
         if rank == 0:
             np.savez(out_path, **got)
             np.savez(out_path + ".pairs.npz", **got2)
+            np.savez(out_path + ".elements.npz", **got3)
     finally:
         dist.destroy_process_group()
 
@@ -72,4 +91,11 @@ def test_two_rank_screen_equals_one_process(tmp_path):
     whole2 = oracle.screen_sets(m, _pairs(m), o)
     for k in ("status", "iterations", "viol_ptr", "viol_kind", "viol_element", "islanded"):
         assert np.array_equal(got2[k], whole2[k]), k
+    # element outages with shared dispatch shard by (kind, index) rows, their notes gathered in order
+    got3 = np.load(out + ".elements.npz", allow_pickle=True)
+    whole3 = _shared(m, _elements(m))
+    for k in ("status", "iterations", "viol_ptr", "viol_kind", "viol_element", "islanded"):
+        assert np.array_equal(got3[k], whole3[k]), k
+    assert list(got3["share_notes"]) == list(whole3["share_notes"])
+    assert any(n is not None for n in whole3["share_notes"])
     del torch
