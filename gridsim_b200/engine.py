@@ -696,16 +696,16 @@ class ContingencyAnalysis:
         of its own grid: the model with the units moved and the reference already re-elected (ReelectReference
         works on the output before the sharing), so each costs a grid upload; "share_notes" holds the sharing notes
         (None where nothing was shared: branch outages, and outages that leave no unit to take the reference)."""
+        if dispatch not in ("reference", "droop", "inertia"):
+            raise ValueError(f"unknown outage dispatch {dispatch!r}: reference, droop or inertia")
+        if dispatch != "reference" and options.warm_start_from_base:
+            raise ValueError("a shared outage dispatch solves each outage from the model's stored voltages, as the "
+                             "reference does; warm_start_from_base is not offered with it")
         k = np.ascontiguousarray(kinds, dtype=np.int32)
         idx = np.ascontiguousarray(indices, dtype=np.int32)
         raw = ContingencyAnalysis._screen_call(model, idx, ("elements", k), solver, options, keep_states)
         if dispatch == "reference":
             return raw
-        if dispatch not in ("droop", "inertia"):
-            raise ValueError(f"unknown outage dispatch {dispatch!r}: reference, droop or inertia")
-        if options.warm_start_from_base:
-            raise ValueError("a shared outage dispatch solves each outage from the model's stored voltages, as the "
-                             "reference does; warm_start_from_base is not offered with it")
         notes = [None] * k.shape[0]
         own = SparseNewtonRaphsonPowerFlow(solver.precision, solver.ctx)
         subs = {}

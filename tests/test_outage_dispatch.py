@@ -316,3 +316,14 @@ def test_shared_rows_are_merged_in_outage_order():
     assert list(raw["viol_ptr"]) == [0, 2, 3, 3]
     assert list(raw["viol_kind"]) == [0, 2, 0] and list(raw["viol_element"]) == [4, 11, 7]
     assert list(raw["viol_value"]) == [120.0, 0.93, 101.0] and raw["viol_kind"].dtype == np.int32
+
+
+def test_bad_dispatch_options_are_refused_before_any_device_call():
+    """An unknown dispatch, and a warm start with a shared one, fail before the library is reached (no device here)."""
+    m = n124()
+    solver = SparseNewtonRaphsonPowerFlow()
+    with pytest.raises(ValueError, match="unknown outage dispatch"):
+        ContingencyAnalysis.screen_elements_raw(m, [1], [0], solver, PowerFlowOptions(), dispatch="proportional")
+    with pytest.raises(ValueError, match="warm_start_from_base"):
+        ContingencyAnalysis.screen_elements_raw(m, [1], [0], solver, PowerFlowOptions(warm_start_from_base=True),
+                                                dispatch="droop")
