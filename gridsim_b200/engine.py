@@ -336,7 +336,8 @@ class UnevenBatch:
 
     The grids are uploaded once; every :meth:`solve` runs ``counts[k]`` cases of grid k, each from its case's
     stored voltages, optionally with per-bus load multipliers and a branch outage. The CTA shape is autotuned on
-    the first call for this set of grids and reused afterwards."""
+    the first call for this set of grids and reused afterwards. With Q limits or the DC retry (StudyOptions) each
+    grid's cases run as one batch solve instead."""
 
     def __init__(self, models: Sequence[GridModel], ctx: Optional[CudaContext] = None):
         self.ctx = ctx or CudaContext.default()

@@ -57,7 +57,10 @@ class ServeResponse:
 
 
 class LoadFlowServer:
-    """gs_server: register grids, start, then submit and poll from any thread."""
+    """gs_server: register grids, start, then submit and poll from any thread. With Q limits or the DC retry in
+    the options (the reference's rpc solve runs with Q limits, ``src/GridSim.Cli/RpcCommand.cs:675-676``) the loop
+    answers each grid's queued requests in batches; warm starts are refused then, and no other solve may use the
+    context while the loop runs."""
 
     def __init__(self, options: Optional[PowerFlowOptions] = None, ctx: Optional[CudaContext] = None,
                  slots_per_grid: int = 0, state_slots: int = 0, hbm_fraction: float = 0.0):
