@@ -1570,6 +1570,20 @@ struct DevBuf {
     template <typename X> X* as() const { return reinterpret_cast<X*>(p); }
 };
 
+// Two events bracketing device work on one stream; ms() once both have completed.
+struct EventPair {
+    cudaEvent_t a = nullptr, b = nullptr;
+    EventPair() = default;
+    EventPair(const EventPair&) = delete;
+    EventPair& operator=(const EventPair&) = delete;
+    ~EventPair() { if (a) cudaEventDestroy(a); if (b) cudaEventDestroy(b); }
+    cudaError_t create() {
+        cudaError_t e = cudaEventCreate(&a);
+        return e == cudaSuccess ? cudaEventCreate(&b) : e;
+    }
+    float ms() const { float t = 0; cudaEventElapsedTime(&t, a, b); return t; }
+};
+
 struct Workspace {
     int B = 0;
     int precision = -1;
@@ -1597,6 +1611,7 @@ struct gs_ctx {
     int* pinnedCount = nullptr;
     std::map<std::string, int> multiTune;  // the multi-grid batch's CTA shape per set of grids (autotuned)
     std::vector<std::unique_ptr<MatrixPattern>> patterns;  // most recently used last
+    unsigned long long* noallocScratch = nullptr;  // device address of the allocation-free check's static scratch
     ~gs_ctx();
 };
 
@@ -3006,9 +3021,13 @@ int ScreenOutageLists(gs_grid* G, int nOut, const std::vector<Element>& els, con
         totalMs += ms;
         res->n_batches++;
         stats.launches += 2;  // classification and compaction
-        // classification of converged systems
+        // classification of converged systems (its device time counts in the screen's device_ms)
         GS_CUDA(w.chunkCount.alloc((size_t)nChunks * Bz * 4));
         GS_CUDA(w.chunkOffset.alloc((size_t)nChunks * Bz * 4));
+        EventPair clsEv, cmpEv;
+        GS_CUDA(clsEv.create());
+        GS_CUDA(cmpEv.create());
+        GS_CUDA(cudaEventRecord(clsEv.a, ctx->stream));
         GS_CUDA(cudaMemsetAsync(w.chunkCount.p, 0, (size_t)nChunks * Bz * 4, ctx->stream));
         GS_CUDA(cudaMemsetAsync(w.maxLoad.p, 0, Bz * 8, ctx->stream));
         GS_CUDA(cudaMemsetAsync(w.minVmNeg.p, 0, Bz * 8, ctx->stream));
@@ -3021,6 +3040,7 @@ int ScreenOutageLists(gs_grid* G, int nOut, const std::vector<Element>& els, con
         DevBatch b = MakeBatch(G, cnt, false);
         k_classify<<<dim3((nItems + 7) / 8, B / 32), dim3(32, 8), 0, ctx->stream>>>(G->view, b, c);
         GS_CUDA(cudaGetLastError());
+        GS_CUDA(cudaEventRecord(clsEv.b, ctx->stream));
         std::vector<int> cc((size_t)nChunks * Bz), off((size_t)nChunks * Bz);
         GS_CUDA(cudaMemcpyAsync(cc.data(), w.chunkCount.p, cc.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
         std::vector<int> st(cnt), it(cnt), fl(cnt);
@@ -3037,6 +3057,7 @@ int ScreenOutageLists(gs_grid* G, int nOut, const std::vector<Element>& els, con
         GS_CUDA(cudaMemcpyAsync(mxv.data(), w.maxVmB.p, cnt * 8, cudaMemcpyDeviceToHost, ctx->stream));
         GS_CUDA(cudaMemcpyAsync(wbd.data(), w.worstBnd.p, cnt * 8, cudaMemcpyDeviceToHost, ctx->stream));
         GS_CUDA(cudaStreamSynchronize(ctx->stream));
+        totalMs += clsEv.ms();
         int batchTotal = 0;
         std::vector<int> sysStart(cnt);
         for (int k = 0; k < cnt; k++) {
@@ -3070,14 +3091,17 @@ int ScreenOutageLists(gs_grid* G, int nOut, const std::vector<Element>& els, con
             GS_CUDA(w.outKind.alloc((size_t)batchTotal * 4));
             GS_CUDA(w.outElem.alloc((size_t)batchTotal * 4));
             GS_CUDA(w.outVal.alloc((size_t)batchTotal * 8));
+            GS_CUDA(cudaEventRecord(cmpEv.a, ctx->stream));
             k_compact<<<dim3((nChunks + 3) / 4, B / 32), dim3(32, 4), 0, ctx->stream>>>(
                 G->view, b, c, w.chunkOffset.as<int>(), w.outKind.as<int>(), w.outElem.as<int>(), w.outVal.as<double>(),
                 dbusId.as<int>());
             GS_CUDA(cudaGetLastError());
+            GS_CUDA(cudaEventRecord(cmpEv.b, ctx->stream));
             GS_CUDA(cudaMemcpyAsync(res->viol_kind + written, w.outKind.p, (size_t)batchTotal * 4, cudaMemcpyDeviceToHost, ctx->stream));
             GS_CUDA(cudaMemcpyAsync(res->viol_element + written, w.outElem.p, (size_t)batchTotal * 4, cudaMemcpyDeviceToHost, ctx->stream));
             GS_CUDA(cudaMemcpyAsync(res->viol_value + written, w.outVal.p, (size_t)batchTotal * 8, cudaMemcpyDeviceToHost, ctx->stream));
             GS_CUDA(cudaStreamSynchronize(ctx->stream));
+            totalMs += cmpEv.ms();
         }
         written += batchTotal;
         if (res->vm || res->va_deg) {
@@ -3432,12 +3456,13 @@ int gs_sparse_solve_batch(gs_ctx* ctx, int32_t count, const int32_t* n, const in
 // =============================================================================================
 // Allocation-free mismatch evaluation.
 //
-// For callers that may not allocate device memory at the point where they need a mismatch check: a
-// host loop that owns all device memory through its own pool, or code running while a CUDA stream is being
-// captured into a graph (cudaMalloc / cudaFree are not allowed there). They hand in device arrays they
-// already own; the only scratch this entry point needs (one max-norm accumulator and one flag word per
-// system) lives in the file-scope array below, which every GPU that loads this library holds until the
-// process exits. Calls that overlap on the GPU share it and race: issue them one after another.
+// For callers that must not allocate device memory at the point where they check a state: a host whose device
+// memory is all handed out up front by its own pool (a managed host that reserves its budget once, a process held
+// to a fixed share of a GPU it shares with others), or a latency-bound control loop, where cudaMalloc / cudaFree
+// may synchronise the whole device and stall its other streams. They hand in device arrays they already own; the
+// only scratch this entry point needs (one max-norm accumulator and one flag word per system, 16 bytes) lives in
+// the file-scope array below: 2 x 65,536 x 8 bytes = 1 MiB, which every GPU that loads this library holds until
+// the process exits. Calls that overlap on the GPU share it and race: issue them one after another.
 namespace gs {
 
 constexpr int kNoAllocMaxSystems = 65536;
@@ -3514,8 +3539,7 @@ __global__ void k_noalloc_finish(int count, const unsigned long long* acc, const
 }
 
 namespace {
-std::mutex gNoAllocMu;
-unsigned long long* gNoAllocPtr[64] = {nullptr};  // device address of gNoAllocScratch, per device ordinal
+std::mutex gNoAllocMu;  // guards the per-context lookup of the scratch array's device address
 }  // namespace
 
 }  // namespace gs
@@ -3529,20 +3553,23 @@ extern "C" int gs_pf_mismatch_noalloc(gs_grid* G, int32_t count, const double* d
         return SetErr(ctx, GS_ERR_CAPACITY, "gs_pf_mismatch_noalloc: " + std::to_string(count) +
                                               " systems requested, at most " + std::to_string(kNoAllocMaxSystems));
     if (count == 0) return GS_OK;
-    if (ctx->device < 0 || ctx->device >= 64) return SetErr(ctx, GS_ERR_INVALID_ARG, "device ordinal out of range");
     GS_CUDA(cudaSetDevice(ctx->device));
     unsigned long long* scratch = nullptr;
     {
-        // once per device, with that device current: the device address of the static scratch array
+        // On the context's first call, with its device current: the device address of the static scratch array.
+        // The host-side name gNoAllocScratch is only a stand-in for it, never a device address. The address is
+        // kept per context (not per device ordinal for the whole process): a context is created against the
+        // device's current CUDA context, so a device reset, after which the module may load elsewhere, comes
+        // with a new gs_ctx and a new lookup.
         std::lock_guard<std::mutex> lock(gNoAllocMu);
-        if (!gNoAllocPtr[ctx->device]) {
+        if (!ctx->noallocScratch) {
             void* p = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&p, gNoAllocScratch);
             if (e != cudaSuccess)
                 return SetErr(ctx, GS_ERR_CUDA, std::string("cudaGetSymbolAddress(gNoAllocScratch): ") + cudaGetErrorString(e));
-            gNoAllocPtr[ctx->device] = static_cast<unsigned long long*>(p);
+            ctx->noallocScratch = static_cast<unsigned long long*>(p);
         }
-        scratch = gNoAllocPtr[ctx->device];
+        scratch = ctx->noallocScratch;
     }
     unsigned long long* acc = scratch;
     unsigned long long* bad = scratch + kNoAllocMaxSystems;

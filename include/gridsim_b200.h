@@ -193,7 +193,8 @@ typedef struct gs_n1_result {
     /* base case (ScreenBaseCase) when warm_start_from_base is set, else status GS_PF_NOT_RUN */
     int32_t base_status;
     int32_t base_iterations;
-    /* device timing of the screen, milliseconds (CUDA events) */
+    /* device time of the screen, milliseconds (CUDA events): the base solve, the Newton batches, the retry,
+     * and the classification and compaction of the results */
     double device_ms;
     int32_t n_singular_pivot;  /* systems whose static pivot failed */
     int32_t n_batches;
@@ -439,16 +440,21 @@ int gs_serve_stop(gs_server *srv, int32_t timeout_ms);
 int gs_serve_destroy(gs_server *srv);
 
 /* ---- allocation-free mismatch check (no counterpart in the reference) ---------------------
- * For callers that cannot allocate device memory where they need the check: a loop whose device memory all
- * comes from its own pool, or code running while a stream is captured into a CUDA graph, where cudaMalloc
- * is not allowed. Computes, for `count` states of the grid, the FP64 max |mismatch| (the quantity the Newton
- * iteration tests against its tolerance) into d_max_mismatch[count] (NaN for a non-finite mismatch).
- * d_vm / d_va are the caller's DEVICE arrays, system-major [count][n_bus], angles in radians; d_outage
- * (device, [count], -1 = none) may be NULL. No device memory is allocated or freed: the only scratch is a
- * file-scope device array sized for GS_NOALLOC_MAX_SYSTEMS systems (768 KiB, held by every GPU that loads the
- * library). More systems than that are refused with GS_ERR_CAPACITY. The first call on a device looks up
- * that array's device address, so make it once before any stream capture. Calls share the array: calls
- * that overlap on the GPU race, so issue them one after another. Synchronous on the context's stream. */
+ * For callers that must not allocate device memory where they check a state: a host whose device memory is
+ * all handed out up front by its own pool (a managed host that reserves its budget once, a process held to a
+ * fixed share of a shared GPU), or a latency-bound loop, where cudaMalloc / cudaFree may synchronise the whole
+ * device. Computes, for `count` states of the grid, the FP64 max |mismatch| over the grid's equations into
+ * d_max_mismatch[count] (NaN for a non-finite mismatch): the mismatch under the grid's own bus types and its
+ * base generation and load, with at most one branch out per state. It does not model what some solve options
+ * change (Q-limit PV-to-PQ switches, load scalings, generator and bus outages, outage sets), so for solves
+ * with those it is not the quantity the solver tested. d_vm / d_va are the caller's DEVICE arrays,
+ * system-major [count][n_bus], angles in radians; d_outage (device, [count], -1 = none) may be NULL. No
+ * device memory is allocated or freed: the only scratch is a file-scope device array sized for
+ * GS_NOALLOC_MAX_SYSTEMS systems (16 bytes each: 1 MiB, held by every GPU that loads the library until the
+ * process exits). More systems than that are refused with GS_ERR_CAPACITY. The first call on a context
+ * looks up that array's device address, so make that first call before any stream capture. Every call
+ * shares the array (cleared at the start of each call): calls that overlap on the GPU race, so issue them
+ * one after another. Synchronous on the context's stream. */
 #define GS_NOALLOC_MAX_SYSTEMS 65536
 int gs_pf_mismatch_noalloc(gs_grid *grid, int32_t count, const double *d_vm, const double *d_va,
                            const int32_t *d_outage, double *d_max_mismatch);

@@ -48,6 +48,7 @@ def _load():
                                              i32, vp, vp, vp]
         lib.gso_outage_topology.argtypes = [ctypes.POINTER(_abi.GridDesc), ctypes.c_double, i32, vp, vp, vp]
         lib.gso_sparse_solve.argtypes = [i32, vp, vp, vp, vp, vp]
+        lib.gso_max_mismatch.argtypes = [ctypes.POINTER(_abi.GridDesc), i32, vp, vp, vp, vp]
         _lib = lib
     return _lib
 
@@ -232,6 +233,21 @@ def jacobian(model):
     if rc != 0:
         raise RuntimeError(f"oracle jacobian failed: {rc}")
     return rp, ci, val, mis
+
+
+def max_mismatch(model, vm, va_rad, outage=None):
+    """Max |mismatch| of given states ([count][n], angles in radians), each with branch outage[s] out (None: none)."""
+    lib = _load()
+    vm = np.ascontiguousarray(vm, np.float64)
+    va = np.ascontiguousarray(va_rad, np.float64)
+    count = vm.shape[0]
+    out = np.zeros(count)
+    o = None if outage is None else np.ascontiguousarray(outage, np.int32)
+    d = model.desc()
+    rc = lib.gso_max_mismatch(ctypes.byref(d), count, None if o is None else _p(o), _p(vm), _p(va), _p(out))
+    if rc != 0:
+        raise RuntimeError(f"oracle mismatch failed: {rc}")
+    return out
 
 
 def md_order(row_ptr, col_idx):

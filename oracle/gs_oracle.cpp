@@ -1416,6 +1416,36 @@ int gso_jacobian(const gs_grid_desc* d, int32_t* m_out, int32_t* nnz_out, int32_
     return GS_OK;
 }
 
+// The max |mismatch| of `count` given states (system-major [count][n], Va in radians), each on the grid with branch
+// outage[s] removed (-1 or a null `outage`: the intact grid): Y rebuilt as BuildY does (:382-402), the bus
+// specification of BuildBusSpec (NewtonShell.cs:433-486), the injections of ComputeInjections (:269-289) and the
+// infinity norm of RunNewton's mismatch vector (:216-235). NaN when a mismatch is not finite.
+int gso_max_mismatch(const gs_grid_desc* d, int32_t count, const int32_t* outage, const double* vm, const double* va,
+                     double* out) {
+    if (!d || count < 0 || (count > 0 && (!vm || !va || !out))) return GS_ERR_INVALID_ARG;
+    Model mdl = FromDesc(d);
+    const int n = mdl.n;
+    BusSpec s = BuildBusSpec(mdl, false);
+    std::vector<int> pPos, qPos;
+    EquationPositions(s.type0, pPos, qPos);
+    std::vector<double> V(n), A(n), P(n), Q(n);
+    for (int c = 0; c < count; c++) {
+        const int o = outage ? outage[c] : -1;
+        if (o >= (int)mdl.br.size()) return GS_ERR_INVALID_ARG;
+        ComplexCsr y = BuildY(mdl, o);
+        for (int i = 0; i < n; i++) { V[i] = vm[(size_t)c * n + i]; A[i] = va[(size_t)c * n + i]; }
+        ComputeInjections(y, V, A, P, Q);
+        double mx = 0.0;
+        bool finite = true;
+        for (int i = 0; i < n; i++) {
+            if (pPos[i] >= 0) { double f = s.pspec[i] - P[i]; finite = finite && std::isfinite(f); mx = std::max(mx, std::fabs(f)); }
+            if (qPos[i] >= 0) { double f = s.qspec[i] - Q[i]; finite = finite && std::isfinite(f); mx = std::max(mx, std::fabs(f)); }
+        }
+        out[c] = finite ? mx : NAN;
+    }
+    return GS_OK;
+}
+
 // Minimum-degree order of a CSR pattern (for ordering tests).
 int gso_md_order(int32_t n, const int32_t* rowPtr, const int32_t* colIdx, int32_t* order) {
     std::vector<int> rp(rowPtr, rowPtr + n + 1), ci(colIdx, colIdx + rowPtr[n]);

@@ -115,6 +115,8 @@ def cli_screens(ref_root):
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <root of the GridSim source tree>")
+    root = sys.argv[1]
     main(root)
     cli_screens(root)

@@ -66,3 +66,20 @@ def test_case14_base_and_raw_counts(study_opts):
     raw = oracle.screen(m, m.in_service_branches(), study_opts)
     assert _counts(raw) == (0, 19, 1)
     assert b["viol_ptr"].shape == (1,)
+
+
+def test_max_mismatch_of_screen_states_is_the_screens_own():
+    """oracle.max_mismatch (the checker of the allocation-free entry point) gives, for the states an N-1 screen
+    ends in, the max mismatch that screen reports for them (both cut short after two steps, so they are large)."""
+    from gridsim_b200 import synthetic
+    m = synthetic.config_grid(0, 0)
+    idx = synthetic.outage_set(m, None, 0)[:24].astype(np.int32)
+    o = _abi.default_opts()
+    o.max_iterations = 2
+    o.warm_start_from_base = 0
+    r = oracle.screen(m, idx, o, keep_states=True)
+    got = oracle.max_mismatch(m, r["vm"], np.radians(r["va_deg"]), idx)
+    assert np.allclose(got, r["max_mismatch"], rtol=1e-9, atol=1e-13)
+    assert got.max() > 1e-6
+    intact = oracle.max_mismatch(m, r["vm"], np.radians(r["va_deg"]))
+    assert not np.allclose(intact, got)
