@@ -1224,13 +1224,32 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(DevGrid g, DevBatch b, T*
 // shared memory of the piece counters of a walk over every level of a grid
 inline size_t QueueBytes(int nLevels) { return (size_t)6 * nLevels * sizeof(int); }
 
+}  // namespace gs
+#include "gs_cluster.cuh"
+namespace gs {
+
 // One step of the few systems of a batch (their list in b.activeList): factorisation, backward substitution and,
-// in mixed precision, the FP64-residual refinement. Levels below `lt` (many entries each) run as per-level launches
-// over the batch, the levels above as one CTA per system.
+// in mixed precision, the FP64-residual refinement. With `cluster` (at most kClusterMaxSystems systems) every level
+// runs as one cluster of CTAs per system (gs_cluster.cuh); otherwise levels below `lt` (many entries each) run as
+// per-level launches over the batch, the levels above as one CTA per system.
 template <typename T>
 int64_t FewSystemsSolve(const DevGrid& g, const DevBatch& b, const Symbolic& s, int nActive, int lt, bool refine,
-                        cudaStream_t st, cudaEvent_t afterFactor) {
+                        cudaStream_t st, cudaEvent_t afterFactor, bool cluster = false) {
     int64_t launches = 0;
+    if (cluster && nActive <= kClusterMaxSystems) {
+        const int L = s.nLevels;
+        LaunchTailCluster<T, kWorkFactor>(g, b, (T*)b.y, 0, L, nActive, st);
+        if (afterFactor) cudaEventRecord(afterFactor, st);
+        LaunchTailCluster<T, kWorkBackward>(g, b, (T*)b.y, 0, L, nActive, st);
+        launches += 2;
+        if (refine) {
+            k_residual<T><<<dim3((s.n + 7) / 8, (nActive + 31) / 32), dim3(32, 8), 0, st>>>(g, b, b.activeList, nActive);
+            LaunchTailCluster<T, kWorkForward>(g, b, (T*)b.z, 0, L, nActive, st);
+            LaunchTailCluster<T, kWorkBackward>(g, b, (T*)b.z, 0, L, nActive, st);
+            launches += 3;
+        }
+        return launches;
+    }
     const int groups = b.B / Lay<T>::S;
     const dim3 blk4(32, 4), blk8(32, 8);
     auto level = [&](auto kernel, T* vec, int i0, int i1) {
@@ -1612,6 +1631,7 @@ struct gs_ctx {
     std::map<std::string, int> multiTune;  // the multi-grid batch's CTA shape per set of grids (autotuned)
     std::vector<std::unique_ptr<MatrixPattern>> patterns;  // most recently used last
     unsigned long long* noallocScratch = nullptr;  // device address of the allocation-free check's static scratch
+    bool clusterOk = false;  // the few-systems cluster walk can be scheduled on this device
     ~gs_ctx();
 };
 
@@ -2149,7 +2169,8 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             // one CTA per active system (k_tail), in FP64 (the compact workspace's precision)
             cudaMemsetAsync(cur.activeCount, 0, sizeof(int), st);
             k_collect_active<<<(cur.count + 255) / 256, 256, 0, st>>>(cur);
-            launches += 1 + FewSystemsSolve<double>(g, cur, s, nActive, G->tailSplit, false, st, timed ? ev[2] : nullptr);
+            launches += 1 + FewSystemsSolve<double>(g, cur, s, nActive, G->tailSplit, false, st, timed ? ev[2] : nullptr,
+                                                    ctx->clusterOk);
             if (timed) cudaEventRecord(ev[3], st);
             {
                 const int grp = (nActive + 31) / 32;
@@ -2550,6 +2571,7 @@ extern "C" {
 
 namespace gs {
 cudaError_t SetKernelAttributes();  // defined after the multi-grid kernels
+bool ClusterWalkAvailable();
 }
 
 int gs_ctx_create(int device, const gs_ctx_opts* opts, gs_ctx** out) {
@@ -2597,6 +2619,7 @@ int gs_ctx_create(int device, const gs_ctx_opts* opts, gs_ctx** out) {
     if (cudaSetDevice(device) != cudaSuccess || gs::SetKernelAttributes() != cudaSuccess ||
         cudaStreamCreateWithFlags(&c->partStream[1], cudaStreamNonBlocking) != cudaSuccess) { delete c; return GS_ERR_CUDA; }
     if (cudaMallocHost(&c->pinnedCount, 4 * sizeof(int)) != cudaSuccess) { delete c; return GS_ERR_CUDA; }
+    c->clusterOk = gs::ClusterWalkAvailable() && std::getenv("GS_NO_CLUSTER_TAIL") == nullptr;
     *out = c;
     return GS_OK;
 }
@@ -3605,5 +3628,31 @@ cudaError_t SetKernelAttributes() {
     set((const void*)k_newton<float>);
     set((const void*)k_newton<double>);
     return e;
+}
+}  // namespace gs
+
+namespace gs {
+// Whether a cluster of kClusterCtas CTAs of the few-systems cluster walk fits on this device (checked per context).
+bool ClusterWalkAvailable() {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kClusterCtas);
+    cfg.blockDim = dim3(kClusterThreads);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kClusterCtas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    for (const void* f : {(const void*)k_tail_cluster<double, kWorkFactor>, (const void*)k_tail_cluster<double, kWorkBackward>,
+                          (const void*)k_tail_cluster<float, kWorkFactor>, (const void*)k_tail_cluster<float, kWorkBackward>,
+                          (const void*)k_tail_cluster<float, kWorkForward>}) {
+        if (cudaOccupancyMaxActiveClusters(&n, f, &cfg) != cudaSuccess || n < 1) {
+            cudaGetLastError();
+            return false;
+        }
+    }
+    return true;
 }
 }  // namespace gs
