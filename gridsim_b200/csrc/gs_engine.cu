@@ -1236,7 +1236,7 @@ template <typename T>
 int64_t FewSystemsSolve(const DevGrid& g, const DevBatch& b, const Symbolic& s, int nActive, int lt, bool refine,
                         cudaStream_t st, cudaEvent_t afterFactor, bool cluster = false) {
     int64_t launches = 0;
-    if (cluster && nActive <= kClusterMaxSystems) {
+    if (cluster && nActive <= kClusterMaxSystems && ClusterSmemBytes(s.nLevels) <= kClusterSmemMax) {
         const int L = s.nLevels;
         LaunchTailCluster<T, kWorkFactor>(g, b, (T*)b.y, 0, L, nActive, st);
         if (afterFactor) cudaEventRecord(afterFactor, st);
@@ -3637,6 +3637,7 @@ bool ClusterWalkAvailable() {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(kClusterCtas);
     cfg.blockDim = dim3(kClusterThreads);
+    cfg.dynamicSmemBytes = kClusterSmemMax;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = kClusterCtas;
@@ -3648,7 +3649,8 @@ bool ClusterWalkAvailable() {
     for (const void* f : {(const void*)k_tail_cluster<double, kWorkFactor>, (const void*)k_tail_cluster<double, kWorkBackward>,
                           (const void*)k_tail_cluster<float, kWorkFactor>, (const void*)k_tail_cluster<float, kWorkBackward>,
                           (const void*)k_tail_cluster<float, kWorkForward>}) {
-        if (cudaOccupancyMaxActiveClusters(&n, f, &cfg) != cudaSuccess || n < 1) {
+        if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClusterSmemMax) != cudaSuccess ||
+            cudaOccupancyMaxActiveClusters(&n, f, &cfg) != cudaSuccess || n < 1) {
             cudaGetLastError();
             return false;
         }

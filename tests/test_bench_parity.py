@@ -10,7 +10,8 @@
   (global U(0.7, 1.3) times per-bus lognormal sigma 0.05): per grid the six cases whose global factor is nearest 1
   and the two farthest. Demand alone is scaled and the slack takes the change, as the reference's ScaleLoads does
   (Analysis/ContinuationPowerFlow.cs:311-319), so most cases away from 1 have no solution: the test holds the
-  engine to the oracle's status on each case, converged or not, and to its voltages where it converged.
+  engine to the oracle's status on each case, converged or not, and to its voltages where it converged (iteration
+  counts: equal in FP64, within one step in mixed precision).
 """
 from concurrent.futures import ThreadPoolExecutor
 
@@ -106,7 +107,12 @@ def test_uneven_batch_on_the_largest_population_grids_matches_the_oracle(precisi
             assert r["status"][k][c] == ref["status"], (k, c, r["status"][k][c], ref["status"])
             if ref["status"] == _abi.PF_CONVERGED:
                 n_conv += 1
-                assert r["iterations"][k][c] == ref["iterations"], (k, c)
+                # FP64 follows the oracle's Newton path step for step; the FP32 factor makes mixed precision an
+                # inexact Newton, which on a slowly converging case may cross the tolerance one step apart
+                if precision == "fp64":
+                    assert r["iterations"][k][c] == ref["iterations"], (k, c)
+                else:
+                    assert abs(int(r["iterations"][k][c]) - int(ref["iterations"])) <= 1, (k, c)
                 assert np.max(np.abs(r["vm"][k][c] - ref["vm"])) <= VM_TOL, (k, c)
                 assert np.max(np.abs(np.radians(r["va_deg"][k][c] - ref["va_deg"]))) <= VA_TOL_RAD, (k, c)
             else:
