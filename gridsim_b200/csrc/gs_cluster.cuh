@@ -33,44 +33,68 @@ __device__ __forceinline__ T ldL2(const T* p) { return __ldcg(p); }
 template <typename T>
 __device__ __forceinline__ void stL2(T* p, T v) { __stcg(p, v); }
 
-// A piece and its first round of index pairs for this lane, loaded ahead: (LU slot, right-hand-side index) for
-// factorisation and forward entries, (U slot, row) for a backward node; x = -1 past the end.
-struct Ahead {
-    int4 d;
-    int2 a[4];
-};
+// Pairs a lane keeps in flight per round: 256 for a warp-wide piece, 64 for an 8-lane group, 8 for a thread, which
+// covers every piece of the benchmark grids in one round (the longest has 245 pairs; short pieces have at most 8).
+constexpr int kClusterInFlight = 8;
 
+// A phase's work cut into warp-sized units: unit u < nw is wide piece u (the whole warp), the next ceil(nm / 4) units
+// hold four mid-length pieces each (one per 8-lane group), the rest 32 short pieces each (one per lane). Warp w of the
+// cluster takes units w, w + kClusterWarps, ...; with at most kClusterWarps units a warp has one class of work per
+// phase. Returns the schedule position of this lane's piece in unit u (-1: none) and its class (0, 1, 2 = G 32, 8, 1).
+__device__ __forceinline__ int unitPiece(const int4 P, int u, int lane, int& cls) {
+    const int nw = P.y, nm = P.z, nr = P.w - P.x - P.y - P.z, m4 = (nm + 3) >> 2;
+    if (u < nw) { cls = 0; return P.x + u; }
+    if (u < nw + m4) {
+        cls = 1;
+        const int p = 4 * (u - nw) + (lane >> 3);
+        return p < nm ? P.x + nw + p : -1;
+    }
+    cls = 2;
+    const int p = 32 * (u - nw - m4) + lane;
+    return p < nr ? P.x + nw + nm + p : -1;
+}
+__device__ __forceinline__ int unitCount(const int4 P) {
+    const int nw = P.y, nm = P.z, nr = P.w - P.x - P.y - P.z;
+    return nw + ((nm + 3) >> 2) + ((nr + 31) >> 5);
+}
+
+// This lane's first round of index pairs of piece d for a group of G lanes: (LU slot, right-hand-side index) for
+// factorisation and forward entries, (U slot, row) for a backward node; x = -1 past the end.
 template <int W, int G>
-__device__ __forceinline__ void clLoadAhead(const DevGrid& g, const int4* __restrict__ desc, int pos, Ahead& x) {
-    x.d = __ldg(desc + pos);
+__device__ __forceinline__ void clPairs(const DevGrid& g, const int4 d, int2 (&a)[kClusterInFlight]) {
     const int j = G == 1 ? 0 : (int)(threadIdx.x & (G - 1));
     if (W == kWorkBackward) {
-        const int c = x.d.z;
-        const int base = x.d.y;  // LU slots fit 32 bits (checked by the symbolic analysis)
-        const int* rows = g.pRows + x.d.w;
+        const int c = d.z, base = d.y;  // LU slots fit 32 bits (checked by the symbolic analysis)
+        const int* rows = g.pRows + d.w;
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
+        for (int u = 0; u < kClusterInFlight; u++) {
             const int t = j + u * G;
-            x.a[u] = t < c ? make_int2(base + 1 + t, __ldg(rows + t)) : make_int2(-1, -1);
+            a[u] = t < c ? make_int2(base + 1 + t, __ldg(rows + t)) : make_int2(-1, -1);
         }
     } else {
-        const int q0 = x.d.y, q1 = x.d.z;
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const int q = q0 + j + u * G;
-            x.a[u] = q < q1 ? __ldg(g.pairs + q) : make_int2(-1, -1);
+        for (int u = 0; u < kClusterInFlight; u++) {
+            const int q = d.y + j + u * G;
+            a[u] = q < d.z ? __ldg(g.pairs + q) : make_int2(-1, -1);
         }
     }
 }
+template <int W>
+__device__ __forceinline__ void clPairsOf(const DevGrid& g, int cls, const int4 d, int2 (&a)[kClusterInFlight]) {
+    if (cls == 0) clPairs<W, 32>(g, d, a);
+    else if (cls == 1) clPairs<W, 8>(g, d, a);
+    else clPairs<W, 1>(g, d, a);
+}
 
-// One piece by a group of G lanes (G = 32, 8 or 1) from its loaded-ahead first round; the group's first lane writes.
-// Lane j of the group takes pairs j, j + G, ..., four in flight per round, then a fixed butterfly over the group.
+// One piece by a group of G lanes (G = 32, 8 or 1) from its loaded first round; the group's first lane writes. Lane j
+// of the group takes pairs j, j + G, ..., kClusterInFlight in flight per round, then a fixed butterfly over the group.
 template <typename T, int W, int G>
-__device__ __forceinline__ void clRun(const DevGrid& g, const DevBatch& b, T* vec, const Ahead& x, int s, unsigned mask) {
+__device__ __forceinline__ void clRun(const DevGrid& g, const DevBatch& b, T* vec, const int4 d,
+                                      const int2 (&a0)[kClusterInFlight], int s, unsigned mask) {
+    constexpr int U = kClusterInFlight;
     const size_t B = (size_t)b.B;
     T* lu = (T*)b.lu;
     T* piv = (T*)b.piv;
-    const int4 d = x.d;
     const int j = G == 1 ? 0 : (int)(threadIdx.x & (G - 1));
     const bool lead = j == 0;
     // where the result goes and what it combines with, loaded beside the first operands
@@ -78,7 +102,6 @@ __device__ __forceinline__ void clRun(const DevGrid& g, const DevBatch& b, T* ve
     const T* rhs;
     T base = T(0), div = T(1);
     int kind = kUpper;
-    bool hasA = true;
     if (W == kWorkBackward) {
         out = vec + (size_t)d.x * B + s;
         rhs = vec;
@@ -89,7 +112,6 @@ __device__ __forceinline__ void clRun(const DevGrid& g, const DevBatch& b, T* ve
         if (lead) base = ldL2(out);
     } else {
         kind = descKind(d);
-        hasA = descHasA(d);
         const int node = descNode(d);
         T* y = (T*)b.y;
         rhs = kind == kFwd ? y : lu;
@@ -97,59 +119,52 @@ __device__ __forceinline__ void clRun(const DevGrid& g, const DevBatch& b, T* ve
                            : (kind == kDiag ? piv + (size_t)node * B + s : lu + (size_t)d.x * B + s);
         if (lead) {
             if (kind == kFwd) base = ldL2(out);
-            else if (hasA) base = ldL2(lu + (size_t)d.x * B + s);
+            else if (descHasA(d)) base = ldL2(lu + (size_t)d.x * B + s);
             if (kind == kLower) div = ldL2(piv + (size_t)node * B + s);
         }
     }
     T acc = T(0);
     {
-        T l[4], r[4];
+        T l[U], r[U];
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const bool ok = x.a[u].x >= 0;
-            l[u] = ok ? ldL2(lu + (size_t)x.a[u].x * B + s) : T(0);
-            r[u] = ok ? ldL2(rhs + (size_t)x.a[u].y * B + s) : T(0);
+        for (int u = 0; u < U; u++) {
+            const bool ok = a0[u].x >= 0;
+            l[u] = ok ? ldL2(lu + (size_t)a0[u].x * B + s) : T(0);
+            r[u] = ok ? ldL2(rhs + (size_t)a0[u].y * B + s) : T(0);
         }
 #pragma unroll
-        for (int u = 0; u < 4; u++) acc += l[u] * r[u];
+        for (int u = 0; u < U; u++) acc += l[u] * r[u];
     }
-    // further rounds (pieces longer than 4 G)
-    if (W == kWorkBackward) {
-        const int c = d.z;
-        const int* rows = g.pRows + d.w;
-        for (int t = j + 4 * G; t < c; t += 4 * G) {
-            int rr[4];
+    // further rounds (pieces longer than U G pairs)
+    const int len = W == kWorkBackward ? d.z : d.z - d.y;
+    for (int off = U * G; off < len; off += U * G) {
+        int2 a[U];
+        if (W == kWorkBackward) {
+            const int* rows = g.pRows + d.w;
 #pragma unroll
-            for (int u = 0; u < 4; u++) rr[u] = t + u * G < c ? __ldg(rows + t + u * G) : -1;
-            T uu[4], xv[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                const bool ok = rr[u] >= 0;
-                uu[u] = ok ? ldL2(lu + (size_t)(d.y + 1 + t + u * G) * B + s) : T(0);
-                xv[u] = ok ? ldL2(vec + (size_t)rr[u] * B + s) : T(0);
+            for (int u = 0; u < U; u++) {
+                const int t = off + j + u * G;
+                a[u] = t < len ? make_int2(d.y + 1 + t, __ldg(rows + t)) : make_int2(-1, -1);
             }
+        } else {
 #pragma unroll
-            for (int u = 0; u < 4; u++) acc += uu[u] * xv[u];
-        }
-    } else {
-        const int q1 = d.z;
-        for (int q = d.y + j + 4 * G; q < q1; q += 4 * G) {
-            int2 a[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) a[u] = q + u * G < q1 ? __ldg(g.pairs + q + u * G) : make_int2(-1, -1);
-            T l[4], r[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                const bool ok = a[u].x >= 0;
-                l[u] = ok ? ldL2(lu + (size_t)a[u].x * B + s) : T(0);
-                r[u] = ok ? ldL2(rhs + (size_t)a[u].y * B + s) : T(0);
+            for (int u = 0; u < U; u++) {
+                const int q = d.y + off + j + u * G;
+                a[u] = q < d.z ? __ldg(g.pairs + q) : make_int2(-1, -1);
             }
-#pragma unroll
-            for (int u = 0; u < 4; u++) acc += l[u] * r[u];
         }
+        T l[U], r[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const bool ok = a[u].x >= 0;
+            l[u] = ok ? ldL2(lu + (size_t)a[u].x * B + s) : T(0);
+            r[u] = ok ? ldL2(rhs + (size_t)a[u].y * B + s) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) acc += l[u] * r[u];
     }
 #pragma unroll
-    for (int off = G / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(mask, acc, off);
+    for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(mask, acc, o);
     if (!lead) return;
     if (W == kWorkBackward) { stL2(out, (base - acc) / div); return; }
     T v = base - acc;
@@ -193,35 +208,54 @@ __global__ void __launch_bounds__(kClusterThreads) k_tail_cluster(DevGrid g, Dev
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int gw = clusterRank() * (kClusterThreads / 32) + (int)(threadIdx.x >> 5);  // warp of the cluster
-    const int pm0 = gw * 4 + (lane >> 3);  // this 8-lane group's first mid-length piece
-    const int ps0 = gw * 32 + lane;        // this thread's first short piece
     const unsigned gmask = 0xFFu << (lane & 24);
-    Ahead aw, am, as;
-    auto ahead = [&](int k) {
-        const int4 P = clPhase[k];  // {w0, nw, nm, w1}
-        if (gw < P.y) clLoadAhead<W, 32>(g, desc, P.x + gw, aw);
-        if (pm0 < P.z) clLoadAhead<W, 8>(g, desc, P.x + P.y + pm0, am);
-        if (ps0 < P.w - P.x - P.y - P.z) clLoadAhead<W, 1>(g, desc, P.x + P.y + P.z + ps0, as);
+    // the first unit of this warp two phases deep: its descriptor for phase k + 1, its descriptor and pairs for k
+    int clsCur = -1, posCur = -1, clsNext = -1, posNext = -1;
+    int4 dCur = make_int4(0, 0, 0, 0), dNext = make_int4(0, 0, 0, 0);
+    int2 aCur[kClusterInFlight];
+    auto firstOf = [&](int k, int& cls, int& pos, int4& d) {
+        cls = -1;
+        pos = -1;
+        if (k < nPh && gw < unitCount(clPhase[k])) {
+            pos = unitPiece(clPhase[k], gw, lane, cls);
+            if (pos >= 0) d = __ldg(desc + pos);
+        }
     };
-    if (nPh > 0) ahead(0);
+    firstOf(0, clsCur, posCur, dCur);
+    if (posCur >= 0) clPairsOf<W>(g, clsCur, dCur, aCur);
+    firstOf(1, clsNext, posNext, dNext);
     for (int k = 0; k < nPh; k++) {
         const int4 P = clPhase[k];
-        const int w0 = P.x, nw = P.y, nm = P.z, nr = P.w - P.x - P.y - P.z;
-        for (int p = gw; p < nw; p += kClusterWarps) {
-            if (p != gw) clLoadAhead<W, 32>(g, desc, w0 + p, aw);
-            clRun<T, W, 32>(g, b, vec, aw, s, 0xffffffffu);
-        }
-        for (int p = pm0; p < nm; p += kClusterWarps * 4) {
-            if (p != pm0) clLoadAhead<W, 8>(g, desc, w0 + nw + p, am);
-            clRun<T, W, 8>(g, b, vec, am, s, gmask);
-        }
-        for (int p = ps0; p < nr; p += kClusterWarps * 32) {
-            if (p != ps0) clLoadAhead<W, 1>(g, desc, w0 + nw + nm + p, as);
-            clRun<T, W, 1>(g, b, vec, as, s, 0u);
+        const int nu = unitCount(P);
+        for (int u = gw; u < nu; u += kClusterWarps) {
+            int cls, pos;
+            int4 d;
+            int2 a[kClusterInFlight];
+            if (u == gw) {
+                cls = clsCur;
+                pos = posCur;
+                d = dCur;
+#pragma unroll
+                for (int q = 0; q < kClusterInFlight; q++) a[q] = aCur[q];
+            } else {
+                pos = unitPiece(P, u, lane, cls);
+                if (pos >= 0) {
+                    d = __ldg(desc + pos);
+                    clPairsOf<W>(g, cls, d, a);
+                }
+            }
+            if (cls == 0) clRun<T, W, 32>(g, b, vec, d, a, s, 0xffffffffu);          // pos is warp-uniform here
+            else if (cls == 1) { if (pos >= 0) clRun<T, W, 8>(g, b, vec, d, a, s, gmask); }  // group-uniform
+            else if (pos >= 0) clRun<T, W, 1>(g, b, vec, d, a, s, 0u);
         }
         __syncwarp();  // the barrier below is .aligned: every warp arrives converged
         clusterArrive();
-        if (k + 1 < nPh) ahead(k + 1);  // static data only: safe before the acquire
+        // static data only, safe before the acquire: the next phase's first pairs, the phase after's descriptor
+        clsCur = clsNext;
+        posCur = posNext;
+        dCur = dNext;
+        if (posCur >= 0) clPairsOf<W>(g, clsCur, dCur, aCur);
+        firstOf(k + 2, clsNext, posNext, dNext);
         clusterWait();
     }
 }
