@@ -22,10 +22,11 @@
 
 namespace gs {
 
-constexpr int kClusterCtas = 8;        // CTAs per system (the portable cluster size)
-constexpr int kClusterThreads = 512;   // threads per CTA
-constexpr int kClusterWarps = kClusterCtas * kClusterThreads / 32;
-constexpr int kClusterMaxSystems = 16; // more systems than this: one CTA each (k_tail) keeps the GPU fuller
+constexpr int kClusterCtas = 8;        // the largest cluster: CTAs per system (the portable cluster size)
+constexpr int kClusterThreads = 512;   // threads per CTA (one CTA per SM at the walk's register count)
+constexpr int kClusterMaxSystems = 296; // more systems than this: the full-batch step
+// CTAs per system for n systems: as many as keep the systems' clusters within about one wave of the 148 SMs
+inline int ClusterCtasFor(int n) { return n <= 18 ? 8 : n <= 37 ? 4 : n <= 74 ? 2 : 1; }
 constexpr size_t kClusterSmemMax = 64 * 1024;  // the per-phase table in shared memory (16 bytes a phase)
 
 template <typename T>
@@ -39,7 +40,7 @@ constexpr int kClusterInFlight = 8;
 
 // A phase's work cut into warp-sized units: unit u < nw is wide piece u (the whole warp), the next ceil(nm / 4) units
 // hold four mid-length pieces each (one per 8-lane group), the rest 32 short pieces each (one per lane). Warp w of the
-// cluster takes units w, w + kClusterWarps, ...; with at most kClusterWarps units a warp has one class of work per
+// cluster takes units w, w + (warps of the cluster), ...; with at most that many units a warp has one class of work per
 // phase. Returns the schedule position of this lane's piece in unit u (-1: none) and its class (0, 1, 2 = G 32, 8, 1).
 __device__ __forceinline__ int unitPiece(const int4 P, int u, int lane, int& cls) {
     const int nw = P.y, nm = P.z, nr = P.w - P.x - P.y - P.z, m4 = (nm + 3) >> 2;
@@ -187,10 +188,11 @@ __device__ __forceinline__ int clusterRank() {
 
 // Levels [l0, l1) of a schedule (top down for the backward substitution) for the listed system of this cluster.
 // Dynamic shared memory: the walk's phases as {first piece, wide, mid-length, end} (16 bytes each).
-template <typename T, int W>
+template <typename T, int W, int C>
 __global__ void __launch_bounds__(kClusterThreads) k_tail_cluster(DevGrid g, DevBatch b, T* vec, int l0, int l1) {
+    constexpr int kClusterWarps = C * kClusterThreads / 32;
     extern __shared__ int4 clPhase[];
-    const int s = b.activeList[blockIdx.x / kClusterCtas];
+    const int s = b.activeList[blockIdx.x / C];
     // uniform over the cluster: every CTA of it returns, or none does (no CTA may miss a cluster barrier)
     if (W != kWorkFactor && vec != (T*)b.y && !b.refine[s]) return;
     const int* ptr = W == kWorkFactor ? g.fWorkPtr : (W == kWorkBackward ? g.bWorkPtr : g.vWorkPtr);
@@ -262,22 +264,31 @@ __global__ void __launch_bounds__(kClusterThreads) k_tail_cluster(DevGrid g, Dev
 
 inline size_t ClusterSmemBytes(int nLevels) { return (size_t)2 * nLevels * sizeof(int4); }
 
-// Launch a cluster walk of levels [l0, l1) for the nActive listed systems of b.
-template <typename T, int W>
-cudaError_t LaunchTailCluster(const DevGrid& g, const DevBatch& b, T* vec, int l0, int l1, int nActive, cudaStream_t st) {
+// Launch a walk of levels [l0, l1) for the nActive listed systems of b, one cluster of C CTAs per system.
+template <typename T, int W, int C>
+cudaError_t LaunchTailClusterC(const DevGrid& g, const DevBatch& b, T* vec, int l0, int l1, int nActive, cudaStream_t st) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(nActive * kClusterCtas);
+    cfg.gridDim = dim3(nActive * C);
     cfg.blockDim = dim3(kClusterThreads);
     cfg.dynamicSmemBytes = ClusterSmemBytes(l1 - l0);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = kClusterCtas;
+    attr[0].val.clusterDim.x = C;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_tail_cluster<T, W>, g, b, vec, l0, l1);
+    return cudaLaunchKernelEx(&cfg, k_tail_cluster<T, W, C>, g, b, vec, l0, l1);
+}
+template <typename T, int W>
+cudaError_t LaunchTailCluster(const DevGrid& g, const DevBatch& b, T* vec, int l0, int l1, int nActive, cudaStream_t st) {
+    switch (ClusterCtasFor(nActive)) {
+        case 8: return LaunchTailClusterC<T, W, 8>(g, b, vec, l0, l1, nActive, st);
+        case 4: return LaunchTailClusterC<T, W, 4>(g, b, vec, l0, l1, nActive, st);
+        case 2: return LaunchTailClusterC<T, W, 2>(g, b, vec, l0, l1, nActive, st);
+        default: return LaunchTailClusterC<T, W, 1>(g, b, vec, l0, l1, nActive, st);
+    }
 }
 
 }  // namespace gs

@@ -1229,8 +1229,8 @@ inline size_t QueueBytes(int nLevels) { return (size_t)6 * nLevels * sizeof(int)
 namespace gs {
 
 // One step of the few systems of a batch (their list in b.activeList): factorisation, backward substitution and,
-// in mixed precision, the FP64-residual refinement. With `cluster` (at most kClusterMaxSystems systems) every level
-// runs as one cluster of CTAs per system (gs_cluster.cuh); otherwise levels below `lt` (many entries each) run as
+// in mixed precision, the FP64-residual refinement. With `cluster` every level runs as one cluster of CTAs per system
+// (gs_cluster.cuh; 8 CTAs each for a handful of systems, fewer as they grow); otherwise levels below `lt` (many entries each) run as
 // per-level launches over the batch, the levels above as one CTA per system.
 template <typename T>
 int64_t FewSystemsSolve(const DevGrid& g, const DevBatch& b, const Symbolic& s, int nActive, int lt, bool refine,
@@ -3646,15 +3646,23 @@ bool ClusterWalkAvailable() {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int n = 0;
-    for (const void* f : {(const void*)k_tail_cluster<double, kWorkFactor>, (const void*)k_tail_cluster<double, kWorkBackward>,
-                          (const void*)k_tail_cluster<float, kWorkFactor>, (const void*)k_tail_cluster<float, kWorkBackward>,
-                          (const void*)k_tail_cluster<float, kWorkForward>}) {
-        if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClusterSmemMax) != cudaSuccess ||
-            cudaOccupancyMaxActiveClusters(&n, f, &cfg) != cudaSuccess || n < 1) {
+#define GS_CLUSTER_KERNELS(C)                                                                                    \
+    (const void*)k_tail_cluster<double, kWorkFactor, C>, (const void*)k_tail_cluster<double, kWorkBackward, C>,     \
+        (const void*)k_tail_cluster<double, kWorkForward, C>, (const void*)k_tail_cluster<float, kWorkFactor, C>,   \
+        (const void*)k_tail_cluster<float, kWorkBackward, C>, (const void*)k_tail_cluster<float, kWorkForward, C>
+    for (const void* f : {GS_CLUSTER_KERNELS(1), GS_CLUSTER_KERNELS(2), GS_CLUSTER_KERNELS(4), GS_CLUSTER_KERNELS(8)})
+        if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClusterSmemMax) != cudaSuccess) {
             cudaGetLastError();
             return false;
         }
-    }
+#undef GS_CLUSTER_KERNELS
+    // the largest cluster must fit (the smaller ones then do)
+    for (const void* f : {(const void*)k_tail_cluster<double, kWorkFactor, kClusterCtas>,
+                          (const void*)k_tail_cluster<float, kWorkFactor, kClusterCtas>})
+        if (cudaOccupancyMaxActiveClusters(&n, f, &cfg) != cudaSuccess || n < 1) {
+            cudaGetLastError();
+            return false;
+        }
     return true;
 }
 }  // namespace gs
