@@ -443,77 +443,9 @@ __device__ __forceinline__ int descKind(const int4& d) { return d.w & 3; }
 __device__ __forceinline__ bool descHasA(const int4& d) { return (d.w >> 2) & 1; }
 __device__ __forceinline__ int descNode(const int4& d) { return d.w >> 3; }
 
-// How a piece of work is shared: one lane alone (serial sums; the one-system walks give each thread its own piece),
-// the S lanes of a lane group (its S systems) with the index data loaded together, or the whole warp (pair lanes).
-enum PieceMode { kModeThread = 0, kModeGroup = 1, kModeWarp = 2 };
-
-// One lane group's sums for its S systems over a short piece (at most 32 index pairs): the group's lanes load the
-// pairs together, 32 / S each in one round, and every lane then gathers its own system's operands for all of them in
-// rounds of eight pairs that do not depend on each other, summed in pair order: two dependent rounds of loads instead
-// of two per four pairs.
-template <typename T>
-__device__ __forceinline__ T dotGroupShort(const T* __restrict__ lu, const T* __restrict__ rhs, const int2* __restrict__ pr,
-                                           int64_t q0, int64_t q1, size_t B, int s) {
-    constexpr int S = Lay<T>::S, K = 32 / S, R = 8 / S;  // pair slots per lane; slots per round of eight pairs
-    const int lane = threadIdx.x & 31, gbase = lane & ~(S - 1), j = lane & (S - 1);
-    const unsigned mask = ((1u << S) - 1u) << gbase;
-    const int n = (int)(q1 - q0);
-    int2 mine[K];
-#pragma unroll
-    for (int k = 0; k < K; k++) mine[k] = j + k * S < n ? __ldg(pr + q0 + j + k * S) : make_int2(0, 0);
-    T acc = T(0);
-#pragma unroll
-    for (int k0 = 0; k0 < K; k0 += R) {
-        if (k0 * S >= n) break;  // uniform over the group
-        T l[8], r[8];
-#pragma unroll
-        for (int kk = 0; kk < R; kk++)
-#pragma unroll
-            for (int jj = 0; jj < S; jj++) {
-                const int u = kk * S + jj;
-                const int a = __shfl_sync(mask, mine[k0 + kk].x, gbase + jj);
-                const int c = __shfl_sync(mask, mine[k0 + kk].y, gbase + jj);
-                const bool ok = (k0 + kk) * S + jj < n;
-                l[u] = ok ? lu[a * B + s] : T(0);
-                r[u] = ok ? rhs[c * B + s] : T(0);
-            }
-#pragma unroll
-        for (int u = 0; u < 8; u++) acc += l[u] * r[u];
-    }
-    return acc;
-}
-
-// The same for a backward node of at most 32 U entries: the group loads the rows together; U(k, r) sits in the
-// node's consecutive slots base + 1 + t.
-template <typename T>
-__device__ __forceinline__ T backGroupShort(const T* __restrict__ lu, const T* __restrict__ y, const int* __restrict__ rows,
-                                            int64_t base, int c, size_t B, int s) {
-    constexpr int S = Lay<T>::S, K = 32 / S, R = 8 / S;
-    const int lane = threadIdx.x & 31, gbase = lane & ~(S - 1), j = lane & (S - 1);
-    const unsigned mask = ((1u << S) - 1u) << gbase;
-    int mine[K];
-#pragma unroll
-    for (int k = 0; k < K; k++) mine[k] = j + k * S < c ? __ldg(rows + j + k * S) : 0;
-    T acc = T(0);
-#pragma unroll
-    for (int k0 = 0; k0 < K; k0 += R) {
-        if (k0 * S >= c) break;  // uniform over the group
-        T uu[8], x[8];
-#pragma unroll
-        for (int kk = 0; kk < R; kk++)
-#pragma unroll
-            for (int jj = 0; jj < S; jj++) {
-                const int u = kk * S + jj, t = (k0 + kk) * S + jj;
-                const int r = __shfl_sync(mask, mine[k0 + kk], gbase + jj);
-                const bool ok = t < c;
-                uu[u] = ok ? lu[(base + 1 + t) * B + s] : T(0);
-                x[u] = ok ? y[r * B + s] : T(0);
-            }
-#pragma unroll
-        for (int u = 0; u < 8; u++) acc += uu[u] * x[u];
-    }
-    return acc;
-}
+// How a piece of work is shared: one lane alone (serial sums: a lane group's short piece in the batched layouts, a
+// thread's own piece in the one-system walks) or the whole warp (pair lanes).
+enum PieceMode { kModeThread = 0, kModeWarp = 2 };
 
 // One entry of the fused factorisation: A - sum(left * right), divided by the node's pivot for lower entries;
 // the diagonal's result is the pivot (kept in its own array: the diagonal slot keeps A(k, k)). The value the entry
@@ -530,9 +462,7 @@ __device__ __forceinline__ void factorPiece(const DevGrid& g, const DevBatch& b,
     const T a = kind == kFwd ? y[slot * B + s] : (descHasA(d) ? lu[slot * B + s] : T(0));
     const T pv = kind == kLower ? ((const T*)b.piv)[node * B + s] : T(1);
     const T* rhs = kind == kFwd ? y : lu;
-    const T dot = M == kModeWarp    ? dotSP<T>(lu, rhs, g.pairs, q0, q1, B, s)
-                  : M == kModeGroup ? dotGroupShort<T>(lu, rhs, g.pairs, q0, q1, B, s)
-                                    : dotSerial<T>(lu, rhs, g.pairs, q0, q1, B, s);
+    const T dot = M == kModeWarp ? dotSP<T>(lu, rhs, g.pairs, q0, q1, B, s) : dotSerial<T>(lu, rhs, g.pairs, q0, q1, B, s);
     const bool writer = M != kModeWarp || (threadIdx.x & 31) < Lay<T>::S;
     T v = a - dot;
     if (kind == kFwd) {
@@ -584,8 +514,6 @@ __device__ __forceinline__ void backwardPiece(const DevGrid& g, const DevBatch& 
         }
 #pragma unroll
         for (int off = S; off < 32; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-    } else if (M == kModeGroup) {
-        acc = backGroupShort<T>(lu, y, rows, base, c, B, s);
     } else {
         int t = 0;
         for (; t + 4 <= c; t += 4) {
@@ -618,9 +546,7 @@ __device__ __forceinline__ void forwardPiece(const DevGrid& g, const DevBatch& b
     const int64_t q0 = d.y, q1 = d.z;
     const T* lu = (const T*)b.lu;
     const T vk = v[k * B + s];
-    const T dot = M == kModeWarp    ? dotSP<T>(lu, v, g.pairs, q0, q1, B, s)
-                  : M == kModeGroup ? dotGroupShort<T>(lu, v, g.pairs, q0, q1, B, s)
-                                    : dotSerial<T>(lu, v, g.pairs, q0, q1, B, s);
+    const T dot = M == kModeWarp ? dotSP<T>(lu, v, g.pairs, q0, q1, B, s) : dotSerial<T>(lu, v, g.pairs, q0, q1, B, s);
     const T r = vk - dot;
     if (M != kModeWarp || (threadIdx.x & 31) < Lay<T>::S) v[k * B + s] = r;
 }
@@ -647,30 +573,19 @@ __device__ __forceinline__ void runItem(const int4* __restrict__ desc, const int
 
 enum WhichWork { kWorkFactor = 0, kWorkBackward = 1, kWorkForward = 2 };
 
-// A work item of the batched layouts (S systems x P pair lanes per warp): a wide piece by the whole warp, short pieces
-// by the lane groups, their index data loaded by each group together.
 template <typename T, int W>
 __device__ __forceinline__ void doItem(const DevGrid& g, const DevBatch& b, T* vec, int it, int s, bool act) {
     if (W == kWorkFactor)
-        runItem<T>(g.fDesc, g.fItems, it, [&](const int4 d, bool wide) {
-            if (wide) factorPiece<T, kModeWarp>(g, b, d, s, act);
-            else factorPiece<T, kModeGroup>(g, b, d, s, act);
-        });
+        runItem<T>(g.fDesc, g.fItems, it, [&](const int4 d, bool wide) { factorEntry<T>(g, b, d, s, act, wide); });
     else if (W == kWorkBackward)
-        runItem<T>(g.bDesc, g.bItems, it, [&](const int4 d, bool wide) {
-            if (wide) backwardPiece<T, kModeWarp>(g, b, vec, d, s);
-            else backwardPiece<T, kModeGroup>(g, b, vec, d, s);
-        });
+        runItem<T>(g.bDesc, g.bItems, it, [&](const int4 d, bool wide) { backwardNode<T>(g, b, vec, d, s, wide); });
     else
-        runItem<T>(g.vDesc, g.vItems, it, [&](const int4 d, bool wide) {
-            if (wide) forwardPiece<T, kModeWarp>(g, b, vec, d, s);
-            else forwardPiece<T, kModeGroup>(g, b, vec, d, s);
-        });
+        runItem<T>(g.vDesc, g.vItems, it, [&](const int4 d, bool wide) { forwardEntry<T>(g, b, vec, d, s, wide); });
 }
 
 // One level (or phase) of a schedule, items [i0, i1): block (32, 4), a warp per item, S systems per warp.
 template <typename T, int W>
-__global__ void __launch_bounds__(128, 8) k_level(DevGrid g, DevBatch b, T* vec, int i0, int i1) {
+__global__ void __launch_bounds__(128, 10) k_level(DevGrid g, DevBatch b, T* vec, int i0, int i1) {
     const int it = i0 + blockIdx.x * 4 + threadIdx.y;
     const int s = laneSystem<T>(blockIdx.y);
     if (it >= i1) return;
