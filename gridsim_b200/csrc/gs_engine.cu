@@ -1675,6 +1675,7 @@ struct gs_grid {
     int split = 0;      // first level run by the persistent kernels (factorisation)
     int splitB = 0;     // first level run by the persistent kernels in the triangular solves
     int tailSplit = 0;  // first level the few-systems path runs as one CTA per system
+    int tailMax = gs::kTailMaxSystems;  // the few-systems path takes over at this many systems still stepping
 };
 
 struct MatrixPattern {
@@ -1807,6 +1808,7 @@ int UploadGrid(gs_grid* G) {
     // it) fit twice in a CTA's warps in each phase; the wide levels below run one launch per level and phase
     // the few-systems path runs the lowest levels as per-level launches while a phase of them holds more short
     // pieces than one CTA's threads (more than one round of a one-system walk)
+    if (const char* e = std::getenv("GS_TAIL_MAX")) G->tailMax = std::max(0, std::min(kTailMaxSystems, std::atoi(e)));
     G->tailSplit = 0;
     for (int l = 0; l < s.nLevels; l++) {
         bool wideLevel = false;
@@ -2177,7 +2179,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
         const int nActive = ctx->pinnedCount[0];
         const int anyRefine = refine && ctx->pinnedCount[1] > 0 ? 1 : 0;
         sysIters += nActive;
-        if (nActive <= kTailMaxSystems) {
+        if (nActive <= G->tailMax) {
             if (midOn) {  // the mid workspace's systems go back to the batch, which the few-systems path gathers from
                 k_scatter<<<dim3(nodeBlocks.x, cur.B / 32), blk8, 0, st>>>(cur, b, G->mws.origin.as<int>(), s.n);
                 launches++;
