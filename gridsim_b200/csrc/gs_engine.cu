@@ -32,6 +32,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "gs_host.h"
@@ -1247,6 +1248,7 @@ __global__ void __launch_bounds__(kTailThreads) k_tail(DevGrid g, DevBatch b, T*
 inline size_t QueueBytes(int nLevels) { return (size_t)6 * nLevels * sizeof(int); }
 
 }  // namespace gs
+#include "gs_paired.cuh"
 #include "gs_cluster.cuh"
 namespace gs {
 
@@ -1676,6 +1678,8 @@ struct gs_grid {
     int splitB = 0;     // first level run by the persistent kernels in the triangular solves
     int tailSplit = 0;  // first level the few-systems path runs as one CTA per system
     int tailMax = gs::kTailMaxSystems;  // the few-systems path takes over at this many systems still stepping
+    int psSplit = 0, psSplitB = 0;      // the same first persistent levels on the paired schedule
+    bool paired = true;                 // the full-batch step and the cluster walk run the paired schedule
 };
 
 struct MatrixPattern {
@@ -1802,6 +1806,50 @@ int UploadGrid(gs_grid* G) {
         UPT(t.bWalk, bWalk); UPT(t.bWalkPtr, bWalkPtr); UPT(t.bWalkWide, bWalkWide);
         UPT(t.bRowPtr, bRowPtr); UPT(t.bRowSm, bRowSm);
 #undef UPT
+    }
+    v.psLevels = 0;
+    G->paired = std::getenv("GS_SCALAR_SCHEDULE") == nullptr;  // the scalar schedule everywhere, for comparison
+    if (s.ps.on) {
+        const Symbolic::PairSchedule& P = s.ps;
+        std::vector<int2> pp(P.pairs.size() / 2);
+        for (size_t q = 0; q < pp.size(); q++) pp[q] = make_int2(P.pairs[2 * q], P.pairs[2 * q + 1]);
+        // descriptors in schedule order (position = work index)
+        auto order = [](const std::vector<int32_t>& work, const std::vector<int32_t>& ta, const std::vector<int32_t>& tb,
+                        std::vector<int4>& oa, std::vector<int4>& ob) {
+            for (int t : work) {
+                oa.push_back(make_int4(ta[4 * t], ta[4 * t + 1], ta[4 * t + 2], ta[4 * t + 3]));
+                ob.push_back(make_int4(tb[4 * t], tb[4 * t + 1], tb[4 * t + 2], tb[4 * t + 3]));
+            }
+        };
+        std::vector<int4> fa, fb, ba, bb, va, vb;
+        order(P.factor.work, P.taskA, P.taskB, fa, fb);
+        order(P.backward.work, P.bTaskA, P.bTaskB, ba, bb);
+        order(P.forward.work, P.taskA, P.taskB, va, vb);
+        UP(pp, psPairs);
+        UP(fa, pfA); UP(fb, pfB); UP(ba, pbA); UP(bb, pbB); UP(va, pvA); UP(vb, pvB);
+        UP(P.factor.items, pfItems); UP(P.backward.items, pbItems); UP(P.forward.items, pvItems);
+        UP(P.factor.levelItemPtr, pfLevelPtr); UP(P.backward.levelItemPtr, pbLevelPtr); UP(P.forward.levelItemPtr, pvLevelPtr);
+        UP(P.factor.levelWorkPtr, pfWorkPtr); UP(P.backward.levelWorkPtr, pbWorkPtr); UP(P.forward.levelWorkPtr, pvWorkPtr);
+        UP(P.factor.levelWide, pfWide); UP(P.backward.levelWide, pbWide); UP(P.forward.levelWide, pvWide);
+        UP(P.factor.levelMid, pfMid); UP(P.backward.levelMid, pbMid); UP(P.forward.levelMid, pvMid);
+        v.psLevels = P.nLevels;
+        // the persistent walks' first levels, as for the scalar schedule below
+        G->psSplit = P.nLevels;
+        for (int l = P.nLevels - 1; l >= 0; l--) {
+            const auto& fp = P.factor.levelItemPtr;
+            const int a = fp[2 * l + 1] - fp[2 * l], b2 = fp[2 * l + 2] - fp[2 * l + 1];
+            const int c = P.backward.levelItemPtr[l + 1] - P.backward.levelItemPtr[l];
+            if (std::max(std::max(a, b2), c) > 2 * kPersistWarps) break;
+            G->psSplit = l;
+        }
+        G->psSplitB = P.nLevels;
+        for (int l = P.nLevels - 1; l >= 0; l--) {
+            const int c = P.backward.levelItemPtr[l + 1] - P.backward.levelItemPtr[l];
+            const int vv = P.forward.levelItemPtr[l + 1] - P.forward.levelItemPtr[l];
+            if (std::max(c, vv) > 2 * kPersistWarps) break;
+            G->psSplitB = l;
+        }
+        G->psSplitB = std::min(G->psSplitB, G->psSplit);
     }
 #undef UP
     // the persistent kernels take every level from the first one whose items (and those of all levels above
@@ -2002,7 +2050,10 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
     int64_t stepLaunches = 0;
     // levels [0, split) run one launch per level (wide: thousands of tasks); levels [split, nLevels) run in
     // one persistent launch per phase (narrow: a few tasks per level, latency-bound)
-    const int split = G->split, splitB = G->splitB;
+    // the full-batch step runs the paired schedule (units of one node or a 2 x 2 pair) where the grid has one
+    const bool pairedOn = G->paired && g.psLevels > 0;
+    const int nLv = pairedOn ? g.psLevels : s.nLevels;
+    const int split = pairedOn ? G->psSplit : G->split, splitB = pairedOn ? G->psSplitB : G->splitB;
     const int persistThreads = 32;
     // warps per persistent CTA: as many as let every system group's CTA be resident at once (one wave), at most
     // kPersistWarps (a second partial wave would double the launch)
@@ -2021,7 +2072,8 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
         for (int wpc = kPersistWarps; wpc >= 4; wpc--) {
             persistWarps = wpc;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_persistent<T, kWorkFactor>, 32 * wpc, 0) == cudaSuccess &&
+            const void* pk = pairedOn ? (const void*)k_ppersistent<T, kWorkFactor> : (const void*)k_persistent<T, kWorkFactor>;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pk, 32 * wpc, 0) == cudaSuccess &&
                 (int64_t)occ * sms >= base.B / Lay<T>::S)
                 break;
         }
@@ -2044,39 +2096,43 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
         const int grp = (bb.count + Lay<T>::S - 1) / Lay<T>::S;
         if (i1 > i0 && grp > 0) { kernel<<<dim3((i1 - i0 + 3) / 4, grp), blk4, 0, ss>>>(g, bb, vec, i0, i1); stepLaunches++; }
     };
-    const auto& fp = s.factor.levelItemPtr;
-    const auto& bp = s.backward.levelItemPtr;
-    const auto& vp = s.forward.levelItemPtr;
+    const auto& fp = pairedOn ? s.ps.factor.levelItemPtr : s.factor.levelItemPtr;
+    const auto& bp = pairedOn ? s.ps.backward.levelItemPtr : s.backward.levelItemPtr;
+    const auto& vp = pairedOn ? s.ps.forward.levelItemPtr : s.forward.levelItemPtr;
+    // one level of schedule W: the paired kernels or the scalar ones
+    auto level = [&](const DevBatch& bb, cudaStream_t ss, auto wTag, T* vec, int i0, int i1) {
+        constexpr int W = decltype(wTag)::value;
+        if (pairedOn) launchLevel(bb, ss, k_plevel<T, W>, vec, i0, i1);
+        else launchLevel(bb, ss, k_level<T, W>, vec, i0, i1);
+    };
+    auto persistent = [&](const DevBatch& bb, cudaStream_t ss, auto wTag, T* vec, int l0) {
+        constexpr int W = decltype(wTag)::value;
+        const dim3 grid((bb.count + Lay<T>::S - 1) / Lay<T>::S), blk(persistThreads, persistWarps);
+        if (pairedOn) k_ppersistent<T, W><<<grid, blk, 0, ss>>>(g, bb, vec, l0, nLv);
+        else k_persistent<T, W><<<grid, blk, 0, ss>>>(g, bb, vec, l0, nLv);
+        stepLaunches++;
+    };
+    using FW = std::integral_constant<int, kWorkFactor>;
+    using BW = std::integral_constant<int, kWorkBackward>;
+    using VW = std::integral_constant<int, kWorkForward>;
     auto factorPhase = [&](const DevBatch& bb, cudaStream_t ss) {
         for (int l = 0; l < split; l++) {
-            launchLevel(bb, ss, k_level<T, kWorkFactor>, (T*)bb.y, fp[2 * l], fp[2 * l + 1]);
-            launchLevel(bb, ss, k_level<T, kWorkFactor>, (T*)bb.y, fp[2 * l + 1], fp[2 * l + 2]);
+            level(bb, ss, FW{}, (T*)bb.y, fp[2 * l], fp[2 * l + 1]);
+            level(bb, ss, FW{}, (T*)bb.y, fp[2 * l + 1], fp[2 * l + 2]);
         }
-        if (split < s.nLevels) {
-            k_persistent<T, kWorkFactor><<<(bb.count + Lay<T>::S - 1) / Lay<T>::S, dim3(persistThreads, persistWarps), 0, ss>>>(
-                g, bb, (T*)bb.y, split, s.nLevels);
-            stepLaunches++;
-        }
+        if (split < nLv) persistent(bb, ss, FW{}, (T*)bb.y, split);
     };
     auto backward = [&](const DevBatch& bb, cudaStream_t ss, T* vec) {
-        if (splitB < s.nLevels) {
-            k_persistent<T, kWorkBackward><<<(bb.count + Lay<T>::S - 1) / Lay<T>::S, dim3(persistThreads, persistWarps), 0, ss>>>(
-                g, bb, vec, splitB, s.nLevels);
-            stepLaunches++;
-        }
-        for (int l = splitB - 1; l >= 0; l--) launchLevel(bb, ss, k_level<T, kWorkBackward>, vec, bp[l], bp[l + 1]);
+        if (splitB < nLv) persistent(bb, ss, BW{}, vec, splitB);
+        for (int l = splitB - 1; l >= 0; l--) level(bb, ss, BW{}, vec, bp[l], bp[l + 1]);
     };
     auto solvePhase = [&](const DevBatch& bb, cudaStream_t ss, bool doRefine) {
         backward(bb, ss, (T*)bb.y);
         if (doRefine) {
             k_residual<T><<<dim3((s.n + 7) / 8, (bb.count + 31) / 32), blk8, 0, ss>>>(g, bb, nullptr, 0);
             stepLaunches++;
-            for (int l = 0; l < splitB; l++) launchLevel(bb, ss, k_level<T, kWorkForward>, (T*)bb.z, vp[l], vp[l + 1]);
-            if (splitB < s.nLevels) {
-                k_persistent<T, kWorkForward><<<(bb.count + Lay<T>::S - 1) / Lay<T>::S, dim3(persistThreads, persistWarps), 0, ss>>>(
-                    g, bb, (T*)bb.z, splitB, s.nLevels);
-                stepLaunches++;
-            }
+            for (int l = 0; l < splitB; l++) level(bb, ss, VW{}, (T*)bb.z, vp[l], vp[l + 1]);
+            if (splitB < nLv) persistent(bb, ss, VW{}, (T*)bb.z, splitB);
             backward(bb, ss, (T*)bb.z);
         }
     };
@@ -3430,7 +3486,10 @@ int LinearSolve(gs_grid* G, int cnt) {
     };
     const auto& fp = s.factor.levelItemPtr;
     const auto& bp = s.backward.levelItemPtr;
-    const int split = G->split, splitB = G->splitB;
+    // the full-batch step runs the paired schedule (units of one node or a 2 x 2 pair) where the grid has one
+    const bool pairedOn = G->paired && g.psLevels > 0;
+    const int nLv = pairedOn ? g.psLevels : s.nLevels;
+    const int split = pairedOn ? G->psSplit : G->split, splitB = pairedOn ? G->psSplitB : G->splitB;
     for (int l = 0; l < split; l++) {
         level(k_level<T, kWorkFactor>, fp[2 * l], fp[2 * l + 1]);
         level(k_level<T, kWorkFactor>, fp[2 * l + 1], fp[2 * l + 2]);

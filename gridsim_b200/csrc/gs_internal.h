@@ -31,6 +31,10 @@ struct HostGrid {
 
 // Entry kinds of the fused factor + forward-substitution schedule.
 enum EntryKind : int32_t { kDiag = 0, kUpper = 1, kFwd = 2, kLower = 3 };
+// Task kinds of the paired schedule (Symbolic::PairSchedule): the entry kinds above for single nodes, then a pair's
+// diagonal block, upper rows, lower columns and forward entry; backward tasks of a single node and of a pair.
+enum PairTaskKind : int32_t { kPDiag = 4, kPUpper = 5, kPLower = 6, kPFwd = 7 };
+enum PairBackKind : int32_t { kBNode = 0, kBPair = 1 };
 
 // Shared symbolic analysis of one grid (SparseNewtonRaphsonPowerFlow.BuildY / BuildJacobianStructure,
 // NewtonShell.BuildBusSpec / EquationPositions, then the static-pivot LU pattern and its schedule).
@@ -95,6 +99,31 @@ struct Symbolic {
         std::vector<int32_t> levelMid;     // how many of the short pieces after them are longer than 8 pairs
     };
     Schedule factor, backward, forward;
+
+    // The paired schedule: two consecutive nodes k, k + 1 whose structure makes them one 2 x 2 block (a PQ bus's angle
+    // and magnitude: parent(k) = k + 1, P_k = {k + 1} + P_{k+1}, and the row subtree of k + 1 is that of k plus k) form
+    // one unit, every other node a unit of its own. A pair's entries are computed together, so that L(k + 1, j) =
+    // L(k, j) + 1 slot and U(j, k + 1) = U(j, k) + 1 slot share one index pair and the elimination tree of units has
+    // about half the levels. The LU storage is the node-major one above. Tasks (8 ints each, taskA / taskB):
+    //   taskA = {first pair, end of pairs, kind | hasA bits << 3, node k}, taskB = {s0, s1, aux, 0} with
+    //   kDiag / kUpper / kFwd / kLower (a single node's entries as above): s0 = slot (y index for kFwd);
+    //   kPDiag: the 2 x 2 diagonal block, s0 = luBase[k], s1 = luBase[k + 1], aux = |P_{k+1}|, pairs (L(k, j), U(j, k));
+    //   kPUpper: U(k, r), U(k + 1, r) in s0, s1, aux = slot of L(k + 1, k), pairs (L(k, j), U(j, r));
+    //   kPLower: L(r, k), L(r, k + 1) in s0, s1, aux = slot of U(k, k + 1), pairs (L(r, j), U(j, k));
+    //   kPFwd: y(k), y(k + 1), aux = slot of L(k + 1, k), pairs (L(k, j), j);
+    //   backward kBNode: x(k) over U(k, r) from s0 + 1, rows pRows[first .. end); kBPair: x(k + 1) then x(k), U(k, r)
+    //   from s0, U(k + 1, r) from s1, U(k, k + 1) at aux, rows P_{k+1}.
+    // hasA bits: whether each output starts from a value of A (bit i for output i; the block's 4 outputs in the order
+    // (k, k), (k, k + 1), (k + 1, k), (k + 1, k + 1)).
+    struct PairSchedule {
+        bool on = false;
+        int nUnits = 0, nPaired = 0, nLevels = 0;
+        std::vector<int32_t> taskA, taskB;  // factorisation and forward tasks, 4 ints each
+        std::vector<int32_t> bTaskA, bTaskB;
+        std::vector<int32_t> pairs;         // 2 per pair
+        Schedule factor, backward, forward; // work: task indices (backward: into bTask*)
+    };
+    PairSchedule ps;
 
     // The top of the elimination tree (levels >= L0) held in shared memory by the one-system walks: the LU
     // values of its nodes (node k's [diag, U..., L...] from smemBase[k]) and then their right-hand-side values

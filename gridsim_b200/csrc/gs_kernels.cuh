@@ -128,6 +128,31 @@ struct DevGrid {
     const int* pRowPtr;
     const int* pRows;
     DevTop top[2];        // [0] FP64, [1] FP32
+    // the paired schedule (Symbolic::PairSchedule): units of one node or a 2 x 2 pair; per schedule the task
+    // descriptors A / B in schedule order, the items and the per-level (phase) item and work ranges
+    int psLevels;         // 0: no paired schedule
+    const int2* psPairs;
+    const int4* pfA;
+    const int4* pfB;
+    const int* pfItems;
+    const int* pfLevelPtr;
+    const int* pfWorkPtr;
+    const int* pfWide;
+    const int* pfMid;
+    const int4* pbA;
+    const int4* pbB;
+    const int* pbItems;
+    const int* pbLevelPtr;
+    const int* pbWorkPtr;
+    const int* pbWide;
+    const int* pbMid;
+    const int4* pvA;
+    const int4* pvB;
+    const int* pvItems;
+    const int* pvLevelPtr;
+    const int* pvWorkPtr;
+    const int* pvWide;
+    const int* pvMid;
 };
 
 struct DevBatch {

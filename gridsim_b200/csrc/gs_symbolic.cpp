@@ -459,6 +459,145 @@ std::string FactorSymbolic(Symbolic& s, const std::function<void(const std::func
         pack(s.backward, bwd, lenBwd);
         pack(s.forward, fwd, lenFwd);
     }
+
+    // ---------------- the paired schedule (Symbolic::PairSchedule) ----------------
+    {
+        Symbolic::PairSchedule& P = s.ps;
+        P = Symbolic::PairSchedule();
+        // units: k, k + 1 paired when parent(k) = k + 1, |P_k| = |P_{k+1}| + 1 (so P_k = {k + 1} + P_{k+1} by the
+        // fill property) and the row subtree of k + 1 is that of k plus k; every other node alone
+        std::vector<int> unitOf(m, -1), unitFirst;
+        std::vector<char> unitPair;
+        for (int k = 0; k < m;) {
+            bool pair = false;
+            if (k + 1 < m && s.parent[k] == k + 1 && s.luCnt[k] == s.luCnt[k + 1] + 1) {
+                const std::vector<int>& a = rowSub[k];
+                const std::vector<int>& b2 = rowSub[k + 1];
+                pair = b2.size() == a.size() + 1 && b2.back() == k && std::equal(a.begin(), a.end(), b2.begin());
+            }
+            unitOf[k] = (int)unitFirst.size();
+            if (pair) unitOf[k + 1] = (int)unitFirst.size();
+            unitFirst.push_back(k);
+            unitPair.push_back(pair ? 1 : 0);
+            k += pair ? 2 : 1;
+        }
+        const int nU = (int)unitFirst.size();
+        std::vector<int> uLevel(nU, 0);
+        for (int u = 0; u < nU; u++) {  // a unit's parent unit holds the parent of its last node (a later unit)
+            const int par = s.parent[unitFirst[u] + unitPair[u]];
+            if (par >= 0) uLevel[unitOf[par]] = std::max(uLevel[unitOf[par]], uLevel[u] + 1);
+        }
+        int nL = 0;
+        for (int u = 0; u < nU; u++) nL = std::max(nL, uLevel[u] + 1);
+        std::vector<std::vector<int>> byLevel(nL);
+        for (int u = 0; u < nU; u++) byLevel[uLevel[u]].push_back(u);
+        auto npairs = [&]() { return (int64_t)P.pairs.size() / 2; };
+        auto addTask = [&](int64_t q0, int kindFlags, int k, int64_t s0, int64_t s1, int64_t aux) {
+            P.taskA.insert(P.taskA.end(), {(int32_t)q0, (int32_t)npairs(), kindFlags, k});
+            P.taskB.insert(P.taskB.end(), {(int32_t)s0, (int32_t)s1, (int32_t)aux, 0});
+            return (int32_t)(P.taskA.size() / 4 - 1);
+        };
+        auto addBack = [&](int r0, int r1, int kind, int k, int64_t s0, int64_t s1, int64_t aux) {
+            P.bTaskA.insert(P.bTaskA.end(), {r0, r1, kind, k});
+            P.bTaskB.insert(P.bTaskB.end(), {(int32_t)s0, (int32_t)s1, (int32_t)aux, 0});
+            return (int32_t)(P.bTaskA.size() / 4 - 1);
+        };
+        auto hb = [&](int64_t slot) { return (int)hasA[slot]; };
+        for (Symbolic::Schedule* sc : {&P.factor, &P.backward, &P.forward}) {
+            sc->levelItemPtr.assign(1, 0);
+            sc->levelWorkPtr.assign(1, 0);
+        }
+        std::vector<int> posK1(m, -1);
+        std::vector<std::vector<int32_t>> up, lo;
+        std::vector<int32_t> dg, fw;
+        for (int l = 0; l < nL; l++) {
+            std::vector<int32_t> phA, phB, bwd, fwd;
+            std::vector<int64_t> lenA, lenB, lenBwd, lenFwd;
+            for (int u : byLevel[l]) {
+                const int k = unitFirst[u];
+                if (!unitPair[u]) {  // a single node: its entries as in the scalar schedule
+                    const int e0 = s.diagPairNode[k], c = s.luCnt[k];
+                    for (int e = e0; e < e0 + 2 * c + 2; e++) {
+                        const int64_t p0 = s.entPairPtr[e], p1 = s.entPairPtr[e + 1];
+                        const int kind = s.entKind[e];
+                        if ((kind == kUpper || kind == kFwd) && p1 == p0 && s.entHasA[e]) continue;
+                        const int64_t q0 = npairs();
+                        P.pairs.insert(P.pairs.end(), s.pairs.begin() + 2 * p0, s.pairs.begin() + 2 * p1);
+                        const int32_t t = addTask(q0, kind | (s.entHasA[e] << 3), k, s.entSlot[e], 0, 0);
+                        if (kind == kLower) { phB.push_back(t); lenB.push_back(p1 - p0); }
+                        else { phA.push_back(t); lenA.push_back(p1 - p0); }
+                        if (kind == kFwd) { fwd.push_back(t); lenFwd.push_back(p1 - p0); }
+                    }
+                    bwd.push_back(addBack(s.pRowPtr[k], s.pRowPtr[k + 1], kBNode, k, s.luBase[k], 0, 0));
+                    lenBwd.push_back(c);
+                    continue;
+                }
+                // a pair k, k + 1: c = |P_{k+1}|, |P_k| = c + 1. Slots: U(k, k + 1) = bk + 1, L(k + 1, k) = bk + 2 + c,
+                // U(k, P_{k+1}[t]) = bk + 2 + t, L(P_{k+1}[t], k) = bk + 3 + c + t, U(k + 1, P_{k+1}[t]) = bk1 + 1 + t,
+                // L(P_{k+1}[t], k + 1) = bk1 + 1 + c + t
+                const int c = s.luCnt[k + 1];
+                const int64_t bk = s.luBase[k], bk1 = s.luBase[k + 1];
+                const int64_t sUkk1 = bk + 1, sLk1k = bk + 2 + c;
+                for (int t = 0; t < c; t++) posK1[s.pRows[s.pRowPtr[k + 1] + t]] = t;
+                up.assign(c, {});
+                lo.assign(c, {});
+                dg.clear();
+                fw.clear();
+                for (int j : rowSub[k]) {
+                    const int cj = s.luCnt[j];
+                    const int tk = posIn(j, k);  // k + 1 follows at tk + 1 (the pairing rule)
+                    if (tk < 0 || tk + 1 >= cj || s.pRows[s.pRowPtr[j] + tk + 1] != k + 1)
+                        return "paired schedule: node " + std::to_string(j) + " breaks the pair " + std::to_string(k);
+                    const int64_t Lkj = s.luBase[j] + 1 + cj + tk, Ujk = s.luBase[j] + 1 + tk;
+                    dg.push_back((int32_t)Lkj); dg.push_back((int32_t)Ujk);
+                    fw.push_back((int32_t)Lkj); fw.push_back(j);
+                    for (int t2 = tk + 2; t2 < cj; t2++) {  // r of P_j beyond k + 1 lies in P_{k+1}
+                        const int tr = posK1[s.pRows[s.pRowPtr[j] + t2]];
+                        if (tr < 0) return "paired schedule: fill outside P_{k+1} at node " + std::to_string(k);
+                        up[tr].push_back((int32_t)Lkj); up[tr].push_back((int32_t)(s.luBase[j] + 1 + t2));
+                        lo[tr].push_back((int32_t)(s.luBase[j] + 1 + cj + t2)); lo[tr].push_back((int32_t)Ujk);
+                    }
+                }
+                int64_t q0 = npairs();
+                P.pairs.insert(P.pairs.end(), dg.begin(), dg.end());
+                int32_t t = addTask(q0, kPDiag | (hb(bk) | hb(sUkk1) << 1 | hb(sLk1k) << 2 | hb(bk1) << 3) << 3, k, bk, bk1, c);
+                phA.push_back(t);
+                lenA.push_back((int64_t)dg.size());  // four products a pair
+                q0 = npairs();
+                P.pairs.insert(P.pairs.end(), fw.begin(), fw.end());
+                t = addTask(q0, kPFwd, k, k, 0, sLk1k);
+                phB.push_back(t);
+                lenB.push_back((int64_t)fw.size() / 2);
+                fwd.push_back(t);
+                lenFwd.push_back((int64_t)fw.size() / 2);
+                for (int tt = 0; tt < c; tt++) {
+                    const int64_t sU0 = bk + 2 + tt, sU1 = bk1 + 1 + tt, sL0 = bk + 3 + c + tt, sL1 = bk1 + 1 + c + tt;
+                    q0 = npairs();
+                    P.pairs.insert(P.pairs.end(), up[tt].begin(), up[tt].end());
+                    t = addTask(q0, kPUpper | (hb(sU0) | hb(sU1) << 1) << 3, k, sU0, sU1, sLk1k);
+                    phB.push_back(t);
+                    lenB.push_back((int64_t)up[tt].size() / 2);
+                    q0 = npairs();
+                    P.pairs.insert(P.pairs.end(), lo[tt].begin(), lo[tt].end());
+                    t = addTask(q0, kPLower | (hb(sL0) | hb(sL1) << 1) << 3, k, sL0, sL1, sUkk1);
+                    phB.push_back(t);
+                    lenB.push_back((int64_t)lo[tt].size() / 2);
+                }
+                for (int tt = 0; tt < c; tt++) posK1[s.pRows[s.pRowPtr[k + 1] + tt]] = -1;
+                bwd.push_back(addBack(s.pRowPtr[k + 1], s.pRowPtr[k + 1] + c, kBPair, k, bk + 2, bk1 + 1, sUkk1));
+                lenBwd.push_back(c);
+                P.nPaired++;
+            }
+            pack(P.factor, phA, lenA);
+            pack(P.factor, phB, lenB);
+            pack(P.backward, bwd, lenBwd);
+            pack(P.forward, fwd, lenFwd);
+        }
+        if (npairs() >= (int64_t)INT32_MAX) return "the paired schedule is too large for 32-bit pair indices";
+        P.nUnits = nU;
+        P.nLevels = nL;
+        P.on = true;
+    }
     BuildTopPart(s, 0, sizeof(double), kTopBudgetBytes);
     BuildTopPart(s, 1, sizeof(float), kTopBudgetBytes);
     return "";
