@@ -178,6 +178,175 @@ __device__ __forceinline__ void clRun(const DevGrid& g, const DevBatch& b, T* ve
     stL2(out, v);
 }
 
+// ---- the same walk on the paired schedule (gs_paired.cuh): a task's descriptors A, D and its index pairs ----
+
+// This lane's first round of a paired task's index pairs: (a, c) of a factorisation or forward task, (t, row) of a
+// backward task (row r = pRows[A.x + t]); x = -1 past the end.
+template <int W, int G>
+__device__ __forceinline__ void clPairsP(const DevGrid& g, const int4 A, int2 (&a)[kClusterInFlight]) {
+    const int j = G == 1 ? 0 : (int)(threadIdx.x & (G - 1));
+    if (W == kWorkBackward) {
+        const int c = A.y - A.x;
+        const int* rows = g.pRows + A.x;
+#pragma unroll
+        for (int u = 0; u < kClusterInFlight; u++) {
+            const int t = j + u * G;
+            a[u] = t < c ? make_int2(t, __ldg(rows + t)) : make_int2(-1, -1);
+        }
+    } else {
+#pragma unroll
+        for (int u = 0; u < kClusterInFlight; u++) {
+            const int q = A.x + j + u * G;
+            a[u] = q < A.y ? __ldg(g.psPairs + q) : make_int2(-1, -1);
+        }
+    }
+}
+template <int W>
+__device__ __forceinline__ void clPairsPOf(const DevGrid& g, int cls, const int4 A, int2 (&a)[kClusterInFlight]) {
+    if (cls == 0) clPairsP<W, 32>(g, A, a);
+    else if (cls == 1) clPairsP<W, 8>(g, A, a);
+    else clPairsP<W, 1>(g, A, a);
+}
+
+// the K products of one index pair of a paired task (backward: U(k, r) from s0 + t, U(k + 1, r) from s1 + t, times x(r))
+template <typename T, int W>
+__device__ __forceinline__ void clAccP(const T* lu, const T* R, int K, int s0, int s1, int2 p, size_t B, int s, T (&acc)[4]) {
+    if (p.x < 0) return;
+    if (W == kWorkBackward) {
+        const T xr = ldL2(R + (size_t)p.y * B + s);
+        acc[0] += ldL2(lu + (size_t)(s0 + p.x) * B + s) * xr;
+        if (K == 2) acc[1] += ldL2(lu + (size_t)(s1 + p.x) * B + s) * xr;
+        return;
+    }
+    const T l0 = ldL2(lu + (size_t)p.x * B + s), r0 = ldL2(R + (size_t)p.y * B + s);
+    acc[0] += l0 * r0;
+    if (K == 2) {
+        acc[1] += ldL2(lu + (size_t)(p.x + 1) * B + s) * r0;
+    } else if (K == 3) {
+        acc[1] += l0 * ldL2(R + (size_t)(p.y + 1) * B + s);
+    } else if (K == 4) {
+        const T l1 = ldL2(lu + (size_t)(p.x + 1) * B + s), r1 = ldL2(R + (size_t)(p.y + 1) * B + s);
+        acc[1] += l0 * r1;
+        acc[2] += l1 * r0;
+        acc[3] += l1 * r1;
+    }
+}
+
+// One paired task by a group of G lanes from its loaded first round; the group's first lane writes its outputs.
+template <typename T, int W, int G>
+__device__ __forceinline__ void clRunP(const DevGrid& g, const DevBatch& b, T* vec, const int4 A, const int4 D,
+                                       const int2 (&a0)[kClusterInFlight], int s, unsigned mask) {
+    constexpr int U = kClusterInFlight;
+    const size_t B = (size_t)b.B;
+    T* lu = (T*)b.lu;
+    T* piv = (T*)b.piv;
+    T* y = (T*)b.y;
+    const int j = G == 1 ? 0 : (int)(threadIdx.x & (G - 1));
+    const bool lead = j == 0;
+    const int k = A.w;
+    const int kind = W == kWorkBackward ? A.z : pkKind(A);
+    const int K = W == kWorkBackward ? (kind == kBPair ? 2 : 1) : pkProducts(kind);
+    const T* R = W == kWorkFactor ? ((kind == kFwd || kind == kPFwd) ? y : lu) : vec;
+    const int s0 = W == kWorkBackward ? (kind == kBPair ? D.x : D.x + 1) : 0, s1 = D.y;
+    auto at = [&](const T* p, int idx) { return ldL2(p + (size_t)idx * B + s); };
+    // the values the task's outputs combine with, loaded beside the first operands
+    T e[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+    if (lead) {
+        if (W == kWorkBackward) {
+            e[0] = at(vec, k); e[1] = at(piv, k);
+            if (kind == kBPair) { e[2] = at(vec, k + 1); e[3] = at(piv, k + 1); e[4] = at(lu, D.z); }
+        } else if (kind == kFwd) {
+            e[0] = at(W == kWorkFactor ? y : vec, D.x);
+        } else if (kind == kPFwd) {
+            const T* v = W == kWorkFactor ? y : vec;
+            e[0] = at(v, k); e[1] = at(v, k + 1); e[2] = at(lu, D.z);
+        } else if (kind < 4) {
+            e[0] = pkHasA(A, 0) ? at(lu, D.x) : T(0);
+            if (kind == kLower) e[1] = at(piv, k);
+        } else if (kind == kPDiag) {
+            const int c = D.z;
+            e[0] = pkHasA(A, 0) ? at(lu, D.x) : T(0);
+            e[1] = pkHasA(A, 1) ? at(lu, D.x + 1) : T(0);
+            e[2] = pkHasA(A, 2) ? at(lu, D.x + 2 + c) : T(0);
+            e[3] = pkHasA(A, 3) ? at(lu, D.y) : T(0);
+        } else {  // kPUpper (aux L(k + 1, k)) or kPLower (aux U(k, k + 1) and the two pivots)
+            e[0] = pkHasA(A, 0) ? at(lu, D.x) : T(0);
+            e[1] = pkHasA(A, 1) ? at(lu, D.y) : T(0);
+            e[2] = at(lu, D.z);
+            if (kind == kPLower) { e[3] = at(piv, k); e[4] = at(piv, k + 1); }
+        }
+    }
+    T acc[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+    for (int u = 0; u < U; u++) clAccP<T, W>(lu, R, K, s0, s1, a0[u], B, s, acc);
+    const int len = A.y - A.x;
+    for (int off = U * G; off < len; off += U * G) {
+        int2 a[U];
+        if (W == kWorkBackward) {
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int t = off + j + u * G;
+                a[u] = t < len ? make_int2(t, __ldg(g.pRows + A.x + t)) : make_int2(-1, -1);
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int q = A.x + off + j + u * G;
+                a[u] = q < A.y ? __ldg(g.psPairs + q) : make_int2(-1, -1);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) clAccP<T, W>(lu, R, K, s0, s1, a[u], B, s, acc);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) acc[i] += __shfl_xor_sync(mask, acc[i], o);
+    if (!lead) return;
+    auto put = [&](T* p, int idx, T v) { stL2(p + (size_t)idx * B + s, v); };
+    if (W == kWorkBackward) {
+        if (kind == kBNode) { put(vec, k, (e[0] - acc[0]) / e[1]); return; }
+        const T v1 = (e[2] - acc[1]) / e[3];
+        put(vec, k + 1, v1);
+        put(vec, k, (e[0] - e[4] * v1 - acc[0]) / e[1]);
+        return;
+    }
+    if (kind == kFwd) { put(W == kWorkFactor ? y : vec, D.x, e[0] - acc[0]); return; }
+    if (kind == kPFwd) {
+        T* v = W == kWorkFactor ? y : vec;
+        const T v0 = e[0] - acc[0];
+        put(v, k, v0);
+        put(v, k + 1, e[1] - acc[1] - e[2] * v0);
+        return;
+    }
+    if (kind < 4) {  // kDiag, kUpper, kLower
+        T v = e[0] - acc[0];
+        if (kind == kDiag) { put(piv, k, pkPivot<T>(b, s, e[0], v, true)); return; }
+        if (kind == kLower) v = v / e[1];
+        put(lu, D.x, v);
+        return;
+    }
+    if (kind == kPDiag) {
+        const T p0 = pkPivot<T>(b, s, e[0], e[0] - acc[0], true);
+        const T u01 = e[1] - acc[1];
+        const T l10 = (e[2] - acc[2]) / p0;
+        put(piv, k, p0);
+        put(lu, D.x + 1, u01);
+        put(lu, D.x + 2 + D.z, l10);
+        put(piv, k + 1, pkPivot<T>(b, s, e[3], e[3] - acc[3] - l10 * u01, true));
+        return;
+    }
+    if (kind == kPUpper) {
+        const T v0 = e[0] - acc[0];
+        put(lu, D.x, v0);
+        put(lu, D.y, e[1] - acc[1] - e[2] * v0);
+        return;
+    }
+    const T v0 = (e[0] - acc[0]) / e[3];  // kPLower
+    put(lu, D.x, v0);
+    put(lu, D.y, (e[1] - acc[1] - v0 * e[2]) / e[4]);
+}
+
 __device__ __forceinline__ void clusterArrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
 __device__ __forceinline__ void clusterWait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
 __device__ __forceinline__ int clusterRank() {
@@ -186,19 +355,25 @@ __device__ __forceinline__ int clusterRank() {
     return (int)r;
 }
 
-// Levels [l0, l1) of a schedule (top down for the backward substitution) for the listed system of this cluster.
-// Dynamic shared memory: the walk's phases as {first piece, wide, mid-length, end} (16 bytes each).
-template <typename T, int W, int C>
+// Levels [l0, l1) of a schedule (top down for the backward substitution) for the listed system of this cluster; PK:
+// the paired schedule (its tasks' second descriptors loaded beside the first). Dynamic shared memory: the walk's
+// phases as {first piece, wide, mid-length, end} (16 bytes each).
+template <typename T, int W, int C, bool PK>
 __global__ void __launch_bounds__(kClusterThreads) k_tail_cluster(DevGrid g, DevBatch b, T* vec, int l0, int l1) {
     constexpr int kClusterWarps = C * kClusterThreads / 32;
     extern __shared__ int4 clPhase[];
     const int s = b.activeList[blockIdx.x / C];
     // uniform over the cluster: every CTA of it returns, or none does (no CTA may miss a cluster barrier)
     if (W != kWorkFactor && vec != (T*)b.y && !b.refine[s]) return;
-    const int* ptr = W == kWorkFactor ? g.fWorkPtr : (W == kWorkBackward ? g.bWorkPtr : g.vWorkPtr);
-    const int4* desc = W == kWorkFactor ? g.fDesc : (W == kWorkBackward ? g.bDesc : g.vDesc);
-    const int* midCnt = W == kWorkFactor ? g.fMid : (W == kWorkBackward ? g.bMid : g.vMid);
-    const int* wide = W == kWorkFactor ? g.fWide : (W == kWorkBackward ? g.bWide : g.vWide);
+    const int* ptr = PK ? (W == kWorkFactor ? g.pfWorkPtr : (W == kWorkBackward ? g.pbWorkPtr : g.pvWorkPtr))
+                        : (W == kWorkFactor ? g.fWorkPtr : (W == kWorkBackward ? g.bWorkPtr : g.vWorkPtr));
+    const int4* desc = PK ? (W == kWorkFactor ? g.pfA : (W == kWorkBackward ? g.pbA : g.pvA))
+                          : (W == kWorkFactor ? g.fDesc : (W == kWorkBackward ? g.bDesc : g.vDesc));
+    const int4* descB = W == kWorkFactor ? g.pfB : (W == kWorkBackward ? g.pbB : g.pvB);
+    const int* midCnt = PK ? (W == kWorkFactor ? g.pfMid : (W == kWorkBackward ? g.pbMid : g.pvMid))
+                           : (W == kWorkFactor ? g.fMid : (W == kWorkBackward ? g.bMid : g.vMid));
+    const int* wide = PK ? (W == kWorkFactor ? g.pfWide : (W == kWorkBackward ? g.pbWide : g.pvWide))
+                         : (W == kWorkFactor ? g.fWide : (W == kWorkBackward ? g.bWide : g.vWide));
     const int phases = W == kWorkFactor ? 2 : 1;
     const int nPh = phases * (l1 - l0);
     for (int k = threadIdx.x; k < nPh; k += blockDim.x) {
@@ -211,53 +386,70 @@ __global__ void __launch_bounds__(kClusterThreads) k_tail_cluster(DevGrid g, Dev
     const int lane = threadIdx.x & 31;
     const int gw = clusterRank() * (kClusterThreads / 32) + (int)(threadIdx.x >> 5);  // warp of the cluster
     const unsigned gmask = 0xFFu << (lane & 24);
-    // the first unit of this warp two phases deep: its descriptor for phase k + 1, its descriptor and pairs for k
+    auto loadPairs = [&](int cls, const int4 d, int2 (&a)[kClusterInFlight]) {
+        if (PK) clPairsPOf<W>(g, cls, d, a);
+        else clPairsOf<W>(g, cls, d, a);
+    };
+    // the first unit of this warp two phases deep: its descriptors for phase k + 1, its descriptors and pairs for k
     int clsCur = -1, posCur = -1, clsNext = -1, posNext = -1;
     int4 dCur = make_int4(0, 0, 0, 0), dNext = make_int4(0, 0, 0, 0);
+    int4 eCur = make_int4(0, 0, 0, 0), eNext = make_int4(0, 0, 0, 0);
     int2 aCur[kClusterInFlight];
-    auto firstOf = [&](int k, int& cls, int& pos, int4& d) {
+    auto firstOf = [&](int k, int& cls, int& pos, int4& d, int4& e) {
         cls = -1;
         pos = -1;
         if (k < nPh && gw < unitCount(clPhase[k])) {
             pos = unitPiece(clPhase[k], gw, lane, cls);
-            if (pos >= 0) d = __ldg(desc + pos);
+            if (pos >= 0) {
+                d = __ldg(desc + pos);
+                if (PK) e = __ldg(descB + pos);
+            }
         }
     };
-    firstOf(0, clsCur, posCur, dCur);
-    if (posCur >= 0) clPairsOf<W>(g, clsCur, dCur, aCur);
-    firstOf(1, clsNext, posNext, dNext);
+    firstOf(0, clsCur, posCur, dCur, eCur);
+    if (posCur >= 0) loadPairs(clsCur, dCur, aCur);
+    firstOf(1, clsNext, posNext, dNext, eNext);
     for (int k = 0; k < nPh; k++) {
         const int4 P = clPhase[k];
         const int nu = unitCount(P);
         for (int u = gw; u < nu; u += kClusterWarps) {
             int cls, pos;
-            int4 d;
+            int4 d, e = make_int4(0, 0, 0, 0);
             int2 a[kClusterInFlight];
             if (u == gw) {
                 cls = clsCur;
                 pos = posCur;
                 d = dCur;
+                e = eCur;
 #pragma unroll
                 for (int q = 0; q < kClusterInFlight; q++) a[q] = aCur[q];
             } else {
                 pos = unitPiece(P, u, lane, cls);
                 if (pos >= 0) {
                     d = __ldg(desc + pos);
-                    clPairsOf<W>(g, cls, d, a);
+                    if (PK) e = __ldg(descB + pos);
+                    loadPairs(cls, d, a);
                 }
             }
-            if (cls == 0) clRun<T, W, 32>(g, b, vec, d, a, s, 0xffffffffu);          // pos is warp-uniform here
-            else if (cls == 1) { if (pos >= 0) clRun<T, W, 8>(g, b, vec, d, a, s, gmask); }  // group-uniform
-            else if (pos >= 0) clRun<T, W, 1>(g, b, vec, d, a, s, 0u);
+            if (PK) {
+                if (cls == 0) clRunP<T, W, 32>(g, b, vec, d, e, a, s, 0xffffffffu);          // pos is warp-uniform
+                else if (cls == 1) { if (pos >= 0) clRunP<T, W, 8>(g, b, vec, d, e, a, s, gmask); }  // group-uniform
+                else if (pos >= 0) clRunP<T, W, 1>(g, b, vec, d, e, a, s, 0u);
+            } else {
+                if (cls == 0) clRun<T, W, 32>(g, b, vec, d, a, s, 0xffffffffu);
+                else if (cls == 1) { if (pos >= 0) clRun<T, W, 8>(g, b, vec, d, a, s, gmask); }
+                else if (pos >= 0) clRun<T, W, 1>(g, b, vec, d, a, s, 0u);
+            }
         }
         __syncwarp();  // the barrier below is .aligned: every warp arrives converged
         clusterArrive();
-        // static data only, safe before the acquire: the next phase's first pairs, the phase after's descriptor
+        // static data only, safe before the acquire: the next phase's first pairs, the phase after's descriptors
         clsCur = clsNext;
         posCur = posNext;
         dCur = dNext;
-        if (posCur >= 0) clPairsOf<W>(g, clsCur, dCur, aCur);
-        firstOf(k + 2, clsNext, posNext, dNext);
+        eCur = eNext;
+        if (posCur >= 0) loadPairs(clsCur, dCur, aCur);
+        firstOf(k + 2, clsNext, posNext, dNext, eNext);
         clusterWait();
     }
 }
@@ -265,7 +457,7 @@ __global__ void __launch_bounds__(kClusterThreads) k_tail_cluster(DevGrid g, Dev
 inline size_t ClusterSmemBytes(int nLevels) { return (size_t)2 * nLevels * sizeof(int4); }
 
 // Launch a walk of levels [l0, l1) for the nActive listed systems of b, one cluster of C CTAs per system.
-template <typename T, int W, int C>
+template <typename T, int W, int C, bool PK>
 cudaError_t LaunchTailClusterC(const DevGrid& g, const DevBatch& b, T* vec, int l0, int l1, int nActive, cudaStream_t st) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(nActive * C);
@@ -279,16 +471,23 @@ cudaError_t LaunchTailClusterC(const DevGrid& g, const DevBatch& b, T* vec, int 
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_tail_cluster<T, W, C>, g, b, vec, l0, l1);
+    return cudaLaunchKernelEx(&cfg, k_tail_cluster<T, W, C, PK>, g, b, vec, l0, l1);
 }
-template <typename T, int W>
-cudaError_t LaunchTailCluster(const DevGrid& g, const DevBatch& b, T* vec, int l0, int l1, int nActive, cudaStream_t st) {
+template <typename T, int W, bool PK>
+cudaError_t LaunchTailClusterK(const DevGrid& g, const DevBatch& b, T* vec, int l0, int l1, int nActive, cudaStream_t st) {
     switch (ClusterCtasFor(nActive)) {
-        case 8: return LaunchTailClusterC<T, W, 8>(g, b, vec, l0, l1, nActive, st);
-        case 4: return LaunchTailClusterC<T, W, 4>(g, b, vec, l0, l1, nActive, st);
-        case 2: return LaunchTailClusterC<T, W, 2>(g, b, vec, l0, l1, nActive, st);
-        default: return LaunchTailClusterC<T, W, 1>(g, b, vec, l0, l1, nActive, st);
+        case 8: return LaunchTailClusterC<T, W, 8, PK>(g, b, vec, l0, l1, nActive, st);
+        case 4: return LaunchTailClusterC<T, W, 4, PK>(g, b, vec, l0, l1, nActive, st);
+        case 2: return LaunchTailClusterC<T, W, 2, PK>(g, b, vec, l0, l1, nActive, st);
+        default: return LaunchTailClusterC<T, W, 1, PK>(g, b, vec, l0, l1, nActive, st);
     }
+}
+// Levels [l0, l1) of the paired schedule (paired) or of the scalar one.
+template <typename T, int W>
+cudaError_t LaunchTailCluster(const DevGrid& g, const DevBatch& b, T* vec, int l0, int l1, int nActive, cudaStream_t st,
+                              bool paired) {
+    return paired ? LaunchTailClusterK<T, W, true>(g, b, vec, l0, l1, nActive, st)
+                  : LaunchTailClusterK<T, W, false>(g, b, vec, l0, l1, nActive, st);
 }
 
 }  // namespace gs

@@ -1258,18 +1258,19 @@ namespace gs {
 // per-level launches over the batch, the levels above as one CTA per system.
 template <typename T>
 int64_t FewSystemsSolve(const DevGrid& g, const DevBatch& b, const Symbolic& s, int nActive, int lt, bool refine,
-                        cudaStream_t st, cudaEvent_t afterFactor, bool cluster = false) {
+                        cudaStream_t st, cudaEvent_t afterFactor, bool cluster = false, bool paired = false) {
     int64_t launches = 0;
-    if (cluster && nActive <= kClusterMaxSystems && ClusterSmemBytes(s.nLevels) <= kClusterSmemMax) {
-        const int L = s.nLevels;
-        LaunchTailCluster<T, kWorkFactor>(g, b, (T*)b.y, 0, L, nActive, st);
+    const bool pk = paired && g.psLevels > 0;
+    const int Lc = pk ? g.psLevels : s.nLevels;
+    if (cluster && nActive <= kClusterMaxSystems && ClusterSmemBytes(Lc) <= kClusterSmemMax) {
+        LaunchTailCluster<T, kWorkFactor>(g, b, (T*)b.y, 0, Lc, nActive, st, pk);
         if (afterFactor) cudaEventRecord(afterFactor, st);
-        LaunchTailCluster<T, kWorkBackward>(g, b, (T*)b.y, 0, L, nActive, st);
+        LaunchTailCluster<T, kWorkBackward>(g, b, (T*)b.y, 0, Lc, nActive, st, pk);
         launches += 2;
         if (refine) {
             k_residual<T><<<dim3((s.n + 7) / 8, (nActive + 31) / 32), dim3(32, 8), 0, st>>>(g, b, b.activeList, nActive);
-            LaunchTailCluster<T, kWorkForward>(g, b, (T*)b.z, 0, L, nActive, st);
-            LaunchTailCluster<T, kWorkBackward>(g, b, (T*)b.z, 0, L, nActive, st);
+            LaunchTailCluster<T, kWorkForward>(g, b, (T*)b.z, 0, Lc, nActive, st, pk);
+            LaunchTailCluster<T, kWorkBackward>(g, b, (T*)b.z, 0, Lc, nActive, st, pk);
             launches += 3;
         }
         return launches;
@@ -2267,7 +2268,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             cudaMemsetAsync(cur.activeCount, 0, sizeof(int), st);
             k_collect_active<<<(cur.count + 255) / 256, 256, 0, st>>>(cur);
             launches += 1 + FewSystemsSolve<double>(g, cur, s, nActive, G->tailSplit, false, st, timed ? ev[2] : nullptr,
-                                                    ctx->clusterOk);
+                                                    ctx->clusterOk, G->paired);
             if (timed) cudaEventRecord(ev[3], st);
             {
                 const int grp = (nActive + 31) / 32;
@@ -3780,19 +3781,22 @@ bool ClusterWalkAvailable() {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int n = 0;
-#define GS_CLUSTER_KERNELS(C)                                                                                    \
-    (const void*)k_tail_cluster<double, kWorkFactor, C>, (const void*)k_tail_cluster<double, kWorkBackward, C>,     \
-        (const void*)k_tail_cluster<double, kWorkForward, C>, (const void*)k_tail_cluster<float, kWorkFactor, C>,   \
-        (const void*)k_tail_cluster<float, kWorkBackward, C>, (const void*)k_tail_cluster<float, kWorkForward, C>
-    for (const void* f : {GS_CLUSTER_KERNELS(1), GS_CLUSTER_KERNELS(2), GS_CLUSTER_KERNELS(4), GS_CLUSTER_KERNELS(8)})
+#define GS_CLUSTER_KERNELS(C, PK)                                                                                  \
+    (const void*)k_tail_cluster<double, kWorkFactor, C, PK>, (const void*)k_tail_cluster<double, kWorkBackward, C, PK>, \
+        (const void*)k_tail_cluster<double, kWorkForward, C, PK>, (const void*)k_tail_cluster<float, kWorkFactor, C, PK>, \
+        (const void*)k_tail_cluster<float, kWorkBackward, C, PK>, (const void*)k_tail_cluster<float, kWorkForward, C, PK>
+    for (const void* f : {GS_CLUSTER_KERNELS(1, false), GS_CLUSTER_KERNELS(2, false), GS_CLUSTER_KERNELS(4, false),
+                          GS_CLUSTER_KERNELS(8, false), GS_CLUSTER_KERNELS(1, true), GS_CLUSTER_KERNELS(2, true),
+                          GS_CLUSTER_KERNELS(4, true), GS_CLUSTER_KERNELS(8, true)})
         if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClusterSmemMax) != cudaSuccess) {
             cudaGetLastError();
             return false;
         }
 #undef GS_CLUSTER_KERNELS
     // the largest cluster must fit (the smaller ones then do)
-    for (const void* f : {(const void*)k_tail_cluster<double, kWorkFactor, kClusterCtas>,
-                          (const void*)k_tail_cluster<float, kWorkFactor, kClusterCtas>})
+    for (const void* f : {(const void*)k_tail_cluster<double, kWorkFactor, kClusterCtas, false>,
+                          (const void*)k_tail_cluster<double, kWorkFactor, kClusterCtas, true>,
+                          (const void*)k_tail_cluster<float, kWorkFactor, kClusterCtas, true>})
         if (cudaOccupancyMaxActiveClusters(&n, f, &cfg) != cudaSuccess || n < 1) {
             cudaGetLastError();
             return false;
