@@ -61,8 +61,8 @@ __device__ __forceinline__ int unitCount(const int4 P) {
 
 // This lane's first round of index pairs of piece d for a group of G lanes: (LU slot, right-hand-side index) for
 // factorisation and forward entries, (U slot, row) for a backward node; x = -1 past the end.
-template <int W, int G>
-__device__ __forceinline__ void clPairs(const DevGrid& g, const int4 d, int2 (&a)[kClusterInFlight]) {
+template <int W, int G, int UF>
+__device__ __forceinline__ void clPairs(const DevGrid& g, const int4 d, int2 (&a)[UF]) {
     const int j = G == 1 ? 0 : (int)(threadIdx.x & (G - 1));
     if (W == kWorkBackward) {
         const int c = d.z, base = d.y;  // LU slots fit 32 bits (checked by the symbolic analysis)
@@ -80,19 +80,19 @@ __device__ __forceinline__ void clPairs(const DevGrid& g, const int4 d, int2 (&a
         }
     }
 }
-template <int W>
-__device__ __forceinline__ void clPairsOf(const DevGrid& g, int cls, const int4 d, int2 (&a)[kClusterInFlight]) {
-    if (cls == 0) clPairs<W, 32>(g, d, a);
-    else if (cls == 1) clPairs<W, 8>(g, d, a);
-    else clPairs<W, 1>(g, d, a);
+template <int W, int UF>
+__device__ __forceinline__ void clPairsOf(const DevGrid& g, int cls, const int4 d, int2 (&a)[UF]) {
+    if (cls == 0) clPairs<W, 32, UF>(g, d, a);
+    else if (cls == 1) clPairs<W, 8, UF>(g, d, a);
+    else clPairs<W, 1, UF>(g, d, a);
 }
 
 // One piece by a group of G lanes (G = 32, 8 or 1) from its loaded first round; the group's first lane writes. Lane j
 // of the group takes pairs j, j + G, ..., kClusterInFlight in flight per round, then a fixed butterfly over the group.
-template <typename T, int W, int G>
+template <typename T, int W, int G, int UF>
 __device__ __forceinline__ void clRun(const DevGrid& g, const DevBatch& b, T* vec, const int4 d,
-                                      const int2 (&a0)[kClusterInFlight], int s, unsigned mask) {
-    constexpr int U = kClusterInFlight;
+                                      const int2 (&a0)[UF], int s, unsigned mask) {
+    constexpr int U = UF;
     const size_t B = (size_t)b.B;
     T* lu = (T*)b.lu;
     T* piv = (T*)b.piv;
@@ -182,8 +182,8 @@ __device__ __forceinline__ void clRun(const DevGrid& g, const DevBatch& b, T* ve
 
 // This lane's first round of a paired task's index pairs: (a, c) of a factorisation or forward task, (t, row) of a
 // backward task (row r = pRows[A.x + t]); x = -1 past the end.
-template <int W, int G>
-__device__ __forceinline__ void clPairsP(const DevGrid& g, const int4 A, int2 (&a)[kClusterInFlight]) {
+template <int W, int G, int UF>
+__device__ __forceinline__ void clPairsP(const DevGrid& g, const int4 A, int2 (&a)[UF]) {
     const int j = G == 1 ? 0 : (int)(threadIdx.x & (G - 1));
     if (W == kWorkBackward) {
         const int c = A.y - A.x;
@@ -201,42 +201,59 @@ __device__ __forceinline__ void clPairsP(const DevGrid& g, const int4 A, int2 (&
         }
     }
 }
-template <int W>
-__device__ __forceinline__ void clPairsPOf(const DevGrid& g, int cls, const int4 A, int2 (&a)[kClusterInFlight]) {
-    if (cls == 0) clPairsP<W, 32>(g, A, a);
-    else if (cls == 1) clPairsP<W, 8>(g, A, a);
-    else clPairsP<W, 1>(g, A, a);
+template <int W, int UF>
+__device__ __forceinline__ void clPairsPOf(const DevGrid& g, int cls, const int4 A, int2 (&a)[UF]) {
+    if (cls == 0) clPairsP<W, 32, UF>(g, A, a);
+    else if (cls == 1) clPairsP<W, 8, UF>(g, A, a);
+    else clPairsP<W, 1, UF>(g, A, a);
 }
 
-// the K products of one index pair of a paired task (backward: U(k, r) from s0 + t, U(k + 1, r) from s1 + t, times x(r))
-template <typename T, int W>
-__device__ __forceinline__ void clAccP(const T* lu, const T* R, int K, int s0, int s1, int2 p, size_t B, int s, T (&acc)[4]) {
-    if (p.x < 0) return;
-    if (W == kWorkBackward) {
-        const T xr = ldL2(R + (size_t)p.y * B + s);
-        acc[0] += ldL2(lu + (size_t)(s0 + p.x) * B + s) * xr;
-        if (K == 2) acc[1] += ldL2(lu + (size_t)(s1 + p.x) * B + s) * xr;
-        return;
+// The K products of a round of U index pairs of a paired task, added to acc: every operand of the round is loaded
+// (predicated, not branched) before the first product, so the round's loads are in flight together. Backward pairs
+// are (t, row): U(k, r) from s0 + t, U(k + 1, r) from s1 + t, times x(r).
+template <typename T, int W, int K, int UF>
+__device__ __forceinline__ void clRoundP(const T* lu, const T* R, int s0, int s1, const int2 (&p)[UF],
+                                         size_t B, int s, T (&acc)[4]) {
+    constexpr int U = UF;
+    T l0[U], l1[U], r0[U], r1[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        const bool ok = p[u].x >= 0;
+        if (W == kWorkBackward) {
+            r0[u] = ok ? ldL2(R + (size_t)p[u].y * B + s) : T(0);
+            l0[u] = ok ? ldL2(lu + (size_t)(s0 + p[u].x) * B + s) : T(0);
+            l1[u] = (ok && K == 2) ? ldL2(lu + (size_t)(s1 + p[u].x) * B + s) : T(0);
+            r1[u] = T(0);
+        } else {
+            l0[u] = ok ? ldL2(lu + (size_t)p[u].x * B + s) : T(0);
+            r0[u] = ok ? ldL2(R + (size_t)p[u].y * B + s) : T(0);
+            l1[u] = (ok && (K == 2 || K == 4)) ? ldL2(lu + (size_t)(p[u].x + 1) * B + s) : T(0);
+            r1[u] = (ok && (K == 3 || K == 4)) ? ldL2(R + (size_t)(p[u].y + 1) * B + s) : T(0);
+        }
     }
-    const T l0 = ldL2(lu + (size_t)p.x * B + s), r0 = ldL2(R + (size_t)p.y * B + s);
-    acc[0] += l0 * r0;
-    if (K == 2) {
-        acc[1] += ldL2(lu + (size_t)(p.x + 1) * B + s) * r0;
-    } else if (K == 3) {
-        acc[1] += l0 * ldL2(R + (size_t)(p.y + 1) * B + s);
-    } else if (K == 4) {
-        const T l1 = ldL2(lu + (size_t)(p.x + 1) * B + s), r1 = ldL2(R + (size_t)(p.y + 1) * B + s);
-        acc[1] += l0 * r1;
-        acc[2] += l1 * r0;
-        acc[3] += l1 * r1;
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        acc[0] += l0[u] * r0[u];
+        if (W == kWorkBackward) { if (K == 2) acc[1] += l1[u] * r0[u]; continue; }
+        if (K == 2) acc[1] += l1[u] * r0[u];
+        if (K == 3) acc[1] += l0[u] * r1[u];
+        if (K == 4) { acc[1] += l0[u] * r1[u]; acc[2] += l1[u] * r0[u]; acc[3] += l1[u] * r1[u]; }
     }
+}
+template <typename T, int W, int UF>
+__device__ __forceinline__ void clRoundPK(int K, const T* lu, const T* R, int s0, int s1, const int2 (&p)[UF],
+                                          size_t B, int s, T (&acc)[4]) {
+    if (K == 1) clRoundP<T, W, 1, UF>(lu, R, s0, s1, p, B, s, acc);
+    else if (K == 2) clRoundP<T, W, 2, UF>(lu, R, s0, s1, p, B, s, acc);
+    else if (K == 3) clRoundP<T, W, 3, UF>(lu, R, s0, s1, p, B, s, acc);
+    else clRoundP<T, W, 4, UF>(lu, R, s0, s1, p, B, s, acc);
 }
 
 // One paired task by a group of G lanes from its loaded first round; the group's first lane writes its outputs.
-template <typename T, int W, int G>
+template <typename T, int W, int G, int UF>
 __device__ __forceinline__ void clRunP(const DevGrid& g, const DevBatch& b, T* vec, const int4 A, const int4 D,
-                                       const int2 (&a0)[kClusterInFlight], int s, unsigned mask) {
-    constexpr int U = kClusterInFlight;
+                                       const int2 (&a0)[UF], int s, unsigned mask) {
+    constexpr int U = UF;
     const size_t B = (size_t)b.B;
     T* lu = (T*)b.lu;
     T* piv = (T*)b.piv;
@@ -277,8 +294,7 @@ __device__ __forceinline__ void clRunP(const DevGrid& g, const DevBatch& b, T* v
         }
     }
     T acc[4] = {T(0), T(0), T(0), T(0)};
-#pragma unroll
-    for (int u = 0; u < U; u++) clAccP<T, W>(lu, R, K, s0, s1, a0[u], B, s, acc);
+    clRoundPK<T, W, UF>(K, lu, R, s0, s1, a0, B, s, acc);
     const int len = A.y - A.x;
     for (int off = U * G; off < len; off += U * G) {
         int2 a[U];
@@ -295,8 +311,7 @@ __device__ __forceinline__ void clRunP(const DevGrid& g, const DevBatch& b, T* v
                 a[u] = q < A.y ? __ldg(g.psPairs + q) : make_int2(-1, -1);
             }
         }
-#pragma unroll
-        for (int u = 0; u < U; u++) clAccP<T, W>(lu, R, K, s0, s1, a[u], B, s, acc);
+        clRoundPK<T, W, UF>(K, lu, R, s0, s1, a, B, s, acc);
     }
 #pragma unroll
     for (int i = 0; i < 4; i++)
@@ -361,6 +376,9 @@ __device__ __forceinline__ int clusterRank() {
 template <typename T, int W, int C, bool PK>
 __global__ void __launch_bounds__(kClusterThreads) k_tail_cluster(DevGrid g, DevBatch b, T* vec, int l0, int l1) {
     constexpr int kClusterWarps = C * kClusterThreads / 32;
+    // pairs in flight per lane: the paired schedule's products take up to four operands a pair, so it keeps four (its
+    // pieces of more than four pairs go to 8-lane groups)
+    constexpr int UF = PK ? 4 : kClusterInFlight;
     extern __shared__ int4 clPhase[];
     const int s = b.activeList[blockIdx.x / C];
     // uniform over the cluster: every CTA of it returns, or none does (no CTA may miss a cluster barrier)
@@ -386,15 +404,15 @@ __global__ void __launch_bounds__(kClusterThreads) k_tail_cluster(DevGrid g, Dev
     const int lane = threadIdx.x & 31;
     const int gw = clusterRank() * (kClusterThreads / 32) + (int)(threadIdx.x >> 5);  // warp of the cluster
     const unsigned gmask = 0xFFu << (lane & 24);
-    auto loadPairs = [&](int cls, const int4 d, int2 (&a)[kClusterInFlight]) {
-        if (PK) clPairsPOf<W>(g, cls, d, a);
-        else clPairsOf<W>(g, cls, d, a);
+    auto loadPairs = [&](int cls, const int4 d, int2 (&a)[UF]) {
+        if (PK) clPairsPOf<W, UF>(g, cls, d, a);
+        else clPairsOf<W, UF>(g, cls, d, a);
     };
     // the first unit of this warp two phases deep: its descriptors for phase k + 1, its descriptors and pairs for k
     int clsCur = -1, posCur = -1, clsNext = -1, posNext = -1;
     int4 dCur = make_int4(0, 0, 0, 0), dNext = make_int4(0, 0, 0, 0);
     int4 eCur = make_int4(0, 0, 0, 0), eNext = make_int4(0, 0, 0, 0);
-    int2 aCur[kClusterInFlight];
+    int2 aCur[UF];
     auto firstOf = [&](int k, int& cls, int& pos, int4& d, int4& e) {
         cls = -1;
         pos = -1;
@@ -415,14 +433,14 @@ __global__ void __launch_bounds__(kClusterThreads) k_tail_cluster(DevGrid g, Dev
         for (int u = gw; u < nu; u += kClusterWarps) {
             int cls, pos;
             int4 d, e = make_int4(0, 0, 0, 0);
-            int2 a[kClusterInFlight];
+            int2 a[UF];
             if (u == gw) {
                 cls = clsCur;
                 pos = posCur;
                 d = dCur;
                 e = eCur;
 #pragma unroll
-                for (int q = 0; q < kClusterInFlight; q++) a[q] = aCur[q];
+                for (int q = 0; q < UF; q++) a[q] = aCur[q];
             } else {
                 pos = unitPiece(P, u, lane, cls);
                 if (pos >= 0) {
@@ -432,13 +450,13 @@ __global__ void __launch_bounds__(kClusterThreads) k_tail_cluster(DevGrid g, Dev
                 }
             }
             if (PK) {
-                if (cls == 0) clRunP<T, W, 32>(g, b, vec, d, e, a, s, 0xffffffffu);          // pos is warp-uniform
-                else if (cls == 1) { if (pos >= 0) clRunP<T, W, 8>(g, b, vec, d, e, a, s, gmask); }  // group-uniform
-                else if (pos >= 0) clRunP<T, W, 1>(g, b, vec, d, e, a, s, 0u);
+                if (cls == 0) clRunP<T, W, 32, UF>(g, b, vec, d, e, a, s, 0xffffffffu);          // pos warp-uniform
+                else if (cls == 1) { if (pos >= 0) clRunP<T, W, 8, UF>(g, b, vec, d, e, a, s, gmask); }  // group-uniform
+                else if (pos >= 0) clRunP<T, W, 1, UF>(g, b, vec, d, e, a, s, 0u);
             } else {
-                if (cls == 0) clRun<T, W, 32>(g, b, vec, d, a, s, 0xffffffffu);
-                else if (cls == 1) { if (pos >= 0) clRun<T, W, 8>(g, b, vec, d, a, s, gmask); }
-                else if (pos >= 0) clRun<T, W, 1>(g, b, vec, d, a, s, 0u);
+                if (cls == 0) clRun<T, W, 32, UF>(g, b, vec, d, a, s, 0xffffffffu);
+                else if (cls == 1) { if (pos >= 0) clRun<T, W, 8, UF>(g, b, vec, d, a, s, gmask); }
+                else if (pos >= 0) clRun<T, W, 1, UF>(g, b, vec, d, a, s, 0u);
             }
         }
         __syncwarp();  // the barrier below is .aligned: every warp arrives converged

@@ -40,17 +40,35 @@ __device__ __forceinline__ void pkAcc(const T* lu, const T* R, int a, int c, siz
 template <typename T, int K>
 __device__ __forceinline__ void pkSumWarp(const T* lu, const T* R, const int2* __restrict__ pr, int q0, int q1, size_t B,
                                           int s, T (&acc)[4]) {
-    constexpr int S = Lay<T>::S, P = Lay<T>::P;
+    // pairs per round: four, two for FP64 with three or four products a pair (the level kernels' register budget)
+    constexpr int S = Lay<T>::S, P = Lay<T>::P, U = (sizeof(T) == 8 && K >= 3) ? 2 : 4;
     const int lane = threadIdx.x & 31, pl = lane / S;
     for (int base = q0; base < q1; base += 32) {
         const int cnt = min(32, q1 - base);
         const int2 mine = lane < cnt ? __ldg(pr + base + lane) : make_int2(0, 0);
-#pragma unroll 4
-        for (int u = 0; u < S; u++) {
-            const int src = pl + P * u;
-            const int a = __shfl_sync(0xffffffffu, mine.x, src);
-            const int c = __shfl_sync(0xffffffffu, mine.y, src);
-            if (src < cnt) pkAcc<T, K>(lu, R, a, c, B, s, acc);
+        // four pairs' operands loaded (predicated, not branched) before any product, so their loads are in flight
+        // together
+#pragma unroll
+        for (int u0 = 0; u0 < S; u0 += U) {
+            T l0[U], l1[U], r0[U], r1[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int src = pl + P * (u0 + u);
+                const int a = __shfl_sync(0xffffffffu, mine.x, src);
+                const int c = __shfl_sync(0xffffffffu, mine.y, src);
+                const bool ok = src < cnt;
+                l0[u] = ok ? lu[(size_t)a * B + s] : T(0);
+                r0[u] = ok ? R[(size_t)c * B + s] : T(0);
+                l1[u] = (ok && (K == 2 || K == 4)) ? lu[(size_t)(a + 1) * B + s] : T(0);
+                r1[u] = (ok && (K == 3 || K == 4)) ? R[(size_t)(c + 1) * B + s] : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                acc[0] += l0[u] * r0[u];
+                if (K == 2) acc[1] += l1[u] * r0[u];
+                if (K == 3) acc[1] += l0[u] * r1[u];
+                if (K == 4) { acc[1] += l0[u] * r1[u]; acc[2] += l1[u] * r0[u]; acc[3] += l1[u] * r1[u]; }
+            }
         }
     }
 #pragma unroll

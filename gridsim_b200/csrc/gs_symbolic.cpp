@@ -400,7 +400,8 @@ std::string FactorSymbolic(Symbolic& s, const std::function<void(const std::func
     // The short pieces of a level are ordered longest first; the one-system walks give those with more than kMid
     // pairs a group of lanes each (levelMid counts them).
     const int kMid = 8;
-    auto pack = [&](Symbolic::Schedule& sc, const std::vector<int32_t>& list, const std::vector<int64_t>& len) {
+    auto pack = [&](Symbolic::Schedule& sc, const std::vector<int32_t>& list, const std::vector<int64_t>& len,
+                    int64_t midAbove) {
         std::vector<std::pair<int64_t, int32_t>> shortLen;
         int wide = 0;
         for (size_t q = 0; q < list.size(); q++) {
@@ -419,7 +420,7 @@ std::string FactorSymbolic(Symbolic& s, const std::function<void(const std::func
         int mid = 0;
         for (auto& pr : shortLen) {
             shortOnes.push_back(pr.second);
-            if (pr.first > kMid) mid++;
+            if (pr.first > midAbove) mid++;
         }
         sc.levelMid.push_back(mid);
         for (size_t q = 0; q < shortOnes.size(); q += kPack) {
@@ -454,10 +455,10 @@ std::string FactorSymbolic(Symbolic& s, const std::function<void(const std::func
             bwd.push_back(q);
             lenBwd.push_back(c);
         }
-        pack(s.factor, phaseA, lenA);
-        pack(s.factor, phaseB, lenB);
-        pack(s.backward, bwd, lenBwd);
-        pack(s.forward, fwd, lenFwd);
+        pack(s.factor, phaseA, lenA, kMid);
+        pack(s.factor, phaseB, lenB, kMid);
+        pack(s.backward, bwd, lenBwd, kMid);
+        pack(s.forward, fwd, lenFwd, kMid);
     }
 
     // ---------------- the paired schedule (Symbolic::PairSchedule) ----------------
@@ -588,10 +589,12 @@ std::string FactorSymbolic(Symbolic& s, const std::function<void(const std::func
                 lenBwd.push_back(c);
                 P.nPaired++;
             }
-            pack(P.factor, phA, lenA);
-            pack(P.factor, phB, lenB);
-            pack(P.backward, bwd, lenBwd);
-            pack(P.forward, fwd, lenFwd);
+            // the cluster walk keeps four pairs in flight a lane on this schedule: pieces above four pairs go to
+            // 8-lane groups
+            pack(P.factor, phA, lenA, 4);
+            pack(P.factor, phB, lenB, 4);
+            pack(P.backward, bwd, lenBwd, 4);
+            pack(P.forward, fwd, lenFwd, 4);
         }
         if (npairs() >= (int64_t)INT32_MAX) return "the paired schedule is too large for 32-bit pair indices";
         P.nUnits = nU;
