@@ -95,10 +95,55 @@ __device__ __forceinline__ void pkSumThread(const T* lu, const T* R, const int2*
     }
 }
 
-template <typename T, int K, bool WIDE>
+// How a task is shared: one lane per system alone (serial), the S lanes of a lane group (its S systems) with the
+// index pairs loaded by the group together, or the whole warp (pair lanes).
+enum PkMode { kPkThread = 0, kPkGroup = 1, kPkWarp = 2 };
+
+// Group mode, for short tasks (at most 32 index pairs) in the latency-bound walks: the group's S lanes load all the
+// pairs in one round (32 / S each), then every lane gathers its own system's operands in rounds of eight pairs that
+// do not depend on each other: two dependent rounds of loads however long the task.
+template <typename T, int K>
+__device__ __forceinline__ void pkSumGroup(const T* lu, const T* R, const int2* __restrict__ pr, int q0, int q1,
+                                           size_t B, int s, T (&acc)[4]) {
+    constexpr int S = Lay<T>::S, KS = 32 / S, RK = 8 / S;  // pair slots per lane; slots per round of eight pairs
+    const int lane = threadIdx.x & 31, gbase = lane & ~(S - 1), j = lane & (S - 1);
+    const unsigned mask = ((1u << S) - 1u) << gbase;
+    const int n = q1 - q0;
+    int2 mine[KS];
+#pragma unroll
+    for (int k = 0; k < KS; k++) mine[k] = j + k * S < n ? __ldg(pr + q0 + j + k * S) : make_int2(0, 0);
+#pragma unroll
+    for (int k0 = 0; k0 < KS; k0 += RK) {
+        if (k0 * S >= n) break;  // uniform over the group
+        T l0[8], l1[8], r0[8], r1[8];
+#pragma unroll
+        for (int kk = 0; kk < RK; kk++)
+#pragma unroll
+            for (int jj = 0; jj < S; jj++) {
+                const int u = kk * S + jj;
+                const int a = __shfl_sync(mask, mine[k0 + kk].x, gbase + jj);
+                const int c = __shfl_sync(mask, mine[k0 + kk].y, gbase + jj);
+                const bool ok = (k0 + kk) * S + jj < n;
+                l0[u] = ok ? lu[(size_t)a * B + s] : T(0);
+                r0[u] = ok ? R[(size_t)c * B + s] : T(0);
+                l1[u] = (ok && (K == 2 || K == 4)) ? lu[(size_t)(a + 1) * B + s] : T(0);
+                r1[u] = (ok && (K == 3 || K == 4)) ? R[(size_t)(c + 1) * B + s] : T(0);
+            }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            acc[0] += l0[u] * r0[u];
+            if (K == 2) acc[1] += l1[u] * r0[u];
+            if (K == 3) acc[1] += l0[u] * r1[u];
+            if (K == 4) { acc[1] += l0[u] * r1[u]; acc[2] += l1[u] * r0[u]; acc[3] += l1[u] * r1[u]; }
+        }
+    }
+}
+
+template <typename T, int K, int M>
 __device__ __forceinline__ void pkSum(const T* lu, const T* R, const int2* pr, int q0, int q1, size_t B, int s,
                                       T (&acc)[4]) {
-    if (WIDE) pkSumWarp<T, K>(lu, R, pr, q0, q1, B, s, acc);
+    if (M == kPkWarp) pkSumWarp<T, K>(lu, R, pr, q0, q1, B, s, acc);
+    else if (M == kPkGroup) pkSumGroup<T, K>(lu, R, pr, q0, q1, B, s, acc);
     else pkSumThread<T, K>(lu, R, pr, q0, q1, B, s, acc);
 }
 
@@ -116,9 +161,10 @@ __device__ __forceinline__ T pkPivot(const DevBatch& b, int s, T a, T v, bool fl
 // One task of the fused factorisation + forward substitution for this lane's system (WIDE: the whole warp, pair
 // lanes; else this lane alone). The values a task combines with its sums (A, pivots, L(k + 1, k), U(k, k + 1)) are
 // loaded before the sums, beside their operands.
-template <typename T, bool WIDE>
+template <typename T, int M>
 __device__ __forceinline__ void pkFactorTask(const DevGrid& g, const DevBatch& b, const int4 A, const int4 D, int s,
                                              bool act) {
+    constexpr bool WIDE = M == kPkWarp;
     const size_t B = (size_t)b.B;
     T* lu = (T*)b.lu;
     T* y = (T*)b.y;
@@ -134,7 +180,7 @@ __device__ __forceinline__ void pkFactorTask(const DevGrid& g, const DevBatch& b
         const int slot = D.x;
         const T a = kind == kFwd ? at(y, slot) : (pkHasA(A, 0) ? at(lu, slot) : T(0));
         const T pv = kind == kLower ? at(piv, k) : T(1);
-        pkSum<T, 1, WIDE>(lu, kind == kFwd ? y : lu, pr, A.x, A.y, B, s, acc);
+        pkSum<T, 1, M>(lu, kind == kFwd ? y : lu, pr, A.x, A.y, B, s, acc);
         T v = a - acc[0];
         if (kind == kDiag) { put(piv, k, pkPivot<T>(b, s, a, v, flag)); return; }
         if (kind == kLower) v = v / pv;
@@ -145,7 +191,7 @@ __device__ __forceinline__ void pkFactorTask(const DevGrid& g, const DevBatch& b
         const int bk = D.x, bk1 = D.y, c = D.z;
         const T a00 = pkHasA(A, 0) ? at(lu, bk) : T(0), a01 = pkHasA(A, 1) ? at(lu, bk + 1) : T(0);
         const T a10 = pkHasA(A, 2) ? at(lu, bk + 2 + c) : T(0), a11 = pkHasA(A, 3) ? at(lu, bk1) : T(0);
-        pkSum<T, 4, WIDE>(lu, lu, pr, A.x, A.y, B, s, acc);
+        pkSum<T, 4, M>(lu, lu, pr, A.x, A.y, B, s, acc);
         const T p0 = pkPivot<T>(b, s, a00, a00 - acc[0], flag);
         const T u01 = a01 - acc[1];
         const T l10 = (a10 - acc[2]) / p0;
@@ -159,7 +205,7 @@ __device__ __forceinline__ void pkFactorTask(const DevGrid& g, const DevBatch& b
     if (kind == kPUpper) {  // U(k, r), U(k + 1, r)
         const T a0 = pkHasA(A, 0) ? at(lu, D.x) : T(0), a1 = pkHasA(A, 1) ? at(lu, D.y) : T(0);
         const T l10 = at(lu, D.z);
-        pkSum<T, 2, WIDE>(lu, lu, pr, A.x, A.y, B, s, acc);
+        pkSum<T, 2, M>(lu, lu, pr, A.x, A.y, B, s, acc);
         const T v0 = a0 - acc[0];
         put(lu, D.x, v0);
         put(lu, D.y, a1 - acc[1] - l10 * v0);
@@ -168,7 +214,7 @@ __device__ __forceinline__ void pkFactorTask(const DevGrid& g, const DevBatch& b
     if (kind == kPLower) {  // L(r, k), L(r, k + 1)
         const T a0 = pkHasA(A, 0) ? at(lu, D.x) : T(0), a1 = pkHasA(A, 1) ? at(lu, D.y) : T(0);
         const T u01 = at(lu, D.z), p0 = at(piv, k), p1 = at(piv, k + 1);
-        pkSum<T, 3, WIDE>(lu, lu, pr, A.x, A.y, B, s, acc);
+        pkSum<T, 3, M>(lu, lu, pr, A.x, A.y, B, s, acc);
         const T v0 = (a0 - acc[0]) / p0;
         put(lu, D.x, v0);
         put(lu, D.y, (a1 - acc[1] - v0 * u01) / p1);
@@ -176,7 +222,7 @@ __device__ __forceinline__ void pkFactorTask(const DevGrid& g, const DevBatch& b
     }
     {  // kPFwd: y(k), y(k + 1)
         const T y0 = at(y, k), y1 = at(y, k + 1), l10 = at(lu, D.z);
-        pkSum<T, 2, WIDE>(lu, y, pr, A.x, A.y, B, s, acc);
+        pkSum<T, 2, M>(lu, y, pr, A.x, A.y, B, s, acc);
         const T v0 = y0 - acc[0];
         put(y, k, v0);
         put(y, k + 1, y1 - acc[1] - l10 * v0);
@@ -184,21 +230,22 @@ __device__ __forceinline__ void pkFactorTask(const DevGrid& g, const DevBatch& b
 }
 
 // forward substitution of a second right-hand side v (the refinement): a single node's forward entry, or a pair's
-template <typename T, bool WIDE>
+template <typename T, int M>
 __device__ __forceinline__ void pkForwardTask(const DevGrid& g, const DevBatch& b, T* v, const int4 A, const int4 D, int s) {
+    constexpr bool WIDE = M == kPkWarp;
     const size_t B = (size_t)b.B;
     const T* lu = (const T*)b.lu;
     const bool writer = !WIDE || (threadIdx.x & 31) < Lay<T>::S;
     T acc[4] = {T(0), T(0), T(0), T(0)};
     if (pkKind(A) == kFwd) {
         const T a = v[(size_t)D.x * B + s];
-        pkSum<T, 1, WIDE>(lu, v, g.psPairs, A.x, A.y, B, s, acc);
+        pkSum<T, 1, M>(lu, v, g.psPairs, A.x, A.y, B, s, acc);
         if (writer) v[(size_t)D.x * B + s] = a - acc[0];
         return;
     }
     const int k = A.w;
     const T y0 = v[(size_t)k * B + s], y1 = v[(size_t)(k + 1) * B + s], l10 = lu[(size_t)D.z * B + s];
-    pkSum<T, 2, WIDE>(lu, v, g.psPairs, A.x, A.y, B, s, acc);
+    pkSum<T, 2, M>(lu, v, g.psPairs, A.x, A.y, B, s, acc);
     const T v0 = y0 - acc[0];
     if (writer) {
         v[(size_t)k * B + s] = v0;
@@ -208,8 +255,9 @@ __device__ __forceinline__ void pkForwardTask(const DevGrid& g, const DevBatch& 
 
 // backward substitution of a unit: x(k) over U(k, r) from s0 + 1 (a single node), or x(k + 1) then x(k) over
 // U(k + 1, r) from s1 and U(k, r) from s0, with U(k, k + 1) at aux (a pair); r over pRows[A.x .. A.y)
-template <typename T, bool WIDE>
+template <typename T, int M>
 __device__ __forceinline__ void pkBackTask(const DevGrid& g, const DevBatch& b, T* x, const int4 A, const int4 D, int s) {
+    constexpr bool WIDE = M == kPkWarp;
     constexpr int S = Lay<T>::S, P = Lay<T>::P;
     const size_t B = (size_t)b.B;
     const T* lu = (const T*)b.lu;
@@ -242,6 +290,34 @@ __device__ __forceinline__ void pkBackTask(const DevGrid& g, const DevBatch& b, 
             a0 += __shfl_xor_sync(0xffffffffu, a0, off);
             a1 += __shfl_xor_sync(0xffffffffu, a1, off);
         }
+    } else if (M == kPkGroup) {  // at most 32 rows: the group loads them together, then every operand at once
+        constexpr int KS = 32 / S, RK = 8 / S;
+        const int lane = threadIdx.x & 31, gbase = lane & ~(S - 1), j = lane & (S - 1);
+        const unsigned mask = ((1u << S) - 1u) << gbase;
+        int mine[KS];
+#pragma unroll
+        for (int kk = 0; kk < KS; kk++) mine[kk] = j + kk * S < c ? __ldg(rows + j + kk * S) : 0;
+#pragma unroll
+        for (int k0 = 0; k0 < KS; k0 += RK) {
+            if (k0 * S >= c) break;  // uniform over the group
+            T xr[8], u0[8], u1[8];
+#pragma unroll
+            for (int kk = 0; kk < RK; kk++)
+#pragma unroll
+                for (int jj = 0; jj < S; jj++) {
+                    const int u = kk * S + jj, t = (k0 + kk) * S + jj;
+                    const int r = __shfl_sync(mask, mine[k0 + kk], gbase + jj);
+                    const bool ok = t < c;
+                    xr[u] = ok ? x[(size_t)r * B + s] : T(0);
+                    u0[u] = ok ? lu[(size_t)(s0 + t) * B + s] : T(0);
+                    u1[u] = (ok && pair) ? lu[(size_t)(s1 + t) * B + s] : T(0);
+                }
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                a0 += u0[u] * xr[u];
+                a1 += u1[u] * xr[u];
+            }
+        }
     } else {
         for (int t = 0; t < c; t++) {
             const T xr = x[(size_t)__ldg(rows + t) * B + s];
@@ -258,23 +334,25 @@ __device__ __forceinline__ void pkBackTask(const DevGrid& g, const DevBatch& b, 
 }
 
 // One work item of the paired schedule W: a wide task by the whole warp, or up to `count` short tasks over the lane
-// groups (the batched layout).
-template <typename T, int W>
+// groups (the batched layout), each by its group in mode SHORT (serial lanes in the wide level launches, where many
+// warps hide the latency; group loads in the latency-bound persistent walks).
+template <typename T, int W, int SHORT>
 __device__ __forceinline__ void pkDoItem(const DevGrid& g, const DevBatch& b, T* vec, int it, int s, bool act) {
     const int* items = W == kWorkFactor ? g.pfItems : (W == kWorkBackward ? g.pbItems : g.pvItems);
     const int4* da = W == kWorkFactor ? g.pfA : (W == kWorkBackward ? g.pbA : g.pvA);
     const int4* db = W == kWorkFactor ? g.pfB : (W == kWorkBackward ? g.pbB : g.pvB);
     const int start = __ldg(items + 2 * it), count = __ldg(items + 2 * it + 1);
-    auto run = [&](int pos, auto wideTag) {
-        constexpr bool WD = decltype(wideTag)::value;
+    auto run = [&](int pos, auto modeTag) {
+        constexpr int MD = decltype(modeTag)::value;
         const int4 A = __ldg(da + pos), D = __ldg(db + pos);
-        if (W == kWorkFactor) pkFactorTask<T, WD>(g, b, A, D, s, act);
-        else if (W == kWorkBackward) pkBackTask<T, WD>(g, b, vec, A, D, s);
-        else pkForwardTask<T, WD>(g, b, vec, A, D, s);
+        if (W == kWorkFactor) pkFactorTask<T, MD>(g, b, A, D, s, act);
+        else if (W == kWorkBackward) pkBackTask<T, MD>(g, b, vec, A, D, s);
+        else pkForwardTask<T, MD>(g, b, vec, A, D, s);
     };
-    if (count < 0) run(start, std::true_type{});
+    if (count < 0) run(start, std::integral_constant<int, kPkWarp>{});
     else
-        for (int p = (threadIdx.x & 31) / Lay<T>::S; p < count; p += Lay<T>::P) run(start + p, std::false_type{});
+        for (int p = (threadIdx.x & 31) / Lay<T>::S; p < count; p += Lay<T>::P)
+            run(start + p, std::integral_constant<int, SHORT>{});
 }
 
 // One level (or phase) of the paired schedule, items [i0, i1): block (32, 4), a warp per item, S systems per warp.
@@ -286,7 +364,7 @@ __global__ void __launch_bounds__(128, 10) k_plevel(DevGrid g, DevBatch b, T* ve
     bool act = s < b.count && b.active[s];
     if (W != kWorkFactor && vec != (T*)b.y) act = act && b.refine[s];
     if (!__any_sync(0xffffffffu, act)) return;
-    pkDoItem<T, W>(g, b, vec, it, s, act);
+    pkDoItem<T, W, kPkThread>(g, b, vec, it, s, act);
 }
 
 // The narrow top of the unit tree: one CTA per system group walks its levels [l0, l1) with block barriers.
@@ -302,7 +380,7 @@ __global__ void __launch_bounds__(32 * kPersistWarps) k_ppersistent(DevGrid g, D
         const int l = W == kWorkBackward ? l1 - 1 - step : l0 + step;
         for (int ph = 0; ph < phases; ph++) {
             const int i0 = ptr[phases * l + ph], i1 = ptr[phases * l + ph + 1];
-            for (int it = i0 + threadIdx.y; it < i1; it += blockDim.y) pkDoItem<T, W>(g, b, vec, it, s, act);
+            for (int it = i0 + threadIdx.y; it < i1; it += blockDim.y) pkDoItem<T, W, kPkGroup>(g, b, vec, it, s, act);
             __syncthreads();
         }
     }
