@@ -44,6 +44,7 @@ class GridDesc(ctypes.Structure):
         ("shift_deg", c_vp), ("rate_a", c_vp), ("br_in_service", c_vp), ("rate_b", c_vp), ("rate_c", c_vp),
         ("n_boundary", c_i32), ("reserved1", c_i32), ("bnd_ptr", c_vp), ("bnd_branch", c_vp), ("bnd_dir", c_vp),
         ("bnd_limit_mw", c_vp),
+        ("zip", c_vp),
     ]
 
 

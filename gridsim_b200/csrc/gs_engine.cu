@@ -55,6 +55,22 @@ __device__ __forceinline__ int sysAt(int idx, const int* list, int nList) {
     return idx < nList ? list[idx] : -1;
 }
 
+// The voltage-dependent (ZIP) load of bus i at vm (ZipLoad, Model/Model.cs:45-63; NewtonShell.ZipDeviationPu :396-402,
+// ZipJacobianDiagPu :407-413): its deviation from the nominal load pd, qd (pu) and the deviation's derivative in vm.
+// False for a constant-power bus.
+__device__ __forceinline__ bool zipLoad(const DevGrid& g, int i, double vm, double pd, double qd, double& dP, double& dQ,
+                                        double& dPdV, double& dQdV) {
+    if (!g.zip) return false;
+    const double* c = g.zip + 6 * (size_t)i;
+    const double ap = c[0], bp = c[1], cp = c[2], aq = c[3], bq = c[4], cq = c[5];
+    if (ap == 0.0 && bp == 0.0 && aq == 0.0 && bq == 0.0) return false;
+    dP = pd * (ap * vm * vm + bp * vm + cp - 1.0);
+    dQ = qd * (aq * vm * vm + bq * vm + cq - 1.0);
+    dPdV = pd * (2.0 * ap * vm + bp);
+    dQdV = qd * (2.0 * aq * vm + bq);
+    return true;
+}
+
 // ---------------------------------------------------------------------------------------------
 // 1. mismatch + Jacobian fill of bus i of system s: injections over row i of Y (the outaged branch's four cells
 //    replaced by their reduced values), the mismatch into the right-hand side (and its FP64 copy in mixed
@@ -105,11 +121,17 @@ __device__ __forceinline__ void busMismatchJac(const DevGrid& g, const DevBatch&
         bad |= (isfinite(H) && isfinite(N) && isfinite(M) && isfinite(L)) ? 0 : 2;
     }
     const double P = vmi * pi, Q = vmi * qi;
+    const double sc = b.loadScale ? b.loadScale[i * B + s] : 1.0;
+    // a ZIP load's deviation comes off the mismatch, its derivative onto the N and L diagonals of a bus with a voltage
+    // column (SparseNewtonRaphsonPowerFlow.cs:223-231, :241-248)
+    double zdP = 0.0, zdQ = 0.0, zdPdV = 0.0, zdQdV = 0.0;
+    const bool zip = zipLoad(g, i, vmi, sc * g.pload[i], sc * g.qload[i], zdP, zdQ, zdPdV, zdQdV);
+    const bool vcol = zip && kq >= 0 && !qId;
     if (fill && pd >= 0) {
         const double H = pId ? 1.0 : -Q - Bd * vmi * vmi;
-        const double N = pId ? 0.0 : P / vmi + Gd * vmi;
+        const double N = pId ? 0.0 : P / vmi + Gd * vmi + (vcol ? zdPdV : 0.0);
         const double M = qId ? 0.0 : P - Gd * vmi * vmi;
-        const double L = qId ? 1.0 : Q / vmi - Bd * vmi;
+        const double L = qId ? 1.0 : Q / vmi - Bd * vmi + (vcol ? zdQdV : 0.0);
         const int4 sl = *reinterpret_cast<const int4*>(g.ySlot + 4 * pd);
         if (sl.x >= 0) lu[sl.x * B + s] = (T)H;
         if (sl.y >= 0) lu[sl.y * B + s] = (T)N;
@@ -118,7 +140,6 @@ __device__ __forceinline__ void busMismatchJac(const DevGrid& g, const DevBatch&
         bad |= (isfinite(H) && isfinite(N) && isfinite(M) && isfinite(L)) ? 0 : 2;
     }
     if (pOut) { pOut[i * B + s] = P; qOut[i * B + s] = Q; }
-    double sc = b.loadScale ? b.loadScale[i * B + s] : 1.0;
     double pspec = b.loadScale ? g.pgen[i] - sc * g.pload[i] : g.pgen[i] - g.pload[i];
     double qspec = b.loadScale ? g.qgen[i] - sc * g.qload[i] : g.qgen[i] - g.qload[i];
     if (b.specBus && b.specBus[s] == i) {  // a generator outage: the bus loses the unit's output
@@ -134,7 +155,7 @@ __device__ __forceinline__ void busMismatchJac(const DevGrid& g, const DevBatch&
         y[kp * B + s] = T(0);
         if (b.rhs64) b.rhs64[kp * B + s] = 0.0;
     } else if (kp >= 0) {
-        const double f = pspec - P;
+        const double f = pspec - P - zdP;
         y[kp * B + s] = (T)f;
         if (b.rhs64) b.rhs64[kp * B + s] = f;
         localMax = fmax(localMax, fabs(f));
@@ -144,7 +165,7 @@ __device__ __forceinline__ void busMismatchJac(const DevGrid& g, const DevBatch&
         y[kq * B + s] = T(0);
         if (b.rhs64) b.rhs64[kq * B + s] = 0.0;
     } else if (kq >= 0) {
-        const double f = qspec - Q;
+        const double f = qspec - Q - zdQ;
         y[kq * B + s] = (T)f;
         if (b.rhs64) b.rhs64[kq * B + s] = f;
         localMax = fmax(localMax, fabs(f));
@@ -303,8 +324,11 @@ __global__ void k_qapply(DevGrid g, DevBatch b) {
         if (g.qlimRevert && tryRevertPin(g, b, i, s, idx)) atomicOr(&b.qState[s], kQChanged);
         return;
     }
-    const double qd = (b.loadScale ? b.loadScale[idx] : 1.0) * g.qload[i];  // the bus's load, pu
-    const double qGen = (b.qinj[idx] + qd) * g.baseMva;
+    const double qd = (b.loadScale ? b.loadScale[idx] : 1.0) * g.qload[i];  // the bus's nominal load, pu
+    // the generators' output: the injection plus the load drawn at the solved voltage (NewtonShell.cs:533-537)
+    double zdP, zdQ = 0.0, zdPdV, zdQdV;
+    zipLoad(g, i, b.vm[idx], 0.0, qd, zdP, zdQ, zdPdV, zdQdV);
+    const double qGen = (b.qinj[idx] + qd + zdQ) * g.baseMva;
     // the aggregate limits of the bus's units (those left after a generator outage)
     const bool spec = b.specBus && b.specBus[s] == i;
     const double qmin = spec ? b.specQmin[s] : g.qminMvar[i], qmax = spec ? b.specQmax[s] : g.qmaxMvar[i];
@@ -666,10 +690,13 @@ __device__ __forceinline__ void busResidual(const DevGrid& g, const DevBatch& b,
     }
     {
         const double P = vmi * pi, Q = vmi * qi;
+        const double sc = b.loadScale ? b.loadScale[i * B + s] : 1.0;
+        double zdP, zdQ, zdPdV = 0.0, zdQdV = 0.0;
+        const bool vcol = zipLoad(g, i, vmi, sc * g.pload[i], sc * g.qload[i], zdP, zdQ, zdPdV, zdQdV) && kq >= 0 && !qId;
         const double H = -Q - Bd * vmi * vmi;
-        const double N = P / vmi + Gd * vmi;
+        const double N = P / vmi + Gd * vmi + (vcol ? zdPdV : 0.0);
         const double M = P - Gd * vmi * vmi;
-        const double L = Q / vmi - Bd * vmi;
+        const double L = Q / vmi - Bd * vmi + (vcol ? zdQdV : 0.0);
         const double dth = kp >= 0 ? (double)dx[kp * B + s] : 0.0;
         const double dv = kq >= 0 ? (double)dx[kq * B + s] : 0.0;
         jp += H * dth + N * dv;
@@ -1758,6 +1785,8 @@ int UploadGrid(gs_grid* G) {
     UP(h.brF, brF); UP(h.brT, brT); UP(rate, rateA); UP(rateB, rateB); UP(rateC, rateC); UP(h.brOn, brOn);
     UP(h.bndPtr, bndPtr); UP(h.bndBranch, bndBranch); UP(h.bndDir, bndDir); UP(h.bndLimit, bndLimit);
     UP(G->pgen, pgen); UP(G->qgen, qgen); UP(G->pload, pload); UP(G->qload, qload);
+    v.zip = nullptr;
+    if (!h.zip.empty()) UP(h.zip, zip);
     {
         std::vector<double> qminPu(n), qmaxPu(n);
         for (int i = 0; i < n; i++) { qminPu[i] = s.qminMvar[i] / h.base; qmaxPu[i] = s.qmaxMvar[i] / h.base; }
@@ -3487,10 +3516,7 @@ int LinearSolve(gs_grid* G, int cnt) {
     };
     const auto& fp = s.factor.levelItemPtr;
     const auto& bp = s.backward.levelItemPtr;
-    // the full-batch step runs the paired schedule (units of one node or a 2 x 2 pair) where the grid has one
-    const bool pairedOn = G->paired && g.psLevels > 0;
-    const int nLv = pairedOn ? g.psLevels : s.nLevels;
-    const int split = pairedOn ? G->psSplit : G->split, splitB = pairedOn ? G->psSplitB : G->splitB;
+    const int split = G->split, splitB = G->splitB;  // the scalar schedule
     for (int l = 0; l < split; l++) {
         level(k_level<T, kWorkFactor>, fp[2 * l], fp[2 * l + 1]);
         level(k_level<T, kWorkFactor>, fp[2 * l + 1], fp[2 * l + 2]);
@@ -3710,6 +3736,8 @@ extern "C" int gs_pf_mismatch_noalloc(gs_grid* G, int32_t count, const double* d
     if (count > kNoAllocMaxSystems)
         return SetErr(ctx, GS_ERR_CAPACITY, "gs_pf_mismatch_noalloc: " + std::to_string(count) +
                                               " systems requested, at most " + std::to_string(kNoAllocMaxSystems));
+    if (!G->host.zip.empty())
+        return SetErr(ctx, GS_ERR_UNSUPPORTED, "gs_pf_mismatch_noalloc: the grid has voltage-dependent (ZIP) loads");
     if (count == 0) return GS_OK;
     GS_CUDA(cudaSetDevice(ctx->device));
     unsigned long long* scratch = nullptr;

@@ -55,6 +55,16 @@ std::string CopyGrid(const gs_grid_desc* d, HostGrid& g) {
     g.rateC.assign(nb, 0.0);
     if (d->rate_b && nb > 0) g.rateB.assign(d->rate_b, d->rate_b + nb);
     if (d->rate_c && nb > 0) g.rateC.assign(d->rate_c, d->rate_c + nb);
+    if (d->zip) {  // kept only when some load varies with voltage (ZipLoad.VariesWithVoltage, Model/Model.cs:49)
+        bool varies = false;
+        for (int i = 0; i < n; i++) {
+            const double* c = d->zip + 6 * (size_t)i;
+            for (int q = 0; q < 6; q++)
+                if (!std::isfinite(c[q])) return "zip coefficients must be finite numbers";
+            varies = varies || c[0] != 0 || c[1] != 0 || c[3] != 0 || c[4] != 0;
+        }
+        if (varies) g.zip.assign(d->zip, d->zip + 6 * (size_t)n);
+    }
     g.brOn.assign(nb, 1);
     if (d->br_in_service && nb > 0) g.brOn.assign(d->br_in_service, d->br_in_service + nb);
     for (int k = 0; k < nb; k++) {

@@ -27,6 +27,8 @@ struct HostGrid {
     int nBnd = 0;
     std::vector<int> bndPtr, bndBranch, bndDir;
     std::vector<double> bndLimit;
+    // voltage-dependent (ZIP) loads: [6 n] Ap Bp Cp Aq Bq Cq per bus, empty when every load is constant power
+    std::vector<double> zip;
 };
 
 // Entry kinds of the fused factor + forward-substitution schedule.

@@ -82,6 +82,7 @@ struct DevGrid {
     const int* bndBranch;
     const int* bndDir;
     const double* bndLimit;
+    const double* zip;    // [6 n] ZIP load coefficients per bus (Ap Bp Cp Aq Bq Cq), null: every load constant power
     const double* pgen;   // generation per bus (pu)
     const double* qgen;
     const double* pload;  // load per bus (pu)

@@ -31,6 +31,43 @@ import numpy as np
 PQ, PV, SLACK = 1, 2, 3
 
 
+# ZipLoad.VariesWithVoltage (Model/Model.cs:49): a load other than pure constant power
+def zip_varies(c) -> bool:
+    return bool(c[0] != 0 or c[1] != 0 or c[3] != 0 or c[4] != 0)
+
+
+ZIP_SUM_TOLERANCE = 1e-9  # JsonGridLoader.ZipSumTolerance (IO/Json/JsonGridLoader.cs:385)
+
+
+def _json_zip(buses) -> Optional[np.ndarray]:
+    """The buses' optional "zip" blocks (JsonGridLoader.ParseZip / ParseZipValues, IO/Json/JsonGridLoader.cs:395-427):
+    all six coefficients present and finite, each triple summing to 1 within 1e-9, else ValueError naming the bus;
+    None when no bus gives one."""
+    if not any(b.get("zip") is not None for b in buses):
+        return None
+    out = np.tile(np.array([0.0, 0.0, 1.0, 0.0, 0.0, 1.0]), (len(buses), 1))
+    for i, b in enumerate(buses):
+        z = b.get("zip")
+        if z is None:
+            continue
+        where = f"buses.json: bus {b['id']}" + (f" ('{b['name']}')" if b.get("name") is not None else "")
+        vals = []
+        for key in ("ap", "bp", "cp", "aq", "bq", "cq"):
+            v = z.get(key)
+            if v is None:
+                raise ValueError(f"{where}: zip is missing coefficient '{key}' (all of ap, bp, cp, aq, bq, cq are required).")
+            v = float(v)
+            if not math.isfinite(v):
+                raise ValueError(f"{where}: zip coefficient '{key}' is {v!r}, which is not a finite number.")
+            vals.append(v)
+        if not abs(sum(vals[:3]) - 1.0) <= ZIP_SUM_TOLERANCE:
+            raise ValueError(f"{where}: zip real-power coefficients ap + bp + cp sum to {sum(vals[:3])!r}, not 1.")
+        if not abs(sum(vals[3:]) - 1.0) <= ZIP_SUM_TOLERANCE:
+            raise ValueError(f"{where}: zip reactive-power coefficients aq + bq + cq sum to {sum(vals[3:])!r}, not 1.")
+        out[i] = vals
+    return out
+
+
 @dataclass
 class GridModel:
     name: str
@@ -81,6 +118,9 @@ class GridModel:
     gen_type: Optional[List[str]] = None
     pf_only: Optional[np.ndarray] = None
     converter: Optional[np.ndarray] = None
+    # voltage-dependent (ZIP) loads (Bus.Zip, Model/Model.cs:33,45-90): [n_bus, 6] Ap Bp Cp Aq Bq Cq, the load drawn at
+    # V pu being Pd (Ap V^2 + Bp V + Cp), Qd (Aq V^2 + Bq V + Cq); None = every load constant power (0, 0, 1)
+    zip: Optional[np.ndarray] = None
     meta: dict = field(default_factory=dict)
     _keep: list = field(default_factory=list, repr=False)
 
@@ -203,6 +243,8 @@ class GridModel:
             d.n_boundary = len(self.boundaries)
             d.bnd_ptr, d.bnd_branch = arr(ptr, np.int32), arr(br, np.int32)
             d.bnd_dir, d.bnd_limit_mw = arr(dr, np.int32), arr(lim, np.float64)
+        if self.zip is not None:
+            d.zip = arr(np.asarray(self.zip, np.float64).reshape(-1), np.float64)
         return d
 
     # ---- JSON round trip of the whole model (golden fixtures) -------------------------------------
@@ -239,7 +281,8 @@ class GridModel:
             mbase=f64("mbase") if "mbase" in d else None, inertia_h=f64("inertia_h") if "inertia_h" in d else None,
             gen_type=list(d["gen_type"]) if "gen_type" in d else None,
             pf_only=u8("pf_only") if "pf_only" in d else None,
-            converter=np.array(d["converter"], np.int8) if "converter" in d else None)
+            converter=np.array(d["converter"], np.int8) if "converter" in d else None,
+            zip=np.array(d["zip"], np.float64).reshape(-1, 6) if "zip" in d else None)
 
 
 # =============================================================================================
@@ -331,6 +374,8 @@ def save_case_dir(m: GridModel, path: str) -> None:
             d["vminPu"] = float(m.vmin[i])
         if not math.isnan(m.vmax[i]):
             d["vmaxPu"] = float(m.vmax[i])
+        if m.zip is not None and zip_varies(m.zip[i]):
+            d["zip"] = dict(zip(("ap", "bp", "cp", "aq", "bq", "cq"), (float(c) for c in m.zip[i])))
         buses.append(d)
     dump("buses.json", buses)
     gens = []
@@ -438,6 +483,7 @@ def load_case_dir(path: str) -> GridModel:
         rate_a=cat(f(lines, "ratingMva") * circ, f(txs, "ratingMva")),
         br_in_service=np.ones(len(lines) + ntx, np.uint8),
         is_transformer=np.array([1 if l.get("isTransformer", False) else 0 for l in lines] + [1] * ntx, np.uint8),
+        zip=_json_zip(buses),
         rate_b=cat(f(lines, "ratingBMva") * circ, f(txs, "ratingBMva") * one),
         rate_c=cat(f(lines, "ratingCMva") * circ, f(txs, "ratingCMva") * one),
         br_name=[l.get("name") or "" for l in lines + txs],

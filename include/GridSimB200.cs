@@ -21,8 +21,8 @@
 // Per-system outcomes never throw: they come back as statuses. A failed call maps GS_ERR_OOM to OutOfMemoryException,
 // GS_ERR_INVALID_ARG to ArgumentException, GS_ERR_UNSUPPORTED to NotSupportedException, GS_ERR_TIMEOUT to
 // TimeoutException and every other code to InvalidOperationException, each with the context's last error text.
-// Models the library does not solve (voltage-dependent ZIP loads, HVDC links) are refused with NotSupportedException
-// before any device call, so a caller can fall back to the CPU engines.
+// Models the library does not solve (HVDC links) are refused with NotSupportedException before any device call, so a
+// caller can fall back to the CPU engines. Voltage-dependent (ZIP) loads are solved on the device.
 
 namespace GridSim.Core.PowerFlow.B200
 {
@@ -39,7 +39,7 @@ namespace GridSim.Core.PowerFlow.B200
     public static unsafe class GsNative
     {
         public const string Lib = "gridsim_b200";
-        public const int GS_ABI_VERSION = 1;
+        public const int GS_ABI_VERSION = 2;
 
         // enum gs_status
         public const int GS_OK = 0, GS_ERR_INVALID_ARG = 1, GS_ERR_CUDA = 2, GS_ERR_OOM = 3, GS_ERR_NO_DEVICE = 4,
@@ -76,6 +76,7 @@ namespace GridSim.Core.PowerFlow.B200
             public IntPtr RateB, RateC;                                                // double*, may be zero
             public int NBoundary, Reserved1;
             public IntPtr BndPtr, BndBranch, BndDir, BndLimitMw;                       // CSR of (branch, +1/-1); MW
+            public IntPtr Zip;                                                         // [6 n_bus] ZIP loads or 0
         }
 
         [StructLayout(LayoutKind.Sequential)]
@@ -348,9 +349,6 @@ namespace GridSim.Core.PowerFlow.B200
         {
             if (model.HasCoupledDevices)
                 throw new NotSupportedException("HVDC links are solved by HvdcCoupling on the CPU engines.");
-            foreach (Bus b in model.Buses)
-                if (b.Zip is { VariesWithVoltage: true })
-                    throw new NotSupportedException($"bus {b.Id} has a voltage-dependent (ZIP) load; the device path solves constant-power loads.");
         }
 
         /// <summary>The grid handle; gs_grid_destroy runs when the model and this wrapper are collected.</summary>
@@ -455,6 +453,21 @@ namespace GridSim.Core.PowerFlow.B200
                     Desc.BndBranch = Pin(member.ToArray());
                     Desc.BndDir = Pin(dir.ToArray());
                     Desc.BndLimitMw = Pin(limit);
+                }
+
+                // voltage-dependent loads (Bus.Zip): six coefficients a bus, constant power (0, 0, 1) where none varies
+                bool anyZip = false;
+                foreach (Bus b in buses) anyZip |= b.Zip is { VariesWithVoltage: true };
+                if (anyZip)
+                {
+                    var zip = new double[6 * n];
+                    for (int i = 0; i < n; i++)
+                    {
+                        ZipLoad z = buses[i].Zip is { VariesWithVoltage: true } v ? v : new ZipLoad();
+                        zip[6 * i] = z.Ap; zip[6 * i + 1] = z.Bp; zip[6 * i + 2] = z.Cp;
+                        zip[6 * i + 3] = z.Aq; zip[6 * i + 4] = z.Bq; zip[6 * i + 5] = z.Cq;
+                    }
+                    Desc.Zip = Pin(zip);
                 }
             }
 

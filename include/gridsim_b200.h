@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define GS_ABI_VERSION 1
+#define GS_ABI_VERSION 2
 
 /* ---- call-level status codes ------------------------------------------------------------ */
 enum gs_status {
@@ -127,6 +127,10 @@ typedef struct gs_grid_desc {
     const int32_t *bnd_branch;      /* [bnd_ptr[n_boundary]] */
     const int32_t *bnd_dir;
     const double *bnd_limit_mw;     /* [n_boundary] */
+    /* voltage-dependent (ZIP) loads (Bus.Zip / ZipLoad, Model/Model.cs:33,45-90): per bus Ap, Bp, Cp, Aq, Bq, Cq; the
+       load drawn at V pu is Pd (Ap V^2 + Bp V + Cp), Qd (Aq V^2 + Bq V + Cq). A bus whose A and B terms are all 0 is
+       constant power; NULL = every load constant power */
+    const double *zip;              /* [6 * n_bus] */
 } gs_grid_desc;
 
 /* ---- options: PowerFlowOptions (src/GridSim.Core/PowerFlow/PowerFlowOptions.cs:15-158) ---- */

@@ -60,6 +60,7 @@ struct Model {
     std::vector<int> genOfDesc; // descriptor unit -> position in gens (-1: out of service)
     std::vector<Br> br;         // GridModel.Branches order
     std::vector<Bnd> bnd;
+    std::vector<double> zip;    // [6 n] Ap Bp Cp Aq Bq Cq per bus (Bus.Zip, Model/Model.cs:33,45-90); empty: none
 };
 
 Model FromDesc(const gs_grid_desc* d) {
@@ -90,6 +91,7 @@ Model FromDesc(const gs_grid_desc* d) {
                         d->rate_a[k], d->br_in_service ? d->br_in_service[k] != 0 : true,
                         d->rate_b ? d->rate_b[k] : 0.0, d->rate_c ? d->rate_c[k] : 0.0});
     }
+    if (d->zip) m.zip.assign(d->zip, d->zip + 6 * (size_t)m.n);
     for (int q = 0; q < d->n_boundary; q++) {
         Bnd b{d->bnd_limit_mw[q], {}};
         for (int e = d->bnd_ptr[q]; e < d->bnd_ptr[q + 1]; e++) b.members.push_back({d->bnd_branch[e], d->bnd_dir[e]});
@@ -607,7 +609,16 @@ bool BiCgStab(const Csr& a, const std::vector<double>& b, std::vector<double>& x
 struct BusSpec {
     std::vector<int> type0;  // 1 PQ, 2 PV, 3 slack
     std::vector<double> vm, va, pspec, qspec, qd, qmin, qmax, vg;
+    // voltage-dependent loads (BuildBusSpec :482): per bus its ZIP coefficients when they vary with voltage
+    // (ZipLoad.VariesWithVoltage), and the nominal load Pd, Qd (MW, MVAr) they scale
+    std::vector<char> hasZip;
+    std::vector<double> zip, pd;
+    bool anyZip = false;
 };
+
+// ZipLoad.PMultiplier / QMultiplier / DPMultiplier / DQMultiplier (Model/Model.cs:51-63)
+inline double ZipMult(const double* c, double v) { return c[0] * v * v + c[1] * v + c[2]; }
+inline double ZipDMult(const double* c, double v) { return 2 * c[0] * v + c[1]; }
 BusSpec BuildBusSpec(const Model& m, bool flatStart) {
     int n = m.n;
     BusSpec s;
@@ -624,7 +635,19 @@ BusSpec BuildBusSpec(const Model& m, bool flatStart) {
     }
     s.type0.resize(n); s.vm.resize(n); s.va.resize(n); s.pspec.resize(n); s.qspec.resize(n);
     s.qd = m.qd;
+    s.pd = m.pd;
     s.vg = vg;
+    s.hasZip.assign(n, 0);
+    s.zip.assign(6 * (size_t)n, 0.0);
+    if (!m.zip.empty())
+        for (int i = 0; i < n; i++) {
+            const double* c = &m.zip[6 * (size_t)i];
+            if (c[0] != 0 || c[1] != 0 || c[3] != 0 || c[4] != 0) {  // VariesWithVoltage
+                s.hasZip[i] = 1;
+                s.anyZip = true;
+                std::copy(c, c + 6, s.zip.begin() + 6 * (size_t)i);
+            }
+        }
     for (int i = 0; i < n; i++) {
         s.type0[i] = (m.type[i] == 2 && !hasGen[i]) ? 1 : m.type[i];
         bool vc = s.type0[i] == 3 || s.type0[i] == 2;
@@ -740,9 +763,14 @@ struct RunEnd {
 };
 
 // RunNewton (:168-265) with NewtonShell.SolveStep (:74-120) and ApplyStep (:128-136).
+// ZIP loads (zs non-null with anyZip): the deviation of each load from its nominal value at the present voltage comes off
+// the mismatch (:223-231, NewtonShell.ZipDeviationPu :396-402), its derivative onto the N and L diagonals of buses
+// with a voltage column (:241-248, NewtonShell.ZipJacobianDiagPu :407-413).
 RunEnd RunNewton(CpuSparseLuSolver& solver, const ComplexCsr& y, const std::vector<int>& type, std::vector<double>& Vm,
                  std::vector<double>& Va, const std::vector<double>& Pspec, const std::vector<double>& Qspec,
-                 std::vector<double>& P, std::vector<double>& Q, const gs_pf_opts& opt) {
+                 std::vector<double>& P, std::vector<double>& Q, const gs_pf_opts& opt, const BusSpec* zs = nullptr,
+                 double base = 100.0) {
+    const bool zip = zs && zs->anyZip;
     int n = y.n;
     std::vector<int> pPos, qPos;
     int m = EquationPositions(type, pPos, qPos);
@@ -758,6 +786,13 @@ RunEnd RunNewton(CpuSparseLuSolver& solver, const ComplexCsr& y, const std::vect
             if (pPos[i] >= 0) f[pPos[i]] = Pspec[i] - P[i];
             if (qPos[i] >= 0) f[qPos[i]] = Qspec[i] - Q[i];
         }
+        if (zip)
+            for (int i = 0; i < n; i++) {
+                if (!zs->hasZip[i]) continue;
+                const double* c = &zs->zip[6 * (size_t)i];
+                if (pPos[i] >= 0) f[pPos[i]] -= zs->pd[i] * (ZipMult(c, Vm[i]) - 1.0) / base;
+                if (qPos[i] >= 0) f[qPos[i]] -= zs->qd[i] * (ZipMult(c + 3, Vm[i]) - 1.0) / base;
+            }
         double maxMis = 0;
         for (int k = 0; k < m; k++) maxMis = std::max(maxMis, std::fabs(f[k]));
         // Math.Max propagates NaN; std::max does not: restate the .NET rule explicitly.
@@ -770,6 +805,13 @@ RunEnd RunNewton(CpuSparseLuSolver& solver, const ComplexCsr& y, const std::vect
         if (maxMis > lim) { r.diverged = true; break; }
         if (iter >= opt.max_iterations) break;
         RefillJacobian(jac, slots, y, Vm, Va, P, Q);
+        if (zip)
+            for (int i = 0; i < n; i++) {
+                if (qPos[i] < 0 || !zs->hasZip[i]) continue;
+                const double* c = &zs->zip[6 * (size_t)i];
+                if (pPos[i] >= 0) jac.val[Locate(jac, pPos[i], qPos[i])] += zs->pd[i] * ZipDMult(c, Vm[i]) / base;
+                jac.val[Locate(jac, qPos[i], qPos[i])] += zs->qd[i] * ZipDMult(c + 3, Vm[i]) / base;
+            }
         bool ok = true;
         for (double v : jac.val) if (!std::isfinite(v)) { ok = false; break; }
         if (ok) for (double v : f) if (!std::isfinite(v)) { ok = false; break; }
@@ -816,7 +858,8 @@ bool TryRevertPin(int i, std::vector<int>& eff, std::vector<double>& vm, const s
     return true;
 }
 
-// NewtonShell.ApplyQLimits (:519-558), constant-power loads, revert off by default.
+// NewtonShell.ApplyQLimits (:519-558), revert off by default; the generators' output is the net injection plus the
+// load drawn at the solved voltage (LoadAtVoltage.QMvar, :533-537 and PowerFlow/LoadAtVoltage.cs:29-30).
 bool ApplyQLimits(const BusSpec& s, std::vector<int>& eff, const std::vector<double>& Q, std::vector<double>& qspec,
                   double base, std::vector<double>& vm, std::vector<int>& pinned, std::vector<int>& revertCount,
                   bool revert) {
@@ -824,7 +867,7 @@ bool ApplyQLimits(const BusSpec& s, std::vector<int>& eff, const std::vector<dou
     for (size_t i = 0; i < eff.size(); i++) {
         if (s.type0[i] != 2) continue;
         if (eff[i] == 2) {
-            double qGen = Q[i] * base + s.qd[i];
+            double qGen = Q[i] * base + (s.hasZip[i] ? s.qd[i] * ZipMult(&s.zip[6 * i + 3], vm[i]) : s.qd[i]);
             if (qGen > s.qmax[i] + kQLimitTolMva) {
                 eff[i] = 1;
                 qspec[i] = (s.qmax[i] - s.qd[i]) / base;
@@ -983,7 +1026,7 @@ SolveOut SolveModel(const Model& m, int skip, const gs_pf_opts& opt, const doubl
     bool switchPending = false;
     for (int qp = 0; qp < qPasses; qp++) {
         switchPending = false;
-        re = RunNewton(solver, y, eff, Vm, Va, s.pspec, qspec, P, Q, opt);
+        re = RunNewton(solver, y, eff, Vm, Va, s.pspec, qspec, P, Q, opt, &s, m.base);
         converged = re.converged;
         total += re.iters;
         if (!opt.enforce_q_limits) break;
@@ -994,7 +1037,7 @@ SolveOut SolveModel(const Model& m, int skip, const gs_pf_opts& opt, const doubl
         if (!changed) break;
     }
     if (switchPending) {
-        re = RunNewton(solver, y, eff, Vm, Va, s.pspec, qspec, P, Q, opt);
+        re = RunNewton(solver, y, eff, Vm, Va, s.pspec, qspec, P, Q, opt, &s, m.base);
         total += re.iters;
         converged = false;
     }
@@ -1244,6 +1287,7 @@ Reduced ReduceForElement(const Model& m, int kind, int index) {
             r.busOf[i] = j++;
             red.id.push_back(r.m.id[i]); red.type.push_back(r.m.type[i]);
             red.pd.push_back(m.pd[i]); red.qd.push_back(m.qd[i]); red.gs.push_back(m.gs[i]); red.bs.push_back(m.bs[i]);
+            if (!m.zip.empty()) red.zip.insert(red.zip.end(), m.zip.begin() + 6 * i, m.zip.begin() + 6 * i + 6);
             red.vm.push_back(m.vm[i]); red.vaDeg.push_back(m.vaDeg[i]);
             red.vmin.push_back(m.vmin[i]); red.vmax.push_back(m.vmax[i]);
         }
@@ -1438,8 +1482,11 @@ int gso_max_mismatch(const gs_grid_desc* d, int32_t count, const int32_t* outage
         double mx = 0.0;
         bool finite = true;
         for (int i = 0; i < n; i++) {
-            if (pPos[i] >= 0) { double f = s.pspec[i] - P[i]; finite = finite && std::isfinite(f); mx = std::max(mx, std::fabs(f)); }
-            if (qPos[i] >= 0) { double f = s.qspec[i] - Q[i]; finite = finite && std::isfinite(f); mx = std::max(mx, std::fabs(f)); }
+            const double* z = &s.zip[6 * (size_t)i];
+            const double dP = s.hasZip[i] ? s.pd[i] * (ZipMult(z, V[i]) - 1.0) / mdl.base : 0.0;
+            const double dQ = s.hasZip[i] ? s.qd[i] * (ZipMult(z + 3, V[i]) - 1.0) / mdl.base : 0.0;
+            if (pPos[i] >= 0) { double f = s.pspec[i] - P[i] - dP; finite = finite && std::isfinite(f); mx = std::max(mx, std::fabs(f)); }
+            if (qPos[i] >= 0) { double f = s.qspec[i] - Q[i] - dQ; finite = finite && std::isfinite(f); mx = std::max(mx, std::fabs(f)); }
         }
         out[c] = finite ? mx : NAN;
     }

@@ -53,7 +53,7 @@ def test_struct_layouts_match_the_header(tmp_path):
 
 def test_status_strings_and_defaults():
     lib = _abi.load_library()
-    assert lib.gs_abi_version() == 1
+    assert lib.gs_abi_version() == 2
     assert lib.gs_status_str(_abi.GS_ERR_OOM) == b"out of device memory"
     o = _abi.PfOpts()
     lib.gs_pf_opts_default(ctypes.byref(o))
