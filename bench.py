@@ -5,9 +5,11 @@ iterations, per-bus voltage limits), mixed precision (FP32 LU and triangular sol
 update and residual refinement). The plain FP64 batched GPU solve of the same screen is reported beside
 it (`fp64_value`).
 
-A step is one complete screen of the outage set on one GPU. With --gpus N (torchrun, one process per
-GPU) every rank screens its own 5,000 outages of the same grid (weak scaling; no collective on the data
-path); the step time is the max over ranks.
+A step is one complete screen of the outage set through the sharded screen (gridsim_b200.parallel.screen_sharded).
+With --gpus N (torchrun, one process per GPU) the outage list is N sampled sets of 5,000 (N x 5,000 rows, seeds
+0..N-1), dealt to the ranks by estimated cost (outage_costs / balanced_shards: about 5,000 per rank, weak
+scaling), screened on each rank's GPU and all-gathered back into row order on every rank (no collective on the
+data path); the device step time is the max over ranks, and `e2e` includes the gather and the merge.
 
 `--impl reference` times the oracle (the C++ restatement of the reference's FP64 sparse
 Gilbert-Peierls Newton-Raphson screen, one outage per host thread) on a bounded sample of the same
@@ -86,13 +88,16 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def workload(rank=0, outages=N_OUTAGES):
-    """The 10,000-bus grid and its sampled outage set; `outages` < 5,000 takes the first ones of that set (the
-    small cases the committed profiles are captured on)."""
+def workload(rank=0, outages=N_OUTAGES, world=1):
+    """The 10,000-bus grid and the outage rows of the whole job: `world` sampled sets of 5,000 non-islanding
+    outages (seeds 0..world-1) one after the other; `outages` < 5,000 takes the first ones of each set (the small
+    cases the committed profiles are captured on). `rank` is unused (every rank holds the whole list and screens
+    its cost-balanced shard of it)."""
     from gridsim_b200 import synthetic
+    del rank
     m = synthetic.config_grid(2, GRID_SEED)
-    idx = synthetic.outage_set(m, N_OUTAGES, GRID_SEED + rank)
-    return m, idx[:outages]
+    idx = np.concatenate([synthetic.outage_set(m, N_OUTAGES, GRID_SEED + r)[:outages] for r in range(world)])
+    return m, idx.astype(np.int32)
 
 
 def options(precision, timing=False):
@@ -331,7 +336,11 @@ def run_ours(args):
         dist_.init_process_group("nccl", timeout=timedelta(seconds=120))
         dist = dist_
     ctx = CudaContext(local)
-    m, idx = workload(rank, args.outages)
+    from gridsim_b200.parallel import balanced_shards, outage_costs, screen_sharded
+    m, rows = workload(rank, args.outages, world)
+    costs = outage_costs(m, rows) if world > 1 else None
+    # this rank's shard (what its GPU screens); the accuracy check and the CPU legs run on it
+    idx = rows[balanced_shards(costs, world)[rank]] if world > 1 else rows
 
     def screen(precision, timing=False):
         s = SparseNewtonRaphsonPowerFlow(precision, ctx)
@@ -348,18 +357,25 @@ def run_ours(args):
     for prec in precs:
         solver = SparseNewtonRaphsonPowerFlow(prec, ctx)
         opt = options(prec)
+        own = {}
+
+        def screen_shard(mm, ii):
+            own["r"] = ContingencyAnalysis.screen_raw(mm, ii, solver, opt)
+            return own["r"]
+
         for _ in range(args.warmup):
-            ContingencyAnalysis.screen_raw(m, idx, solver, opt)
+            screen_sharded(m, rows, screen_shard, costs=costs)
         dev, wall, conv, launches = [], [], [], []
         sampler = ClockSampler(local)
         barrier()
         with sampler:
             for _ in range(args.steps):
                 t = time.perf_counter()
-                r = ContingencyAnalysis.screen_raw(m, idx, solver, opt)
+                merged = screen_sharded(m, rows, screen_shard, costs=costs)
                 wall.append(time.perf_counter() - t)
+                r = own["r"]
                 dev.append(r["device_ms"] / 1e3)
-                conv.append(int((r["status"] == 0).sum()))
+                conv.append(int((merged["status"] == 0).sum()))
                 launches.append(int(r["kernel_launches"]))
         barrier()
         dev_t = float(np.sum(dev))
@@ -369,11 +385,8 @@ def run_ours(args):
             t = torch.tensor([dev_t, wall_t], device=f"cuda:{local}", dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             dev_t, wall_t = float(t[0]), float(t[1])
-            c = torch.tensor([sum(conv)], device=f"cuda:{local}", dtype=torch.float64)
-            dist.all_reduce(c)
-            total_conv = float(c[0])
-        else:
-            total_conv = float(sum(conv))
+        # every rank holds the merged screen of all rows: its converged count is the job's
+        total_conv = float(sum(conv))
         results[prec] = dict(value=total_conv / dev_t, e2e=total_conv / wall_t, ms=dev_t / args.steps * 1e3,
                              wall_ms=wall_t / args.steps * 1e3, conv=conv[-1], launches=launches[-1],
                              clocks=sampler.summary(), last=r)
@@ -435,7 +448,10 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
             "config": {"workload": "N-1 screen, synthetic 10,000-bus grid, 5,000 non-islanding outages per GPU",
                        "n_bus": m.n_bus, "n_branch": m.n_branch, "n_pv": int(np.sum(m.bus_type == 2)),
-                       "outages": int(len(idx)), "max_iterations": 20, "tolerance": 1e-8, "precision": "mixed" if "mixed" in results else "fp64",
+                       "outages": int(len(rows)), "outages_rank0": int(len(idx)),
+                       "sharding": "screen_sharded: rows dealt by estimated iterations (balanced_shards), "
+                                   "results all-gathered in row order" if world > 1 else "screen_sharded, one rank",
+                       "max_iterations": 20, "tolerance": 1e-8, "precision": "mixed" if "mixed" in results else "fp64",
                        "l2": "working set (LU of 5,000 systems, >1 GB) larger than L2",
                        "newton_iterations": int(last["newton_iterations"])},
             "fp64_value": fp["value"], "fp64_ms_per_step": fp["ms"],

@@ -4,7 +4,7 @@ import numpy as np
 import oracle
 from gridsim_b200 import _abi, synthetic
 from gridsim_b200.engine import ContingencyAnalysis, PowerFlowOptions
-from gridsim_b200.parallel import merge, shard
+from gridsim_b200.parallel import balanced_shards, merge, outage_costs, reorder, shard
 from tests.conftest import golden_model
 
 
@@ -71,5 +71,55 @@ def test_merged_shards_equal_one_screen():
     parts = [oracle.screen(m, idx[shard(len(idx), r, 3)], o) for r in range(3)]
     got = merge(parts)
     for k in ("status", "iterations", "viol_ptr", "viol_kind", "viol_element"):
+        assert np.array_equal(got[k], whole[k]), k
+    assert np.array_equal(got["viol_value"], whole["viol_value"])
+
+
+def test_balanced_shards_cover_every_row_once_and_even_the_costs():
+    rng = np.random.default_rng(3)
+    for n in (0, 1, 7, 100, 1001):
+        for world in (1, 2, 3, 8):
+            costs = rng.uniform(2.3, 20.0, n)
+            shards = balanced_shards(costs, world)
+            assert sorted(np.concatenate(shards).tolist()) == list(range(n))
+            assert all(np.all(np.diff(s) > 0) for s in shards)
+            if n >= world:
+                sums = [costs[s].sum() for s in shards]
+                # longest processing time first: no rank exceeds the others by more than the largest single cost
+                assert max(sums) - min(sums) <= costs.max() + 1e-9
+    # equal costs: counts differ by at most one
+    shards = balanced_shards(np.ones(101), 8)
+    assert max(len(s) for s in shards) - min(len(s) for s in shards) <= 1
+
+
+def test_outage_costs_follow_the_removed_flow():
+    m = synthetic.config_grid(1, 0)
+    idx = synthetic.outage_set(m, None, 0)[:200]
+    c = outage_costs(m, idx)
+    assert c.shape == (200,) and np.all(c >= 2.3) and np.all(c <= 20.0)
+    th = np.radians(m.va_deg)
+    flow = np.abs(th[m.br_from[idx]] - th[m.br_to[idx]] - np.radians(m.shift_deg[idx])) / np.abs(m.x[idx])
+    assert np.array_equal(np.argsort(c, kind="stable"), np.argsort(flow, kind="stable"))
+    sets = np.stack([idx[:50], np.where(np.arange(50) % 2 == 0, idx[50:100], -1)], axis=1)
+    cs = outage_costs(m, sets, "sets")
+    assert np.all(cs >= c[:50] - 1e-12)
+    on = np.nonzero(m.gen_in_service)[0][:5]
+    rows = np.array([[0, int(idx[0])]] + [[1, int(g)] for g in on] + [[2, 3]], np.int32)
+    ce = outage_costs(m, rows, "elements")
+    assert ce[0] == c[0] and ce.shape == (7,)
+
+
+def test_reordered_balanced_merge_equals_one_screen():
+    m = synthetic.config_grid(0, 0)
+    idx = synthetic.outage_set(m, None, 0)[:40]
+    o = _abi.default_opts()
+    o.max_iterations = 20
+    o.per_bus_voltage_limits = 1
+    o.warm_start_from_base = 1
+    whole = oracle.screen(m, idx, o)
+    shards = balanced_shards(outage_costs(m, idx), 3)
+    parts = [oracle.screen(m, idx[s], o) for s in shards]
+    got = reorder(merge(parts), np.concatenate(shards))
+    for k in ("status", "iterations", "viol_ptr", "viol_kind", "viol_element", "max_loading_pct"):
         assert np.array_equal(got[k], whole[k]), k
     assert np.array_equal(got["viol_value"], whole["viol_value"])

@@ -1,5 +1,5 @@
 """Two ranks over gloo on CPU: each screens its shard (with the oracle standing in for the device engine) and
-the all-gathered result equals the single-process screen."""
+the all-gathered result equals the single-process screen, for contiguous and for cost-balanced shards."""
 import os
 import socket
 
@@ -48,7 +48,7 @@ def _worker(rank, world, port, out_path):
 
     import oracle
     from gridsim_b200 import _abi, synthetic
-    from gridsim_b200.parallel import screen_sharded
+    from gridsim_b200.parallel import outage_costs, screen_sharded
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         m = synthetic.config_grid(0, 0)
@@ -60,10 +60,19 @@ def _worker(rank, world, port, out_path):
         pairs = _pairs(m)
         got2 = screen_sharded(m, pairs, lambda mm, ss: oracle.screen_sets(mm, ss, o, threads=1))
         got3 = screen_sharded(m, _elements(m), lambda mm, ee: _shared(mm, ee))
+        # cost-balanced shards (rows dealt by estimated iterations), merged back in the caller's row order
+        got4 = screen_sharded(m, idx, lambda mm, ii: oracle.screen(mm, ii, o, threads=1), costs=outage_costs(m, idx))
+        got5 = screen_sharded(m, pairs, lambda mm, ss: oracle.screen_sets(mm, ss, o, threads=1),
+                              costs=outage_costs(m, pairs, "sets"))
+        els = _elements(m)
+        got6 = screen_sharded(m, els, lambda mm, ee: _shared(mm, ee), costs=outage_costs(m, els, "elements"))
         if rank == 0:
             np.savez(out_path, **got)
             np.savez(out_path + ".pairs.npz", **got2)
             np.savez(out_path + ".elements.npz", **got3)
+            np.savez(out_path + ".balanced.npz", **got4)
+            np.savez(out_path + ".balanced_pairs.npz", **got5)
+            np.savez(out_path + ".balanced_elements.npz", **got6)
     finally:
         dist.destroy_process_group()
 
@@ -98,4 +107,10 @@ def test_two_rank_screen_equals_one_process(tmp_path):
         assert np.array_equal(got3[k], whole3[k]), k
     assert list(got3["share_notes"]) == list(whole3["share_notes"])
     assert any(n is not None for n in whole3["share_notes"])
+    # the cost-balanced shards give the same screens, row for row
+    for suffix, ref in ((".balanced.npz", whole), (".balanced_pairs.npz", whole2), (".balanced_elements.npz", whole3)):
+        got_b = np.load(out + suffix, allow_pickle=True)
+        for k in ("status", "iterations", "viol_ptr", "viol_kind", "viol_element", "viol_value", "islanded"):
+            assert np.array_equal(got_b[k], ref[k]), (suffix, k)
+    assert list(np.load(out + ".balanced_elements.npz", allow_pickle=True)["share_notes"]) == list(whole3["share_notes"])
     del torch
