@@ -54,7 +54,7 @@ class PfOpts(ctypes.Structure):
         ("enforce_q_limits", c_i32), ("retry_from_dc_start", c_i32), ("per_bus_voltage_limits", c_i32),
         ("precision", c_i32), ("warm_start_from_base", c_i32), ("batch_width", c_i32), ("phase_timing", c_i32),
         ("post_fault_rating", c_i32), ("max_q_limit_passes", c_i32), ("revert_q_limits", c_i32),
-        ("reserved", c_i32 * 4),
+        ("partial_pivoting", c_i32), ("reserved", c_i32 * 3),
     ]
 
 
@@ -72,7 +72,7 @@ class N1Result(ctypes.Structure):
         ("max_loading_pct", c_vp), ("viol_ptr", c_vp), ("viol_capacity", c_i32), ("viol_count", c_i32),
         ("viol_kind", c_vp), ("viol_element", c_vp), ("viol_value", c_vp), ("vm", c_vp), ("va_deg", c_vp),
         ("base_status", c_i32), ("base_iterations", c_i32), ("device_ms", c_f64), ("n_singular_pivot", c_i32),
-        ("n_batches", c_i32), ("kernel_launches", ctypes.c_int64), ("newton_iterations", c_i32), ("reserved1", c_i32),
+        ("n_batches", c_i32), ("kernel_launches", ctypes.c_int64), ("newton_iterations", c_i32), ("n_partial_pivot", c_i32),
         ("factor_ms", c_f64), ("solve_ms", c_f64), ("mismatch_ms", c_f64), ("other_ms", c_f64), ("factor_bytes", c_f64),
         ("level_factor_ms", c_f64), ("level_factor_bytes", c_f64), ("tail_ms", c_f64), ("islanded", c_vp),
         ("worst_boundary_pct", c_vp),

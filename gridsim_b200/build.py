@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = [os.path.join(HERE, "csrc", f) for f in ("gs_engine.cu", "gs_host.cpp", "gs_symbolic.cpp", "gs_dc.cpp",
                                                 "gs_topology.cpp")]
 OUT = os.path.join(HERE, "libgridsim_b200.so")
-DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("gs_internal.h", "gs_host.h", "gs_kernels.cuh", "gs_multi.cuh", "gs_serve.cuh", "gs_cluster.cuh")] + [
+DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("gs_internal.h", "gs_host.h", "gs_kernels.cuh", "gs_multi.cuh", "gs_serve.cuh", "gs_cluster.cuh", "gs_paired.cuh", "gs_pivot.cuh")] + [
     os.path.join(os.path.dirname(HERE), "include", "gridsim_b200.h")]
 
 

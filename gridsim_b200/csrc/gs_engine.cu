@@ -1277,6 +1277,7 @@ inline size_t QueueBytes(int nLevels) { return (size_t)6 * nLevels * sizeof(int)
 }  // namespace gs
 #include "gs_paired.cuh"
 #include "gs_cluster.cuh"
+#include "gs_pivot.cuh"
 namespace gs {
 
 // One step of the few systems of a batch (their list in b.activeList): factorisation, backward substitution and,
@@ -1669,6 +1670,16 @@ struct Workspace {
     DevBuf startVm, startVa;
 };
 
+// The partial-pivoting re-solve of one grid (or matrix pattern): the matrix's cells by column (Symbolic::aColPtr,
+// aRow, aSlot) on the device, and the factorisation scratch of up to `maxSys` systems with `cap` L and U entries each.
+struct GpData {
+    DevBuf colPtr, row, slot;
+    DevBuf x, rowMax, xi, pstack, mark, pinv, lp, up, li, ui, lx, ux, result;
+    int maxSys = 0;
+    int64_t cap = 0;
+    bool uploaded = false;
+};
+
 }  // namespace gs
 
 struct MatrixPattern;  // an analysed sparse-matrix pattern of the batched linear solve (kept per context)
@@ -1708,6 +1719,10 @@ struct gs_grid {
     int tailMax = gs::kTailMaxSystems;  // the few-systems path takes over at this many systems still stepping
     int psSplit = 0, psSplitB = 0;      // the same first persistent levels on the paired schedule
     bool paired = true;                 // the full-batch step and the cluster walk run the paired schedule
+    // partial-pivoting mode (the re-solve of systems whose static pivot collapsed): every iteration steps on the
+    // few-systems path with k_gp_solve in place of the static factorisation
+    bool gpMode = false;
+    gs::GpData gp;
 };
 
 struct MatrixPattern {
@@ -2046,6 +2061,72 @@ DevBatch HalfView(const DevBatch& b, int off, int n) {
 
 // Run the Newton iteration of `count` systems already placed in the workspace (outage, loadScale).
 // `startFromWs`: start every system from ws.startVm / startVa (a solved base), else from the grid start.
+// The partial-pivoting re-solve's marks: a solved system is flagged kFlagPivoted; one the factorisation could not
+// solve (singular at the row floor, out of capacity, not finite) has its step refused (its run stops with the state
+// it has, as NewtonShell.SolveStep's refusal stops the reference's) and is flagged kFlagPivotFailed.
+__global__ void k_gp_mark(DevBatch b, const int* list, const int* result, int nList) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nList) return;
+    const int s = list[q];
+    if (result[q] == GP_OK) atomicOr(&b.flags[s], kFlagPivoted);
+    else atomicOr(&b.flags[s], kFlagPivotFailed | kFlagStepBad);
+}
+
+// The step of the listed systems of batch `cur` (FP64; Jacobian or matrix in its LU slots, right-hand side in y, both
+// before any static factorisation) by the partial-pivoting factorisation, in chunks the scratch holds; the solution
+// replaces y. Returns the kernels launched.
+int GpStep(gs_grid* G, const DevBatch& cur, const int* dList, int nList, cudaStream_t st, int* launched) {
+    gs_ctx* ctx = G->ctx;
+    const Symbolic& s = G->sym;
+    GpData& d = G->gp;
+    *launched = 0;
+    if (nList <= 0) return GS_OK;
+    const int m = s.m;
+    if (!d.uploaded) {
+        GS_CUDA(d.colPtr.alloc((s.aColPtr.size()) * 4));
+        GS_CUDA(d.row.alloc(std::max<size_t>(1, s.aRow.size()) * 4));
+        GS_CUDA(d.slot.alloc(std::max<size_t>(1, s.aSlot.size()) * 4));
+        GS_CUDA(cudaMemcpy(d.colPtr.p, s.aColPtr.data(), s.aColPtr.size() * 4, cudaMemcpyHostToDevice));
+        if (!s.aRow.empty()) {
+            GS_CUDA(cudaMemcpy(d.row.p, s.aRow.data(), s.aRow.size() * 4, cudaMemcpyHostToDevice));
+            GS_CUDA(cudaMemcpy(d.slot.p, s.aSlot.data(), s.aSlot.size() * 4, cudaMemcpyHostToDevice));
+        }
+        d.uploaded = true;
+    }
+    // L and U capacity per system: twice the static pattern's entries, plus room for rows pivoted off the diagonal
+    const int64_t cap = 2 * s.nnzLU + 8 * (int64_t)m;
+    const size_t perSys = (size_t)m * (8 + 8 + 4 * 4) + 2 * (size_t)(m + 1) * 4 + (size_t)cap * 24 + 4;
+    // systems per launch: up to two per SM, within 2 GB of scratch
+    const int want = (int)std::max<size_t>(1, std::min<size_t>(296, ((size_t)2 << 30) / perSys));
+    if (d.maxSys < want || d.cap != cap) {
+        const size_t k = (size_t)want;
+        GS_CUDA(d.x.alloc(k * m * 8)); GS_CUDA(d.rowMax.alloc(k * m * 8));
+        GS_CUDA(d.xi.alloc(k * m * 4)); GS_CUDA(d.pstack.alloc(k * m * 4)); GS_CUDA(d.mark.alloc(k * m * 4));
+        GS_CUDA(d.pinv.alloc(k * m * 4));
+        GS_CUDA(d.lp.alloc(k * (m + 1) * 4)); GS_CUDA(d.up.alloc(k * (m + 1) * 4));
+        GS_CUDA(d.li.alloc(k * cap * 4)); GS_CUDA(d.ui.alloc(k * cap * 4));
+        GS_CUDA(d.lx.alloc(k * cap * 8)); GS_CUDA(d.ux.alloc(k * cap * 8));
+        GS_CUDA(d.result.alloc(k * 4));
+        d.maxSys = want;
+        d.cap = cap;
+    }
+    GpView v{};
+    v.m = m; v.cap = cap;
+    v.colPtr = d.colPtr.as<int>(); v.row = d.row.as<int>(); v.slot = d.slot.as<int>();
+    v.x = d.x.as<double>(); v.rowMax = d.rowMax.as<unsigned long long>();
+    v.xi = d.xi.as<int>(); v.pstack = d.pstack.as<int>(); v.mark = d.mark.as<int>(); v.pinv = d.pinv.as<int>();
+    v.lp = d.lp.as<int>(); v.up = d.up.as<int>(); v.li = d.li.as<int>(); v.ui = d.ui.as<int>();
+    v.lx = d.lx.as<double>(); v.ux = d.ux.as<double>(); v.result = d.result.as<int>();
+    for (int off = 0; off < nList; off += d.maxSys) {
+        const int c = std::min(d.maxSys, nList - off);
+        k_gp_solve<<<c, 32, 0, st>>>(v, (const double*)cur.lu, (double*)cur.y, cur.B, dList + off, c);
+        k_gp_mark<<<(c + 127) / 128, 128, 0, st>>>(cur, dList + off, v.result, c);
+        *launched += 2;
+    }
+    GS_CUDA(cudaGetLastError());
+    return GS_OK;
+}
+
 struct NewtonStats {
     int64_t launches = 0;
     int iterations = 0;
@@ -2195,7 +2276,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
     // (re)capture the step graphs for stepB (its parts set)
     auto captureStep = [&]() -> int {
         for (auto& x : exec) if (x) { cudaGraphExecDestroy(x); x = nullptr; }
-        if (timed) return GS_OK;
+        if (timed || G->gpMode) return GS_OK;  // the partial-pivoting re-solve never takes a full-batch step
         for (int r = 0; r <= refine; r++) {
             cudaGraph_t graph;
             stepLaunches = 0;
@@ -2265,7 +2346,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
         const int nActive = ctx->pinnedCount[0];
         const int anyRefine = refine && ctx->pinnedCount[1] > 0 ? 1 : 0;
         sysIters += nActive;
-        if (nActive <= G->tailMax) {
+        if (nActive <= G->tailMax || G->gpMode) {
             if (midOn) {  // the mid workspace's systems go back to the batch, which the few-systems path gathers from
                 k_scatter<<<dim3(nodeBlocks.x, cur.B / 32), blk8, 0, st>>>(cur, b, G->mws.origin.as<int>(), s.n);
                 launches++;
@@ -2296,8 +2377,16 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             // one CTA per active system (k_tail), in FP64 (the compact workspace's precision)
             cudaMemsetAsync(cur.activeCount, 0, sizeof(int), st);
             k_collect_active<<<(cur.count + 255) / 256, 256, 0, st>>>(cur);
-            launches += 1 + FewSystemsSolve<double>(g, cur, s, nActive, G->tailSplit, false, st, timed ? ev[2] : nullptr,
-                                                    ctx->clusterOk, G->paired);
+            if (G->gpMode) {
+                // the partial-pivoting re-solve: the step by k_gp_solve from the Jacobian just filled
+                if (timed) cudaEventRecord(ev[2], st);
+                int gl = 0;
+                if ((rc = GpStep(G, cur, cur.activeList, nActive, st, &gl)) != GS_OK) break;
+                launches += 1 + gl;
+            } else {
+                launches += 1 + FewSystemsSolve<double>(g, cur, s, nActive, G->tailSplit, false, st,
+                                                        timed ? ev[2] : nullptr, ctx->clusterOk, G->paired);
+            }
             if (timed) cudaEventRecord(ev[3], st);
             {
                 const int grp = (nActive + 31) / 32;
@@ -2413,6 +2502,13 @@ int NewtonDispatch(gs_grid* G, int count, bool useScale, bool startFromWs, const
                    NewtonStats* stats = nullptr, const double* vmSys = nullptr, const double* vaSys = nullptr) {
     G->view.qlimRevert = o.revert_q_limits ? 1 : 0;  // the call's Q-limit options (PowerFlowOptions.cs:101, 110)
     G->view.qlimMaxPasses = o.max_q_limit_passes > 0 ? o.max_q_limit_passes : kMaxQPasses;
+    if (o.partial_pivoting) {  // every step by the per-system partial-pivoting factorisation (FP64)
+        const bool was = G->gpMode;
+        G->gpMode = true;
+        const int rc = Newton<double>(G, count, useScale, startFromWs, o, ms, stats, vmSys, vaSys);
+        G->gpMode = was;
+        return rc;
+    }
     if (o.precision == GS_PREC_MIXED) return Newton<float>(G, count, useScale, startFromWs, o, ms, stats, vmSys, vaSys);
     return Newton<double>(G, count, useScale, startFromWs, o, ms, stats, vmSys, vaSys);
 }
@@ -2657,6 +2753,87 @@ int RetryStalled(gs_grid* G, int count, const int* outage, const double* loadSca
     return GS_OK;
 }
 
+// Systems of the batch whose static pivot collapsed (kFlagPivotPerturbed) are solved again from their start with row
+// partial pivoting at every step (k_gp_solve, FP64, in the twin grid's workspace), as the reference factors every
+// system (SparseLuFactorization.Factor, NewtonShell.SolveStep :74-120). A re-solve the factorisation carries to its
+// end replaces the system's state, status, iterations and flags (kFlagPivoted); where the factorisation finds the
+// matrix singular too, the system keeps its static result, still flagged. `outage` and `loadScale` are the batch's
+// own arrays; `warm`: the batch started from ws.startVm / startVa.
+int ResolvePivoted(gs_grid* G, int count, const int* outage, const double* loadScale, bool warm, const gs_pf_opts& o,
+                   float* msOut) {
+    if (count <= 0) return GS_OK;
+    gs_ctx* ctx = G->ctx;
+    const Symbolic& s = G->sym;
+    Workspace& w = G->ws;
+    std::vector<int> fl(count);
+    GS_CUDA(cudaMemcpy(fl.data(), w.flags.p, count * 4, cudaMemcpyDeviceToHost));
+    std::vector<int> cand;
+    for (int k = 0; k < count; k++)
+        if (fl[k] & kFlagPivotPerturbed) cand.push_back(k);
+    if (cand.empty()) return GS_OK;
+    gs_grid* R = nullptr;
+    int rc = RetryGridOf(G, &R);
+    if (rc) return rc;
+    if (G->view.nSet > 0 && (rc = InstallSets(R, G->sets)) != GS_OK) return rc;  // the same outage ids
+    R->view.qlimOn = G->view.qlimOn;
+    struct Restore {
+        gs_grid* r;
+        ~Restore() { r->gpMode = false; r->ws.ovOn = r->tws.ovOn = r->mws.ovOn = false; r->elemBatch.clear(); }
+    } restore{R};
+    const bool elems = !G->elemBatch.empty();
+    const int n = s.n;
+    gs_pf_opts o64 = o;
+    o64.precision = GS_PREC_FP64;
+    constexpr int kChunk = 256;  // within the compact workspace of the few-systems path
+    for (size_t c0 = 0; c0 < cand.size(); c0 += kChunk) {
+        const int nc = (int)std::min<size_t>(kChunk, cand.size() - c0);
+        const int B = std::max(32, (nc + 31) / 32 * 32);
+        if ((rc = EnsureWorkspace(R, B, GS_PREC_FP64, false, loadScale != nullptr)) != GS_OK) return rc;
+        Workspace& rw = R->ws;
+        std::vector<int> outs(B, -1);
+        for (int c = 0; c < nc; c++) outs[c] = outage ? outage[cand[c0 + c]] : -1;
+        GS_CUDA(cudaMemcpy(rw.outage.p, outs.data(), B * 4, cudaMemcpyHostToDevice));
+        if (elems) {
+            R->elemBatch.clear();
+            for (int c = 0; c < nc; c++) R->elemBatch.push_back(G->elemBatch[cand[c0 + c]]);
+            if ((rc = UploadElements(R, rw, R->elemBatch)) != GS_OK) return rc;
+            rw.ovOn = R->tws.ovOn = true;
+        }
+        if (loadScale) {
+            std::vector<double> scl((size_t)n * B, 1.0);
+            for (int c = 0; c < nc; c++)
+                for (int i = 0; i < n; i++) scl[(size_t)i * B + c] = loadScale[(size_t)cand[c0 + c] * n + i];
+            GS_CUDA(cudaMemcpy(rw.loadScale.p, scl.data(), scl.size() * 8, cudaMemcpyHostToDevice));
+        }
+        if (warm) {
+            GS_CUDA(cudaMemcpy(rw.startVm.p, w.startVm.p, (size_t)n * 8, cudaMemcpyDeviceToDevice));
+            GS_CUDA(cudaMemcpy(rw.startVa.p, w.startVa.p, (size_t)n * 8, cudaMemcpyDeviceToDevice));
+        }
+        R->gpMode = true;
+        float ms = 0;
+        rc = NewtonDispatch(R, nc, loadScale != nullptr, warm, o64, &ms);
+        R->gpMode = false;
+        if (rc) return rc;
+        if (msOut) *msOut += ms;
+        std::vector<int> rfl(nc);
+        GS_CUDA(cudaMemcpy(rfl.data(), rw.flags.p, nc * 4, cudaMemcpyDeviceToHost));
+        std::vector<int2> pairs;
+        for (int c = 0; c < nc; c++)
+            if (!(rfl[c] & kFlagPivotFailed)) pairs.push_back(make_int2(c, cand[c0 + c]));
+        if (pairs.empty()) continue;
+        DevBuf dp;
+        GS_CUDA(dp.alloc(pairs.size() * sizeof(int2)));
+        GS_CUDA(cudaMemcpy(dp.p, pairs.data(), pairs.size() * sizeof(int2), cudaMemcpyHostToDevice));
+        const DevBatch from = MakeBatchWs(rw, R->sym.nLevels, rw.B, nc, loadScale != nullptr);
+        const DevBatch to = MakeBatch(G, count, loadScale != nullptr);
+        k_move_listed<<<dim3((n + 7) / 8, ((int)pairs.size() + 31) / 32), dim3(32, 8), 0, ctx->stream>>>(
+            from, to, dp.as<int2>(), (int)pairs.size(), n);
+        GS_CUDA(cudaGetLastError());
+        GS_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    return GS_OK;
+}
+
 int CheckOpts(gs_ctx* ctx, const gs_pf_opts* o) {
     if (!o) return SetErr(ctx, GS_ERR_INVALID_ARG, "null options");
     if (!(o->tolerance > 0) || o->tolerance > 1e-2) return SetErr(ctx, GS_ERR_INVALID_ARG, "tolerance must be in (0, 1e-2]");
@@ -2678,6 +2855,7 @@ int ChooseB(gs_grid* G, int want, const gs_pf_opts& o) {
                                                  G->ws.value.bytes + G->ws.y.bytes))) / per;
     int B = (int)std::min<size_t>(cap, (size_t)1 << 20);
     if (o.batch_width > 0) B = std::min(B, o.batch_width);
+    if (o.partial_pivoting) B = std::min(B, 256);  // such batches step on the few-systems path's compact workspace
     B = std::min(B, ((want + 31) / 32) * 32);
     B = (B / 32) * 32;
     return std::max(B, 32);
@@ -2710,6 +2888,8 @@ int SolveBase(gs_grid* G, const gs_pf_opts& o, int* status, int* iters, double* 
     rc = NewtonDispatch(G, 1, false, false, o, ms);
     if (rc) return rc;
     const int none = -1;
+    rc = ResolvePivoted(G, 1, &none, nullptr, false, o, ms);
+    if (rc) return rc;
     rc = RetryStalled(G, 1, &none, nullptr, false, o, ms, nullptr);
     if (rc) return rc;
     const size_t B = G->ws.B;
@@ -2937,6 +3117,8 @@ int gs_pf_solve_batch(gs_grid* G, int32_t count, const double* loadScale, const 
         float ms = 0;
         rc = NewtonDispatch(G, cnt, loadScale != nullptr, false, o, &ms);
         if (rc) return rc;
+        rc = ResolvePivoted(G, cnt, out.data(), loadScale ? loadScale + (size_t)done * n : nullptr, false, o, &ms);
+        if (rc) return rc;
         rc = RetryStalled(G, cnt, out.data(), loadScale ? loadScale + (size_t)done * n : nullptr, false, o, &ms, nullptr);
         if (rc) return rc;
         std::vector<int> st(cnt), it(cnt);
@@ -3146,6 +3328,7 @@ int ScreenOutageLists(gs_grid* G, int nOut, const std::vector<Element>& els, con
     res->base_status = GS_PF_NOT_RUN;
     res->base_iterations = 0;
     res->n_singular_pivot = 0;
+    res->n_partial_pivot = 0;
     res->n_batches = 0;
     double totalMs = 0;
     bool warm = false;
@@ -3199,6 +3382,8 @@ int ScreenOutageLists(gs_grid* G, int nOut, const std::vector<Element>& els, con
         }
         float ms = 0;
         rc = NewtonDispatch(G, cnt, false, warm, o, &ms, &stats);
+        if (rc) return rc;
+        rc = ResolvePivoted(G, cnt, out.data(), nullptr, warm, o, &ms);
         if (rc) return rc;
         rc = RetryStalled(G, cnt, out.data(), nullptr, warm, o, &ms, &stats);
         if (rc) return rc;
@@ -3267,6 +3452,7 @@ int ScreenOutageLists(gs_grid* G, int nOut, const std::vector<Element>& els, con
             if (res->islanded) res->islanded[g] = !conv && splits[g];
             if (res->viol_ptr) res->viol_ptr[g] = written + sysStart[k];
             if (fl[k] & kFlagPivotPerturbed) res->n_singular_pivot++;
+            if (fl[k] & kFlagPivoted) res->n_partial_pivot++;
         }
         if (written + batchTotal > res->viol_capacity || !res->viol_kind || !res->viol_element || !res->viol_value) {
             capacityOk = false;
@@ -3621,12 +3807,32 @@ int gs_sparse_solve_batch(gs_ctx* ctx, int32_t count, const int32_t* n, const in
                 GS_CUDA(cudaMemcpyAsync(fl.data(), G->ws.flags.p, cnt * 4, cudaMemcpyDeviceToHost, ctx->stream));
                 GS_CUDA(cudaStreamSynchronize(ctx->stream));
                 const std::vector<int>& pinv = G->sym.pinv;
+                std::vector<int> redo;  // systems whose static pivot collapsed (or whose solution is not finite)
                 for (int c = 0; c < cnt; c++) {
                     const int q = same[done + c];
                     bool good = !(fl[c] & kFlagPivotPerturbed);
                     for (int i = 0; i < nq && good; i++) good = std::isfinite(y[(size_t)pinv[i] * B + c]);
-                    if (!good) { status[q] = GS_LS_SINGULAR; continue; }
+                    if (!good) { redo.push_back(c); continue; }
                     for (int i = 0; i < nq; i++) x[vOff[q] + i] = y[(size_t)pinv[i] * B + c];
+                }
+                if (!redo.empty()) {
+                    // solved again with row partial pivoting (the reference's factorisation) from the reloaded
+                    // matrix; singular only if that fails too
+                    k_load_matrix<<<dim3((std::max(nnz, nq) + 7) / 8, B / 32), dim3(32, 8), 0, ctx->stream>>>(
+                        b, cnt, nnz, nq, P->dSlot.as<int>(), P->dPinv.as<int>(), dv.as<double>(), db.as<double>());
+                    DevBuf dl;
+                    GS_CUDA(dl.alloc(redo.size() * 4));
+                    GS_CUDA(cudaMemcpy(dl.p, redo.data(), redo.size() * 4, cudaMemcpyHostToDevice));
+                    int gl = 0;
+                    if ((rc = GpStep(G, b, dl.as<int>(), (int)redo.size(), ctx->stream, &gl)) != GS_OK) return rc;
+                    GS_CUDA(cudaMemcpyAsync(y.data(), G->ws.y.p, y.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+                    GS_CUDA(cudaMemcpyAsync(fl.data(), G->ws.flags.p, cnt * 4, cudaMemcpyDeviceToHost, ctx->stream));
+                    GS_CUDA(cudaStreamSynchronize(ctx->stream));
+                    for (int c : redo) {
+                        const int q = same[done + c];
+                        if (fl[c] & kFlagPivotFailed) { status[q] = GS_LS_SINGULAR; continue; }
+                        for (int i = 0; i < nq; i++) x[vOff[q] + i] = y[(size_t)pinv[i] * B + c];
+                    }
                 }
                 done += cnt;
             }

@@ -76,6 +76,9 @@ struct Symbolic {
     int64_t flops = 0;  // multiply-adds of one numeric factorisation (+ forward substitution)
     std::vector<int> ySlot;          // [4*nnzY] Y cell -> LU slot of H, N, M, L (-1 absent)
     std::vector<int> busP, busQ;     // bus -> pivot step of its P / Q equation (-1 none)
+    // the matrix's own cells (the Jacobian's, or a loaded matrix's; fill left out) by column in pivot order: rows
+    // aRow[aColPtr[l] .. aColPtr[l+1]) ascending, each with its LU slot; what the partial-pivoting re-solve reads
+    std::vector<int32_t> aColPtr, aRow, aSlot;
     // ---- schedule ----
     int nLevels = 0;
     std::vector<int> level;          // per node

@@ -17,6 +17,8 @@ enum : int32_t {
     kFlagStepBad = 2,         // the step was not finite (NewtonShell.SolveStep refuses it)
     kFlagPivotPerturbed = 4,  // a static pivot fell below its floor and was perturbed
     kFlagJacBad = 8,          // the Jacobian held a NaN / Inf (the step is refused)
+    kFlagPivoted = 16,        // solved with row partial pivoting (the re-solve of a collapsed static pivot)
+    kFlagPivotFailed = 32,    // the partial-pivoting solve found the matrix singular (or out of capacity)
 };
 
 // Symbolic::TopPart on the device (one per element size).

@@ -238,8 +238,9 @@ extern "C" int gs_pf_solve_multi(gs_ctx* ctx, int32_t nGrids, gs_grid* const* gr
     cudaStream_t st = ctx->stream;
     // Q limits and the DC retry (ContingencyAnalysis.StudyOptions, ContingencyAnalysis.cs:263-268): a case's system
     // changes between Newton passes, which the one-CTA-per-case solve does not carry; each grid's cases then run as
-    // one batch solve (the load scales, outages and states of a grid are contiguous in both layouts)
-    if (o.enforce_q_limits || o.retry_from_dc_start) {
+    // one batch solve (the load scales, outages and states of a grid are contiguous in both layouts). So do cases
+    // under partial pivoting, whose steps the batch solve takes with the per-system partial-pivoting factorisation.
+    if (o.enforce_q_limits || o.retry_from_dc_start || o.partial_pivoting) {
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         GS_CUDA(cudaEventCreate(&e0));
         GS_CUDA(cudaEventCreate(&e1));

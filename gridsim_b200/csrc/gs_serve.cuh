@@ -438,7 +438,7 @@ int gs_serve_create(gs_ctx* ctx, const gs_serve_opts* opts, gs_server** out) {
     if (opts->pf.flat_start) return SetErr(ctx, GS_ERR_UNSUPPORTED, "flat_start: pass a flat start in the descriptor");
     // Q limits and the DC retry (the options of the reference's rpc solve, src/GridSim.Cli/RpcCommand.cs:675-676):
     // answered in batches (AdvanceBatch), each request from the case's stored voltages as gs_pf_solve_batch starts them
-    const bool batch = opts->pf.enforce_q_limits || opts->pf.retry_from_dc_start;
+    const bool batch = opts->pf.enforce_q_limits || opts->pf.retry_from_dc_start || opts->pf.partial_pivoting;
     if (batch && opts->pf.warm_start_from_base)
         return SetErr(ctx, GS_ERR_UNSUPPORTED, "warm_start_from_base with Q limits or the DC retry: not in the request loop");
     const int slots = opts->slots_per_grid ? opts->slots_per_grid : GS_SERVE_MAX_SLOTS;

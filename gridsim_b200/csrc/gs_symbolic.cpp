@@ -324,6 +324,28 @@ std::string FactorSymbolic(Symbolic& s, const std::function<void(const std::func
     };
     std::vector<char> hasA(s.nnzLU, 0);
     mapA(slotOf, hasA);
+    {
+        // the cells that receive a value of A, by column: node k holds (k, k), U(k, l) and L(l, k) for l in P_k
+        std::vector<std::vector<std::pair<int, int32_t>>> cols(m);
+        for (int k = 0; k < m; k++) {
+            const int64_t b0 = s.luBase[k];
+            const int c = s.luCnt[k];
+            if (hasA[b0]) cols[k].push_back({k, (int32_t)b0});
+            for (int t = 0; t < c; t++) {
+                const int l = s.pRows[s.pRowPtr[k] + t];
+                if (hasA[b0 + 1 + t]) cols[l].push_back({k, (int32_t)(b0 + 1 + t)});
+                if (hasA[b0 + 1 + c + t]) cols[k].push_back({l, (int32_t)(b0 + 1 + c + t)});
+            }
+        }
+        s.aColPtr.assign(m + 1, 0);
+        s.aRow.clear();
+        s.aSlot.clear();
+        for (int l = 0; l < m; l++) {
+            std::sort(cols[l].begin(), cols[l].end());
+            for (const auto& e : cols[l]) { s.aRow.push_back(e.first); s.aSlot.push_back(e.second); }
+            s.aColPtr[l + 1] = (int32_t)s.aRow.size();
+        }
+    }
 
     // ---------------- levels ----------------
     s.level.assign(m, 0);

@@ -49,6 +49,9 @@ class PowerFlowOptions:
     post_fault_rating: str = "A"     # "A", "B" or "C": the rating outage states are judged against (screens)
     max_q_limit_passes: int = 100    # MaxQLimitPasses
     revert_q_limits: bool = False    # RevertQLimits
+    # every Newton step by the per-system partial-pivoting LU (the reference's factorisation, FP64) instead of the
+    # batched static-pivot factorisation; that LU runs anyway for a system whose static pivot collapses
+    partial_pivoting: bool = False
 
     def to_c(self) -> _abi.PfOpts:
         o = _abi.default_opts()
@@ -66,6 +69,7 @@ class PowerFlowOptions:
         o.post_fault_rating = {"A": _abi.RATE_A, "B": _abi.RATE_B, "C": _abi.RATE_C}[self.post_fault_rating.upper()]
         o.max_q_limit_passes = int(self.max_q_limit_passes)
         o.revert_q_limits = int(self.revert_q_limits)
+        o.partial_pivoting = int(self.partial_pivoting)
         return o
 
     def device_model(self, model: GridModel) -> GridModel:
@@ -769,7 +773,7 @@ class ContingencyAnalysis:
             out["vm"] = out["vm"].reshape(k, n)
             out["va_deg"] = out["va_deg"].reshape(k, n)
         out.update(base_status=r.base_status, base_iterations=r.base_iterations, device_ms=r.device_ms,
-                   n_singular_pivot=r.n_singular_pivot, n_batches=r.n_batches, kernel_launches=r.kernel_launches,
+                   n_singular_pivot=r.n_singular_pivot, n_partial_pivot=r.n_partial_pivot, n_batches=r.n_batches, kernel_launches=r.kernel_launches,
                    newton_iterations=r.newton_iterations, factor_ms=r.factor_ms, solve_ms=r.solve_ms,
                    mismatch_ms=r.mismatch_ms, other_ms=r.other_ms, factor_bytes=r.factor_bytes,
                    level_factor_ms=r.level_factor_ms, level_factor_bytes=r.level_factor_bytes, tail_ms=r.tail_ms)

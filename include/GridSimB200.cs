@@ -84,8 +84,9 @@ namespace GridSim.Core.PowerFlow.B200
         {
             public double Tolerance, DivergeLimitPu;
             public int MaxIterations, FlatStart, EnforceQLimits, RetryFromDcStart, PerBusVoltageLimits, Precision,
-                       WarmStartFromBase, BatchWidth, PhaseTiming, PostFaultRating, MaxQLimitPasses, RevertQLimits;
-            public fixed int Reserved[4];
+                       WarmStartFromBase, BatchWidth, PhaseTiming, PostFaultRating, MaxQLimitPasses, RevertQLimits,
+                       PartialPivoting;
+            public fixed int Reserved[3];
         }
 
         [StructLayout(LayoutKind.Sequential)]
@@ -108,7 +109,7 @@ namespace GridSim.Core.PowerFlow.B200
             public double DeviceMs;
             public int NSingularPivot, NBatches;
             public long KernelLaunches;
-            public int NewtonIterations, Reserved1;
+            public int NewtonIterations, NPartialPivot;
             public double FactorMs, SolveMs, MismatchMs, OtherMs, FactorBytes, LevelFactorMs, LevelFactorBytes, TailMs;
             public IntPtr Islanded, WorstBoundaryPct;                                    // byte*, double* [nOut] or zero
         }

@@ -154,7 +154,11 @@ typedef struct gs_pf_opts {
     int32_t post_fault_rating;      /* enum gs_post_fault_rating, screens only; default GS_RATE_A */
     int32_t max_q_limit_passes;     /* cap on PV->PQ switching passes (MaxQLimitPasses); 0 = the default 100 */
     int32_t revert_q_limits;        /* RevertQLimits: a pinned bus may go back to PV within a switching pass; 0 */
-    int32_t reserved[4];
+    int32_t partial_pivoting;       /* 1: every Newton step of every system by the per-system sparse LU with row partial
+                                       pivoting (the reference's SparseLuFactorization.Factor, FP64, one warp per
+                                       system) instead of the batched static-pivot factorisation; 0 (default): that
+                                       factorisation only for systems whose static pivot collapses */
+    int32_t reserved[3];
 } gs_pf_opts;
 
 /* Fill `o` with the reference defaults (PowerFlowOptions()) plus precision = FP64. */
@@ -200,12 +204,12 @@ typedef struct gs_n1_result {
     /* device time of the screen, milliseconds (CUDA events): the base solve, the Newton batches, the retry,
      * and the classification and compaction of the results */
     double device_ms;
-    int32_t n_singular_pivot;  /* systems whose static pivot failed */
+    int32_t n_singular_pivot;  /* systems whose static pivot failed and whose partial-pivoting re-solve failed too */
     int32_t n_batches;
     /* work and phase timing of the screen (phase times only with gs_pf_opts.phase_timing) */
     int64_t kernel_launches;   /* kernels this call launched */
     int32_t newton_iterations; /* Newton iterations of the largest batch (device loop trips) */
-    int32_t reserved1;
+    int32_t n_partial_pivot;   /* systems solved again with row partial pivoting after a static pivot failed */
     double factor_ms;          /* fused factorisation + forward substitution */
     double solve_ms;           /* backward substitution (+ the refinement solves in mixed precision) */
     double mismatch_ms;        /* mismatch + Jacobian fill (+ residual) */

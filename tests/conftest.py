@@ -73,3 +73,37 @@ def assert_states_close(m, removed_branches, gpu_vm, gpu_va_deg, ref_vm, ref_va_
         else:
             f = first[root[i]]
             assert abs((ga[i] - ga[f]) - (ra[i] - ra[f])) <= va_tol_rad, i
+
+
+def resistive_leaf_grid(at_bus: int = 4, r: float = 0.05):
+    """case9 with a tenth bus hung from bus `at_bus` (position) by a purely resistive branch (x = 0), carrying 10 MW
+    and 3 MVAr of load, every PQ bus starting at 1 pu and 0 degrees and the new bus at its neighbour's start.
+
+    At that start the new bus's 2 x 2 Jacobian block is [[0, N], [M, 0]]: with no reactance between equal voltages
+    dP/dtheta and dQ/dV vanish, so a diagonal pivot of a leaf bus (eliminated before its neighbour) collapses in any
+    order, while the matrix is regular and the reference's row partial pivoting takes the off-diagonal entries."""
+    import numpy as np
+    m, _ = golden_model("case9")
+    m = m.copy()
+    n = m.n_bus
+
+    def app(name, v):
+        a = getattr(m, name)
+        if a is not None:
+            setattr(m, name, np.concatenate([a, np.array([v], dtype=a.dtype)]))
+    for name, v in (("bus_id", int(m.bus_id.max()) + 1), ("bus_type", 1), ("pd", 10.0), ("qd", 3.0), ("gs", 0.0),
+                    ("bs", 0.0), ("vm", 1.0), ("va_deg", 0.0), ("vmin", np.nan), ("vmax", np.nan),
+                    ("base_kv", float(m.base_kv[at_bus]))):
+        app(name, v)
+    if m.zip is not None:
+        m.zip = np.vstack([m.zip, [0.0, 0.0, 1.0, 0.0, 0.0, 1.0]])
+    for name, v in (("br_from", at_bus), ("br_to", n), ("r", r), ("x", 0.0), ("b", 0.0), ("tap", 0.0),
+                    ("shift_deg", 0.0), ("rate_a", 0.0), ("br_in_service", 1), ("is_transformer", 0), ("rate_b", 0.0),
+                    ("rate_c", 0.0)):
+        app(name, v)
+    if m.br_name is not None:
+        m.br_name = list(m.br_name) + [""]
+    m.vm[:] = np.where(m.bus_type == 1, 1.0, m.vm)
+    m.va_deg[:] = 0.0
+    m.vm[n] = m.vm[at_bus]
+    return m

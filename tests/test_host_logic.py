@@ -123,3 +123,30 @@ def test_reordered_balanced_merge_equals_one_screen():
     for k in ("status", "iterations", "viol_ptr", "viol_kind", "viol_element", "max_loading_pct"):
         assert np.array_equal(got[k], whole[k]), k
     assert np.array_equal(got["viol_value"], whole["viol_value"])
+
+
+def test_resistive_leaf_collapses_a_static_diagonal_pivot():
+    """The crafted grid of the partial-pivoting GPU tests: under the oracle's minimum-degree order the static
+    diagonal elimination of its start Jacobian meets a zero pivot, the matrix is regular, and the oracle (row partial
+    pivoting) converges."""
+    from tests.conftest import resistive_leaf_grid
+    m = resistive_leaf_grid()
+    rp, ci, val, _ = oracle.jacobian(m)
+    n = len(rp) - 1
+    a = np.zeros((n, n))
+    for i in range(n):
+        a[i, ci[rp[i]:rp[i + 1]]] = val[rp[i]:rp[i + 1]]
+    q = oracle.md_order(rp, ci)
+    p = a[np.ix_(q, q)].copy()
+    collapsed = False
+    for k in range(n):
+        if abs(p[k, k]) <= 1e-12 * max(1.0, abs(p[k, k])):
+            collapsed = True
+            break
+        p[k + 1:, k] /= p[k, k]
+        p[k + 1:, k + 1:] -= np.outer(p[k + 1:, k], p[k, k + 1:])
+    assert collapsed
+    assert np.linalg.cond(a) < 1e4
+    o = _abi.default_opts()
+    o.max_iterations = 20
+    assert oracle.solve(m, o)["status"] == _abi.PF_CONVERGED
