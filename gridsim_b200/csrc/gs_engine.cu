@@ -1678,6 +1678,12 @@ struct GpData {
     int maxSys = 0;
     int64_t cap = 0;
     bool uploaded = false;
+    // the iterative fallback (ILU(0) + BiCGSTAB) of the Newton step: the Jacobian in equation order and the Y cells'
+    // stamps, and its scratch
+    DevBuf jRowPtr, jCol, jSlot, jYcell, eqPinv, ccPtr, ccOwner;
+    DevBuf itVal, itA, itPresent, itDiag, itIw, itVec;
+    int itSys = 0;
+    bool itUploaded = false;
 };
 
 }  // namespace gs
@@ -2068,14 +2074,15 @@ __global__ void k_gp_mark(DevBatch b, const int* list, const int* result, int nL
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nList) return;
     const int s = list[q];
-    if (result[q] == GP_OK) atomicOr(&b.flags[s], kFlagPivoted);
+    if (result[q] == GP_OK || result[q] == GP_ITERATIVE) atomicOr(&b.flags[s], kFlagPivoted);
     else atomicOr(&b.flags[s], kFlagPivotFailed | kFlagStepBad);
 }
 
 // The step of the listed systems of batch `cur` (FP64; Jacobian or matrix in its LU slots, right-hand side in y, both
 // before any static factorisation) by the partial-pivoting factorisation, in chunks the scratch holds; the solution
 // replaces y. Returns the kernels launched.
-int GpStep(gs_grid* G, const DevBatch& cur, const int* dList, int nList, cudaStream_t st, int* launched) {
+int GpStep(gs_grid* G, const DevBatch& cur, const int* dList, int nList, cudaStream_t st, int* launched,
+           bool iterative = false, double tol = 1e-8) {
     gs_ctx* ctx = G->ctx;
     const Symbolic& s = G->sym;
     GpData& d = G->gp;
@@ -2117,9 +2124,43 @@ int GpStep(gs_grid* G, const DevBatch& cur, const int* dList, int nList, cudaStr
     v.xi = d.xi.as<int>(); v.pstack = d.pstack.as<int>(); v.mark = d.mark.as<int>(); v.pinv = d.pinv.as<int>();
     v.lp = d.lp.as<int>(); v.up = d.up.as<int>(); v.li = d.li.as<int>(); v.ui = d.ui.as<int>();
     v.lx = d.lx.as<double>(); v.ux = d.ux.as<double>(); v.result = d.result.as<int>();
+    IterView iv{};
+    if (iterative) {
+        // NewtonShell.SolveStep's fallback when the factorisation finds the Jacobian singular (NewtonShell.cs:96-105)
+        if (!d.itUploaded) {
+            auto up = [&](DevBuf& buf, const std::vector<int>& h) -> cudaError_t {
+                cudaError_t e = buf.alloc(std::max<size_t>(1, h.size()) * 4);
+                if (e == cudaSuccess && !h.empty()) e = cudaMemcpy(buf.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice);
+                return e;
+            };
+            GS_CUDA(up(d.jRowPtr, s.jRowPtr)); GS_CUDA(up(d.jCol, s.jCol)); GS_CUDA(up(d.jSlot, s.jSlot));
+            GS_CUDA(up(d.jYcell, s.jYcell)); GS_CUDA(up(d.eqPinv, s.pinv)); GS_CUDA(up(d.ccPtr, s.ccPtr));
+            GS_CUDA(up(d.ccOwner, s.ccOwner));
+            d.itUploaded = true;
+        }
+        if (d.itSys < d.maxSys) {
+            const size_t k = (size_t)d.maxSys, nz = (size_t)std::max(1, s.nnzJ);
+            GS_CUDA(d.itVal.alloc(k * nz * 8)); GS_CUDA(d.itA.alloc(k * nz * 8)); GS_CUDA(d.itPresent.alloc(k * nz * 4));
+            GS_CUDA(d.itDiag.alloc(k * m * 4)); GS_CUDA(d.itIw.alloc(k * m * 4)); GS_CUDA(d.itVec.alloc(k * 10 * m * 8));
+            d.itSys = d.maxSys;
+        }
+        iv.m = m; iv.nnz = s.nnzJ; iv.nbr = s.nbr;
+        iv.rowPtr = d.jRowPtr.as<int>(); iv.col = d.jCol.as<int>(); iv.slot = d.jSlot.as<int>();
+        iv.ycell = d.jYcell.as<int>(); iv.pinv = d.eqPinv.as<int>(); iv.ccPtr = d.ccPtr.as<int>();
+        iv.ccOwner = d.ccOwner.as<int>(); iv.setBr = G->view.setBr; iv.outage = cur.outage;
+        iv.tol = std::min(1e-10, tol * 1e-3);  // NumericTolerances.cs:256-260
+        iv.maxIter = 4 * m + 200;
+        iv.budgetNs = 2000000000LL;  // a run that has not converged in 2 s gives up (GP_TIMEOUT)
+        iv.val = d.itVal.as<double>(); iv.a = d.itA.as<double>(); iv.present = d.itPresent.as<int>();
+        iv.diag = d.itDiag.as<int>(); iv.iw = d.itIw.as<int>(); iv.vec = d.itVec.as<double>(); iv.result = v.result;
+    }
     for (int off = 0; off < nList; off += d.maxSys) {
         const int c = std::min(d.maxSys, nList - off);
         k_gp_solve<<<c, 32, 0, st>>>(v, (const double*)cur.lu, (double*)cur.y, cur.B, dList + off, c);
+        if (iterative) {
+            k_gp_iterative<<<c, 32, 0, st>>>(iv, (const double*)cur.lu, (double*)cur.y, cur.B, dList + off, c, s.nbr);
+            *launched += 1;
+        }
         k_gp_mark<<<(c + 127) / 128, 128, 0, st>>>(cur, dList + off, v.result, c);
         *launched += 2;
     }
@@ -2381,7 +2422,7 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
                 // the partial-pivoting re-solve: the step by k_gp_solve from the Jacobian just filled
                 if (timed) cudaEventRecord(ev[2], st);
                 int gl = 0;
-                if ((rc = GpStep(G, cur, cur.activeList, nActive, st, &gl)) != GS_OK) break;
+                if ((rc = GpStep(G, cur, cur.activeList, nActive, st, &gl, true, o.tolerance)) != GS_OK) break;
                 launches += 1 + gl;
             } else {
                 launches += 1 + FewSystemsSolve<double>(g, cur, s, nActive, G->tailSplit, false, st,

@@ -79,6 +79,10 @@ struct Symbolic {
     // the matrix's own cells (the Jacobian's, or a loaded matrix's; fill left out) by column in pivot order: rows
     // aRow[aColPtr[l] .. aColPtr[l+1]) ascending, each with its LU slot; what the partial-pivoting re-solve reads
     std::vector<int32_t> aColPtr, aRow, aSlot;
+    // the Jacobian pattern in equation order (jRowPtr / jCol) for the iterative fallback of a singular step: each
+    // cell's LU slot, and the Y cell between its two buses (-1 within one bus), whose branch stamps decide whether the
+    // cell exists in a system with branches out
+    std::vector<int32_t> jSlot, jYcell;
     // ---- schedule ----
     int nLevels = 0;
     std::vector<int> level;          // per node

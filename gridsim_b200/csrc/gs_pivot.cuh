@@ -246,4 +246,243 @@ __global__ void __launch_bounds__(32) k_gp_solve(GpView v, const double* __restr
     if (lane == 0) v.result[q] = GP_OK;
 }
 
+// ---------------------------------------------------------------------------------------------
+// The step of a system whose matrix the factorisation found singular: ILU(0) with the row-relative pivot guard
+// (Numerics/Sparse.cs:232-300, NumericTolerances.Ilu0PivotGuard :226-234) and ILU-preconditioned BiCGSTAB with the
+// true-residual acceptance (Sparse.cs:305-405), tolerance min(1e-10, tol x 1e-3), at most 4 m + 200 iterations
+// (NumericTolerances.cs:256-260), as NewtonShell.SolveStep falls back to (NewtonShell.cs:96-105). It runs on the
+// Jacobian in equation order, on the cells of the system's own grid: a cell between two buses exists only while
+// one of the branches stamped into it is in service in the system (the reference rebuilds Y without the outage's
+// branches). Identity rows (a PV bus's Q row, a reference or removed bus) stay identities through ILU(0) and keep
+// their components at zero through BiCGSTAB, so the iteration is that of the reference's reduced system.
+// One warp per system, for the listed systems whose result is GP_SINGULAR: GP_ITERATIVE when BiCGSTAB is accepted,
+// else GP_SINGULAR stays; a run longer than `budgetNs` gives up as GP_TIMEOUT.
+enum : int32_t { GP_ITERATIVE = 4, GP_TIMEOUT = 5 };
+
+struct IterView {
+    int m, nnz, nbr;
+    const int* rowPtr;   // Jacobian, equation order
+    const int* col;
+    const int* slot;     // LU slot of each cell
+    const int* ycell;    // Y cell between the cell's buses, -1 within one bus
+    const int* pinv;     // equation -> pivot position (where y holds its right-hand side and solution)
+    const int* ccPtr;    // per Y cell its stamps' owners (branch, or -1 for a shunt)
+    const int* ccOwner;
+    const int* setBr;    // outage sets: kSetBranches branches each (-1 after the last), ids nbr ...
+    const int* outage;   // per system of the batch: branch, set id, or -1
+    double tol;
+    int maxIter;
+    long long budgetNs;
+    double* val;         // [nnz] per listed system: ILU(0) values
+    double* a;           // [nnz] the matrix's values
+    int* present;        // [nnz]
+    int* diag;           // [m]
+    int* iw;             // [m]
+    double* vec;         // [10 m]: x r rhat p v s t ph sh b
+    int* result;
+};
+
+__device__ __forceinline__ long long gpNowNs() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return (long long)t;
+}
+
+// Sums in the reference's order (index order, one accumulator): the null-space component of a singular system's
+// BiCGSTAB solution follows its rounding, so the reductions keep the reference's sequence. Lane 0 sums; all get it.
+// Products and sums rounded one by one (no fused multiply-add), as the reference's C# evaluates them
+__device__ __forceinline__ double fmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double fadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double fsub(double a, double b) { return __dsub_rn(a, b); }
+
+__device__ double gpDot(const double* a, const double* b, int m, int lane) {
+    double t = 0.0;
+    if (lane == 0)
+        for (int i = 0; i < m; i++) t = fadd(t, fmul(a[i], b[i]));
+    return __shfl_sync(0xffffffffu, t, 0);
+}
+
+__device__ void gpSpMV(const IterView& v, const double* A, const int* pres, const double* x, double* y, int lane) {
+    for (int i = lane; i < v.m; i += 32) {
+        double t = 0.0;
+        for (int q = v.rowPtr[i]; q < v.rowPtr[i + 1]; q++)
+            if (pres[q]) t = fadd(t, fmul(A[q], x[v.col[q]]));
+        y[i] = t;
+    }
+    __syncwarp();
+}
+
+// z = (LU)^-1 r with the ILU(0) factors (Ilu0.Apply): rows in order, then in reverse, each row's terms subtracted
+// one by one in the reference's order (lane 0)
+__device__ void gpIluApply(const IterView& v, const double* lu, const int* pres, const int* diag, const double* r,
+                           double* z, int lane) {
+    if (lane == 0) {
+        for (int i = 0; i < v.m; i++) {
+            double t = r[i];
+            for (int q = v.rowPtr[i]; q < diag[i]; q++)
+                if (pres[q]) t = fsub(t, fmul(lu[q], z[v.col[q]]));
+            z[i] = t;
+        }
+        for (int i = v.m - 1; i >= 0; i--) {
+            double t = z[i];
+            for (int q = diag[i] + 1; q < v.rowPtr[i + 1]; q++)
+                if (pres[q]) t = fsub(t, fmul(lu[q], z[v.col[q]]));
+            z[i] = t / lu[diag[i]];
+        }
+    }
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(32) k_gp_iterative(IterView v, const double* __restrict__ lu, double* y, int B,
+                                                     const int* list, int nList, int nbrSet) {
+    const int q = blockIdx.x;
+    if (q >= nList || v.result[q] != GP_SINGULAR) return;
+    const long long t0 = gpNowNs();
+    const int s = list ? list[q] : q;
+    const int lane = threadIdx.x;
+    const int m = v.m, nnz = v.nnz;
+    const size_t Bz = (size_t)B;
+    double* val = v.val + (size_t)q * nnz;
+    double* A = v.a + (size_t)q * nnz;
+    int* pres = v.present + (size_t)q * nnz;
+    int* diag = v.diag + (size_t)q * m;
+    int* iw = v.iw + (size_t)q * m;
+    double* x = v.vec + (size_t)q * 10 * m;
+    double *r = x + m, *rhat = r + m, *p = rhat + m, *vv = p + m, *sv = vv + m, *t = sv + m, *ph = t + m, *sh = ph + m,
+           *b = sh + m;
+    // the outage's branches
+    const int o = v.outage[s];
+    int outBr[kSetBranches];
+    int nOut = 0;
+    if (o >= 0 && o < nbrSet) outBr[nOut++] = o;
+    else if (o >= nbrSet)
+        for (int j = 0; j < kSetBranches; j++) {
+            const int br = v.setBr[(size_t)kSetBranches * (o - nbrSet) + j];
+            if (br < 0) break;
+            outBr[nOut++] = br;
+        }
+    // the cells of the system's own grid, their values
+    for (int c = lane; c < nnz; c += 32) {
+        int here = 1;
+        const int yc = v.ycell[c];
+        if (yc >= 0 && nOut > 0) {
+            here = 0;
+            for (int e = v.ccPtr[yc]; e < v.ccPtr[yc + 1] && !here; e++) {
+                const int ow = v.ccOwner[e];
+                bool gone = false;
+                for (int j = 0; j < nOut; j++) gone |= ow == outBr[j];
+                if (!gone) here = 1;
+            }
+        }
+        pres[c] = here;
+        A[c] = lu[(size_t)v.slot[c] * Bz + s];
+        val[c] = A[c];
+    }
+    int noDiag = 0;
+    for (int i = lane; i < m; i += 32) {
+        iw[i] = -1;
+        b[i] = y[(size_t)v.pinv[i] * Bz + s];
+        int d = -1;
+        for (int c = v.rowPtr[i]; c < v.rowPtr[i + 1]; c++)
+            if (v.col[c] == i) d = c;
+        diag[i] = d;
+        noDiag |= d < 0;
+    }
+    if (__any_sync(0xffffffffu, noDiag)) return;  // every Jacobian row holds its diagonal cell; stays GP_SINGULAR
+    __syncwarp();
+    // ILU(0) (Ilu0.Factor)
+    for (int i = 0; i < m; i++) {
+        const int r0 = v.rowPtr[i], r1 = v.rowPtr[i + 1];
+        for (int c = r0 + lane; c < r1; c += 32)
+            if (pres[c]) iw[v.col[c]] = c;
+        __syncwarp();
+        for (int k = r0; k < diag[i]; k++) {
+            if (!pres[k]) continue;
+            const int j = v.col[k];
+            const double piv = val[diag[j]];
+            const double lij = piv != 0.0 ? val[k] / piv : 0.0;
+            __syncwarp();
+            if (lane == 0) val[k] = lij;
+            __syncwarp();
+            if (lij == 0.0) continue;
+            for (int kk = diag[j] + 1 + lane; kk < v.rowPtr[j + 1]; kk += 32) {
+                if (!pres[kk]) continue;
+                const int pos = iw[v.col[kk]];
+                if (pos != -1) val[pos] = fsub(val[pos], fmul(lij, val[kk]));
+            }
+            __syncwarp();
+        }
+        double rs = 0.0;
+        for (int c = r0 + lane; c < r1; c += 32)
+            if (pres[c]) rs = fmax(rs, fabs(A[c]));
+        for (int o2 = 16; o2 > 0; o2 >>= 1) rs = fmax(rs, __shfl_xor_sync(0xffffffffu, rs, o2));
+        const double guard = 1e-12 * (rs > 0.0 ? rs : 1.0);
+        const double d = val[diag[i]];
+        __syncwarp();
+        if (lane == 0 && fabs(d) < guard) val[diag[i]] = d < 0 ? -guard : guard;
+        for (int c = r0 + lane; c < r1; c += 32)
+            if (pres[c]) iw[v.col[c]] = -1;
+        __syncwarp();
+    }
+    // BiCGSTAB (BiCgStab)
+    for (int i = lane; i < m; i += 32) {
+        x[i] = 0.0; r[i] = b[i]; rhat[i] = b[i]; p[i] = 0.0; vv[i] = 0.0;
+    }
+    __syncwarp();
+    const double bnorm = sqrt(gpDot(b, b, m, lane));
+    int ok = 0;
+    if (bnorm == 0.0) {
+        ok = 1;  // b is zero (a NaN makes bnorm NaN, which fails below)
+    } else {
+        auto trueResidual = [&]() {
+            gpSpMV(v, A, pres, x, t, lane);
+            double sum = 0.0;
+            if (lane == 0)
+                for (int i = 0; i < m; i++) { const double d = b[i] - t[i]; sum = fadd(sum, fmul(d, d)); }
+            sum = __shfl_sync(0xffffffffu, sum, 0);
+            return sqrt(sum) / bnorm < v.tol ? 1 : 0;
+        };
+        double rho = 1.0, alpha = 1.0, omega = 1.0;
+        for (int it = 0; it < v.maxIter; it++) {
+            if (gpNowNs() - t0 > v.budgetNs) { ok = -1; break; }
+            const double rhoNew = gpDot(rhat, r, m, lane);
+            if (fabs(rhoNew) < 1e-300 || isnan(rhoNew)) break;
+            const double beta = (rhoNew / rho) * (alpha / omega);
+            for (int i = lane; i < m; i += 32) p[i] = fadd(r[i], fmul(beta, fsub(p[i], fmul(omega, vv[i]))));
+            __syncwarp();
+            gpIluApply(v, val, pres, diag, p, ph, lane);
+            gpSpMV(v, A, pres, ph, vv, lane);
+            const double rhatV = gpDot(rhat, vv, m, lane);
+            if (rhatV == 0.0 || isnan(rhatV)) break;
+            alpha = rhoNew / rhatV;
+            for (int i = lane; i < m; i += 32) sv[i] = fsub(r[i], fmul(alpha, vv[i]));
+            __syncwarp();
+            if (sqrt(gpDot(sv, sv, m, lane)) / bnorm < v.tol) {
+                for (int i = lane; i < m; i += 32) x[i] = fadd(x[i], fmul(alpha, ph[i]));
+                __syncwarp();
+                ok = trueResidual();
+                break;
+            }
+            gpIluApply(v, val, pres, diag, sv, sh, lane);
+            gpSpMV(v, A, pres, sh, t, lane);
+            const double tt = gpDot(t, t, m, lane);
+            omega = tt > 0 ? gpDot(t, sv, m, lane) / tt : 0.0;
+            for (int i = lane; i < m; i += 32) {
+                x[i] = fadd(x[i], fadd(fmul(alpha, ph[i]), fmul(omega, sh[i])));
+                r[i] = fsub(sv[i], fmul(omega, t[i]));
+            }
+            __syncwarp();
+            rho = rhoNew;
+            if (sqrt(gpDot(r, r, m, lane)) / bnorm < v.tol) { ok = trueResidual(); break; }
+            if (omega == 0.0) break;
+        }
+    }
+    if (ok == 1) {
+        for (int i = lane; i < m; i += 32) y[(size_t)v.pinv[i] * Bz + s] = x[i];
+        if (lane == 0) v.result[q] = GP_ITERATIVE;
+    } else if (ok < 0 && lane == 0) {
+        v.result[q] = GP_TIMEOUT;
+    }
+}
+
 }  // namespace gs

@@ -267,6 +267,23 @@ std::string Analyze(const HostGrid& g, Symbolic& s, bool qlim) {
         }
         // which LU slots hold a Jacobian value (the rest are fill, which start from zero)
         for (int v : s.ySlot) if (v >= 0) hasA[v] = 1;
+        // the Jacobian's cells in equation order: LU slot, and the Y cell between their buses
+        std::vector<int> eqBus(m, -1);
+        for (int i = 0; i < n; i++) {
+            if (s.pPos[i] >= 0) eqBus[s.pPos[i]] = i;
+            if (s.qPos[i] >= 0) eqBus[s.qPos[i]] = i;
+        }
+        s.jSlot.assign(s.nnzJ, -1);
+        s.jYcell.assign(s.nnzJ, -1);
+        for (int r = 0; r < m; r++)
+            for (int q = s.jRowPtr[r]; q < s.jRowPtr[r + 1]; q++) {
+                const int c = s.jCol[q];
+                s.jSlot[q] = (int32_t)slotOf(s.pinv[r], s.pinv[c]);
+                const int bi = eqBus[r], bj = eqBus[c];
+                if (bi == bj) continue;
+                for (int p = s.yRowPtr[bi]; p < s.yRowPtr[bi + 1]; p++)
+                    if (s.yCol[p] == bj) { s.jYcell[q] = p; break; }
+            }
     });
 }
 

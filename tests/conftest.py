@@ -35,13 +35,21 @@ def study_opts():
     return o
 
 
+# A part without a reference bus is solved, as in the reference, through the singular-step fallback (ILU(0) +
+# BiCGSTAB): its common angle offset comes from the iteration's rounding, amplified along the null space. With the
+# engine running that fallback in the reference's order and roundings, the offsets agree within 2.1e-8 rad on every
+# such outage of the tests; the bound below holds them to that, beside the 1e-8 bar on the in-part differences.
+FLOATING_PART_ABS_TOL_RAD = 1e-7
+
+
 def assert_states_close(m, removed_branches, gpu_vm, gpu_va_deg, ref_vm, ref_va_deg, vm_tol, va_tol_rad, removed_bus=-1):
     """Voltage magnitudes within vm_tol, angles within va_tol_rad, on the buses of the reduced grid.
 
     A connected part left with no reference bus by the outage, that still balances (a synchronous condenser or a
     zero-injection pair cut off, for example), has angles fixed only up to a common offset: every offset solves its
     equations, and the reference's linear solver and this engine leave it at different ones. There the angles are
-    compared as differences from the part's first bus; everywhere else absolutely."""
+    compared as differences from the part's first bus (and absolutely within FLOATING_PART_ABS_TOL_RAD); everywhere
+    else absolutely."""
     n = m.n_bus
     parent = list(range(n))
 
@@ -69,10 +77,11 @@ def assert_states_close(m, removed_branches, gpu_vm, gpu_va_deg, ref_vm, ref_va_
         first.setdefault(root[i], i)
     for i in keep:
         if root[i] in slack_parts:
-            assert abs(ga[i] - ra[i]) <= va_tol_rad, i
+            assert abs(ga[i] - ra[i]) <= va_tol_rad, (i, ga[i] - ra[i])
         else:
             f = first[root[i]]
             assert abs((ga[i] - ga[f]) - (ra[i] - ra[f])) <= va_tol_rad, i
+            assert abs(ga[i] - ra[i]) <= FLOATING_PART_ABS_TOL_RAD, (i, ga[i] - ra[i])
 
 
 def resistive_leaf_grid(at_bus: int = 4, r: float = 0.05):
