@@ -342,8 +342,10 @@ def run_ours(args):
     # this rank's shard (what its GPU screens); the accuracy check and the CPU legs run on it
     idx = rows[balanced_shards(costs, world)[rank]] if world > 1 else rows
 
+    solvers = {}
+
     def screen(precision, timing=False):
-        s = SparseNewtonRaphsonPowerFlow(precision, ctx)
+        s = solvers.get(precision) or SparseNewtonRaphsonPowerFlow(precision, ctx)
         return s, ContingencyAnalysis.screen_raw(m, idx, s, options(precision, timing))
 
     def barrier():
@@ -356,8 +358,12 @@ def run_ours(args):
     precs = ("mixed", "fp64") if args.precision == "both" else (args.precision,)
     for prec in precs:
         solver = SparseNewtonRaphsonPowerFlow(prec, ctx)
+        solvers[prec] = solver
         opt = options(prec)
         own = {}
+        # the grid's schedule (few-systems threshold, level-group cuts), autotuned on the rank's shard before the
+        # warm-up (untimed; a 1,000-outage sample picked schedules that were no faster on the whole screen)
+        tune = ContingencyAnalysis.tune_screen(m, idx, solver, opt) if not args.no_tune else None
 
         def screen_shard(mm, ii):
             own["r"] = ContingencyAnalysis.screen_raw(mm, ii, solver, opt)
@@ -387,9 +393,17 @@ def run_ours(args):
             dev_t, wall_t = float(t[0]), float(t[1])
         # every rank holds the merged screen of all rows: its converged count is the job's
         total_conv = float(sum(conv))
+        if tune is not None:
+            # one untimed screen of the rank's shard under the default schedule, beside the tuned one's timed steps
+            grid = solver.grid_for(m, opt)
+            tuned = grid.schedule()
+            grid.set_schedule()
+            tune["default_screen_ms"] = float(ContingencyAnalysis.screen_raw(m, idx, solver, opt)["device_ms"])
+            grid.set_schedule(**tuned)
+            tune["tuned_screen_ms"] = float(np.mean(dev) * 1e3)
         results[prec] = dict(value=total_conv / dev_t, e2e=total_conv / wall_t, ms=dev_t / args.steps * 1e3,
                              wall_ms=wall_t / args.steps * 1e3, conv=conv[-1], launches=launches[-1],
-                             clocks=sampler.summary(), last=r)
+                             clocks=sampler.summary(), last=r, schedule=tune)
     # phase timing (one extra untimed screen) for the roofline of the dominant kernel
     _, prof = screen("mixed", timing=True)
     peak, peak_kind = load_peaks()
@@ -469,6 +483,7 @@ def run_ours(args):
             "phase_ms": {"factor": prof["factor_ms"], "solve": prof["solve_ms"], "mismatch": prof["mismatch_ms"],
                          "other": prof["other_ms"], "few_systems_path": prof["tail_ms"],
                          "full_batch_factor": prof["level_factor_ms"]},
+            "schedule": {p: results[p]["schedule"] for p in results},
             "cpu_baseline": cpu, "clocks": mx["clocks"], "gpu_launches": mx["launches"], "accuracy_vs_oracle": acc,
             "serve_p99_ms": head["p99_ms"] if head else None,
             "serve_rate_rps": SERVE_HEADLINE_RATE if head else None,
@@ -490,6 +505,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="keep the grids' default schedule (no autotuning)")
     ap.add_argument("--outages", type=int, default=N_OUTAGES,
                     help="screen the first K of the 5,000 sampled outages (small cases for profiling)")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],

@@ -87,6 +87,11 @@ class GridInfo(ctypes.Structure):
     ]
 
 
+class Schedule(ctypes.Structure):
+    _fields_ = [("factor_cut", c_i32), ("solve_cut", c_i32), ("tail_max", c_i32), ("candidates", c_i32),
+                ("default_ms", c_f64), ("tuned_ms", c_f64), ("reserved", c_i32 * 4)]
+
+
 class MultiStats(ctypes.Structure):
     _fields_ = [("device_ms", c_f64), ("tune_ms", c_f64), ("threads_per_cta", c_i32), ("ctas", c_i32),
                 ("items", c_i32), ("tuned_now", c_i32), ("system_steps", ctypes.c_int64), ("shared_top", c_i32),
@@ -133,6 +138,9 @@ EXPORTS = {
     "gs_nk_screen": (c_i32, [c_vp, c_i32, c_i32, c_vp, ctypes.POINTER(PfOpts), ctypes.POINTER(N1Result)]),
     "gs_element_screen": (c_i32, [c_vp, c_i32, c_vp, c_vp, ctypes.POINTER(PfOpts), ctypes.POINTER(N1Result)]),
     "gs_analyze_host": (c_i32, [ctypes.POINTER(GridDesc), ctypes.POINTER(GridInfo)]),
+    "gs_grid_schedule_get": (c_i32, [c_vp, ctypes.POINTER(Schedule)]),
+    "gs_grid_schedule_set": (c_i32, [c_vp, ctypes.POINTER(Schedule)]),
+    "gs_screen_tune": (c_i32, [c_vp, c_i32, c_vp, ctypes.POINTER(PfOpts), ctypes.POINTER(Schedule)]),
     "gs_outage_topology": (c_i32, [ctypes.POINTER(GridDesc), c_f64, c_i32, c_vp, c_vp, c_vp]),
     "gs_sparse_solve_batch": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "gs_pf_mismatch_noalloc": (c_i32, [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp]),

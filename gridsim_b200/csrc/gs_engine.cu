@@ -1686,6 +1686,24 @@ struct GpData {
     bool itUploaded = false;
 };
 
+// The full-batch step's CUDA graphs, kept across calls: a graph is replayed while every launch it holds would be the
+// same (the key: the kernels' by-value arguments, the batch parts and the launch shapes), and captured again
+// otherwise. Capture and instantiation of a step's ~1,400 launches is host work the device waits for.
+struct StepGraphCache {
+    std::vector<unsigned char> key;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    int64_t launches[2] = {0, 0};
+    StepGraphCache() = default;
+    StepGraphCache(const StepGraphCache&) = delete;
+    StepGraphCache& operator=(const StepGraphCache&) = delete;
+    ~StepGraphCache() { release(); }
+    void release() {
+        for (auto& x : exec)
+            if (x) { cudaGraphExecDestroy(x); x = nullptr; }
+        key.clear();
+    }
+};
+
 }  // namespace gs
 
 struct MatrixPattern;  // an analysed sparse-matrix pattern of the batched linear solve (kept per context)
@@ -1729,6 +1747,9 @@ struct gs_grid {
     // few-systems path with k_gp_solve in place of the static factorisation
     bool gpMode = false;
     gs::GpData gp;
+    // the level-group cut and few-systems threshold in force (gs::SetSchedule; gs_screen_tune picks them)
+    gs_schedule sched{2, 2, gs::kTailMaxSystems, 0, 0.0, 0.0, {0, 0, 0, 0}};
+    gs::StepGraphCache stepGraphs[2];  // the full-batch step's graphs: [0] the whole batch, [1] the mid workspace
 };
 
 struct MatrixPattern {
@@ -1767,6 +1788,41 @@ int Upload(gs_grid* G, const std::vector<X>& v, const X** out) {
     *out = buf->as<X>();
     G->bufs.push_back(std::move(buf));
     return GS_OK;
+}
+
+// The grid's level-group cut and few-systems threshold. The persistent kernels take every level from the first
+// one whose phases (and those of all levels above it) hold at most factorCut x kPersistWarps items (the
+// factorisation, on the items of its two phases and of the backward substitution) or solveCut x kPersistWarps
+// items (the triangular solves); the levels below run one launch per level and phase. The few-systems path takes
+// over once at most tailMax systems still step.
+void SetSchedule(gs_grid* G, const gs_schedule& sc) {
+    const Symbolic& s = G->sym;
+    G->sched = sc;
+    G->tailMax = std::max(1, std::min(kTailMaxSystems, sc.tail_max));
+    const int fCut = sc.factor_cut * kPersistWarps, sCut = sc.solve_cut * kPersistWarps;
+    auto cuts = [&](const Symbolic::Schedule& f, const Symbolic::Schedule& b, const Symbolic::Schedule& v, int nLv,
+                    int& split, int& splitB) {
+        split = nLv;
+        for (int l = nLv - 1; l >= 0; l--) {
+            const auto& fp = f.levelItemPtr;
+            const int a = fp[2 * l + 1] - fp[2 * l], bb = fp[2 * l + 2] - fp[2 * l + 1];
+            const int c = b.levelItemPtr[l + 1] - b.levelItemPtr[l];
+            if (std::max(std::max(a, bb), c) > fCut) break;
+            split = l;
+        }
+        // the solves have one item per level for a few nodes (short pieces packed), so their persistent walk can
+        // start lower in the tree than the factorisation's
+        splitB = nLv;
+        for (int l = nLv - 1; l >= 0; l--) {
+            const int c = b.levelItemPtr[l + 1] - b.levelItemPtr[l];
+            const int vv = v.levelItemPtr[l + 1] - v.levelItemPtr[l];
+            if (std::max(c, vv) > sCut) break;
+            splitB = l;
+        }
+        splitB = std::min(splitB, split);
+    };
+    cuts(s.factor, s.backward, s.forward, s.nLevels, G->split, G->splitB);
+    if (s.ps.on) cuts(s.ps.factor, s.ps.backward, s.ps.forward, s.ps.nLevels, G->psSplit, G->psSplitB);
 }
 
 int UploadGrid(gs_grid* G) {
@@ -1884,30 +1940,10 @@ int UploadGrid(gs_grid* G) {
         UP(P.factor.levelWide, pfWide); UP(P.backward.levelWide, pbWide); UP(P.forward.levelWide, pvWide);
         UP(P.factor.levelMid, pfMid); UP(P.backward.levelMid, pbMid); UP(P.forward.levelMid, pvMid);
         v.psLevels = P.nLevels;
-        // the persistent walks' first levels, as for the scalar schedule below
-        G->psSplit = P.nLevels;
-        for (int l = P.nLevels - 1; l >= 0; l--) {
-            const auto& fp = P.factor.levelItemPtr;
-            const int a = fp[2 * l + 1] - fp[2 * l], b2 = fp[2 * l + 2] - fp[2 * l + 1];
-            const int c = P.backward.levelItemPtr[l + 1] - P.backward.levelItemPtr[l];
-            if (std::max(std::max(a, b2), c) > 2 * kPersistWarps) break;
-            G->psSplit = l;
-        }
-        G->psSplitB = P.nLevels;
-        for (int l = P.nLevels - 1; l >= 0; l--) {
-            const int c = P.backward.levelItemPtr[l + 1] - P.backward.levelItemPtr[l];
-            const int vv = P.forward.levelItemPtr[l + 1] - P.forward.levelItemPtr[l];
-            if (std::max(c, vv) > 2 * kPersistWarps) break;
-            G->psSplitB = l;
-        }
-        G->psSplitB = std::min(G->psSplitB, G->psSplit);
     }
 #undef UP
-    // the persistent kernels take every level from the first one whose items (and those of all levels above
-    // it) fit twice in a CTA's warps in each phase; the wide levels below run one launch per level and phase
     // the few-systems path runs the lowest levels as per-level launches while a phase of them holds more short
     // pieces than one CTA's threads (more than one round of a one-system walk)
-    if (const char* e = std::getenv("GS_TAIL_MAX")) G->tailMax = std::max(0, std::min(kTailMaxSystems, std::atoi(e)));
     G->tailSplit = 0;
     for (int l = 0; l < s.nLevels; l++) {
         bool wideLevel = false;
@@ -1919,24 +1955,7 @@ int UploadGrid(gs_grid* G) {
         if (!wideLevel) break;
         G->tailSplit = l + 1;
     }
-    G->split = s.nLevels;
-    for (int l = s.nLevels - 1; l >= 0; l--) {
-        const auto& fp = s.factor.levelItemPtr;
-        const int a = fp[2 * l + 1] - fp[2 * l], bb = fp[2 * l + 2] - fp[2 * l + 1];
-        const int c = s.backward.levelItemPtr[l + 1] - s.backward.levelItemPtr[l];
-        if (std::max(std::max(a, bb), c) > 2 * kPersistWarps) break;
-        G->split = l;
-    }
-    // the solves have one item per level for a few nodes (short pieces packed), so their persistent walk can start
-    // lower in the tree than the factorisation's
-    G->splitB = s.nLevels;
-    for (int l = s.nLevels - 1; l >= 0; l--) {
-        const int c = s.backward.levelItemPtr[l + 1] - s.backward.levelItemPtr[l];
-        const int v = s.forward.levelItemPtr[l + 1] - s.forward.levelItemPtr[l];
-        if (std::max(c, v) > 2 * kPersistWarps) break;
-        G->splitB = l;
-    }
-    G->splitB = std::min(G->splitB, G->split);
+    SetSchedule(G, G->sched);
     return GS_OK;
 }
 
@@ -2316,8 +2335,25 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
     cudaError_t ce = cudaSuccess;
     // (re)capture the step graphs for stepB (its parts set)
     auto captureStep = [&]() -> int {
-        for (auto& x : exec) if (x) { cudaGraphExecDestroy(x); x = nullptr; }
+        exec[0] = exec[1] = nullptr;
         if (timed || G->gpMode) return GS_OK;  // the partial-pivoting re-solve never takes a full-batch step
+        // the graphs of the last call on this workspace are replayed when they hold the same launches
+        StepGraphCache& gc = G->stepGraphs[stepB.lu == b.lu ? 0 : 1];
+        std::vector<unsigned char> key;
+        auto put = [&](const void* p, size_t n) {
+            const unsigned char* c = static_cast<const unsigned char*>(p);
+            key.insert(key.end(), c, c + n);
+        };
+        const int shape[8] = {(int)sizeof(T), refine, parts, persistWarps, split, splitB, pairedOn ? 1 : 0, nLv};
+        put(shape, sizeof shape);
+        put(&g, sizeof g);
+        put(&stepB, sizeof stepB);
+        for (int q = 0; q < parts; q++) put(&hb[q], sizeof hb[q]);
+        if (gc.exec[0] && gc.key == key) {
+            for (int r = 0; r <= refine; r++) { exec[r] = gc.exec[r]; launchesPerStep[r] = gc.launches[r]; }
+            return GS_OK;
+        }
+        gc.release();
         for (int r = 0; r <= refine; r++) {
             cudaGraph_t graph;
             stepLaunches = 0;
@@ -2329,16 +2365,20 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             updatePhase(r != 0);
             ce = cudaStreamEndCapture(st, &graph);
             if (ce == cudaSuccess) {
-                ce = cudaGraphInstantiate(&exec[r], graph, 0);
+                ce = cudaGraphInstantiate(&gc.exec[r], graph, 0);
                 cudaGraphDestroy(graph);
             }
-            if (ce != cudaSuccess) return SetErr(ctx, GS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
-            launchesPerStep[r] = stepLaunches;
+            if (ce != cudaSuccess) {
+                gc.release();
+                return SetErr(ctx, GS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+            }
+            gc.launches[r] = launchesPerStep[r] = stepLaunches;
+            exec[r] = gc.exec[r];
         }
+        gc.key = std::move(key);
         return GS_OK;
     };
     if (int rcCap = captureStep(); rcCap != GS_OK) {
-        for (auto& x : exec) if (x) cudaGraphExecDestroy(x);
         cudaEventDestroy(evFork);
         for (auto& e : evJoin) cudaEventDestroy(e);
         return rcCap;
@@ -2528,7 +2568,6 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
         stats->levelFactorBytes += (double)levelSys * (double)sizeof(T) * ((double)s.nnzJ + (double)s.nnzLU);
         stats->tailMs += tMs;
     }
-    for (auto& x : exec) if (x) cudaGraphExecDestroy(x);
     cudaEventDestroy(evFork);
     for (auto& e : evJoin) cudaEventDestroy(e);
     cudaEventRecord(e1, st);
@@ -3051,6 +3090,95 @@ int gs_grid_destroy(gs_grid* g) {
 int gs_grid_info_get(gs_grid* g, gs_grid_info* info) {
     if (!g || !info) return GS_ERR_INVALID_ARG;
     FillInfo(g->host, g->sym, info);
+    return GS_OK;
+}
+
+int gs_grid_schedule_get(gs_grid* g, gs_schedule* out) {
+    if (!g || !out) return GS_ERR_INVALID_ARG;
+    *out = g->sched;
+    return GS_OK;
+}
+
+int gs_grid_schedule_set(gs_grid* g, const gs_schedule* sc) {
+    if (!g || !sc) return GS_ERR_INVALID_ARG;
+    if (sc->factor_cut < 1 || sc->solve_cut < 1 || sc->tail_max < 1)
+        return SetErr(g->ctx, GS_ERR_INVALID_ARG, "schedule: factor_cut, solve_cut and tail_max must be at least 1");
+    gs_schedule c = *sc;
+    c.tail_max = std::min(c.tail_max, kTailMaxSystems);
+    SetSchedule(g, c);
+    return GS_OK;
+}
+
+int gs_screen_tune(gs_grid* G0, int32_t nOut, const int32_t* idx, const gs_pf_opts* opts, gs_schedule* out) {
+    if (!G0 || nOut <= 0 || !idx || !out) return GS_ERR_INVALID_ARG;
+    gs_ctx* ctx = G0->ctx;
+    int rc = CheckOpts(ctx, opts);
+    if (rc) return rc;
+    gs_pf_opts o = *opts;
+    if (o.flat_start) return SetErr(ctx, GS_ERR_UNSUPPORTED, "flat_start: pass a flat start in the descriptor");
+    if (o.partial_pivoting) return SetErr(ctx, GS_ERR_UNSUPPORTED, "partial_pivoting steps on no batched schedule");
+    o.phase_timing = 0;
+    GS_CUDA(cudaSetDevice(ctx->device));
+    gs_grid* G = G0;
+    if (o.enforce_q_limits && (rc = QGridOf(G0, &G)) != GS_OK) return rc;
+    const Symbolic& s = G->sym;
+    for (int k = 0; k < nOut; k++)
+        if (idx[k] < 0 || idx[k] >= s.nbr || !G->host.brOn[idx[k]])
+            return SetErr(ctx, GS_ERR_INVALID_ARG, "outage index out of range or out of service");
+    G->view.qlimOn = o.enforce_q_limits ? 1 : 0;
+    const bool warm = o.warm_start_from_base != 0;
+    if (warm) {
+        int bst = 0, bit = 0;
+        double bmis = 0;
+        float bms = 0;
+        if ((rc = SolveBase(G, o, &bst, &bit, &bmis, &bms)) != GS_OK) return rc;
+    }
+    const int B = ChooseB(G, nOut, o);
+    const int cnt = std::min(B, (int)nOut);
+    if ((rc = EnsureWorkspace(G, B, o.precision, false, false)) != GS_OK) return rc;
+    std::vector<int> outs(B, -1);
+    std::copy(idx, idx + cnt, outs.begin());
+    GS_CUDA(cudaMemcpy(G->ws.outage.p, outs.data(), (size_t)B * 4, cudaMemcpyHostToDevice));
+    int timed = 0;
+    // the sample's Newton batch under one schedule: the best device time of two runs
+    auto run = [&](const gs_schedule& sc, float* best) -> int {
+        SetSchedule(G, sc);
+        *best = 3.0e38f;
+        for (int r = 0; r < 2; r++) {
+            float ms = 0;
+            const int rc2 = NewtonDispatch(G, cnt, false, warm, o, &ms);
+            if (rc2) return rc2;
+            *best = std::min(*best, ms);
+        }
+        timed++;
+        return GS_OK;
+    };
+    const gs_schedule before = G->sched;
+    gs_schedule best = before;
+    float base = 0;
+    if ((rc = run(before, &base)) != GS_OK) return rc;
+    float bestMs = base;
+    // coordinate descent: the few-systems threshold, then the factorisation's cut, then the solves' cut
+    const int tails[3] = {74, 148, kTailMaxSystems};
+    const int cutOpts[3] = {1, 2, 4};
+    for (int dim = 0; dim < 3; dim++) {
+        const gs_schedule start = best;
+        for (int k = 0; k < 3; k++) {
+            gs_schedule c = start;
+            if (dim == 0) c.tail_max = tails[k];
+            else if (dim == 1) c.factor_cut = cutOpts[k];
+            else c.solve_cut = cutOpts[k];
+            if (c.tail_max == start.tail_max && c.factor_cut == start.factor_cut && c.solve_cut == start.solve_cut) continue;
+            float ms = 0;
+            if ((rc = run(c, &ms)) != GS_OK) { SetSchedule(G, before); return rc; }
+            if (ms < bestMs) { bestMs = ms; best = c; }
+        }
+    }
+    best.candidates = timed;
+    best.default_ms = base;
+    best.tuned_ms = bestMs;
+    SetSchedule(G, best);
+    *out = best;
     return GS_OK;
 }
 

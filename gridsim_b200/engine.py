@@ -184,6 +184,18 @@ class CudaGrid:
         self.ctx.check(self.ctx.lib.gs_grid_info_get(self.handle, ctypes.byref(i)), "gs_grid_info_get")
         return i
 
+    def schedule(self) -> dict:
+        """The batched-solve schedule in force (gs_grid_schedule_get): factor_cut, solve_cut, tail_max."""
+        sc = _abi.Schedule()
+        self.ctx.check(self.ctx.lib.gs_grid_schedule_get(self.handle, ctypes.byref(sc)), "gs_grid_schedule_get")
+        return {"factor_cut": sc.factor_cut, "solve_cut": sc.solve_cut, "tail_max": sc.tail_max}
+
+    def set_schedule(self, factor_cut: int = 2, solve_cut: int = 2, tail_max: int = 296) -> None:
+        """gs_grid_schedule_set; the defaults are the schedule a grid starts with."""
+        sc = _abi.Schedule()
+        sc.factor_cut, sc.solve_cut, sc.tail_max = int(factor_cut), int(solve_cut), int(tail_max)
+        self.ctx.check(self.ctx.lib.gs_grid_schedule_set(self.handle, ctypes.byref(sc)), "gs_grid_schedule_set")
+
     def close(self) -> None:
         if self.handle:
             self.ctx.lib.gs_grid_destroy(self.handle)
@@ -677,6 +689,21 @@ class ContingencyAnalysis:
         """One ``gs_n1_screen`` call; returns the raw arrays (status, iterations, violation CSR, ...)."""
         idx = np.ascontiguousarray(branch_indices, dtype=np.int32)
         return ContingencyAnalysis._screen_call(model, idx, None, solver, options, keep_states)
+
+    @staticmethod
+    def tune_screen(model: GridModel, branch_indices: Sequence[int], solver: SparseNewtonRaphsonPowerFlow,
+                    options: PowerFlowOptions) -> dict:
+        """``gs_screen_tune``: time the candidate schedules (few-systems threshold, factorisation and solve cuts) on
+        the Newton batch of these outages under `options` and keep the fastest on the solver's grid for its later
+        screens. Returns the schedule chosen, the candidates timed and the sample's device time before and after."""
+        g = solver.grid_for(model, options)
+        idx = np.ascontiguousarray(branch_indices, dtype=np.int32)
+        sc = _abi.Schedule()
+        c = options.device_c()
+        g.ctx.check(g.ctx.lib.gs_screen_tune(g.handle, idx.shape[0], _p(idx), ctypes.byref(c), ctypes.byref(sc)),
+                    "gs_screen_tune")
+        return {"factor_cut": sc.factor_cut, "solve_cut": sc.solve_cut, "tail_max": sc.tail_max,
+                "candidates": sc.candidates, "default_ms": sc.default_ms, "tuned_ms": sc.tuned_ms}
 
     @staticmethod
     def screen_sets_raw(model: GridModel, branch_sets, solver: SparseNewtonRaphsonPowerFlow,

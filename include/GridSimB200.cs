@@ -123,6 +123,15 @@ namespace GridSim.Core.PowerFlow.B200
             public fixed int Reserved[7];
         }
 
+        // a grid's batched-solve schedule (no counterpart in the reference); gs_screen_tune picks it
+        [StructLayout(LayoutKind.Sequential)]
+        public struct Schedule
+        {
+            public int FactorCut, SolveCut, TailMax, Candidates;
+            public double DefaultMs, TunedMs;
+            public fixed int Reserved[4];
+        }
+
         [StructLayout(LayoutKind.Sequential)]
         public struct MultiStats
         {
@@ -177,6 +186,10 @@ namespace GridSim.Core.PowerFlow.B200
         [DllImport(Lib)] public static extern int gs_grid_destroy(IntPtr grid);
         [DllImport(Lib)] public static extern int gs_grid_info_get(IntPtr grid, out GridInfo info);
         [DllImport(Lib)] public static extern int gs_analyze_host(ref GridDesc desc, out GridInfo info);
+        [DllImport(Lib)] public static extern int gs_grid_schedule_get(IntPtr grid, out Schedule sched);
+        [DllImport(Lib)] public static extern int gs_grid_schedule_set(IntPtr grid, ref Schedule sched);
+        [DllImport(Lib)] public static extern int gs_screen_tune(IntPtr grid, int nOut, int[] branchIdx, ref PfOpts opts,
+            out Schedule sched);
 
         // solves and screens
         [DllImport(Lib)] public static extern int gs_pf_solve(IntPtr grid, ref PfOpts opts, ref PfResult res);

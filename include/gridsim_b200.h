@@ -354,6 +354,32 @@ int gs_outage_topology(const gs_grid_desc *desc, double tolerance, int32_t n_out
  * With Q limits or the DC retry (ContingencyAnalysis.StudyOptions) a case's system changes between Newton passes,
  * which the one-CTA-per-case solve does not carry: each grid's cases then run as one gs_pf_solve_batch, and stats
  * reports the CUDA-event time around them, the cases and the summed iterations (no CTA shape). */
+/* ---- schedule of a grid's batched solves, and its autotuner (no counterpart in the reference: GridSim solves one
+ *      system at a time) ------------------------------------------------------------------------- */
+typedef struct gs_schedule {
+    int32_t factor_cut;  /* the factorisation's persistent walk starts at the lowest level from which every level's
+                            phases hold at most factor_cut x 16 items; the levels below run one launch each (default 2) */
+    int32_t solve_cut;   /* the same cut for the triangular solves (default 2) */
+    int32_t tail_max;    /* the few-systems path (one CTA or cluster per system) takes over once at most this many
+                            systems still step, 1..296 (default 296) */
+    int32_t candidates;  /* out (gs_screen_tune): schedules timed */
+    double default_ms;   /* out (gs_screen_tune): device time of the sample's Newton batch under the schedule the grid
+                            had before the call */
+    double tuned_ms;     /* out (gs_screen_tune): the same under the schedule chosen */
+    int32_t reserved[4];
+} gs_schedule;
+
+/* The schedule in force on a grid, and setting one (factor_cut, solve_cut >= 1; tail_max clamped to 1..296). */
+int gs_grid_schedule_get(gs_grid *g, gs_schedule *out);
+int gs_grid_schedule_set(gs_grid *g, const gs_schedule *sched);
+
+/* Autotune the grid's schedule on a sample screen: the outages idx[0 .. n_out) (at most one batch) solved as
+ * gs_n1_screen solves them under `opts` (warm start from the base case when set), timed with CUDA events for each
+ * candidate (the few-systems threshold of 74, 148 or 296 systems, then the factorisation cut of 1, 2 or 4, then the
+ * solve cut of 1, 2 or 4, each the best of two runs), the fastest kept on the grid for every later solve and screen.
+ * `out` gets the schedule chosen and both times. Q limits: the schedule of the grid analysed for them is tuned. */
+int gs_screen_tune(gs_grid *g, int32_t n_out, const int32_t *idx, const gs_pf_opts *opts, gs_schedule *out);
+
 typedef struct gs_multi_stats {
     double device_ms;          /* the graph launch (CUDA events) */
     double tune_ms;            /* autotuning trials of this call (0 when the choice was cached) */

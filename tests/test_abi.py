@@ -33,7 +33,7 @@ def test_struct_layouts_match_the_header(tmp_path):
     structs = {"gs_grid_desc": _abi.GridDesc, "gs_pf_opts": _abi.PfOpts, "gs_pf_result": _abi.PfResult,
                "gs_n1_result": _abi.N1Result, "gs_grid_info": _abi.GridInfo, "gs_ctx_opts": _abi.CtxOpts,
                "gs_serve_opts": _abi.ServeOpts, "gs_request": _abi.Request, "gs_response": _abi.Response,
-               "gs_serve_stats": _abi.ServeStats, "gs_multi_stats": _abi.MultiStats}
+               "gs_serve_stats": _abi.ServeStats, "gs_multi_stats": _abi.MultiStats, "gs_schedule": _abi.Schedule}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for cname, cls in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

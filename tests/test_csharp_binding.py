@@ -171,7 +171,7 @@ def test_pinvoke_signatures_match_the_prototypes():
 
 
 @pytest.mark.parametrize("name", ["CtxOpts", "GridDesc", "PfOpts", "PfResult", "N1Result", "GridInfo", "MultiStats",
-                                  "ServeOpts", "Request", "Response", "ServeStats"])
+                                  "ServeOpts", "Request", "Response", "ServeStats", "Schedule"])
 def test_struct_layouts_match_the_c_structs(name):
     structs = cs_structs()
     assert name in structs
