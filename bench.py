@@ -138,7 +138,7 @@ def cpu_single_thread(m, idx, count=6):
 # counts log-uniform in 100-25,000; each request the base case or one random non-islanding branch outage of a
 # random grid, 50/50), answered by the request loop (gs_serve_*, mixed precision). Latency runs from the
 # request's scheduled arrival to its result on the host.
-SERVE_RATES = (100, 1000, 5000, 20000)
+SERVE_RATES = (100, 1000, 2000, 5000, 10000, 20000)
 SERVE_HEADLINE_RATE = 1000
 SERVE_SECONDS = 2.0
 

@@ -100,7 +100,7 @@ class MultiStats(ctypes.Structure):
 
 class ServeOpts(ctypes.Structure):
     _fields_ = [("pf", PfOpts), ("slots_per_grid", c_i32), ("state_slots", c_i32), ("hbm_fraction", c_f64),
-                ("reserved", c_i32 * 8)]
+                ("scheduler_threads", c_i32), ("reserved", c_i32 * 7)]
 
 
 class Request(ctypes.Structure):

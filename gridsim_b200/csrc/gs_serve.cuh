@@ -3,17 +3,17 @@
 // few-systems LU path, the FP64 refinement and the damped update).
 //
 // Continuous batching, one lane per registered grid. A lane owns a batch of C request slots (C <= 128, so
-// that every stepping system gets one k_tail CTA in a single wave), its own stream and pinned staging. A tick
-// is one Newton iteration of the lane's occupied slots, in two halves:
+// that every stepping system gets its CTA or cluster of the few-systems walk in a single wave), its own stream and
+// pinned staging. A tick is one Newton iteration of the lane's occupied slots, in two halves:
 //   A: admit queued requests into free slots (k_admit: start voltages, Newton control), then mismatch +
 //      Jacobian of every occupied slot, then the status test at each slot's own step count
 //      (k_status_each lists the systems that stop); copy the counts, the stop list and the per-slot
 //      results to pinned memory; event A.
 //   B: copy out the solved states that were asked for (k_pack), then factor, solve and update the systems
 //      still stepping; event B.
-// The scheduler thread polls the lanes' events and never blocks on the device: a request that arrives while
-// its grid is mid-tick joins at the next tick, a finished request is answered as soon as half A shows it
-// stopped (or, with a state, when half B has copied it), and the lanes of different grids overlap on the GPU.
+// Scheduler threads (each owning every k-th lane) poll their lanes' events and never block on the device: a request
+// that arrives while its grid is mid-tick joins at the next tick, a finished request is answered as soon as half A
+// shows it stopped (or, with a state, when half B has copied it), and the lanes of different grids overlap on the GPU.
 // The reference's nearest host is sequential (src/GridSim.Cli/RpcCommand.cs:11-50: one request at a time).
 #pragma once
 
@@ -121,10 +121,11 @@ struct gs_server {
     gs_serve_opts opts{};
     std::vector<std::unique_ptr<gs::serve::Lane>> lanes;
     double budget = 0, slotBytes = 0;
-    std::thread thread;
+    std::vector<std::thread> threads;  // scheduler threads; thread t owns the lanes k with k % threads.size() == t
+    int threadsRunning = 0;
     std::mutex mu;
     std::condition_variable cvIn, cvOut, cvDone;
-    std::deque<gs::serve::ServeTicket> incoming;
+    std::vector<std::deque<gs::serve::ServeTicket>> inbox;  // submitted requests, per scheduler thread
     std::deque<gs::serve::ServeResponse> done;
     uint64_t nextTicket = 1;
     bool batch = false;  // Q limits or the DC retry: queued requests answered in batches (AdvanceBatch)
@@ -239,7 +240,8 @@ cudaError_t LaunchB(gs_server* S, Lane& L) {
     if (na > 0) {
         cudaMemsetAsync(b.activeCount, 0, sizeof(int), L.st);
         k_collect_active<<<(L.C + 255) / 256, 256, 0, L.st>>>(b);
-        FewSystemsSolve<T>(g, b, L.G->sym, na, L.G->tailSplit, refine != 0, L.st, nullptr);
+        FewSystemsSolve<T>(g, b, L.G->sym, na, L.G->tailSplit, refine != 0, L.st, nullptr, S->ctx->clusterOk,
+                           L.G->paired);
         constexpr int rowsPerBlock = 512;
         k_dxmax<T><<<dim3((m + rowsPerBlock - 1) / rowsPerBlock, (na + 31) / 32), blk8, 0, L.st>>>(g, b, rowsPerBlock, refine,
                                                                                                 b.activeList, na);
@@ -357,8 +359,10 @@ void FailOutstanding(gs_server* S) {
         L.pending.clear();
     }
     std::lock_guard<std::mutex> l(S->mu);
-    for (auto& t : S->incoming) all.push_back(t);
-    S->incoming.clear();
+    for (auto& q : S->inbox) {
+        for (auto& t : q) all.push_back(t);
+        q.clear();
+    }
     const auto now = ServeClock::now();
     for (auto& t : all) {
         ServeResponse out;
@@ -376,32 +380,40 @@ void FailOutstanding(gs_server* S) {
     S->inFlight = 0;
 }
 
-void ServeLoop(gs_server* S) {
+// Scheduler thread `t` of `nt`: it owns the lanes k with k % nt == t, takes their requests from its inbox, and
+// launches and polls their iterations. Several threads issue the lanes' launches in parallel (a lane's iteration is
+// tens of launches, and with one thread their issue time, not the device, set the latency once many grids were busy).
+// A CUDA error in any thread stops all of them; the last to leave answers what is outstanding.
+void ServeLoop(gs_server* S, int t, int nt) {
     cudaSetDevice(S->ctx->device);
     const bool mixed = S->opts.pf.precision == GS_PREC_MIXED;
+    std::vector<int> mine;
+    for (int k = t; k < (int)S->lanes.size(); k += nt) mine.push_back(k);
     for (;;) {
         {
             std::unique_lock<std::mutex> lk(S->mu);
-            while (!S->incoming.empty()) {
-                ServeTicket t = S->incoming.front();
-                S->incoming.pop_front();
-                S->lanes[t.req.grid]->pending.push_back(t);
+            auto& in = S->inbox[t];
+            while (!in.empty()) {
+                ServeTicket tk = in.front();
+                in.pop_front();
+                S->lanes[tk.req.grid]->pending.push_back(tk);
             }
-            if (S->abort) break;
+            if (S->abort || S->failed) break;
             bool busy = false;
-            for (auto& lp : S->lanes) busy = busy || lp->Busy();
+            for (int k : mine) busy = busy || S->lanes[k]->Busy();
             if (!busy) {
                 if (S->stopping) break;
-                S->cvIn.wait(lk, [&] { return !S->incoming.empty() || S->stopping || S->abort; });
+                S->cvIn.wait(lk, [&] { return !S->inbox[t].empty() || S->stopping || S->abort || S->failed; });
                 continue;
             }
         }
         bool progress = false;
         cudaError_t err = cudaSuccess;
         int rc = GS_OK;
-        for (size_t k = 0; k < S->lanes.size() && err == cudaSuccess && rc == GS_OK; k++) {
-            if (S->batch) progress |= AdvanceBatch(S, *S->lanes[k], (int)k, &rc);
-            else progress |= mixed ? Advance<float>(S, *S->lanes[k], (int)k, &err) : Advance<double>(S, *S->lanes[k], (int)k, &err);
+        for (size_t q = 0; q < mine.size() && err == cudaSuccess && rc == GS_OK; q++) {
+            const int k = mine[q];
+            if (S->batch) progress |= AdvanceBatch(S, *S->lanes[k], k, &rc);
+            else progress |= mixed ? Advance<float>(S, *S->lanes[k], k, &err) : Advance<double>(S, *S->lanes[k], k, &err);
         }
         if (err != cudaSuccess || rc != GS_OK) {
             if (err != cudaSuccess) SetErr(S->ctx, GS_ERR_CUDA, std::string("request loop: ") + cudaGetErrorString(err));
@@ -409,13 +421,21 @@ void ServeLoop(gs_server* S) {
                 std::lock_guard<std::mutex> l(S->mu);
                 S->failed = true;
             }
-            FailOutstanding(S);
-            S->cvOut.notify_all();
+            S->cvIn.notify_all();
             break;
         }
         if (!progress) std::this_thread::sleep_for(std::chrono::microseconds(5));
     }
-    for (auto& lp : S->lanes) if (lp->st) cudaStreamSynchronize(lp->st);
+    for (int k : mine)
+        if (S->lanes[k]->st) cudaStreamSynchronize(S->lanes[k]->st);
+    bool last = false, failed = false;
+    {
+        std::lock_guard<std::mutex> l(S->mu);
+        last = --S->threadsRunning == 0;
+        failed = S->failed;
+    }
+    if (!last) return;
+    if (failed) FailOutstanding(S);  // every scheduler thread has left: the lanes are no one's now
     {
         std::lock_guard<std::mutex> l(S->mu);
         S->loopEnded = true;
@@ -444,6 +464,7 @@ int gs_serve_create(gs_ctx* ctx, const gs_serve_opts* opts, gs_server** out) {
     const int slots = opts->slots_per_grid ? opts->slots_per_grid : GS_SERVE_MAX_SLOTS;
     if (slots < 32 || slots > GS_SERVE_MAX_SLOTS || slots % 32)
         return SetErr(ctx, GS_ERR_INVALID_ARG, "slots_per_grid must be a multiple of 32 in [32, 128]");
+    if (opts->scheduler_threads < 0) return SetErr(ctx, GS_ERR_INVALID_ARG, "scheduler_threads >= 0");
     if (opts->state_slots < 0 || opts->hbm_fraction < 0 || opts->hbm_fraction > 1)
         return SetErr(ctx, GS_ERR_INVALID_ARG, "state_slots >= 0 and hbm_fraction in [0, 1]");
     GS_CUDA(cudaSetDevice(ctx->device));
@@ -529,8 +550,15 @@ int gs_serve_start(gs_server* S) {
     if (!S) return GS_ERR_INVALID_ARG;
     if (S->started) return SetErr(S->ctx, GS_ERR_STATE, "the request loop is already running");
     if (S->lanes.empty()) return SetErr(S->ctx, GS_ERR_STATE, "no grid added");
+    // scheduler threads: one per grid up to 8 (or as asked); the batch mode runs its solves on the context's one
+    // stream, so it keeps one thread
+    int nt = S->opts.scheduler_threads > 0 ? S->opts.scheduler_threads : 8;
+    nt = std::max(1, std::min<int>(nt, (int)S->lanes.size()));
+    if (S->batch) nt = 1;
+    S->inbox.assign(nt, {});
+    S->threadsRunning = nt;
     S->started = true;
-    S->thread = std::thread(ServeLoop, S);
+    for (int t = 0; t < nt; t++) S->threads.emplace_back(ServeLoop, S, t, nt);
     return GS_OK;
 }
 
@@ -559,12 +587,12 @@ int gs_serve_submit(gs_server* S, int32_t n, const gs_request* req, uint64_t* ti
             t.submit = now;
             t.admit = now;
             if (tickets) tickets[k] = t.ticket;
-            S->incoming.push_back(t);
+            S->inbox[t.req.grid % S->inbox.size()].push_back(t);
         }
         S->submitted += n;
         S->inFlight += n;
     }
-    S->cvIn.notify_one();
+    S->cvIn.notify_all();
     return GS_OK;
 }
 
@@ -606,7 +634,7 @@ int gs_serve_stats_get(gs_server* S, gs_serve_stats* st) {
     st->grids = (int32_t)S->lanes.size();
     for (auto& lp : S->lanes) st->slots_total += lp->C;
     st->in_flight = S->inFlight;
-    st->queued = (int32_t)S->incoming.size();
+    for (auto& q : S->inbox) st->queued += (int32_t)q.size();
     st->slot_bytes = S->slotBytes;
     st->failed = S->failed ? 1 : 0;
     return GS_OK;
@@ -628,7 +656,9 @@ int gs_serve_stop(gs_server* S, int32_t timeout_ms) {
             rc = SetErr(S->ctx, GS_ERR_TIMEOUT, "the request loop did not drain within the timeout");
         }
     }
-    if (S->thread.joinable()) S->thread.join();
+    for (auto& th : S->threads)
+        if (th.joinable()) th.join();
+    S->threads.clear();
     S->started = false;
     return rc;
 }

@@ -63,7 +63,7 @@ class LoadFlowServer:
     context while the loop runs."""
 
     def __init__(self, options: Optional[PowerFlowOptions] = None, ctx: Optional[CudaContext] = None,
-                 slots_per_grid: int = 0, state_slots: int = 0, hbm_fraction: float = 0.0):
+                 slots_per_grid: int = 0, state_slots: int = 0, hbm_fraction: float = 0.0, scheduler_threads: int = 0):
         self.ctx = ctx or CudaContext.default()
         self.lib = self.ctx.lib
         self.options = options or PowerFlowOptions()
@@ -72,6 +72,7 @@ class LoadFlowServer:
         o.slots_per_grid = slots_per_grid
         o.state_slots = state_slots
         o.hbm_fraction = hbm_fraction
+        o.scheduler_threads = scheduler_threads
         self.handle = ctypes.c_void_p()
         self.ctx.check(self.lib.gs_serve_create(self.ctx.handle, ctypes.byref(o), ctypes.byref(self.handle)),
                        "gs_serve_create")

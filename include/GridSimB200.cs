@@ -148,7 +148,8 @@ namespace GridSim.Core.PowerFlow.B200
             public PfOpts Pf;
             public int SlotsPerGrid, StateSlots;
             public double HbmFraction;
-            public fixed int Reserved[8];
+            public int SchedulerThreads;
+            public fixed int Reserved[7];
         }
 
         [StructLayout(LayoutKind.Sequential)]

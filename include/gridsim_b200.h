@@ -422,7 +422,9 @@ typedef struct gs_serve_opts {
     int32_t slots_per_grid;    /* concurrent systems per grid, a multiple of 32, at most GS_SERVE_MAX_SLOTS; 0 = 128 */
     int32_t state_slots;       /* solved states returned per grid and iteration; 0 = 16 */
     double hbm_fraction;       /* share of the free device memory the slot batches may take; 0 = 0.5 */
-    int32_t reserved[8];
+    int32_t scheduler_threads; /* host threads that launch the grids' iterations (each owns every k-th grid); 0 = one
+                                  per grid up to 8; the batch mode (Q limits, the DC retry, partial pivoting) uses one */
+    int32_t reserved[7];
 } gs_serve_opts;
 
 typedef struct gs_request {
