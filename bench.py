@@ -287,7 +287,8 @@ def run_serving(ctx, grids, outs, gen_s):
     out = {"population": f"64 synthetic grids, bus counts log-uniform 100-25,000 "
                          f"({sum(m.n_bus for m in grids):,} buses), built in {gen_s:.0f} s",
            "requests": "base case or one random non-islanding branch outage of a random grid (50/50)",
-           "precision": "mixed", "slots_per_grid": 128, "slot_gb": st["slot_bytes"] / 1e9, "runs": runs,
+           "precision": "mixed", "max_slots_per_grid": 128, "slots_at_end": st["slots_total"],
+           "slot_gb": st["slot_bytes"] / 1e9, "runs": runs,
            "batched_fp64_rps": batched_rps(ctx, grids, ref_reqs, "fp64"),
            "batched_mixed_rps": batched_rps(ctx, grids, ref_reqs, "mixed")}
     head = next(r for r in runs if r["rate_rps"] == SERVE_HEADLINE_RATE)

@@ -88,10 +88,13 @@ struct PinnedBuf {
 
 struct Lane {
     gs_grid* G = nullptr;
-    int C = 0;           // slots (the batch's interleave stride)
+    int C = 0;           // slots (the batch's interleave stride), grown in steps of 32 up to Cmax as requests queue
+    int Cmax = 0;
+    double perSlot = 0;  // device bytes of one slot
     int stateSlots = 0;  // states copied out per tick
     bool warm = false;
-    Workspace ws;
+    std::unique_ptr<Workspace> ws;
+    std::vector<std::unique_ptr<Workspace>> retired;  // batches outgrown, freed when the loop is destroyed
     DevBuf admitD, doneD, stateD, baseVm, baseVa;
     cudaStream_t st = nullptr;
     cudaEvent_t evA = nullptr, evB = nullptr;
@@ -129,6 +132,7 @@ struct gs_server {
     std::deque<gs::serve::ServeResponse> done;
     uint64_t nextTicket = 1;
     bool batch = false;  // Q limits or the DC retry: queued requests answered in batches (AdvanceBatch)
+    std::atomic<int> slotsTotal{0};  // slots of every lane
     bool started = false, stopping = false, abort = false, loopEnded = false, failed = false;
     int64_t submitted = 0, completed = 0;
     std::atomic<int64_t> ticks{0}, systemSteps{0};
@@ -166,10 +170,58 @@ void Post(gs_server* S, const Lane& L, int laneIndex, int s, const double* state
     S->cvOut.notify_all();
 }
 
+// Admission by device memory: a lane with more requests waiting than free slots grows, in steps of 32 slots to the
+// width its systems in flight and waiting need (at most Cmax), if the request loop's device-memory budget still holds
+// them (shared by every grid: memory goes to the grids that have requests). The systems in flight move into the wider
+// batch (their voltages and Newton control; the Jacobian and right-hand side are rebuilt at the next half A). Called
+// with the lane's stream idle (before half A). The outgrown batch is kept until the loop is destroyed: freeing device
+// memory waits for the whole device, which would stall every other grid's iteration.
+cudaError_t GrowLane(gs_server* S, Lane& L) {
+    if (L.pending.size() <= L.freeSlots.size() || L.C >= L.Cmax) return cudaSuccess;
+    const int want = L.C - (int)L.freeSlots.size() + (int)L.pending.size();
+    const int C2 = std::min(L.Cmax, std::max(L.C + 32, (want + 31) / 32 * 32));
+    {
+        std::lock_guard<std::mutex> l(S->mu);
+        const double more = C2 * L.perSlot;  // the new batch (the outgrown one stays allocated)
+        if (S->slotBytes + more > S->budget) return cudaSuccess;  // no room: the requests wait for a free slot
+        S->slotBytes += more;
+    }
+    const Symbolic& s = L.G->sym;
+    auto nw = std::make_unique<Workspace>();
+    if (EnsureWs(S->ctx, s, *nw, C2, S->opts.pf.precision, 0, false) != GS_OK) {
+        std::lock_guard<std::mutex> l(S->mu);
+        S->slotBytes -= C2 * L.perSlot;
+        cudaGetLastError();
+        return cudaSuccess;  // the allocation failed: stay at this width
+    }
+    cudaError_t e = cudaMemsetAsync(nw->active.p, 0, (size_t)C2 * sizeof(int), L.st);
+    const DevBatch nb = MakeBatchWs(*nw, s.nLevels, C2, C2, false);
+    std::vector<int2> pairs;
+    for (int k = 0; k < L.C; k++) pairs.push_back(make_int2(k, k));  // every slot keeps its index (free ones inactive)
+    DevBuf dp;
+    if (e == cudaSuccess) e = dp.alloc(pairs.size() * sizeof(int2));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dp.p, pairs.data(), pairs.size() * sizeof(int2), cudaMemcpyHostToDevice, L.st);
+    if (e == cudaSuccess) {
+        k_move_listed<<<dim3((s.n + 7) / 8, (L.C + 31) / 32), dim3(32, 8), 0, L.st>>>(L.batch, nb, dp.as<int2>(), L.C, s.n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(L.st);
+    if (e != cudaSuccess) return e;
+    L.retired.push_back(std::move(L.ws));
+    L.ws = std::move(nw);
+    L.batch = nb;
+    L.slot.resize(C2);
+    for (int k = C2 - 1; k >= L.C; k--) L.freeSlots.push_back(k);
+    S->slotsTotal += C2 - L.C;
+    L.C = C2;
+    return cudaSuccess;
+}
+
 template <typename T>
 cudaError_t LaunchA(gs_server* S, Lane& L) {
     const gs_pf_opts& o = S->opts.pf;
     const DevGrid& g = L.G->view;
+    if (cudaError_t e = GrowLane(S, L); e != cudaSuccess) return e;
     const DevBatch& b = L.batch;
     const dim3 blk8(32, 8);
     int nAdmit = 0;
@@ -501,10 +553,14 @@ int gs_serve_add_grid(gs_server* S, gs_grid* G, int32_t* index) {
     L->stateSlots = std::min(S->opts.state_slots, S->opts.slots_per_grid);
     const double per = (double)PerSystemBytes(s, o.precision);
     const double fixed = (double)L->stateSlots * 2.0 * s.n * 8.0 + 2.0 * s.n * 8.0;
-    int C = S->opts.slots_per_grid;
-    while (C >= 32 && S->slotBytes + fixed + C * per > S->budget) C -= 32;
-    if (C < 32) return SetErr(ctx, GS_ERR_OOM, "the device memory budget of the request loop holds no more slots");
+    // every grid starts with 32 slots; it grows by 32 at a time (up to slots_per_grid) while its requests queue and
+    // the budget holds the memory (GrowLane)
+    const int C = 32;
+    if (S->slotBytes + fixed + C * per > S->budget)
+        return SetErr(ctx, GS_ERR_OOM, "the device memory budget of the request loop holds no more slots");
     L->C = C;
+    L->Cmax = S->opts.slots_per_grid;
+    L->perSlot = per;
     if (o.warm_start_from_base) {
         int st = 0, it = 0;
         double mis = 0;
@@ -519,26 +575,30 @@ int gs_serve_add_grid(gs_server* S, gs_grid* G, int32_t* index) {
         GS_CUDA(cudaMemcpy(L->baseVm.p, G->ws.startVm.p, (size_t)s.n * 8, cudaMemcpyDeviceToDevice));
         GS_CUDA(cudaMemcpy(L->baseVa.p, G->ws.startVa.p, (size_t)s.n * 8, cudaMemcpyDeviceToDevice));
     }
-    int rc = EnsureWs(ctx, s, L->ws, C, o.precision, 0, false);
+    L->ws = std::make_unique<Workspace>();
+    int rc = EnsureWs(ctx, s, *L->ws, C, o.precision, 0, false);
     if (rc) return rc;
-    GS_CUDA(cudaMemset(L->ws.active.p, 0, (size_t)C * sizeof(int)));
-    GS_CUDA(L->admitD.alloc((size_t)2 * C * sizeof(int)));
-    GS_CUDA(L->doneD.alloc((size_t)(1 + C) * sizeof(int)));
+    GS_CUDA(cudaMemset(L->ws->active.p, 0, (size_t)C * sizeof(int)));
+    // per-slot staging sized for the widest the lane may grow to
+    const int Cm = L->Cmax;
+    GS_CUDA(L->admitD.alloc((size_t)2 * Cm * sizeof(int)));
+    GS_CUDA(L->doneD.alloc((size_t)(1 + Cm) * sizeof(int)));
     GS_CUDA(L->stateD.alloc((size_t)L->stateSlots * 2 * s.n * sizeof(double)));
-    GS_CUDA(L->hAdmit.alloc((size_t)2 * C));
+    GS_CUDA(L->hAdmit.alloc((size_t)2 * Cm));
     GS_CUDA(L->hCounts.alloc(4));
-    GS_CUDA(L->hDone.alloc((size_t)1 + C));
-    GS_CUDA(L->hStatus.alloc(C));
-    GS_CUDA(L->hIters.alloc(C));
-    GS_CUDA(L->hMis.alloc(C));
+    GS_CUDA(L->hDone.alloc((size_t)1 + Cm));
+    GS_CUDA(L->hStatus.alloc(Cm));
+    GS_CUDA(L->hIters.alloc(Cm));
+    GS_CUDA(L->hMis.alloc(Cm));
     GS_CUDA(L->hState.alloc((size_t)L->stateSlots * 2 * s.n));
     GS_CUDA(cudaStreamCreateWithFlags(&L->st, cudaStreamNonBlocking));
     GS_CUDA(cudaEventCreateWithFlags(&L->evA, cudaEventDisableTiming));
     GS_CUDA(cudaEventCreateWithFlags(&L->evB, cudaEventDisableTiming));
-    L->batch = MakeBatchWs(L->ws, s.nLevels, C, C, false);
+    L->batch = MakeBatchWs(*L->ws, s.nLevels, C, C, false);
     L->slot.resize(C);
     for (int k = C - 1; k >= 0; k--) L->freeSlots.push_back(k);
     S->slotBytes += fixed + C * per;
+    S->slotsTotal += C;
     *index = (int32_t)S->lanes.size();
     S->lanes.push_back(std::move(L));
     return GS_OK;
@@ -632,7 +692,7 @@ int gs_serve_stats_get(gs_server* S, gs_serve_stats* st) {
     st->ticks = S->ticks;
     st->system_steps = S->systemSteps;
     st->grids = (int32_t)S->lanes.size();
-    for (auto& lp : S->lanes) st->slots_total += lp->C;
+    st->slots_total = S->slotsTotal;
     st->in_flight = S->inFlight;
     for (auto& q : S->inbox) st->queued += (int32_t)q.size();
     st->slot_bytes = S->slotBytes;

@@ -419,9 +419,12 @@ typedef struct gs_server gs_server;
 
 typedef struct gs_serve_opts {
     gs_pf_opts pf;             /* options of every request (precision, tolerance, iteration cap, warm start) */
-    int32_t slots_per_grid;    /* concurrent systems per grid, a multiple of 32, at most GS_SERVE_MAX_SLOTS; 0 = 128 */
+    int32_t slots_per_grid;    /* the most concurrent systems a grid may hold, a multiple of 32, at most
+                                  GS_SERVE_MAX_SLOTS; 0 = 128. A grid starts with 32 slots and grows by 32 while its
+                                  requests queue and the budget below holds the memory (admission by device memory) */
     int32_t state_slots;       /* solved states returned per grid and iteration; 0 = 16 */
-    double hbm_fraction;       /* share of the free device memory the slot batches may take; 0 = 0.5 */
+    double hbm_fraction;       /* share of the free device memory (at gs_serve_create) that all grids' slot batches
+                                  share; 0 = 0.5 */
     int32_t scheduler_threads; /* host threads that launch the grids' iterations (each owns every k-th grid); 0 = one
                                   per grid up to 8; the batch mode (Q limits, the DC retry, partial pivoting) uses one */
     int32_t reserved[7];

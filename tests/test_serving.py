@@ -138,6 +138,50 @@ def test_many_more_requests_than_slots(population):
         srv.close()
 
 
+def test_slots_grow_with_queued_requests_within_the_memory_budget(population):
+    """Admission by device memory: a grid starts with 32 slots and takes 32 more at a time while its requests queue
+    and the loop's budget holds them; results equal the oracle's whatever width the batch has grown to. With a
+    budget that holds only the first 32 slots, the grid stays at 32 and every request is still answered."""
+    import torch
+    grids, outages = population
+    m, idx = grids[0], outages[0]
+    opt = _opts().to_c()
+    ref = oracle.screen(m, idx, opt, keep_states=True)
+    reqs = [(0, int(idx[k % len(idx)]), 1) for k in range(600)]
+    srv = LoadFlowServer(_opts(), slots_per_grid=128)
+    try:
+        srv.add_grid(m)
+        first = srv.stats()
+        assert first["slots_total"] == 32
+        srv.start()
+        tickets = srv.submit(reqs)
+        got = {r.ticket: r for r in drain(srv, len(reqs))}
+        st = srv.stats()
+        assert st["slots_total"] > 32 and st["slot_bytes"] > first["slot_bytes"]
+        n = m.n_bus
+        for req, t in zip(reqs, tickets):
+            k = int(np.nonzero(idx == req[1])[0][0])
+            r = got[int(t)]
+            assert r.status == ref["status"][k]
+            if r.status == _abi.PF_CONVERGED:
+                assert np.max(np.abs(r.vm - np.asarray(ref["vm"]).reshape(len(idx), n)[k])) <= VM_TOL
+                assert np.max(np.abs(np.radians(r.va_deg - np.asarray(ref["va_deg"]).reshape(len(idx), n)[k]))) <= VA_TOL_RAD
+    finally:
+        srv.close()
+    # a budget for the first 32 slots only (their bytes with a 20 % margin, as a share of the free memory now)
+    free, _ = torch.cuda.mem_get_info()
+    srv = LoadFlowServer(_opts(), slots_per_grid=128, hbm_fraction=1.2 * first["slot_bytes"] / free)
+    try:
+        srv.add_grid(m)
+        srv.start()
+        srv.submit(reqs)
+        res = drain(srv, len(reqs))
+        assert len(res) == len(reqs)
+        assert srv.stats()["slots_total"] == 32
+    finally:
+        srv.close()
+
+
 def test_bad_requests_are_refused(population):
     grids, _ = population
     srv = LoadFlowServer(_opts(), slots_per_grid=32)
