@@ -224,6 +224,53 @@ def batched_rps(ctx, grids, reqs, precision):
     return len(reqs) / (time.perf_counter() - t)
 
 
+STRESSED_MARGIN = 0.9
+
+
+def run_stressed(ctx, outages, steps=2, warmup=1, check=True):
+    """The same screen on the grid's stressed variant: the operating point at 0.9 (not 0.6) of the last solvable load
+    level (same topology and outage set): outages take more Newton iterations, more of them fail and run to the cap.
+    Both precisions, device-timed as the headline; a 48-outage check against the oracle."""
+    from gridsim_b200 import synthetic
+    from gridsim_b200.engine import ContingencyAnalysis, SparseNewtonRaphsonPowerFlow
+    t = time.perf_counter()
+    m = synthetic.config_grid(2, GRID_SEED, margin=STRESSED_MARGIN)
+    gen_s = time.perf_counter() - t
+    idx = synthetic.outage_set(m, N_OUTAGES, GRID_SEED)[:outages]
+    out = {"workload": f"N-1 screen of the 10,000-bus grid stressed to {STRESSED_MARGIN} of its last solvable load "
+                       f"level (load scale {m.meta.get('load_scale', 0):.4f}; the headline grid is at 0.6), "
+                       f"{len(idx)} outages", "grid_build_s": gen_s}
+    for prec in ("mixed", "fp64"):
+        solver = SparseNewtonRaphsonPowerFlow(prec, ctx)
+        opt = options(prec)
+        for _ in range(warmup):
+            ContingencyAnalysis.screen_raw(m, idx, solver, opt)
+        dev = []
+        for _ in range(steps):
+            r = ContingencyAnalysis.screen_raw(m, idx, solver, opt)
+            dev.append(r["device_ms"])
+        conv = int((r["status"] == 0).sum())
+        it = r["iterations"][r["status"] == 0]
+        out[prec] = {"load_flows_per_s": conv / (float(np.mean(dev)) / 1e3), "ms_per_screen": float(np.mean(dev)),
+                     "converged": conv, "not_converged": int(len(idx) - conv),
+                     "mean_iterations_converged": float(it.mean()) if len(it) else None,
+                     "newton_iterations": int(r["newton_iterations"])}
+    out["mixed_over_fp64"] = out["mixed"]["load_flows_per_s"] / out["fp64"]["load_flows_per_s"]
+    if check:
+        import oracle
+        sub = idx[:48]
+        g = ContingencyAnalysis.screen_raw(m, sub, SparseNewtonRaphsonPowerFlow("mixed", ctx), options("mixed"),
+                                           keep_states=True)
+        o = oracle.screen(m, sub, options("fp64").to_c(), keep_states=True)
+        cv = o["status"] == 0
+        out["accuracy_vs_oracle"] = {
+            "outages": int(len(sub)), "statuses_identical": bool(np.array_equal(g["status"], o["status"])),
+            "max_dvm_pu": float(np.max(np.abs(g["vm"][cv] - o["vm"][cv]))),
+            "max_dva_rad": float(np.max(np.abs(np.radians(g["va_deg"][cv] - o["va_deg"][cv])))),
+            "violations_identical": bool(np.array_equal(g["viol_element"], o["viol_element"]))}
+    return out
+
+
 def run_uneven(ctx, grids, steps=3):
     """4,096 independent load flows (64 load scalings of each of the 64 grids: a global U(0.7, 1.3) times per-bus
     lognormal sigma 0.05), FP32 factor with FP64 mismatch, in one persistent graph-captured launch
@@ -438,6 +485,9 @@ def run_ours(args):
                "max_dva_rad": float(np.max(np.abs(np.radians(g["va_deg"][cv] - o["va_deg"][cv])))),
                "violations_identical": bool(np.array_equal(g["viol_element"], o["viol_element"]) and
                                             np.array_equal(g["viol_kind"], o["viol_kind"]))}
+    stressed = None
+    if rank == 0 and world == 1 and not args.no_stress:
+        stressed = run_stressed(ctx, args.outages, check=not args.no_check)
     serving, head, uneven = None, None, None
     if rank == 0 and not args.no_serve:
         t = time.perf_counter()
@@ -490,6 +540,7 @@ def run_ours(args):
             "serve_rate_rps": SERVE_HEADLINE_RATE if head else None,
             "serving": serving,
             "uneven_batch": uneven,
+            "stressed": stressed,
         }
         print(json.dumps(line), flush=True)
     if dist:
@@ -507,6 +558,7 @@ def main():
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the grids' default schedule (no autotuning)")
+    ap.add_argument("--no-stress", action="store_true", help="skip the screen of the stressed grid")
     ap.add_argument("--outages", type=int, default=N_OUTAGES,
                     help="screen the first K of the 5,000 sampled outages (small cases for profiling)")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],

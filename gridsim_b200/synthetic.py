@@ -242,8 +242,10 @@ def _newton(Y, sbus: np.ndarray, V: np.ndarray, pv: np.ndarray, pq: np.ndarray, 
     return None
 
 
-def find_operating_point(m: GridModel) -> GridModel:
-    """Scale the load to a solvable level by continuation and store the solved state as the start point."""
+def find_operating_point(m: GridModel, margin: float = OPERATING_MARGIN) -> GridModel:
+    """Scale the load to a solvable level by continuation and store the solved state as the start point: the last
+    solvable load level times `margin` (0.6 for the benchmark grids; closer to 1 gives a stressed grid, whose
+    outages need more Newton iterations and fail more often)."""
     slack = np.nonzero(m.bus_type == SLACK)[0]
     pv = np.nonzero(m.bus_type == PV)[0]
     pq = np.nonzero(m.bus_type == PQ)[0]
@@ -294,7 +296,7 @@ def find_operating_point(m: GridModel) -> GridModel:
             continue
         V, lam = Vn, lam_try
         V_at[lam] = V
-    final = lam if lam >= 1.0 else lam * OPERATING_MARGIN
+    final = lam if lam >= 1.0 else lam * margin
     if final != lam:
         Vf = _newton(_ybus(m, taps, final), sbus(final), V, pv, pq)
         if Vf is None:
@@ -324,7 +326,7 @@ def find_operating_point(m: GridModel) -> GridModel:
 
 
 def make_grid(n_bus: int, n_branch: int, n_pv: int, seed: int, name: str | None = None,
-              operating_point: bool = True) -> GridModel:
+              operating_point: bool = True, margin: float = OPERATING_MARGIN) -> GridModel:
     rng = np.random.Generator(np.random.PCG64(seed))
     pts = rng.uniform(0.0, 1.0, size=(n_bus, 2))
     e = _edges(pts, n_branch, rng)
@@ -382,12 +384,15 @@ def make_grid(n_bus: int, n_branch: int, n_pv: int, seed: int, name: str | None 
         br_from=e[:, 0].astype(np.int32), br_to=e[:, 1].astype(np.int32), r=r, x=x, b=bch, tap=tap,
         shift_deg=np.zeros(nb), rate_a=np.zeros(nb), br_in_service=np.ones(nb, np.uint8),
         is_transformer=tx.astype(np.uint8), meta={"seed": seed})
-    return find_operating_point(m) if operating_point else m
+    return find_operating_point(m, margin) if operating_point else m
 
 
-def config_grid(config: int, seed: int = 0) -> GridModel:
+def config_grid(config: int, seed: int = 0, margin: float = OPERATING_MARGIN) -> GridModel:
+    """The grid of a benchmark configuration; `margin` other than 0.6 gives its stressed variant (same topology,
+    parameters and outage sets, the operating point at that share of the last solvable load level)."""
     n, b, p = CONFIG_SIZES[config]
-    return make_grid(n, b, p, seed, name=f"synthetic-config{config}-{n}bus-s{seed}")
+    suffix = "" if margin == OPERATING_MARGIN else f"-m{margin:g}"
+    return make_grid(n, b, p, seed, name=f"synthetic-config{config}-{n}bus-s{seed}{suffix}", margin=margin)
 
 
 def bridges(m: GridModel) -> np.ndarray:

@@ -61,6 +61,41 @@ def test_10k_bus_screen_of_5000_outages_matches_the_oracle(screen_workload, prec
     assert np.allclose(got["max_loading_pct"][conv], ref["max_loading_pct"][conv], rtol=1e-7, atol=1e-7)
 
 
+STRESSED_MARGIN = 0.9
+STRESSED_OUTAGES = 1000
+
+
+@pytest.fixture(scope="module")
+def stressed_workload():
+    """The benchmarked grid's stressed variant: the operating point at 0.9 (not 0.6) of the last solvable load
+    level, the same topology and outage set; its outages take more Newton iterations and more of them fail."""
+    from gridsim_b200.engine import PowerFlowOptions
+    m = synthetic.config_grid(2, 0, margin=STRESSED_MARGIN)
+    idx = synthetic.outage_set(m, N_OUTAGES, 0)[:STRESSED_OUTAGES]
+    opt = PowerFlowOptions(max_iterations=20, per_bus_voltage_limits=True, warm_start_from_base=True)
+    ref = oracle.screen(m, idx, opt.to_c(), keep_states=True)
+    return m, idx, ref
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_stressed_10k_bus_screen_matches_the_oracle(stressed_workload, precision):
+    from gridsim_b200.engine import ContingencyAnalysis, PowerFlowOptions, SparseNewtonRaphsonPowerFlow
+    m, idx, ref = stressed_workload
+    opt = PowerFlowOptions(max_iterations=20, per_bus_voltage_limits=True, warm_start_from_base=True,
+                           precision=precision)
+    got = ContingencyAnalysis.screen_raw(m, idx, SparseNewtonRaphsonPowerFlow(precision), opt, keep_states=True)
+    assert got["n_singular_pivot"] == 0
+    assert np.array_equal(got["status"], ref["status"])
+    assert np.array_equal(got["iterations"], ref["iterations"])
+    conv = ref["status"] == _abi.PF_CONVERGED
+    assert (~conv).sum() >= 5 and ref["iterations"][conv].mean() > 2.5  # the stress shows
+    assert np.max(np.abs(got["vm"][conv] - ref["vm"][conv])) <= VM_TOL
+    assert np.max(np.abs(np.radians(got["va_deg"][conv] - ref["va_deg"][conv]))) <= VA_TOL_RAD
+    assert np.array_equal(got["viol_ptr"], ref["viol_ptr"])
+    assert np.array_equal(got["viol_kind"], ref["viol_kind"])
+    assert np.array_equal(got["viol_element"], ref["viol_element"])
+
+
 def _population_sample():
     specs = synthetic.population_specs(64, 0, 100, 25000)
     by_size = sorted(range(len(specs)), key=lambda k: -specs[k][0])
