@@ -2233,21 +2233,27 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
     // part's dependent-load latency and wave tails overlap the other's; small batches run as one. parts: as many as
     // keep each part at 148 or more system groups and at least one system, at most kParts.
     DevBatch stepB = b;
-    int persistWarps = kPersistWarps;
+    int persistWarps[3] = {kPersistWarps, kPersistWarps, kPersistWarps};  // per walk: factorisation, backward, forward
     int parts = 1;
     DevBatch hb[kParts];
     auto setParts = [&](const DevBatch& base) {
-        // warps per persistent CTA: as many as let every system group's CTA be resident at once (one wave), at most
-        // kPersistWarps (a second partial wave would double the launch)
+        // warps per persistent CTA, for each walk (the three kernels use different numbers of registers): as many as
+        // let every system group's CTA be resident at once (one wave), at most kPersistWarps. A second wave doubles
+        // the walk: measured on the 10,000-bus screen, the backward walk (104 registers a thread) sized by the
+        // factorisation's (90) ran 625 CTAs in two waves of 592.
         int sms = 0, occ = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-        for (int wpc = kPersistWarps; wpc >= 4; wpc--) {
-            persistWarps = wpc;
-            const void* pk = pairedOn ? (const void*)k_ppersistent<T, kWorkFactor> : (const void*)k_persistent<T, kWorkFactor>;
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pk, 32 * wpc, 0) == cudaSuccess &&
-                (int64_t)occ * sms >= base.B / Lay<T>::S)
-                break;
-        }
+        const void* pks[3] = {
+            pairedOn ? (const void*)k_ppersistent<T, kWorkFactor> : (const void*)k_persistent<T, kWorkFactor>,
+            pairedOn ? (const void*)k_ppersistent<T, kWorkBackward> : (const void*)k_persistent<T, kWorkBackward>,
+            pairedOn ? (const void*)k_ppersistent<T, kWorkForward> : (const void*)k_persistent<T, kWorkForward>};
+        for (int wk = 0; wk < 3; wk++)
+            for (int wpc = kPersistWarps; wpc >= 1; wpc--) {
+                persistWarps[wk] = wpc;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pks[wk], 32 * wpc, 0) == cudaSuccess &&
+                    (int64_t)occ * sms >= base.B / Lay<T>::S)
+                    break;
+            }
         const int cnt = base.count;
         parts = 1;
         const int groupsAll = base.B / Lay<T>::S;
@@ -2278,7 +2284,8 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
     };
     auto persistent = [&](const DevBatch& bb, cudaStream_t ss, auto wTag, T* vec, int l0) {
         constexpr int W = decltype(wTag)::value;
-        const dim3 grid((bb.count + Lay<T>::S - 1) / Lay<T>::S), blk(persistThreads, persistWarps);
+        const int wk = W == kWorkFactor ? 0 : (W == kWorkBackward ? 1 : 2);
+        const dim3 grid((bb.count + Lay<T>::S - 1) / Lay<T>::S), blk(persistThreads, persistWarps[wk]);
         if (pairedOn) k_ppersistent<T, W><<<grid, blk, 0, ss>>>(g, bb, vec, l0, nLv);
         else k_persistent<T, W><<<grid, blk, 0, ss>>>(g, bb, vec, l0, nLv);
         stepLaunches++;
@@ -2344,7 +2351,8 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             const unsigned char* c = static_cast<const unsigned char*>(p);
             key.insert(key.end(), c, c + n);
         };
-        const int shape[8] = {(int)sizeof(T), refine, parts, persistWarps, split, splitB, pairedOn ? 1 : 0, nLv};
+        const int shape[10] = {(int)sizeof(T), refine, parts, persistWarps[0], persistWarps[1], persistWarps[2], split,
+                               splitB, pairedOn ? 1 : 0, nLv};
         put(shape, sizeof shape);
         put(&g, sizeof g);
         put(&stepB, sizeof stepB);
