@@ -89,7 +89,7 @@ class GridInfo(ctypes.Structure):
 
 class Schedule(ctypes.Structure):
     _fields_ = [("factor_cut", c_i32), ("solve_cut", c_i32), ("tail_max", c_i32), ("candidates", c_i32),
-                ("default_ms", c_f64), ("tuned_ms", c_f64), ("reserved", c_i32 * 4)]
+                ("default_ms", c_f64), ("tuned_ms", c_f64), ("subtree_cut", c_i32), ("reserved", c_i32 * 3)]
 
 
 class MultiStats(ctypes.Structure):

@@ -1748,8 +1748,11 @@ struct gs_grid {
     bool gpMode = false;
     gs::GpData gp;
     // the level-group cut and few-systems threshold in force (gs::SetSchedule; gs_screen_tune picks them)
-    gs_schedule sched{2, 2, gs::kTailMaxSystems, 0, 0.0, 0.0, {0, 0, 0, 0}};
+    gs_schedule sched{2, 2, gs::kTailMaxSystems, 0, 0.0, 0.0, -1, {0, 0, 0}};
     gs::StepGraphCache stepGraphs[2];  // the full-batch step's graphs: [0] the whole batch, [1] the mid workspace
+    // the subtree schedule of sched.subtree_cut (gs::BuildSubtrees) on the device; cut -1: none
+    int subCut = -1, nSub = 0;
+    gs::DevBuf subStage, subStagePtr, subWork;
 };
 
 struct MatrixPattern {
@@ -1823,6 +1826,42 @@ void SetSchedule(gs_grid* G, const gs_schedule& sc) {
     };
     cuts(s.factor, s.backward, s.forward, s.nLevels, G->split, G->splitB);
     if (s.ps.on) cuts(s.ps.factor, s.ps.backward, s.ps.forward, s.ps.nLevels, G->psSplit, G->psSplitB);
+    // the subtrees below the subtree cut, kept below the persistent walk's first level
+    const int cut = s.ps.on ? std::min(sc.subtree_cut, G->psSplit - 1) : -1;
+    G->sched.subtree_cut = cut;
+    if (cut != G->subCut) {
+        G->subCut = -1;
+        G->nSub = 0;
+        if (cut >= 0) {
+            const SubtreeSchedule st = BuildSubtrees(s, cut);
+            auto up = [](DevBuf& d, const std::vector<int32_t>& h) {
+                cudaError_t e = d.alloc(std::max<size_t>(1, h.size()) * 4);
+                if (e == cudaSuccess && !h.empty()) e = cudaMemcpy(d.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice);
+                return e;
+            };
+            if (st.nSub > 0 && up(G->subStage, st.subStage) == cudaSuccess &&
+                up(G->subStagePtr, st.stagePtr) == cudaSuccess && up(G->subWork, st.work) == cudaSuccess) {
+                G->subCut = cut;
+                G->nSub = st.nSub;
+            } else {
+                cudaGetLastError();
+                G->sched.subtree_cut = -1;  // no subtree schedule: every level its own launch
+            }
+        }
+    }
+}
+
+// The subtree cut whose largest subtree holds at most `bytes` of FP32 LU for a system group (eight systems), or -1.
+int SubtreeCutFor(const gs_grid* G, double bytes) {
+    const Symbolic& s = G->sym;
+    if (!s.ps.on) return -1;
+    int best = -1;
+    for (int cut = 0; cut < G->psSplit; cut++) {
+        const SubtreeSchedule st = BuildSubtrees(s, cut);
+        if ((double)st.maxEntries * 4.0 * 8.0 > bytes) break;
+        best = cut;
+    }
+    return best;
 }
 
 int UploadGrid(gs_grid* G) {
@@ -2294,7 +2333,17 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
     using BW = std::integral_constant<int, kWorkBackward>;
     using VW = std::integral_constant<int, kWorkForward>;
     auto factorPhase = [&](const DevBatch& bb, cudaStream_t ss) {
-        for (int l = 0; l < split; l++) {
+        int l0 = 0;
+        if (pairedOn && G->subCut >= 0 && G->nSub > 0) {  // the subtrees below the cut: one launch
+            const int grp = (bb.count + Lay<T>::S - 1) / Lay<T>::S;
+            if (grp > 0) {
+                k_psubtree<T><<<dim3(grp, G->nSub), blk4, 0, ss>>>(g, bb, G->subStage.as<int>(), G->subStagePtr.as<int>(),
+                                                                 G->subWork.as<int>());
+                stepLaunches++;
+            }
+            l0 = G->subCut + 1;
+        }
+        for (int l = l0; l < split; l++) {
             level(bb, ss, FW{}, (T*)bb.y, fp[2 * l], fp[2 * l + 1]);
             level(bb, ss, FW{}, (T*)bb.y, fp[2 * l + 1], fp[2 * l + 2]);
         }
@@ -2351,9 +2400,11 @@ int Newton(gs_grid* G, int count, bool useScale, bool startFromWs, const gs_pf_o
             const unsigned char* c = static_cast<const unsigned char*>(p);
             key.insert(key.end(), c, c + n);
         };
-        const int shape[10] = {(int)sizeof(T), refine, parts, persistWarps[0], persistWarps[1], persistWarps[2], split,
-                               splitB, pairedOn ? 1 : 0, nLv};
+        const int shape[12] = {(int)sizeof(T), refine, parts, persistWarps[0], persistWarps[1], persistWarps[2], split,
+                               splitB, pairedOn ? 1 : 0, nLv, G->subCut, G->nSub};
         put(shape, sizeof shape);
+        const void* subPtrs[3] = {G->subStage.p, G->subStagePtr.p, G->subWork.p};
+        put(subPtrs, sizeof subPtrs);
         put(&g, sizeof g);
         put(&stepB, sizeof stepB);
         for (int q = 0; q < parts; q++) put(&hb[q], sizeof hb[q]);
@@ -3109,8 +3160,9 @@ int gs_grid_schedule_get(gs_grid* g, gs_schedule* out) {
 
 int gs_grid_schedule_set(gs_grid* g, const gs_schedule* sc) {
     if (!g || !sc) return GS_ERR_INVALID_ARG;
-    if (sc->factor_cut < 1 || sc->solve_cut < 1 || sc->tail_max < 1)
-        return SetErr(g->ctx, GS_ERR_INVALID_ARG, "schedule: factor_cut, solve_cut and tail_max must be at least 1");
+    if (sc->factor_cut < 1 || sc->solve_cut < 1 || sc->tail_max < 1 || sc->subtree_cut < -1)
+        return SetErr(g->ctx, GS_ERR_INVALID_ARG,
+                      "schedule: factor_cut, solve_cut and tail_max must be at least 1, subtree_cut at least -1");
     gs_schedule c = *sc;
     c.tail_max = std::min(c.tail_max, kTailMaxSystems);
     SetSchedule(g, c);
@@ -3166,17 +3218,30 @@ int gs_screen_tune(gs_grid* G0, int32_t nOut, const int32_t* idx, const gs_pf_op
     float base = 0;
     if ((rc = run(before, &base)) != GS_OK) return rc;
     float bestMs = base;
-    // coordinate descent: the few-systems threshold, then the factorisation's cut, then the solves' cut
-    const int tails[3] = {74, 148, kTailMaxSystems};
-    const int cutOpts[3] = {1, 2, 4};
-    for (int dim = 0; dim < 3; dim++) {
+    // coordinate descent: the few-systems threshold, then the factorisation's cut, then the solves' cut, then the
+    // subtree cut (off, or the levels whose subtrees hold at most 16, 64 or 256 KB of FP32 LU for a system group)
+    const int tails[4] = {74, 148, kTailMaxSystems, kTailMaxSystems};
+    const int cutOpts[4] = {1, 2, 4, 4};
+    for (int dim = 0; dim < 4; dim++) {
         const gs_schedule start = best;
-        for (int k = 0; k < 3; k++) {
+        int subOpts[4] = {-1, -1, -1, -1};
+        if (dim == 3) {
+            SetSchedule(G, start);  // the persistent walk's first level under the schedule so far
+            subOpts[1] = SubtreeCutFor(G, 16.0 * 1024);
+            subOpts[2] = SubtreeCutFor(G, 64.0 * 1024);
+            subOpts[3] = SubtreeCutFor(G, 256.0 * 1024);
+        }
+        const int nOpt = dim == 3 ? 4 : 3;
+        for (int k = 0; k < nOpt; k++) {
             gs_schedule c = start;
             if (dim == 0) c.tail_max = tails[k];
             else if (dim == 1) c.factor_cut = cutOpts[k];
-            else c.solve_cut = cutOpts[k];
-            if (c.tail_max == start.tail_max && c.factor_cut == start.factor_cut && c.solve_cut == start.solve_cut) continue;
+            else if (dim == 2) c.solve_cut = cutOpts[k];
+            else c.subtree_cut = subOpts[k];
+            if (c.tail_max == start.tail_max && c.factor_cut == start.factor_cut && c.solve_cut == start.solve_cut &&
+                c.subtree_cut == start.subtree_cut)
+                continue;
+            if (dim == 3 && k > 0 && subOpts[k] == subOpts[k - 1]) continue;
             float ms = 0;
             if ((rc = run(c, &ms)) != GS_OK) { SetSchedule(G, before); return rc; }
             if (ms < bestMs) { bestMs = ms; best = c; }

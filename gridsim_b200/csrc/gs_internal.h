@@ -131,6 +131,7 @@ struct Symbolic {
         std::vector<int32_t> bTaskA, bTaskB;
         std::vector<int32_t> pairs;         // 2 per pair
         Schedule factor, backward, forward; // work: task indices (backward: into bTask*)
+        std::vector<int32_t> unitOf, unitLevel, unitParent;  // node -> unit; per unit its level and parent unit (-1)
     };
     PairSchedule ps;
 
@@ -165,6 +166,21 @@ struct Symbolic {
     };
     TopPart top[2];  // [0] FP64, [1] FP32
 };
+
+// The subtrees below a cut of the paired schedule's unit tree: every unit at level <= cut belongs to the subtree of
+// its highest ancestor at level <= cut, and a subtree's tasks read only entries of its own units, so one CTA per
+// (subtree, system group) can factor it alone, level by level with block barriers. Per subtree its stages (unit
+// levels bottom-up, the two factorisation phases each, empty ones left out), each a range of factorisation work
+// positions: stages of subtree t are subStage[t] .. subStage[t + 1] - 1, stage q holds work[stagePtr[q] ..
+// stagePtr[q + 1]). Subtrees are ordered largest first (by task pairs).
+struct SubtreeSchedule {
+    int cut = -1;
+    int nSub = 0;
+    std::vector<int32_t> subStage, stagePtr, work;
+    int64_t maxEntries = 0;     // LU entries of the largest subtree
+    double pairShare = 0.0;     // share of the factorisation's pairs below the cut
+};
+SubtreeSchedule BuildSubtrees(const Symbolic& s, int cut);
 
 // Build s.top[which] for values of `elem` bytes within `budget` bytes of shared memory.
 void BuildTopPart(Symbolic& s, int which, size_t elem, size_t budget);

@@ -367,6 +367,28 @@ __global__ void __launch_bounds__(128, 10) k_plevel(DevGrid g, DevBatch b, T* ve
     pkDoItem<T, W, kPkThread>(g, b, vec, it, s, act);
 }
 
+// The subtrees below the subtree cut (BuildSubtrees): one CTA per (system group, subtree) factors its subtree alone,
+// its stages bottom-up with block barriers, a warp per task (the task's pairs over the warp's pair lanes). A subtree's
+// tasks read only its own entries, which its CTA has just written: they come back from L1 / L2 instead of DRAM, which
+// the per-level launches over the whole batch cannot give. Grid (system groups, subtrees): the largest subtrees of
+// every group start first.
+template <typename T>
+__global__ void __launch_bounds__(128) k_psubtree(DevGrid g, DevBatch b, const int* __restrict__ subStage,
+                                                 const int* __restrict__ stagePtr, const int* __restrict__ work) {
+    const int s = laneSystem<T>(blockIdx.x);
+    const bool act = s < b.count && b.active[s];
+    if (!__syncthreads_or(act)) return;
+    const int q0 = __ldg(subStage + blockIdx.y), q1 = __ldg(subStage + blockIdx.y + 1);
+    for (int q = q0; q < q1; q++) {
+        const int w0 = __ldg(stagePtr + q), w1 = __ldg(stagePtr + q + 1);
+        for (int w = w0 + threadIdx.y; w < w1; w += blockDim.y) {
+            const int pos = __ldg(work + w);  // the task's position in the factorisation's descriptor arrays
+            pkFactorTask<T, kPkWarp>(g, b, __ldg(g.pfA + pos), __ldg(g.pfB + pos), s, act);
+        }
+        __syncthreads();
+    }
+}
+
 // The narrow top of the unit tree: one CTA per system group walks its levels [l0, l1) with block barriers.
 template <typename T, int W>
 __global__ void __launch_bounds__(32 * kPersistWarps) k_ppersistent(DevGrid g, DevBatch b, T* vec, int l0, int l1) {

@@ -638,6 +638,13 @@ std::string FactorSymbolic(Symbolic& s, const std::function<void(const std::func
         if (npairs() >= (int64_t)INT32_MAX) return "the paired schedule is too large for 32-bit pair indices";
         P.nUnits = nU;
         P.nLevels = nL;
+        P.unitOf = unitOf;
+        P.unitLevel = uLevel;
+        P.unitParent.assign(nU, -1);
+        for (int u = 0; u < nU; u++) {
+            const int par = s.parent[unitFirst[u] + unitPair[u]];
+            if (par >= 0) P.unitParent[u] = unitOf[par];
+        }
         P.on = true;
     }
     BuildTopPart(s, 0, sizeof(double), kTopBudgetBytes);
@@ -689,6 +696,66 @@ std::string AnalyzeMatrix(int n, const int* rowPtr, const int* colIdx, Symbolic&
                 hasA[aSlot[p]] = 1;
             }
     });
+}
+
+SubtreeSchedule BuildSubtrees(const Symbolic& s, int cut) {
+    SubtreeSchedule out;
+    const Symbolic::PairSchedule& P = s.ps;
+    if (!P.on || cut < 0) return out;
+    cut = std::min(cut, P.nLevels - 1);
+    const int nU = P.nUnits;
+    // the subtree root of every unit at or below the cut
+    std::vector<int> root(nU, -1);
+    for (int u = 0; u < nU; u++) {
+        if (P.unitLevel[u] > cut) continue;
+        int r = u;
+        while (P.unitParent[r] >= 0 && P.unitLevel[P.unitParent[r]] <= cut) r = P.unitParent[r];
+        root[u] = r;
+    }
+    std::vector<int> subOf(nU, -1), rootsOrder;
+    for (int u = 0; u < nU; u++)
+        if (root[u] == u) { subOf[u] = (int)rootsOrder.size(); rootsOrder.push_back(u); }
+    const int nSub = (int)rootsOrder.size();
+    // per subtree and stage (level, phase): its work positions
+    std::vector<std::vector<std::vector<int32_t>>> lists(nSub, std::vector<std::vector<int32_t>>(2 * (cut + 1)));
+    std::vector<int64_t> pairs(nSub, 0), entries(nSub, 0);
+    int64_t allPairs = 0, below = 0;
+    for (int l = 0; l < P.nLevels; l++)
+        for (int ph = 0; ph < 2; ph++)
+            for (int w = P.factor.levelWorkPtr[2 * l + ph]; w < P.factor.levelWorkPtr[2 * l + ph + 1]; w++) {
+                const int t = P.factor.work[w];
+                const int64_t np = (int64_t)P.taskA[4 * t + 1] - P.taskA[4 * t];
+                allPairs += np;
+                if (l > cut) continue;
+                const int u = P.unitOf[P.taskA[4 * t + 3]];
+                const int sub = subOf[root[u]];
+                lists[sub][2 * l + ph].push_back(w);
+                pairs[sub] += np;
+                below += np;
+            }
+    // the LU entries of each subtree: its nodes' diagonal, U row and L column
+    for (int k = 0; k < s.m; k++) {
+        const int u = P.unitOf[k];
+        if (root[u] >= 0) entries[subOf[root[u]]] += 1 + 2 * (int64_t)s.luCnt[k];
+    }
+    std::vector<int> order(nSub);
+    for (int q = 0; q < nSub; q++) order[q] = q;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return pairs[a] > pairs[b]; });
+    out.cut = cut;
+    out.nSub = nSub;
+    out.subStage.push_back(0);
+    out.stagePtr.push_back(0);
+    for (int q : order) {
+        for (const auto& st : lists[q]) {
+            if (st.empty()) continue;
+            out.work.insert(out.work.end(), st.begin(), st.end());
+            out.stagePtr.push_back((int32_t)out.work.size());
+        }
+        out.subStage.push_back((int32_t)out.stagePtr.size() - 1);
+        out.maxEntries = std::max(out.maxEntries, entries[q]);
+    }
+    out.pairShare = allPairs > 0 ? (double)below / (double)allPairs : 0.0;
+    return out;
 }
 
 void BuildTopPart(Symbolic& s, int which, size_t elem, size_t budget) {

@@ -185,15 +185,17 @@ class CudaGrid:
         return i
 
     def schedule(self) -> dict:
-        """The batched-solve schedule in force (gs_grid_schedule_get): factor_cut, solve_cut, tail_max."""
+        """The batched-solve schedule in force (gs_grid_schedule_get): factor_cut, solve_cut, tail_max, subtree_cut."""
         sc = _abi.Schedule()
         self.ctx.check(self.ctx.lib.gs_grid_schedule_get(self.handle, ctypes.byref(sc)), "gs_grid_schedule_get")
-        return {"factor_cut": sc.factor_cut, "solve_cut": sc.solve_cut, "tail_max": sc.tail_max}
+        return {"factor_cut": sc.factor_cut, "solve_cut": sc.solve_cut, "tail_max": sc.tail_max,
+                "subtree_cut": sc.subtree_cut}
 
-    def set_schedule(self, factor_cut: int = 2, solve_cut: int = 2, tail_max: int = 296) -> None:
+    def set_schedule(self, factor_cut: int = 2, solve_cut: int = 2, tail_max: int = 296, subtree_cut: int = -1) -> None:
         """gs_grid_schedule_set; the defaults are the schedule a grid starts with."""
         sc = _abi.Schedule()
         sc.factor_cut, sc.solve_cut, sc.tail_max = int(factor_cut), int(solve_cut), int(tail_max)
+        sc.subtree_cut = int(subtree_cut)
         self.ctx.check(self.ctx.lib.gs_grid_schedule_set(self.handle, ctypes.byref(sc)), "gs_grid_schedule_set")
 
     def close(self) -> None:
@@ -703,7 +705,8 @@ class ContingencyAnalysis:
         g.ctx.check(g.ctx.lib.gs_screen_tune(g.handle, idx.shape[0], _p(idx), ctypes.byref(c), ctypes.byref(sc)),
                     "gs_screen_tune")
         return {"factor_cut": sc.factor_cut, "solve_cut": sc.solve_cut, "tail_max": sc.tail_max,
-                "candidates": sc.candidates, "default_ms": sc.default_ms, "tuned_ms": sc.tuned_ms}
+                "subtree_cut": sc.subtree_cut, "candidates": sc.candidates, "default_ms": sc.default_ms,
+                "tuned_ms": sc.tuned_ms}
 
     @staticmethod
     def screen_sets_raw(model: GridModel, branch_sets, solver: SparseNewtonRaphsonPowerFlow,

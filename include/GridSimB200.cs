@@ -129,7 +129,8 @@ namespace GridSim.Core.PowerFlow.B200
         {
             public int FactorCut, SolveCut, TailMax, Candidates;
             public double DefaultMs, TunedMs;
-            public fixed int Reserved[4];
+            public int SubtreeCut;
+            public fixed int Reserved[3];
         }
 
         [StructLayout(LayoutKind.Sequential)]

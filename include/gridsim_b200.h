@@ -366,17 +366,22 @@ typedef struct gs_schedule {
     double default_ms;   /* out (gs_screen_tune): device time of the sample's Newton batch under the schedule the grid
                             had before the call */
     double tuned_ms;     /* out (gs_screen_tune): the same under the schedule chosen */
-    int32_t reserved[4];
+    int32_t subtree_cut; /* the factorisation's unit levels up to this one run as one launch of independent subtrees
+                            (one CTA per subtree and system group, level by level with block barriers, so a subtree's
+                            entries are re-read from cache); -1 = every level its own launch (default) */
+    int32_t reserved[3];
 } gs_schedule;
 
-/* The schedule in force on a grid, and setting one (factor_cut, solve_cut >= 1; tail_max clamped to 1..296). */
+/* The schedule in force on a grid, and setting one (factor_cut, solve_cut >= 1; tail_max clamped to 1..296;
+ * subtree_cut >= -1, clamped below the factorisation's persistent walk). */
 int gs_grid_schedule_get(gs_grid *g, gs_schedule *out);
 int gs_grid_schedule_set(gs_grid *g, const gs_schedule *sched);
 
 /* Autotune the grid's schedule on a sample screen: the outages idx[0 .. n_out) (at most one batch) solved as
  * gs_n1_screen solves them under `opts` (warm start from the base case when set), timed with CUDA events for each
  * candidate (the few-systems threshold of 74, 148 or 296 systems, then the factorisation cut of 1, 2 or 4, then the
- * solve cut of 1, 2 or 4, each the best of two runs), the fastest kept on the grid for every later solve and screen.
+ * solve cut of 1, 2 or 4, then the subtree cut: off or the levels whose subtrees hold at most 16, 64 or 256 KB of FP32
+ * LU for a system group, each the best of two runs), the fastest kept on the grid for every later solve and screen.
  * `out` gets the schedule chosen and both times. Q limits: the schedule of the grid analysed for them is tuned. */
 int gs_screen_tune(gs_grid *g, int32_t n_out, const int32_t *idx, const gs_pf_opts *opts, gs_schedule *out);
 
