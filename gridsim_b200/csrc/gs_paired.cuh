@@ -368,7 +368,7 @@ __global__ void __launch_bounds__(128, 10) k_plevel(DevGrid g, DevBatch b, T* ve
 }
 
 // The subtrees below the subtree cut (BuildSubtrees): one CTA per (system group, subtree) factors its subtree alone,
-// its stages bottom-up with block barriers, a warp per task (the task's pairs over the warp's pair lanes). A subtree's
+// its stages bottom-up with block barriers. A subtree's
 // tasks read only its own entries, which its CTA has just written: they come back from L1 / L2 instead of DRAM, which
 // the per-level launches over the whole batch cannot give. Grid (system groups, subtrees): the largest subtrees of
 // every group start first.
@@ -378,12 +378,33 @@ __global__ void __launch_bounds__(128) k_psubtree(DevGrid g, DevBatch b, const i
     const int s = laneSystem<T>(blockIdx.x);
     const bool act = s < b.count && b.active[s];
     if (!__syncthreads_or(act)) return;
+    constexpr int S = Lay<T>::S, P = Lay<T>::P;
+    const int lane = threadIdx.x & 31, grp = lane / S;
+    const unsigned full = 0xffffffffu;
     const int q0 = __ldg(subStage + blockIdx.y), q1 = __ldg(subStage + blockIdx.y + 1);
     for (int q = q0; q < q1; q++) {
         const int w0 = __ldg(stagePtr + q), w1 = __ldg(stagePtr + q + 1);
-        for (int w = w0 + threadIdx.y; w < w1; w += blockDim.y) {
-            const int pos = __ldg(work + w);  // the task's position in the factorisation's descriptor arrays
-            pkFactorTask<T, kPkWarp>(g, b, __ldg(g.pfA + pos), __ldg(g.pfB + pos), s, act);
+        // a warp takes P tasks at a time: a short one (at most 32 pairs) by one lane group serially, as the level
+        // kernels run short tasks; a long one by the whole warp (pair lanes)
+        for (int base = w0 + threadIdx.y * P; base < w1; base += blockDim.y * P) {
+            const int w = base + grp;
+            const bool have = w < w1;
+            int4 A = make_int4(0, 0, 0, 0), D = A;
+            if (have) {
+                const int pos = __ldg(work + w);  // the task's position in the factorisation's descriptor arrays
+                A = __ldg(g.pfA + pos);
+                D = __ldg(g.pfB + pos);
+            }
+            const bool wide = have && A.y - A.x > 32;
+            if (have && !wide) pkFactorTask<T, kPkThread>(g, b, A, D, s, act);
+            for (int j = 0; j < P; j++) {
+                if (!__shfl_sync(full, (int)wide, j * S)) continue;
+                const int4 Aw = make_int4(__shfl_sync(full, A.x, j * S), __shfl_sync(full, A.y, j * S),
+                                          __shfl_sync(full, A.z, j * S), __shfl_sync(full, A.w, j * S));
+                const int4 Dw = make_int4(__shfl_sync(full, D.x, j * S), __shfl_sync(full, D.y, j * S),
+                                          __shfl_sync(full, D.z, j * S), __shfl_sync(full, D.w, j * S));
+                pkFactorTask<T, kPkWarp>(g, b, Aw, Dw, s, act);
+            }
         }
         __syncthreads();
     }
