@@ -4135,13 +4135,16 @@ __global__ void __launch_bounds__(256) k_mismatch_noalloc(DevGrid g, int count, 
             qi += vmj * (G * sn - Bv * cs);
         }
         const double P = vmi * pi, Q = vmi * qi;
+        // a voltage-dependent (ZIP) load's deviation from its nominal power, as the solver's mismatch takes it
+        double zdP = 0.0, zdQ = 0.0, zdPdV = 0.0, zdQdV = 0.0;
+        zipLoad(g, i, vmi, g.pload[i], g.qload[i], zdP, zdQ, zdPdV, zdQdV);
         if (g.busP[i] >= 0) {
-            const double f = (g.pgen[i] - g.pload[i]) - P;
+            const double f = (g.pgen[i] - g.pload[i]) - P - zdP;
             localMax = fmax(localMax, fabs(f));
             nonFinite |= isfinite(f) ? 0 : 1;
         }
         if (g.busQ[i] >= 0) {
-            const double f = (g.qgen[i] - g.qload[i]) - Q;
+            const double f = (g.qgen[i] - g.qload[i]) - Q - zdQ;
             localMax = fmax(localMax, fabs(f));
             nonFinite |= isfinite(f) ? 0 : 1;
         }

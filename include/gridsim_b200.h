@@ -489,7 +489,7 @@ int gs_serve_destroy(gs_server *srv);
  * fixed share of a shared GPU), or a latency-bound loop, where cudaMalloc / cudaFree may synchronise the whole
  * device. Computes, for `count` states of the grid, the FP64 max |mismatch| over the grid's equations into
  * d_max_mismatch[count] (NaN for a non-finite mismatch): the mismatch under the grid's own bus types and its
- * base generation and load, with at most one branch out per state. It does not model what some solve options
+ * base generation and load (voltage-dependent loads at the state's voltage), with at most one branch out per state. It does not model what some solve options
  * change (Q-limit PV-to-PQ switches, load scalings, generator and bus outages, outage sets), so for solves
  * with those it is not the quantity the solver tested. d_vm / d_va are the caller's DEVICE arrays,
  * system-major [count][n_bus], angles in radians; d_outage (device, [count], -1 = none) may be NULL. No

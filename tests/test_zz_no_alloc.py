@@ -68,6 +68,36 @@ def test_noalloc_mismatch_matches_the_oracle_and_the_batch_solve_twice():
         assert np.allclose(got, want_intact, rtol=RTOL, atol=ATOL), (call, got, want_intact)
 
 
+def test_noalloc_mismatch_takes_voltage_dependent_loads():
+    """With ZIP loads (a load drawn as Pd (Ap V^2 + Bp V + Cp), Qd likewise) the mismatch is taken at each state's
+    voltages, as the oracle's and the batch solve's are."""
+    import torch
+
+    import oracle
+    from gridsim_b200 import _abi, synthetic
+    from gridsim_b200.engine import PowerFlowOptions, SparseNewtonRaphsonPowerFlow
+
+    m = synthetic.config_grid(0, 0).copy()
+    z = np.tile([0.0, 0.0, 1.0, 0.0, 0.0, 1.0], (m.n_bus, 1))
+    z[::3] = [0.3, 0.3, 0.4, 0.2, 0.3, 0.5]
+    m.zip = z
+    idx = synthetic.outage_set(m, None, 0)[:24].astype(np.int32)
+    solver = SparseNewtonRaphsonPowerFlow("fp64")
+    ref = solver.solve_batch(m, outage=idx, options=PowerFlowOptions(max_iterations=2), keep_states=True)
+    grid = solver.grid_for(m)
+    va_rad = np.radians(ref["va_deg"])
+    dev = torch.device("cuda:0")
+    d_vm = torch.tensor(ref["vm"], dtype=torch.float64, device=dev).contiguous()
+    d_va = torch.tensor(va_rad, dtype=torch.float64, device=dev).contiguous()
+    d_out = torch.tensor(idx, dtype=torch.int32, device=dev)
+    want = oracle.max_mismatch(m, ref["vm"], va_rad, idx)
+    lib = _abi.load_library()
+    for call in range(2):
+        got = _call(lib, grid, idx.shape[0], d_vm, d_va, d_out)
+        assert np.allclose(got, want, rtol=RTOL, atol=ATOL), (call, got, want)
+        assert np.allclose(got, ref["max_mismatch"], rtol=RTOL, atol=ATOL), (call, got, ref["max_mismatch"])
+
+
 def test_noalloc_refuses_more_systems_than_its_scratch_holds():
     from gridsim_b200 import _abi, synthetic
     from gridsim_b200.engine import SparseNewtonRaphsonPowerFlow
