@@ -4187,8 +4187,6 @@ extern "C" int gs_pf_mismatch_noalloc(gs_grid* G, int32_t count, const double* d
     if (count > kNoAllocMaxSystems)
         return SetErr(ctx, GS_ERR_CAPACITY, "gs_pf_mismatch_noalloc: " + std::to_string(count) +
                                               " systems requested, at most " + std::to_string(kNoAllocMaxSystems));
-    if (!G->host.zip.empty())
-        return SetErr(ctx, GS_ERR_UNSUPPORTED, "gs_pf_mismatch_noalloc: the grid has voltage-dependent (ZIP) loads");
     if (count == 0) return GS_OK;
     GS_CUDA(cudaSetDevice(ctx->device));
     unsigned long long* scratch = nullptr;

@@ -160,14 +160,3 @@ def test_zip_with_q_limits_matches_the_oracle(name):
     if ref["status"] == _abi.PF_CONVERGED:
         assert np.max(np.abs(r.vm - ref["vm"])) <= VM_TOL
         assert np.max(np.abs(np.radians(r.va_deg - ref["va_deg"]))) <= VA_TOL_RAD
-
-
-@pytest.mark.gpu
-def test_noalloc_check_refuses_zip_grids():
-    import ctypes
-    from gridsim_b200.engine import SparseNewtonRaphsonPowerFlow
-    m = with_random_zip(synthetic.config_grid(0, 0), 6)
-    grid = SparseNewtonRaphsonPowerFlow("fp64").grid_for(m)
-    dummy = ctypes.c_void_p(16)
-    rc = grid.ctx.lib.gs_pf_mismatch_noalloc(grid.handle, 1, dummy, dummy, None, dummy)
-    assert rc == _abi.GS_ERR_UNSUPPORTED
