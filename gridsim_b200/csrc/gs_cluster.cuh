@@ -22,11 +22,20 @@
 
 namespace gs {
 
-constexpr int kClusterCtas = 8;        // the largest cluster: CTAs per system (the portable cluster size)
+constexpr int kClusterCtas = 8;        // the largest portable cluster: CTAs per system
+constexpr int kClusterCtasWide = 16;   // the non-portable cluster size sm_100a allows, where the device takes it
 constexpr int kClusterThreads = 512;   // threads per CTA (one CTA per SM at the walk's register count)
 constexpr int kClusterMaxSystems = 296; // more systems than this: the full-batch step
+// whether 16-CTA clusters of the walk can be scheduled (set once with the kernels' attributes)
+inline bool& Cluster16Ok() {
+    static bool ok = false;
+    return ok;
+}
 // CTAs per system for n systems: as many as keep the systems' clusters within about one wave of the 148 SMs
-inline int ClusterCtasFor(int n) { return n <= 18 ? 8 : n <= 37 ? 4 : n <= 74 ? 2 : 1; }
+inline int ClusterCtasFor(int n) {
+    if (n <= 9 && Cluster16Ok()) return kClusterCtasWide;
+    return n <= 18 ? 8 : n <= 37 ? 4 : n <= 74 ? 2 : 1;
+}
 constexpr size_t kClusterSmemMax = 64 * 1024;  // the per-phase table in shared memory (16 bytes a phase)
 
 template <typename T>
@@ -494,6 +503,7 @@ cudaError_t LaunchTailClusterC(const DevGrid& g, const DevBatch& b, T* vec, int 
 template <typename T, int W, bool PK>
 cudaError_t LaunchTailClusterK(const DevGrid& g, const DevBatch& b, T* vec, int l0, int l1, int nActive, cudaStream_t st) {
     switch (ClusterCtasFor(nActive)) {
+        case 16: return LaunchTailClusterC<T, W, 16, PK>(g, b, vec, l0, l1, nActive, st);
         case 8: return LaunchTailClusterC<T, W, 8, PK>(g, b, vec, l0, l1, nActive, st);
         case 4: return LaunchTailClusterC<T, W, 4, PK>(g, b, vec, l0, l1, nActive, st);
         case 2: return LaunchTailClusterC<T, W, 2, PK>(g, b, vec, l0, l1, nActive, st);

@@ -4270,7 +4270,11 @@ bool ClusterWalkAvailable() {
             return false;
         }
 #undef GS_CLUSTER_KERNELS
-    // the largest cluster must fit (the smaller ones then do)
+#define GS_CLUSTER_KERNELS16(PK)                                                                                   \
+    (const void*)k_tail_cluster<double, kWorkFactor, 16, PK>, (const void*)k_tail_cluster<double, kWorkBackward, 16, PK>, \
+        (const void*)k_tail_cluster<double, kWorkForward, 16, PK>, (const void*)k_tail_cluster<float, kWorkFactor, 16, PK>, \
+        (const void*)k_tail_cluster<float, kWorkBackward, 16, PK>, (const void*)k_tail_cluster<float, kWorkForward, 16, PK>
+    // the largest portable cluster must fit (the smaller ones then do)
     for (const void* f : {(const void*)k_tail_cluster<double, kWorkFactor, kClusterCtas, false>,
                           (const void*)k_tail_cluster<double, kWorkFactor, kClusterCtas, true>,
                           (const void*)k_tail_cluster<float, kWorkFactor, kClusterCtas, true>})
@@ -4278,6 +4282,21 @@ bool ClusterWalkAvailable() {
             cudaGetLastError();
             return false;
         }
+    // 16-CTA clusters (non-portable) for the last few systems, where the device schedules them
+    bool ok16 = true;
+    const void* k16[] = {GS_CLUSTER_KERNELS16(false), GS_CLUSTER_KERNELS16(true)};
+    for (const void* f : k16)
+        ok16 = ok16 && cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess &&
+               cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClusterSmemMax) == cudaSuccess;
+    if (ok16) {
+        cfg.gridDim = dim3(kClusterCtasWide);
+        attr[0].val.clusterDim.x = kClusterCtasWide;
+        for (const void* f : k16)
+            if (cudaOccupancyMaxActiveClusters(&n, f, &cfg) != cudaSuccess || n < 1) { ok16 = false; break; }
+    }
+#undef GS_CLUSTER_KERNELS16
+    cudaGetLastError();
+    Cluster16Ok() = ok16;
     return true;
 }
 }  // namespace gs
