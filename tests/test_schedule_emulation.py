@@ -7,6 +7,8 @@ Q-limit superset pattern) or a bare matrix (gs::AnalyzeMatrix, the batched linea
 random diagonally dominant matrix and every fill slot with 1e30 (so a wrong "starts from A" bit shows), and runs:
 
 * the paired schedule (2 x 2 units: kPDiag / kPUpper / kPLower / kPFwd and single-node entries) and the scalar one;
+* the one-system walks' top part (FP64 and FP32 budgets): the levels below it on the scalar schedule, the top loaded
+  into a shared-memory image with its external pairs applied, walked there phase by phase and stored back;
 * the fused factorisation + forward substitution, then the backward substitution level by level from the root;
 * the forward-only schedule of a second right-hand side (the mixed-precision refinement's solve).
 
@@ -44,6 +46,7 @@ struct Out {
     int64_t perturbed;  // pivots at or below their floor
     int32_t phases;     // factorisation phases run
     int32_t paired;     // 1 when the paired schedule ran
+    int32_t topLevels;  // levels walked in the top part's shared-memory image
 };
 
 struct Emu {
@@ -184,15 +187,96 @@ void NodeBack(Emu& e, int k) {
     e.y[k] = (e.Y[k] - a) / e.piv[k];
 }
 
+// phases [0, nPh) of a schedule (all of them when nPh < 0), in order or from the last one down
 template <class F>
-void RunPhases(Emu& e, const Symbolic::Schedule& sc, bool reverse, F task) {
-    const int nPh = (int)sc.levelWorkPtr.size() - 1;
+void RunPhases(Emu& e, const Symbolic::Schedule& sc, bool reverse, F task, int nPh = -1) {
+    if (nPh < 0) nPh = (int)sc.levelWorkPtr.size() - 1;
     for (int i = 0; i < nPh; i++) {
         const int ph = reverse ? nPh - 1 - i : i;
         e.snap();
         for (int w = sc.levelWorkPtr[ph]; w < sc.levelWorkPtr[ph + 1]; w++) task(sc.work[w]);
     }
 }
+
+// The one-system walks' top part (factorSystem / backwardSystem / forwardSystem): the levels from L0 up held in a
+// shared-memory image `sm`, loaded from global memory with the external pairs applied, walked phase by phase (every
+// entry of a phase reading the image from before the phase), stored back. Every image value starts as 1e30, so a
+// value read before it is loaded shows.
+struct TopEmu {
+    Emu& e;
+    const Symbolic::TopPart& t;
+    std::vector<double> sm, S;
+    TopEmu(Emu& em, const Symbolic::TopPart& tp) : e(em), t(tp) {}
+    double ext(int ti, const std::vector<double>& rhs, bool fwd) {
+        double acc = 0.0;
+        for (int q = t.extPtr[ti]; q < t.extPtr[ti + 1]; q++)
+            acc += e.lu[t.extPairs[2 * q]] * (fwd ? rhs[t.extPairs[2 * q + 1]] : e.lu[t.extPairs[2 * q + 1]]);
+        return acc;
+    }
+    double dot(int ti) {
+        double acc = 0.0;
+        for (int q = t.intPtr[ti]; q < t.intPtr[ti + 1]; q++) acc += S[t.intPairs[2 * q]] * S[t.intPairs[2 * q + 1]];
+        return acc;
+    }
+    void load(const std::vector<int32_t>& list, const std::vector<double>& rhs) {
+        const Symbolic& s = e.s;
+        for (int ti : list) {
+            const int en = t.ent[ti];
+            const bool fwd = s.entKind[en] == gs::kFwd;
+            const double base = fwd ? rhs[s.entNode[en]] : (s.entHasA[en] ? e.lu[s.entSlot[en]] : 0.0);
+            sm[t.entSm[ti]] = base - ext(ti, rhs, fwd);
+        }
+    }
+    void factor() {
+        const Symbolic& s = e.s;
+        sm.assign(t.nSlots + t.nNodes, 1e30);
+        load(t.loadList, e.y);
+        const int nTop = s.nLevels - t.L0;
+        for (int i = 0; i < 2 * nTop; i++) {
+            S = sm;
+            for (int w = t.fWalkPtr[i]; w < t.fWalkPtr[i + 1]; w++) {
+                const int ti = t.fWalk[w], en = t.ent[ti], idx = t.entSm[ti], kind = s.entKind[en];
+                double v = S[idx] - dot(ti);
+                if (kind == gs::kDiag) v = e.pivot(s.entHasA[en] ? e.lu[s.entSlot[en]] : 0.0, v);
+                else if (kind == gs::kLower) v = v / S[t.smemBase[s.entNode[en]]];
+                sm[idx] = v;
+            }
+        }
+        for (int q = 0; q < t.nSlots; q++) {
+            if (t.slotDiagNode[q] >= 0) e.putPiv(t.slotDiagNode[q], sm[q]);
+            else e.putLu(t.slotGlobal[q], sm[q]);
+        }
+        for (int i = 0; i < t.nNodes; i++) e.putY(t.nodes[i], sm[t.nSlots + i]);
+    }
+    void backward() {
+        const Symbolic& s = e.s;
+        sm.assign(t.nSlots + t.nNodes, 1e30);
+        for (int q = 0; q < t.nSlots; q++)
+            sm[q] = t.slotDiagNode[q] >= 0 ? e.piv[t.slotDiagNode[q]] : e.lu[t.slotGlobal[q]];
+        for (int i = 0; i < t.nNodes; i++) sm[t.nSlots + i] = e.y[t.nodes[i]];
+        for (int lt = s.nLevels - t.L0 - 1; lt >= 0; lt--) {
+            S = sm;
+            for (int w = t.bWalkPtr[lt]; w < t.bWalkPtr[lt + 1]; w++) {
+                const int ni = t.bWalk[w], k = t.nodes[ni], base = t.smemBase[k], c = s.luCnt[k];
+                double acc = 0.0;
+                for (int u = 0; u < c; u++) acc += S[base + 1 + u] * S[t.bRowSm[t.bRowPtr[ni] + u]];
+                sm[t.nSlots + ni] = (S[t.nSlots + ni] - acc) / S[base];
+            }
+        }
+        for (int i = 0; i < t.nNodes; i++) e.y[t.nodes[i]] = sm[t.nSlots + i];
+    }
+    void forward() {
+        const Symbolic& s = e.s;
+        sm.assign(t.nSlots + t.nNodes, 1e30);
+        for (int q = 0; q < t.nSlots; q++) sm[q] = e.lu[t.slotGlobal[q]];
+        load(t.fwdLoadList, e.y);
+        for (int lt = 0; lt < s.nLevels - t.L0; lt++) {
+            S = sm;
+            for (int w = t.vWalkPtr[lt]; w < t.vWalkPtr[lt + 1]; w++) sm[t.entSm[t.vWalk[w]]] = S[t.entSm[t.vWalk[w]]] - dot(t.vWalk[w]);
+        }
+        for (int i = 0; i < t.nNodes; i++) e.y[t.nodes[i]] = sm[t.nSlots + i];
+    }
+};
 
 double Residual(const Symbolic& s, const std::vector<double>& a, const std::vector<double>& x,
                 const std::vector<double>& b) {
@@ -204,9 +288,15 @@ double Residual(const Symbolic& s, const std::vector<double>& a, const std::vect
     return num / den;
 }
 
-int Emulate(const Symbolic& s, bool usePaired, uint64_t seed, Out* out) {
+// mode 0: the scalar schedule; 1: the paired one; 2 / 3: the scalar one below the FP64 / FP32 top part, the top
+// part walked as the one-system kernels walk it
+int Emulate(const Symbolic& s, int mode, uint64_t seed, Out* out) {
     const Symbolic::PairSchedule& P = s.ps;
+    const bool usePaired = mode == 1;
     if (usePaired && !P.on) return -3;
+    const Symbolic::TopPart* tp = mode >= 2 ? &s.top[mode - 2] : nullptr;
+    const bool top = tp && tp->L0 < s.nLevels;
+    const int L0 = top ? tp->L0 : s.nLevels;
     std::mt19937_64 rng(seed);
     std::uniform_real_distribution<double> U(-1.0, 1.0);
     // a random row diagonally dominant matrix on the matrix's own cells; every other slot holds 1e30
@@ -240,10 +330,12 @@ int Emulate(const Symbolic& s, bool usePaired, uint64_t seed, Out* out) {
         RunPhases(e, s.factor, false, [&](int en) {
             Entry(e, s.entKind[en], s.entHasA[en] != 0, s.entNode[en], s.entSlot[en], s.pairs, s.entPairPtr[en],
                   s.entPairPtr[en + 1]);
-        });
+        }, 2 * L0);
     }
-    const Symbolic::Schedule& fs = usePaired ? P.factor : s.factor;
-    out->phases = (int)fs.levelWorkPtr.size() - 1;
+    TopEmu te(e, top ? *tp : s.top[0]);
+    if (top) te.factor();
+    out->phases = usePaired ? (int)P.factor.levelWorkPtr.size() - 1 : 2 * s.nLevels;
+    out->topLevels = s.nLevels - L0;
     int64_t rewrites = 0;
     for (int v : e.wLu) rewrites += v > 1;
     for (int v : e.wY) rewrites += v > 1;
@@ -252,8 +344,9 @@ int Emulate(const Symbolic& s, bool usePaired, uint64_t seed, Out* out) {
     out->perturbed = e.perturbed;
     out->paired = usePaired ? 1 : 0;
     auto backward = [&]() {
-        if (usePaired) RunPhases(e, P.backward, true, [&](int t) { PairBack(e, P, t); });
-        else RunPhases(e, s.backward, true, [&](int q) { NodeBack(e, s.levelNodes[q]); });
+        if (usePaired) { RunPhases(e, P.backward, true, [&](int t) { PairBack(e, P, t); }); return; }
+        if (top) te.backward();
+        RunPhases(e, s.backward, true, [&](int q) { NodeBack(e, s.levelNodes[q]); }, L0);
     };
     backward();
     out->resid = Residual(s, a, e.y, b);
@@ -266,7 +359,8 @@ int Emulate(const Symbolic& s, bool usePaired, uint64_t seed, Out* out) {
             double acc[4];
             Sums(s.pairs, s.entPairPtr[en], s.entPairPtr[en + 1], 1, e.L, e.Y, acc);
             e.y[s.entSlot[en]] = e.Y[s.entSlot[en]] - acc[0];
-        });
+        }, L0);
+        if (top) te.forward();
     }
     backward();
     out->residFwd = Residual(s, a, e.y, b2);
@@ -274,27 +368,31 @@ int Emulate(const Symbolic& s, bool usePaired, uint64_t seed, Out* out) {
 }
 }  // namespace
 
-extern "C" int emulate_grid(const gs_grid_desc* d, int qlim, int paired, unsigned long long seed, Out* out) {
+extern "C" int emulate_grid(const gs_grid_desc* d, int qlim, int mode, unsigned long long seed, Out* out) {
     gs::HostGrid g;
     if (!gs::CopyGrid(d, g).empty()) return -1;
     Symbolic s;
     if (!gs::Analyze(g, s, qlim != 0).empty()) return -2;
-    return Emulate(s, paired != 0, seed, out);
+    return Emulate(s, mode, seed, out);
 }
 
-extern "C" int emulate_matrix(int n, const int* rowPtr, const int* colIdx, int paired, unsigned long long seed,
+extern "C" int emulate_matrix(int n, const int* rowPtr, const int* colIdx, int mode, unsigned long long seed,
                               Out* out) {
     Symbolic s;
     std::vector<int> aSlot;
     if (!gs::AnalyzeMatrix(n, rowPtr, colIdx, s, aSlot).empty()) return -2;
-    return Emulate(s, paired != 0, seed, out);
+    return Emulate(s, mode, seed, out);
 }
 '''
 
 
 class Out(ctypes.Structure):
     _fields_ = [("resid", ctypes.c_double), ("resid_fwd", ctypes.c_double), ("rewrites", ctypes.c_int64),
-                ("perturbed", ctypes.c_int64), ("phases", ctypes.c_int32), ("paired", ctypes.c_int32)]
+                ("perturbed", ctypes.c_int64), ("phases", ctypes.c_int32), ("paired", ctypes.c_int32),
+                ("top_levels", ctypes.c_int32)]
+
+# the schedules run: the paired one, the scalar one, and the scalar one below the FP64 / FP32 top part
+MODES = {"paired": 1, "scalar": 0, "top_fp64": 2, "top_fp32": 3}
 
 
 # rounding level of a diagonally dominant solve of a few thousand unknowns in FP64
@@ -320,8 +418,9 @@ def grid_2000():
     return synthetic.config_grid(1, 0)
 
 
-def _check(out):
+def _check(out, mode):
     assert out.rewrites == 0
+    assert (out.top_levels > 0) == (mode >= 2)
     assert out.perturbed == 0
     assert out.phases > 0
     assert out.resid < RESID_TOL
@@ -329,25 +428,25 @@ def _check(out):
 
 
 @pytest.mark.parametrize("qlim", [0, 1])
-@pytest.mark.parametrize("paired", [1, 0])
+@pytest.mark.parametrize("schedule", list(MODES))
 @pytest.mark.parametrize("name", ["case9", "case118", "case300"])
-def test_case_schedules_solve(harness, name, paired, qlim):
+def test_case_schedules_solve(harness, name, schedule, qlim):
     m, _ = golden_model(name)
     d = m.desc()
     out = Out()
-    rc = harness.emulate_grid(ctypes.byref(d), qlim, paired, 7, ctypes.byref(out))
+    rc = harness.emulate_grid(ctypes.byref(d), qlim, MODES[schedule], 7, ctypes.byref(out))
     assert rc == 0
-    _check(out)
+    _check(out, MODES[schedule])
 
 
 @pytest.mark.parametrize("qlim", [0, 1])
-@pytest.mark.parametrize("paired", [1, 0])
-def test_2000_bus_schedules_solve(harness, grid_2000, paired, qlim):
+@pytest.mark.parametrize("schedule", list(MODES))
+def test_2000_bus_schedules_solve(harness, grid_2000, schedule, qlim):
     d = grid_2000.desc()
     out = Out()
-    rc = harness.emulate_grid(ctypes.byref(d), qlim, paired, 11, ctypes.byref(out))
+    rc = harness.emulate_grid(ctypes.byref(d), qlim, MODES[schedule], 11, ctypes.byref(out))
     assert rc == 0
-    _check(out)
+    _check(out, MODES[schedule])
 
 
 def _random_pattern(n, per_row, symmetric, seed):
@@ -374,12 +473,12 @@ def _random_pattern(n, per_row, symmetric, seed):
                                                        (300, 3, True, 3), (600, 2, False, 4), (1500, 3, False, 5)])
 def test_matrix_schedules_solve(harness, n, per_row, symmetric, seed):
     row_ptr, col = _random_pattern(n, per_row, symmetric, seed)
-    for paired in (1, 0):
+    for mode in MODES.values():
         out = Out()
         rc = harness.emulate_matrix(n, row_ptr.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
-                                    col.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), paired, seed,
+                                    col.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), mode, seed,
                                     ctypes.byref(out))
-        if paired and rc == -3:  # no paired schedule for this pattern: the scalar one serves it
+        if mode == 1 and rc == -3:  # no paired schedule for this pattern: the scalar one serves it
             continue
         assert rc == 0
-        _check(out)
+        _check(out, mode)
