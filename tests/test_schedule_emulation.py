@@ -30,6 +30,7 @@ CSRC = os.path.join(ROOT, "gridsim_b200", "csrc")
 
 HARNESS = r'''
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdint>
 #include <random>
@@ -47,6 +48,7 @@ struct Out {
     int32_t phases;     // factorisation phases run
     int32_t paired;     // 1 when the paired schedule ran
     int32_t topLevels;  // levels walked in the top part's shared-memory image
+    int64_t itemErrors; // violations of the item structure the kernels rely on (CheckItems)
 };
 
 struct Emu {
@@ -278,6 +280,65 @@ struct TopEmu {
     }
 };
 
+// The item structure the kernels rely on, per phase of a schedule: items cover the phase's work in order; the wide
+// ones (count -1, one piece for the whole warp) come first, levelWide of them; the others hold 1 .. 8 pieces (a warp's
+// lane groups), each short enough for a lane group's one round of loads (at most 32 index pairs or rows), ordered
+// longest first, with levelMid of them longer than `midAbove`. `len` gives a piece's length as the packing measured it,
+// `raw` its index pairs (or rows). Returns the number of violations.
+template <class Len, class Raw>
+int64_t CheckItems(const Symbolic::Schedule& sc, int midAbove, Len len, Raw raw) {
+    int64_t bad = 0;
+    const int nPh = (int)sc.levelWorkPtr.size() - 1;
+    if ((int)sc.levelItemPtr.size() != nPh + 1 || (int)sc.levelWide.size() != nPh || (int)sc.levelMid.size() != nPh)
+        return 1;
+    for (int ph = 0; ph < nPh; ph++) {
+        int w = sc.levelWorkPtr[ph], wide = 0, mid = 0;
+        bool inShort = false;
+        int64_t prev = INT64_MAX;
+        for (int it = sc.levelItemPtr[ph]; it < sc.levelItemPtr[ph + 1]; it++) {
+            const int start = sc.items[2 * it], count = sc.items[2 * it + 1];
+            if (start != w) bad++;
+            if (count < 0) {
+                if (inShort) bad++;
+                if (len(sc.work[start]) <= 32) bad++;
+                wide++;
+                w++;
+                continue;
+            }
+            inShort = true;
+            if (count < 1 || count > 8) bad++;
+            for (int q = start; q < start + count; q++) {
+                const int64_t l = len(sc.work[q]);
+                if (l > 32 || raw(sc.work[q]) > 32 || l > prev) bad++;
+                if (l > midAbove) mid++;
+                prev = l;
+            }
+            w += std::max(count, 0);
+        }
+        if (w != sc.levelWorkPtr[ph + 1] || wide != sc.levelWide[ph] || mid != sc.levelMid[ph]) bad++;
+    }
+    return bad;
+}
+
+int64_t CheckAllItems(const Symbolic& s) {
+    int64_t bad = 0;
+    auto ePairs = [&](int e) { return s.entPairPtr[e + 1] - s.entPairPtr[e]; };
+    bad += CheckItems(s.factor, 8, ePairs, ePairs);
+    bad += CheckItems(s.forward, 8, ePairs, ePairs);
+    auto nRows = [&](int q) { return (int64_t)s.luCnt[s.levelNodes[q]]; };
+    bad += CheckItems(s.backward, 8, nRows, nRows);
+    const Symbolic::PairSchedule& P = s.ps;
+    if (P.on) {
+        auto tPairs = [&](int t) { return (int64_t)P.taskA[4 * (size_t)t + 1] - P.taskA[4 * (size_t)t]; };
+        auto tLen = [&](int t) { return ((P.taskA[4 * (size_t)t + 2] & 7) == gs::kPDiag ? 2 : 1) * tPairs(t); };
+        bad += CheckItems(P.factor, 4, tLen, tPairs);
+        bad += CheckItems(P.forward, 4, tPairs, tPairs);
+        auto bRows = [&](int t) { return (int64_t)P.bTaskA[4 * (size_t)t + 1] - P.bTaskA[4 * (size_t)t]; };
+        bad += CheckItems(P.backward, 4, bRows, bRows);
+    }
+    return bad;
+}
+
 double Residual(const Symbolic& s, const std::vector<double>& a, const std::vector<double>& x,
                 const std::vector<double>& b) {
     std::vector<double> r(b);
@@ -343,6 +404,7 @@ int Emulate(const Symbolic& s, int mode, uint64_t seed, Out* out) {
     out->rewrites = rewrites;
     out->perturbed = e.perturbed;
     out->paired = usePaired ? 1 : 0;
+    out->itemErrors = CheckAllItems(s);
     auto backward = [&]() {
         if (usePaired) { RunPhases(e, P.backward, true, [&](int t) { PairBack(e, P, t); }); return; }
         if (top) te.backward();
@@ -389,7 +451,7 @@ extern "C" int emulate_matrix(int n, const int* rowPtr, const int* colIdx, int m
 class Out(ctypes.Structure):
     _fields_ = [("resid", ctypes.c_double), ("resid_fwd", ctypes.c_double), ("rewrites", ctypes.c_int64),
                 ("perturbed", ctypes.c_int64), ("phases", ctypes.c_int32), ("paired", ctypes.c_int32),
-                ("top_levels", ctypes.c_int32)]
+                ("top_levels", ctypes.c_int32), ("item_errors", ctypes.c_int64)]
 
 # the schedules run: the paired one, the scalar one, and the scalar one below the FP64 / FP32 top part
 MODES = {"paired": 1, "scalar": 0, "top_fp64": 2, "top_fp32": 3}
@@ -419,6 +481,7 @@ def grid_2000():
 
 
 def _check(out, mode):
+    assert out.item_errors == 0
     assert out.rewrites == 0
     assert (out.top_levels > 0) == (mode >= 2)
     assert out.perturbed == 0
