@@ -1,5 +1,6 @@
 """The seeded synthetic grids of the benchmark workloads (CPU)."""
 import numpy as np
+import pytest
 
 import oracle
 from gridsim_b200 import _abi, synthetic
@@ -64,3 +65,19 @@ def test_case_directory_round_trip(tmp_path):
     assert np.array_equal(back.bus_type, m.bus_type)
     r1, r2 = oracle.solve(m), oracle.solve(back)
     assert np.allclose(r1["vm"], r2["vm"], atol=1e-12)
+
+
+def test_stressed_operating_point_is_a_solution_closer_to_the_limit():
+    """margin 0.9 (the stressed screen): the stored start still solves, at 1.5 x the load of the default 0.6 margin
+    (both a fraction of the same last solvable level), and its outages take at least as many Newton steps."""
+    base = synthetic.config_grid(1, 0)
+    stressed = synthetic.config_grid(1, 0, margin=0.9)
+    r = oracle.solve(stressed)
+    assert r["status"] == _abi.PF_CONVERGED
+    assert r["iterations"] <= 1
+    assert stressed.meta["load_scale"] / base.meta["load_scale"] == pytest.approx(0.9 / 0.6, rel=1e-12)
+    assert np.array_equal(stressed.tap, base.tap) and np.array_equal(stressed.vg, base.vg)
+    idx = np.arange(0, 40, dtype=np.int32)
+    it_base = oracle.screen(base, idx)["iterations"]
+    it_stressed = oracle.screen(stressed, idx)["iterations"]
+    assert np.sum(it_stressed) >= np.sum(it_base)
