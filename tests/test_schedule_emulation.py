@@ -10,7 +10,9 @@ random diagonally dominant matrix and every fill slot with 1e30 (so a wrong "sta
 * the one-system walks' top part (FP64 and FP32 budgets): the levels below it on the scalar schedule, the top loaded
   into a shared-memory image with its external pairs applied, walked there phase by phase and stored back;
 * the fused factorisation + forward substitution, then the backward substitution level by level from the root;
-* the forward-only schedule of a second right-hand side (the mixed-precision refinement's solve).
+* the forward-only schedule of a second right-hand side (the mixed-precision refinement's solve);
+* the factorisation with a subtree cut: the subtrees below the cut each alone, stage by stage (k_psubtree), then the
+  paired schedule's levels above it.
 
 Each solve must leave |A x - b| at rounding level; no LU slot, pivot or right-hand-side entry may be written twice in
 one factorisation, and no pivot may collapse. The task semantics restate the device's (gs_paired.cuh pkFactorTask,
@@ -189,12 +191,12 @@ void NodeBack(Emu& e, int k) {
     e.y[k] = (e.Y[k] - a) / e.piv[k];
 }
 
-// phases [0, nPh) of a schedule (all of them when nPh < 0), in order or from the last one down
+// phases [from, nPh) of a schedule (nPh < 0: to the last), in order or from the last one down
 template <class F>
-void RunPhases(Emu& e, const Symbolic::Schedule& sc, bool reverse, F task, int nPh = -1) {
+void RunPhases(Emu& e, const Symbolic::Schedule& sc, bool reverse, F task, int nPh = -1, int from = 0) {
     if (nPh < 0) nPh = (int)sc.levelWorkPtr.size() - 1;
-    for (int i = 0; i < nPh; i++) {
-        const int ph = reverse ? nPh - 1 - i : i;
+    for (int i = from; i < nPh; i++) {
+        const int ph = reverse ? nPh - 1 - (i - from) : i;
         e.snap();
         for (int w = sc.levelWorkPtr[ph]; w < sc.levelWorkPtr[ph + 1]; w++) task(sc.work[w]);
     }
@@ -350,12 +352,13 @@ double Residual(const Symbolic& s, const std::vector<double>& a, const std::vect
 }
 
 // mode 0: the scalar schedule; 1: the paired one; 2 / 3: the scalar one below the FP64 / FP32 top part, the top
-// part walked as the one-system kernels walk it
-int Emulate(const Symbolic& s, int mode, uint64_t seed, Out* out) {
+// part walked as the one-system kernels walk it; 4: the paired one with the subtrees below unit level `cut` factored
+// first (k_psubtree: each subtree alone, stage by stage), then the levels above the cut
+int Emulate(const Symbolic& s, int mode, uint64_t seed, Out* out, int cut = -1) {
     const Symbolic::PairSchedule& P = s.ps;
-    const bool usePaired = mode == 1;
+    const bool usePaired = mode == 1 || mode == 4;
     if (usePaired && !P.on) return -3;
-    const Symbolic::TopPart* tp = mode >= 2 ? &s.top[mode - 2] : nullptr;
+    const Symbolic::TopPart* tp = (mode == 2 || mode == 3) ? &s.top[mode - 2] : nullptr;
     const bool top = tp && tp->L0 < s.nLevels;
     const int L0 = top ? tp->L0 : s.nLevels;
     std::mt19937_64 rng(seed);
@@ -385,7 +388,16 @@ int Emulate(const Symbolic& s, int mode, uint64_t seed, Out* out) {
     e.wLu.assign(s.nnzLU, 0);
     e.wPiv.assign(s.m, 0);
     e.wY.assign(s.m, 0);
-    if (usePaired) {
+    if (mode == 4) {
+        const gs::SubtreeSchedule st = gs::BuildSubtrees(s, cut);
+        if (st.nSub <= 0) return -5;
+        for (int sub = 0; sub < st.nSub; sub++)
+            for (int q = st.subStage[sub]; q < st.subStage[sub + 1]; q++) {
+                e.snap();
+                for (int w = st.stagePtr[q]; w < st.stagePtr[q + 1]; w++) PairTask(e, P, P.factor.work[st.work[w]]);
+            }
+        RunPhases(e, P.factor, false, [&](int t) { PairTask(e, P, t); }, -1, 2 * (cut + 1));
+    } else if (usePaired) {
         RunPhases(e, P.factor, false, [&](int t) { PairTask(e, P, t); });
     } else {
         RunPhases(e, s.factor, false, [&](int en) {
@@ -438,6 +450,14 @@ extern "C" int emulate_grid(const gs_grid_desc* d, int qlim, int mode, unsigned 
     return Emulate(s, mode, seed, out);
 }
 
+extern "C" int emulate_grid_subtrees(const gs_grid_desc* d, int cut, unsigned long long seed, Out* out) {
+    gs::HostGrid g;
+    if (!gs::CopyGrid(d, g).empty()) return -1;
+    Symbolic s;
+    if (!gs::Analyze(g, s).empty()) return -2;
+    return Emulate(s, 4, seed, out, cut);
+}
+
 extern "C" int emulate_matrix(int n, const int* rowPtr, const int* colIdx, int mode, unsigned long long seed,
                               Out* out) {
     Symbolic s;
@@ -472,6 +492,7 @@ def harness(tmp_path_factory):
     h = ctypes.CDLL(str(lib))
     h.emulate_grid.restype = ctypes.c_int
     h.emulate_matrix.restype = ctypes.c_int
+    h.emulate_grid_subtrees.restype = ctypes.c_int
     return h
 
 
@@ -545,3 +566,14 @@ def test_matrix_schedules_solve(harness, n, per_row, symmetric, seed):
             continue
         assert rc == 0
         _check(out, mode)
+
+
+@pytest.mark.parametrize("cut", [0, 2, 4, 12, 30])
+def test_2000_bus_subtrees_then_levels_solve(harness, grid_2000, cut):
+    """The factorisation as it runs with a subtree cut: the subtrees below unit level `cut` each alone, stage by stage
+    (one CTA per subtree and system group), then the paired schedule's levels above the cut."""
+    d = grid_2000.desc()
+    out = Out()
+    rc = harness.emulate_grid_subtrees(ctypes.byref(d), cut, 13, ctypes.byref(out))
+    assert rc == 0
+    _check(out, 1)
