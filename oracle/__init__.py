@@ -48,6 +48,8 @@ def _load():
                                              i32, vp, vp, vp]
         lib.gso_outage_topology.argtypes = [ctypes.POINTER(_abi.GridDesc), ctypes.c_double, i32, vp, vp, vp]
         lib.gso_sparse_solve.argtypes = [i32, vp, vp, vp, vp, vp]
+        lib.gso_ilu0_apply.argtypes = [i32, vp, vp, vp, vp, vp]
+        lib.gso_bicgstab.argtypes = [i32, vp, vp, vp, vp, ctypes.c_double, i32, vp]
         lib.gso_max_mismatch.argtypes = [ctypes.POINTER(_abi.GridDesc), i32, vp, vp, vp, vp]
         _lib = lib
     return _lib
@@ -269,3 +271,29 @@ def sparse_solve(row_ptr, col_idx, val, b):
     x = np.zeros(rp.shape[0] - 1)
     rc = lib.gso_sparse_solve(rp.shape[0] - 1, _p(rp), _p(ci), _p(v), _p(bb), _p(x))
     return None if rc else x
+
+
+def _csr(row_ptr, col_idx, val):
+    return (np.ascontiguousarray(row_ptr, np.int32), np.ascontiguousarray(col_idx, np.int32),
+            np.ascontiguousarray(val, np.float64))
+
+
+def ilu0_apply(row_ptr, col_idx, val, r):
+    """Ilu0.Factor(A).Apply(r) (Numerics/Sparse.cs:240-300): z with the ILU(0) factors and the row-relative guard."""
+    lib = _load()
+    rp, ci, v = _csr(row_ptr, col_idx, val)
+    rr = np.ascontiguousarray(r, np.float64)
+    z = np.zeros(rp.shape[0] - 1)
+    lib.gso_ilu0_apply(rp.shape[0] - 1, _p(rp), _p(ci), _p(v), _p(rr), _p(z))
+    return z
+
+
+def bicgstab(row_ptr, col_idx, val, b, tol=1e-10, max_iter=0):
+    """BiCgStab.Solve with the ILU(0) preconditioner (Numerics/Sparse.cs:319-405; tol default
+    NumericTolerances.DefaultKrylovTolerance, max_iter 0 = 4n + 200): (accepted, x)."""
+    lib = _load()
+    rp, ci, v = _csr(row_ptr, col_idx, val)
+    bb = np.ascontiguousarray(b, np.float64)
+    x = np.zeros(rp.shape[0] - 1)
+    rc = lib.gso_bicgstab(rp.shape[0] - 1, _p(rp), _p(ci), _p(v), _p(bb), float(tol), int(max_iter), _p(x))
+    return rc == 0, x

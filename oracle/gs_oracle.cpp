@@ -1516,6 +1516,39 @@ int gso_sparse_solve(int32_t n, const int32_t* rowPtr, const int32_t* colIdx, co
     return GS_OK;
 }
 
+// The singular-step fallback's two pieces on their own, for pinning them on the reference's known answers:
+// Ilu0.Factor then Apply (Numerics/Sparse.cs:240-300), and BiCgStab.Solve with that preconditioner
+// (Sparse.cs:319-405; maxIter 0 = the shared cap 4n + 200, NumericTolerances.cs:256-260). BiCGSTAB returns 1 when
+// it is not accepted.
+int gso_ilu0_apply(int32_t n, const int32_t* rowPtr, const int32_t* colIdx, const double* val, const double* r,
+                   double* z) {
+    Csr a;
+    a.n = n;
+    a.rowPtr.assign(rowPtr, rowPtr + n + 1);
+    a.colIdx.assign(colIdx, colIdx + rowPtr[n]);
+    a.val.assign(val, val + rowPtr[n]);
+    Ilu0 pc;
+    pc.Factor(a);
+    std::vector<double> rv(r, r + n), zv(n, 0.0);
+    pc.Apply(rv, zv);
+    for (int i = 0; i < n; i++) z[i] = zv[i];
+    return GS_OK;
+}
+int gso_bicgstab(int32_t n, const int32_t* rowPtr, const int32_t* colIdx, const double* val, const double* b,
+                 double tol, int32_t maxIter, double* x) {
+    Csr a;
+    a.n = n;
+    a.rowPtr.assign(rowPtr, rowPtr + n + 1);
+    a.colIdx.assign(colIdx, colIdx + rowPtr[n]);
+    a.val.assign(val, val + rowPtr[n]);
+    Ilu0 pc;
+    pc.Factor(a);
+    std::vector<double> bv(b, b + n), xv;
+    const bool ok = BiCgStab(a, bv, xv, pc, tol, maxIter > 0 ? maxIter : 4 * n + 200);
+    for (int i = 0; i < n; i++) x[i] = xv[i];
+    return ok ? GS_OK : 1;
+}
+
 }  // extern "C"
 
 namespace {

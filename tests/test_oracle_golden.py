@@ -83,3 +83,57 @@ def test_max_mismatch_of_screen_states_is_the_screens_own():
     assert got.max() > 1e-6
     intact = oracle.max_mismatch(m, r["vm"], np.radians(r["va_deg"]))
     assert not np.allclose(intact, got)
+
+
+def _dense_csr(a):
+    """CSR of a dense matrix: its nonzero cells and the diagonal."""
+    a = np.asarray(a, float)
+    rp, ci, v = [0], [], []
+    for i, row in enumerate(a):
+        for j, x in enumerate(row):
+            if x != 0.0 or i == j:
+                ci.append(j)
+                v.append(x)
+        rp.append(len(ci))
+    return rp, ci, v
+
+
+def test_ilu0_guard_is_relative_at_a_tiny_scale():
+    """NumericTolerancesTests.cs:287-301 (Ilu0_guard_is_relative_so_a_small_scale_matrix_keeps_its_exact_factors):
+    for a 2 x 2 matrix ILU(0) is the full LU, so Apply solves A z = r exactly even at scale 1e-14."""
+    s = 1e-14
+    z = oracle.ilu0_apply(*_dense_csr([[4 * s, 1 * s], [1 * s, 3 * s]]), [5 * s, 4 * s])
+    assert abs(z[0] - 1.0) < 1e-12 and abs(z[1] - 1.0) < 1e-12
+
+
+def test_ilu0_guard_regularises_a_zero_pivot():
+    """NumericTolerancesTests.cs:303-310: a structurally zero second pivot is pushed to 1e-12 x its row scale, so
+    Apply stays finite."""
+    z = oracle.ilu0_apply(*_dense_csr([[1, 1], [1, 1]]), [1.0, 1.0])
+    assert np.all(np.isfinite(z))
+
+
+def test_bicgstab_solves_the_reference_two_by_two():
+    """NumericTolerancesTests.cs:312-323: BiCGSTAB with the default tolerance and cap solves [[4,1],[1,3]] x = [5,4]
+    to x = [1, 1] (ten decimals)."""
+    ok, x = oracle.bicgstab(*_dense_csr([[4, 1], [1, 3]]), [5.0, 4.0])
+    assert ok
+    assert x == pytest.approx([1.0, 1.0], abs=5e-11)
+
+
+def test_bicgstab_on_a_larger_system_matches_a_dense_solve():
+    """The same pieces on a sparse, diagonally dominant 200 x 200 system: accepted, and within the true-residual
+    tolerance of the dense solution."""
+    rng = np.random.default_rng(5)
+    n = 200
+    a = np.zeros((n, n))
+    for i in range(n):
+        for j in rng.choice(n, 4, replace=False):
+            a[i, j] = rng.uniform(-1, 1)
+        a[i, i] = np.sum(np.abs(a[i])) + 1.0
+    b = rng.uniform(-1, 1, n)
+    ok, x = oracle.bicgstab(*_dense_csr(a), b)
+    assert ok
+    want = np.linalg.solve(a, b)
+    assert np.linalg.norm(a @ x - b) / np.linalg.norm(b) < 1e-10
+    assert np.max(np.abs(x - want)) < 1e-8
