@@ -162,3 +162,35 @@ def test_zero_diagonals_are_solved_through_a_row_transversal():
     rp = np.array([0, 1, 2, 4], np.int32)
     ci = np.array([1, 2, 1, 2], np.int32)
     assert solver.solve((rp, ci, np.array([1.0, 2.0, 3.0, 4.0])), np.ones(3)) is None
+
+
+def _csr_of(a):
+    a = np.asarray(a, float)
+    rows, cols = np.nonzero(a)
+    indptr = np.searchsorted(rows, np.arange(a.shape[0] + 1)).astype(np.int32)
+    return indptr, cols.astype(np.int32), a[rows, cols]
+
+
+def test_oracle_pivot_floor_is_per_row():
+    """Gr044RowRelativePivotFloorTests.cs:85-100: diag(1e6, 1e-9) is well conditioned row by row (row 1's floor is
+    1e-21), so the sparse LU solves it, bit for bit 1 / 1e6 and 1 / 1e-9."""
+    x = oracle.sparse_solve(*_csr_of([[1e6, 0.0], [0.0, 1e-9]]), [1.0, 1.0])
+    assert x is not None
+    assert x[0] == 1.0 / 1e6 and x[1] == 1.0 / 1e-9
+
+
+def test_oracle_pivot_floor_boundary():
+    """Gr044RowRelativePivotFloorTests.cs:143-157: [[1, 0], [1, p]] with row 1's scale 1, so its floor is exactly
+    1e-12 (NumericTolerances.PivotFloor(1.0)): p at the floor is singular, the next double above it is not."""
+    at_floor = 1e-12 * 1.0
+    above = np.nextafter(at_floor, np.inf)
+    assert oracle.sparse_solve(*_csr_of([[1.0, 0.0], [1.0, at_floor]]), [1.0, 1.0]) is None
+    x = oracle.sparse_solve(*_csr_of([[1.0, 0.0], [1.0, above]]), [1.0, 2.0])
+    assert x is not None
+    assert x[0] == 1.0 and x[1] == (2.0 - 1.0) / above
+
+
+def test_oracle_near_singular_row_in_small_units_is_refused():
+    """Gr044RowRelativePivotFloorTests.cs:170-176: row 1 has scale 1 and its pivot 1e-13 is below its own 1e-12
+    floor."""
+    assert oracle.sparse_solve(*_csr_of([[1e6, 0.0], [1.0, 1e-13]]), [1.0, 1.0]) is None
