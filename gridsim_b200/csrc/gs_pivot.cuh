@@ -9,8 +9,10 @@
 // pivot, refused at or below the row's floor 1e-12 x max |A(row, :)| (:129-162, NumericTolerances.cs:36,
 // RowPivotFloorsCsc :99-116)), then the forward and backward solve (:314-371). Cells whose value is exactly zero
 // are left out, as SparseLu.ToCsc does (Numerics/SparseLu.cs:63-91). The column order is the static order itself:
-// the matrix is held in pivot order, which is the minimum-degree order of its pattern, the order the reference's
-// CpuSparseLuSolver takes (PowerFlow/CpuSparseLuSolver.cs:30-48).
+// the matrix is held in pivot order, which is the minimum-degree order of its pattern. On a symmetric pattern (every
+// Jacobian) that is the order the reference's CpuSparseLuSolver takes (PowerFlow/CpuSparseLuSolver.cs:30-48); on a
+// nonsymmetric bare matrix the reference breaks minimum-degree ties by its scan order of A and may order it
+// differently.
 //
 // One warp per system. The reach is a sequential depth-first search (lane 0); the column updates, the pivot search
 // and the writes of L and U are spread over the lanes. The factors live in global scratch of a fixed capacity per
