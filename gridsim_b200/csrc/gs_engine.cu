@@ -3977,8 +3977,12 @@ int gs_sparse_solve_batch(gs_ctx* ctx, int32_t count, const int32_t* n, const in
         a += n[q] + 1; z += nnz; v += n[q];
     }
     GS_CUDA(cudaSetDevice(ctx->device));
-    // per-system checks (ArgumentException per system in the reference), then systems grouped by pattern
+    // per-system checks (ArgumentException per system in the reference), then systems grouped by pattern. A system
+    // whose right-hand side is not finite is factorised all the same (with a zero right-hand side in its place), as
+    // CpuSparseLuSolver factors before it checks b (PowerFlow/CpuSparseLuSolver.cs:41-47): singular if the
+    // factorisation fails, else refused for its right-hand side; its x is never written.
     std::map<uint64_t, std::vector<int>> groups;
+    std::vector<char> rhsBad(count, 0);
     for (int q = 0; q < count; q++) {
         const int nq = n[q];
         const int* rp = rowPtr + rpOff[q];
@@ -3994,8 +3998,8 @@ int gs_sparse_solve_batch(gs_ctx* ctx, int32_t count, const int32_t* n, const in
         if (!ok) { status[q] = GS_LS_MALFORMED; continue; }
         bool finite = true;
         for (int p = 0; p < rp[nq] && finite; p++) finite = std::isfinite(values[nzOff[q] + p]);
-        for (int i = 0; i < nq && finite; i++) finite = std::isfinite(rhs[vOff[q] + i]);
         if (!finite) { status[q] = GS_LS_NON_FINITE_INPUT; continue; }
+        for (int i = 0; i < nq && !rhsBad[q]; i++) rhsBad[q] = !std::isfinite(rhs[vOff[q] + i]);
         status[q] = GS_LS_OK;
         groups[PatternHash(nq, rp, ci)].push_back(q);
     }
@@ -4031,7 +4035,8 @@ int gs_sparse_solve_batch(gs_ctx* ctx, int32_t count, const int32_t* n, const in
                 for (int c = 0; c < cnt; c++) {
                     const int q = same[done + c];
                     std::copy(values + nzOff[q], values + nzOff[q] + nnz, hv.begin() + (size_t)c * nnz);
-                    std::copy(rhs + vOff[q], rhs + vOff[q] + nq, hb.begin() + (size_t)c * nq);
+                    if (rhsBad[q]) std::fill(hb.begin() + (size_t)c * nq, hb.begin() + (size_t)(c + 1) * nq, 0.0);
+                    else std::copy(rhs + vOff[q], rhs + vOff[q] + nq, hb.begin() + (size_t)c * nq);
                 }
                 DevBuf dv, db;
                 GS_CUDA(dv.alloc(std::max<size_t>(8, hv.size() * 8)));
@@ -4055,6 +4060,7 @@ int gs_sparse_solve_batch(gs_ctx* ctx, int32_t count, const int32_t* n, const in
                     bool good = !(fl[c] & kFlagPivotPerturbed);
                     for (int i = 0; i < nq && good; i++) good = std::isfinite(y[(size_t)pinv[i] * B + c]);
                     if (!good) { redo.push_back(c); continue; }
+                    if (rhsBad[q]) { status[q] = GS_LS_NON_FINITE_INPUT; continue; }
                     for (int i = 0; i < nq; i++) x[vOff[q] + i] = y[(size_t)pinv[i] * B + c];
                 }
                 if (!redo.empty()) {
@@ -4073,6 +4079,7 @@ int gs_sparse_solve_batch(gs_ctx* ctx, int32_t count, const int32_t* n, const in
                     for (int c : redo) {
                         const int q = same[done + c];
                         if (fl[c] & kFlagPivotFailed) { status[q] = GS_LS_SINGULAR; continue; }
+                        if (rhsBad[q]) { status[q] = GS_LS_NON_FINITE_INPUT; continue; }
                         for (int i = 0; i < nq; i++) x[vOff[q] + i] = y[(size_t)pinv[i] * B + c];
                     }
                 }

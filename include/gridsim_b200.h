@@ -323,7 +323,9 @@ int gs_element_screen(gs_grid *grid, int32_t n_out, const int32_t *kind, const i
 enum gs_ls_status {
     GS_LS_OK = 0,
     GS_LS_SINGULAR = 1,        /* a pivot fell below 1e-12 x max(1, |A(k,k)|), or x is not finite: no result */
-    GS_LS_NON_FINITE_INPUT = 2,/* a value or right-hand side is not finite (the reference's ArgumentException) */
+    GS_LS_NON_FINITE_INPUT = 2,/* a value is not finite, or the right-hand side is not finite and the matrix is not
+                                * singular (the reference's ArgumentException; it factors before it checks b, so a
+                                * singular matrix reports GS_LS_SINGULAR whatever its right-hand side) */
     GS_LS_MALFORMED = 3        /* this system's CSR is malformed (offsets, a column out of range or twice) */
 };
 int gs_sparse_solve_batch(gs_ctx *ctx, int32_t count, const int32_t *n, const int32_t *row_ptr,

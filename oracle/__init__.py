@@ -263,6 +263,8 @@ def md_order(row_ptr, col_idx):
 
 
 def sparse_solve(row_ptr, col_idx, val, b):
+    """CpuSparseLuSolver.Solve (PowerFlow/CpuSparseLuSolver.cs:30-48): x, or None when the matrix is singular;
+    ValueError (the reference's ArgumentException) when it factorises but b has a non-finite entry."""
     lib = _load()
     rp = np.ascontiguousarray(row_ptr, np.int32)
     ci = np.ascontiguousarray(col_idx, np.int32)
@@ -270,6 +272,8 @@ def sparse_solve(row_ptr, col_idx, val, b):
     bb = np.ascontiguousarray(b, np.float64)
     x = np.zeros(rp.shape[0] - 1)
     rc = lib.gso_sparse_solve(rp.shape[0] - 1, _p(rp), _p(ci), _p(v), _p(bb), _p(x))
+    if rc == 2:
+        raise ValueError("Sparse LU: the right-hand side has a non-finite entry")
     return None if rc else x
 
 

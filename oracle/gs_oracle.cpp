@@ -1501,7 +1501,9 @@ int gso_md_order(int32_t n, const int32_t* rowPtr, const int32_t* colIdx, int32_
     return GS_OK;
 }
 
-// Sparse direct solve A x = b (ISparseLinearSolver via CpuSparseLuSolver). Returns 1 when singular.
+// Sparse direct solve A x = b (ISparseLinearSolver via CpuSparseLuSolver). Returns 1 when singular, 2 when the
+// matrix factorises but b has a non-finite entry (the ArgumentException CpuSparseLuSolver.cs:41-47 throws after the
+// factorisation, so a singular matrix stays 1 whatever b holds).
 int gso_sparse_solve(int32_t n, const int32_t* rowPtr, const int32_t* colIdx, const double* val, const double* b,
                      double* x) {
     Csr a;
@@ -1511,6 +1513,9 @@ int gso_sparse_solve(int32_t n, const int32_t* rowPtr, const int32_t* colIdx, co
     a.val.assign(val, val + rowPtr[n]);
     CpuSparseLuSolver s;
     std::vector<double> bv(b, b + n), xv;
+    bool bFinite = true;
+    for (double v : bv) bFinite = bFinite && std::isfinite(v);
+    if (!bFinite) return s.Solve(a, std::vector<double>(n, 0.0), xv) ? 2 : 1;
     if (!s.Solve(a, bv, xv)) return 1;
     for (int i = 0; i < n; i++) x[i] = xv[i];
     return GS_OK;

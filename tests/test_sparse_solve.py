@@ -194,3 +194,48 @@ def test_oracle_near_singular_row_in_small_units_is_refused():
     """Gr044RowRelativePivotFloorTests.cs:170-176: row 1 has scale 1 and its pivot 1e-13 is below its own 1e-12
     floor."""
     assert oracle.sparse_solve(*_csr_of([[1e6, 0.0], [1.0, 1e-13]]), [1.0, 1.0]) is None
+
+
+NR_DENSE = np.array([[4.0, -1.0, 0.5], [-1.0, 5.0, -2.0], [0.5, -2.0, 6.0]])
+NR_RHS = np.array([1.0, -2.5, 0.75])
+
+
+@pytest.mark.parametrize("bad", [np.nan, np.inf, -np.inf])
+def test_oracle_refuses_a_non_finite_right_hand_side(bad):
+    """NonFiniteRightHandSideTests.cs:43-51: the sparse LU refuses a NaN or infinite right-hand side (an
+    ArgumentException after the factorisation) instead of returning a non-finite solution."""
+    b = NR_RHS.copy()
+    b[2] = bad
+    with pytest.raises(ValueError):
+        oracle.sparse_solve(*_csr_of(NR_DENSE), b)
+
+
+def test_oracle_singular_matrix_returns_none_whatever_its_right_hand_side():
+    """NonFiniteRightHandSideTests.cs:53-66: the factorisation comes first, so a singular matrix returns null even
+    with a NaN in b; and the finite solve is unchanged."""
+    assert oracle.sparse_solve(*_csr_of([[1.0, 1.0], [1.0, 1.0]]), [np.nan, 1.0]) is None
+    x = oracle.sparse_solve(*_csr_of(NR_DENSE), NR_RHS)
+    assert np.max(np.abs(NR_DENSE @ x - NR_RHS)) < 1e-14
+
+
+@pytest.mark.gpu
+def test_non_finite_right_hand_side_is_checked_after_the_factorisation():
+    """The same contract through the batched solve: in one call a singular matrix with a NaN right-hand side gives no
+    result and no error (null), a regular one with an infinite right-hand side its refusal (ValueError), and the
+    systems beside them are solved as alone; the bad systems' x are not written."""
+    from gridsim_b200.engine import CudaSparseLinearSolver
+    sing = _csr_of([[1.0, 1.0], [1.0, 1.0]])
+    reg2 = _csr_of([[3.0, 1.0], [1.0, 2.0]])
+    good = _csr_of(NR_DENSE)
+    b_nan = np.array([np.nan, 1.0])
+    b_inf = np.array([1.0, np.inf])
+    solver = CudaSparseLinearSolver()
+    errors = [None] * 4
+    xs = solver.solve_batch([sing, reg2, good, reg2], [b_nan, b_inf, NR_RHS, np.array([4.0, 3.0])], errors)
+    assert xs[0] is None and errors[0] is None
+    assert xs[1] is None and isinstance(errors[1], ValueError)
+    assert errors[2] is None and np.max(np.abs(NR_DENSE @ xs[2] - NR_RHS)) < 1e-12
+    assert errors[3] is None and np.allclose(xs[3], [1.0, 1.0], rtol=0, atol=1e-14)
+    with pytest.raises(ValueError):
+        oracle.sparse_solve(*reg2, b_inf)
+    assert oracle.sparse_solve(*sing, b_nan) is None
